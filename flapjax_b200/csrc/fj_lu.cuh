@@ -1,0 +1,30 @@
+// fj_lu.cuh -- dense LU with partial pivoting, solves and FP64 iterative refinement.
+#pragma once
+
+#include "fj_common.cuh"
+
+namespace fj {
+
+// Row-major n x n, in place (L unit-lower below the diagonal, U on and above), 0-based
+// pivot rows in piv (row i was swapped with piv[i], applied in increasing i, as LAPACK
+// getrf).  *d_info (device int) receives 0 or 1 + the first zero-pivot column.
+int lu_factor64(double* a, int n, int32_t* piv, int* d_info, cudaStream_t s);
+int lu_factor32(float* a, int n, int32_t* piv, int* d_info, cudaStream_t s);
+
+// getrs: b <- A^-1 b using the factors (single right-hand side, in place).
+int lu_solve64(const double* lu, int n, const int32_t* piv, double* b, cudaStream_t s);
+
+// X <- A^-1 (row-major n x n) from FP32 factors.
+int lu_inverse32(const float* lu, int n, const int32_t* piv, float* x, cudaStream_t s);
+
+// Round an FP64 matrix to FP32.
+int convert64to32(const double* a, float* b, int64_t count, cudaStream_t s);
+
+// Mixed solve, given FP64 A and the FP32 inverse X of (a matrix close to) A:
+//   x = X b;  repeat n_iter times: r = b - A x (FP64);  x += X r.
+// Writes ||b - A x||_inf / ||b||_inf of the final x to *d_resid.
+// r_buf: n doubles of scratch.
+int refine_solve(const double* a, const float* xinv, int n, const double* b, double* x,
+                 double* r_buf, double* d_resid, int n_iter, cudaStream_t s);
+
+}  // namespace fj

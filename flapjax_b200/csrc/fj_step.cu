@@ -1,0 +1,1255 @@
+// fj_step.cu -- one UVLM time step on the device, the case driver and the C ABI.
+//
+// A dynamic step at slot i (case_solve -> base_solve_from_grid, aero/uvlm.py:824-1215):
+//   1. node frames -> lattices: zeta_b(i), zeta_b_dot(i), zeta_b(i-1)   (uvlm.py:537-621)
+//      and collocation points / area normals / c_dot                     (uvlm.py:885-893)
+//   2. free wake: v at wake vertices of slot i-1 from bound(i-1) + wake(i-1)
+//      (uvlm.py:914-929); shed the TE row and convect (aero/utils.py:400-500)
+//   3. AIC of the bound lattice (aero/aic.py:137-187)
+//   4. RHS = -((U - c_dot + v_wake) . n)                                 (uvlm.py:961-983)
+//   5. solve                                                               (uvlm.py:985)
+//   6. forces: v at filament midpoints from bound(i) + wake(i), Kutta-Joukowski per
+//      filament, split to vertices                                        (aero/utils.py:126-223)
+//   7. gamma_dot filter, unsteady force, strip alpha, force total         (uvlm.py:1048-1103)
+// Every array is addressed as field + slot * slot_size, surfaces concatenated.
+#include <cmath>
+#include <cstring>
+#include <algorithm>
+#include <vector>
+
+#include "fj_aic.cuh"
+#include "fj_lu.cuh"
+#include "fj_vind.cuh"
+
+namespace fj {
+
+const char* last_error();
+int biot_savart_pairs(const double* x, const double* y, int64_t n, int kernel, double r_cut, double* out,
+                      cudaStream_t s);
+
+// ------------------------------------------------------------------------------------
+// Layout of the per-surface blocks inside one time slot
+// ------------------------------------------------------------------------------------
+struct Layout {
+    int n_surf;
+    int m[FJ_MAX_SURF], n[FJ_MAX_SURF], ms[FJ_MAX_SURF];
+    int64_t vo[FJ_MAX_SURF + 1];   // bound vertices
+    int64_t po[FJ_MAX_SURF + 1];   // bound panels
+    int64_t wvo[FJ_MAX_SURF + 1];  // wake vertices
+    int64_t wpo[FJ_MAX_SURF + 1];  // wake panels
+    int64_t so[FJ_MAX_SURF + 1];   // strips
+    int64_t dofo[FJ_MAX_SURF + 1]; // dof mapping entries (n+1)
+    int64_t fo[FJ_MAX_SURF + 1];   // bound filaments m(n+1) + (m+1)n
+    int64_t wto[FJ_MAX_SURF + 1];  // free-wake targets m_star(n+1)
+    int n_nodes;                   // beam nodes in the frame arrays
+};
+
+static Layout make_layout(const fj_case_config& c) {
+    Layout L;
+    memset(&L, 0, sizeof(L));
+    L.n_surf = c.n_surf;
+    L.n_nodes = c.n_nodes;
+    for (int s = 0; s < c.n_surf; ++s) {
+        const int m = c.m[s], n = c.n[s], ms = c.m_star[s];
+        L.m[s] = m;
+        L.n[s] = n;
+        L.ms[s] = ms;
+        L.vo[s + 1] = L.vo[s] + (int64_t)(m + 1) * (n + 1);
+        L.po[s + 1] = L.po[s] + (int64_t)m * n;
+        L.wvo[s + 1] = L.wvo[s] + (int64_t)(ms + 1) * (n + 1);
+        L.wpo[s + 1] = L.wpo[s] + (int64_t)ms * n;
+        L.so[s + 1] = L.so[s] + n;
+        L.dofo[s + 1] = L.dofo[s] + n + 1;
+        L.fo[s + 1] = L.fo[s] + (int64_t)m * (n + 1) + (int64_t)(m + 1) * n;
+        L.wto[s + 1] = L.wto[s] + (int64_t)ms * (n + 1);
+    }
+    return L;
+}
+
+__device__ __forceinline__ int find_surf(const int64_t* off, int n_surf, int64_t idx) {
+    int s = 0;
+    while (s + 1 < n_surf && idx >= off[s + 1]) ++s;
+    return s;
+}
+
+// Background flow, aero/flowfields.py:87-181.
+__device__ __forceinline__ void flow_eval(const fj_flowfield& f, const double x[3], double t, double u[3]) {
+    if (f.kind == FJ_FLOW_ONE_MINUS_COSINE) {
+        double rx = x[0] - f.gust_x0[0], ry = x[1] - f.gust_x0[1], rz = x[2] - f.gust_x0[2];
+        if (f.relative_motion) {
+            rx -= f.u_inf[0] * t;
+            ry -= f.u_inf[1] * t;
+            rz -= f.u_inf[2] * t;
+        }
+        const double gx = rx * f.gust_travel_dir[0] + ry * f.gust_travel_dir[1] + rz * f.gust_travel_dir[2];
+        if (gx > 0.0 && gx < 2.0 * f.gust_length) {
+            const double w = 1.0 - cos(kPi * gx / f.gust_length);
+            u[0] = f.gust_amplitude_dir[0] * f.gust_amplitude * 0.5 * w;
+            u[1] = f.gust_amplitude_dir[1] * f.gust_amplitude * 0.5 * w;
+            u[2] = f.gust_amplitude_dir[2] * f.gust_amplitude * 0.5 * w;
+        } else {
+            u[0] = u[1] = u[2] = 0.0;
+        }
+        if (f.relative_motion) {
+            u[0] += f.u_inf[0];
+            u[1] += f.u_inf[1];
+            u[2] += f.u_inf[2];
+        }
+    } else {
+        if (f.relative_motion) {
+            u[0] = f.u_inf[0];
+            u[1] = f.u_inf[1];
+            u[2] = f.u_inf[2];
+        } else {
+            u[0] = u[1] = u[2] = 0.0;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// 1. geometry
+// ------------------------------------------------------------------------------------
+// se3.vect_product (algebra/se3.py:209-216): hg[:3,:3] @ x + hg[:3,3]
+__device__ __forceinline__ void se3_apply(const double* hg, const double x[3], double o[3]) {
+#pragma unroll
+    for (int r = 0; r < 3; ++r) o[r] = (hg[r * 4 + 0] * x[0] + hg[r * 4 + 1] * x[1] + hg[r * 4 + 2] * x[2]) + hg[r * 4 + 3];
+}
+
+// hg_to_zeta_b / hg_dot_to_zeta_b_dot (aero/uvlm.py:537-621), one thread per vertex.
+__global__ void geom_vertices_kernel(Layout L, const double* __restrict__ zeta0, const int32_t* __restrict__ dof,
+                                     const double* __restrict__ hg_n, const double* __restrict__ hgd_n,
+                                     const double* __restrict__ hg_nm1, double* __restrict__ zeta_n,
+                                     double* __restrict__ zeta_dot_n, double* __restrict__ zeta_nm1,
+                                     double* __restrict__ t_slot, double t_prev, double dt) {
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v == 0 && t_slot != nullptr) *t_slot = t_prev + dt;  // case_solve, uvlm.py:1158-1161
+    if (v >= L.vo[L.n_surf]) return;
+    const int s = find_surf(L.vo, L.n_surf, v);
+    const int64_t lv = v - L.vo[s];
+    const int j = (int)(lv % (L.n[s] + 1));
+    // the host validates the mapping; the clamp only keeps a bad entry in bounds
+    const int node = min(max(dof[L.dofo[s] + j], 0), L.n_nodes - 1);
+    const double x0[3] = {zeta0[v * 3], zeta0[v * 3 + 1], zeta0[v * 3 + 2]};
+    double o[3];
+    se3_apply(hg_n + (int64_t)node * 16, x0, o);
+    zeta_n[v * 3] = o[0];
+    zeta_n[v * 3 + 1] = o[1];
+    zeta_n[v * 3 + 2] = o[2];
+    if (zeta_dot_n != nullptr) {
+        if (hgd_n != nullptr) {
+            se3_apply(hgd_n + (int64_t)node * 16, x0, o);
+        } else {
+            o[0] = o[1] = o[2] = 0.0;
+        }
+        zeta_dot_n[v * 3] = o[0];
+        zeta_dot_n[v * 3 + 1] = o[1];
+        zeta_dot_n[v * 3 + 2] = o[2];
+    }
+    if (zeta_nm1 != nullptr) {
+        se3_apply(hg_nm1 + (int64_t)node * 16, x0, o);
+        zeta_nm1[v * 3] = o[0];
+        zeta_nm1[v * 3 + 1] = o[1];
+        zeta_nm1[v * 3 + 2] = o[2];
+    }
+}
+
+// compute_surf_c / compute_surf_nc (aero/utils.py:87-105) and c_dot (uvlm.py:891-893).
+__global__ void geom_panels_kernel(Layout L, const double* __restrict__ zeta, const double* __restrict__ zeta_dot,
+                                   double* __restrict__ c, double* __restrict__ nc, double* __restrict__ c_dot) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= L.po[L.n_surf]) return;
+    const int s = find_surf(L.po, L.n_surf, p);
+    const int64_t lp = p - L.po[s];
+    const int n = L.n[s];
+    const int k = (int)(lp / n), l = (int)(lp % n);
+    const double* z = zeta + L.vo[s] * 3;
+    const double* z00 = z + ((int64_t)k * (n + 1) + l) * 3;
+    const double* z01 = z00 + 3;
+    const double* z10 = z00 + (n + 1) * 3;
+    const double* z11 = z10 + 3;
+    for (int d = 0; d < 3; ++d) {
+        // neighbour_average over axis 0 then axis 1 (algebra/array_utils.py:106-136)
+        const double a0 = 0.5 * (z00[d] + z10[d]);
+        const double a1 = 0.5 * (z01[d] + z11[d]);
+        c[p * 3 + d] = 0.5 * (a0 + a1);
+    }
+    const double d1[3] = {z11[0] - z00[0], z11[1] - z00[1], z11[2] - z00[2]};
+    const double d2[3] = {z10[0] - z01[0], z10[1] - z01[1], z10[2] - z01[2]};
+    nc[p * 3 + 0] = d1[1] * d2[2] - d1[2] * d2[1];
+    nc[p * 3 + 1] = d1[2] * d2[0] - d1[0] * d2[2];
+    nc[p * 3 + 2] = d1[0] * d2[1] - d1[1] * d2[0];
+    if (c_dot != nullptr) {
+        const double* w = zeta_dot + L.vo[s] * 3;
+        const double* w00 = w + ((int64_t)k * (n + 1) + l) * 3;
+        const double* w01 = w00 + 3;
+        const double* w10 = w00 + (n + 1) * 3;
+        const double* w11 = w10 + 3;
+        for (int d = 0; d < 3; ++d) {
+            const double a0 = 0.5 * (w00[d] + w10[d]);
+            const double a1 = 0.5 * (w01[d] + w11[d]);
+            c_dot[p * 3 + d] = 0.5 * (a0 + a1);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// 2. wake
+// ------------------------------------------------------------------------------------
+// initialise_wake (uvlm.py:662-689): TE + cumsum(dt |U|) along the freestream direction.
+// `hs_len` > 0 builds the 2-row horseshoe wake instead (uvlm.py:642-660).
+__global__ void init_wake_kernel(Layout L, const double* __restrict__ zeta_b, fj_flowfield f, double dt,
+                                 double hs_len, double* __restrict__ zeta_w, int rows_override) {
+    // rows_override > 0: that many rows for every surface that has a wake, 0 rows
+    // (the TE only) for surfaces with m_star == 0 (uvlm.py:652-660)
+    int64_t tot = 0;
+    for (int q = 0; q < L.n_surf; ++q) {
+        const int rows = rows_override > 0 ? (L.ms[q] == 0 ? 0 : rows_override) : L.ms[q];
+        tot += (int64_t)(rows + 1) * (L.n[q] + 1);
+    }
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= tot) return;
+    int s = 0;
+    int64_t base = 0, nxt = 0;
+    for (s = 0; s < L.n_surf; ++s) {
+        const int rows = rows_override > 0 ? (L.ms[s] == 0 ? 0 : rows_override) : L.ms[s];
+        nxt = base + (int64_t)(rows + 1) * (L.n[s] + 1);
+        if (v < nxt) break;
+        base = nxt;
+    }
+    const int64_t lv = v - base;
+    const int n = L.n[s];
+    const int r = (int)(lv / (n + 1)), l = (int)(lv % (n + 1));
+    const double* te = zeta_b + (L.vo[s] + (int64_t)L.m[s] * (n + 1) + l) * 3;
+    const double umag = sqrt(f.u_inf[0] * f.u_inf[0] + f.u_inf[1] * f.u_inf[1] + f.u_inf[2] * f.u_inf[2]);
+    double sdist;
+    if (hs_len > 0.0) {
+        sdist = r == 0 ? 0.0 : hs_len;
+    } else {
+        sdist = 0.0;  // cumsum of equal increments, summed in order as jnp.cumsum
+        const double inc = 1.0 * dt * umag;
+        for (int q = 0; q < r; ++q) sdist += inc;
+    }
+    for (int d = 0; d < 3; ++d) zeta_w[v * 3 + d] = te[d] + sdist * (f.u_inf[d] / umag);
+}
+
+// Rows 0..m_star-1 of every surface's wake, packed as the free-wake target list.
+__global__ void gather_wake_targets_kernel(Layout L, const double* __restrict__ zeta_w, double* __restrict__ out) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= L.wto[L.n_surf]) return;
+    const int s = find_surf(L.wto, L.n_surf, t);
+    const int64_t src = L.wvo[s] + (t - L.wto[s]);
+    out[t * 3] = zeta_w[src * 3];
+    out[t * 3 + 1] = zeta_w[src * 3 + 1];
+    out[t * 3 + 2] = zeta_w[src * 3 + 2];
+}
+
+// propagate_surf_wake, uniform branch (aero/utils.py:427-450): shed the TE row and
+// circulation of step n-1, drop the last row, convect the rest by dt * (U + v_ind).
+__global__ void wake_shed_kernel(Layout L, const double* __restrict__ zeta_b_n, const double* __restrict__ zeta_w_nm1,
+                                 const double* __restrict__ gamma_b_nm1, const double* __restrict__ gamma_w_nm1,
+                                 const double* __restrict__ v_ind, fj_flowfield f, const double* __restrict__ t_slot,
+                                 double dt, double* __restrict__ zeta_w_n, double* __restrict__ gamma_w_n) {
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t nv = L.wvo[L.n_surf];
+    const double t = *t_slot;
+    if (v < nv) {
+        const int s = find_surf(L.wvo, L.n_surf, v);
+        const int64_t lv = v - L.wvo[s];
+        const int n = L.n[s];
+        const int r = (int)(lv / (n + 1)), l = (int)(lv % (n + 1));
+        if (r == 0) {
+            const double* te = zeta_b_n + (L.vo[s] + (int64_t)L.m[s] * (n + 1) + l) * 3;
+            zeta_w_n[v * 3] = te[0];
+            zeta_w_n[v * 3 + 1] = te[1];
+            zeta_w_n[v * 3 + 2] = te[2];
+        } else {
+            const int64_t src = L.wvo[s] + (int64_t)(r - 1) * (n + 1) + l;
+            const double x[3] = {zeta_w_nm1[src * 3], zeta_w_nm1[src * 3 + 1], zeta_w_nm1[src * 3 + 2]};
+            double u[3];
+            flow_eval(f, x, t, u);
+            if (v_ind != nullptr) {
+                const int64_t ti = L.wto[s] + (int64_t)(r - 1) * (n + 1) + l;
+                u[0] += v_ind[ti * 3];
+                u[1] += v_ind[ti * 3 + 1];
+                u[2] += v_ind[ti * 3 + 2];
+            }
+            zeta_w_n[v * 3] = x[0] + dt * u[0];
+            zeta_w_n[v * 3 + 1] = x[1] + dt * u[1];
+            zeta_w_n[v * 3 + 2] = x[2] + dt * u[2];
+        }
+    }
+    const int64_t g = v - nv;
+    if (g >= 0 && g < L.wpo[L.n_surf]) {
+        const int s = find_surf(L.wpo, L.n_surf, g);
+        const int64_t lg = g - L.wpo[s];
+        const int n = L.n[s];
+        const int r = (int)(lg / n), l = (int)(lg % n);
+        gamma_w_n[g] = r == 0 ? gamma_b_nm1[L.po[s] + (int64_t)(L.m[s] - 1) * n + l]
+                              : gamma_w_nm1[L.wpo[s] + (int64_t)(r - 1) * n + l];
+    }
+}
+
+// Static wake circulation: broadcast of the TE row (uvlm.py:995-1012).
+__global__ void static_gamma_w_kernel(Layout L, const double* __restrict__ gamma_b, double* __restrict__ gamma_w,
+                                      int rows_override) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t base = 0;
+    for (int s = 0; s < L.n_surf; ++s) {
+        const int rows = rows_override >= 0 ? (L.ms[s] == 0 ? 0 : rows_override) : L.ms[s];
+        const int64_t cnt = (int64_t)rows * L.n[s];
+        if (g < base + cnt) {
+            const int l = (int)((g - base) % L.n[s]);
+            gamma_w[g] = gamma_b[L.po[s] + (int64_t)(L.m[s] - 1) * L.n[s] + l];
+            return;
+        }
+        base += cnt;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// 4. right-hand side (uvlm.py:961-985): b = -((U(c) - c_dot + v_wake) . n)
+// ------------------------------------------------------------------------------------
+__global__ void rhs_kernel(int64_t np, const double* __restrict__ c, const double* __restrict__ c_dot,
+                           const double* __restrict__ nc, const double* __restrict__ v, fj_flowfield f,
+                           const double* __restrict__ t_slot, double t_fixed, double* __restrict__ b) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    const double t = t_slot != nullptr ? *t_slot : t_fixed;
+    const double x[3] = {c[p * 3], c[p * 3 + 1], c[p * 3 + 2]};
+    double u[3];
+    flow_eval(f, x, t, u);
+    if (c_dot != nullptr) {
+        u[0] -= c_dot[p * 3];
+        u[1] -= c_dot[p * 3 + 1];
+        u[2] -= c_dot[p * 3 + 2];
+    }
+    if (v != nullptr) {
+        u[0] += v[p * 3];
+        u[1] += v[p * 3 + 1];
+        u[2] += v[p * 3 + 2];
+    }
+    b[p] = -(u[0] * nc[p * 3] + u[1] * nc[p * 3 + 1] + u[2] * nc[p * 3 + 2]);
+}
+
+// ------------------------------------------------------------------------------------
+// 6. forces (aero/utils.py:126-223)
+// ------------------------------------------------------------------------------------
+// Filament f of surface s: f < m(n+1): chordwise (k,l)->(k+1,l); else spanwise (k,l)->(k,l+1).
+__device__ __forceinline__ void filament_ends(const Layout& L, int s, int64_t lf, int& k0, int& l0, int& k1,
+                                              int& l1, bool& chord) {
+    const int m = L.m[s], n = L.n[s];
+    const int64_t nm = (int64_t)m * (n + 1);
+    if (lf < nm) {
+        chord = true;
+        k0 = (int)(lf / (n + 1));
+        l0 = (int)(lf % (n + 1));
+        k1 = k0 + 1;
+        l1 = l0;
+    } else {
+        chord = false;
+        const int64_t t = lf - nm;
+        k0 = (int)(t / n);
+        l0 = (int)(t % n);
+        k1 = k0;
+        l1 = l0 + 1;
+    }
+}
+
+__global__ void force_targets_kernel(Layout L, const double* __restrict__ zeta, double* __restrict__ out) {
+    const int64_t fi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (fi >= L.fo[L.n_surf]) return;
+    const int s = find_surf(L.fo, L.n_surf, fi);
+    int k0, l0, k1, l1;
+    bool chord;
+    filament_ends(L, s, fi - L.fo[s], k0, l0, k1, l1, chord);
+    const int n = L.n[s];
+    const double* a = zeta + (L.vo[s] + (int64_t)k0 * (n + 1) + l0) * 3;
+    const double* b = zeta + (L.vo[s] + (int64_t)k1 * (n + 1) + l1) * 3;
+    for (int d = 0; d < 3; ++d) out[fi * 3 + d] = 0.5 * (a[d] + b[d]);
+}
+
+__global__ void force_filament_kernel(Layout L, const double* __restrict__ zeta, const double* __restrict__ zeta_dot,
+                                      const double* __restrict__ gamma_b, const double* __restrict__ gamma_w,
+                                      const double* __restrict__ targets, const double* __restrict__ v,
+                                      fj_flowfield f, const double* __restrict__ t_slot, double t_fixed,
+                                      double* __restrict__ ffil) {
+    const int64_t fi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (fi >= L.fo[L.n_surf]) return;
+    const double t = t_slot != nullptr ? *t_slot : t_fixed;
+    const int s = find_surf(L.fo, L.n_surf, fi);
+    int k0, l0, k1, l1;
+    bool chord;
+    filament_ends(L, s, fi - L.fo[s], k0, l0, k1, l1, chord);
+    const int m = L.m[s], n = L.n[s];
+    const double* gb = gamma_b + L.po[s];
+    const double* a = zeta + (L.vo[s] + (int64_t)k0 * (n + 1) + l0) * 3;
+    const double* b = zeta + (L.vo[s] + (int64_t)k1 * (n + 1) + l1) * 3;
+    const double x[3] = {targets[fi * 3], targets[fi * 3 + 1], targets[fi * 3 + 2]};
+    double u[3];
+    flow_eval(f, x, t, u);
+    double vr[3];
+    for (int d = 0; d < 3; ++d) {
+        const double mpd = zeta_dot != nullptr
+                               ? 0.5 * (zeta_dot[(L.vo[s] + (int64_t)k0 * (n + 1) + l0) * 3 + d] +
+                                        zeta_dot[(L.vo[s] + (int64_t)k1 * (n + 1) + l1) * 3 + d])
+                               : 0.0;
+        vr[d] = (u[d] + v[fi * 3 + d]) - mpd;
+    }
+    double g;
+    if (chord) {  // gamma_chordwise[:, :-1] = G; gamma_chordwise[:, 1:] += -G
+        g = 0.0;
+        if (l0 < n) g = gb[(int64_t)k0 * n + l0];
+        if (l0 >= 1) g += -gb[(int64_t)k0 * n + l0 - 1];
+    } else {      // gamma_spanwise[:-1, :] = -G; gamma_spanwise[1:, :] += G; [-1] += -Gw[0]
+        g = 0.0;
+        if (k0 < m) g = -gb[(int64_t)k0 * n + l0];
+        if (k0 >= 1) g += gb[(int64_t)(k0 - 1) * n + l0];
+        if (k0 == m && gamma_w != nullptr && L.ms[s] > 0) g += -gamma_w[L.wpo[s] + l0];
+    }
+    const double r[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+    const double cr[3] = {vr[1] * r[2] - vr[2] * r[1], vr[2] * r[0] - vr[0] * r[2], vr[0] * r[1] - vr[1] * r[0]};
+    for (int d = 0; d < 3; ++d) ffil[fi * 3 + d] = f.rho * (g * cr[d]);
+}
+
+// ------------------------------------------------------------------------------------
+// 7. post-processing
+// ------------------------------------------------------------------------------------
+// compute_gamma_dot (uvlm.py:691-715)
+__global__ void gamma_dot_kernel(int64_t np, const double* __restrict__ gb_n, const double* __restrict__ gb_nm1,
+                                 const double* __restrict__ gbd_nm1, double dt, double relax,
+                                 double* __restrict__ gbd_n) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    const double cur = (gb_n[p] - gb_nm1[p]) / dt;
+    gbd_n[p] = cur * relax + gbd_nm1[p] * (1.0 - relax);
+}
+
+// split_to_vertex of the filament forces (aero/utils.py:220-222) and of
+// rho * gamma_dot * n (uvlm.py:1093-1103), algebra/array_utils.py:332-367.
+__global__ void vertex_forces_kernel(Layout L, const double* __restrict__ ffil, const double* __restrict__ gbd,
+                                     const double* __restrict__ nc, double rho, double* __restrict__ f_steady,
+                                     double* __restrict__ f_unsteady) {
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= L.vo[L.n_surf]) return;
+    const int s = find_surf(L.vo, L.n_surf, v);
+    const int64_t lv = v - L.vo[s];
+    const int m = L.m[s], n = L.n[s];
+    const int k = (int)(lv / (n + 1)), l = (int)(lv % (n + 1));
+    const double* fc = ffil + L.fo[s] * 3;                          // (m, n+1, 3)
+    const double* fs = ffil + (L.fo[s] + (int64_t)m * (n + 1)) * 3;  // (m+1, n, 3)
+    for (int d = 0; d < 3; ++d) {
+        double a = 0.0;  // split_to_vertex(f_chordwise, 0)
+        if (k < m) a = 0.5 * fc[((int64_t)k * (n + 1) + l) * 3 + d];
+        if (k >= 1) a += 0.5 * fc[((int64_t)(k - 1) * (n + 1) + l) * 3 + d];
+        double b = 0.0;  // split_to_vertex(f_spanwise, 1)
+        if (l < n) b = 0.5 * fs[((int64_t)k * n + l) * 3 + d];
+        if (l >= 1) b += 0.5 * fs[((int64_t)k * n + l - 1) * 3 + d];
+        f_steady[v * 3 + d] = a + b;
+    }
+    if (f_unsteady == nullptr) return;
+    for (int d = 0; d < 3; ++d) {
+        double out = 0.0;
+        if (gbd != nullptr) {
+            const double* g = gbd + L.po[s];
+            const double* nn = nc + L.po[s] * 3;
+            // split along axis 0 into (m+1, n), then along axis 1 into (m+1, n+1)
+            auto s0 = [&](int kk, int ll) -> double {
+                double r = 0.0;
+                if (kk < m) r = 0.5 * (rho * g[(int64_t)kk * n + ll] * nn[((int64_t)kk * n + ll) * 3 + d]);
+                if (kk >= 1) r += 0.5 * (rho * g[(int64_t)(kk - 1) * n + ll] * nn[((int64_t)(kk - 1) * n + ll) * 3 + d]);
+                return r;
+            };
+            if (l < n) out = 0.5 * s0(k, l);
+            if (l >= 1) out += 0.5 * s0(k, l - 1);
+        }
+        f_unsteady[v * 3 + d] = out;
+    }
+}
+
+// strip_alpha (aero/utils.py:226-273), one thread per strip.
+__global__ void strip_alpha_kernel(Layout L, const double* __restrict__ zeta, const double* __restrict__ f_steady,
+                                   fj_flowfield f, const double* __restrict__ t_slot, double t_fixed,
+                                   double* __restrict__ alpha) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= L.so[L.n_surf]) return;
+    const double t = t_slot != nullptr ? *t_slot : t_fixed;
+    const int s = find_surf(L.so, L.n_surf, j);
+    const int l = (int)(j - L.so[s]);
+    const int m = L.m[s], n = L.n[s];
+    const double* z = zeta + L.vo[s] * 3;
+    const double* le0 = z + (int64_t)l * 3;
+    const double* le1 = le0 + 3;
+    const double* te0 = z + ((int64_t)m * (n + 1) + l) * 3;
+    const double* te1 = te0 + 3;
+    double le[3], te[3], chord[3], span[3], mid[3];
+    for (int d = 0; d < 3; ++d) {
+        le[d] = 0.5 * (le0[d] + le1[d]);
+        te[d] = 0.5 * (te0[d] + te1[d]);
+        chord[d] = te[d] - le[d];
+        span[d] = 0.5 * ((le1[d] + te1[d]) - (le0[d] + te0[d]));
+        mid[d] = 0.5 * (le[d] + te[d]);
+    }
+    const double c_len = sqrt(chord[0] * chord[0] + chord[1] * chord[1] + chord[2] * chord[2]);
+    const double b_len = sqrt(span[0] * span[0] + span[1] * span[1] + span[2] * span[2]);
+    const double es[3] = {span[0] / b_len, span[1] / b_len, span[2] / b_len};
+    double vr[3];
+    flow_eval(f, mid, t, vr);
+    const double vmag2 = vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2];
+    double el[3] = {vr[1] * es[2] - vr[2] * es[1], vr[2] * es[0] - vr[0] * es[2], vr[0] * es[1] - vr[1] * es[0]};
+    const double eln = sqrt(el[0] * el[0] + el[1] * el[1] + el[2] * el[2]);
+    el[0] /= eln;
+    el[1] /= eln;
+    el[2] /= eln;
+    double fst[3] = {0.0, 0.0, 0.0};
+    const double* fs = f_steady + L.vo[s] * 3;
+    for (int k = 0; k <= m; ++k)
+        for (int d = 0; d < 3; ++d)
+            fst[d] += 0.5 * (fs[((int64_t)k * (n + 1) + l) * 3 + d] + fs[((int64_t)k * (n + 1) + l + 1) * 3 + d]);
+    const double q = 0.5 * f.rho * vmag2;
+    const double cl = (fst[0] * el[0] + fst[1] * el[1] + fst[2] * el[2]) / (q * c_len * b_len);
+    alpha[j] = cl / (2.0 * kPi);
+}
+
+// Sum over vertices of f_steady + f_unsteady (one CTA, fixed order).
+__global__ void force_total_kernel(int64_t nv, const double* __restrict__ fs, const double* __restrict__ fu,
+                                   double* __restrict__ out) {
+    __shared__ double sh[3][256];
+    double a[3] = {0.0, 0.0, 0.0};
+    for (int64_t v = threadIdx.x; v < nv; v += blockDim.x)
+        for (int d = 0; d < 3; ++d) a[d] += fs[v * 3 + d] + (fu != nullptr ? fu[v * 3 + d] : 0.0);
+    for (int d = 0; d < 3; ++d) sh[d][threadIdx.x] = a[d];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int d = 0; d < 3; ++d) sh[d][threadIdx.x] += sh[d][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int d = 0; d < 3; ++d) out[d] = sh[d][0];
+}
+
+__global__ void changed_kernel(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
+                               int* __restrict__ flag) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && a[i] != b[i]) *flag = 1;
+}
+
+__global__ void max_reduce_kernel(const double* __restrict__ x, int n, double* __restrict__ out) {
+    __shared__ double sh[256];
+    double m = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double v = x[i];
+        m = (v != v) ? INFINITY : fmax(m, v);
+    }
+    sh[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sh[0];
+}
+
+static inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
+
+// ------------------------------------------------------------------------------------
+// Case plan: layout, workspace carve-up, validation
+// ------------------------------------------------------------------------------------
+struct Plan {
+    fj_case_config cfg;
+    Layout L;
+    int nb;                      // AIC order
+    int64_t sz_zb, sz_zw, sz_pan, sz_gw, sz_strip;  // per-slot element counts
+    int64_t max_targets, max_stream;
+    int64_t part_elems;
+    size_t ws_needed;    // bytes of workspace this plan carves
+    // workspace
+    int* flags;          // [0] lu info, [1] geometry changed
+    double* zeta_nm1;    // bound vertices at n-1
+    double* c_dot;
+    double* targets;
+    double* v;
+    double* part;
+    void* stream;
+    double* hs_zw;       // horseshoe wake scratch
+    double* hs_gw;
+    double* a64;         // FP64 AIC (factored in place on the FP64 path)
+    float* a32;          // FP32 LU factors (mixed)
+    float* x32;          // FP32 inverse (mixed)
+    double* zeta_ref;    // lattice of the cached AIC (mixed)
+    int32_t* piv;
+    double* rhs;
+    double* r;
+    double* resid;       // per-slot refinement residual (mixed)
+    double* ffil;
+    double* scalar;      // 1 double scratch
+};
+
+static int validate(const fj_case_config* c) {
+    if (c == nullptr) return fail(FJ_ERR_SHAPE, "config is NULL");
+    if (c->n_surf < 1 || c->n_surf > FJ_MAX_SURF) return fail(FJ_ERR_SHAPE, "n_surf=%d not in [1,%d]", c->n_surf, FJ_MAX_SURF);
+    for (int s = 0; s < c->n_surf; ++s) {
+        if (c->m[s] < 1 || c->n[s] < 1 || c->m_star[s] < 0)
+            return fail(FJ_ERR_SHAPE, "surface %d: m=%d n=%d m_star=%d", s, c->m[s], c->n[s], c->m_star[s]);
+    }
+    if (c->n_tstep < 1) return fail(FJ_ERR_SHAPE, "n_tstep=%d", c->n_tstep);
+    if (c->n_nodes < 1) return fail(FJ_ERR_SHAPE, "n_nodes=%d", c->n_nodes);
+    if (!(c->dt > 0.0) || !std::isfinite(c->dt)) return fail(FJ_ERR_SHAPE, "dt=%g must be positive", c->dt);
+    if (c->kernel < 0 || c->kernel > 2) return fail(FJ_ERR_UNSUPPORTED, "kernel id %d", c->kernel);
+    if (c->precision != FJ_PREC_FP64 && c->precision != FJ_PREC_MIXED)
+        return fail(FJ_ERR_UNSUPPORTED, "precision id %d", c->precision);
+    if (c->precision == FJ_PREC_MIXED && c->kernel == FJ_KERNEL_PLAIN)
+        return fail(FJ_ERR_UNSUPPORTED, "the unregularised kernel is FP64-only");
+    if (c->kernel == FJ_KERNEL_CUTOFF && !(c->r_cut >= 0.0)) return fail(FJ_ERR_SHAPE, "r_cut=%g", c->r_cut);
+    const double* u = c->flow.u_inf;
+    if (!(u[0] * u[0] + u[1] * u[1] + u[2] * u[2] > 0.0)) return fail(FJ_ERR_SHAPE, "u_inf must be non-zero");
+    int64_t nb = 0;
+    for (int s = 0; s < c->n_surf; ++s) nb += (int64_t)c->m[s] * c->n[s];
+    if (nb > 6144) return fail(FJ_ERR_UNSUPPORTED, "AIC order %lld exceeds 6144", (long long)nb);
+    return FJ_OK;
+}
+
+static int make_plan(const fj_case_config* cfg, void* ws, size_t ws_bytes, Plan& p) {
+    FJ_TRY(validate(cfg));
+    p.cfg = *cfg;
+    p.L = make_layout(*cfg);
+    const Layout& L = p.L;
+    const int ns = L.n_surf;
+    p.nb = (int)L.po[ns];
+    p.sz_zb = L.vo[ns] * 3;
+    p.sz_zw = L.wvo[ns] * 3;
+    p.sz_pan = L.po[ns];
+    p.sz_gw = L.wpo[ns];
+    p.sz_strip = L.so[ns];
+    const int img = cfg->mirror ? 2 : 1;
+    int64_t stream = 0;
+    for (int s = 0; s < ns; ++s)
+        stream += img * (stream_len(L.m[s], L.n[s]) + stream_len(std::max(L.ms[s], 1), L.n[s]));
+    p.max_stream = stream;
+    p.max_targets = std::max<int64_t>(std::max<int64_t>(L.wto[ns], L.fo[ns]), L.po[ns]);
+    // partial buffers for each of the three target sets at the full stream length
+    int64_t part = 0;
+    const int64_t sets[3] = {L.wto[ns], L.fo[ns], L.po[ns]};
+    for (int64_t nt : sets) {
+        if (nt == 0) continue;
+        part = std::max<int64_t>(part, (int64_t)choose_split(nt, stream, cfg->precision) * nt * 3);
+    }
+    p.part_elems = part;
+
+    Arena a(ws, ws_bytes);
+    p.flags = a.carve<int>(16);
+    p.zeta_nm1 = a.carve<double>(p.sz_zb);
+    p.c_dot = a.carve<double>(p.sz_pan * 3);
+    p.targets = a.carve<double>(p.max_targets * 3);
+    p.v = a.carve<double>(p.max_targets * 3);
+    p.part = a.carve<double>(std::max<int64_t>(part, 1));
+    p.stream = a.carve<Elem64>(stream);
+    int64_t hs = 0, hsg = 0;
+    for (int s = 0; s < ns; ++s) {
+        hs += 2ll * (L.n[s] + 1) * 3;
+        hsg += L.n[s];
+    }
+    p.hs_zw = a.carve<double>(hs);
+    p.hs_gw = a.carve<double>(hsg);
+    p.a64 = a.carve<double>((int64_t)p.nb * p.nb);
+    if (cfg->precision == FJ_PREC_MIXED) {
+        p.a32 = a.carve<float>((int64_t)p.nb * p.nb);
+        p.x32 = a.carve<float>((int64_t)p.nb * p.nb);
+        p.zeta_ref = a.carve<double>(p.sz_zb);
+    } else {
+        p.a32 = nullptr;
+        p.x32 = nullptr;
+        p.zeta_ref = nullptr;
+    }
+    p.piv = a.carve<int32_t>(p.nb);
+    p.rhs = a.carve<double>(p.nb);
+    p.r = a.carve<double>(p.nb);
+    p.resid = a.carve<double>(cfg->n_tstep);
+    p.ffil = a.carve<double>(L.fo[ns] * 3);
+    p.scalar = a.carve<double>(4);
+    if (ws != nullptr && !a.fits())
+        return fail(FJ_ERR_NOMEM, "workspace of %zu bytes is smaller than the %zu required", ws_bytes, a.used);
+    p.ws_needed = a.used;
+    return FJ_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// v_ind driver: pack the stream then sum over a target set
+// ------------------------------------------------------------------------------------
+struct StreamBuilder {
+    PackArgs a;
+    int n = 0;
+    void init(const Plan& p) {
+        memset(&a, 0, sizeof(a));
+        a.kernel = p.cfg.kernel;
+        a.r_cut = p.cfg.r_cut;
+        for (int d = 0; d < 3; ++d) {
+            a.mirror.p[d] = p.cfg.mirror_point[d];
+            a.mirror.nrm[d] = p.cfg.mirror_normal[d];
+        }
+        n = 0;
+        a.offset[0] = 0;
+    }
+    void add(const Plan& p, const double* zeta, const double* gamma, int rows, int cols) {
+        const int img = p.cfg.mirror ? 2 : 1;
+        for (int i = 0; i < img; ++i) {
+            LatticeRef& L = a.lat[n];
+            L.zeta = zeta;
+            L.gamma = gamma;
+            L.rows = rows;
+            L.cols = cols;
+            L.sign = i == 0 ? 1.0f : -1.0f;
+            L.mirrored = i;
+            a.offset[n + 1] = a.offset[n] + stream_len(rows, cols);
+            ++n;
+        }
+        a.n_lat = n;
+    }
+    int64_t len() const { return a.offset[n]; }
+};
+
+static int pack(const Plan& p, const StreamBuilder& sb, int64_t elem_offset, cudaStream_t s) {
+    // pack lattices into the stream starting at element `elem_offset`
+    PackArgs a = sb.a;
+    if (p.cfg.precision == FJ_PREC_FP64)
+        return pack_stream64(a, (Elem64*)p.stream + elem_offset, s);
+    return pack_stream32(a, (Elem32*)p.stream + elem_offset, s);
+}
+
+static int vind_sum(const Plan& p, const double* targets, int64_t nt, int64_t n_elem, double* out, cudaStream_t s) {
+    if (nt == 0) return FJ_OK;
+    if (n_elem == 0) {
+        FJ_CUDA(cudaMemsetAsync(out, 0, nt * 3 * sizeof(double), s));
+        return FJ_OK;
+    }
+    VindJob j;
+    j.targets = targets;
+    j.n_targets = nt;
+    j.stream = p.stream;
+    j.n_elem = n_elem;
+    j.n_split = choose_split(nt, n_elem, p.cfg.precision);
+    j.part = p.part;
+    if ((int64_t)j.n_split * nt * 3 > p.part_elems) return fail(FJ_ERR_NOMEM, "partial buffer too small");
+    FJ_TRY(vind_launch(j, p.cfg.precision, p.cfg.kernel, p.cfg.r_cut, s));
+    return reduce_partials(p.part, j.n_split, nt, out, 0, 1.0, s);
+}
+
+static void fill_aic_args(const Plan& p, AicArgs& a, const double* zeta, const double* c, const double* nc,
+                          const double* zeta_w_static, int rows_static) {
+    memset(&a, 0, sizeof(a));
+    const Layout& L = p.L;
+    a.n_surf = L.n_surf;
+    int64_t wo = 0;
+    a.max_fil = 0;
+    for (int s = 0; s < L.n_surf; ++s) {
+        a.zeta_b[s] = zeta + L.vo[s] * 3;
+        a.m[s] = L.m[s];
+        a.n[s] = L.n[s];
+        a.col_off[s] = L.po[s];
+        a.max_fil = std::max(a.max_fil, L.m[s] * (L.n[s] + 1) + (L.m[s] + 1) * L.n[s]);
+        if (zeta_w_static != nullptr) {
+            const int rows = rows_static >= 0 ? (L.ms[s] == 0 ? 0 : rows_static) : L.ms[s];
+            a.zeta_w[s] = rows > 0 ? zeta_w_static + wo : nullptr;
+            a.m_star[s] = rows;
+            wo += (int64_t)(rows + 1) * (L.n[s] + 1) * 3;
+        }
+    }
+    a.n_rows = L.po[L.n_surf];
+    a.mirror = p.cfg.mirror;
+    for (int d = 0; d < 3; ++d) {
+        a.mp.p[d] = p.cfg.mirror_point[d];
+        a.mp.nrm[d] = p.cfg.mirror_normal[d];
+    }
+    a.kernel = p.cfg.kernel;
+    a.rc2 = p.cfg.r_cut * p.cfg.r_cut;
+    a.c = c;
+    a.nc = nc;
+    a.aic = p.a64;
+    a.ld = p.nb;
+}
+
+// ------------------------------------------------------------------------------------
+// Static solve (uvlm.py:1286-1333 through base_solve_from_grid with static=True)
+// ------------------------------------------------------------------------------------
+static int run_static(const Plan& p, const fj_case_buffers* B, const double* hg, int horseshoe, double t0,
+                      cudaStream_t s) {
+    const Layout& L = p.L;
+    const fj_case_config& c = p.cfg;
+    double* zb = B->d_zeta_b;
+    double* zw = B->d_zeta_w;
+    double* cc = B->d_c;
+    double* nc = B->d_nc;
+    double* gb = B->d_gamma_b;
+    double* gw = B->d_gamma_w;
+    FJ_CUDA(cudaMemcpyAsync(B->d_t, &t0, sizeof(double), cudaMemcpyHostToDevice, s));
+    geom_vertices_kernel<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(L, B->d_zeta_b0, B->d_dof_mapping, hg, nullptr, nullptr,
+                                                                zb, B->d_zeta_b_dot, nullptr, nullptr, 0.0, 0.0);
+    geom_panels_kernel<<<nblk(L.po[L.n_surf]), 256, 0, s>>>(L, zb, nullptr, cc, nc, nullptr);
+    // wake of the solve: initialise_wake or the horseshoe (rows 1, far end at HORSESHOE_LENGTH)
+    const double* zw_solve;
+    int rows_solve;
+    if (horseshoe) {
+        init_wake_kernel<<<nblk(2 * (p.sz_strip + L.n_surf)), 256, 0, s>>>(L, zb, c.flow, c.dt, 1e3, p.hs_zw, 1);
+        zw_solve = p.hs_zw;
+        rows_solve = 1;
+    } else {
+        init_wake_kernel<<<nblk(L.wvo[L.n_surf]), 256, 0, s>>>(L, zb, c.flow, c.dt, 0.0, zw, 0);
+        zw_solve = zw;
+        rows_solve = -1;
+    }
+    FJ_LAUNCH_CHECK("static geometry");
+    AicArgs aa;
+    fill_aic_args(p, aa, zb, cc, nc, zw_solve, rows_solve);
+    FJ_TRY(aic_launch(aa, nullptr, s));
+    rhs_kernel<<<nblk(p.nb), 256, 0, s>>>(p.nb, cc, nullptr, nc, nullptr, c.flow, nullptr, t0, p.rhs);
+    FJ_TRY(lu_factor64(p.a64, p.nb, p.piv, p.flags, s));
+    FJ_TRY(lu_solve64(p.a64, p.nb, p.piv, p.rhs, s));
+    FJ_CUDA(cudaMemcpyAsync(gb, p.rhs, p.nb * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    // wake circulation of the solve, and of the stored slot (broadcast over m_star rows)
+    double* gw_solve = gw;
+    if (horseshoe) {
+        static_gamma_w_kernel<<<nblk(p.sz_strip), 256, 0, s>>>(L, gb, p.hs_gw, 1);
+        gw_solve = p.hs_gw;
+    }
+    static_gamma_w_kernel<<<nblk(p.sz_gw + 1), 256, 0, s>>>(L, gb, gw, -1);
+    // forces: v at midpoints from bound + solve wake, zeta_dot = 0
+    StreamBuilder sb;
+    sb.init(p);
+    int64_t wo = 0, go = 0;
+    for (int q = 0; q < L.n_surf; ++q) {
+        const int rows = horseshoe ? (L.ms[q] == 0 ? 0 : 1) : L.ms[q];
+        sb.add(p, zw_solve + wo, gw_solve + go, rows, L.n[q]);
+        wo += (int64_t)(rows + 1) * (L.n[q] + 1) * 3;
+        go += (int64_t)rows * L.n[q];
+    }
+    for (int q = 0; q < L.n_surf; ++q) sb.add(p, zb + L.vo[q] * 3, gb + L.po[q], L.m[q], L.n[q]);
+    FJ_TRY(pack(p, sb, 0, s));
+    force_targets_kernel<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(L, zb, p.targets);
+    FJ_TRY(vind_sum(p, p.targets, L.fo[L.n_surf], sb.len(), p.v, s));
+    force_filament_kernel<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(L, zb, nullptr, gb, gw_solve, p.targets, p.v, c.flow,
+                                                                 nullptr, t0, p.ffil);
+    vertex_forces_kernel<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(L, p.ffil, nullptr, nc, c.flow.rho, B->d_f_steady,
+                                                                B->d_f_unsteady);
+    strip_alpha_kernel<<<nblk(p.sz_strip), 256, 0, s>>>(L, zb, B->d_f_steady, c.flow, nullptr, t0, B->d_alpha);
+    FJ_CUDA(cudaMemsetAsync(B->d_gamma_b_dot, 0, p.sz_pan * sizeof(double), s));
+    if (horseshoe)  // stored wake geometry is the regular initial wake (uvlm.py:1329-1331)
+        init_wake_kernel<<<nblk(L.wvo[L.n_surf]), 256, 0, s>>>(L, zb, c.flow, c.dt, 0.0, zw, 0);
+    force_total_kernel<<<1, 256, 0, s>>>(L.vo[L.n_surf], B->d_f_steady, B->d_f_unsteady, B->d_force_total);
+    FJ_LAUNCH_CHECK("static solve");
+    return FJ_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// Dynamic step at slot i (case_solve, uvlm.py:1119-1215)
+// ------------------------------------------------------------------------------------
+__global__ void advance_time_kernel(double* t, int i, double dt) { t[i] = t[i - 1] + dt; }
+
+static int run_step(const Plan& p, const fj_case_buffers* B, int i, const double* hg_n, const double* hgd_n,
+                    const double* hg_nm1, bool refactor, cudaStream_t s) {
+    const Layout& L = p.L;
+    const fj_case_config& c = p.cfg;
+    double* zb_n = B->d_zeta_b + (int64_t)i * p.sz_zb;
+    double* zbd_n = B->d_zeta_b_dot + (int64_t)i * p.sz_zb;
+    double* zw_n = B->d_zeta_w + (int64_t)i * p.sz_zw;
+    const double* zw_nm1 = B->d_zeta_w + (int64_t)(i - 1) * p.sz_zw;
+    double* cc = B->d_c + (int64_t)i * p.sz_pan * 3;
+    double* nc = B->d_nc + (int64_t)i * p.sz_pan * 3;
+    double* gb_n = B->d_gamma_b + (int64_t)i * p.sz_pan;
+    const double* gb_nm1 = B->d_gamma_b + (int64_t)(i - 1) * p.sz_pan;
+    double* gbd_n = B->d_gamma_b_dot + (int64_t)i * p.sz_pan;
+    const double* gbd_nm1 = B->d_gamma_b_dot + (int64_t)(i - 1) * p.sz_pan;
+    double* gw_n = B->d_gamma_w + (int64_t)i * p.sz_gw;
+    const double* gw_nm1 = B->d_gamma_w + (int64_t)(i - 1) * p.sz_gw;
+    double* t_n = B->d_t + i;
+    const bool mixed = c.precision == FJ_PREC_MIXED;
+
+    // 1. geometry, and t_n = t_{n-1} + dt on the device (case_solve, uvlm.py:1158-1161)
+    advance_time_kernel<<<1, 1, 0, s>>>(B->d_t, i, c.dt);
+    geom_vertices_kernel<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(L, B->d_zeta_b0, B->d_dof_mapping, hg_n, hgd_n, hg_nm1,
+                                                                zb_n, zbd_n, p.zeta_nm1, nullptr, 0.0, 0.0);
+    geom_panels_kernel<<<nblk(L.po[L.n_surf]), 256, 0, s>>>(L, zb_n, zbd_n, cc, nc, p.c_dot);
+    FJ_LAUNCH_CHECK("geometry");
+
+    // 2. wake: free-wake velocities from bound(n-1) + wake(n-1), then shed + convect
+    const double* vw = nullptr;
+    if (c.free_wake && L.wto[L.n_surf] > 0) {
+        StreamBuilder sb;
+        sb.init(p);
+        for (int q = 0; q < L.n_surf; ++q) sb.add(p, p.zeta_nm1 + L.vo[q] * 3, gb_nm1 + L.po[q], L.m[q], L.n[q]);
+        for (int q = 0; q < L.n_surf; ++q) sb.add(p, zw_nm1 + L.wvo[q] * 3, gw_nm1 + L.wpo[q], L.ms[q], L.n[q]);
+        FJ_TRY(pack(p, sb, 0, s));
+        gather_wake_targets_kernel<<<nblk(L.wto[L.n_surf]), 256, 0, s>>>(L, zw_nm1, p.targets);
+        FJ_TRY(vind_sum(p, p.targets, L.wto[L.n_surf], sb.len(), p.v, s));
+        vw = p.v;
+    }
+    wake_shed_kernel<<<nblk(L.wvo[L.n_surf] + L.wpo[L.n_surf]), 256, 0, s>>>(L, zb_n, zw_nm1, gb_nm1, gw_nm1, vw, c.flow,
+                                                                             t_n, c.dt, zw_n, gw_n);
+    FJ_LAUNCH_CHECK("wake_shed_kernel");
+
+    // 3. AIC (dynamic: bound only)
+    AicArgs aa;
+    fill_aic_args(p, aa, zb_n, cc, nc, nullptr, -1);
+    const int* run_flag = nullptr;
+    if (mixed && !refactor) {
+        // re-assemble only if the bound lattice differs from the one of the cached AIC
+        FJ_CUDA(cudaMemsetAsync(p.flags + 1, 0, sizeof(int), s));
+        changed_kernel<<<nblk(p.sz_zb), 256, 0, s>>>(zb_n, p.zeta_ref, p.sz_zb, p.flags + 1);
+        run_flag = p.flags + 1;
+    }
+    FJ_TRY(aic_launch(aa, run_flag, s));
+
+    // 4. RHS with the wake of step n: stream = [wake_n (+ images)] ++ [bound_n (+ images)]
+    StreamBuilder sw;
+    sw.init(p);
+    for (int q = 0; q < L.n_surf; ++q) sw.add(p, zw_n + L.wvo[q] * 3, gw_n + L.wpo[q], L.ms[q], L.n[q]);
+    const int64_t n_wake_elem = sw.len();
+    FJ_TRY(pack(p, sw, 0, s));
+    FJ_TRY(vind_sum(p, cc, p.nb, n_wake_elem, p.v, s));
+    rhs_kernel<<<nblk(p.nb), 256, 0, s>>>(p.nb, cc, p.c_dot, nc, p.v, c.flow, t_n, 0.0, p.rhs);
+    FJ_LAUNCH_CHECK("rhs_kernel");
+
+    // 5. solve
+    if (!mixed) {
+        FJ_TRY(lu_factor64(p.a64, p.nb, p.piv, p.flags, s));
+        FJ_TRY(lu_solve64(p.a64, p.nb, p.piv, p.rhs, s));
+        FJ_CUDA(cudaMemcpyAsync(gb_n, p.rhs, p.nb * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    } else {
+        if (refactor) {
+            FJ_TRY(convert64to32(p.a64, p.a32, (int64_t)p.nb * p.nb, s));
+            FJ_TRY(lu_factor32(p.a32, p.nb, p.piv, p.flags, s));
+            FJ_TRY(lu_inverse32(p.a32, p.nb, p.piv, p.x32, s));
+            FJ_CUDA(cudaMemcpyAsync(p.zeta_ref, zb_n, p.sz_zb * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        }
+        FJ_TRY(refine_solve(p.a64, p.x32, p.nb, p.rhs, gb_n, p.r, p.resid + i, 3, s));
+    }
+
+    // 6. forces with bound(n) + wake(n)
+    StreamBuilder sbd;
+    sbd.init(p);
+    for (int q = 0; q < L.n_surf; ++q) sbd.add(p, zb_n + L.vo[q] * 3, gb_n + L.po[q], L.m[q], L.n[q]);
+    FJ_TRY(pack(p, sbd, n_wake_elem, s));
+    force_targets_kernel<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(L, zb_n, p.targets);
+    FJ_TRY(vind_sum(p, p.targets, L.fo[L.n_surf], n_wake_elem + sbd.len(), p.v, s));
+    force_filament_kernel<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(L, zb_n, zbd_n, gb_n, gw_n, p.targets, p.v, c.flow,
+                                                                 t_n, 0.0, p.ffil);
+    // 7. gamma_dot, vertex forces, strip alpha, totals
+    gamma_dot_kernel<<<nblk(p.nb), 256, 0, s>>>(p.nb, gb_n, gb_nm1, gbd_nm1, c.dt, c.gamma_dot_relaxation, gbd_n);
+    vertex_forces_kernel<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(L, p.ffil, gbd_n, nc, c.flow.rho,
+                                                                B->d_f_steady + (int64_t)i * p.sz_zb,
+                                                                B->d_f_unsteady + (int64_t)i * p.sz_zb);
+    strip_alpha_kernel<<<nblk(p.sz_strip), 256, 0, s>>>(L, zb_n, B->d_f_steady + (int64_t)i * p.sz_zb, c.flow, t_n,
+                                                        0.0, B->d_alpha + (int64_t)i * p.sz_strip);
+    force_total_kernel<<<1, 256, 0, s>>>(L.vo[L.n_surf], B->d_f_steady + (int64_t)i * p.sz_zb,
+                                         B->d_f_unsteady + (int64_t)i * p.sz_zb, B->d_force_total + (int64_t)i * 3);
+    FJ_LAUNCH_CHECK("post-processing");
+    return FJ_OK;
+}
+
+static int check_buffers(const fj_case_buffers* B, bool dynamic) {
+    if (B == nullptr) return fail(FJ_ERR_SHAPE, "buffers struct is NULL");
+    if (!B->d_zeta_b0 || !B->d_dof_mapping || !B->d_t || !B->d_zeta_b || !B->d_zeta_b_dot || !B->d_zeta_w ||
+        !B->d_c || !B->d_nc || !B->d_gamma_b || !B->d_gamma_b_dot || !B->d_gamma_w || !B->d_f_steady ||
+        !B->d_f_unsteady || !B->d_alpha || !B->d_force_total)
+        return fail(FJ_ERR_SHAPE, "a required device buffer is NULL");
+    if (dynamic && (!B->d_hg_t || !B->d_hg_dot_t)) return fail(FJ_ERR_SHAPE, "hg_t / hg_dot_t are NULL");
+    return FJ_OK;
+}
+
+static int run_dynamic(const Plan& p, const fj_case_buffers* B, int i_first, int i_last, cudaStream_t s) {
+    const int64_t hs = (int64_t)p.cfg.n_nodes * 16;
+    const bool mixed = p.cfg.precision == FJ_PREC_MIXED;
+    bool refactor_all = false;
+    int i = i_first;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        for (int k = i; k < i_last; ++k) {
+            const bool refactor = mixed && (refactor_all || k == i);
+            FJ_TRY(run_step(p, B, k, B->d_hg_t + (int64_t)k * hs, B->d_hg_dot_t + (int64_t)k * hs,
+                            B->d_hg_t + (int64_t)(k - 1) * hs, refactor, s));
+        }
+        if (!mixed) break;
+        // read the refinement residuals back once; re-run from the first failure with a
+        // fresh factorisation every step if the cached factors were not good enough
+        std::vector<double> res(i_last - i);
+        FJ_CUDA(cudaMemcpyAsync(res.data(), p.resid + i, res.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        FJ_CUDA(cudaStreamSynchronize(s));
+        int bad = -1;
+        for (size_t q = 0; q < res.size(); ++q)
+            if (!(res[q] <= 1e-12)) {
+                bad = (int)q + i;
+                break;
+            }
+        if (bad < 0) return FJ_OK;
+        if (refactor_all)
+            return fail(FJ_ERR_NOT_CONVERGED, "refinement residual %.3g at slot %d after refactorisation",
+                        res[bad - i], bad);
+        refactor_all = true;
+        i = bad;
+    }
+    return FJ_OK;
+}
+
+}  // namespace fj
+
+// =====================================================================================
+// C ABI
+// =====================================================================================
+using namespace fj;
+
+extern "C" {
+
+const char* fj_last_error_string(void) { return fj::last_error(); }
+
+int fj_version(void) { return 100; }
+
+int fj_case_workspace_size(const fj_case_config* cfg, size_t* bytes) {
+    if (bytes == nullptr) return fail(FJ_ERR_SHAPE, "bytes is NULL");
+    Plan p;
+    FJ_TRY(make_plan(cfg, nullptr, 0, p));
+    *bytes = p.ws_needed + 256;
+    return FJ_OK;
+}
+
+int fj_solve_static(const fj_case_config* cfg, const fj_case_buffers* bufs, int horseshoe, double t0, void* d_ws,
+                    size_t ws_bytes, fj_stream_t stream) {
+    Plan p;
+    FJ_TRY(make_plan(cfg, d_ws, ws_bytes, p));
+    FJ_TRY(check_buffers(bufs, false));
+    const double* hg = bufs->d_hg_t;
+    if (hg == nullptr) return fail(FJ_ERR_SHAPE, "d_hg_t is NULL (slot 0 holds the static frames)");
+    return run_static(p, bufs, hg, horseshoe, t0, (cudaStream_t)stream);
+}
+
+int fj_solve_prescribed_dynamic(const fj_case_config* cfg, const fj_case_buffers* bufs, int i_first, int i_last,
+                                void* d_ws, size_t ws_bytes, fj_stream_t stream) {
+    Plan p;
+    FJ_TRY(make_plan(cfg, d_ws, ws_bytes, p));
+    FJ_TRY(check_buffers(bufs, true));
+    if (i_first < 1 || i_last > cfg->n_tstep || i_first > i_last)
+        return fail(FJ_ERR_SHAPE, "step range [%d, %d) not within [1, %d)", i_first, i_last, cfg->n_tstep);
+    if (i_first == i_last) return FJ_OK;
+    return run_dynamic(p, bufs, i_first, i_last, (cudaStream_t)stream);
+}
+
+int fj_case_step(const fj_case_config* cfg, const fj_case_buffers* bufs, int i_ts, void* d_ws, size_t ws_bytes,
+                 fj_stream_t stream) {
+    return fj_solve_prescribed_dynamic(cfg, bufs, i_ts, i_ts + 1, d_ws, ws_bytes, stream);
+}
+
+int fj_biot_savart(const double* d_x, const double* d_y, int64_t n_pairs, int kernel, double r_cut, double* d_out,
+                   fj_stream_t stream) {
+    return biot_savart_pairs(d_x, d_y, n_pairs, kernel, r_cut, d_out, (cudaStream_t)stream);
+}
+
+static int vind_plan(int64_t n_targets, const int* rows, const int* cols, int n_lattices, int mirror, int precision,
+                     int64_t& n_elem, int& n_split, size_t& bytes) {
+    if (n_targets < 0 || n_lattices < 0 || n_lattices > FJ_MAX_SURF * 2)
+        return fail(FJ_ERR_SHAPE, "vind: n_targets=%lld n_lattices=%d", (long long)n_targets, n_lattices);
+    if (precision != FJ_PREC_FP64 && precision != FJ_PREC_MIXED) return fail(FJ_ERR_UNSUPPORTED, "precision %d", precision);
+    n_elem = 0;
+    for (int i = 0; i < n_lattices; ++i) {
+        if (rows[i] < 0 || cols[i] < 0) return fail(FJ_ERR_SHAPE, "vind: lattice %d has rows=%d cols=%d", i, rows[i], cols[i]);
+        n_elem += (mirror ? 2 : 1) * stream_len(rows[i], cols[i]);
+    }
+    n_split = choose_split(std::max<int64_t>(n_targets, 1), n_elem, precision);
+    Arena a(nullptr, 0);
+    a.carve<Elem64>(n_elem);
+    a.carve<double>((int64_t)n_split * std::max<int64_t>(n_targets, 1) * 3);
+    bytes = a.used + 256;
+    return FJ_OK;
+}
+
+int fj_vind_workspace_size(int64_t n_targets, const int* rows, const int* cols, int n_lattices, int mirror,
+                           int precision, size_t* bytes) {
+    int64_t ne;
+    int sp;
+    size_t b;
+    FJ_TRY(vind_plan(n_targets, rows, cols, n_lattices, mirror, precision, ne, sp, b));
+    *bytes = b;
+    return FJ_OK;
+}
+
+int fj_vind(const double* d_targets, int64_t n_targets, const double* const* d_zetas, const double* const* d_gammas,
+            const int* rows, const int* cols, int n_lattices, const double* mirror_point, const double* mirror_normal,
+            int kernel, double r_cut, int precision, double* d_v_out, void* d_ws, size_t ws_bytes,
+            fj_stream_t stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    const int mirror = mirror_point != nullptr && mirror_normal != nullptr;
+    int64_t ne;
+    int sp;
+    size_t need;
+    FJ_TRY(vind_plan(n_targets, rows, cols, n_lattices, mirror, precision, ne, sp, need));
+    if (kernel < 0 || kernel > 2) return fail(FJ_ERR_UNSUPPORTED, "kernel %d", kernel);
+    if (precision == FJ_PREC_MIXED && kernel == FJ_KERNEL_PLAIN)
+        return fail(FJ_ERR_UNSUPPORTED, "the unregularised kernel is FP64-only");
+    if (ws_bytes < need) return fail(FJ_ERR_NOMEM, "vind workspace %zu < %zu", ws_bytes, need);
+    if (n_targets == 0) return FJ_OK;
+    Arena a(d_ws, ws_bytes);
+    void* st = a.carve<Elem64>(ne);
+    double* part = a.carve<double>((int64_t)sp * n_targets * 3);
+    PackArgs pa;
+    memset(&pa, 0, sizeof(pa));
+    pa.kernel = kernel;
+    pa.r_cut = r_cut;
+    if (mirror)
+        for (int d = 0; d < 3; ++d) {
+            pa.mirror.p[d] = mirror_point[d];
+            pa.mirror.nrm[d] = mirror_normal[d];
+        }
+    int n = 0;
+    for (int i = 0; i < n_lattices; ++i) {
+        for (int img = 0; img < (mirror ? 2 : 1); ++img) {
+            LatticeRef& L = pa.lat[n];
+            L.zeta = d_zetas[i];
+            L.gamma = d_gammas[i];
+            L.rows = rows[i];
+            L.cols = cols[i];
+            L.sign = img ? -1.0f : 1.0f;
+            L.mirrored = img;
+            pa.offset[n + 1] = pa.offset[n] + stream_len(rows[i], cols[i]);
+            ++n;
+        }
+    }
+    pa.n_lat = n;
+    if (ne == 0) {
+        FJ_CUDA(cudaMemsetAsync(d_v_out, 0, n_targets * 3 * sizeof(double), s));
+        return FJ_OK;
+    }
+    if (precision == FJ_PREC_FP64)
+        FJ_TRY(pack_stream64(pa, (Elem64*)st, s));
+    else
+        FJ_TRY(pack_stream32(pa, (Elem32*)st, s));
+    VindJob j;
+    j.targets = d_targets;
+    j.n_targets = n_targets;
+    j.stream = st;
+    j.n_elem = ne;
+    j.n_split = sp;
+    j.part = part;
+    FJ_TRY(vind_launch(j, precision, kernel, r_cut, s));
+    return reduce_partials(part, sp, n_targets, d_v_out, 0, 1.0, s);
+}
+
+int fj_aic_workspace_size(const int* m, const int* n, int n_surf, size_t* bytes) {
+    if (bytes == nullptr || n_surf < 1 || n_surf > FJ_MAX_SURF) return fail(FJ_ERR_SHAPE, "aic workspace: n_surf=%d", n_surf);
+    int64_t nb = 0;
+    for (int s = 0; s < n_surf; ++s) nb += (int64_t)m[s] * n[s];
+    Arena a(nullptr, 0);
+    a.carve<double>(nb * 3);
+    a.carve<double>(nb * 3);
+    *bytes = a.used + 256;
+    return FJ_OK;
+}
+
+int fj_aic_assemble(const double* const* d_zetas_b, const int* m, const int* n, int n_surf,
+                    const double* const* d_zetas_w, const int* m_star, const double* mirror_point,
+                    const double* mirror_normal, int kernel, double r_cut, double* d_aic, void* d_ws, size_t ws_bytes,
+                    fj_stream_t stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    size_t need;
+    FJ_TRY(fj_aic_workspace_size(m, n, n_surf, &need));
+    if (ws_bytes < need) return fail(FJ_ERR_NOMEM, "aic workspace %zu < %zu", ws_bytes, need);
+    if (kernel < 0 || kernel > 2) return fail(FJ_ERR_UNSUPPORTED, "kernel %d", kernel);
+    fj_case_config cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.n_surf = n_surf;
+    for (int s = 0; s < n_surf; ++s) {
+        if (m[s] < 1 || n[s] < 1) return fail(FJ_ERR_SHAPE, "surface %d: m=%d n=%d", s, m[s], n[s]);
+        cfg.m[s] = m[s];
+        cfg.n[s] = n[s];
+        cfg.m_star[s] = d_zetas_w != nullptr ? m_star[s] : 0;
+    }
+    Layout L = make_layout(cfg);
+    const int64_t nb = L.po[n_surf];
+    Arena a(d_ws, ws_bytes);
+    double* c = a.carve<double>(nb * 3);
+    double* nc = a.carve<double>(nb * 3);
+    for (int s = 0; s < n_surf; ++s) {
+        fj_case_config one;
+        memset(&one, 0, sizeof(one));
+        one.n_surf = 1;
+        one.m[0] = m[s];
+        one.n[0] = n[s];
+        Layout L1 = make_layout(one);
+        geom_panels_kernel<<<nblk(L1.po[1]), 256, 0, st>>>(L1, d_zetas_b[s], nullptr, c + L.po[s] * 3,
+                                                           nc + L.po[s] * 3, nullptr);
+    }
+    FJ_LAUNCH_CHECK("aic geometry");
+    AicArgs aa;
+    memset(&aa, 0, sizeof(aa));
+    aa.n_surf = n_surf;
+    aa.max_fil = 0;
+    for (int s = 0; s < n_surf; ++s) {
+        aa.zeta_b[s] = d_zetas_b[s];
+        aa.m[s] = m[s];
+        aa.n[s] = n[s];
+        aa.col_off[s] = L.po[s];
+        aa.max_fil = std::max(aa.max_fil, m[s] * (n[s] + 1) + (m[s] + 1) * n[s]);
+        aa.zeta_w[s] = (d_zetas_w != nullptr && m_star[s] > 0) ? d_zetas_w[s] : nullptr;
+        aa.m_star[s] = d_zetas_w != nullptr ? m_star[s] : 0;
+    }
+    aa.n_rows = nb;
+    aa.mirror = mirror_point != nullptr && mirror_normal != nullptr;
+    if (aa.mirror)
+        for (int d = 0; d < 3; ++d) {
+            aa.mp.p[d] = mirror_point[d];
+            aa.mp.nrm[d] = mirror_normal[d];
+        }
+    aa.kernel = kernel;
+    aa.rc2 = r_cut * r_cut;
+    aa.c = c;
+    aa.nc = nc;
+    aa.aic = d_aic;
+    aa.ld = nb;
+    return aic_launch(aa, nullptr, st);
+}
+
+int fj_lu_workspace_size(int n, size_t* bytes) {
+    *bytes = 256;
+    (void)n;
+    return FJ_OK;
+}
+
+int fj_lu_factor(double* d_a, int n, int32_t* d_piv, void* d_ws, size_t ws_bytes, fj_stream_t stream) {
+    if (ws_bytes < sizeof(int)) return fail(FJ_ERR_NOMEM, "lu workspace too small");
+    return lu_factor64(d_a, n, d_piv, (int*)d_ws, (cudaStream_t)stream);
+}
+
+int fj_lu_solve(const double* d_lu, int n, const int32_t* d_piv, double* d_b, void* d_ws, size_t ws_bytes,
+                fj_stream_t stream) {
+    (void)d_ws;
+    (void)ws_bytes;
+    return lu_solve64(d_lu, n, d_piv, d_b, (cudaStream_t)stream);
+}
+
+int fj_solve_mixed_workspace_size(int n, size_t* bytes) {
+    Arena a(nullptr, 0);
+    a.carve<float>((int64_t)n * n);
+    a.carve<float>((int64_t)n * n);
+    a.carve<int32_t>(n);
+    a.carve<double>(n);
+    a.carve<int>(4);
+    *bytes = a.used + 256;
+    return FJ_OK;
+}
+
+int fj_solve_mixed(const double* d_a, int n, const double* d_b, double* d_x, int refactor, double* d_resid, void* d_ws,
+                   size_t ws_bytes, fj_stream_t stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    size_t need;
+    FJ_TRY(fj_solve_mixed_workspace_size(n, &need));
+    if (ws_bytes < need) return fail(FJ_ERR_NOMEM, "solve_mixed workspace %zu < %zu", ws_bytes, need);
+    Arena a(d_ws, ws_bytes);
+    float* a32 = a.carve<float>((int64_t)n * n);
+    float* x32 = a.carve<float>((int64_t)n * n);
+    int32_t* piv = a.carve<int32_t>(n);
+    double* r = a.carve<double>(n);
+    int* info = a.carve<int>(4);
+    if (refactor) {
+        FJ_TRY(convert64to32(d_a, a32, (int64_t)n * n, s));
+        FJ_TRY(lu_factor32(a32, n, piv, info, s));
+        FJ_TRY(lu_inverse32(a32, n, piv, x32, s));
+    }
+    return refine_solve(d_a, x32, n, d_b, d_x, r, d_resid, 3, s);
+}
+
+}  // extern "C"

@@ -1,0 +1,482 @@
+// fj_vind.cu -- stream packing and the all-pairs Biot-Savart sums (FP64 and FP32).
+//
+// FP64 path: each (target, filament) pair is evaluated with the reference's own
+// formulas (aero/utils.py:580-648) and the products with the filament strengths summed
+// in FP64 (aero/aic.py:237-242).
+//
+// FP32 path ("mixed"): the same sum with
+//   - differences x - y formed from hi+lo FP32 splits of the FP64 coordinates,
+//   - MUFU rsqrt / fast division,
+//   - an explicit collinearity test (sin < kCollinearSin -> exactly 0) standing in for
+//     the epsilon regulariser, which FP32 cannot resolve (EPSILON*|r0|^4 ~ 1e-12 is far
+//     below FP32 noise in |r1 x r2|^2),
+//   - FP32 sums over one staged chunk of filaments, added into FP64 accumulators.
+#include <cstdio>
+#include <cstdarg>
+#include <algorithm>
+
+#include "fj_bs.cuh"
+#include "fj_vind.cuh"
+
+namespace fj {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+int fail(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+const char* last_error() { return g_err; }
+
+// ------------------------------------------------------------------------------------
+// Stream packing
+// ------------------------------------------------------------------------------------
+struct PackedLink {
+    double v[3];
+    double g;
+    double r0[3];
+    double q;
+};
+
+__device__ __forceinline__ void lattice_vertex(const LatticeRef& L, const MirrorPlane& mp, int k,
+                                               int l, double out[3]) {
+    const double* p = L.zeta + ((int64_t)k * (L.cols + 1) + l) * 3;
+    double z0 = p[0], z1 = p[1], z2 = p[2];
+    if (L.mirrored) {
+        // mirror_grid, aero/utils.py:651-663
+        double d0 = z0 - mp.p[0], d1 = z1 - mp.p[1], d2 = z2 - mp.p[2];
+        double dn = d0 * mp.nrm[0] + d1 * mp.nrm[1] + d2 * mp.nrm[2];
+        z0 = z0 - 2.0 * dn * mp.nrm[0];
+        z1 = z1 - 2.0 * dn * mp.nrm[1];
+        z2 = z2 - 2.0 * dn * mp.nrm[2];
+    }
+    out[0] = z0;
+    out[1] = z1;
+    out[2] = z2;
+}
+
+__device__ __forceinline__ double ring_gamma(const LatticeRef& L, int k, int l) {
+    if (k < 0 || l < 0 || k >= L.rows || l >= L.cols) return 0.0;
+    return L.gamma[(int64_t)k * L.cols + l];
+}
+
+__device__ void pack_one(const PackArgs& a, int64_t e, PackedLink& o) {
+    int li = 0;
+    while (li + 1 < a.n_lat && e >= a.offset[li + 1]) ++li;
+    const LatticeRef& L = a.lat[li];
+    int64_t j = e - a.offset[li];
+    const int R = L.rows, C = L.cols;
+    const int64_t n_chord = (int64_t)(C + 1) * (R + 1);
+    int k, l, k1, l1;
+    bool brk;
+    double g;
+    if (j < n_chord) {
+        // chordwise chain l: zeta[k,l] -> zeta[k+1,l], strength G[k,l] - G[k,l-1]
+        l = (int)(j / (R + 1));
+        k = (int)(j % (R + 1));
+        brk = (k == R);
+        k1 = k + 1;
+        l1 = l;
+        g = brk ? 0.0 : ring_gamma(L, k, l) - ring_gamma(L, k, l - 1);
+    } else {
+        // spanwise chain k: zeta[k,l] -> zeta[k,l+1], strength G[k-1,l] - G[k,l]
+        int64_t jj = j - n_chord;
+        k = (int)(jj / (C + 1));
+        l = (int)(jj % (C + 1));
+        brk = (l == C);
+        k1 = k;
+        l1 = l + 1;
+        g = brk ? 0.0 : ring_gamma(L, k - 1, l) - ring_gamma(L, k, l);
+    }
+    lattice_vertex(L, a.mirror, k, l, o.v);
+    o.g = g * (double)L.sign;
+    if (brk) {
+        o.r0[0] = o.r0[1] = o.r0[2] = 0.0;
+        o.q = -1.0;
+        return;
+    }
+    double w[3];
+    lattice_vertex(L, a.mirror, k1, l1, w);
+    o.r0[0] = w[0] - o.v[0];
+    o.r0[1] = w[1] - o.v[1];
+    o.r0[2] = w[2] - o.v[2];
+    const double r0sq = o.r0[0] * o.r0[0] + o.r0[1] * o.r0[1] + o.r0[2] * o.r0[2];
+    if (a.kernel == FJ_KERNEL_EPSILON)
+        o.q = kEps * r0sq * r0sq;  // aero/utils.py:621-622
+    else
+        o.q = r0sq;
+}
+
+__global__ void pack64_kernel(PackArgs a, Elem64* __restrict__ out) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.offset[a.n_lat]) return;
+    PackedLink o;
+    pack_one(a, e, o);
+    Elem64 r;
+    r.x = o.v[0];
+    r.y = o.v[1];
+    r.z = o.v[2];
+    r.g = o.g;
+    r.r0x = o.r0[0];
+    r.r0y = o.r0[1];
+    r.r0z = o.r0[2];
+    r.q = o.q;
+    out[e] = r;
+}
+
+__global__ void pack32_kernel(PackArgs a, Elem32* __restrict__ out) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.offset[a.n_lat]) return;
+    PackedLink o;
+    pack_one(a, e, o);
+    Elem32 r;
+    r.xh = (float)o.v[0];
+    r.yh = (float)o.v[1];
+    r.zh = (float)o.v[2];
+    r.xl = (float)(o.v[0] - (double)r.xh);
+    r.yl = (float)(o.v[1] - (double)r.yh);
+    r.zl = (float)(o.v[2] - (double)r.zh);
+    r.g = (float)(o.g / kFourPi);
+    r.r0x = (float)o.r0[0];
+    r.r0y = (float)o.r0[1];
+    r.r0z = (float)o.r0[2];
+    if (o.q < 0.0)
+        r.q = -1.0f;
+    else if (a.kernel == FJ_KERNEL_EPSILON)
+        r.q = (float)o.q;
+    else  // cutoff: keep iff |r1 x r2|^2 > r_cut^2 |r0|^2  (aero/utils.py:637-648)
+        r.q = (float)(a.r_cut * a.r_cut * o.q);
+    r.pad = 0.f;
+    out[e] = r;
+}
+
+int pack_stream64(const PackArgs& a, Elem64* out, cudaStream_t s) {
+    int64_t n = a.offset[a.n_lat];
+    if (n == 0) return FJ_OK;
+    pack64_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, out);
+    FJ_LAUNCH_CHECK("pack64_kernel");
+    return FJ_OK;
+}
+
+int pack_stream32(const PackArgs& a, Elem32* out, cudaStream_t s) {
+    int64_t n = a.offset[a.n_lat];
+    if (n == 0) return FJ_OK;
+    pack32_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, out);
+    FJ_LAUNCH_CHECK("pack32_kernel");
+    return FJ_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// FP64 sum: the reference's kernels, evaluated on chains.
+// ------------------------------------------------------------------------------------
+constexpr int kBlock = 128;  // threads per CTA == staged elements per chunk
+
+template <int KER, int T>
+__global__ void __launch_bounds__(kBlock) vind64_kernel(const double* __restrict__ tgt, int64_t n_t,
+                                                        const Elem64* __restrict__ st, int64_t n_elem,
+                                                        int n_split, double* __restrict__ part,
+                                                        double rc2) {
+    __shared__ Elem64 sh[kBlock];
+    const int split = blockIdx.y;
+    const int64_t per = (n_elem + n_split - 1) / n_split;
+    const int64_t e0 = (int64_t)split * per;
+    const int64_t e1 = min(n_elem, e0 + per);  // links [e0, e1)
+    const int64_t vend = min(e1, n_elem - 1);  // last vertex needed
+
+    double x[T][3];
+    int64_t ti[T];
+#pragma unroll
+    for (int j = 0; j < T; ++j) {
+        ti[j] = (int64_t)blockIdx.x * kBlock * T + threadIdx.x + (int64_t)j * kBlock;
+        const int64_t tc = min(ti[j], n_t - 1);
+        x[j][0] = tgt[tc * 3 + 0];
+        x[j][1] = tgt[tc * 3 + 1];
+        x[j][2] = tgt[tc * 3 + 2];
+    }
+    double acc[T][3];
+#pragma unroll
+    for (int j = 0; j < T; ++j) acc[j][0] = acc[j][1] = acc[j][2] = 0.0;
+
+    if (e0 < e1) {
+        Vtx64<KER> prev[T];
+        Elem64 pl = st[e0];
+#pragma unroll
+        for (int j = 0; j < T; ++j) vtx64<KER>(x[j], pl.x, pl.y, pl.z, prev[j]);
+        for (int64_t c0 = e0 + 1; c0 <= vend; c0 += kBlock) {
+            const int cnt = (int)min((int64_t)kBlock, vend + 1 - c0);
+            __syncthreads();
+            if (threadIdx.x < cnt) sh[threadIdx.x] = st[c0 + threadIdx.x];
+            __syncthreads();
+            for (int i = 0; i < cnt; ++i) {
+                const Elem64 cur = sh[i];
+#pragma unroll
+                for (int j = 0; j < T; ++j) {
+                    Vtx64<KER> v;
+                    vtx64<KER>(x[j], cur.x, cur.y, cur.z, v);
+                    if (pl.q >= 0.0) link64<KER>(prev[j], v, pl.g, pl.r0x, pl.r0y, pl.r0z, pl.q, rc2, acc[j]);
+                    prev[j] = v;
+                }
+                pl = cur;
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < T; ++j) {
+        if (ti[j] < n_t) {
+            double* o = part + ((int64_t)split * n_t + ti[j]) * 3;
+            o[0] = acc[j][0];
+            o[1] = acc[j][1];
+            o[2] = acc[j][2];
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// FP32 sum.
+// ------------------------------------------------------------------------------------
+struct Vtx32 {
+    float d[3];
+    float u[3];
+    float s;  // kCollinearSin * ||d||_eps^2; a pair is collinear when |r1 x r2|^2 <= s1*s2
+};
+
+__device__ __forceinline__ void vtx32(const float xh[3], const float xl[3], const float4 hi,
+                                      const float4 lo, Vtx32& o) {
+    o.d[0] = (xh[0] - hi.x) + (xl[0] - lo.x);
+    o.d[1] = (xh[1] - hi.y) + (xl[1] - lo.y);
+    o.d[2] = (xh[2] - hi.z) + (xl[2] - lo.z);
+    const float n2 = fmaf(o.d[2], o.d[2], fmaf(o.d[1], o.d[1], fmaf(o.d[0], o.d[0], (float)(kEps * kEps))));
+    const float inv = rsqrtf(n2);
+    o.u[0] = o.d[0] * inv;
+    o.u[1] = o.d[1] * inv;
+    o.u[2] = o.d[2] * inv;
+    o.s = kCollinearSin * n2;
+}
+
+template <int KER>
+__device__ __forceinline__ void link32(const Vtx32& a, const Vtx32& b, float g, float r0x,
+                                       float r0y, float r0z, float q, float acc[3]) {
+    const float cx = fmaf(a.d[1], b.d[2], -a.d[2] * b.d[1]);
+    const float cy = fmaf(a.d[2], b.d[0], -a.d[0] * b.d[2]);
+    const float cz = fmaf(a.d[0], b.d[1], -a.d[1] * b.d[0]);
+    const float c2 = fmaf(cz, cz, fmaf(cy, cy, cx * cx));
+    const float dot = fmaf(r0z, a.u[2] - b.u[2], fmaf(r0y, a.u[1] - b.u[1], r0x * (a.u[0] - b.u[0])));
+    float coef;
+    if (KER == FJ_KERNEL_EPSILON) {
+        coef = (c2 > a.s * b.s) ? __fdividef(g * dot, c2 + q) : 0.0f;
+    } else {
+        coef = (c2 > fmaxf(q, a.s * b.s)) ? __fdividef(g * dot, c2) : 0.0f;
+    }
+    acc[0] = fmaf(cx, coef, acc[0]);
+    acc[1] = fmaf(cy, coef, acc[1]);
+    acc[2] = fmaf(cz, coef, acc[2]);
+}
+
+template <int KER, int T>
+__global__ void __launch_bounds__(kBlock) vind32_kernel(const double* __restrict__ tgt, int64_t n_t,
+                                                        const Elem32* __restrict__ st, int64_t n_elem,
+                                                        int n_split, double* __restrict__ part) {
+    __shared__ float4 sh[kBlock * 3];
+    const int split = blockIdx.y;
+    const int64_t per = (n_elem + n_split - 1) / n_split;
+    const int64_t e0 = (int64_t)split * per;
+    const int64_t e1 = min(n_elem, e0 + per);
+    const int64_t vend = min(e1, n_elem - 1);
+
+    float xh[T][3], xl[T][3];
+    int64_t ti[T];
+#pragma unroll
+    for (int j = 0; j < T; ++j) {
+        ti[j] = (int64_t)blockIdx.x * kBlock * T + threadIdx.x + (int64_t)j * kBlock;
+        const int64_t tc = min(ti[j], n_t - 1);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double v = tgt[tc * 3 + c];
+            xh[j][c] = (float)v;
+            xl[j][c] = (float)(v - (double)xh[j][c]);
+        }
+    }
+    double acc[T][3];
+#pragma unroll
+    for (int j = 0; j < T; ++j) acc[j][0] = acc[j][1] = acc[j][2] = 0.0;
+
+    if (e0 < e1) {
+        const float4* s4 = reinterpret_cast<const float4*>(st);
+        Vtx32 prev[T];
+        float4 pa = s4[e0 * 3 + 0], pb = s4[e0 * 3 + 1], pc = s4[e0 * 3 + 2];
+#pragma unroll
+        for (int j = 0; j < T; ++j) vtx32(xh[j], xl[j], pa, pb, prev[j]);
+        for (int64_t c0 = e0 + 1; c0 <= vend; c0 += kBlock) {
+            const int cnt = (int)min((int64_t)kBlock, vend + 1 - c0);
+            __syncthreads();
+            if (threadIdx.x < cnt) {
+                sh[threadIdx.x * 3 + 0] = s4[(c0 + threadIdx.x) * 3 + 0];
+                sh[threadIdx.x * 3 + 1] = s4[(c0 + threadIdx.x) * 3 + 1];
+                sh[threadIdx.x * 3 + 2] = s4[(c0 + threadIdx.x) * 3 + 2];
+            }
+            __syncthreads();
+            float accf[T][3];
+#pragma unroll
+            for (int j = 0; j < T; ++j) accf[j][0] = accf[j][1] = accf[j][2] = 0.f;
+            for (int i = 0; i < cnt; ++i) {
+                const float4 ca = sh[i * 3 + 0], cb = sh[i * 3 + 1], cc = sh[i * 3 + 2];
+                const bool live = pb.w >= 0.0f;  // link (prev -> cur) is not a chain break
+#pragma unroll
+                for (int j = 0; j < T; ++j) {
+                    Vtx32 v;
+                    vtx32(xh[j], xl[j], ca, cb, v);
+                    if (live) link32<KER>(prev[j], v, pa.w, pc.x, pc.y, pc.z, pb.w, accf[j]);
+                    prev[j] = v;
+                }
+                pa = ca;
+                pb = cb;
+                pc = cc;
+            }
+#pragma unroll
+            for (int j = 0; j < T; ++j) {
+                acc[j][0] += (double)accf[j][0];
+                acc[j][1] += (double)accf[j][1];
+                acc[j][2] += (double)accf[j][2];
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < T; ++j) {
+        if (ti[j] < n_t) {
+            double* o = part + ((int64_t)split * n_t + ti[j]) * 3;
+            o[0] = acc[j][0];
+            o[1] = acc[j][1];
+            o[2] = acc[j][2];
+        }
+    }
+}
+
+__global__ void reduce_partials_kernel(const double* __restrict__ part, int n_split, int64_t n3,
+                                       double* __restrict__ out, int accumulate, double scale) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n3) return;
+    double s = 0.0;
+    for (int k = 0; k < n_split; ++k) s += part[(int64_t)k * n3 + i];
+    s *= scale;
+    out[i] = accumulate ? out[i] + s : s;
+}
+
+int reduce_partials(const double* part, int n_split, int64_t n_targets, double* out, int accumulate,
+                    double scale, cudaStream_t s) {
+    const int64_t n3 = n_targets * 3;
+    if (n3 == 0) return FJ_OK;
+    reduce_partials_kernel<<<(unsigned)((n3 + 255) / 256), 256, 0, s>>>(part, n_split, n3, out,
+                                                                         accumulate, scale);
+    FJ_LAUNCH_CHECK("reduce_partials_kernel");
+    return FJ_OK;
+}
+
+constexpr int kT64 = 2;
+constexpr int kT32 = 2;
+
+int choose_split(int64_t n_targets, int64_t n_elem, int precision) {
+    const int T = precision == FJ_PREC_FP64 ? kT64 : kT32;
+    const int64_t ctas = (n_targets + (int64_t)kBlock * T - 1) / ((int64_t)kBlock * T);
+    const int64_t want = 148 * 8;  // CTAs to cover the SMs a few times over
+    int64_t sp = (want + ctas - 1) / std::max<int64_t>(ctas, 1);
+    const int64_t max_sp = std::max<int64_t>(1, n_elem / 256);
+    if (sp > max_sp) sp = max_sp;
+    if (sp < 1) sp = 1;
+    if (sp > 1024) sp = 1024;
+    return (int)sp;
+}
+
+int vind_launch(const VindJob& job, int precision, int kernel, double r_cut, cudaStream_t s) {
+    if (job.n_targets == 0) return FJ_OK;
+    const int T = precision == FJ_PREC_FP64 ? kT64 : kT32;
+    const int64_t gx = (job.n_targets + (int64_t)kBlock * T - 1) / ((int64_t)kBlock * T);
+    if (gx > 0x7fffffff || job.n_split > 65535) return fail(FJ_ERR_SHAPE, "vind: grid too large");
+    dim3 grid((unsigned)gx, (unsigned)job.n_split);
+    if (precision == FJ_PREC_FP64) {
+        const Elem64* st = (const Elem64*)job.stream;
+        const double rc2 = r_cut * r_cut;
+        switch (kernel) {
+            case FJ_KERNEL_EPSILON:
+                vind64_kernel<FJ_KERNEL_EPSILON, kT64><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part, rc2);
+                break;
+            case FJ_KERNEL_CUTOFF:
+                vind64_kernel<FJ_KERNEL_CUTOFF, kT64><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part, rc2);
+                break;
+            case FJ_KERNEL_PLAIN:
+                vind64_kernel<FJ_KERNEL_PLAIN, kT64><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part, rc2);
+                break;
+            default:
+                return fail(FJ_ERR_UNSUPPORTED, "vind: unknown kernel %d", kernel);
+        }
+    } else {
+        const Elem32* st = (const Elem32*)job.stream;
+        switch (kernel) {
+            case FJ_KERNEL_EPSILON:
+                vind32_kernel<FJ_KERNEL_EPSILON, kT32><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part);
+                break;
+            case FJ_KERNEL_CUTOFF:
+                vind32_kernel<FJ_KERNEL_CUTOFF, kT32><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part);
+                break;
+            default:
+                return fail(FJ_ERR_UNSUPPORTED, "vind: kernel %d has no FP32 variant (use FJ_PREC_FP64)", kernel);
+        }
+    }
+    FJ_LAUNCH_CHECK("vind kernel");
+    return FJ_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// Pairwise kernel evaluation (the reference's per-pair functions, for known-answer tests)
+// ------------------------------------------------------------------------------------
+__global__ void bs_pairs_kernel(const double* __restrict__ x, const double* __restrict__ y, int64_t n,
+                                int kernel, double rc2, double* __restrict__ out) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double xx[3] = {x[i * 3], x[i * 3 + 1], x[i * 3 + 2]};
+    const double* yy = y + i * 6;
+    const double r0x = yy[3] - yy[0], r0y = yy[4] - yy[1], r0z = yy[5] - yy[2];
+    const double r0sq = r0x * r0x + r0y * r0y + r0z * r0z;
+    double acc[3] = {0.0, 0.0, 0.0};
+    if (kernel == FJ_KERNEL_EPSILON) {
+        Vtx64<FJ_KERNEL_EPSILON> a, b;
+        vtx64<FJ_KERNEL_EPSILON>(xx, yy[0], yy[1], yy[2], a);
+        vtx64<FJ_KERNEL_EPSILON>(xx, yy[3], yy[4], yy[5], b);
+        link64<FJ_KERNEL_EPSILON>(a, b, 1.0, r0x, r0y, r0z, kEps * r0sq * r0sq, rc2, acc);
+    } else if (kernel == FJ_KERNEL_CUTOFF) {
+        Vtx64<FJ_KERNEL_CUTOFF> a, b;
+        vtx64<FJ_KERNEL_CUTOFF>(xx, yy[0], yy[1], yy[2], a);
+        vtx64<FJ_KERNEL_CUTOFF>(xx, yy[3], yy[4], yy[5], b);
+        link64<FJ_KERNEL_CUTOFF>(a, b, 1.0, r0x, r0y, r0z, r0sq, rc2, acc);
+    } else {
+        Vtx64<FJ_KERNEL_PLAIN> a, b;
+        vtx64<FJ_KERNEL_PLAIN>(xx, yy[0], yy[1], yy[2], a);
+        vtx64<FJ_KERNEL_PLAIN>(xx, yy[3], yy[4], yy[5], b);
+        link64<FJ_KERNEL_PLAIN>(a, b, 1.0, r0x, r0y, r0z, r0sq, rc2, acc);
+    }
+    out[i * 3 + 0] = acc[0];
+    out[i * 3 + 1] = acc[1];
+    out[i * 3 + 2] = acc[2];
+}
+
+int biot_savart_pairs(const double* x, const double* y, int64_t n, int kernel, double r_cut,
+                      double* out, cudaStream_t s) {
+    if (n < 0) return fail(FJ_ERR_SHAPE, "fj_biot_savart: n_pairs < 0");
+    if (kernel < 0 || kernel > 2) return fail(FJ_ERR_UNSUPPORTED, "fj_biot_savart: kernel %d", kernel);
+    if (n == 0) return FJ_OK;
+    bs_pairs_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(x, y, n, kernel, r_cut * r_cut, out);
+    FJ_LAUNCH_CHECK("bs_pairs_kernel");
+    return FJ_OK;
+}
+
+}  // namespace fj

@@ -1,0 +1,206 @@
+/*
+ * fj_uvlm.h -- C ABI of libfj_uvlm.so, the B200 (sm_100a) UVLM hot path.
+ *
+ * The reference (FLAPJAX, src/flapjax/aero/) has no FFI layer: its hot path is a set of
+ * JAX functions that uvlm.py imports by name.  Each entry point below replaces one of
+ * them, with the same array layouts (C-contiguous float64, lattice zeta
+ * (rows+1, cols+1, 3), circulation (rows, cols)).  The reference function replaced is
+ * cited beside each declaration (paths relative to src/flapjax/).
+ *
+ * Conventions
+ *   - Every pointer argument named d_* is DEVICE memory; everything else is host memory.
+ *   - The caller owns every buffer.  No entry point allocates device memory: scratch
+ *     space comes from the caller through (ws, ws_bytes), sized by the matching
+ *     *_workspace_size function.
+ *   - Calls are ordered on the given stream and return without synchronising, except
+ *     where a function says it reads a device result back.
+ *   - The return value is FJ_OK (0) or a negative FJ_ERR_* code; fj_last_error_string()
+ *     (thread-local) then describes the failure.
+ */
+#ifndef FJ_UVLM_H
+#define FJ_UVLM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define FJ_API __attribute__((visibility("default")))
+#else
+#define FJ_API
+#endif
+
+typedef struct CUstream_st* fj_stream_t; /* a cudaStream_t; NULL = legacy default stream */
+
+/* status codes */
+#define FJ_OK 0
+#define FJ_ERR_SHAPE (-1)         /* a size/shape argument is invalid */
+#define FJ_ERR_NONFINITE (-2)     /* a NaN/Inf was found where it is not allowed */
+#define FJ_ERR_SINGULAR (-3)      /* exact zero pivot in a factorisation */
+#define FJ_ERR_TIMEOUT (-4)       /* a bounded device wait gave up */
+#define FJ_ERR_NOMEM (-5)         /* the workspace given is smaller than required */
+#define FJ_ERR_CUDA (-6)          /* a CUDA runtime call failed */
+#define FJ_ERR_UNSUPPORTED (-7)   /* option combination not implemented */
+#define FJ_ERR_NOT_CONVERGED (-8) /* iterative refinement did not reach its tolerance */
+
+/* Biot-Savart segment kernels, aero/utils.py:580-648 (selected by UVLM(kernel=...),
+ * aero/uvlm.py:173, 280-285). */
+#define FJ_KERNEL_EPSILON 0 /* biot_savart_epsilon, aero/utils.py:606-623 (default) */
+#define FJ_KERNEL_CUTOFF 1  /* biot_savart_cutoff, aero/utils.py:626-648, run-time radius */
+#define FJ_KERNEL_PLAIN 2   /* biot_savart, aero/utils.py:580-592 (FP64 only) */
+
+/* arithmetic of the Biot-Savart sums and the solve */
+#define FJ_PREC_FP64 0  /* plain FP64 everywhere: the reference's arithmetic */
+#define FJ_PREC_MIXED 1 /* FP32 Biot-Savart with FP64 accumulation, FP32 factors + FP64 refinement */
+
+/* background flow, aero/flowfields.py */
+#define FJ_FLOW_CONSTANT 0         /* Constant, aero/flowfields.py:87-97 */
+#define FJ_FLOW_ONE_MINUS_COSINE 1 /* OneMinusCosine, aero/flowfields.py:100-181 */
+
+#define FJ_MAX_SURF 8
+
+typedef struct fj_flowfield {
+    int kind;            /* FJ_FLOW_* */
+    int relative_motion; /* FlowField.relative_motion */
+    double u_inf[3];
+    double rho;
+    double gust_length;        /* OneMinusCosine: half the full gust length */
+    double gust_amplitude;
+    double gust_travel_dir[3]; /* unit vectors, normalised by the caller */
+    double gust_amplitude_dir[3];
+    double gust_x0[3];
+} fj_flowfield;
+
+/* Everything about a UVLM case that is fixed for its lifetime: UVLM.__init__
+ * (aero/uvlm.py:166-339) plus set_design_variables (:387-472) scalars. */
+typedef struct fj_case_config {
+    int n_surf;
+    int m[FJ_MAX_SURF];      /* chordwise bound panels per surface */
+    int n[FJ_MAX_SURF];      /* spanwise panels per surface */
+    int m_star[FJ_MAX_SURF]; /* wake rows per surface */
+    int n_nodes;             /* beam nodes in the hg arrays */
+    int n_tstep;             /* time slots in the output arrays */
+    int kernel;              /* FJ_KERNEL_* */
+    double r_cut;            /* cutoff radius for FJ_KERNEL_CUTOFF */
+    int free_wake;
+    int mirror;              /* 1: image system across (mirror_point, mirror_normal) */
+    double mirror_point[3];
+    double mirror_normal[3]; /* unit */
+    double dt;
+    double gamma_dot_relaxation;
+    fj_flowfield flow;
+    int precision;           /* FJ_PREC_* */
+} fj_case_config;
+
+/* Device buffers of one case.  Surfaces are concatenated in the innermost extent of
+ * each time slot: field[i_ts][sum over surfaces of the per-surface block], so slot
+ * i_ts of surface s is a C-contiguous block in the AeroCase layout
+ * (aero/data_structures.py:43-615, AeroCase fields). */
+typedef struct fj_case_buffers {
+    /* inputs */
+    const double* d_zeta_b0;   /* sum_s (m+1)(n+1)*3: local grid (UVLM.zeta_b0) */
+    const int32_t* d_dof_mapping; /* sum_s (n+1): spanwise vertex -> beam node */
+    const double* d_hg_t;      /* (n_tstep, n_nodes, 4, 4) SE(3) node frames */
+    const double* d_hg_dot_t;  /* (n_tstep, n_nodes, 4, 4) their time derivatives */
+    /* outputs, time-major (n_tstep, ...) */
+    double* d_t;               /* (n_tstep,) */
+    double* d_zeta_b;          /* (m+1, n+1, 3) per surface */
+    double* d_zeta_b_dot;      /* (m+1, n+1, 3) */
+    double* d_zeta_w;          /* (m_star+1, n+1, 3) */
+    double* d_c;               /* (m, n, 3) collocation points */
+    double* d_nc;              /* (m, n, 3) area normals */
+    double* d_gamma_b;         /* (m, n) */
+    double* d_gamma_b_dot;     /* (m, n) */
+    double* d_gamma_w;         /* (m_star, n) */
+    double* d_f_steady;        /* (m+1, n+1, 3) */
+    double* d_f_unsteady;      /* (m+1, n+1, 3) */
+    double* d_alpha;           /* (n,) strip angle of attack */
+    double* d_force_total;     /* (3,) per slot: sum over vertices of f_steady+f_unsteady */
+} fj_case_buffers;
+
+/* ---------------------------------------------------------------------------------
+ * Library
+ * ------------------------------------------------------------------------------- */
+FJ_API const char* fj_last_error_string(void);
+FJ_API int fj_version(void); /* major*10000 + minor*100 + patch */
+
+/* ---------------------------------------------------------------------------------
+ * Case-level entry points (replace UVLM.solve_static / solve_prescribed_dynamic /
+ * case_solve, aero/uvlm.py:1119-1406).  The workspace carries cached state between
+ * calls of one case (factors, streams) and must stay alive for the case's lifetime.
+ * ------------------------------------------------------------------------------- */
+FJ_API int fj_case_workspace_size(const fj_case_config* cfg, size_t* bytes);
+
+/* UVLM.solve_static (aero/uvlm.py:1286-1333): writes time slot 0 of the outputs
+ * (zeta_b from hg_t[0]; zeta_b_dot, gamma_b_dot, f_unsteady zero). */
+FJ_API int fj_solve_static(const fj_case_config* cfg, const fj_case_buffers* bufs, int horseshoe,
+                    double t0, void* d_ws, size_t ws_bytes, fj_stream_t stream);
+
+/* UVLM.solve_prescribed_dynamic (aero/uvlm.py:1335-1406): time steps
+ * i_first..i_last-1 (1 <= i_first), each a case_solve (aero/uvlm.py:1119-1215) reading
+ * slot i-1 and writing slot i.  Slot i_first-1 must hold a solution (e.g. from
+ * fj_solve_static).  Reads one status word back after the last step. */
+FJ_API int fj_solve_prescribed_dynamic(const fj_case_config* cfg, const fj_case_buffers* bufs,
+                                int i_first, int i_last, void* d_ws, size_t ws_bytes,
+                                fj_stream_t stream);
+
+/* One case_solve (aero/uvlm.py:1119-1215) at slot i_ts >= 1 with the node frames of
+ * slots i_ts (hg_n, hg_dot_n) and i_ts-1 (hg_nm1) taken from the hg arrays.  This is
+ * the call the coupled FSI loop makes (structure/beam.py:2656-2667). */
+FJ_API int fj_case_step(const fj_case_config* cfg, const fj_case_buffers* bufs, int i_ts,
+                 void* d_ws, size_t ws_bytes, fj_stream_t stream);
+
+/* ---------------------------------------------------------------------------------
+ * Function-level entry points (the names uvlm.py imports, aero/uvlm.py:15, :32-43).
+ * ------------------------------------------------------------------------------- */
+
+/* biot_savart_epsilon / biot_savart_cutoff / biot_savart (aero/utils.py:580-648)
+ * evaluated pairwise: d_x (n_pairs, 3), d_y (n_pairs, 2, 3) -> d_out (n_pairs, 3). */
+FJ_API int fj_biot_savart(const double* d_x, const double* d_y, int64_t n_pairs, int kernel,
+                   double r_cut, double* d_out, fj_stream_t stream);
+
+/* compute_v_ind (aero/aic.py:248-310): induced velocity at n_targets points of the
+ * lattices d_zetas[i] ((rows[i]+1, cols[i]+1, 3)) with ring circulations d_gammas[i]
+ * ((rows[i], cols[i])), minus their images when mirror_point != NULL.  d_zetas and
+ * d_gammas are HOST arrays of device pointers. */
+FJ_API int fj_vind_workspace_size(int64_t n_targets, const int* rows, const int* cols,
+                           int n_lattices, int mirror, int precision, size_t* bytes);
+FJ_API int fj_vind(const double* d_targets, int64_t n_targets, const double* const* d_zetas,
+            const double* const* d_gammas, const int* rows, const int* cols, int n_lattices,
+            const double* mirror_point, const double* mirror_normal, int kernel, double r_cut,
+            int precision, double* d_v_out, void* d_ws, size_t ws_bytes, fj_stream_t stream);
+
+/* compute_aic_solve (aero/aic.py:137-187): the (sum m*n)^2 row-major AIC of the bound
+ * lattices at their own collocation points, projected on the area normals.  When
+ * d_zetas_w != NULL (static solve) each surface's wake influence is lumped onto its
+ * trailing-edge column (add_wake_influence, aero/aic.py:190-205). */
+FJ_API int fj_aic_assemble(const double* const* d_zetas_b, const int* m, const int* n, int n_surf,
+                    const double* const* d_zetas_w, const int* m_star,
+                    const double* mirror_point, const double* mirror_normal, int kernel,
+                    double r_cut, double* d_aic, void* d_ws, size_t ws_bytes,
+                    fj_stream_t stream);
+FJ_API int fj_aic_workspace_size(const int* m, const int* n, int n_surf, size_t* bytes);
+
+/* jnp.linalg.solve (aero/uvlm.py:985) split as LAPACK getrf/getrs, row-major A.
+ * fj_lu_factor overwrites d_a with L\U and writes 0-based pivot rows to d_piv (n). */
+FJ_API int fj_lu_workspace_size(int n, size_t* bytes);
+FJ_API int fj_lu_factor(double* d_a, int n, int32_t* d_piv, void* d_ws, size_t ws_bytes,
+                 fj_stream_t stream);
+FJ_API int fj_lu_solve(const double* d_lu, int n, const int32_t* d_piv, double* d_b, void* d_ws,
+                size_t ws_bytes, fj_stream_t stream);
+
+/* Mixed-precision solve of A x = b: FP32 factors of A (recomputed when refactor != 0)
+ * kept in the workspace, then FP64 iterative refinement x += M (b - A x) with the FP64
+ * residual.  Writes the final relative residual ||b-Ax||_inf / ||b||_inf to
+ * *d_resid (device, 1 double). */
+FJ_API int fj_solve_mixed_workspace_size(int n, size_t* bytes);
+FJ_API int fj_solve_mixed(const double* d_a, int n, const double* d_b, double* d_x, int refactor,
+                   double* d_resid, void* d_ws, size_t ws_bytes, fj_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FJ_UVLM_H */
