@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""UVLM time-step throughput on B200.
+
+Workload (the configuration the headline metric is quoted on): free-wake UVLM, 16 x 128
+bound panels (AIC 2048 x 2048), 200 wake rows (25 600 wake rings), linear twist and
+NACA camber from a seeded RNG, cutoff kernel with core radius 1e-3 c, started from the
+static solution.  A "step" is one UVLM time step (case_solve).
+
+value   steps/s of the mixed-precision path (FP32 Biot-Savart, FP32 factors + FP64
+        refinement), device-timed with CUDA events per step, L2 flushed between steps
+        (a 256 MB write outside the timed events), max over ranks.
+e2e     the same metric through the C ABI with host buffers: every step copies its node
+        frames from pinned host memory, runs fj_solve_prescribed_dynamic, and reads the
+        step's solution slot back to pinned host memory.
+fp64_gpu  the plain FP64 path on the same steps, and the mixed path's CL/CD error
+        against it.
+
+--impl reference  times the CPU FP64 oracle (the reference's arithmetic restated; the
+        reference itself is JAX, which is not installed) on a bounded sample of the same
+        workload and prints the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "UVLM time-steps/s (free wake 16x128, W=200)"
+UNIT = "steps/s"
+FLOPS_PER_PAIR = 70.0  # Biot-Savart convention: FMA = 2, rsqrt/div = 1 per (target, filament)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
+    ap.add_argument("--small", action="store_true", help="a reduced workload (for quick checks)")
+    return ap.parse_args()
+
+
+def workload(args, n_steps):
+    from flapjax_b200 import cases
+
+    if args.small:
+        return cases.wing_free(m=8, n=32, m_star=40, n_steps=n_steps)
+    return cases.wing_free(n_steps=n_steps)
+
+
+# --------------------------------------------------------------------------------------
+# clocks
+# --------------------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": [], "samples": 0}
+        loaded = [v for v in sm if v > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------------------
+def make_case(case, precision, n_slots):
+    import flapjax_b200 as fj
+
+    kernel = fj.cutoff_kernel(case.r_cut) if case.kernel == "cutoff" else fj.biot_savart_epsilon
+    uv = fj.UVLM([fj.GridDiscretisation(case.m, case.n, case.m_star)], np.arange(case.n + 1), kernel=kernel,
+                 free_wake=case.free_wake, precision=precision)
+    ff = fj.Constant(case.u_inf, case.rho, True)
+    uv.set_design_variables(dt=case.dt, flowfield=ff, zeta_b0=case.zeta_b0, hg0=case.hg0)
+    init = uv.solve_static()
+    dc = uv.make_device_case(n_slots)
+    uv.load_initial(dc, init)
+    dc.set_hg(case.hg_t[:n_slots], case.hg_dot_t[:n_slots])
+    return uv, dc
+
+
+def coeffs(ft, case):
+    a = np.deg2rad(case.alpha_deg)
+    q = 0.5 * case.rho * case.u_mag**2 * case.s_ref
+    return ft @ np.array((-np.sin(a), 0.0, np.cos(a))) / q, ft @ np.array((np.cos(a), 0.0, np.sin(a))) / q
+
+
+def run_device_steps(dc, first, last, flush, torch, profile=False):
+    """Steps first..last-1 one call each; returns per-step device ms (events) and the
+    profile of the Biot-Savart kernels if requested."""
+    from flapjax_b200 import _lib
+
+    stream = torch.cuda.current_stream()
+    times = []
+    prof = _lib.FjProfile()
+    if profile:
+        _lib.call("fj_profile_begin")
+    for i in range(first, last):
+        if flush is not None:
+            flush.fill_(i & 0xFF)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dc.solve_dynamic(i, i + 1, reuse_factors=i > 1)
+        e1.record(stream)
+        times.append((e0, e1))
+    torch.cuda.synchronize()
+    if profile:
+        _lib.call("fj_profile_end", C_byref(prof))
+    return [a.elapsed_time(b) for a, b in times], prof
+
+
+def C_byref(x):
+    import ctypes
+
+    return ctypes.byref(x)
+
+
+def e2e_run(uv, dc, case, first, last, torch):
+    """Per step: H2D of the step's frames (pinned), the step through the C ABI, D2H of
+    the step's solution slot (pinned).  Returns (ms per step list, bytes in, bytes out)."""
+    n_nodes = case.hg0.shape[0]
+    hg = torch.from_numpy(np.ascontiguousarray(case.hg_t)).pin_memory()
+    hgd = torch.from_numpy(np.ascontiguousarray(case.hg_dot_t)).pin_memory()
+    fields = list(dc.arrays)
+    outs = {k: torch.empty(dc.arrays[k].shape[1], dtype=torch.float64).pin_memory() for k in fields}
+    out_ft = torch.empty(3, dtype=torch.float64).pin_memory()
+    stream = torch.cuda.current_stream()
+    bytes_in = 2 * n_nodes * 16 * 8
+    bytes_out = sum(v.numel() * 8 for v in outs.values()) + 3 * 8
+    ev = []
+    for i in range(first, last):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dc.hg_t[i].copy_(hg[i], non_blocking=True)
+        dc.hg_dot_t[i].copy_(hgd[i], non_blocking=True)
+        dc.solve_dynamic(i, i + 1, reuse_factors=i > 1)
+        for k in fields:
+            outs[k].copy_(dc.arrays[k][i], non_blocking=True)
+        out_ft.copy_(dc.force_total[i], non_blocking=True)
+        e1.record(stream)
+        ev.append((e0, e1))
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev], bytes_in, bytes_out
+
+
+def cpu_sample(case, budget_s):
+    """Time the FP64 oracle (NumPy, one thread of BLAS-free array code) on a bounded
+    sample of a step: the induced velocity at a subset of the wake vertices from the
+    bound and wake lattices.  Steps/s = (pairs/s) / (pairs per step); the dense solve's
+    share of a CPU step is below 1 % at this size and is not sampled."""
+    from oracle import uvlm_ref as R
+
+    zb = case.zeta_b0 + case.hg0[0, :3, 3]
+    w = case.m_star
+    zw = zb[-1][None] + np.arange(w + 1)[:, None, None] * (case.dt * case.u_inf)[None, None, :]
+    rng = np.random.default_rng(0)
+    gb = rng.normal(size=(case.m, case.n)) * 0.1
+    gw = rng.normal(size=(w, case.n)) * 0.1
+    targets = zw[:-1].reshape(-1, 3)
+    filaments = sum(r * (c + 1) + (r + 1) * c for r, c in ((case.m, case.n), (w, case.n)))
+    n_t, t0, chunk = 0, time.perf_counter(), 32
+    while time.perf_counter() - t0 < budget_s and n_t < targets.shape[0]:
+        R.compute_v_ind(targets[n_t:n_t + chunk], [zb, zw], [gb, gw], case.kernel, None, case.r_cut)
+        n_t += chunk
+    el = time.perf_counter() - t0
+    pairs = n_t * filaments
+    steps_per_s = pairs / el / case.pairs_per_step()
+    return {"value": steps_per_s, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"NumPy FP64 oracle: induced velocity at {n_t} wake vertices from {filaments} filaments "
+                      f"({pairs:.3g} pairs in {el:.1f} s), scaled by {case.pairs_per_step():.4g} pairs per step",
+            "pairs_per_s": pairs / el}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+    import torch.distributed as dist
+
+    from flapjax_b200 import _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    assert args.warmup >= 3, "at least 3 warm-up steps"
+    K, W = args.steps, args.warmup
+    n_slots = 1 + W + K
+    case = workload(args, n_slots - 1)
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    # -- mixed path: value ---------------------------------------------------------------
+    uv, dc = make_case(case, "mixed", n_slots)
+    run_device_steps(dc, 1, 1 + W, flush, torch)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = _lib.load().fj_launch_count()
+    with ClockSampler(local) as clk:
+        ms, prof = run_device_steps(dc, 1 + W, n_slots, flush, torch, profile=True)
+    launches = _lib.load().fj_launch_count() - launches0
+    torch.cuda.synchronize()
+    t_ms = sum(ms)
+    if world > 1:
+        tt = torch.tensor([t_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+        dist.barrier()
+    value = world * K / (t_ms * 1e-3)
+    ft_mixed = dc.force_total[1 + W:n_slots].cpu().numpy()
+
+    # -- roofline of the dominant kernel (Biot-Savart sums) -------------------------------
+    peak = ctypes_peak(torch)
+    achieved = prof.vind_pairs * FLOPS_PER_PAIR / (prof.vind_ms * 1e-3) / 1e12 if prof.vind_ms > 0 else None
+    roof = {"kernel": "vind32 (FP32 Biot-Savart sums)", "bound": "fp32", "achieved": achieved,
+            "peak": peak, "unit": "TFLOP/s", "frac": (achieved / peak) if achieved and peak else None,
+            "traffic": None, "peak_source": "measured in-run (fj_peak_fp32: FP32 FMA chains); "
+                                             "MEASURED_PEAKS.json has no FP32 CUDA-core figure",
+            "pairs_per_launch": prof.vind_pairs / max(prof.vind_launches, 1),
+            "kernel_ms_per_step": prof.vind_ms / K, "share_of_step": prof.vind_ms / t_ms if t_ms else None,
+            "pairs_per_s": prof.vind_pairs / (prof.vind_ms * 1e-3) if prof.vind_ms else None}
+
+    # -- plain FP64 path and CL error -----------------------------------------------------
+    fp64 = None
+    if not args.no_fp64:
+        del dc
+        _, d64 = make_case(case, "fp64", n_slots)
+        run_device_steps(d64, 1, 1 + W, flush, torch)
+        ms64, _ = run_device_steps(d64, 1 + W, n_slots, flush, torch)
+        ft64 = d64.force_total[1 + W:n_slots].cpu().numpy()
+        cl64, cd64 = coeffs(ft64, case)
+        clm, cdm = coeffs(ft_mixed, case)
+        fp64 = {"value": K / (sum(ms64) * 1e-3), "unit": UNIT, "ms_per_step": sum(ms64) / K,
+                "speedup_mixed_over_fp64": (sum(ms64) / t_ms) if t_ms else None,
+                "cl_rel_err_max": float(np.max(np.abs(clm - cl64) / np.abs(cl64))),
+                "cd_rel_err_max": float(np.max(np.abs(cdm - cd64)) / np.max(np.abs(cd64)))}
+        del d64
+
+    # -- e2e through the C ABI with host buffers -------------------------------------------
+    e2e = None
+    if not args.no_e2e:
+        uv2, dce = make_case(case, "mixed", n_slots)
+        e2e_run(uv2, dce, case, 1, 1 + W, torch)
+        if world > 1:
+            dist.barrier()
+        ms_e, bi, bo = e2e_run(uv2, dce, case, 1 + W, n_slots, torch)
+        te = sum(ms_e)
+        if world > 1:
+            tt = torch.tensor([te], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt.item())
+        e2e = {"value": world * K / (te * 1e-3), "unit": UNIT, "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo}
+        del dce
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    cpu = cpu_sample(case, args.cpu_seconds) if world == 1 else None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32+fp64", "data": "synthetic (seeded wing geometry, no dataset)",
+        "config": {"workload": "free-wake UVLM 16x128 bound, W=200 wake rows, cutoff kernel r=1e-3c, twist+camber "
+                               "seeded, static-solve start" + (" [SMALL]" if args.small else ""),
+                   "m": case.m, "n": case.n, "m_star": case.m_star, "pairs_per_step": case.pairs_per_step(),
+                   "precision": "mixed (FP32 Biot-Savart, FP32 factors + FP64 refinement)",
+                   "l2": "flushed between steps (256 MB write outside the timed events)",
+                   "parallelism": f"independent case replica per GPU x{world}", "seed": case.seed},
+        "e2e": e2e, "fp64_gpu": fp64, "roofline": roof, "cpu_baseline": cpu,
+        "gpu_launches": int(launches), "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def ctypes_peak(torch):
+    import ctypes
+
+    from flapjax_b200 import _lib
+
+    v = ctypes.c_double()
+    _lib.call("fj_peak_fp32", ctypes.byref(v), torch.cuda.current_stream().cuda_stream)
+    return v.value
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    case = workload(args, 1)
+    steps = []
+    for _ in range(args.warmup):
+        cpu_sample(case, min(2.0, args.cpu_seconds))
+    total = 0.0
+    budget = max(1.0, args.cpu_seconds / max(1, min(args.steps, 10)))
+    for _ in range(min(args.steps, 10)):
+        r = cpu_sample(case, budget)
+        steps.append(r["value"])
+        total += 1.0 / r["value"]
+    value = len(steps) / total
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+            "steps": len(steps), "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "dtype": "fp64", "data": "synthetic", "config": {"workload": "free-wake UVLM 16x128, W=200"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                             "sample": r["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -98,6 +98,18 @@ class FjCaseBuffers(C.Structure):
     ]
 
 
+class FjProfile(C.Structure):
+    _fields_ = [
+        ("launches", C.c_int64),
+        ("vind_launches", C.c_int64),
+        ("vind_ms", C.c_double),
+        ("vind_ms_max", C.c_double),
+        ("vind_pairs", C.c_double),
+    ]
+
+
+FJ_REUSE_FACTORS = 1
+
 # name -> (restype, argtypes)
 _SIGS = {
     "fj_last_error_string": (C.c_char_p, []),
@@ -106,8 +118,13 @@ _SIGS = {
     "fj_solve_static": (C.c_int, [C.POINTER(FjCaseConfig), C.POINTER(FjCaseBuffers), C.c_int, C.c_double, _P,
                                   C.c_size_t, _P]),
     "fj_solve_prescribed_dynamic": (C.c_int, [C.POINTER(FjCaseConfig), C.POINTER(FjCaseBuffers), C.c_int, C.c_int,
-                                              _P, C.c_size_t, _P]),
-    "fj_case_step": (C.c_int, [C.POINTER(FjCaseConfig), C.POINTER(FjCaseBuffers), C.c_int, _P, C.c_size_t, _P]),
+                                              C.c_int, _P, C.c_size_t, _P]),
+    "fj_case_step": (C.c_int, [C.POINTER(FjCaseConfig), C.POINTER(FjCaseBuffers), C.c_int, C.c_int, _P, C.c_size_t,
+                               _P]),
+    "fj_peak_fp32": (C.c_int, [C.POINTER(C.c_double), _P]),
+    "fj_launch_count": (C.c_int64, []),
+    "fj_profile_begin": (C.c_int, []),
+    "fj_profile_end": (C.c_int, [C.c_void_p]),
     "fj_biot_savart": (C.c_int, [_P, _P, C.c_int64, C.c_int, C.c_double, _P, _P]),
     "fj_vind_workspace_size": (C.c_int, [C.c_int64, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.c_int, C.c_int,
                                          C.POINTER(C.c_size_t)]),

@@ -134,15 +134,15 @@ int aic_launch(const AicArgs& a, const int* d_run_flag, cudaStream_t s) {
     switch (a.kernel) {
         case FJ_KERNEL_EPSILON:
             FJ_CUDA(cudaFuncSetAttribute(aic_kernel<FJ_KERNEL_EPSILON>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            aic_kernel<FJ_KERNEL_EPSILON><<<(unsigned)a.n_rows, 256, smem, s>>>(a, d_run_flag);
+            aic_kernel<FJ_KERNEL_EPSILON><<<(unsigned)a.n_rows, 256, smem, s>>>(a, d_run_flag); note_launch();
             break;
         case FJ_KERNEL_CUTOFF:
             FJ_CUDA(cudaFuncSetAttribute(aic_kernel<FJ_KERNEL_CUTOFF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            aic_kernel<FJ_KERNEL_CUTOFF><<<(unsigned)a.n_rows, 256, smem, s>>>(a, d_run_flag);
+            aic_kernel<FJ_KERNEL_CUTOFF><<<(unsigned)a.n_rows, 256, smem, s>>>(a, d_run_flag); note_launch();
             break;
         case FJ_KERNEL_PLAIN:
             FJ_CUDA(cudaFuncSetAttribute(aic_kernel<FJ_KERNEL_PLAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            aic_kernel<FJ_KERNEL_PLAIN><<<(unsigned)a.n_rows, 256, smem, s>>>(a, d_run_flag);
+            aic_kernel<FJ_KERNEL_PLAIN><<<(unsigned)a.n_rows, 256, smem, s>>>(a, d_run_flag); note_launch();
             break;
         default:
             return fail(FJ_ERR_UNSUPPORTED, "aic: unknown kernel %d", a.kernel);

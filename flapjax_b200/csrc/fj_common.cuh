@@ -24,6 +24,14 @@ constexpr float kCollinearSin = 4e-6f;
 void set_error(const char* fmt, ...);
 int fail(int code, const char* fmt, ...);
 
+// Count of kernels this library has launched (read through fj_launch_count).
+void note_launch(int n = 1);
+
+// Opt-in timing of the Biot-Savart sum kernels with CUDA events on their stream
+// (fj_profile_begin / fj_profile_end).  prof_start returns -1 when profiling is off.
+int prof_start(cudaStream_t s);
+void prof_stop(int slot, cudaStream_t s, double pairs);
+
 inline int cuda_status(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return FJ_OK;
     return fail(FJ_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));

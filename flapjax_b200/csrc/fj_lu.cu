@@ -179,12 +179,14 @@ static int lu_factor_impl(T* a, int n, int32_t* piv, int* d_info, cudaStream_t s
     FJ_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int), s));
     for (int k = 0; k < n; k += NB) {
         const int nb = min(NB, n - k);
-        lu_panel_kernel<T, NB><<<1, 1024, (size_t)(n - k) * NB * sizeof(T), s>>>(a, n, k, piv, d_info);
-        if (n > nb) lu_swap_trsm_kernel<T, NB><<<(n + 255) / 256, 256, 0, s>>>(a, n, k, piv);
+        lu_panel_kernel<T, NB><<<1, 1024, (size_t)(n - k) * NB * sizeof(T), s>>>(a, n, k, piv, d_info); note_launch();
+        if (n > nb) {
+            lu_swap_trsm_kernel<T, NB><<<(n + 255) / 256, 256, 0, s>>>(a, n, k, piv); note_launch();
+        }
         const int rem = n - k - nb;
         if (rem > 0) {
             dim3 g((rem + 63) / 64, (rem + 63) / 64);
-            lu_update_kernel<T, NB><<<g, 256, 0, s>>>(a, n, k);
+            lu_update_kernel<T, NB><<<g, 256, 0, s>>>(a, n, k); note_launch();
         }
     }
     FJ_LAUNCH_CHECK("lu_factor");
@@ -262,7 +264,7 @@ int lu_solve64(const double* lu, int n, const int32_t* piv, double* b, cudaStrea
     const size_t smem = (size_t)n * sizeof(double);
     if (smem > 220 * 1024) return fail(FJ_ERR_UNSUPPORTED, "lu_solve: n=%d too large", n);
     FJ_CUDA(cudaFuncSetAttribute(lu_solve64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    lu_solve64_kernel<<<1, 1024, smem, s>>>(lu, n, piv, b);
+    lu_solve64_kernel<<<1, 1024, smem, s>>>(lu, n, piv, b); note_launch();
     FJ_LAUNCH_CHECK("lu_solve64_kernel");
     return FJ_OK;
 }
@@ -350,7 +352,7 @@ int lu_inverse32(const float* lu, int n, const int32_t* piv, float* x, cudaStrea
     const size_t smem = (size_t)n * kInvCols * sizeof(float);
     if (smem > 220 * 1024) return fail(FJ_ERR_UNSUPPORTED, "lu_inverse32: n=%d too large", n);
     FJ_CUDA(cudaFuncSetAttribute(lu_inverse32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    lu_inverse32_kernel<<<(n + kInvCols - 1) / kInvCols, 512, smem, s>>>(lu, n, piv, x);
+    lu_inverse32_kernel<<<(n + kInvCols - 1) / kInvCols, 512, smem, s>>>(lu, n, piv, x); note_launch();
     FJ_LAUNCH_CHECK("lu_inverse32_kernel");
     return FJ_OK;
 }
@@ -362,7 +364,7 @@ __global__ void convert64to32_kernel(const double* __restrict__ a, float* __rest
 
 int convert64to32(const double* a, float* b, int64_t count, cudaStream_t s) {
     if (count == 0) return FJ_OK;
-    convert64to32_kernel<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(a, b, count);
+    convert64to32_kernel<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(a, b, count); note_launch();
     FJ_LAUNCH_CHECK("convert64to32_kernel");
     return FJ_OK;
 }
@@ -429,13 +431,13 @@ int refine_solve(const double* a, const float* xinv, int n, const double* b, dou
                  double* d_resid, int n_iter, cudaStream_t s) {
     const int wpb = 8;
     const unsigned grid = (unsigned)((n + wpb - 1) / wpb);
-    gemv32_kernel<<<grid, wpb * 32, 0, s>>>(xinv, b, n, x, 0);
+    gemv32_kernel<<<grid, wpb * 32, 0, s>>>(xinv, b, n, x, 0); note_launch();
     for (int it = 0; it < n_iter; ++it) {
-        residual64_kernel<<<grid, wpb * 32, 0, s>>>(a, x, b, n, r_buf);
-        gemv32_kernel<<<grid, wpb * 32, 0, s>>>(xinv, r_buf, n, x, 1);
+        residual64_kernel<<<grid, wpb * 32, 0, s>>>(a, x, b, n, r_buf); note_launch();
+        gemv32_kernel<<<grid, wpb * 32, 0, s>>>(xinv, r_buf, n, x, 1); note_launch();
     }
-    residual64_kernel<<<grid, wpb * 32, 0, s>>>(a, x, b, n, r_buf);
-    rel_resid_kernel<<<1, 1024, 0, s>>>(r_buf, b, n, d_resid);
+    residual64_kernel<<<grid, wpb * 32, 0, s>>>(a, x, b, n, r_buf); note_launch();
+    rel_resid_kernel<<<1, 1024, 0, s>>>(r_buf, b, n, d_resid); note_launch();
     FJ_LAUNCH_CHECK("refine_solve");
     return FJ_OK;
 }

@@ -679,6 +679,7 @@ static int make_plan(const fj_case_config* cfg, void* ws, size_t ws_bytes, Plan&
 struct StreamBuilder {
     PackArgs a;
     int n = 0;
+    int64_t n_links = 0;
     void init(const Plan& p) {
         memset(&a, 0, sizeof(a));
         a.kernel = p.cfg.kernel;
@@ -688,6 +689,7 @@ struct StreamBuilder {
             a.mirror.nrm[d] = p.cfg.mirror_normal[d];
         }
         n = 0;
+        n_links = 0;
         a.offset[0] = 0;
     }
     void add(const Plan& p, const double* zeta, const double* gamma, int rows, int cols) {
@@ -701,6 +703,7 @@ struct StreamBuilder {
             L.sign = i == 0 ? 1.0f : -1.0f;
             L.mirrored = i;
             a.offset[n + 1] = a.offset[n] + stream_len(rows, cols);
+            n_links += lattice_links(rows, cols);
             ++n;
         }
         a.n_lat = n;
@@ -716,7 +719,8 @@ static int pack(const Plan& p, const StreamBuilder& sb, int64_t elem_offset, cud
     return pack_stream32(a, (Elem32*)p.stream + elem_offset, s);
 }
 
-static int vind_sum(const Plan& p, const double* targets, int64_t nt, int64_t n_elem, double* out, cudaStream_t s) {
+static int vind_sum(const Plan& p, const double* targets, int64_t nt, int64_t n_elem, int64_t n_links, double* out,
+                    cudaStream_t s) {
     if (nt == 0) return FJ_OK;
     if (n_elem == 0) {
         FJ_CUDA(cudaMemsetAsync(out, 0, nt * 3 * sizeof(double), s));
@@ -729,6 +733,7 @@ static int vind_sum(const Plan& p, const double* targets, int64_t nt, int64_t n_
     j.n_elem = n_elem;
     j.n_split = choose_split(nt, n_elem, p.cfg.precision);
     j.part = p.part;
+    j.n_links = n_links;
     if ((int64_t)j.n_split * nt * 3 > p.part_elems) return fail(FJ_ERR_NOMEM, "partial buffer too small");
     FJ_TRY(vind_launch(j, p.cfg.precision, p.cfg.kernel, p.cfg.r_cut, s));
     return reduce_partials(p.part, j.n_split, nt, out, 0, 1.0, s);
@@ -783,17 +788,17 @@ static int run_static(const Plan& p, const fj_case_buffers* B, const double* hg,
     double* gw = B->d_gamma_w;
     FJ_CUDA(cudaMemcpyAsync(B->d_t, &t0, sizeof(double), cudaMemcpyHostToDevice, s));
     geom_vertices_kernel<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(L, B->d_zeta_b0, B->d_dof_mapping, hg, nullptr, nullptr,
-                                                                zb, B->d_zeta_b_dot, nullptr, nullptr, 0.0, 0.0);
-    geom_panels_kernel<<<nblk(L.po[L.n_surf]), 256, 0, s>>>(L, zb, nullptr, cc, nc, nullptr);
+                                                                zb, B->d_zeta_b_dot, nullptr, nullptr, 0.0, 0.0); note_launch();
+    geom_panels_kernel<<<nblk(L.po[L.n_surf]), 256, 0, s>>>(L, zb, nullptr, cc, nc, nullptr); note_launch();
     // wake of the solve: initialise_wake or the horseshoe (rows 1, far end at HORSESHOE_LENGTH)
     const double* zw_solve;
     int rows_solve;
     if (horseshoe) {
-        init_wake_kernel<<<nblk(2 * (p.sz_strip + L.n_surf)), 256, 0, s>>>(L, zb, c.flow, c.dt, 1e3, p.hs_zw, 1);
+        init_wake_kernel<<<nblk(2 * (p.sz_strip + L.n_surf)), 256, 0, s>>>(L, zb, c.flow, c.dt, 1e3, p.hs_zw, 1); note_launch();
         zw_solve = p.hs_zw;
         rows_solve = 1;
     } else {
-        init_wake_kernel<<<nblk(L.wvo[L.n_surf]), 256, 0, s>>>(L, zb, c.flow, c.dt, 0.0, zw, 0);
+        init_wake_kernel<<<nblk(L.wvo[L.n_surf]), 256, 0, s>>>(L, zb, c.flow, c.dt, 0.0, zw, 0); note_launch();
         zw_solve = zw;
         rows_solve = -1;
     }
@@ -801,17 +806,17 @@ static int run_static(const Plan& p, const fj_case_buffers* B, const double* hg,
     AicArgs aa;
     fill_aic_args(p, aa, zb, cc, nc, zw_solve, rows_solve);
     FJ_TRY(aic_launch(aa, nullptr, s));
-    rhs_kernel<<<nblk(p.nb), 256, 0, s>>>(p.nb, cc, nullptr, nc, nullptr, c.flow, nullptr, t0, p.rhs);
+    rhs_kernel<<<nblk(p.nb), 256, 0, s>>>(p.nb, cc, nullptr, nc, nullptr, c.flow, nullptr, t0, p.rhs); note_launch();
     FJ_TRY(lu_factor64(p.a64, p.nb, p.piv, p.flags, s));
     FJ_TRY(lu_solve64(p.a64, p.nb, p.piv, p.rhs, s));
     FJ_CUDA(cudaMemcpyAsync(gb, p.rhs, p.nb * sizeof(double), cudaMemcpyDeviceToDevice, s));
     // wake circulation of the solve, and of the stored slot (broadcast over m_star rows)
     double* gw_solve = gw;
     if (horseshoe) {
-        static_gamma_w_kernel<<<nblk(p.sz_strip), 256, 0, s>>>(L, gb, p.hs_gw, 1);
+        static_gamma_w_kernel<<<nblk(p.sz_strip), 256, 0, s>>>(L, gb, p.hs_gw, 1); note_launch();
         gw_solve = p.hs_gw;
     }
-    static_gamma_w_kernel<<<nblk(p.sz_gw + 1), 256, 0, s>>>(L, gb, gw, -1);
+    static_gamma_w_kernel<<<nblk(p.sz_gw + 1), 256, 0, s>>>(L, gb, gw, -1); note_launch();
     // forces: v at midpoints from bound + solve wake, zeta_dot = 0
     StreamBuilder sb;
     sb.init(p);
@@ -824,17 +829,18 @@ static int run_static(const Plan& p, const fj_case_buffers* B, const double* hg,
     }
     for (int q = 0; q < L.n_surf; ++q) sb.add(p, zb + L.vo[q] * 3, gb + L.po[q], L.m[q], L.n[q]);
     FJ_TRY(pack(p, sb, 0, s));
-    force_targets_kernel<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(L, zb, p.targets);
-    FJ_TRY(vind_sum(p, p.targets, L.fo[L.n_surf], sb.len(), p.v, s));
+    force_targets_kernel<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(L, zb, p.targets); note_launch();
+    FJ_TRY(vind_sum(p, p.targets, L.fo[L.n_surf], sb.len(), sb.n_links, p.v, s));
     force_filament_kernel<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(L, zb, nullptr, gb, gw_solve, p.targets, p.v, c.flow,
-                                                                 nullptr, t0, p.ffil);
+                                                                 nullptr, t0, p.ffil); note_launch();
     vertex_forces_kernel<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(L, p.ffil, nullptr, nc, c.flow.rho, B->d_f_steady,
-                                                                B->d_f_unsteady);
-    strip_alpha_kernel<<<nblk(p.sz_strip), 256, 0, s>>>(L, zb, B->d_f_steady, c.flow, nullptr, t0, B->d_alpha);
+                                                                B->d_f_unsteady); note_launch();
+    strip_alpha_kernel<<<nblk(p.sz_strip), 256, 0, s>>>(L, zb, B->d_f_steady, c.flow, nullptr, t0, B->d_alpha); note_launch();
     FJ_CUDA(cudaMemsetAsync(B->d_gamma_b_dot, 0, p.sz_pan * sizeof(double), s));
-    if (horseshoe)  // stored wake geometry is the regular initial wake (uvlm.py:1329-1331)
-        init_wake_kernel<<<nblk(L.wvo[L.n_surf]), 256, 0, s>>>(L, zb, c.flow, c.dt, 0.0, zw, 0);
-    force_total_kernel<<<1, 256, 0, s>>>(L.vo[L.n_surf], B->d_f_steady, B->d_f_unsteady, B->d_force_total);
+    if (horseshoe) {  // stored wake geometry is the regular initial wake (uvlm.py:1329-1331)
+        init_wake_kernel<<<nblk(L.wvo[L.n_surf]), 256, 0, s>>>(L, zb, c.flow, c.dt, 0.0, zw, 0); note_launch();
+    }
+    force_total_kernel<<<1, 256, 0, s>>>(L.vo[L.n_surf], B->d_f_steady, B->d_f_unsteady, B->d_force_total); note_launch();
     FJ_LAUNCH_CHECK("static solve");
     return FJ_OK;
 }
@@ -864,10 +870,10 @@ static int run_step(const Plan& p, const fj_case_buffers* B, int i, const double
     const bool mixed = c.precision == FJ_PREC_MIXED;
 
     // 1. geometry, and t_n = t_{n-1} + dt on the device (case_solve, uvlm.py:1158-1161)
-    advance_time_kernel<<<1, 1, 0, s>>>(B->d_t, i, c.dt);
+    advance_time_kernel<<<1, 1, 0, s>>>(B->d_t, i, c.dt); note_launch();
     geom_vertices_kernel<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(L, B->d_zeta_b0, B->d_dof_mapping, hg_n, hgd_n, hg_nm1,
-                                                                zb_n, zbd_n, p.zeta_nm1, nullptr, 0.0, 0.0);
-    geom_panels_kernel<<<nblk(L.po[L.n_surf]), 256, 0, s>>>(L, zb_n, zbd_n, cc, nc, p.c_dot);
+                                                                zb_n, zbd_n, p.zeta_nm1, nullptr, 0.0, 0.0); note_launch();
+    geom_panels_kernel<<<nblk(L.po[L.n_surf]), 256, 0, s>>>(L, zb_n, zbd_n, cc, nc, p.c_dot); note_launch();
     FJ_LAUNCH_CHECK("geometry");
 
     // 2. wake: free-wake velocities from bound(n-1) + wake(n-1), then shed + convect
@@ -878,12 +884,12 @@ static int run_step(const Plan& p, const fj_case_buffers* B, int i, const double
         for (int q = 0; q < L.n_surf; ++q) sb.add(p, p.zeta_nm1 + L.vo[q] * 3, gb_nm1 + L.po[q], L.m[q], L.n[q]);
         for (int q = 0; q < L.n_surf; ++q) sb.add(p, zw_nm1 + L.wvo[q] * 3, gw_nm1 + L.wpo[q], L.ms[q], L.n[q]);
         FJ_TRY(pack(p, sb, 0, s));
-        gather_wake_targets_kernel<<<nblk(L.wto[L.n_surf]), 256, 0, s>>>(L, zw_nm1, p.targets);
-        FJ_TRY(vind_sum(p, p.targets, L.wto[L.n_surf], sb.len(), p.v, s));
+        gather_wake_targets_kernel<<<nblk(L.wto[L.n_surf]), 256, 0, s>>>(L, zw_nm1, p.targets); note_launch();
+        FJ_TRY(vind_sum(p, p.targets, L.wto[L.n_surf], sb.len(), sb.n_links, p.v, s));
         vw = p.v;
     }
     wake_shed_kernel<<<nblk(L.wvo[L.n_surf] + L.wpo[L.n_surf]), 256, 0, s>>>(L, zb_n, zw_nm1, gb_nm1, gw_nm1, vw, c.flow,
-                                                                             t_n, c.dt, zw_n, gw_n);
+                                                                             t_n, c.dt, zw_n, gw_n); note_launch();
     FJ_LAUNCH_CHECK("wake_shed_kernel");
 
     // 3. AIC (dynamic: bound only)
@@ -893,7 +899,7 @@ static int run_step(const Plan& p, const fj_case_buffers* B, int i, const double
     if (mixed && !refactor) {
         // re-assemble only if the bound lattice differs from the one of the cached AIC
         FJ_CUDA(cudaMemsetAsync(p.flags + 1, 0, sizeof(int), s));
-        changed_kernel<<<nblk(p.sz_zb), 256, 0, s>>>(zb_n, p.zeta_ref, p.sz_zb, p.flags + 1);
+        changed_kernel<<<nblk(p.sz_zb), 256, 0, s>>>(zb_n, p.zeta_ref, p.sz_zb, p.flags + 1); note_launch();
         run_flag = p.flags + 1;
     }
     FJ_TRY(aic_launch(aa, run_flag, s));
@@ -904,8 +910,8 @@ static int run_step(const Plan& p, const fj_case_buffers* B, int i, const double
     for (int q = 0; q < L.n_surf; ++q) sw.add(p, zw_n + L.wvo[q] * 3, gw_n + L.wpo[q], L.ms[q], L.n[q]);
     const int64_t n_wake_elem = sw.len();
     FJ_TRY(pack(p, sw, 0, s));
-    FJ_TRY(vind_sum(p, cc, p.nb, n_wake_elem, p.v, s));
-    rhs_kernel<<<nblk(p.nb), 256, 0, s>>>(p.nb, cc, p.c_dot, nc, p.v, c.flow, t_n, 0.0, p.rhs);
+    FJ_TRY(vind_sum(p, cc, p.nb, n_wake_elem, sw.n_links, p.v, s));
+    rhs_kernel<<<nblk(p.nb), 256, 0, s>>>(p.nb, cc, p.c_dot, nc, p.v, c.flow, t_n, 0.0, p.rhs); note_launch();
     FJ_LAUNCH_CHECK("rhs_kernel");
 
     // 5. solve
@@ -928,19 +934,19 @@ static int run_step(const Plan& p, const fj_case_buffers* B, int i, const double
     sbd.init(p);
     for (int q = 0; q < L.n_surf; ++q) sbd.add(p, zb_n + L.vo[q] * 3, gb_n + L.po[q], L.m[q], L.n[q]);
     FJ_TRY(pack(p, sbd, n_wake_elem, s));
-    force_targets_kernel<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(L, zb_n, p.targets);
-    FJ_TRY(vind_sum(p, p.targets, L.fo[L.n_surf], n_wake_elem + sbd.len(), p.v, s));
+    force_targets_kernel<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(L, zb_n, p.targets); note_launch();
+    FJ_TRY(vind_sum(p, p.targets, L.fo[L.n_surf], n_wake_elem + sbd.len(), sw.n_links + sbd.n_links, p.v, s));
     force_filament_kernel<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(L, zb_n, zbd_n, gb_n, gw_n, p.targets, p.v, c.flow,
-                                                                 t_n, 0.0, p.ffil);
+                                                                 t_n, 0.0, p.ffil); note_launch();
     // 7. gamma_dot, vertex forces, strip alpha, totals
-    gamma_dot_kernel<<<nblk(p.nb), 256, 0, s>>>(p.nb, gb_n, gb_nm1, gbd_nm1, c.dt, c.gamma_dot_relaxation, gbd_n);
+    gamma_dot_kernel<<<nblk(p.nb), 256, 0, s>>>(p.nb, gb_n, gb_nm1, gbd_nm1, c.dt, c.gamma_dot_relaxation, gbd_n); note_launch();
     vertex_forces_kernel<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(L, p.ffil, gbd_n, nc, c.flow.rho,
                                                                 B->d_f_steady + (int64_t)i * p.sz_zb,
-                                                                B->d_f_unsteady + (int64_t)i * p.sz_zb);
+                                                                B->d_f_unsteady + (int64_t)i * p.sz_zb); note_launch();
     strip_alpha_kernel<<<nblk(p.sz_strip), 256, 0, s>>>(L, zb_n, B->d_f_steady + (int64_t)i * p.sz_zb, c.flow, t_n,
-                                                        0.0, B->d_alpha + (int64_t)i * p.sz_strip);
+                                                        0.0, B->d_alpha + (int64_t)i * p.sz_strip); note_launch();
     force_total_kernel<<<1, 256, 0, s>>>(L.vo[L.n_surf], B->d_f_steady + (int64_t)i * p.sz_zb,
-                                         B->d_f_unsteady + (int64_t)i * p.sz_zb, B->d_force_total + (int64_t)i * 3);
+                                         B->d_f_unsteady + (int64_t)i * p.sz_zb, B->d_force_total + (int64_t)i * 3); note_launch();
     FJ_LAUNCH_CHECK("post-processing");
     return FJ_OK;
 }
@@ -955,14 +961,15 @@ static int check_buffers(const fj_case_buffers* B, bool dynamic) {
     return FJ_OK;
 }
 
-static int run_dynamic(const Plan& p, const fj_case_buffers* B, int i_first, int i_last, cudaStream_t s) {
+static int run_dynamic(const Plan& p, const fj_case_buffers* B, int i_first, int i_last, int flags, cudaStream_t s) {
     const int64_t hs = (int64_t)p.cfg.n_nodes * 16;
     const bool mixed = p.cfg.precision == FJ_PREC_MIXED;
     bool refactor_all = false;
     int i = i_first;
     for (int attempt = 0; attempt < 2; ++attempt) {
         for (int k = i; k < i_last; ++k) {
-            const bool refactor = mixed && (refactor_all || k == i);
+            const bool first = (k == i) && !(attempt == 0 && (flags & FJ_REUSE_FACTORS));
+            const bool refactor = mixed && (refactor_all || first);
             FJ_TRY(run_step(p, B, k, B->d_hg_t + (int64_t)k * hs, B->d_hg_dot_t + (int64_t)k * hs,
                             B->d_hg_t + (int64_t)(k - 1) * hs, refactor, s));
         }
@@ -1020,19 +1027,19 @@ int fj_solve_static(const fj_case_config* cfg, const fj_case_buffers* bufs, int 
 }
 
 int fj_solve_prescribed_dynamic(const fj_case_config* cfg, const fj_case_buffers* bufs, int i_first, int i_last,
-                                void* d_ws, size_t ws_bytes, fj_stream_t stream) {
+                                int flags, void* d_ws, size_t ws_bytes, fj_stream_t stream) {
     Plan p;
     FJ_TRY(make_plan(cfg, d_ws, ws_bytes, p));
     FJ_TRY(check_buffers(bufs, true));
     if (i_first < 1 || i_last > cfg->n_tstep || i_first > i_last)
         return fail(FJ_ERR_SHAPE, "step range [%d, %d) not within [1, %d)", i_first, i_last, cfg->n_tstep);
     if (i_first == i_last) return FJ_OK;
-    return run_dynamic(p, bufs, i_first, i_last, (cudaStream_t)stream);
+    return run_dynamic(p, bufs, i_first, i_last, flags, (cudaStream_t)stream);
 }
 
-int fj_case_step(const fj_case_config* cfg, const fj_case_buffers* bufs, int i_ts, void* d_ws, size_t ws_bytes,
-                 fj_stream_t stream) {
-    return fj_solve_prescribed_dynamic(cfg, bufs, i_ts, i_ts + 1, d_ws, ws_bytes, stream);
+int fj_case_step(const fj_case_config* cfg, const fj_case_buffers* bufs, int i_ts, int flags, void* d_ws,
+                 size_t ws_bytes, fj_stream_t stream) {
+    return fj_solve_prescribed_dynamic(cfg, bufs, i_ts, i_ts + 1, flags, d_ws, ws_bytes, stream);
 }
 
 int fj_biot_savart(const double* d_x, const double* d_y, int64_t n_pairs, int kernel, double r_cut, double* d_out,
@@ -1125,6 +1132,8 @@ int fj_vind(const double* d_targets, int64_t n_targets, const double* const* d_z
     j.n_elem = ne;
     j.n_split = sp;
     j.part = part;
+    j.n_links = 0;
+    for (int i = 0; i < n_lattices; ++i) j.n_links += (mirror ? 2 : 1) * lattice_links(rows[i], cols[i]);
     FJ_TRY(vind_launch(j, precision, kernel, r_cut, s));
     return reduce_partials(part, sp, n_targets, d_v_out, 0, 1.0, s);
 }
@@ -1171,7 +1180,7 @@ int fj_aic_assemble(const double* const* d_zetas_b, const int* m, const int* n, 
         one.n[0] = n[s];
         Layout L1 = make_layout(one);
         geom_panels_kernel<<<nblk(L1.po[1]), 256, 0, st>>>(L1, d_zetas_b[s], nullptr, c + L.po[s] * 3,
-                                                           nc + L.po[s] * 3, nullptr);
+                                                           nc + L.po[s] * 3, nullptr); note_launch();
     }
     FJ_LAUNCH_CHECK("aic geometry");
     AicArgs aa;

@@ -11,9 +11,12 @@
 //     the epsilon regulariser, which FP32 cannot resolve (EPSILON*|r0|^4 ~ 1e-12 is far
 //     below FP32 noise in |r1 x r2|^2),
 //   - FP32 sums over one staged chunk of filaments, added into FP64 accumulators.
-#include <cstdio>
-#include <cstdarg>
 #include <algorithm>
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <mutex>
+#include <vector>
 
 #include "fj_bs.cuh"
 #include "fj_vind.cuh"
@@ -38,6 +41,70 @@ int fail(int code, const char* fmt, ...) {
 }
 
 const char* last_error() { return g_err; }
+
+static std::atomic<int64_t> g_launches{0};
+void note_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+int64_t launch_count() { return g_launches.load(); }
+
+struct ProfState {
+    std::mutex mu;
+    bool on = false;
+    std::vector<cudaEvent_t> ev;  // 2 per slot
+    std::vector<double> pairs;
+    int used = 0;
+    int64_t launches0 = 0;
+};
+static ProfState g_prof;
+constexpr int kMaxProfSlots = 1 << 16;
+
+int prof_start(cudaStream_t s) {
+    std::lock_guard<std::mutex> g(g_prof.mu);
+    if (!g_prof.on || g_prof.used >= kMaxProfSlots) return -1;
+    const int slot = g_prof.used;
+    while ((int)g_prof.ev.size() < 2 * (slot + 1)) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return -1;
+        g_prof.ev.push_back(e);
+    }
+    if ((int)g_prof.pairs.size() <= slot) g_prof.pairs.resize(slot + 1);
+    cudaEventRecord(g_prof.ev[2 * slot], s);
+    g_prof.used = slot + 1;
+    return slot;
+}
+
+void prof_stop(int slot, cudaStream_t s, double pairs) {
+    if (slot < 0) return;
+    std::lock_guard<std::mutex> g(g_prof.mu);
+    cudaEventRecord(g_prof.ev[2 * slot + 1], s);
+    g_prof.pairs[slot] = pairs;
+}
+
+int prof_begin() {
+    std::lock_guard<std::mutex> g(g_prof.mu);
+    g_prof.on = true;
+    g_prof.used = 0;
+    g_prof.launches0 = launch_count();
+    return FJ_OK;
+}
+
+int prof_end(fj_profile* out) {
+    std::lock_guard<std::mutex> g(g_prof.mu);
+    g_prof.on = false;
+    fj_profile r;
+    memset(&r, 0, sizeof(r));
+    r.launches = launch_count() - g_prof.launches0;
+    for (int i = 0; i < g_prof.used; ++i) {
+        FJ_CUDA(cudaEventSynchronize(g_prof.ev[2 * i + 1]));
+        float ms = 0.f;
+        FJ_CUDA(cudaEventElapsedTime(&ms, g_prof.ev[2 * i], g_prof.ev[2 * i + 1]));
+        r.vind_ms += ms;
+        r.vind_ms_max = std::max(r.vind_ms_max, (double)ms);
+        r.vind_pairs += g_prof.pairs[i];
+    }
+    r.vind_launches = g_prof.used;
+    if (out) *out = r;
+    return FJ_OK;
+}
 
 // ------------------------------------------------------------------------------------
 // Stream packing
@@ -164,7 +231,7 @@ __global__ void pack32_kernel(PackArgs a, Elem32* __restrict__ out) {
 int pack_stream64(const PackArgs& a, Elem64* out, cudaStream_t s) {
     int64_t n = a.offset[a.n_lat];
     if (n == 0) return FJ_OK;
-    pack64_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, out);
+    pack64_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, out); note_launch();
     FJ_LAUNCH_CHECK("pack64_kernel");
     return FJ_OK;
 }
@@ -172,7 +239,7 @@ int pack_stream64(const PackArgs& a, Elem64* out, cudaStream_t s) {
 int pack_stream32(const PackArgs& a, Elem32* out, cudaStream_t s) {
     int64_t n = a.offset[a.n_lat];
     if (n == 0) return FJ_OK;
-    pack32_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, out);
+    pack32_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, out); note_launch();
     FJ_LAUNCH_CHECK("pack32_kernel");
     return FJ_OK;
 }
@@ -377,7 +444,7 @@ int reduce_partials(const double* part, int n_split, int64_t n_targets, double* 
     const int64_t n3 = n_targets * 3;
     if (n3 == 0) return FJ_OK;
     reduce_partials_kernel<<<(unsigned)((n3 + 255) / 256), 256, 0, s>>>(part, n_split, n3, out,
-                                                                         accumulate, scale);
+                                                                         accumulate, scale); note_launch();
     FJ_LAUNCH_CHECK("reduce_partials_kernel");
     return FJ_OK;
 }
@@ -403,18 +470,19 @@ int vind_launch(const VindJob& job, int precision, int kernel, double r_cut, cud
     const int64_t gx = (job.n_targets + (int64_t)kBlock * T - 1) / ((int64_t)kBlock * T);
     if (gx > 0x7fffffff || job.n_split > 65535) return fail(FJ_ERR_SHAPE, "vind: grid too large");
     dim3 grid((unsigned)gx, (unsigned)job.n_split);
+    const int prof = prof_start(s);
     if (precision == FJ_PREC_FP64) {
         const Elem64* st = (const Elem64*)job.stream;
         const double rc2 = r_cut * r_cut;
         switch (kernel) {
             case FJ_KERNEL_EPSILON:
-                vind64_kernel<FJ_KERNEL_EPSILON, kT64><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part, rc2);
+                vind64_kernel<FJ_KERNEL_EPSILON, kT64><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part, rc2); note_launch();
                 break;
             case FJ_KERNEL_CUTOFF:
-                vind64_kernel<FJ_KERNEL_CUTOFF, kT64><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part, rc2);
+                vind64_kernel<FJ_KERNEL_CUTOFF, kT64><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part, rc2); note_launch();
                 break;
             case FJ_KERNEL_PLAIN:
-                vind64_kernel<FJ_KERNEL_PLAIN, kT64><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part, rc2);
+                vind64_kernel<FJ_KERNEL_PLAIN, kT64><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part, rc2); note_launch();
                 break;
             default:
                 return fail(FJ_ERR_UNSUPPORTED, "vind: unknown kernel %d", kernel);
@@ -423,15 +491,16 @@ int vind_launch(const VindJob& job, int precision, int kernel, double r_cut, cud
         const Elem32* st = (const Elem32*)job.stream;
         switch (kernel) {
             case FJ_KERNEL_EPSILON:
-                vind32_kernel<FJ_KERNEL_EPSILON, kT32><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part);
+                vind32_kernel<FJ_KERNEL_EPSILON, kT32><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part); note_launch();
                 break;
             case FJ_KERNEL_CUTOFF:
-                vind32_kernel<FJ_KERNEL_CUTOFF, kT32><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part);
+                vind32_kernel<FJ_KERNEL_CUTOFF, kT32><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part); note_launch();
                 break;
             default:
                 return fail(FJ_ERR_UNSUPPORTED, "vind: kernel %d has no FP32 variant (use FJ_PREC_FP64)", kernel);
         }
     }
+    prof_stop(prof, s, (double)job.n_targets * (double)job.n_links);
     FJ_LAUNCH_CHECK("vind kernel");
     return FJ_OK;
 }
@@ -474,9 +543,56 @@ int biot_savart_pairs(const double* x, const double* y, int64_t n, int kernel, d
     if (n < 0) return fail(FJ_ERR_SHAPE, "fj_biot_savart: n_pairs < 0");
     if (kernel < 0 || kernel > 2) return fail(FJ_ERR_UNSUPPORTED, "fj_biot_savart: kernel %d", kernel);
     if (n == 0) return FJ_OK;
-    bs_pairs_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(x, y, n, kernel, r_cut * r_cut, out);
+    bs_pairs_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(x, y, n, kernel, r_cut * r_cut, out); note_launch();
     FJ_LAUNCH_CHECK("bs_pairs_kernel");
     return FJ_OK;
 }
 
 }  // namespace fj
+
+namespace fj {
+// Eight independent FMA chains per thread, all in registers.
+__global__ void __launch_bounds__(256) fma_peak_kernel(float* out, int iters, float a, float b) {
+    float x[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = threadIdx.x * 1e-3f + k;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) x[k] = fmaf(x[k], a, b);
+    }
+    float sum = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) sum += x[k];
+    if (sum == 1234.5f) out[0] = sum;  // keeps the chains live; practically never true
+}
+
+int peak_fp32(double* tflops, cudaStream_t s) {
+    int dev = 0, sms = 0;
+    FJ_CUDA(cudaGetDevice(&dev));
+    FJ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+    cudaEvent_t e0, e1;
+    FJ_CUDA(cudaEventCreate(&e0));
+    FJ_CUDA(cudaEventCreate(&e1));
+    float ms = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {
+        cudaEventRecord(e0, s);
+        fma_peak_kernel<<<blocks, threads, 0, s>>>(nullptr, iters, 0.999999f, 1e-7f); note_launch();
+        cudaEventRecord(e1, s);
+    }
+    FJ_LAUNCH_CHECK("fma_peak_kernel");
+    FJ_CUDA(cudaEventSynchronize(e1));
+    FJ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *tflops = 2.0 * 8.0 * iters * (double)blocks * threads / (ms * 1e-3) / 1e12;
+    return FJ_OK;
+}
+}  // namespace fj
+
+extern "C" {
+int fj_peak_fp32(double* tflops, fj_stream_t stream) { return fj::peak_fp32(tflops, (cudaStream_t)stream); }
+int fj_profile_begin(void) { return fj::prof_begin(); }
+int fj_profile_end(fj_profile* out) { return fj::prof_end(out); }
+int64_t fj_launch_count(void) { return fj::launch_count(); }
+}

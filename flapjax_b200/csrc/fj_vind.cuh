@@ -77,7 +77,13 @@ struct VindJob {
     int64_t n_elem;
     int n_split;
     double* part;           // (n_split, n_targets, 3)
+    int64_t n_links;        // filaments in the stream (for pair counting)
 };
+
+// filaments of an (rows, cols) lattice: rows(cols+1) chordwise + (rows+1)cols spanwise
+inline int64_t lattice_links(int rows, int cols) {
+    return (int64_t)rows * (cols + 1) + (int64_t)(rows + 1) * cols;
+}
 
 int vind_launch(const VindJob& job, int precision, int kernel, double r_cut, cudaStream_t s);
 int reduce_partials(const double* part, int n_split, int64_t n_targets, double* out,

@@ -135,20 +135,25 @@ class DeviceCase:
             srd = self.torch.as_tensor(hg_dot_t, dtype=self.torch.float64)
             self.hg_dot_t[: srd.shape[0]].copy_(srd, non_blocking=non_blocking)
 
-    def load_slot(self, slot: int, values: dict, t: float):
+    def load_slot(self, slot: int, values: dict, t: float, force_total=None):
         """Write one solution slot from host arrays (per-field, surfaces concatenated)."""
         for name, arr in values.items():
             self.arrays[name][slot].copy_(self.torch.as_tensor(np.ascontiguousarray(arr).ravel()))
         self.t[slot] = float(t)
+        if force_total is not None:
+            self.force_total[slot].copy_(self.torch.as_tensor(np.asarray(force_total, dtype=np.float64)))
 
     # -- compute ----------------------------------------------------------------------
     def solve_static(self, horseshoe: bool, t0: float):
         _lib.call("fj_solve_static", C.byref(self.cfg), C.byref(self._bufs), int(horseshoe), float(t0),
                   self.ws.data_ptr(), self.ws.numel(), self._stream())
 
-    def solve_dynamic(self, i_first: int, i_last: int):
+    def solve_dynamic(self, i_first: int, i_last: int, reuse_factors: bool = False):
+        """Steps i_first..i_last-1.  ``reuse_factors``: keep the mixed path's cached
+        factors from the previous call on this case."""
+        flags = _lib.FJ_REUSE_FACTORS if reuse_factors else 0
         _lib.call("fj_solve_prescribed_dynamic", C.byref(self.cfg), C.byref(self._bufs), int(i_first), int(i_last),
-                  self.ws.data_ptr(), self.ws.numel(), self._stream())
+                  flags, self.ws.data_ptr(), self.ws.numel(), self._stream())
 
     # -- outputs ----------------------------------------------------------------------
     def host_arrays(self, slots=None):

@@ -289,7 +289,11 @@ class UVLM:
                 "gamma_b": self._flat(init_case.gamma_b), "gamma_b_dot": self._flat(init_case.gamma_b_dot),
                 "gamma_w": self._flat(init_case.gamma_w), "f_steady": self._flat(init_case.f_steady),
                 "f_unsteady": self._flat(init_case.f_unsteady), "alpha": self._flat(init_case.alpha)}
-        dc.load_slot(0, vals, float(np.asarray(init_case.t)))
+        ft = init_case.force_total
+        if ft is None:  # a snapshot built elsewhere: recompute the sum of vertex forces
+            ft = sum(np.asarray(fs).reshape(-1, 3).sum(0) + np.asarray(fu).reshape(-1, 3).sum(0)
+                     for fs, fu in zip(init_case.f_steady, init_case.f_unsteady))
+        dc.load_slot(0, vals, float(np.asarray(init_case.t)), ft)
 
     def solve_prescribed_dynamic(self, init_case: AeroCase, hg_t, hg_dot_t, cs_ang_t=None, cs_vel_t=None) -> AeroCase:
         """aero/uvlm.py:1335-1406: a batched AeroCase of ``hg_t.shape[0]`` slots."""

@@ -127,6 +127,21 @@ typedef struct fj_case_buffers {
 FJ_API const char* fj_last_error_string(void);
 FJ_API int fj_version(void); /* major*10000 + minor*100 + patch */
 
+/* Instrumentation (no counterpart in the reference, which has no timers beyond
+ * utils/utils.py:130-175).  fj_launch_count: kernels launched by this library so far.
+ * fj_profile_begin/_end bracket a region in which every Biot-Savart sum kernel is timed
+ * with CUDA events on its own stream; _end waits for those events. */
+typedef struct fj_profile {
+    int64_t launches;      /* kernels launched in the region */
+    int64_t vind_launches; /* Biot-Savart sum kernels timed */
+    double vind_ms;        /* their summed device time */
+    double vind_ms_max;    /* longest single launch */
+    double vind_pairs;     /* (target, filament) pairs they evaluated */
+} fj_profile;
+FJ_API int64_t fj_launch_count(void);
+FJ_API int fj_profile_begin(void);
+FJ_API int fj_profile_end(fj_profile* out);
+
 /* ---------------------------------------------------------------------------------
  * Case-level entry points (replace UVLM.solve_static / solve_prescribed_dynamic /
  * case_solve, aero/uvlm.py:1119-1406).  The workspace carries cached state between
@@ -142,16 +157,25 @@ FJ_API int fj_solve_static(const fj_case_config* cfg, const fj_case_buffers* buf
 /* UVLM.solve_prescribed_dynamic (aero/uvlm.py:1335-1406): time steps
  * i_first..i_last-1 (1 <= i_first), each a case_solve (aero/uvlm.py:1119-1215) reading
  * slot i-1 and writing slot i.  Slot i_first-1 must hold a solution (e.g. from
- * fj_solve_static).  Reads one status word back after the last step. */
+ * fj_solve_static).
+ * FJ_PREC_MIXED: the FP32 factors are computed at step i_first, unless flags has
+ * FJ_REUSE_FACTORS and an earlier call on this workspace left factors there; the
+ * refinement residuals are read back after the last step (one synchronisation) and
+ * the steps from the first one above 1e-12 are re-run with fresh factors. */
+#define FJ_REUSE_FACTORS 1
 FJ_API int fj_solve_prescribed_dynamic(const fj_case_config* cfg, const fj_case_buffers* bufs,
-                                int i_first, int i_last, void* d_ws, size_t ws_bytes,
-                                fj_stream_t stream);
+                                int i_first, int i_last, int flags, void* d_ws,
+                                size_t ws_bytes, fj_stream_t stream);
 
 /* One case_solve (aero/uvlm.py:1119-1215) at slot i_ts >= 1 with the node frames of
  * slots i_ts (hg_n, hg_dot_n) and i_ts-1 (hg_nm1) taken from the hg arrays.  This is
  * the call the coupled FSI loop makes (structure/beam.py:2656-2667). */
 FJ_API int fj_case_step(const fj_case_config* cfg, const fj_case_buffers* bufs, int i_ts,
-                 void* d_ws, size_t ws_bytes, fj_stream_t stream);
+                 int flags, void* d_ws, size_t ws_bytes, fj_stream_t stream);
+
+/* Measured FP32 FMA throughput of the current device (TFLOP/s, an FMA counted as two),
+ * from a register-resident FMA-chain kernel timed with CUDA events.  Synchronises. */
+FJ_API int fj_peak_fp32(double* tflops, fj_stream_t stream);
 
 /* ---------------------------------------------------------------------------------
  * Function-level entry points (the names uvlm.py imports, aero/uvlm.py:15, :32-43).
