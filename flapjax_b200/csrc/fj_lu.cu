@@ -25,7 +25,8 @@ template <typename T, int NB>
 __global__ void __launch_bounds__(1024) lu_panel_kernel(T* __restrict__ a, int n, int k,
                                                         int32_t* __restrict__ piv, int* __restrict__ info) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* P = reinterpret_cast<T*>(smraw);  // (n-k) x NB, row-major
+    T* P = reinterpret_cast<T*>(smraw);  // (n-k) x LDP, row-major; odd stride avoids bank conflicts
+    constexpr int LDP = NB + 1;
     __shared__ T s_val[32];
     __shared__ int s_idx[32];
     __shared__ int s_piv;
@@ -35,14 +36,14 @@ __global__ void __launch_bounds__(1024) lu_panel_kernel(T* __restrict__ a, int n
     const int nwarps = (blockDim.x + 31) >> 5;
     for (int idx = threadIdx.x; idx < rows * NB; idx += blockDim.x) {
         const int r = idx / NB, c = idx % NB;
-        P[idx] = c < nb ? a[(int64_t)(k + r) * n + k + c] : T(0);
+        P[r * LDP + c] = c < nb ? a[(int64_t)(k + r) * n + k + c] : T(0);
     }
     __syncthreads();
     for (int j = 0; j < nb; ++j) {
         T best = T(-1);
         int bi = INT_MAX;
         for (int r = j + threadIdx.x; r < rows; r += blockDim.x) {
-            const T v = absval(P[r * NB + j]);
+            const T v = absval(P[r * LDP + j]);
             if (v > best) {
                 best = v;
                 bi = r;
@@ -83,26 +84,26 @@ __global__ void __launch_bounds__(1024) lu_panel_kernel(T* __restrict__ a, int n
         __syncthreads();
         const int p = s_piv;
         if (p != j && threadIdx.x < NB) {
-            const T t = P[j * NB + threadIdx.x];
-            P[j * NB + threadIdx.x] = P[p * NB + threadIdx.x];
-            P[p * NB + threadIdx.x] = t;
+            const T t = P[j * LDP + threadIdx.x];
+            P[j * LDP + threadIdx.x] = P[p * LDP + threadIdx.x];
+            P[p * LDP + threadIdx.x] = t;
         }
         __syncthreads();
-        const T pv = P[j * NB + j];
+        const T pv = P[j * LDP + j];
         if (pv == T(0)) {
             if (threadIdx.x == 0 && *info == 0) *info = k + j + 1;
         } else {
             for (int r = j + 1 + threadIdx.x; r < rows; r += blockDim.x) {
-                const T l = P[r * NB + j] / pv;
-                P[r * NB + j] = l;
-                for (int c = j + 1; c < nb; ++c) P[r * NB + c] -= l * P[j * NB + c];
+                const T l = P[r * LDP + j] / pv;
+                P[r * LDP + j] = l;
+                for (int c = j + 1; c < nb; ++c) P[r * LDP + c] -= l * P[j * LDP + c];
             }
         }
         __syncthreads();
     }
     for (int idx = threadIdx.x; idx < rows * NB; idx += blockDim.x) {
         const int r = idx / NB, c = idx % NB;
-        if (c < nb) a[(int64_t)(k + r) * n + k + c] = P[idx];
+        if (c < nb) a[(int64_t)(k + r) * n + k + c] = P[r * LDP + c];
     }
 }
 
@@ -173,13 +174,13 @@ __global__ void __launch_bounds__(256) lu_update_kernel(T* __restrict__ a, int n
 template <typename T, int NB>
 static int lu_factor_impl(T* a, int n, int32_t* piv, int* d_info, cudaStream_t s) {
     if (n <= 0) return fail(FJ_ERR_SHAPE, "lu_factor: n=%d", n);
-    const size_t smem = (size_t)n * NB * sizeof(T);
+    const size_t smem = (size_t)n * (NB + 1) * sizeof(T);
     if (smem > 220 * 1024) return fail(FJ_ERR_UNSUPPORTED, "lu_factor: n=%d too large for the shared-memory panel", n);
     FJ_CUDA(cudaFuncSetAttribute(lu_panel_kernel<T, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     FJ_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int), s));
     for (int k = 0; k < n; k += NB) {
         const int nb = min(NB, n - k);
-        lu_panel_kernel<T, NB><<<1, 1024, (size_t)(n - k) * NB * sizeof(T), s>>>(a, n, k, piv, d_info); note_launch();
+        lu_panel_kernel<T, NB><<<1, 1024, (size_t)(n - k) * (NB + 1) * sizeof(T), s>>>(a, n, k, piv, d_info); note_launch();
         if (n > nb) {
             lu_swap_trsm_kernel<T, NB><<<(n + 255) / 256, 256, 0, s>>>(a, n, k, piv); note_launch();
         }
@@ -201,71 +202,102 @@ int lu_factor32(float* a, int n, int32_t* piv, int* d_info, cudaStream_t s) {
 }
 
 // ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) lu_solve64_kernel(const double* __restrict__ lu, int n,
-                                                          const int32_t* __restrict__ piv,
-                                                          double* __restrict__ b) {
-    extern __shared__ double x[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = b[i];
+// getrs: x = P b, then blocked substitution.  Per block of kTrsvBlk rows one CTA solves
+// the diagonal block in shared memory and a grid of warps (one per remaining row) applies
+// the block's contribution to the rows still to be solved.
+constexpr int kTrsvBlk = 128;
+
+// x[i] = b[perm[i]], perm from the getrf row swaps applied in order to the identity.
+__global__ void __launch_bounds__(1024) permute_kernel(const int32_t* __restrict__ piv, int n,
+                                                       const double* __restrict__ b, double* __restrict__ x) {
+    extern __shared__ int perm[];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = i;
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int i = 0; i < n; ++i) {
             const int p = piv[i];
             if (p != i) {
-                const double t = x[i];
-                x[i] = x[p];
-                x[p] = t;
+                const int t = perm[i];
+                perm[i] = perm[p];
+                perm[p] = t;
             }
         }
     }
     __syncthreads();
-    for (int kb = 0; kb < n; kb += 32) {  // forward, unit lower
-        const int bw = min(32, n - kb);
-        if (warp == 0) {
-            for (int jj = 0; jj < bw; ++jj) {
-                __syncwarp();
-                const double xj = x[kb + jj];
-                if (lane > jj && lane < bw) x[kb + lane] -= lu[(int64_t)(kb + lane) * n + kb + jj] * xj;
-            }
-        }
-        __syncthreads();
-        for (int i = kb + bw + threadIdx.x; i < n; i += blockDim.x) {
-            double sacc = x[i];
-            const double* row = lu + (int64_t)i * n + kb;
-            for (int jj = 0; jj < bw; ++jj) sacc -= row[jj] * x[kb + jj];
-            x[i] = sacc;
-        }
-        __syncthreads();
-    }
-    for (int kb = ((n - 1) / 32) * 32; kb >= 0; kb -= 32) {  // backward, upper
-        const int be = min(kb + 32, n);
-        if (warp == 0) {
-            for (int j = be - 1; j >= kb; --j) {
-                __syncwarp();
-                if (lane == j - kb) x[j] = x[j] / lu[(int64_t)j * n + j];
-                __syncwarp();
-                const double xj = x[j];
-                if (lane < j - kb) x[kb + lane] -= lu[(int64_t)(kb + lane) * n + j] * xj;
-            }
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < kb; i += blockDim.x) {
-            double sacc = x[i];
-            const double* row = lu + (int64_t)i * n;
-            for (int j = kb; j < be; ++j) sacc -= row[j] * x[j];
-            x[i] = sacc;
-        }
-        __syncthreads();
-    }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) b[i] = x[i];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = b[perm[i]];
 }
 
-int lu_solve64(const double* lu, int n, const int32_t* piv, double* b, cudaStream_t s) {
-    const size_t smem = (size_t)n * sizeof(double);
-    if (smem > 220 * 1024) return fail(FJ_ERR_UNSUPPORTED, "lu_solve: n=%d too large", n);
-    FJ_CUDA(cudaFuncSetAttribute(lu_solve64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    lu_solve64_kernel<<<1, 1024, smem, s>>>(lu, n, piv, b); note_launch();
-    FJ_LAUNCH_CHECK("lu_solve64_kernel");
+// Solve the diagonal block [i0, i0+bw) of L (unit lower, upper = false) or U (upper = true)
+// in place on x, with the block held in shared memory.
+__global__ void __launch_bounds__(kTrsvBlk) trsv_diag_kernel(const double* __restrict__ lu, int n, int i0, int bw,
+                                                             bool upper, double* __restrict__ x) {
+    extern __shared__ double blk[];  // bw x (bw + 1)
+    __shared__ double xs[kTrsvBlk];
+    const int ld = bw + 1;
+    for (int idx = threadIdx.x; idx < bw * bw; idx += blockDim.x) {
+        const int r = idx / bw, c = idx % bw;
+        blk[r * ld + c] = lu[(int64_t)(i0 + r) * n + i0 + c];
+    }
+    const int r = threadIdx.x;
+    if (r < bw) xs[r] = x[i0 + r];
+    __syncthreads();
+    if (!upper) {
+        for (int j = 0; j < bw; ++j) {
+            const double xj = xs[j];
+            if (r > j && r < bw) xs[r] -= blk[r * ld + j] * xj;
+            __syncthreads();
+        }
+    } else {
+        for (int j = bw - 1; j >= 0; --j) {
+            if (r == j) xs[j] = xs[j] / blk[j * ld + j];
+            __syncthreads();
+            const double xj = xs[j];
+            if (r < j) xs[r] -= blk[r * ld + j] * xj;
+            __syncthreads();
+        }
+    }
+    if (r < bw) x[i0 + r] = xs[r];
+}
+
+// x[i] -= sum_{j in [j0, j0+bw)} lu[i][j] x[j] for i in [r0, r1): one warp per row.
+__global__ void trsv_update_kernel(const double* __restrict__ lu, int n, int j0, int bw, int r0, int r1,
+                                   double* __restrict__ x) {
+    const int row = r0 + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= r1) return;
+    const double* a = lu + (int64_t)row * n + j0;
+    double acc = 0.0;
+    for (int j = lane; j < bw; j += 32) acc += a[j] * x[j0 + j];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if (lane == 0) x[row] -= acc;
+}
+
+int lu_solve64(const double* lu, int n, const int32_t* piv, double* b, double* work, cudaStream_t s) {
+    if (n <= 0) return fail(FJ_ERR_SHAPE, "lu_solve: n=%d", n);
+    if ((size_t)n * sizeof(int) > 220 * 1024) return fail(FJ_ERR_UNSUPPORTED, "lu_solve: n=%d too large", n);
+    const size_t dsm = (size_t)kTrsvBlk * (kTrsvBlk + 1) * sizeof(double);
+    FJ_CUDA(cudaFuncSetAttribute(permute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(n * sizeof(int))));
+    FJ_CUDA(cudaFuncSetAttribute(trsv_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
+    permute_kernel<<<1, 1024, n * sizeof(int), s>>>(piv, n, b, work); note_launch();
+    const int wpb = 8;
+    for (int i0 = 0; i0 < n; i0 += kTrsvBlk) {  // forward, unit lower
+        const int bw = min(kTrsvBlk, n - i0);
+        trsv_diag_kernel<<<1, kTrsvBlk, (size_t)bw * (bw + 1) * sizeof(double), s>>>(lu, n, i0, bw, false, work); note_launch();
+        const int r0 = i0 + bw;
+        if (r0 < n) {
+            trsv_update_kernel<<<(n - r0 + wpb - 1) / wpb, wpb * 32, 0, s>>>(lu, n, i0, bw, r0, n, work); note_launch();
+        }
+    }
+    for (int i0 = ((n - 1) / kTrsvBlk) * kTrsvBlk; i0 >= 0; i0 -= kTrsvBlk) {  // backward, upper
+        const int bw = min(kTrsvBlk, n - i0);
+        trsv_diag_kernel<<<1, kTrsvBlk, (size_t)bw * (bw + 1) * sizeof(double), s>>>(lu, n, i0, bw, true, work); note_launch();
+        if (i0 > 0) {
+            trsv_update_kernel<<<(i0 + wpb - 1) / wpb, wpb * 32, 0, s>>>(lu, n, i0, bw, 0, i0, work); note_launch();
+        }
+    }
+    FJ_CUDA(cudaMemcpyAsync(b, work, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    FJ_LAUNCH_CHECK("lu_solve64");
     return FJ_OK;
 }
 

@@ -11,8 +11,8 @@ namespace fj {
 int lu_factor64(double* a, int n, int32_t* piv, int* d_info, cudaStream_t s);
 int lu_factor32(float* a, int n, int32_t* piv, int* d_info, cudaStream_t s);
 
-// getrs: b <- A^-1 b using the factors (single right-hand side, in place).
-int lu_solve64(const double* lu, int n, const int32_t* piv, double* b, cudaStream_t s);
+// getrs: b <- A^-1 b using the factors (single right-hand side, in place); work: n doubles.
+int lu_solve64(const double* lu, int n, const int32_t* piv, double* b, double* work, cudaStream_t s);
 
 // X <- A^-1 (row-major n x n) from FP32 factors.
 int lu_inverse32(const float* lu, int n, const int32_t* piv, float* x, cudaStream_t s);

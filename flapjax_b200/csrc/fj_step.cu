@@ -632,7 +632,7 @@ static int make_plan(const fj_case_config* cfg, void* ws, size_t ws_bytes, Plan&
     const int64_t sets[3] = {L.wto[ns], L.fo[ns], L.po[ns]};
     for (int64_t nt : sets) {
         if (nt == 0) continue;
-        part = std::max<int64_t>(part, (int64_t)choose_split(nt, stream, cfg->precision) * nt * 3);
+        part = std::max<int64_t>(part, (int64_t)split_bound(nt, stream, cfg->precision) * nt * 3);
     }
     p.part_elems = part;
 
@@ -808,7 +808,7 @@ static int run_static(const Plan& p, const fj_case_buffers* B, const double* hg,
     FJ_TRY(aic_launch(aa, nullptr, s));
     rhs_kernel<<<nblk(p.nb), 256, 0, s>>>(p.nb, cc, nullptr, nc, nullptr, c.flow, nullptr, t0, p.rhs); note_launch();
     FJ_TRY(lu_factor64(p.a64, p.nb, p.piv, p.flags, s));
-    FJ_TRY(lu_solve64(p.a64, p.nb, p.piv, p.rhs, s));
+    FJ_TRY(lu_solve64(p.a64, p.nb, p.piv, p.rhs, p.r, s));
     FJ_CUDA(cudaMemcpyAsync(gb, p.rhs, p.nb * sizeof(double), cudaMemcpyDeviceToDevice, s));
     // wake circulation of the solve, and of the stored slot (broadcast over m_star rows)
     double* gw_solve = gw;
@@ -917,7 +917,7 @@ static int run_step(const Plan& p, const fj_case_buffers* B, int i, const double
     // 5. solve
     if (!mixed) {
         FJ_TRY(lu_factor64(p.a64, p.nb, p.piv, p.flags, s));
-        FJ_TRY(lu_solve64(p.a64, p.nb, p.piv, p.rhs, s));
+        FJ_TRY(lu_solve64(p.a64, p.nb, p.piv, p.rhs, p.r, s));
         FJ_CUDA(cudaMemcpyAsync(gb_n, p.rhs, p.nb * sizeof(double), cudaMemcpyDeviceToDevice, s));
     } else {
         if (refactor) {
@@ -1057,7 +1057,7 @@ static int vind_plan(int64_t n_targets, const int* rows, const int* cols, int n_
         if (rows[i] < 0 || cols[i] < 0) return fail(FJ_ERR_SHAPE, "vind: lattice %d has rows=%d cols=%d", i, rows[i], cols[i]);
         n_elem += (mirror ? 2 : 1) * stream_len(rows[i], cols[i]);
     }
-    n_split = choose_split(std::max<int64_t>(n_targets, 1), n_elem, precision);
+    n_split = split_bound(std::max<int64_t>(n_targets, 1), n_elem, precision);
     Arena a(nullptr, 0);
     a.carve<Elem64>(n_elem);
     a.carve<double>((int64_t)n_split * std::max<int64_t>(n_targets, 1) * 3);
@@ -1130,7 +1130,7 @@ int fj_vind(const double* d_targets, int64_t n_targets, const double* const* d_z
     j.n_targets = n_targets;
     j.stream = st;
     j.n_elem = ne;
-    j.n_split = sp;
+    j.n_split = std::min(sp, choose_split(n_targets, ne, precision));
     j.part = part;
     j.n_links = 0;
     for (int i = 0; i < n_lattices; ++i) j.n_links += (mirror ? 2 : 1) * lattice_links(rows[i], cols[i]);
@@ -1213,8 +1213,8 @@ int fj_aic_assemble(const double* const* d_zetas_b, const int* m, const int* n, 
 }
 
 int fj_lu_workspace_size(int n, size_t* bytes) {
-    *bytes = 256;
-    (void)n;
+    if (bytes == nullptr || n < 0) return fail(FJ_ERR_SHAPE, "lu workspace: n=%d", n);
+    *bytes = 256 + (size_t)n * sizeof(double);  // info word, then n doubles of solve scratch
     return FJ_OK;
 }
 
@@ -1225,9 +1225,8 @@ int fj_lu_factor(double* d_a, int n, int32_t* d_piv, void* d_ws, size_t ws_bytes
 
 int fj_lu_solve(const double* d_lu, int n, const int32_t* d_piv, double* d_b, void* d_ws, size_t ws_bytes,
                 fj_stream_t stream) {
-    (void)d_ws;
-    (void)ws_bytes;
-    return lu_solve64(d_lu, n, d_piv, d_b, (cudaStream_t)stream);
+    if (ws_bytes < 256 + (size_t)n * sizeof(double)) return fail(FJ_ERR_NOMEM, "lu_solve workspace too small");
+    return lu_solve64(d_lu, n, d_piv, d_b, (double*)((char*)d_ws + 256), (cudaStream_t)stream);
 }
 
 int fj_solve_mixed_workspace_size(int n, size_t* bytes) {

@@ -218,8 +218,8 @@ __global__ void pack32_kernel(PackArgs a, Elem32* __restrict__ out) {
     r.r0x = (float)o.r0[0];
     r.r0y = (float)o.r0[1];
     r.r0z = (float)o.r0[2];
-    if (o.q < 0.0)
-        r.q = -1.0f;
+    if (o.q < 0.0)  // chain break: g = 0 and a q that keeps the link finite (eps) or
+        r.q = a.kernel == FJ_KERNEL_EPSILON ? 1.0f : 3.0e38f;  // never kept (cutoff)
     else if (a.kernel == FJ_KERNEL_EPSILON)
         r.q = (float)o.q;
     else  // cutoff: keep iff |r1 x r2|^2 > r_cut^2 |r0|^2  (aero/utils.py:637-648)
@@ -396,14 +396,16 @@ __global__ void __launch_bounds__(kBlock) vind32_kernel(const double* __restrict
             float accf[T][3];
 #pragma unroll
             for (int j = 0; j < T; ++j) accf[j][0] = accf[j][1] = accf[j][2] = 0.f;
+            // Chain breaks carry g = 0 and a q that keeps their (discarded) term finite,
+            // so every element is processed without a branch.
+#pragma unroll 4
             for (int i = 0; i < cnt; ++i) {
                 const float4 ca = sh[i * 3 + 0], cb = sh[i * 3 + 1], cc = sh[i * 3 + 2];
-                const bool live = pb.w >= 0.0f;  // link (prev -> cur) is not a chain break
 #pragma unroll
                 for (int j = 0; j < T; ++j) {
                     Vtx32 v;
                     vtx32(xh[j], xl[j], ca, cb, v);
-                    if (live) link32<KER>(prev[j], v, pa.w, pc.x, pc.y, pc.z, pb.w, accf[j]);
+                    link32<KER>(prev[j], v, pa.w, pc.x, pc.y, pc.z, pb.w, accf[j]);
                     prev[j] = v;
                 }
                 pa = ca;
@@ -452,20 +454,62 @@ int reduce_partials(const double* part, int n_split, int64_t n_targets, double* 
 constexpr int kT64 = 2;
 constexpr int kT32 = 2;
 
+// CTAs resident per SM for the sum kernels and the SM count, queried once.
+static int g_sms = 0, g_res64 = 0, g_res32 = 0;
+
+static void query_occupancy() {
+    if (g_sms > 0) return;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_res64, vind64_kernel<FJ_KERNEL_EPSILON, kT64>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_res32, vind32_kernel<FJ_KERNEL_CUTOFF, kT32>, kBlock, 0);
+    if (g_sms <= 0) g_sms = 148;
+    if (g_res64 <= 0) g_res64 = 1;
+    if (g_res32 <= 0) g_res32 = 1;
+}
+
+// Split the stream so that (target blocks) x (splits) fills whole waves: the smallest
+// split count with at least two waves' worth of CTAs whose last wave is >= 90 % full
+// (or the best efficiency found), bounded by >= 256 elements per split.
+// Upper bound on choose_split for any stream of at most n_elem_max elements (workspace
+// sizing): independent of the device queried.
+int split_bound(int64_t n_targets, int64_t n_elem_max, int precision) {
+    const int T = precision == FJ_PREC_FP64 ? kT64 : kT32;
+    const int64_t ctas = std::max<int64_t>(1, (n_targets + (int64_t)kBlock * T - 1) / ((int64_t)kBlock * T));
+    const int64_t cap = (4ll * 160 * 16 + ctas - 1) / ctas;  // 4 waves of 160 SMs x 16 CTAs
+    return (int)std::max<int64_t>(1, std::min<int64_t>({1024, cap, std::max<int64_t>(1, n_elem_max / 256)}));
+}
+
 int choose_split(int64_t n_targets, int64_t n_elem, int precision) {
+    query_occupancy();
     const int T = precision == FJ_PREC_FP64 ? kT64 : kT32;
     const int64_t ctas = (n_targets + (int64_t)kBlock * T - 1) / ((int64_t)kBlock * T);
-    const int64_t want = 148 * 8;  // CTAs to cover the SMs a few times over
-    int64_t sp = (want + ctas - 1) / std::max<int64_t>(ctas, 1);
-    const int64_t max_sp = std::max<int64_t>(1, n_elem / 256);
-    if (sp > max_sp) sp = max_sp;
-    if (sp < 1) sp = 1;
-    if (sp > 1024) sp = 1024;
-    return (int)sp;
+    int sms = 148, res = precision == FJ_PREC_FP64 ? 4 : 6;
+    if (g_sms > 0) {
+        sms = g_sms;
+        res = precision == FJ_PREC_FP64 ? g_res64 : g_res32;
+    }
+    const int64_t wave = (int64_t)sms * res;
+    const int64_t max_sp = split_bound(n_targets, n_elem, precision);
+    int64_t best = 1;
+    double best_eff = -1.0;
+    for (int64_t sp = 1; sp <= max_sp; ++sp) {
+        const int64_t total = ctas * sp;
+        const int64_t waves = (total + wave - 1) / wave;
+        const double eff = (double)total / (double)(waves * wave);
+        if (total >= 2 * wave && eff >= 0.9) return (int)sp;
+        if (eff > best_eff + 1e-9 || (total < 2 * wave && eff >= best_eff - 1e-9)) {
+            best_eff = eff;
+            best = sp;
+        }
+    }
+    return (int)best;
 }
 
 int vind_launch(const VindJob& job, int precision, int kernel, double r_cut, cudaStream_t s) {
     if (job.n_targets == 0) return FJ_OK;
+    query_occupancy();
     const int T = precision == FJ_PREC_FP64 ? kT64 : kT32;
     const int64_t gx = (job.n_targets + (int64_t)kBlock * T - 1) / ((int64_t)kBlock * T);
     if (gx > 0x7fffffff || job.n_split > 65535) return fail(FJ_ERR_SHAPE, "vind: grid too large");

@@ -89,5 +89,6 @@ int vind_launch(const VindJob& job, int precision, int kernel, double r_cut, cud
 int reduce_partials(const double* part, int n_split, int64_t n_targets, double* out,
                     int accumulate, double scale, cudaStream_t s);
 int choose_split(int64_t n_targets, int64_t n_elem, int precision);
+int split_bound(int64_t n_targets, int64_t n_elem_max, int precision);
 
 }  // namespace fj

@@ -143,6 +143,13 @@ class DeviceCase:
         if force_total is not None:
             self.force_total[slot].copy_(self.torch.as_tensor(np.asarray(force_total, dtype=np.float64)))
 
+    def copy_slot_from(self, other: "DeviceCase", slot: int):
+        """Device-to-device copy of one solution slot from a case of the same layout."""
+        for name, a in self.arrays.items():
+            a[slot].copy_(other.arrays[name][slot])
+        self.t[slot].copy_(other.t[slot])
+        self.force_total[slot].copy_(other.force_total[slot])
+
     # -- compute ----------------------------------------------------------------------
     def solve_static(self, horseshoe: bool, t0: float):
         _lib.call("fj_solve_static", C.byref(self.cfg), C.byref(self._bufs), int(horseshoe), float(t0),

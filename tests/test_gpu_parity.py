@@ -217,7 +217,9 @@ def test_lu_factor_solve_and_mixed(cuda):
         want = np.linalg.solve(a, b)
         ta = _t(a, cuda)
         piv = torch.empty(n, dtype=torch.int32, device=cuda)
-        ws = torch.empty(256, dtype=torch.uint8, device=cuda)
+        nb_ = C.c_size_t()
+        _lib.call("fj_lu_workspace_size", n, C.byref(nb_))
+        ws = torch.empty(nb_.value, dtype=torch.uint8, device=cuda)
         s = torch.cuda.current_stream(cuda).cuda_stream
         _lib.call("fj_lu_factor", ta.data_ptr(), n, piv.data_ptr(), ws.data_ptr(), ws.numel(), s)
         tb = _t(b, cuda)
