@@ -197,6 +197,20 @@ FJ_API int fj_vind(const double* d_targets, int64_t n_targets, const double* con
             const double* mirror_point, const double* mirror_normal, int kernel, double r_cut,
             int precision, double* d_v_out, void* d_ws, size_t ws_bytes, fj_stream_t stream);
 
+/* fj_vind without a caller workspace, for callers that cannot allocate device memory
+ * (a plugin host that owns the device memory pool, a real-time loop that may not block in
+ * cudaMalloc).  No counterpart in the reference.  Its scratch is a fixed 8 MiB array in
+ * the library's device memory, reserved on every GPU that loads the library; sizes whose
+ * filament stream plus one set of partial velocities exceed it are refused with
+ * FJ_ERR_SHAPE.  The first call on a device looks the array up (cudaGetSymbolAddress) and
+ * should come before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU (other streams, other host threads) race and must be serialised. */
+FJ_API int fj_vind_noalloc(const double* d_targets, int64_t n_targets, const double* const* d_zetas,
+                           const double* const* d_gammas, const int* rows, const int* cols,
+                           int n_lattices, const double* mirror_point, const double* mirror_normal,
+                           int kernel, double r_cut, int precision, double* d_v_out,
+                           fj_stream_t stream);
+
 /* compute_aic_solve (aero/aic.py:137-187): the (sum m*n)^2 row-major AIC of the bound
  * lattices at their own collocation points, projected on the area normals.  When
  * d_zetas_w != NULL (static solve) each surface's wake influence is lumped onto its
