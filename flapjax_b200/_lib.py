@@ -110,6 +110,17 @@ class FjProfile(C.Structure):
 
 FJ_REUSE_FACTORS = 1
 
+
+class FjBatchItem(C.Structure):
+    _fields_ = [
+        ("cfg", C.POINTER(FjCaseConfig)),
+        ("bufs", C.POINTER(FjCaseBuffers)),
+        ("d_ws", C.c_void_p),
+        ("ws_bytes", C.c_size_t),
+        ("i_ts", C.c_int),
+        ("flags", C.c_int),
+    ]
+
 # name -> (restype, argtypes)
 _SIGS = {
     "fj_last_error_string": (C.c_char_p, []),
@@ -122,6 +133,9 @@ _SIGS = {
     "fj_case_step": (C.c_int, [C.POINTER(FjCaseConfig), C.POINTER(FjCaseBuffers), C.c_int, C.c_int, _P, C.c_size_t,
                                _P]),
     "fj_peak_fp32": (C.c_int, [C.POINTER(C.c_double), _P]),
+    "fj_batch_workspace_size": (C.c_int, [C.c_int, C.POINTER(C.c_size_t)]),
+    "fj_step_batched": (C.c_int, [C.POINTER(FjBatchItem), C.c_int, _P, C.c_size_t, _P]),
+    "fj_case_residual": (C.c_int, [C.POINTER(FjCaseConfig), _P, C.c_size_t, C.c_int, C.POINTER(C.c_double), _P]),
     "fj_launch_count": (C.c_int64, []),
     "fj_profile_begin": (C.c_int, []),
     "fj_profile_end": (C.c_int, [C.c_void_p]),

@@ -67,10 +67,7 @@ __device__ __forceinline__ double filament_influence(const double* zeta, int R, 
 }
 
 template <int KER>
-__global__ void __launch_bounds__(256) aic_kernel(AicArgs a, const int* __restrict__ run_flag) {
-    if (run_flag != nullptr && *run_flag == 0) return;
-    extern __shared__ double sm_inf[];  // [2][max filaments]
-    const int64_t i = blockIdx.x;       // global collocation index
+__device__ __forceinline__ void aic_row(const AicArgs& a, int64_t i, double* sm_inf) {
     const double x[3] = {a.c[i * 3 + 0], a.c[i * 3 + 1], a.c[i * 3 + 2]};
     const double nrm[3] = {a.nc[i * 3 + 0], a.nc[i * 3 + 1], a.nc[i * 3 + 2]};
     double* row = a.aic + i * a.ld;
@@ -124,6 +121,49 @@ __global__ void __launch_bounds__(256) aic_kernel(AicArgs a, const int* __restri
             }
         }
     }
+}
+
+template <int KER>
+__global__ void __launch_bounds__(256) aic_kernel(AicArgs a, const int* __restrict__ run_flag) {
+    if (run_flag != nullptr && *run_flag == 0) return;
+    extern __shared__ double sm_inf[];  // [2][max filaments]
+    aic_row<KER>(a, blockIdx.x, sm_inf);
+}
+
+template <int KER>
+__global__ void __launch_bounds__(256) aic_jobs_kernel(const AicArgs* __restrict__ tab) {
+    const AicArgs& a = tab[blockIdx.y];
+    if (blockIdx.x >= a.n_rows) return;
+    if (a.run_flag != nullptr && *a.run_flag == 0) return;
+    extern __shared__ double sm_inf[];
+    aic_row<KER>(a, blockIdx.x, sm_inf);
+}
+
+int aic_launch_jobs(const AicArgs* d_tab, int n_jobs, int64_t max_rows, int max_fil, int any_mirror, int kernel,
+                    cudaStream_t s) {
+    const size_t smem = (size_t)(any_mirror ? 2 : 1) * max_fil * sizeof(double);
+    if (smem > 200 * 1024)
+        return fail(FJ_ERR_UNSUPPORTED, "aic: a surface with %d filaments exceeds shared memory", max_fil);
+    if (n_jobs == 0 || max_rows == 0) return FJ_OK;
+    dim3 g((unsigned)max_rows, (unsigned)n_jobs);
+    switch (kernel) {
+        case FJ_KERNEL_EPSILON:
+            FJ_CUDA(cudaFuncSetAttribute(aic_jobs_kernel<FJ_KERNEL_EPSILON>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            aic_jobs_kernel<FJ_KERNEL_EPSILON><<<g, 256, smem, s>>>(d_tab); note_launch();
+            break;
+        case FJ_KERNEL_CUTOFF:
+            FJ_CUDA(cudaFuncSetAttribute(aic_jobs_kernel<FJ_KERNEL_CUTOFF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            aic_jobs_kernel<FJ_KERNEL_CUTOFF><<<g, 256, smem, s>>>(d_tab); note_launch();
+            break;
+        case FJ_KERNEL_PLAIN:
+            FJ_CUDA(cudaFuncSetAttribute(aic_jobs_kernel<FJ_KERNEL_PLAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            aic_jobs_kernel<FJ_KERNEL_PLAIN><<<g, 256, smem, s>>>(d_tab); note_launch();
+            break;
+        default:
+            return fail(FJ_ERR_UNSUPPORTED, "aic: unknown kernel %d", kernel);
+    }
+    FJ_LAUNCH_CHECK("aic_jobs_kernel");
+    return FJ_OK;
 }
 
 int aic_launch(const AicArgs& a, const int* d_run_flag, cudaStream_t s) {

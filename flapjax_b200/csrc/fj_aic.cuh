@@ -22,7 +22,12 @@ struct AicArgs {
     const double* nc;  // (n_rows, 3) area normals
     double* aic;       // row-major (n_rows, ld)
     int64_t ld;
+    const int* run_flag;  // batched launches: skip this job when *run_flag == 0 (may be null)
 };
+
+// Batched: one launch for many AIC jobs (table in device memory); grid = (max rows, jobs).
+int aic_launch_jobs(const AicArgs* d_tab, int n_jobs, int64_t max_rows, int max_fil, int any_mirror, int kernel,
+                    cudaStream_t s);
 
 // d_run_flag (device int, may be null): when *d_run_flag == 0 the kernel returns at once
 // (used to skip re-assembly when the bound lattice is bitwise unchanged).

@@ -474,4 +474,76 @@ int refine_solve(const double* a, const float* xinv, int n, const double* b, dou
     return FJ_OK;
 }
 
+// ---------------------------------------------------------------------------------
+// Batched refinement sweeps (grid.y = system).
+__global__ void gemv32_jobs_kernel(const RefineJob* __restrict__ jobs, int from_residual, int accumulate) {
+    const RefineJob& J = jobs[blockIdx.y];
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= J.n) return;
+    const float* xr = J.xinv + (int64_t)row * J.n;
+    const double* v = from_residual ? J.r : J.b;
+    double acc = 0.0;
+    for (int j = lane; j < J.n; j += 32) acc += (double)xr[j] * v[j];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if (lane == 0) J.x[row] = accumulate ? J.x[row] + acc : acc;
+}
+
+__global__ void residual64_jobs_kernel(const RefineJob* __restrict__ jobs) {
+    const RefineJob& J = jobs[blockIdx.y];
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= J.n) return;
+    const double* ar = J.a + (int64_t)row * J.n;
+    double acc = 0.0;
+    for (int j = lane; j < J.n; j += 32) acc += ar[j] * J.x[j];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if (lane == 0) J.r[row] = J.b[row] - acc;
+}
+
+__global__ void rel_resid_jobs_kernel(const RefineJob* __restrict__ jobs) {
+    const RefineJob& J = jobs[blockIdx.x];
+    __shared__ double sr[32], sb[32];
+    double mr = 0.0, mb = 0.0;
+    for (int i = threadIdx.x; i < J.n; i += blockDim.x) {
+        mr = fmax(mr, fabs(J.r[i]));
+        mb = fmax(mb, fabs(J.b[i]));
+        if (J.r[i] != J.r[i]) mr = INFINITY;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        mr = fmax(mr, __shfl_down_sync(0xffffffffu, mr, off));
+        mb = fmax(mb, __shfl_down_sync(0xffffffffu, mb, off));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sr[threadIdx.x >> 5] = mr;
+        sb[threadIdx.x >> 5] = mb;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            mr = fmax(mr, sr[w]);
+            mb = fmax(mb, sb[w]);
+        }
+        *J.resid = mb > 0.0 ? mr / mb : mr;
+    }
+}
+
+int refine_jobs(const RefineJob* d_jobs, int n_jobs, int max_n, int n_iter, cudaStream_t s) {
+    if (n_jobs == 0 || max_n == 0) return FJ_OK;
+    const int wpb = 8;
+    dim3 g((unsigned)((max_n + wpb - 1) / wpb), (unsigned)n_jobs);
+    gemv32_jobs_kernel<<<g, wpb * 32, 0, s>>>(d_jobs, 0, 0); note_launch();
+    for (int it = 0; it < n_iter; ++it) {
+        residual64_jobs_kernel<<<g, wpb * 32, 0, s>>>(d_jobs); note_launch();
+        gemv32_jobs_kernel<<<g, wpb * 32, 0, s>>>(d_jobs, 1, 1); note_launch();
+    }
+    residual64_jobs_kernel<<<g, wpb * 32, 0, s>>>(d_jobs); note_launch();
+    rel_resid_jobs_kernel<<<n_jobs, 1024, 0, s>>>(d_jobs); note_launch();
+    FJ_LAUNCH_CHECK("refine_jobs");
+    return FJ_OK;
+}
+
 }  // namespace fj

@@ -27,4 +27,16 @@ int convert64to32(const double* a, float* b, int64_t count, cudaStream_t s);
 int refine_solve(const double* a, const float* xinv, int n, const double* b, double* x,
                  double* r_buf, double* d_resid, int n_iter, cudaStream_t s);
 
+// Batched refinement: one launch per sweep for many systems (table in device memory).
+struct RefineJob {
+    const double* a;    // FP64 A (n x n)
+    const float* xinv;  // FP32 inverse
+    int n;
+    const double* b;
+    double* x;
+    double* r;          // n doubles of scratch
+    double* resid;      // 1 double: final relative residual
+};
+int refine_jobs(const RefineJob* d_jobs, int n_jobs, int max_n, int n_iter, cudaStream_t s);
+
 }  // namespace fj

@@ -115,55 +115,95 @@ __device__ __forceinline__ void se3_apply(const double* hg, const double x[3], d
     for (int r = 0; r < 3; ++r) o[r] = (hg[r * 4 + 0] * x[0] + hg[r * 4 + 1] * x[1] + hg[r * 4 + 2] * x[2]) + hg[r * 4 + 3];
 }
 
+// ------------------------------------------------------------------------------------
+// Per-step kernels.  Each reads its case from a table (blockIdx.y = case), so one launch
+// advances one case or a whole batch of cases.
+// ------------------------------------------------------------------------------------
+struct StepCase {
+    Layout L;
+    int nb;
+    int i;            // slot written by this step
+    int free_wake;
+    double dt, relax;
+    fj_flowfield flow;
+    const double* zeta0;
+    const int32_t* dof;
+    const double* hg_n;
+    const double* hgd_n;   // null: zero lattice velocity (static solve)
+    const double* hg_nm1;  // null: no lattice at n-1 (static solve)
+    double* t;             // time array; t[i] = t[i-1] + dt when i > 0 and advance_time
+    int advance_time;
+    double* zb_n;
+    double* zbd_n;
+    double* zw_n;
+    const double* zw_nm1;
+    double* c;
+    double* nc;
+    double* gb_n;
+    const double* gb_nm1;
+    double* gbd_n;
+    const double* gbd_nm1;  // null: no gamma_dot (static solve)
+    double* gw_n;
+    const double* gw_nm1;
+    const double* gw_force; // wake circulation seen by the trailing-edge filament force
+    double* fs;
+    double* fu;
+    double* alpha;
+    double* ft;
+    double* zb_nm1;         // workspace
+    double* c_dot;          // null: no lattice velocity in the RHS (static solve)
+    double* targets;
+    double* v;
+    double* ffil;
+    double* rhs;
+    const double* v_wake;   // free-wake convection velocities (null: prescribed wake)
+    const double* v_rhs;    // wake velocity at collocation points (null: static solve)
+    const double* zeta_ref; // mixed path: lattice of the cached AIC (null: no comparison)
+    int* changed;           // mixed path: set to 1 when zb_n differs from zeta_ref
+};
+
+__global__ void k_time(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    if (threadIdx.x == 0 && C.advance_time && C.i > 0) C.t[C.i] = C.t[C.i - 1] + C.dt;  // uvlm.py:1158-1161
+}
+
 // hg_to_zeta_b / hg_dot_to_zeta_b_dot (aero/uvlm.py:537-621), one thread per vertex.
-__global__ void geom_vertices_kernel(Layout L, const double* __restrict__ zeta0, const int32_t* __restrict__ dof,
-                                     const double* __restrict__ hg_n, const double* __restrict__ hgd_n,
-                                     const double* __restrict__ hg_nm1, double* __restrict__ zeta_n,
-                                     double* __restrict__ zeta_dot_n, double* __restrict__ zeta_nm1,
-                                     double* __restrict__ t_slot, double t_prev, double dt) {
+__global__ void k_geom_vertices(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    const Layout& L = C.L;
     const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (v == 0 && t_slot != nullptr) *t_slot = t_prev + dt;  // case_solve, uvlm.py:1158-1161
     if (v >= L.vo[L.n_surf]) return;
     const int s = find_surf(L.vo, L.n_surf, v);
-    const int64_t lv = v - L.vo[s];
-    const int j = (int)(lv % (L.n[s] + 1));
+    const int j = (int)((v - L.vo[s]) % (L.n[s] + 1));
     // the host validates the mapping; the clamp only keeps a bad entry in bounds
-    const int node = min(max(dof[L.dofo[s] + j], 0), L.n_nodes - 1);
-    const double x0[3] = {zeta0[v * 3], zeta0[v * 3 + 1], zeta0[v * 3 + 2]};
+    const int node = min(max(C.dof[L.dofo[s] + j], 0), L.n_nodes - 1);
+    const double x0[3] = {C.zeta0[v * 3], C.zeta0[v * 3 + 1], C.zeta0[v * 3 + 2]};
     double o[3];
-    se3_apply(hg_n + (int64_t)node * 16, x0, o);
-    zeta_n[v * 3] = o[0];
-    zeta_n[v * 3 + 1] = o[1];
-    zeta_n[v * 3 + 2] = o[2];
-    if (zeta_dot_n != nullptr) {
-        if (hgd_n != nullptr) {
-            se3_apply(hgd_n + (int64_t)node * 16, x0, o);
-        } else {
-            o[0] = o[1] = o[2] = 0.0;
-        }
-        zeta_dot_n[v * 3] = o[0];
-        zeta_dot_n[v * 3 + 1] = o[1];
-        zeta_dot_n[v * 3 + 2] = o[2];
+    se3_apply(C.hg_n + (int64_t)node * 16, x0, o);
+    for (int d = 0; d < 3; ++d) C.zb_n[v * 3 + d] = o[d];
+    if (C.hgd_n != nullptr) {
+        se3_apply(C.hgd_n + (int64_t)node * 16, x0, o);
+    } else {
+        o[0] = o[1] = o[2] = 0.0;
     }
-    if (zeta_nm1 != nullptr) {
-        se3_apply(hg_nm1 + (int64_t)node * 16, x0, o);
-        zeta_nm1[v * 3] = o[0];
-        zeta_nm1[v * 3 + 1] = o[1];
-        zeta_nm1[v * 3 + 2] = o[2];
+    for (int d = 0; d < 3; ++d) C.zbd_n[v * 3 + d] = o[d];
+    if (C.hg_nm1 != nullptr) {
+        se3_apply(C.hg_nm1 + (int64_t)node * 16, x0, o);
+        for (int d = 0; d < 3; ++d) C.zb_nm1[v * 3 + d] = o[d];
     }
 }
 
 // compute_surf_c / compute_surf_nc (aero/utils.py:87-105) and c_dot (uvlm.py:891-893).
-__global__ void geom_panels_kernel(Layout L, const double* __restrict__ zeta, const double* __restrict__ zeta_dot,
-                                   double* __restrict__ c, double* __restrict__ nc, double* __restrict__ c_dot) {
+__global__ void k_geom_panels(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    const Layout& L = C.L;
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= L.po[L.n_surf]) return;
     const int s = find_surf(L.po, L.n_surf, p);
     const int64_t lp = p - L.po[s];
     const int n = L.n[s];
     const int k = (int)(lp / n), l = (int)(lp % n);
-    const double* z = zeta + L.vo[s] * 3;
-    const double* z00 = z + ((int64_t)k * (n + 1) + l) * 3;
+    const double* z00 = C.zb_n + (L.vo[s] + (int64_t)k * (n + 1) + l) * 3;
     const double* z01 = z00 + 3;
     const double* z10 = z00 + (n + 1) * 3;
     const double* z11 = z10 + 3;
@@ -171,29 +211,28 @@ __global__ void geom_panels_kernel(Layout L, const double* __restrict__ zeta, co
         // neighbour_average over axis 0 then axis 1 (algebra/array_utils.py:106-136)
         const double a0 = 0.5 * (z00[d] + z10[d]);
         const double a1 = 0.5 * (z01[d] + z11[d]);
-        c[p * 3 + d] = 0.5 * (a0 + a1);
+        C.c[p * 3 + d] = 0.5 * (a0 + a1);
     }
     const double d1[3] = {z11[0] - z00[0], z11[1] - z00[1], z11[2] - z00[2]};
     const double d2[3] = {z10[0] - z01[0], z10[1] - z01[1], z10[2] - z01[2]};
-    nc[p * 3 + 0] = d1[1] * d2[2] - d1[2] * d2[1];
-    nc[p * 3 + 1] = d1[2] * d2[0] - d1[0] * d2[2];
-    nc[p * 3 + 2] = d1[0] * d2[1] - d1[1] * d2[0];
-    if (c_dot != nullptr) {
-        const double* w = zeta_dot + L.vo[s] * 3;
-        const double* w00 = w + ((int64_t)k * (n + 1) + l) * 3;
+    C.nc[p * 3 + 0] = d1[1] * d2[2] - d1[2] * d2[1];
+    C.nc[p * 3 + 1] = d1[2] * d2[0] - d1[0] * d2[2];
+    C.nc[p * 3 + 2] = d1[0] * d2[1] - d1[1] * d2[0];
+    if (C.c_dot != nullptr) {
+        const double* w00 = C.zbd_n + (L.vo[s] + (int64_t)k * (n + 1) + l) * 3;
         const double* w01 = w00 + 3;
         const double* w10 = w00 + (n + 1) * 3;
         const double* w11 = w10 + 3;
         for (int d = 0; d < 3; ++d) {
             const double a0 = 0.5 * (w00[d] + w10[d]);
             const double a1 = 0.5 * (w01[d] + w11[d]);
-            c_dot[p * 3 + d] = 0.5 * (a0 + a1);
+            C.c_dot[p * 3 + d] = 0.5 * (a0 + a1);
         }
     }
 }
 
 // ------------------------------------------------------------------------------------
-// 2. wake
+// wake
 // ------------------------------------------------------------------------------------
 // initialise_wake (uvlm.py:662-689): TE + cumsum(dt |U|) along the freestream direction.
 // `hs_len` > 0 builds the 2-row horseshoe wake instead (uvlm.py:642-660).
@@ -232,50 +271,46 @@ __global__ void init_wake_kernel(Layout L, const double* __restrict__ zeta_b, fj
     for (int d = 0; d < 3; ++d) zeta_w[v * 3 + d] = te[d] + sdist * (f.u_inf[d] / umag);
 }
 
-// Rows 0..m_star-1 of every surface's wake, packed as the free-wake target list.
-__global__ void gather_wake_targets_kernel(Layout L, const double* __restrict__ zeta_w, double* __restrict__ out) {
+// Rows 0..m_star-1 of every surface's wake at n-1, packed as the free-wake target list.
+__global__ void k_gather_wake_targets(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    const Layout& L = C.L;
+    if (!C.free_wake) return;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= L.wto[L.n_surf]) return;
     const int s = find_surf(L.wto, L.n_surf, t);
     const int64_t src = L.wvo[s] + (t - L.wto[s]);
-    out[t * 3] = zeta_w[src * 3];
-    out[t * 3 + 1] = zeta_w[src * 3 + 1];
-    out[t * 3 + 2] = zeta_w[src * 3 + 2];
+    for (int d = 0; d < 3; ++d) C.targets[t * 3 + d] = C.zw_nm1[src * 3 + d];
 }
 
 // propagate_surf_wake, uniform branch (aero/utils.py:427-450): shed the TE row and
 // circulation of step n-1, drop the last row, convect the rest by dt * (U + v_ind).
-__global__ void wake_shed_kernel(Layout L, const double* __restrict__ zeta_b_n, const double* __restrict__ zeta_w_nm1,
-                                 const double* __restrict__ gamma_b_nm1, const double* __restrict__ gamma_w_nm1,
-                                 const double* __restrict__ v_ind, fj_flowfield f, const double* __restrict__ t_slot,
-                                 double dt, double* __restrict__ zeta_w_n, double* __restrict__ gamma_w_n) {
+__global__ void k_wake_shed(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    const Layout& L = C.L;
     const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t nv = L.wvo[L.n_surf];
-    const double t = *t_slot;
+    const double t = C.t[C.i];
     if (v < nv) {
         const int s = find_surf(L.wvo, L.n_surf, v);
         const int64_t lv = v - L.wvo[s];
         const int n = L.n[s];
         const int r = (int)(lv / (n + 1)), l = (int)(lv % (n + 1));
         if (r == 0) {
-            const double* te = zeta_b_n + (L.vo[s] + (int64_t)L.m[s] * (n + 1) + l) * 3;
-            zeta_w_n[v * 3] = te[0];
-            zeta_w_n[v * 3 + 1] = te[1];
-            zeta_w_n[v * 3 + 2] = te[2];
+            const double* te = C.zb_n + (L.vo[s] + (int64_t)L.m[s] * (n + 1) + l) * 3;
+            for (int d = 0; d < 3; ++d) C.zw_n[v * 3 + d] = te[d];
         } else {
             const int64_t src = L.wvo[s] + (int64_t)(r - 1) * (n + 1) + l;
-            const double x[3] = {zeta_w_nm1[src * 3], zeta_w_nm1[src * 3 + 1], zeta_w_nm1[src * 3 + 2]};
+            const double x[3] = {C.zw_nm1[src * 3], C.zw_nm1[src * 3 + 1], C.zw_nm1[src * 3 + 2]};
             double u[3];
-            flow_eval(f, x, t, u);
-            if (v_ind != nullptr) {
+            flow_eval(C.flow, x, t, u);
+            if (C.v_wake != nullptr) {
                 const int64_t ti = L.wto[s] + (int64_t)(r - 1) * (n + 1) + l;
-                u[0] += v_ind[ti * 3];
-                u[1] += v_ind[ti * 3 + 1];
-                u[2] += v_ind[ti * 3 + 2];
+                u[0] += C.v_wake[ti * 3];
+                u[1] += C.v_wake[ti * 3 + 1];
+                u[2] += C.v_wake[ti * 3 + 2];
             }
-            zeta_w_n[v * 3] = x[0] + dt * u[0];
-            zeta_w_n[v * 3 + 1] = x[1] + dt * u[1];
-            zeta_w_n[v * 3 + 2] = x[2] + dt * u[2];
+            for (int d = 0; d < 3; ++d) C.zw_n[v * 3 + d] = x[d] + C.dt * u[d];
         }
     }
     const int64_t g = v - nv;
@@ -284,8 +319,8 @@ __global__ void wake_shed_kernel(Layout L, const double* __restrict__ zeta_b_n, 
         const int64_t lg = g - L.wpo[s];
         const int n = L.n[s];
         const int r = (int)(lg / n), l = (int)(lg % n);
-        gamma_w_n[g] = r == 0 ? gamma_b_nm1[L.po[s] + (int64_t)(L.m[s] - 1) * n + l]
-                              : gamma_w_nm1[L.wpo[s] + (int64_t)(r - 1) * n + l];
+        C.gw_n[g] = r == 0 ? C.gb_nm1[L.po[s] + (int64_t)(L.m[s] - 1) * n + l]
+                           : C.gw_nm1[L.wpo[s] + (int64_t)(r - 1) * n + l];
     }
 }
 
@@ -306,33 +341,39 @@ __global__ void static_gamma_w_kernel(Layout L, const double* __restrict__ gamma
     }
 }
 
-// ------------------------------------------------------------------------------------
-// 4. right-hand side (uvlm.py:961-985): b = -((U(c) - c_dot + v_wake) . n)
-// ------------------------------------------------------------------------------------
-__global__ void rhs_kernel(int64_t np, const double* __restrict__ c, const double* __restrict__ c_dot,
-                           const double* __restrict__ nc, const double* __restrict__ v, fj_flowfield f,
-                           const double* __restrict__ t_slot, double t_fixed, double* __restrict__ b) {
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= np) return;
-    const double t = t_slot != nullptr ? *t_slot : t_fixed;
-    const double x[3] = {c[p * 3], c[p * 3 + 1], c[p * 3 + 2]};
-    double u[3];
-    flow_eval(f, x, t, u);
-    if (c_dot != nullptr) {
-        u[0] -= c_dot[p * 3];
-        u[1] -= c_dot[p * 3 + 1];
-        u[2] -= c_dot[p * 3 + 2];
-    }
-    if (v != nullptr) {
-        u[0] += v[p * 3];
-        u[1] += v[p * 3 + 1];
-        u[2] += v[p * 3 + 2];
-    }
-    b[p] = -(u[0] * nc[p * 3] + u[1] * nc[p * 3 + 1] + u[2] * nc[p * 3 + 2]);
+// Mixed path: flag a lattice that differs (bitwise) from the one of the cached AIC.
+__global__ void k_clear_changed(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    if (threadIdx.x == 0 && C.changed != nullptr) *C.changed = 0;
+}
+
+__global__ void k_changed(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    if (C.changed == nullptr) return;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < C.L.vo[C.L.n_surf] * 3 && C.zb_n[i] != C.zeta_ref[i]) *C.changed = 1;
 }
 
 // ------------------------------------------------------------------------------------
-// 6. forces (aero/utils.py:126-223)
+// right-hand side (uvlm.py:961-985): b = -((U(c) - c_dot + v_wake) . n)
+// ------------------------------------------------------------------------------------
+__global__ void k_rhs(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= C.nb) return;
+    const double t = C.t[C.i];
+    const double x[3] = {C.c[p * 3], C.c[p * 3 + 1], C.c[p * 3 + 2]};
+    double u[3];
+    flow_eval(C.flow, x, t, u);
+    if (C.c_dot != nullptr)
+        for (int d = 0; d < 3; ++d) u[d] -= C.c_dot[p * 3 + d];
+    if (C.v_rhs != nullptr)
+        for (int d = 0; d < 3; ++d) u[d] += C.v_rhs[p * 3 + d];
+    C.rhs[p] = -(u[0] * C.nc[p * 3] + u[1] * C.nc[p * 3 + 1] + u[2] * C.nc[p * 3 + 2]);
+}
+
+// ------------------------------------------------------------------------------------
+// forces (aero/utils.py:126-223)
 // ------------------------------------------------------------------------------------
 // Filament f of surface s: f < m(n+1): chordwise (k,l)->(k+1,l); else spanwise (k,l)->(k,l+1).
 __device__ __forceinline__ void filament_ends(const Layout& L, int s, int64_t lf, int& k0, int& l0, int& k1,
@@ -355,7 +396,9 @@ __device__ __forceinline__ void filament_ends(const Layout& L, int s, int64_t lf
     }
 }
 
-__global__ void force_targets_kernel(Layout L, const double* __restrict__ zeta, double* __restrict__ out) {
+__global__ void k_force_targets(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    const Layout& L = C.L;
     const int64_t fi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (fi >= L.fo[L.n_surf]) return;
     const int s = find_surf(L.fo, L.n_surf, fi);
@@ -363,37 +406,34 @@ __global__ void force_targets_kernel(Layout L, const double* __restrict__ zeta, 
     bool chord;
     filament_ends(L, s, fi - L.fo[s], k0, l0, k1, l1, chord);
     const int n = L.n[s];
-    const double* a = zeta + (L.vo[s] + (int64_t)k0 * (n + 1) + l0) * 3;
-    const double* b = zeta + (L.vo[s] + (int64_t)k1 * (n + 1) + l1) * 3;
-    for (int d = 0; d < 3; ++d) out[fi * 3 + d] = 0.5 * (a[d] + b[d]);
+    const double* a = C.zb_n + (L.vo[s] + (int64_t)k0 * (n + 1) + l0) * 3;
+    const double* b = C.zb_n + (L.vo[s] + (int64_t)k1 * (n + 1) + l1) * 3;
+    for (int d = 0; d < 3; ++d) C.targets[fi * 3 + d] = 0.5 * (a[d] + b[d]);
 }
 
-__global__ void force_filament_kernel(Layout L, const double* __restrict__ zeta, const double* __restrict__ zeta_dot,
-                                      const double* __restrict__ gamma_b, const double* __restrict__ gamma_w,
-                                      const double* __restrict__ targets, const double* __restrict__ v,
-                                      fj_flowfield f, const double* __restrict__ t_slot, double t_fixed,
-                                      double* __restrict__ ffil) {
+__global__ void k_force_filament(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    const Layout& L = C.L;
     const int64_t fi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (fi >= L.fo[L.n_surf]) return;
-    const double t = t_slot != nullptr ? *t_slot : t_fixed;
+    const double t = C.t[C.i];
     const int s = find_surf(L.fo, L.n_surf, fi);
     int k0, l0, k1, l1;
     bool chord;
     filament_ends(L, s, fi - L.fo[s], k0, l0, k1, l1, chord);
     const int m = L.m[s], n = L.n[s];
-    const double* gb = gamma_b + L.po[s];
-    const double* a = zeta + (L.vo[s] + (int64_t)k0 * (n + 1) + l0) * 3;
-    const double* b = zeta + (L.vo[s] + (int64_t)k1 * (n + 1) + l1) * 3;
-    const double x[3] = {targets[fi * 3], targets[fi * 3 + 1], targets[fi * 3 + 2]};
+    const double* gb = C.gb_n + L.po[s];
+    const int64_t ia = L.vo[s] + (int64_t)k0 * (n + 1) + l0;
+    const int64_t ib = L.vo[s] + (int64_t)k1 * (n + 1) + l1;
+    const double* a = C.zb_n + ia * 3;
+    const double* b = C.zb_n + ib * 3;
+    const double x[3] = {C.targets[fi * 3], C.targets[fi * 3 + 1], C.targets[fi * 3 + 2]};
     double u[3];
-    flow_eval(f, x, t, u);
+    flow_eval(C.flow, x, t, u);
     double vr[3];
     for (int d = 0; d < 3; ++d) {
-        const double mpd = zeta_dot != nullptr
-                               ? 0.5 * (zeta_dot[(L.vo[s] + (int64_t)k0 * (n + 1) + l0) * 3 + d] +
-                                        zeta_dot[(L.vo[s] + (int64_t)k1 * (n + 1) + l1) * 3 + d])
-                               : 0.0;
-        vr[d] = (u[d] + v[fi * 3 + d]) - mpd;
+        const double mpd = 0.5 * (C.zbd_n[ia * 3 + d] + C.zbd_n[ib * 3 + d]);
+        vr[d] = (u[d] + C.v[fi * 3 + d]) - mpd;
     }
     double g;
     if (chord) {  // gamma_chordwise[:, :-1] = G; gamma_chordwise[:, 1:] += -G
@@ -404,54 +444,52 @@ __global__ void force_filament_kernel(Layout L, const double* __restrict__ zeta,
         g = 0.0;
         if (k0 < m) g = -gb[(int64_t)k0 * n + l0];
         if (k0 >= 1) g += gb[(int64_t)(k0 - 1) * n + l0];
-        if (k0 == m && gamma_w != nullptr && L.ms[s] > 0) g += -gamma_w[L.wpo[s] + l0];
+        if (k0 == m && C.gw_force != nullptr && L.ms[s] > 0) g += -C.gw_force[L.wpo[s] + l0];
     }
     const double r[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
     const double cr[3] = {vr[1] * r[2] - vr[2] * r[1], vr[2] * r[0] - vr[0] * r[2], vr[0] * r[1] - vr[1] * r[0]};
-    for (int d = 0; d < 3; ++d) ffil[fi * 3 + d] = f.rho * (g * cr[d]);
+    for (int d = 0; d < 3; ++d) C.ffil[fi * 3 + d] = C.flow.rho * (g * cr[d]);
 }
 
-// ------------------------------------------------------------------------------------
-// 7. post-processing
-// ------------------------------------------------------------------------------------
 // compute_gamma_dot (uvlm.py:691-715)
-__global__ void gamma_dot_kernel(int64_t np, const double* __restrict__ gb_n, const double* __restrict__ gb_nm1,
-                                 const double* __restrict__ gbd_nm1, double dt, double relax,
-                                 double* __restrict__ gbd_n) {
+__global__ void k_gamma_dot(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    if (C.gbd_nm1 == nullptr) return;
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= np) return;
-    const double cur = (gb_n[p] - gb_nm1[p]) / dt;
-    gbd_n[p] = cur * relax + gbd_nm1[p] * (1.0 - relax);
+    if (p >= C.nb) return;
+    const double cur = (C.gb_n[p] - C.gb_nm1[p]) / C.dt;
+    C.gbd_n[p] = cur * C.relax + C.gbd_nm1[p] * (1.0 - C.relax);
 }
 
 // split_to_vertex of the filament forces (aero/utils.py:220-222) and of
 // rho * gamma_dot * n (uvlm.py:1093-1103), algebra/array_utils.py:332-367.
-__global__ void vertex_forces_kernel(Layout L, const double* __restrict__ ffil, const double* __restrict__ gbd,
-                                     const double* __restrict__ nc, double rho, double* __restrict__ f_steady,
-                                     double* __restrict__ f_unsteady) {
+__global__ void k_vertex_forces(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    const Layout& L = C.L;
     const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= L.vo[L.n_surf]) return;
     const int s = find_surf(L.vo, L.n_surf, v);
     const int64_t lv = v - L.vo[s];
     const int m = L.m[s], n = L.n[s];
     const int k = (int)(lv / (n + 1)), l = (int)(lv % (n + 1));
-    const double* fc = ffil + L.fo[s] * 3;                          // (m, n+1, 3)
-    const double* fs = ffil + (L.fo[s] + (int64_t)m * (n + 1)) * 3;  // (m+1, n, 3)
+    const double* fc = C.ffil + L.fo[s] * 3;                          // (m, n+1, 3)
+    const double* fsp = C.ffil + (L.fo[s] + (int64_t)m * (n + 1)) * 3;  // (m+1, n, 3)
+    const double rho = C.flow.rho;
     for (int d = 0; d < 3; ++d) {
         double a = 0.0;  // split_to_vertex(f_chordwise, 0)
         if (k < m) a = 0.5 * fc[((int64_t)k * (n + 1) + l) * 3 + d];
         if (k >= 1) a += 0.5 * fc[((int64_t)(k - 1) * (n + 1) + l) * 3 + d];
         double b = 0.0;  // split_to_vertex(f_spanwise, 1)
-        if (l < n) b = 0.5 * fs[((int64_t)k * n + l) * 3 + d];
-        if (l >= 1) b += 0.5 * fs[((int64_t)k * n + l - 1) * 3 + d];
-        f_steady[v * 3 + d] = a + b;
+        if (l < n) b = 0.5 * fsp[((int64_t)k * n + l) * 3 + d];
+        if (l >= 1) b += 0.5 * fsp[((int64_t)k * n + l - 1) * 3 + d];
+        C.fs[v * 3 + d] = a + b;
     }
-    if (f_unsteady == nullptr) return;
+    const bool has_gd = C.gbd_nm1 != nullptr;
     for (int d = 0; d < 3; ++d) {
         double out = 0.0;
-        if (gbd != nullptr) {
-            const double* g = gbd + L.po[s];
-            const double* nn = nc + L.po[s] * 3;
+        if (has_gd) {
+            const double* g = C.gbd_n + L.po[s];
+            const double* nn = C.nc + L.po[s] * 3;
             // split along axis 0 into (m+1, n), then along axis 1 into (m+1, n+1)
             auto s0 = [&](int kk, int ll) -> double {
                 double r = 0.0;
@@ -462,21 +500,21 @@ __global__ void vertex_forces_kernel(Layout L, const double* __restrict__ ffil, 
             if (l < n) out = 0.5 * s0(k, l);
             if (l >= 1) out += 0.5 * s0(k, l - 1);
         }
-        f_unsteady[v * 3 + d] = out;
+        C.fu[v * 3 + d] = out;
     }
 }
 
 // strip_alpha (aero/utils.py:226-273), one thread per strip.
-__global__ void strip_alpha_kernel(Layout L, const double* __restrict__ zeta, const double* __restrict__ f_steady,
-                                   fj_flowfield f, const double* __restrict__ t_slot, double t_fixed,
-                                   double* __restrict__ alpha) {
+__global__ void k_strip_alpha(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    const Layout& L = C.L;
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= L.so[L.n_surf]) return;
-    const double t = t_slot != nullptr ? *t_slot : t_fixed;
+    const double t = C.t[C.i];
     const int s = find_surf(L.so, L.n_surf, j);
     const int l = (int)(j - L.so[s]);
     const int m = L.m[s], n = L.n[s];
-    const double* z = zeta + L.vo[s] * 3;
+    const double* z = C.zb_n + L.vo[s] * 3;
     const double* le0 = z + (int64_t)l * 3;
     const double* le1 = le0 + 3;
     const double* te0 = z + ((int64_t)m * (n + 1) + l) * 3;
@@ -493,7 +531,7 @@ __global__ void strip_alpha_kernel(Layout L, const double* __restrict__ zeta, co
     const double b_len = sqrt(span[0] * span[0] + span[1] * span[1] + span[2] * span[2]);
     const double es[3] = {span[0] / b_len, span[1] / b_len, span[2] / b_len};
     double vr[3];
-    flow_eval(f, mid, t, vr);
+    flow_eval(C.flow, mid, t, vr);
     const double vmag2 = vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2];
     double el[3] = {vr[1] * es[2] - vr[2] * es[1], vr[2] * es[0] - vr[0] * es[2], vr[0] * es[1] - vr[1] * es[0]};
     const double eln = sqrt(el[0] * el[0] + el[1] * el[1] + el[2] * el[2]);
@@ -501,22 +539,23 @@ __global__ void strip_alpha_kernel(Layout L, const double* __restrict__ zeta, co
     el[1] /= eln;
     el[2] /= eln;
     double fst[3] = {0.0, 0.0, 0.0};
-    const double* fs = f_steady + L.vo[s] * 3;
+    const double* fsv = C.fs + L.vo[s] * 3;
     for (int k = 0; k <= m; ++k)
         for (int d = 0; d < 3; ++d)
-            fst[d] += 0.5 * (fs[((int64_t)k * (n + 1) + l) * 3 + d] + fs[((int64_t)k * (n + 1) + l + 1) * 3 + d]);
-    const double q = 0.5 * f.rho * vmag2;
+            fst[d] += 0.5 * (fsv[((int64_t)k * (n + 1) + l) * 3 + d] + fsv[((int64_t)k * (n + 1) + l + 1) * 3 + d]);
+    const double q = 0.5 * C.flow.rho * vmag2;
     const double cl = (fst[0] * el[0] + fst[1] * el[1] + fst[2] * el[2]) / (q * c_len * b_len);
-    alpha[j] = cl / (2.0 * kPi);
+    C.alpha[j] = cl / (2.0 * kPi);
 }
 
-// Sum over vertices of f_steady + f_unsteady (one CTA, fixed order).
-__global__ void force_total_kernel(int64_t nv, const double* __restrict__ fs, const double* __restrict__ fu,
-                                   double* __restrict__ out) {
+// Sum over vertices of f_steady + f_unsteady (one CTA per case, fixed order).
+__global__ void k_force_total(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    const int64_t nv = C.L.vo[C.L.n_surf];
     __shared__ double sh[3][256];
     double a[3] = {0.0, 0.0, 0.0};
     for (int64_t v = threadIdx.x; v < nv; v += blockDim.x)
-        for (int d = 0; d < 3; ++d) a[d] += fs[v * 3 + d] + (fu != nullptr ? fu[v * 3 + d] : 0.0);
+        for (int d = 0; d < 3; ++d) a[d] += C.fs[v * 3 + d] + C.fu[v * 3 + d];
     for (int d = 0; d < 3; ++d) sh[d][threadIdx.x] = a[d];
     __syncthreads();
     for (int w = blockDim.x / 2; w > 0; w >>= 1) {
@@ -525,29 +564,7 @@ __global__ void force_total_kernel(int64_t nv, const double* __restrict__ fs, co
         __syncthreads();
     }
     if (threadIdx.x == 0)
-        for (int d = 0; d < 3; ++d) out[d] = sh[d][0];
-}
-
-__global__ void changed_kernel(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
-                               int* __restrict__ flag) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n && a[i] != b[i]) *flag = 1;
-}
-
-__global__ void max_reduce_kernel(const double* __restrict__ x, int n, double* __restrict__ out) {
-    __shared__ double sh[256];
-    double m = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const double v = x[i];
-        m = (v != v) ? INFINITY : fmax(m, v);
-    }
-    sh[threadIdx.x] = m;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + w]);
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) *out = sh[0];
+        for (int d = 0; d < 3; ++d) C.ft[d] = sh[d][0];
 }
 
 static inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
@@ -582,7 +599,8 @@ struct Plan {
     double* r;
     double* resid;       // per-slot refinement residual (mixed)
     double* ffil;
-    double* scalar;      // 1 double scratch
+    char* tab;           // device table of a one-case step
+    size_t tab_bytes;
 };
 
 static int validate(const fj_case_config* c) {
@@ -607,6 +625,36 @@ static int validate(const fj_case_config* c) {
     for (int s = 0; s < c->n_surf; ++s) nb += (int64_t)c->m[s] * c->n[s];
     if (nb > 6144) return fail(FJ_ERR_UNSUPPORTED, "AIC order %lld exceeds 6144", (long long)nb);
     return FJ_OK;
+}
+
+struct TableLayout {
+    size_t step, pack_free, pack_wake, pack_bound, job_free, job_rhs, job_force, cta_free, cta_rhs, cta_force, aic,
+        refine, total;
+};
+
+static TableLayout table_layout(int k) {
+    TableLayout t;
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        o = align_up(o, 256);
+        const size_t at = o;
+        o += bytes;
+        return at;
+    };
+    t.step = take(k * sizeof(StepCase));
+    t.pack_free = take(k * sizeof(PackJob));
+    t.pack_wake = take(k * sizeof(PackJob));
+    t.pack_bound = take(k * sizeof(PackJob));
+    t.job_free = take(k * sizeof(VindJob));
+    t.job_rhs = take(k * sizeof(VindJob));
+    t.job_force = take(k * sizeof(VindJob));
+    t.cta_free = take((k + 1) * sizeof(int64_t));
+    t.cta_rhs = take((k + 1) * sizeof(int64_t));
+    t.cta_force = take((k + 1) * sizeof(int64_t));
+    t.aic = take(k * sizeof(AicArgs));
+    t.refine = take(k * sizeof(RefineJob));
+    t.total = align_up(o, 256);
+    return t;
 }
 
 static int make_plan(const fj_case_config* cfg, void* ws, size_t ws_bytes, Plan& p) {
@@ -666,7 +714,8 @@ static int make_plan(const fj_case_config* cfg, void* ws, size_t ws_bytes, Plan&
     p.r = a.carve<double>(p.nb);
     p.resid = a.carve<double>(cfg->n_tstep);
     p.ffil = a.carve<double>(L.fo[ns] * 3);
-    p.scalar = a.carve<double>(4);
+    p.tab_bytes = table_layout(1).total;
+    p.tab = a.carve<char>(p.tab_bytes);
     if (ws != nullptr && !a.fits())
         return fail(FJ_ERR_NOMEM, "workspace of %zu bytes is smaller than the %zu required", ws_bytes, a.used);
     p.ws_needed = a.used;
@@ -674,7 +723,7 @@ static int make_plan(const fj_case_config* cfg, void* ws, size_t ws_bytes, Plan&
 }
 
 // ------------------------------------------------------------------------------------
-// v_ind driver: pack the stream then sum over a target set
+// Stream packing jobs and induced-velocity jobs
 // ------------------------------------------------------------------------------------
 struct StreamBuilder {
     PackArgs a;
@@ -711,12 +760,15 @@ struct StreamBuilder {
     int64_t len() const { return a.offset[n]; }
 };
 
+static void* stream_at(const Plan& p, int64_t elem_offset) {
+    const size_t es = p.cfg.precision == FJ_PREC_FP64 ? sizeof(Elem64) : sizeof(Elem32);
+    return (char*)p.stream + elem_offset * es;
+}
+
 static int pack(const Plan& p, const StreamBuilder& sb, int64_t elem_offset, cudaStream_t s) {
-    // pack lattices into the stream starting at element `elem_offset`
     PackArgs a = sb.a;
-    if (p.cfg.precision == FJ_PREC_FP64)
-        return pack_stream64(a, (Elem64*)p.stream + elem_offset, s);
-    return pack_stream32(a, (Elem32*)p.stream + elem_offset, s);
+    if (p.cfg.precision == FJ_PREC_FP64) return pack_stream64(a, (Elem64*)stream_at(p, elem_offset), s);
+    return pack_stream32(a, (Elem32*)stream_at(p, elem_offset), s);
 }
 
 static int vind_sum(const Plan& p, const double* targets, int64_t nt, int64_t n_elem, int64_t n_links, double* out,
@@ -727,6 +779,7 @@ static int vind_sum(const Plan& p, const double* targets, int64_t nt, int64_t n_
         return FJ_OK;
     }
     VindJob j;
+    memset(&j, 0, sizeof(j));
     j.targets = targets;
     j.n_targets = nt;
     j.stream = p.stream;
@@ -734,6 +787,7 @@ static int vind_sum(const Plan& p, const double* targets, int64_t nt, int64_t n_
     j.n_split = choose_split(nt, n_elem, p.cfg.precision);
     j.part = p.part;
     j.n_links = n_links;
+    j.out = out;
     if ((int64_t)j.n_split * nt * 3 > p.part_elems) return fail(FJ_ERR_NOMEM, "partial buffer too small");
     FJ_TRY(vind_launch(j, p.cfg.precision, p.cfg.kernel, p.cfg.r_cut, s));
     return reduce_partials(p.part, j.n_split, nt, out, 0, 1.0, s);
@@ -771,6 +825,11 @@ static void fill_aic_args(const Plan& p, AicArgs& a, const double* zeta, const d
     a.nc = nc;
     a.aic = p.a64;
     a.ld = p.nb;
+    a.run_flag = nullptr;
+}
+
+static int upload(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    return cuda_status(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "table upload");
 }
 
 // ------------------------------------------------------------------------------------
@@ -782,42 +841,73 @@ static int run_static(const Plan& p, const fj_case_buffers* B, const double* hg,
     const fj_case_config& c = p.cfg;
     double* zb = B->d_zeta_b;
     double* zw = B->d_zeta_w;
-    double* cc = B->d_c;
-    double* nc = B->d_nc;
     double* gb = B->d_gamma_b;
     double* gw = B->d_gamma_w;
     FJ_CUDA(cudaMemcpyAsync(B->d_t, &t0, sizeof(double), cudaMemcpyHostToDevice, s));
-    geom_vertices_kernel<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(L, B->d_zeta_b0, B->d_dof_mapping, hg, nullptr, nullptr,
-                                                                zb, B->d_zeta_b_dot, nullptr, nullptr, 0.0, 0.0); note_launch();
-    geom_panels_kernel<<<nblk(L.po[L.n_surf]), 256, 0, s>>>(L, zb, nullptr, cc, nc, nullptr); note_launch();
     // wake of the solve: initialise_wake or the horseshoe (rows 1, far end at HORSESHOE_LENGTH)
-    const double* zw_solve;
-    int rows_solve;
+    const double* zw_solve = zw;
+    const double* gw_solve = gw;
+    int rows_solve = -1;
     if (horseshoe) {
-        init_wake_kernel<<<nblk(2 * (p.sz_strip + L.n_surf)), 256, 0, s>>>(L, zb, c.flow, c.dt, 1e3, p.hs_zw, 1); note_launch();
         zw_solve = p.hs_zw;
+        gw_solve = p.hs_gw;
         rows_solve = 1;
-    } else {
-        init_wake_kernel<<<nblk(L.wvo[L.n_surf]), 256, 0, s>>>(L, zb, c.flow, c.dt, 0.0, zw, 0); note_launch();
-        zw_solve = zw;
-        rows_solve = -1;
     }
+    StepCase C;
+    memset(&C, 0, sizeof(C));
+    C.L = L;
+    C.nb = p.nb;
+    C.i = 0;
+    C.dt = c.dt;
+    C.relax = c.gamma_dot_relaxation;
+    C.flow = c.flow;
+    C.zeta0 = B->d_zeta_b0;
+    C.dof = B->d_dof_mapping;
+    C.hg_n = hg;
+    C.t = B->d_t;
+    C.zb_n = zb;
+    C.zbd_n = B->d_zeta_b_dot;
+    C.zw_n = zw;
+    C.c = B->d_c;
+    C.nc = B->d_nc;
+    C.gb_n = gb;
+    C.gbd_n = B->d_gamma_b_dot;
+    C.gw_n = gw;
+    C.gw_force = gw_solve;
+    C.fs = B->d_f_steady;
+    C.fu = B->d_f_unsteady;
+    C.alpha = B->d_alpha;
+    C.ft = B->d_force_total;
+    C.zb_nm1 = p.zeta_nm1;
+    C.targets = p.targets;
+    C.v = p.v;
+    C.ffil = p.ffil;
+    C.rhs = p.rhs;
+    const TableLayout tl = table_layout(1);
+    StepCase* dC = (StepCase*)(p.tab + tl.step);
+    FJ_TRY(upload(dC, &C, sizeof(C), s));
+    k_geom_vertices<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(dC); note_launch();
+    k_geom_panels<<<nblk(L.po[L.n_surf]), 256, 0, s>>>(dC); note_launch();
+    if (horseshoe) {
+        int64_t rows_tot = 0;
+        for (int q = 0; q < L.n_surf; ++q) rows_tot += (int64_t)((L.ms[q] == 0 ? 0 : 1) + 1) * (L.n[q] + 1);
+        init_wake_kernel<<<nblk(rows_tot), 256, 0, s>>>(L, zb, c.flow, c.dt, 1e3, p.hs_zw, 1); note_launch();
+    }
+    init_wake_kernel<<<nblk(L.wvo[L.n_surf]), 256, 0, s>>>(L, zb, c.flow, c.dt, 0.0, zw, 0); note_launch();
     FJ_LAUNCH_CHECK("static geometry");
     AicArgs aa;
-    fill_aic_args(p, aa, zb, cc, nc, zw_solve, rows_solve);
+    fill_aic_args(p, aa, zb, B->d_c, B->d_nc, zw_solve, rows_solve);
     FJ_TRY(aic_launch(aa, nullptr, s));
-    rhs_kernel<<<nblk(p.nb), 256, 0, s>>>(p.nb, cc, nullptr, nc, nullptr, c.flow, nullptr, t0, p.rhs); note_launch();
+    k_rhs<<<nblk(p.nb), 256, 0, s>>>(dC); note_launch();
     FJ_TRY(lu_factor64(p.a64, p.nb, p.piv, p.flags, s));
     FJ_TRY(lu_solve64(p.a64, p.nb, p.piv, p.rhs, p.r, s));
     FJ_CUDA(cudaMemcpyAsync(gb, p.rhs, p.nb * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    // wake circulation of the solve, and of the stored slot (broadcast over m_star rows)
-    double* gw_solve = gw;
+    // wake circulation of the solve (horseshoe: one row) and of the stored slot
     if (horseshoe) {
         static_gamma_w_kernel<<<nblk(p.sz_strip), 256, 0, s>>>(L, gb, p.hs_gw, 1); note_launch();
-        gw_solve = p.hs_gw;
     }
     static_gamma_w_kernel<<<nblk(p.sz_gw + 1), 256, 0, s>>>(L, gb, gw, -1); note_launch();
-    // forces: v at midpoints from bound + solve wake, zeta_dot = 0
+    // forces: v at midpoints from the solve wake + bound, zeta_dot = 0
     StreamBuilder sb;
     sb.init(p);
     int64_t wo = 0, go = 0;
@@ -829,126 +919,320 @@ static int run_static(const Plan& p, const fj_case_buffers* B, const double* hg,
     }
     for (int q = 0; q < L.n_surf; ++q) sb.add(p, zb + L.vo[q] * 3, gb + L.po[q], L.m[q], L.n[q]);
     FJ_TRY(pack(p, sb, 0, s));
-    force_targets_kernel<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(L, zb, p.targets); note_launch();
+    k_force_targets<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(dC); note_launch();
     FJ_TRY(vind_sum(p, p.targets, L.fo[L.n_surf], sb.len(), sb.n_links, p.v, s));
-    force_filament_kernel<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(L, zb, nullptr, gb, gw_solve, p.targets, p.v, c.flow,
-                                                                 nullptr, t0, p.ffil); note_launch();
-    vertex_forces_kernel<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(L, p.ffil, nullptr, nc, c.flow.rho, B->d_f_steady,
-                                                                B->d_f_unsteady); note_launch();
-    strip_alpha_kernel<<<nblk(p.sz_strip), 256, 0, s>>>(L, zb, B->d_f_steady, c.flow, nullptr, t0, B->d_alpha); note_launch();
+    k_force_filament<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(dC); note_launch();
+    k_vertex_forces<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(dC); note_launch();
+    k_strip_alpha<<<nblk(p.sz_strip), 256, 0, s>>>(dC); note_launch();
     FJ_CUDA(cudaMemsetAsync(B->d_gamma_b_dot, 0, p.sz_pan * sizeof(double), s));
-    if (horseshoe) {  // stored wake geometry is the regular initial wake (uvlm.py:1329-1331)
-        init_wake_kernel<<<nblk(L.wvo[L.n_surf]), 256, 0, s>>>(L, zb, c.flow, c.dt, 0.0, zw, 0); note_launch();
-    }
-    force_total_kernel<<<1, 256, 0, s>>>(L.vo[L.n_surf], B->d_f_steady, B->d_f_unsteady, B->d_force_total); note_launch();
+    k_force_total<<<1, 256, 0, s>>>(dC); note_launch();
     FJ_LAUNCH_CHECK("static solve");
     return FJ_OK;
 }
 
 // ------------------------------------------------------------------------------------
-// Dynamic step at slot i (case_solve, uvlm.py:1119-1215)
+// Dynamic steps of a batch of cases (case_solve, uvlm.py:1119-1215)
 // ------------------------------------------------------------------------------------
-__global__ void advance_time_kernel(double* t, int i, double dt) { t[i] = t[i - 1] + dt; }
+struct BatchItem {
+    Plan p;
+    const fj_case_buffers* B;
+    int i;
+    bool refactor;
+    const double* hg_n;
+    const double* hgd_n;
+    const double* hg_nm1;
+};
 
-static int run_step(const Plan& p, const fj_case_buffers* B, int i, const double* hg_n, const double* hgd_n,
-                    const double* hg_nm1, bool refactor, cudaStream_t s) {
-    const Layout& L = p.L;
-    const fj_case_config& c = p.cfg;
-    double* zb_n = B->d_zeta_b + (int64_t)i * p.sz_zb;
-    double* zbd_n = B->d_zeta_b_dot + (int64_t)i * p.sz_zb;
-    double* zw_n = B->d_zeta_w + (int64_t)i * p.sz_zw;
-    const double* zw_nm1 = B->d_zeta_w + (int64_t)(i - 1) * p.sz_zw;
-    double* cc = B->d_c + (int64_t)i * p.sz_pan * 3;
-    double* nc = B->d_nc + (int64_t)i * p.sz_pan * 3;
-    double* gb_n = B->d_gamma_b + (int64_t)i * p.sz_pan;
-    const double* gb_nm1 = B->d_gamma_b + (int64_t)(i - 1) * p.sz_pan;
-    double* gbd_n = B->d_gamma_b_dot + (int64_t)i * p.sz_pan;
-    const double* gbd_nm1 = B->d_gamma_b_dot + (int64_t)(i - 1) * p.sz_pan;
-    double* gw_n = B->d_gamma_w + (int64_t)i * p.sz_gw;
-    const double* gw_nm1 = B->d_gamma_w + (int64_t)(i - 1) * p.sz_gw;
-    double* t_n = B->d_t + i;
-    const bool mixed = c.precision == FJ_PREC_MIXED;
-
-    // 1. geometry, and t_n = t_{n-1} + dt on the device (case_solve, uvlm.py:1158-1161)
-    advance_time_kernel<<<1, 1, 0, s>>>(B->d_t, i, c.dt); note_launch();
-    geom_vertices_kernel<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(L, B->d_zeta_b0, B->d_dof_mapping, hg_n, hgd_n, hg_nm1,
-                                                                zb_n, zbd_n, p.zeta_nm1, nullptr, 0.0, 0.0); note_launch();
-    geom_panels_kernel<<<nblk(L.po[L.n_surf]), 256, 0, s>>>(L, zb_n, zbd_n, cc, nc, p.c_dot); note_launch();
-    FJ_LAUNCH_CHECK("geometry");
-
-    // 2. wake: free-wake velocities from bound(n-1) + wake(n-1), then shed + convect
-    const double* vw = nullptr;
-    if (c.free_wake && L.wto[L.n_surf] > 0) {
-        StreamBuilder sb;
-        sb.init(p);
-        for (int q = 0; q < L.n_surf; ++q) sb.add(p, p.zeta_nm1 + L.vo[q] * 3, gb_nm1 + L.po[q], L.m[q], L.n[q]);
-        for (int q = 0; q < L.n_surf; ++q) sb.add(p, zw_nm1 + L.wvo[q] * 3, gw_nm1 + L.wpo[q], L.ms[q], L.n[q]);
-        FJ_TRY(pack(p, sb, 0, s));
-        gather_wake_targets_kernel<<<nblk(L.wto[L.n_surf]), 256, 0, s>>>(L, zw_nm1, p.targets); note_launch();
-        FJ_TRY(vind_sum(p, p.targets, L.wto[L.n_surf], sb.len(), sb.n_links, p.v, s));
-        vw = p.v;
+// Target CTAs for a batched sum; each job gets a share proportional to its pairs.
+static void assign_splits(std::vector<VindJob>& jobs, int precision) {
+    if (jobs.size() == 1) {
+        jobs[0].n_split = choose_split(jobs[0].n_targets, jobs[0].n_elem, precision);
+        return;
     }
-    wake_shed_kernel<<<nblk(L.wvo[L.n_surf] + L.wpo[L.n_surf]), 256, 0, s>>>(L, zb_n, zw_nm1, gb_nm1, gw_nm1, vw, c.flow,
-                                                                             t_n, c.dt, zw_n, gw_n); note_launch();
-    FJ_LAUNCH_CHECK("wake_shed_kernel");
-
-    // 3. AIC (dynamic: bound only)
-    AicArgs aa;
-    fill_aic_args(p, aa, zb_n, cc, nc, nullptr, -1);
-    const int* run_flag = nullptr;
-    if (mixed && !refactor) {
-        // re-assemble only if the bound lattice differs from the one of the cached AIC
-        FJ_CUDA(cudaMemsetAsync(p.flags + 1, 0, sizeof(int), s));
-        changed_kernel<<<nblk(p.sz_zb), 256, 0, s>>>(zb_n, p.zeta_ref, p.sz_zb, p.flags + 1); note_launch();
-        run_flag = p.flags + 1;
+    double total = 0.0;
+    for (const VindJob& j : jobs) total += (double)j.n_targets * (double)j.n_links;
+    const double target_ctas = 4.0 * 148 * 6;
+    for (VindJob& j : jobs) {
+        const int64_t cx = vind_ctas(j.n_targets, 1, precision);
+        const double share = total > 0 ? target_ctas * ((double)j.n_targets * (double)j.n_links) / total : 1.0;
+        int64_t sp = (int64_t)(share / std::max<int64_t>(cx, 1) + 0.5);
+        sp = std::max<int64_t>(1, std::min<int64_t>(sp, split_bound(j.n_targets, j.n_elem, precision)));
+        j.n_split = (int)sp;
     }
-    FJ_TRY(aic_launch(aa, run_flag, s));
+}
 
-    // 4. RHS with the wake of step n: stream = [wake_n (+ images)] ++ [bound_n (+ images)]
-    StreamBuilder sw;
-    sw.init(p);
-    for (int q = 0; q < L.n_surf; ++q) sw.add(p, zw_n + L.wvo[q] * 3, gw_n + L.wpo[q], L.ms[q], L.n[q]);
-    const int64_t n_wake_elem = sw.len();
-    FJ_TRY(pack(p, sw, 0, s));
-    FJ_TRY(vind_sum(p, cc, p.nb, n_wake_elem, sw.n_links, p.v, s));
-    rhs_kernel<<<nblk(p.nb), 256, 0, s>>>(p.nb, cc, p.c_dot, nc, p.v, c.flow, t_n, 0.0, p.rhs); note_launch();
-    FJ_LAUNCH_CHECK("rhs_kernel");
+static int launch_sum(const std::vector<VindJob>& jobs, const std::vector<int64_t>& cta0, char* d_jobs, char* d_cta0,
+                      int precision, int kernel, double r_cut, cudaStream_t s) {
+    if (jobs.empty()) return FJ_OK;
+    double pairs = 0.0;
+    int64_t max_t = 0;
+    for (const VindJob& j : jobs) {
+        pairs += (double)j.n_targets * (double)j.n_links;
+        max_t = std::max(max_t, j.n_targets);
+    }
+    FJ_TRY(vind_launch_jobs((const VindJob*)d_jobs, (const int64_t*)d_cta0, (int)jobs.size(), cta0.back(), pairs,
+                            precision, kernel, r_cut, s));
+    return reduce_jobs((const VindJob*)d_jobs, (int)jobs.size(), max_t, s);
+}
 
+static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_bytes, cudaStream_t s) {
+    const int K = (int)items.size();
+    if (K == 0) return FJ_OK;
+    const int precision = items[0].p.cfg.precision;
+    const int kernel = items[0].p.cfg.kernel;
+    const double r_cut = items[0].p.cfg.r_cut;
+    for (const BatchItem& it : items)
+        if (it.p.cfg.precision != precision || it.p.cfg.kernel != kernel || it.p.cfg.r_cut != r_cut)
+            return fail(FJ_ERR_UNSUPPORTED, "a batch must share precision, kernel and cutoff radius");
+    const TableLayout tl = table_layout(K);
+    if (tl.total > tab_bytes) return fail(FJ_ERR_NOMEM, "batch table needs %zu bytes, %zu given", tl.total, tab_bytes);
+
+    std::vector<char> h(tl.total, 0);
+    StepCase* hC = (StepCase*)(h.data() + tl.step);
+    std::vector<VindJob> jf, jr, jfo;
+    std::vector<PackJob> pf(K), pw(K), pb(K);
+    std::vector<AicArgs> aic(K);
+    std::vector<RefineJob> ref;
+    std::vector<int> free_idx;
+    int64_t max_v = 0, max_p = 0, max_w = 0, max_wt = 0, max_f = 0, max_e_free = 0, max_e_wake = 0, max_e_bound = 0;
+    int max_n = 0, max_fil = 0, any_mirror = 0, any_free = 0, any_changed = 0;
+    for (int k = 0; k < K; ++k) {
+        BatchItem& it = items[k];
+        const Plan& p = it.p;
+        const Layout& L = p.L;
+        const fj_case_config& c = p.cfg;
+        const fj_case_buffers* B = it.B;
+        const int i = it.i;
+        const bool mixed = c.precision == FJ_PREC_MIXED;
+        StepCase& C = hC[k];
+        C.L = L;
+        C.nb = p.nb;
+        C.i = i;
+        C.free_wake = c.free_wake && L.wto[L.n_surf] > 0;
+        C.dt = c.dt;
+        C.relax = c.gamma_dot_relaxation;
+        C.flow = c.flow;
+        C.zeta0 = B->d_zeta_b0;
+        C.dof = B->d_dof_mapping;
+        C.hg_n = it.hg_n;
+        C.hgd_n = it.hgd_n;
+        C.hg_nm1 = it.hg_nm1;
+        C.t = B->d_t;
+        C.advance_time = 1;
+        C.zb_n = B->d_zeta_b + (int64_t)i * p.sz_zb;
+        C.zbd_n = B->d_zeta_b_dot + (int64_t)i * p.sz_zb;
+        C.zw_n = B->d_zeta_w + (int64_t)i * p.sz_zw;
+        C.zw_nm1 = B->d_zeta_w + (int64_t)(i - 1) * p.sz_zw;
+        C.c = B->d_c + (int64_t)i * p.sz_pan * 3;
+        C.nc = B->d_nc + (int64_t)i * p.sz_pan * 3;
+        C.gb_n = B->d_gamma_b + (int64_t)i * p.sz_pan;
+        C.gb_nm1 = B->d_gamma_b + (int64_t)(i - 1) * p.sz_pan;
+        C.gbd_n = B->d_gamma_b_dot + (int64_t)i * p.sz_pan;
+        C.gbd_nm1 = B->d_gamma_b_dot + (int64_t)(i - 1) * p.sz_pan;
+        C.gw_n = B->d_gamma_w + (int64_t)i * p.sz_gw;
+        C.gw_nm1 = B->d_gamma_w + (int64_t)(i - 1) * p.sz_gw;
+        C.gw_force = C.gw_n;
+        C.fs = B->d_f_steady + (int64_t)i * p.sz_zb;
+        C.fu = B->d_f_unsteady + (int64_t)i * p.sz_zb;
+        C.alpha = B->d_alpha + (int64_t)i * p.sz_strip;
+        C.ft = B->d_force_total + (int64_t)i * 3;
+        C.zb_nm1 = p.zeta_nm1;
+        C.c_dot = p.c_dot;
+        C.targets = p.targets;
+        C.v = p.v;
+        C.ffil = p.ffil;
+        C.rhs = p.rhs;
+        C.v_wake = C.free_wake ? p.v : nullptr;
+        C.v_rhs = p.v;
+        C.zeta_ref = (mixed && !it.refactor) ? p.zeta_ref : nullptr;
+        C.changed = (mixed && !it.refactor) ? p.flags + 1 : nullptr;
+        any_changed |= C.changed != nullptr;
+        max_v = std::max(max_v, L.vo[L.n_surf]);
+        max_p = std::max(max_p, L.po[L.n_surf]);
+        max_w = std::max(max_w, L.wvo[L.n_surf] + L.wpo[L.n_surf]);
+        max_wt = std::max(max_wt, L.wto[L.n_surf]);
+        max_f = std::max(max_f, L.fo[L.n_surf]);
+        max_n = std::max(max_n, p.nb);
+        any_mirror |= c.mirror;
+
+        // free-wake sum: bound(n-1) + wake(n-1) at the wake vertices of n-1
+        if (C.free_wake) {
+            any_free = 1;
+            StreamBuilder sb;
+            sb.init(p);
+            for (int q = 0; q < L.n_surf; ++q)
+                sb.add(p, p.zeta_nm1 + L.vo[q] * 3, C.gb_nm1 + L.po[q], L.m[q], L.n[q]);
+            for (int q = 0; q < L.n_surf; ++q)
+                sb.add(p, C.zw_nm1 + L.wvo[q] * 3, C.gw_nm1 + L.wpo[q], L.ms[q], L.n[q]);
+            pf[k].a = sb.a;
+            pf[k].out = stream_at(p, 0);
+            max_e_free = std::max(max_e_free, sb.len());
+            VindJob j;
+            memset(&j, 0, sizeof(j));
+            j.targets = p.targets;
+            j.n_targets = L.wto[L.n_surf];
+            j.stream = p.stream;
+            j.n_elem = sb.len();
+            j.part = p.part;
+            j.n_links = sb.n_links;
+            j.out = p.v;
+            jf.push_back(j);
+        } else {
+            memset(&pf[k], 0, sizeof(PackJob));  // empty job: offset[0] = 0 packs nothing
+        }
+        // wake(n) stream, then bound(n) appended
+        StreamBuilder sw;
+        sw.init(p);
+        for (int q = 0; q < L.n_surf; ++q) sw.add(p, C.zw_n + L.wvo[q] * 3, C.gw_n + L.wpo[q], L.ms[q], L.n[q]);
+        pw[k].a = sw.a;
+        pw[k].out = stream_at(p, 0);
+        max_e_wake = std::max(max_e_wake, sw.len());
+        StreamBuilder sbd;
+        sbd.init(p);
+        for (int q = 0; q < L.n_surf; ++q) sbd.add(p, C.zb_n + L.vo[q] * 3, C.gb_n + L.po[q], L.m[q], L.n[q]);
+        pb[k].a = sbd.a;
+        pb[k].out = stream_at(p, sw.len());
+        max_e_bound = std::max(max_e_bound, sbd.len());
+        if (p.nb > 0) {
+            VindJob j;
+            memset(&j, 0, sizeof(j));
+            j.targets = C.c;
+            j.n_targets = p.nb;
+            j.stream = p.stream;
+            j.n_elem = sw.len();
+            j.part = p.part;
+            j.n_links = sw.n_links;
+            j.out = p.v;
+            if (j.n_elem > 0) jr.push_back(j);
+        }
+        {
+            VindJob j;
+            memset(&j, 0, sizeof(j));
+            j.targets = p.targets;
+            j.n_targets = L.fo[L.n_surf];
+            j.stream = p.stream;
+            j.n_elem = sw.len() + sbd.len();
+            j.part = p.part;
+            j.n_links = sw.n_links + sbd.n_links;
+            j.out = p.v;
+            jfo.push_back(j);
+        }
+        // AIC of the bound lattice (dynamic: no wake lumping)
+        fill_aic_args(p, aic[k], C.zb_n, C.c, C.nc, nullptr, -1);
+        aic[k].run_flag = C.changed;
+        max_fil = std::max(max_fil, aic[k].max_fil);
+        if (mixed) {
+            RefineJob rj;
+            rj.a = p.a64;
+            rj.xinv = p.x32;
+            rj.n = p.nb;
+            rj.b = p.rhs;
+            rj.x = C.gb_n;
+            rj.r = p.r;
+            rj.resid = p.resid + i;
+            ref.push_back(rj);
+        }
+    }
+    // RHS jobs of cases whose wake stream is empty: zero velocity
+    assign_splits(jf, precision);
+    assign_splits(jr, precision);
+    assign_splits(jfo, precision);
+    auto fill_cta = [&](const std::vector<VindJob>& jobs, size_t off) {
+        int64_t* c0 = (int64_t*)(h.data() + off);
+        c0[0] = 0;
+        for (size_t q = 0; q < jobs.size(); ++q) c0[q + 1] = c0[q] + vind_ctas(jobs[q].n_targets, jobs[q].n_split, precision);
+        return std::vector<int64_t>(c0, c0 + jobs.size() + 1);
+    };
+    const std::vector<int64_t> cf = fill_cta(jf, tl.cta_free), cr = fill_cta(jr, tl.cta_rhs),
+                               cfo = fill_cta(jfo, tl.cta_force);
+    memcpy(h.data() + tl.pack_free, pf.data(), K * sizeof(PackJob));
+    memcpy(h.data() + tl.pack_wake, pw.data(), K * sizeof(PackJob));
+    memcpy(h.data() + tl.pack_bound, pb.data(), K * sizeof(PackJob));
+    if (!jf.empty()) memcpy(h.data() + tl.job_free, jf.data(), jf.size() * sizeof(VindJob));
+    if (!jr.empty()) memcpy(h.data() + tl.job_rhs, jr.data(), jr.size() * sizeof(VindJob));
+    memcpy(h.data() + tl.job_force, jfo.data(), jfo.size() * sizeof(VindJob));
+    memcpy(h.data() + tl.aic, aic.data(), K * sizeof(AicArgs));
+    if (!ref.empty()) memcpy(h.data() + tl.refine, ref.data(), ref.size() * sizeof(RefineJob));
+    FJ_TRY(upload(d_tab, h.data(), tl.total, s));
+    const StepCase* dC = (const StepCase*)(d_tab + tl.step);
+    const dim3 b(256);
+
+    // 1. time, geometry
+    k_time<<<dim3(1, K), 32, 0, s>>>(dC); note_launch();
+    k_geom_vertices<<<dim3(nblk(max_v), K), b, 0, s>>>(dC); note_launch();
+    k_geom_panels<<<dim3(nblk(max_p), K), b, 0, s>>>(dC); note_launch();
+    // 2. free wake, shed + convect
+    if (any_free) {
+        FJ_TRY(pack_jobs((const PackJob*)(d_tab + tl.pack_free), K, max_e_free, precision, s));
+        k_gather_wake_targets<<<dim3(nblk(max_wt), K), b, 0, s>>>(dC); note_launch();
+        FJ_TRY(launch_sum(jf, cf, d_tab + tl.job_free, d_tab + tl.cta_free, precision, kernel, r_cut, s));
+    }
+    k_wake_shed<<<dim3(nblk(max_w), K), b, 0, s>>>(dC); note_launch();
+    // 3. AIC (mixed: only where the lattice changed since the factorisation)
+    if (any_changed) {
+        k_clear_changed<<<dim3(1, K), 32, 0, s>>>(dC); note_launch();
+        k_changed<<<dim3(nblk(max_v * 3), K), b, 0, s>>>(dC); note_launch();
+    }
+    FJ_TRY(aic_launch_jobs((const AicArgs*)(d_tab + tl.aic), K, max_n, max_fil, any_mirror, kernel, s));
+    // 4. RHS
+    FJ_TRY(pack_jobs((const PackJob*)(d_tab + tl.pack_wake), K, max_e_wake, precision, s));
+    for (int k = 0; k < K; ++k)  // cases without wake filaments see no wake velocity
+        if (pw[k].a.offset[pw[k].a.n_lat] == 0 && items[k].p.nb > 0)
+            FJ_CUDA(cudaMemsetAsync(items[k].p.v, 0, items[k].p.nb * 3 * sizeof(double), s));
+    FJ_TRY(launch_sum(jr, cr, d_tab + tl.job_rhs, d_tab + tl.cta_rhs, precision, kernel, r_cut, s));
+    k_rhs<<<dim3(nblk(max_n), K), b, 0, s>>>(dC); note_launch();
+    FJ_LAUNCH_CHECK("step: geometry, wake, RHS");
     // 5. solve
-    if (!mixed) {
-        FJ_TRY(lu_factor64(p.a64, p.nb, p.piv, p.flags, s));
-        FJ_TRY(lu_solve64(p.a64, p.nb, p.piv, p.rhs, p.r, s));
-        FJ_CUDA(cudaMemcpyAsync(gb_n, p.rhs, p.nb * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if (precision == FJ_PREC_FP64) {
+        for (int k = 0; k < K; ++k) {
+            const Plan& p = items[k].p;
+            FJ_TRY(lu_factor64(p.a64, p.nb, p.piv, p.flags, s));
+            FJ_TRY(lu_solve64(p.a64, p.nb, p.piv, p.rhs, p.r, s));
+            FJ_CUDA(cudaMemcpyAsync(hC[k].gb_n, p.rhs, p.nb * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        }
     } else {
-        if (refactor) {
+        for (int k = 0; k < K; ++k) {
+            if (!items[k].refactor) continue;
+            const Plan& p = items[k].p;
             FJ_TRY(convert64to32(p.a64, p.a32, (int64_t)p.nb * p.nb, s));
             FJ_TRY(lu_factor32(p.a32, p.nb, p.piv, p.flags, s));
             FJ_TRY(lu_inverse32(p.a32, p.nb, p.piv, p.x32, s));
-            FJ_CUDA(cudaMemcpyAsync(p.zeta_ref, zb_n, p.sz_zb * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            FJ_CUDA(cudaMemcpyAsync(p.zeta_ref, hC[k].zb_n, p.sz_zb * sizeof(double), cudaMemcpyDeviceToDevice, s));
         }
-        FJ_TRY(refine_solve(p.a64, p.x32, p.nb, p.rhs, gb_n, p.r, p.resid + i, 3, s));
+        FJ_TRY(refine_jobs((const RefineJob*)(d_tab + tl.refine), (int)ref.size(), max_n, 3, s));
     }
-
     // 6. forces with bound(n) + wake(n)
-    StreamBuilder sbd;
-    sbd.init(p);
-    for (int q = 0; q < L.n_surf; ++q) sbd.add(p, zb_n + L.vo[q] * 3, gb_n + L.po[q], L.m[q], L.n[q]);
-    FJ_TRY(pack(p, sbd, n_wake_elem, s));
-    force_targets_kernel<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(L, zb_n, p.targets); note_launch();
-    FJ_TRY(vind_sum(p, p.targets, L.fo[L.n_surf], n_wake_elem + sbd.len(), sw.n_links + sbd.n_links, p.v, s));
-    force_filament_kernel<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(L, zb_n, zbd_n, gb_n, gw_n, p.targets, p.v, c.flow,
-                                                                 t_n, 0.0, p.ffil); note_launch();
+    FJ_TRY(pack_jobs((const PackJob*)(d_tab + tl.pack_bound), K, max_e_bound, precision, s));
+    k_force_targets<<<dim3(nblk(max_f), K), b, 0, s>>>(dC); note_launch();
+    FJ_TRY(launch_sum(jfo, cfo, d_tab + tl.job_force, d_tab + tl.cta_force, precision, kernel, r_cut, s));
+    k_force_filament<<<dim3(nblk(max_f), K), b, 0, s>>>(dC); note_launch();
     // 7. gamma_dot, vertex forces, strip alpha, totals
-    gamma_dot_kernel<<<nblk(p.nb), 256, 0, s>>>(p.nb, gb_n, gb_nm1, gbd_nm1, c.dt, c.gamma_dot_relaxation, gbd_n); note_launch();
-    vertex_forces_kernel<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(L, p.ffil, gbd_n, nc, c.flow.rho,
-                                                                B->d_f_steady + (int64_t)i * p.sz_zb,
-                                                                B->d_f_unsteady + (int64_t)i * p.sz_zb); note_launch();
-    strip_alpha_kernel<<<nblk(p.sz_strip), 256, 0, s>>>(L, zb_n, B->d_f_steady + (int64_t)i * p.sz_zb, c.flow, t_n,
-                                                        0.0, B->d_alpha + (int64_t)i * p.sz_strip); note_launch();
-    force_total_kernel<<<1, 256, 0, s>>>(L.vo[L.n_surf], B->d_f_steady + (int64_t)i * p.sz_zb,
-                                         B->d_f_unsteady + (int64_t)i * p.sz_zb, B->d_force_total + (int64_t)i * 3); note_launch();
-    FJ_LAUNCH_CHECK("post-processing");
+    k_gamma_dot<<<dim3(nblk(max_n), K), b, 0, s>>>(dC); note_launch();
+    k_vertex_forces<<<dim3(nblk(max_v), K), b, 0, s>>>(dC); note_launch();
+    int64_t max_strip = 0;
+    for (const BatchItem& it : items) max_strip = std::max(max_strip, it.p.sz_strip);
+    k_strip_alpha<<<dim3(nblk(max_strip), K), b, 0, s>>>(dC); note_launch();
+    k_force_total<<<dim3(1, K), b, 0, s>>>(dC); note_launch();
+    FJ_LAUNCH_CHECK("step: forces");
     return FJ_OK;
+}
+
+// Collocation points and area normals of one lattice (compute_surf_c / compute_surf_nc).
+__global__ void surface_c_nc_kernel(int m, int n, const double* __restrict__ zeta, double* __restrict__ c,
+                                    double* __restrict__ nc) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (int64_t)m * n) return;
+    const int k = (int)(p / n), l = (int)(p % n);
+    const double* z00 = zeta + ((int64_t)k * (n + 1) + l) * 3;
+    const double* z01 = z00 + 3;
+    const double* z10 = z00 + (n + 1) * 3;
+    const double* z11 = z10 + 3;
+    for (int d = 0; d < 3; ++d) c[p * 3 + d] = 0.5 * (0.5 * (z00[d] + z10[d]) + 0.5 * (z01[d] + z11[d]));
+    const double d1[3] = {z11[0] - z00[0], z11[1] - z00[1], z11[2] - z00[2]};
+    const double d2[3] = {z10[0] - z01[0], z10[1] - z01[1], z10[2] - z01[2]};
+    nc[p * 3 + 0] = d1[1] * d2[2] - d1[2] * d2[1];
+    nc[p * 3 + 1] = d1[2] * d2[0] - d1[0] * d2[2];
+    nc[p * 3 + 2] = d1[0] * d2[1] - d1[1] * d2[0];
 }
 
 static int check_buffers(const fj_case_buffers* B, bool dynamic) {
@@ -969,9 +1253,15 @@ static int run_dynamic(const Plan& p, const fj_case_buffers* B, int i_first, int
     for (int attempt = 0; attempt < 2; ++attempt) {
         for (int k = i; k < i_last; ++k) {
             const bool first = (k == i) && !(attempt == 0 && (flags & FJ_REUSE_FACTORS));
-            const bool refactor = mixed && (refactor_all || first);
-            FJ_TRY(run_step(p, B, k, B->d_hg_t + (int64_t)k * hs, B->d_hg_dot_t + (int64_t)k * hs,
-                            B->d_hg_t + (int64_t)(k - 1) * hs, refactor, s));
+            std::vector<BatchItem> one(1);
+            one[0].p = p;
+            one[0].B = B;
+            one[0].i = k;
+            one[0].refactor = mixed && (refactor_all || first);
+            one[0].hg_n = B->d_hg_t + (int64_t)k * hs;
+            one[0].hgd_n = B->d_hg_dot_t + (int64_t)k * hs;
+            one[0].hg_nm1 = B->d_hg_t + (int64_t)(k - 1) * hs;
+            FJ_TRY(run_steps(one, p.tab, p.tab_bytes, s));
         }
         if (!mixed) break;
         // read the refinement residuals back once; re-run from the first failure with a
@@ -1040,6 +1330,44 @@ int fj_solve_prescribed_dynamic(const fj_case_config* cfg, const fj_case_buffers
 int fj_case_step(const fj_case_config* cfg, const fj_case_buffers* bufs, int i_ts, int flags, void* d_ws,
                  size_t ws_bytes, fj_stream_t stream) {
     return fj_solve_prescribed_dynamic(cfg, bufs, i_ts, i_ts + 1, flags, d_ws, ws_bytes, stream);
+}
+
+int fj_batch_workspace_size(int max_items, size_t* bytes) {
+    if (bytes == nullptr || max_items < 1) return fail(FJ_ERR_SHAPE, "batch workspace: max_items=%d", max_items);
+    *bytes = table_layout(max_items).total + 256;
+    return FJ_OK;
+}
+
+int fj_step_batched(const fj_batch_item* items, int n_items, void* d_batch_ws, size_t batch_ws_bytes,
+                    fj_stream_t stream) {
+    if (n_items < 0 || (n_items > 0 && items == nullptr)) return fail(FJ_ERR_SHAPE, "n_items=%d", n_items);
+    if (n_items == 0) return FJ_OK;
+    std::vector<BatchItem> v(n_items);
+    for (int k = 0; k < n_items; ++k) {
+        const fj_batch_item& it = items[k];
+        FJ_TRY(make_plan(it.cfg, it.d_ws, it.ws_bytes, v[k].p));
+        FJ_TRY(check_buffers(it.bufs, true));
+        if (it.i_ts < 1 || it.i_ts >= it.cfg->n_tstep)
+            return fail(FJ_ERR_SHAPE, "item %d: slot %d not in [1, %d)", k, it.i_ts, it.cfg->n_tstep);
+        const int64_t hs = (int64_t)it.cfg->n_nodes * 16;
+        v[k].B = it.bufs;
+        v[k].i = it.i_ts;
+        v[k].refactor = it.cfg->precision == FJ_PREC_MIXED && !(it.flags & FJ_REUSE_FACTORS);
+        v[k].hg_n = it.bufs->d_hg_t + it.i_ts * hs;
+        v[k].hgd_n = it.bufs->d_hg_dot_t + it.i_ts * hs;
+        v[k].hg_nm1 = it.bufs->d_hg_t + (it.i_ts - 1) * hs;
+    }
+    return run_steps(v, (char*)d_batch_ws, batch_ws_bytes, (cudaStream_t)stream);
+}
+
+int fj_case_residual(const fj_case_config* cfg, void* d_ws, size_t ws_bytes, int i_ts, double* h_out,
+                     fj_stream_t stream) {
+    Plan p;
+    FJ_TRY(make_plan(cfg, d_ws, ws_bytes, p));
+    if (i_ts < 0 || i_ts >= cfg->n_tstep || h_out == nullptr) return fail(FJ_ERR_SHAPE, "slot %d", i_ts);
+    FJ_CUDA(cudaMemcpyAsync(h_out, p.resid + i_ts, sizeof(double), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    FJ_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return FJ_OK;
 }
 
 int fj_biot_savart(const double* d_x, const double* d_y, int64_t n_pairs, int kernel, double r_cut, double* d_out,
@@ -1132,6 +1460,7 @@ int fj_vind(const double* d_targets, int64_t n_targets, const double* const* d_z
     j.n_elem = ne;
     j.n_split = std::min(sp, choose_split(n_targets, ne, precision));
     j.part = part;
+    j.out = d_v_out;
     j.n_links = 0;
     for (int i = 0; i < n_lattices; ++i) j.n_links += (mirror ? 2 : 1) * lattice_links(rows[i], cols[i]);
     FJ_TRY(vind_launch(j, precision, kernel, r_cut, s));
@@ -1173,14 +1502,8 @@ int fj_aic_assemble(const double* const* d_zetas_b, const int* m, const int* n, 
     double* c = a.carve<double>(nb * 3);
     double* nc = a.carve<double>(nb * 3);
     for (int s = 0; s < n_surf; ++s) {
-        fj_case_config one;
-        memset(&one, 0, sizeof(one));
-        one.n_surf = 1;
-        one.m[0] = m[s];
-        one.n[0] = n[s];
-        Layout L1 = make_layout(one);
-        geom_panels_kernel<<<nblk(L1.po[1]), 256, 0, st>>>(L1, d_zetas_b[s], nullptr, c + L.po[s] * 3,
-                                                           nc + L.po[s] * 3, nullptr); note_launch();
+        surface_c_nc_kernel<<<nblk((int64_t)m[s] * n[s]), 256, 0, st>>>(m[s], n[s], d_zetas_b[s], c + L.po[s] * 3,
+                                                                       nc + L.po[s] * 3); note_launch();
     }
     FJ_LAUNCH_CHECK("aic geometry");
     AicArgs aa;

@@ -228,6 +228,54 @@ __global__ void pack32_kernel(PackArgs a, Elem32* __restrict__ out) {
     out[e] = r;
 }
 
+__global__ void pack_jobs_kernel(const PackJob* __restrict__ jobs, int fp64) {
+    const PackJob& J = jobs[blockIdx.y];
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= J.a.offset[J.a.n_lat]) return;
+    PackedLink o;
+    pack_one(J.a, e, o);
+    if (fp64) {
+        Elem64 r;
+        r.x = o.v[0];
+        r.y = o.v[1];
+        r.z = o.v[2];
+        r.g = o.g;
+        r.r0x = o.r0[0];
+        r.r0y = o.r0[1];
+        r.r0z = o.r0[2];
+        r.q = o.q;
+        ((Elem64*)J.out)[e] = r;
+    } else {
+        Elem32 r;
+        r.xh = (float)o.v[0];
+        r.yh = (float)o.v[1];
+        r.zh = (float)o.v[2];
+        r.xl = (float)(o.v[0] - (double)r.xh);
+        r.yl = (float)(o.v[1] - (double)r.yh);
+        r.zl = (float)(o.v[2] - (double)r.zh);
+        r.g = (float)(o.g / kFourPi);
+        r.r0x = (float)o.r0[0];
+        r.r0y = (float)o.r0[1];
+        r.r0z = (float)o.r0[2];
+        if (o.q < 0.0)
+            r.q = J.a.kernel == FJ_KERNEL_EPSILON ? 1.0f : 3.0e38f;
+        else if (J.a.kernel == FJ_KERNEL_EPSILON)
+            r.q = (float)o.q;
+        else
+            r.q = (float)(J.a.r_cut * J.a.r_cut * o.q);
+        r.pad = 0.f;
+        ((Elem32*)J.out)[e] = r;
+    }
+}
+
+int pack_jobs(const PackJob* d_jobs, int n_jobs, int64_t max_elem, int precision, cudaStream_t s) {
+    if (n_jobs == 0 || max_elem == 0) return FJ_OK;
+    dim3 g((unsigned)((max_elem + 255) / 256), (unsigned)n_jobs);
+    pack_jobs_kernel<<<g, 256, 0, s>>>(d_jobs, precision == FJ_PREC_FP64); note_launch();
+    FJ_LAUNCH_CHECK("pack_jobs_kernel");
+    return FJ_OK;
+}
+
 int pack_stream64(const PackArgs& a, Elem64* out, cudaStream_t s) {
     int64_t n = a.offset[a.n_lat];
     if (n == 0) return FJ_OK;
@@ -250,12 +298,10 @@ int pack_stream32(const PackArgs& a, Elem32* out, cudaStream_t s) {
 constexpr int kBlock = 128;  // threads per CTA == staged elements per chunk
 
 template <int KER, int T>
-__global__ void __launch_bounds__(kBlock) vind64_kernel(const double* __restrict__ tgt, int64_t n_t,
-                                                        const Elem64* __restrict__ st, int64_t n_elem,
-                                                        int n_split, double* __restrict__ part,
-                                                        double rc2) {
+__device__ __forceinline__ void vind64_body(const double* __restrict__ tgt, int64_t n_t,
+                                            const Elem64* __restrict__ st, int64_t n_elem, int n_split,
+                                            double* __restrict__ part, double rc2, int64_t tile, int split) {
     __shared__ Elem64 sh[kBlock];
-    const int split = blockIdx.y;
     const int64_t per = (n_elem + n_split - 1) / n_split;
     const int64_t e0 = (int64_t)split * per;
     const int64_t e1 = min(n_elem, e0 + per);  // links [e0, e1)
@@ -265,7 +311,7 @@ __global__ void __launch_bounds__(kBlock) vind64_kernel(const double* __restrict
     int64_t ti[T];
 #pragma unroll
     for (int j = 0; j < T; ++j) {
-        ti[j] = (int64_t)blockIdx.x * kBlock * T + threadIdx.x + (int64_t)j * kBlock;
+        ti[j] = tile * kBlock * T + threadIdx.x + (int64_t)j * kBlock;
         const int64_t tc = min(ti[j], n_t - 1);
         x[j][0] = tgt[tc * 3 + 0];
         x[j][1] = tgt[tc * 3 + 1];
@@ -307,6 +353,12 @@ __global__ void __launch_bounds__(kBlock) vind64_kernel(const double* __restrict
             o[2] = acc[j][2];
         }
     }
+}
+
+template <int KER, int T>
+__global__ void __launch_bounds__(kBlock) vind64_kernel(VindJob job, double rc2) {
+    vind64_body<KER, T>(job.targets, job.n_targets, (const Elem64*)job.stream, job.n_elem, job.n_split, job.part, rc2,
+                        blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------------------------------------------------
@@ -351,11 +403,10 @@ __device__ __forceinline__ void link32(const Vtx32& a, const Vtx32& b, float g, 
 }
 
 template <int KER, int T>
-__global__ void __launch_bounds__(kBlock) vind32_kernel(const double* __restrict__ tgt, int64_t n_t,
-                                                        const Elem32* __restrict__ st, int64_t n_elem,
-                                                        int n_split, double* __restrict__ part) {
+__device__ __forceinline__ void vind32_body(const double* __restrict__ tgt, int64_t n_t,
+                                            const Elem32* __restrict__ st, int64_t n_elem, int n_split,
+                                            double* __restrict__ part, int64_t tile, int split) {
     __shared__ float4 sh[kBlock * 3];
-    const int split = blockIdx.y;
     const int64_t per = (n_elem + n_split - 1) / n_split;
     const int64_t e0 = (int64_t)split * per;
     const int64_t e1 = min(n_elem, e0 + per);
@@ -365,7 +416,7 @@ __global__ void __launch_bounds__(kBlock) vind32_kernel(const double* __restrict
     int64_t ti[T];
 #pragma unroll
     for (int j = 0; j < T; ++j) {
-        ti[j] = (int64_t)blockIdx.x * kBlock * T + threadIdx.x + (int64_t)j * kBlock;
+        ti[j] = tile * kBlock * T + threadIdx.x + (int64_t)j * kBlock;
         const int64_t tc = min(ti[j], n_t - 1);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -431,6 +482,46 @@ __global__ void __launch_bounds__(kBlock) vind32_kernel(const double* __restrict
     }
 }
 
+template <int KER, int T>
+__global__ void __launch_bounds__(kBlock) vind32_kernel(VindJob job) {
+    vind32_body<KER, T>(job.targets, job.n_targets, (const Elem32*)job.stream, job.n_elem, job.n_split, job.part,
+                        blockIdx.x, blockIdx.y);
+}
+
+// Many jobs in one launch: CTA b belongs to the job j with cta0[j] <= b < cta0[j+1];
+// within a job, CTAs are numbered tile-fastest (tile + ctas_x * split).
+__device__ __forceinline__ int find_job(const int64_t* __restrict__ cta0, int n_jobs, int64_t b) {
+    int lo = 0, hi = n_jobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (cta0[mid] <= b) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int KER, int T>
+__global__ void __launch_bounds__(kBlock) vind32_jobs_kernel(const VindJob* __restrict__ jobs,
+                                                             const int64_t* __restrict__ cta0, int n_jobs) {
+    const int j = find_job(cta0, n_jobs, blockIdx.x);
+    const VindJob job = jobs[j];
+    const int64_t local = blockIdx.x - cta0[j];
+    const int64_t ctas_x = (job.n_targets + (int64_t)kBlock * T - 1) / ((int64_t)kBlock * T);
+    vind32_body<KER, T>(job.targets, job.n_targets, (const Elem32*)job.stream, job.n_elem, job.n_split, job.part,
+                        local % ctas_x, (int)(local / ctas_x));
+}
+
+template <int KER, int T>
+__global__ void __launch_bounds__(kBlock) vind64_jobs_kernel(const VindJob* __restrict__ jobs,
+                                                             const int64_t* __restrict__ cta0, int n_jobs,
+                                                             double rc2) {
+    const int j = find_job(cta0, n_jobs, blockIdx.x);
+    const VindJob job = jobs[j];
+    const int64_t local = blockIdx.x - cta0[j];
+    const int64_t ctas_x = (job.n_targets + (int64_t)kBlock * T - 1) / ((int64_t)kBlock * T);
+    vind64_body<KER, T>(job.targets, job.n_targets, (const Elem64*)job.stream, job.n_elem, job.n_split, job.part, rc2,
+                        local % ctas_x, (int)(local / ctas_x));
+}
+
 __global__ void reduce_partials_kernel(const double* __restrict__ part, int n_split, int64_t n3,
                                        double* __restrict__ out, int accumulate, double scale) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -439,6 +530,24 @@ __global__ void reduce_partials_kernel(const double* __restrict__ part, int n_sp
     for (int k = 0; k < n_split; ++k) s += part[(int64_t)k * n3 + i];
     s *= scale;
     out[i] = accumulate ? out[i] + s : s;
+}
+
+__global__ void reduce_jobs_kernel(const VindJob* __restrict__ jobs) {
+    const VindJob& J = jobs[blockIdx.y];
+    const int64_t n3 = J.n_targets * 3;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n3) return;
+    double sacc = 0.0;
+    for (int k = 0; k < J.n_split; ++k) sacc += J.part[(int64_t)k * n3 + i];
+    J.out[i] = sacc;
+}
+
+int reduce_jobs(const VindJob* d_jobs, int n_jobs, int64_t max_targets, cudaStream_t s) {
+    if (n_jobs == 0 || max_targets == 0) return FJ_OK;
+    dim3 g((unsigned)((max_targets * 3 + 255) / 256), (unsigned)n_jobs);
+    reduce_jobs_kernel<<<g, 256, 0, s>>>(d_jobs); note_launch();
+    FJ_LAUNCH_CHECK("reduce_jobs_kernel");
+    return FJ_OK;
 }
 
 int reduce_partials(const double* part, int n_split, int64_t n_targets, double* out, int accumulate,
@@ -516,29 +625,27 @@ int vind_launch(const VindJob& job, int precision, int kernel, double r_cut, cud
     dim3 grid((unsigned)gx, (unsigned)job.n_split);
     const int prof = prof_start(s);
     if (precision == FJ_PREC_FP64) {
-        const Elem64* st = (const Elem64*)job.stream;
         const double rc2 = r_cut * r_cut;
         switch (kernel) {
             case FJ_KERNEL_EPSILON:
-                vind64_kernel<FJ_KERNEL_EPSILON, kT64><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part, rc2); note_launch();
+                vind64_kernel<FJ_KERNEL_EPSILON, kT64><<<grid, kBlock, 0, s>>>(job, rc2); note_launch();
                 break;
             case FJ_KERNEL_CUTOFF:
-                vind64_kernel<FJ_KERNEL_CUTOFF, kT64><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part, rc2); note_launch();
+                vind64_kernel<FJ_KERNEL_CUTOFF, kT64><<<grid, kBlock, 0, s>>>(job, rc2); note_launch();
                 break;
             case FJ_KERNEL_PLAIN:
-                vind64_kernel<FJ_KERNEL_PLAIN, kT64><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part, rc2); note_launch();
+                vind64_kernel<FJ_KERNEL_PLAIN, kT64><<<grid, kBlock, 0, s>>>(job, rc2); note_launch();
                 break;
             default:
                 return fail(FJ_ERR_UNSUPPORTED, "vind: unknown kernel %d", kernel);
         }
     } else {
-        const Elem32* st = (const Elem32*)job.stream;
         switch (kernel) {
             case FJ_KERNEL_EPSILON:
-                vind32_kernel<FJ_KERNEL_EPSILON, kT32><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part); note_launch();
+                vind32_kernel<FJ_KERNEL_EPSILON, kT32><<<grid, kBlock, 0, s>>>(job); note_launch();
                 break;
             case FJ_KERNEL_CUTOFF:
-                vind32_kernel<FJ_KERNEL_CUTOFF, kT32><<<grid, kBlock, 0, s>>>(job.targets, job.n_targets, st, job.n_elem, job.n_split, job.part); note_launch();
+                vind32_kernel<FJ_KERNEL_CUTOFF, kT32><<<grid, kBlock, 0, s>>>(job); note_launch();
                 break;
             default:
                 return fail(FJ_ERR_UNSUPPORTED, "vind: kernel %d has no FP32 variant (use FJ_PREC_FP64)", kernel);
@@ -546,6 +653,50 @@ int vind_launch(const VindJob& job, int precision, int kernel, double r_cut, cud
     }
     prof_stop(prof, s, (double)job.n_targets * (double)job.n_links);
     FJ_LAUNCH_CHECK("vind kernel");
+    return FJ_OK;
+}
+
+int64_t vind_ctas(int64_t n_targets, int n_split, int precision) {
+    const int T = precision == FJ_PREC_FP64 ? kT64 : kT32;
+    return (n_targets + (int64_t)kBlock * T - 1) / ((int64_t)kBlock * T) * n_split;
+}
+
+int vind_launch_jobs(const VindJob* d_jobs, const int64_t* d_cta0, int n_jobs, int64_t total_ctas, double pairs,
+                     int precision, int kernel, double r_cut, cudaStream_t s) {
+    if (n_jobs == 0 || total_ctas == 0) return FJ_OK;
+    if (total_ctas > 0x7fffffff) return fail(FJ_ERR_SHAPE, "vind jobs: grid too large");
+    query_occupancy();
+    const unsigned g = (unsigned)total_ctas;
+    const int prof = prof_start(s);
+    if (precision == FJ_PREC_FP64) {
+        const double rc2 = r_cut * r_cut;
+        switch (kernel) {
+            case FJ_KERNEL_EPSILON:
+                vind64_jobs_kernel<FJ_KERNEL_EPSILON, kT64><<<g, kBlock, 0, s>>>(d_jobs, d_cta0, n_jobs, rc2); note_launch();
+                break;
+            case FJ_KERNEL_CUTOFF:
+                vind64_jobs_kernel<FJ_KERNEL_CUTOFF, kT64><<<g, kBlock, 0, s>>>(d_jobs, d_cta0, n_jobs, rc2); note_launch();
+                break;
+            case FJ_KERNEL_PLAIN:
+                vind64_jobs_kernel<FJ_KERNEL_PLAIN, kT64><<<g, kBlock, 0, s>>>(d_jobs, d_cta0, n_jobs, rc2); note_launch();
+                break;
+            default:
+                return fail(FJ_ERR_UNSUPPORTED, "vind: unknown kernel %d", kernel);
+        }
+    } else {
+        switch (kernel) {
+            case FJ_KERNEL_EPSILON:
+                vind32_jobs_kernel<FJ_KERNEL_EPSILON, kT32><<<g, kBlock, 0, s>>>(d_jobs, d_cta0, n_jobs); note_launch();
+                break;
+            case FJ_KERNEL_CUTOFF:
+                vind32_jobs_kernel<FJ_KERNEL_CUTOFF, kT32><<<g, kBlock, 0, s>>>(d_jobs, d_cta0, n_jobs); note_launch();
+                break;
+            default:
+                return fail(FJ_ERR_UNSUPPORTED, "vind: kernel %d has no FP32 variant (use FJ_PREC_FP64)", kernel);
+        }
+    }
+    prof_stop(prof, s, pairs);
+    FJ_LAUNCH_CHECK("vind jobs kernel");
     return FJ_OK;
 }
 

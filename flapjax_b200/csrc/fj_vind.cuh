@@ -78,7 +78,24 @@ struct VindJob {
     int n_split;
     double* part;           // (n_split, n_targets, 3)
     int64_t n_links;        // filaments in the stream (for pair counting)
+    double* out;            // (n_targets, 3) result of the reduction (batched launches)
 };
+
+// A stream-packing job of a batched launch: lattices -> elements at `out`.
+struct PackJob {
+    PackArgs a;
+    void* out;
+};
+
+// Batched launches (one kernel for many jobs; tables in device memory).
+//  vind: CTAs of job j are cta0[j] .. cta0[j+1]-1 (ctas_x(j) * n_split(j) of them);
+//  all jobs of one launch share precision and kernel.
+int vind_launch_jobs(const VindJob* d_jobs, const int64_t* d_cta0, int n_jobs, int64_t total_ctas, double pairs,
+                     int precision, int kernel, double r_cut, cudaStream_t s);
+int pack_jobs(const PackJob* d_jobs, int n_jobs, int64_t max_elem, int precision, cudaStream_t s);
+int reduce_jobs(const VindJob* d_jobs, int n_jobs, int64_t max_targets, cudaStream_t s);
+// CTAs of one sum (target tiles x splits), for building cta0.
+int64_t vind_ctas(int64_t n_targets, int n_split, int precision);
 
 // filaments of an (rows, cols) lattice: rows(cols+1) chordwise + (rows+1)cols spanwise
 inline int64_t lattice_links(int rows, int cols) {

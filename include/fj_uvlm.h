@@ -173,6 +173,28 @@ FJ_API int fj_solve_prescribed_dynamic(const fj_case_config* cfg, const fj_case_
 FJ_API int fj_case_step(const fj_case_config* cfg, const fj_case_buffers* bufs, int i_ts,
                  int flags, void* d_ws, size_t ws_bytes, fj_stream_t stream);
 
+/* One time step for each of many cases in one set of kernel launches (the serving
+ * path).  Each item is a case (its config, buffers and own workspace) and the slot it
+ * solves; the step is case_solve (aero/uvlm.py:1119-1215) with the node frames of slots
+ * i_ts and i_ts-1 of the case's hg arrays.  All items must share precision, kernel and
+ * cutoff radius.  FJ_PREC_MIXED items reuse the factors cached in their workspace when
+ * flags has FJ_REUSE_FACTORS, else factorise at this step.  Does not synchronise: the
+ * refinement residual of a slot is read with fj_case_residual. */
+typedef struct fj_batch_item {
+    const fj_case_config* cfg;
+    const fj_case_buffers* bufs;
+    void* d_ws;
+    size_t ws_bytes;
+    int i_ts;
+    int flags;
+} fj_batch_item;
+FJ_API int fj_batch_workspace_size(int max_items, size_t* bytes);
+FJ_API int fj_step_batched(const fj_batch_item* items, int n_items, void* d_batch_ws,
+                           size_t batch_ws_bytes, fj_stream_t stream);
+/* Relative refinement residual of slot i_ts of a mixed-precision case (synchronises). */
+FJ_API int fj_case_residual(const fj_case_config* cfg, void* d_ws, size_t ws_bytes, int i_ts,
+                            double* h_out, fj_stream_t stream);
+
 /* Measured FP32 FMA throughput of the current device (TFLOP/s, an FMA counted as two),
  * from a register-resident FMA-chain kernel timed with CUDA events.  Synchronises. */
 FJ_API int fj_peak_fp32(double* tflops, fj_stream_t stream);
