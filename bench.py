@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--small", action="store_true", help="a reduced workload (for quick checks)")
+    ap.add_argument("--serving-cases", type=int, default=512, help="cases in the serving stream (0: skip)")
+    ap.add_argument("--only-serving", action="store_true")
     return ap.parse_args()
 
 
@@ -246,6 +248,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if args.only_serving:
+        print(json.dumps({"serving": serving_bench(args, torch)}))
+        return 0
     assert args.warmup >= 3, "at least 3 warm-up steps"
     K, W = args.steps, args.warmup
     n_slots = 1 + W + K
@@ -337,6 +342,7 @@ def main():
         e2e = {"value": world * K / (te * 1e-3), "unit": UNIT, "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo}
         del dce
 
+    serving = serving_bench(args, torch) if args.serving_cases > 0 else None
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -354,10 +360,41 @@ def main():
                    "l2": "flushed between steps (256 MB write outside the timed events)",
                    "parallelism": f"independent case replica per GPU x{world}", "seed": case.seed},
         "e2e": e2e, "fp64_gpu": fp64, "roofline": roof, "cpu_baseline": cpu,
-        "gpu_launches": int(launches), "clocks": clk.summary(),
+        "gpu_launches": int(launches), "clocks": clk.summary(), "serving": serving,
     }
     print(json.dumps(line))
     return 0
+
+
+def serving_bench(args, torch):
+    """Config 5: Poisson arrivals (200/s) of heaving wings with M ~ U{4..16},
+    N ~ U{16..128}, W ~ U{20..200}, AoA ~ U[0, 8] deg, 100 steps each, mixed precision,
+    continuously batched.  Reports whole-stream throughput and per-step latency."""
+    import flapjax_b200 as fj
+    from flapjax_b200 import cases
+    from flapjax_b200.serving import Request, ServingLoop
+
+    n = args.serving_cases
+    stream, arrivals = cases.serving_stream(n_cases=n, rate=200.0, n_steps=100, seed=0)
+
+    def requests():
+        out = []
+        for k, (c, t) in enumerate(zip(stream, arrivals)):
+            uv = fj.UVLM([fj.GridDiscretisation(c.m, c.n, c.m_star)], np.arange(c.n + 1), precision="mixed")
+            uv.set_design_variables(dt=c.dt, flowfield=fj.Constant(c.u_inf, c.rho, True), zeta_b0=c.zeta_b0, hg0=c.hg0)
+            out.append(Request(uv, c.hg_t, c.hg_dot_t, arrival=float(t), tag=k))
+        return out
+
+    free = torch.cuda.mem_get_info()[0]
+    loop = ServingLoop(memory_budget=int(0.5 * free), max_active=512, keep_results=False)
+    loop.run(requests()[:8], realtime=False)  # warm-up (module load, allocator)
+    torch.cuda.synchronize()
+    res = loop.run(requests(), realtime=True)
+    summ = res.summary()
+    summ.update({"cases": n, "arrival_rate_per_s": 200.0, "steps_per_case": 100,
+                 "workload": "heaving wings, M~U{4..16}, N~U{16..128}, W~U{20..200}, AoA~U[0,8] deg, mixed precision",
+                 "pairs_total": float(sum(c.pairs_per_step() * c.n_steps for c in stream))})
+    return summ
 
 
 def ctypes_peak(torch):

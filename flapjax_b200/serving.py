@@ -129,7 +129,8 @@ class ServingLoop:
     (seconds after ``run`` starts); otherwise all are queued at once.
     """
 
-    def __init__(self, memory_budget: int, max_active: int = 256, device=None, keep_results=True):
+    def __init__(self, memory_budget: int, max_active: int = 256, device=None, keep_results=True,
+                 admit_per_iteration: int = 4):
         import torch
 
         from .runtime import device_of
@@ -140,15 +141,27 @@ class ServingLoop:
         self.max_active = max_active
         self.stepper = BatchStepper(max_active, self.dev)
         self.keep_results = keep_results
+        self.admit_per_iteration = admit_per_iteration
 
     def _admit(self, req: Request, now: float) -> _Active:
+        """Static solve and the first (factorising) step run for the case alone, so the
+        batched steps it joins reuse its cached factors and stay uniform."""
         uv = req.uvlm
         n_tstep = req.hg_t.shape[0]
         init = uv.solve_static()
         dc = uv.make_device_case(n_tstep, req.hg_t.shape[1])
         uv.load_initial(dc, init)
         dc.set_hg(req.hg_t, req.hg_dot_t)
-        return _Active(req, dc, 1, n_tstep, case_footprint_bytes(uv, n_tstep), now)
+        first = 1
+        if n_tstep > 1:
+            dc.solve_dynamic(1, 2)
+            first = 2
+        return _Active(req, dc, first, n_tstep, case_footprint_bytes(uv, n_tstep), now)
+
+    def _retire(self, a: _Active, results: dict):
+        if self.keep_results:
+            results[a.req.tag if a.req.tag is not None else id(a.req)] = a.req.uvlm._to_case(a.dc)
+        a.dc = None
 
     def run(self, requests: list[Request], realtime: bool = True) -> ServeResult:
         torch = self.torch
@@ -165,15 +178,26 @@ class ServingLoop:
         while pending or active:
             now = time.perf_counter() - t0
             # admission: arrived requests, while the footprint budget and batch width allow
-            while pending and (not realtime or pending[0].arrival <= now) and len(active) < self.max_active:
+            # (a few per iteration, so a burst of arrivals does not stall running cases)
+            admitted = 0
+            while (pending and (not realtime or pending[0].arrival <= now) and len(active) < self.max_active
+                   and (admitted < self.admit_per_iteration or not active)):
                 est = case_footprint_bytes(pending[0].uvlm, pending[0].hg_t.shape[0])
                 if active and used + est > self.memory_budget:
                     break
                 req = pending.pop(0)
                 a = self._admit(req, now)
                 used += a.footprint
-                active.append(a)
-                admit_lat.append(max(0.0, now - req.arrival) if realtime else 0.0)
+                admitted += 1
+                if a.next_slot > 1:
+                    steps += 1
+                if a.next_slot >= a.n_tstep:
+                    self._retire(a, results)
+                    used -= a.footprint
+                else:
+                    active.append(a)
+                done_at = time.perf_counter() - t0
+                admit_lat.append(max(0.0, done_at - req.arrival) if realtime else 0.0)
             if not active:
                 if pending and realtime:
                     time.sleep(max(0.0, min(pending[0].arrival - now, 0.002)))
@@ -195,10 +219,8 @@ class ServingLoop:
                 steps += 1
             done = [a for a in active if a.next_slot >= a.n_tstep]
             for a in done:
-                if self.keep_results:
-                    results[a.req.tag if a.req.tag is not None else id(a.req)] = a.req.uvlm._to_case(a.dc)
+                self._retire(a, results)
                 active.remove(a)
                 used -= a.footprint
-                del a.dc
         wall = time.perf_counter() - t0
         return ServeResult(results, np.asarray(lat), steps, wall, busy_s, np.asarray(admit_lat), max_act)
