@@ -148,6 +148,12 @@ _SIGS = {
     "fj_vind_noalloc": (C.c_int, [_P, C.c_int64, C.POINTER(_P), C.POINTER(_P), C.POINTER(C.c_int),
                                   C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int,
                                   C.c_double, C.c_int, _P, _P]),
+    "fj_vind_vjp_workspace_size": (C.c_int, [C.c_int64, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.c_int,
+                                             C.POINTER(C.c_size_t)]),
+    "fj_vind_vjp": (C.c_int, [_P, C.c_int64, C.POINTER(_P), C.POINTER(_P), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                              C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, C.c_double, _P, _P,
+                              C.POINTER(_P), C.POINTER(_P), _P, C.c_size_t, _P]),
+    "fj_lu_solve_t": (C.c_int, [_P, C.c_int, _P, _P, _P, C.c_size_t, _P]),
     "fj_aic_workspace_size": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_size_t)]),
     "fj_aic_assemble": (C.c_int, [C.POINTER(_P), C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.POINTER(_P),
                                   C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int,

@@ -219,6 +219,20 @@ FJ_API int fj_vind(const double* d_targets, int64_t n_targets, const double* con
             const double* mirror_point, const double* mirror_normal, int kernel, double r_cut,
             int precision, double* d_v_out, void* d_ws, size_t ws_bytes, fj_stream_t stream);
 
+/* Adjoint of compute_v_ind (the reference differentiates it with jax.vjp): given the
+ * cotangent d_lam (n_targets, 3) of the velocities, ACCUMULATES (+=) into d_targets_bar
+ * (n_targets, 3), d_zetas_bar[i] (vertex adjoints of lattice i) and d_gammas_bar[i]
+ * (ring-circulation adjoints); any of the three may be NULL to skip it.  FP64, epsilon
+ * kernel only. */
+FJ_API int fj_vind_vjp_workspace_size(int64_t n_targets, const int* rows, const int* cols,
+                                      int n_lattices, int mirror, size_t* bytes);
+FJ_API int fj_vind_vjp(const double* d_targets, int64_t n_targets, const double* const* d_zetas,
+                       const double* const* d_gammas, const int* rows, const int* cols,
+                       int n_lattices, const double* mirror_point, const double* mirror_normal,
+                       int kernel, double r_cut, const double* d_lam, double* d_targets_bar,
+                       double* const* d_zetas_bar, double* const* d_gammas_bar, void* d_ws,
+                       size_t ws_bytes, fj_stream_t stream);
+
 /* fj_vind without a caller workspace, for callers that cannot allocate device memory
  * (a plugin host that owns the device memory pool, a real-time loop that may not block in
  * cudaMalloc).  No counterpart in the reference.  Its scratch is a fixed 8 MiB array in
@@ -251,6 +265,11 @@ FJ_API int fj_lu_factor(double* d_a, int n, int32_t* d_piv, void* d_ws, size_t w
                  fj_stream_t stream);
 FJ_API int fj_lu_solve(const double* d_lu, int n, const int32_t* d_piv, double* d_b, void* d_ws,
                 size_t ws_bytes, fj_stream_t stream);
+
+/* Transpose solve A^T x = b with the factors of fj_lu_factor (the adjoint of the solve at
+ * aero/uvlm.py:985); workspace as fj_lu_workspace_size. */
+FJ_API int fj_lu_solve_t(const double* d_lu, int n, const int32_t* d_piv, double* d_b, void* d_ws,
+                         size_t ws_bytes, fj_stream_t stream);
 
 /* Mixed-precision solve of A x = b: FP32 factors of A (recomputed when refactor != 0)
  * kept in the workspace, then FP64 iterative refinement x += M (b - A x) with the FP64

@@ -36,6 +36,48 @@ KERNEL_PLAIN = "plain"
 
 _PAIR_BUDGET = 1 << 21  # (target, segment) pairs evaluated per NumPy chunk
 
+# Floating type of every array the oracle creates.  float64 (the reference's type)
+# unless a test switches to np.longdouble through ``real_type`` to take finite
+# differences of the forward below the float64 roundoff floor.
+REAL = np.float64
+
+
+class real_type:
+    """Context manager: run the oracle in another floating type (np.longdouble)."""
+
+    def __init__(self, dtype):
+        self.dtype = dtype
+
+    def __enter__(self):
+        global REAL
+        self._old, REAL = REAL, self.dtype
+        return self
+
+    def __exit__(self, *exc):
+        global REAL
+        REAL = self._old
+
+
+def _solve(a, b):
+    """Dense solve: LAPACK getrf/getrs in float64; Gaussian elimination with partial
+    pivoting (row by row, in the array's own type) for extended precision."""
+    if a.dtype == np.float64 and b.dtype == np.float64:
+        return scipy.linalg.lu_solve(scipy.linalg.lu_factor(a), b)
+    a = a.astype(REAL).copy()
+    x = b.astype(REAL).copy()
+    n = a.shape[0]
+    for k in range(n):
+        p = k + int(np.argmax(np.abs(a[k:, k])))
+        if p != k:
+            a[[k, p]] = a[[p, k]]
+            x[[k, p]] = x[[p, k]]
+        f = a[k + 1:, k] / a[k, k]
+        a[k + 1:, k:] -= f[:, None] * a[k, k:]
+        x[k + 1:] -= f * x[k]
+    for k in range(n - 1, -1, -1):
+        x[k] = (x[k] - a[k, k + 1:] @ x[k + 1:]) / a[k, k]
+    return x
+
 
 # ----------------------------------------------------------------------------------
 # Biot-Savart segment kernels, aero/utils.py:580-648.  Vectorised: x (..., 3),
@@ -134,7 +176,7 @@ def split_to_vertex(arr, axes):
     for ax in (axes,) if isinstance(axes, int) else axes:
         shape = list(arr.shape)
         shape[ax] += 1
-        out = np.zeros(shape)
+        out = np.zeros(shape, REAL)
         i1 = [slice(None)] * len(shape)
         i2 = [slice(None)] * len(shape)
         i1[ax] = slice(None, -1)
@@ -221,14 +263,14 @@ def compute_aic_grid(c, n, zeta, kernel, r_cut=R_CUTOFF):
     c_m, c_n = c.shape[:2]
     m_p, n_p = zeta.shape[0] - 1, zeta.shape[1] - 1
     if not c_m or not c_n or not m_p or not n_p:
-        return np.zeros((c_m, c_n, m_p, n_p))
+        return np.zeros((c_m, c_n, m_p, n_p), REAL)
     cf = c.reshape(-1, 3)
     nf = n.reshape(-1, 3)
-    out = np.zeros((cf.shape[0], m_p, n_p))
+    out = np.zeros((cf.shape[0], m_p, n_p), REAL)
     m_segs = chordwise_segments(zeta).reshape(-1, 2, 3)
     n_segs = spanwise_segments(zeta).reshape(-1, 2, 3)
-    m_inf = np.zeros((cf.shape[0], m_segs.shape[0]))
-    n_inf = np.zeros((cf.shape[0], n_segs.shape[0]))
+    m_inf = np.zeros((cf.shape[0], m_segs.shape[0]), REAL)
+    n_inf = np.zeros((cf.shape[0], n_segs.shape[0]), REAL)
 
     def red_m(k, t0, t1):
         m_inf[t0:t1] = np.einsum("tsk,tk->ts", k, nf[t0:t1])
@@ -414,10 +456,10 @@ def calculate_steady_forcing(zeta_b, zeta_dot_b, gamma_b, gamma_w, rho, v_func):
         mpd_s = neighbour_average(zd, 1)
         v_rel_c = v_func(mp_c) - mpd_c
         v_rel_s = v_func(mp_s) - mpd_s
-        g_c = np.zeros(v_rel_c.shape[:-1])
+        g_c = np.zeros(v_rel_c.shape[:-1], REAL)
         g_c[:, :-1] = gb
         g_c[:, 1:] += -gb
-        g_s = np.zeros(v_rel_s.shape[:-1])
+        g_s = np.zeros(v_rel_s.shape[:-1], REAL)
         g_s[:-1, :] = -gb
         g_s[1:, :] += gb
         if gw.shape[0] > 0:
@@ -518,7 +560,7 @@ class UVLMRef:
     def set_design_variables(self, dt, flowfield, zeta_b0, hg0, delta_w=None):
         if isinstance(zeta_b0, np.ndarray):
             zeta_b0 = [zeta_b0]
-        self.zeta_b0 = [np.asarray(z, float) for z in zeta_b0]
+        self.zeta_b0 = [np.asarray(z, REAL) for z in zeta_b0]
         self.hg_ref = np.asarray(hg0, float)
         self.zeta_b_ref = self.hg_to_zeta_b(self.hg_ref)
         self.flowfield = flowfield
@@ -605,7 +647,7 @@ class UVLMRef:
             v_bc = [v - cd for v, cd in zip(v_bc, c_dot_n)]
             v_bc = [v + self.v_ind(c, zeta_w_n, gamma_w_n) for v, c in zip(v_bc, c_n)]
         rhs = np.concatenate([np.einsum("ijk,ijk->ij", v, n).ravel() for v, n in zip(v_bc, nc_n)])
-        gamma_vec = scipy.linalg.lu_solve(scipy.linalg.lu_factor(aic), -rhs)
+        gamma_vec = _solve(aic, -rhs)
         gamma_b_n, off = [], 0
         for gd in self.grid_disc:
             gamma_b_n.append(gamma_vec[off:off + gd.m * gd.n].reshape(gd.m, gd.n))
@@ -637,18 +679,18 @@ class UVLMRef:
         """``initialise_case_object`` uvlm.py:1217-1284 (zero-filled)."""
         gds = self.grid_disc
         return Case(
-            zeta_b=[np.zeros((n_tstep, g.m + 1, g.n + 1, 3)) for g in gds],
-            zeta_b_dot=[np.zeros((n_tstep, g.m + 1, g.n + 1, 3)) for g in gds],
-            zeta_w=[np.zeros((n_tstep, g.m_star + 1, g.n + 1, 3)) for g in gds],
-            c=[np.zeros((n_tstep, g.m, g.n, 3)) for g in gds],
-            nc=[np.zeros((n_tstep, g.m, g.n, 3)) for g in gds],
-            gamma_b=[np.zeros((n_tstep, g.m, g.n)) for g in gds],
-            gamma_b_dot=[np.zeros((n_tstep, g.m, g.n)) for g in gds],
-            gamma_w=[np.zeros((n_tstep, g.m_star, g.n)) for g in gds],
-            f_steady=[np.zeros((n_tstep, g.m + 1, g.n + 1, 3)) for g in gds],
-            f_unsteady=[np.zeros((n_tstep, g.m + 1, g.n + 1, 3)) for g in gds],
-            alpha=[np.zeros((n_tstep, g.n)) for g in gds],
-            t=np.zeros(n_tstep),
+            zeta_b=[np.zeros((n_tstep, g.m + 1, g.n + 1, 3), REAL) for g in gds],
+            zeta_b_dot=[np.zeros((n_tstep, g.m + 1, g.n + 1, 3), REAL) for g in gds],
+            zeta_w=[np.zeros((n_tstep, g.m_star + 1, g.n + 1, 3), REAL) for g in gds],
+            c=[np.zeros((n_tstep, g.m, g.n, 3), REAL) for g in gds],
+            nc=[np.zeros((n_tstep, g.m, g.n, 3), REAL) for g in gds],
+            gamma_b=[np.zeros((n_tstep, g.m, g.n), REAL) for g in gds],
+            gamma_b_dot=[np.zeros((n_tstep, g.m, g.n), REAL) for g in gds],
+            gamma_w=[np.zeros((n_tstep, g.m_star, g.n), REAL) for g in gds],
+            f_steady=[np.zeros((n_tstep, g.m + 1, g.n + 1, 3), REAL) for g in gds],
+            f_unsteady=[np.zeros((n_tstep, g.m + 1, g.n + 1, 3), REAL) for g in gds],
+            alpha=[np.zeros((n_tstep, g.n), REAL) for g in gds],
+            t=np.zeros(n_tstep, REAL),
         )
 
     @staticmethod

@@ -1,0 +1,85 @@
+"""The adjoint's algebra on the CPU: the Biot-Savart VJP, the reverse sweep of
+``PrescribedAdjoint`` (run over oracle stand-ins for the device calls) and the twist
+Jacobian, each against central finite differences (h = 1e-6).
+
+The sweep is checked against differences of the oracle forward evaluated in 80-bit
+extended precision: agreement 1e-6 relative.  (In float64 the forward's own roundoff
+noise, ~1e-11 relative, limits a central difference at h = 1e-6 to ~1e-4.)"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from flapjax_b200 import cases
+from flapjax_b200.adjoint import twist_jacobian
+from oracle import uvlm_ref as R
+from oracle.uvlm_vjp import bs_epsilon_vjp
+from tests.adjoint_oracle import OracleAdjoint, central_difference, coefficient_weights, forward_objective
+from tests.helpers import oracle_uvlm
+
+
+def test_bs_epsilon_vjp_finite_differences():
+    rng = np.random.default_rng(0)
+    x = rng.normal(size=(64, 3))
+    y0 = rng.normal(size=(64, 3))
+    y1 = y0 + rng.normal(size=(64, 3))
+    lam = rng.normal(size=(64, 3))
+    xb, y0b, y1b = bs_epsilon_vjp(x, y0, y1, lam)
+    h = 1e-6
+    for arg, bar in ((0, xb), (1, y0b), (2, y1b)):
+        for k in range(3):
+            args_p = [x.copy(), y0.copy(), y1.copy()]
+            args_m = [x.copy(), y0.copy(), y1.copy()]
+            args_p[arg][:, k] += h
+            args_m[arg][:, k] -= h
+            fd = np.sum(lam * (R.bs_epsilon(*args_p) - R.bs_epsilon(*args_m)), axis=-1) / (2 * h)
+            assert np.max(np.abs(fd - bar[:, k])) <= 1e-7 * max(1.0, np.max(np.abs(bar[:, k])))
+
+
+def test_extended_precision_forward_matches_float64():
+    c = cases.wing_pitch(m=3, n=4, m_star=4, n_steps=3, n_ctrl=3, seed=3)
+    fw = coefficient_weights(c, "CL")
+    j64 = forward_objective(c, c.zeta_b0, fw)
+    with R.real_type(np.longdouble):
+        jld = forward_objective(c, np.asarray(c.zeta_b0, np.longdouble), fw)
+    assert jld.dtype == np.longdouble
+    assert abs(float(jld) - j64) < 1e-12 * abs(j64)
+
+
+@pytest.mark.parametrize("which", ["CL", "CD"])
+def test_reverse_sweep_matches_finite_differences(which):
+    c = cases.wing_pitch(m=3, n=4, m_star=4, n_steps=5, n_ctrl=3, seed=3)
+    fw = coefficient_weights(c, which)
+    uv, _ = oracle_uvlm(c)
+    J, g = OracleAdjoint(uv).gradient(c.hg_t, c.hg_dot_t, fw, checkpoint=2)
+    assert abs(J - forward_objective(c, c.zeta_b0, fw)) < 1e-13 * max(1.0, abs(J))
+    rng = np.random.default_rng(1)
+    for _ in range(2):
+        d = rng.normal(size=c.zeta_b0.shape) * 0.1
+        fd = central_difference(c, d, fw)
+        assert abs(fd - np.sum(g * d)) <= 1e-6 * abs(fd), (fd, np.sum(g * d))
+
+
+def test_checkpoint_interval_does_not_change_the_gradient():
+    c = cases.wing_heave(m=3, n=4, m_star=3, n_steps=6)
+    fw = coefficient_weights(c, "CL")
+    uv, _ = oracle_uvlm(c)
+    g = [OracleAdjoint(uv).gradient(c.hg_t, c.hg_dot_t, fw, checkpoint=k)[1] for k in (1, 4, 100)]
+    assert np.max(np.abs(g[0] - g[1])) < 1e-13 * np.max(np.abs(g[2]))
+    assert np.max(np.abs(g[0] - g[2])) < 1e-13 * np.max(np.abs(g[2]))
+
+
+def test_twist_jacobian_finite_differences():
+    m, n, span = 4, 8, 8.0
+    ctrl_y = np.linspace(0.0, span, 4)
+    span_y = np.linspace(0.0, span, n + 1)
+    theta = np.deg2rad(np.array([1.0, -0.5, 2.0, 0.3]))
+    jac = twist_jacobian(m, n, 1.0, 0.25, ctrl_y, span_y, np.interp(span_y, ctrl_y, theta), camber=0.03)
+    h = 1e-6
+    for k in range(len(theta)):
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += h
+        tm[k] -= h
+        fd = (cases.twisted_grid(m, n, 1.0, 0.25, np.interp(span_y, ctrl_y, tp), 0.03)
+              - cases.twisted_grid(m, n, 1.0, 0.25, np.interp(span_y, ctrl_y, tm), 0.03)) / (2 * h)
+        assert np.max(np.abs(fd - jac[k])) < 1e-9
