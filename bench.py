@@ -15,9 +15,9 @@ e2e     the same metric through the C ABI with host buffers: every step copies i
 fp64_gpu  the plain FP64 path on the same steps, and the mixed path's CL/CD error
         against it.
 
---impl reference  times the CPU FP64 oracle (the reference's arithmetic restated; the
-        reference itself is JAX, which is not installed) on a bounded sample of the same
-        workload and prints the same metric.
+--impl reference  times the FP64 oracle (the reference's arithmetic restated; the
+        reference itself is JAX, which is not installed) with its pair sums in C++/OpenMP on
+        every host thread, full time steps of the same workload, and prints the same metric.
 """
 from __future__ import annotations
 
@@ -201,13 +201,50 @@ def e2e_run(uv, dc, case, first, last, torch):
     return [a.elapsed_time(b) for a, b in ev], bytes_in, bytes_out
 
 
-def cpu_sample(case, budget_s):
-    """Time the FP64 oracle (NumPy, one thread of BLAS-free array code) on a bounded
-    sample of a step: the induced velocity at a subset of the wake vertices from the
-    bound and wake lattices.  Steps/s = (pairs/s) / (pairs per step); the dense solve's
-    share of a CPU step is below 1 % at this size and is not sampled."""
+def _cpu_uvlm(case):
+    from oracle import uvlm_cpp as CP
     from oracle import uvlm_ref as R
 
+    uv = CP.UVLMCpp([(case.m, case.n, case.m_star)], np.arange(case.n + 1), kernel=case.kernel, r_cut=case.r_cut,
+                    free_wake=case.free_wake)
+    uv.set_design_variables(case.dt, R.Constant(case.u_inf, case.rho, True), case.zeta_b0, case.hg0)
+    return uv
+
+
+def cpu_steps(case, threads, warmup, max_steps, budget_s):
+    """Full UVLM time steps of the workload on the host: the FP64 oracle with its
+    induced-velocity sums and AIC assembly in C++/OpenMP (``threads`` threads, SIMD over
+    filaments) and the dense solve in LAPACK.  Static solve, ``warmup`` untimed steps,
+    then up to ``max_steps`` timed steps while the budget lasts."""
+    from oracle import uvlm_cpp as CP
+
+    CP.set_threads(threads)
+    uv = _cpu_uvlm(case)
+    st = uv.solve_static()
+    n_slots = min(case.hg_t.shape[0], 1 + warmup + max_steps)
+    cs = uv._empty_case(n_slots)
+    for key in ("zeta_b", "zeta_b_dot", "zeta_w", "c", "nc", "gamma_b", "gamma_b_dot", "gamma_w", "f_steady",
+                "f_unsteady", "alpha"):
+        for arr, val in zip(getattr(cs, key), getattr(st, key)):
+            arr[0] = val[0]
+    times = []
+    for i in range(1, n_slots):
+        t0 = time.perf_counter()
+        uv.case_step(cs, i, case.hg_t[i], case.hg_t[i - 1], case.hg_dot_t[i])
+        if i > warmup:
+            times.append(time.perf_counter() - t0)
+            if sum(times) >= budget_s:
+                break
+    return len(times) / sum(times), times
+
+
+def cpu_single_thread(case, budget_s):
+    """One-thread pair rate of the C++ oracle's induced-velocity sum (the free-wake
+    convection targets against the bound and wake lattices), scaled to steps/s by the
+    pairs of one step; the sums are > 99 % of a CPU step at this size."""
+    from oracle import uvlm_cpp as CP
+
+    CP.set_threads(1)
     zb = case.zeta_b0 + case.hg0[0, :3, 3]
     w = case.m_star
     zw = zb[-1][None] + np.arange(w + 1)[:, None, None] * (case.dt * case.u_inf)[None, None, :]
@@ -216,17 +253,37 @@ def cpu_sample(case, budget_s):
     gw = rng.normal(size=(w, case.n)) * 0.1
     targets = zw[:-1].reshape(-1, 3)
     filaments = sum(r * (c + 1) + (r + 1) * c for r, c in ((case.m, case.n), (w, case.n)))
-    n_t, t0, chunk = 0, time.perf_counter(), 32
+    n_t, t0, chunk = 0, time.perf_counter(), 64
     while time.perf_counter() - t0 < budget_s and n_t < targets.shape[0]:
-        R.compute_v_ind(targets[n_t:n_t + chunk], [zb, zw], [gb, gw], case.kernel, None, case.r_cut)
+        CP.compute_v_ind(targets[n_t:n_t + chunk], [zb, zw], [gb, gw], case.kernel, None, case.r_cut)
         n_t += chunk
     el = time.perf_counter() - t0
     pairs = n_t * filaments
-    steps_per_s = pairs / el / case.pairs_per_step()
-    return {"value": steps_per_s, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"NumPy FP64 oracle: induced velocity at {n_t} wake vertices from {filaments} filaments "
-                      f"({pairs:.3g} pairs in {el:.1f} s), scaled by {case.pairs_per_step():.4g} pairs per step",
+    return {"value": pairs / el / case.pairs_per_step(), "unit": UNIT, "cores": 1,
+            "sample": f"induced velocity at {n_t} wake vertices from {filaments} filaments ({pairs:.3g} pairs in "
+                      f"{el:.1f} s), scaled by {case.pairs_per_step():.4g} pairs per step",
             "pairs_per_s": pairs / el}
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_sample(case, budget_s):
+    """cpu_baseline: full steps on all host threads plus the one-thread pair rate."""
+    from flapjax_b200 import cases
+
+    th = host_threads()
+    cpu_case = cases.wing_free(m=case.m, n=case.n, m_star=case.m_star, n_steps=12, seed=case.seed)
+    value, times = cpu_steps(cpu_case, th, 1, 10, budget_s)
+    return {"value": value, "unit": UNIT, "cores": th, "kind": "port",
+            "sample": f"C++/OpenMP FP64 oracle (uvlm_ref_cpu.cpp + LAPACK solve), static solve + 1 untimed step, "
+                      f"then {len(times)} full time steps of the same workload on {th} threads "
+                      f"({sum(times):.1f} s)",
+            "step_s": times, "single_thread": cpu_single_thread(cpu_case, max(2.0, budget_s / 3))}
 
 
 def main():
@@ -408,25 +465,29 @@ def ctypes_peak(torch):
 
 
 def reference_arm(args):
+    """The reference's arithmetic on the host CPU (the reference itself is JAX, absent on
+    these machines): the C++/OpenMP FP64 oracle on every host thread, full time steps of
+    the same workload.  Steps beyond what fits in about a minute are not run; the line
+    reports how many were timed."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    case = workload(args, 1)
-    steps = []
-    for _ in range(args.warmup):
-        cpu_sample(case, min(2.0, args.cpu_seconds))
-    total = 0.0
-    budget = max(1.0, args.cpu_seconds / max(1, min(args.steps, 10)))
-    for _ in range(min(args.steps, 10)):
-        r = cpu_sample(case, budget)
-        steps.append(r["value"])
-        total += 1.0 / r["value"]
-    value = len(steps) / total
+    from flapjax_b200 import cases
+
+    th = host_threads()
+    n_max = max(1, min(args.steps, 50))
+    case = cases.wing_free(n_steps=args.warmup + n_max) if not args.small else cases.wing_free(
+        m=8, n=32, m_star=40, n_steps=args.warmup + n_max)
+    value, times = cpu_steps(case, th, args.warmup, n_max, 60.0)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
-            "steps": len(steps), "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "dtype": "fp64", "data": "synthetic", "config": {"workload": "free-wake UVLM 16x128, W=200"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
-                             "sample": r["sample"]},
+            "steps": len(times), "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "dtype": "fp64", "data": "synthetic",
+            "config": {"workload": "free-wake UVLM 16x128 bound, W=200 wake rows, cutoff kernel r=1e-3c, twist+camber "
+                                   "seeded, static-solve start" + (" [SMALL]" if args.small else ""),
+                       "seed": case.seed},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": th, "kind": "port",
+                             "sample": f"C++/OpenMP FP64 oracle, {args.warmup} untimed + {len(times)} timed full "
+                                       f"time steps on {th} threads ({sum(times):.1f} s)"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0

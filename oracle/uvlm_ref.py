@@ -609,6 +609,9 @@ class UVLMRef:
     def v_ind(self, x, zetas, gammas):
         return compute_v_ind(x, zetas, gammas, self.kernel, self.mirror, self.r_cut)
 
+    def aic_solve(self, cs, ns, zetas_b, zetas_w):
+        return compute_aic_solve(cs, ns, zetas_b, zetas_w, self.kernel, self.mirror, self.r_cut)
+
     # uvlm.py:824-1117
     def base_solve_from_grid(self, q_nm1, t_n, zeta_b_n, zeta_b_nm1, zeta_b_dot_n, static,
                              horseshoe=False):
@@ -640,8 +643,7 @@ class UVLMRef:
                 zeta_w_n.append(zw)
                 gamma_w_n.append(gw)
 
-        aic = compute_aic_solve(c_n, nc_n, zeta_b_n, zeta_w_n if static else None, self.kernel,
-                                self.mirror, self.r_cut)
+        aic = self.aic_solve(c_n, nc_n, zeta_b_n, zeta_w_n if static else None)
         v_bc = [ff(c, t_n) for c in c_n]
         if not static:
             v_bc = [v - cd for v, cd in zip(v_bc, c_dot_n)]
