@@ -136,6 +136,7 @@ _SIGS = {
     "fj_batch_workspace_size": (C.c_int, [C.c_int, C.POINTER(C.c_size_t)]),
     "fj_step_batched": (C.c_int, [C.POINTER(FjBatchItem), C.c_int, _P, C.c_size_t, _P]),
     "fj_case_residual": (C.c_int, [C.POINTER(FjCaseConfig), _P, C.c_size_t, C.c_int, C.POINTER(C.c_double), _P]),
+    "fj_case_factors_copy": (C.c_int, [C.POINTER(FjCaseConfig), _P, C.c_size_t, _P, _P, _P]),
     "fj_launch_count": (C.c_int64, []),
     "fj_profile_begin": (C.c_int, []),
     "fj_profile_end": (C.c_int, [C.c_void_p]),

@@ -12,7 +12,8 @@ wake geometry (Zw) and lattice (Zb, Zbdot):
      velocity and filament vector terms; the induced velocity at the filament midpoints
      through the hand-written Biot-Savart VJP (``fj_vind_vjp``);
   2. gamma_dot filter (uvlm.py:691-715);
-  3. solve: mu = A_n^-T Gb_n (``fj_lu_solve_t`` on the getrf factors of A_n);
+  3. solve: mu = A_n^-T Gb_n (``fj_lu_solve_t`` on the getrf factors of A_n that the
+     forward recomputation of the segment kept, ``fj_case_factors_copy``);
   4. right-hand side and AIC: A_n Gamma_n = nc . V_bound(c), so the AIC's geometric
      derivative is the VJP of the bound-lattice sum at the collocation points; with the
      wake term both are one VJP with cotangent -mu nc;
@@ -23,7 +24,8 @@ wake geometry (Zw) and lattice (Zb, Zbdot):
 Slot 0 (the static solve, uvlm.py:1286-1333) closes the sweep with the lumped-wake AIC.
 
 Forward states are recomputed from checkpoints every ``checkpoint`` steps (only the
-checkpoint slots are kept), so device memory is O(checkpoint) slots.
+checkpoint slots are kept), so device memory is O(checkpoint) slots and O(checkpoint)
+factor matrices.
 
 Scope: one surface, epsilon kernel, Constant flow, prescribed wake, no mirror.
 """
@@ -101,6 +103,17 @@ class _Dev:
                   self.stream())
         return (tb.cpu().numpy().reshape(targets.shape), [z.cpu().numpy() for z in zb],
                 [g.cpu().numpy() for g in gb])
+
+    def solve_t_factors(self, lu, piv, rhs):
+        """mu with A^T mu = rhs from stored getrf factors (device tensors)."""
+        n = piv.numel()
+        w = C.c_size_t()
+        _lib.call("fj_lu_workspace_size", n, C.byref(w))
+        wl = self.ws("lu", w.value)
+        b = self.t(rhs.ravel())
+        _lib.call("fj_lu_solve_t", lu.data_ptr(), n, piv.data_ptr(), b.data_ptr(), wl.data_ptr(), wl.numel(),
+                  self.stream())
+        return b.cpu().numpy().reshape(rhs.shape)
 
     def solve_t(self, zeta_b, zeta_w_static, rhs):
         """mu with A^T mu = rhs, A the AIC of zeta_b (with the wake lumped onto the TE
@@ -189,13 +202,27 @@ class PrescribedAdjoint:
     def _static(self):
         return self.uv.solve_static()
 
-    def _run_segment(self, init_case, hg_seg, hgd_seg):
+    def _run_segment(self, init_case, hg_seg, hgd_seg, keep_factors=False):
+        """Forward over one segment; with ``keep_factors`` also the factors of every
+        step's AIC (device tensors, index = slot in the segment)."""
         uv = self.uv
         dc = uv.make_device_case(hg_seg.shape[0], hg_seg.shape[1])
         uv.load_initial(dc, init_case)
         dc.set_hg(hg_seg, hgd_seg)
-        dc.solve_dynamic(1, hg_seg.shape[0])
-        return uv._to_case(dc)
+        if not keep_factors:
+            dc.solve_dynamic(1, hg_seg.shape[0])
+            return uv._to_case(dc)
+        torch = self.d.torch
+        nb = sum(g.m * g.n for g in uv.grid_disc)
+        n = hg_seg.shape[0]
+        lus = torch.empty((n, nb, nb), dtype=torch.float64, device=self.d.dev)
+        pivs = torch.empty((n, nb), dtype=torch.int32, device=self.d.dev)
+        for i in range(1, n):
+            dc.solve_dynamic(i, i + 1)
+            dc.copy_factors(lus[i], pivs[i])
+        seg = uv._to_case(dc)
+        seg.factors = (lus, pivs)
+        return seg
 
     def gradient(self, hg_t, hg_dot_t, force_weights, checkpoint=10):
         """Return (J, dJ/dzeta_b0) for J = sum_{n>=1} force_weights[n] . F_n."""
@@ -230,7 +257,7 @@ class PrescribedAdjoint:
         seg_starts = sorted(k for k in ckpt if k < N)
         for s0 in reversed(seg_starts):
             s1 = min(N, s0 + checkpoint)
-            seg = self._run_segment(ckpt[s0], hg_t[s0:s1 + 1], hg_dot_t[s0:s1 + 1])
+            seg = self._run_segment(ckpt[s0], hg_t[s0:s1 + 1], hg_dot_t[s0:s1 + 1], keep_factors=True)
             for loc in range(s1 - s0, 0, -1):
                 nstep = s0 + loc
                 Gb_prev, Gbd_prev, Gw_prev, Zw_prev = self._reverse_step(
@@ -318,7 +345,8 @@ class PrescribedAdjoint:
         Gb_prev = -(relax / dt) * Gbd
         Gbd_prev = (1.0 - relax) * Gbd
         # 3. transpose solve with A_n
-        mu = d.solve_t(zb, None, Gb)
+        factors = getattr(seg, "factors", None)
+        mu = d.solve_t(zb, None, Gb) if factors is None else d.solve_t_factors(factors[0][loc], factors[1][loc], Gb)
         # 4. RHS + AIC geometry: b = -(U - c_dot + V_w(c)) . nc and A Gamma = nc . V_b(c)
         cdot = 0.5 * (0.5 * (zbd[:-1, :-1] + zbd[1:, :-1]) + 0.5 * (zbd[:-1, 1:] + zbd[1:, 1:]))
         Vtot = d.vind(c, [(zw, gw), (zb, gb)])

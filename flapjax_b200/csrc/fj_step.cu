@@ -1370,6 +1370,19 @@ int fj_case_residual(const fj_case_config* cfg, void* d_ws, size_t ws_bytes, int
     return FJ_OK;
 }
 
+int fj_case_factors_copy(const fj_case_config* cfg, const void* d_ws, size_t ws_bytes, double* d_lu,
+                         int32_t* d_piv, fj_stream_t stream) {
+    if (cfg == nullptr || d_lu == nullptr || d_piv == nullptr) return fail(FJ_ERR_SHAPE, "factors_copy: null argument");
+    if (cfg->precision != FJ_PREC_FP64)
+        return fail(FJ_ERR_UNSUPPORTED, "factors_copy: only FP64 cases keep FP64 factors");
+    Plan p;
+    FJ_TRY(make_plan(cfg, const_cast<void*>(d_ws), ws_bytes, p));
+    cudaStream_t s = (cudaStream_t)stream;
+    FJ_CUDA(cudaMemcpyAsync(d_lu, p.a64, (size_t)p.nb * p.nb * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    FJ_CUDA(cudaMemcpyAsync(d_piv, p.piv, (size_t)p.nb * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+    return FJ_OK;
+}
+
 int fj_biot_savart(const double* d_x, const double* d_y, int64_t n_pairs, int kernel, double r_cut, double* d_out,
                    fj_stream_t stream) {
     return biot_savart_pairs(d_x, d_y, n_pairs, kernel, r_cut, d_out, (cudaStream_t)stream);

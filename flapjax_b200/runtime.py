@@ -162,6 +162,12 @@ class DeviceCase:
         _lib.call("fj_solve_prescribed_dynamic", C.byref(self.cfg), C.byref(self._bufs), int(i_first), int(i_last),
                   flags, self.ws.data_ptr(), self.ws.numel(), self._stream())
 
+    def copy_factors(self, lu, piv):
+        """Copy the FP64 getrf factors and pivots of the last solved step into the
+        device tensors ``lu`` (nb x nb, float64) and ``piv`` (nb, int32)."""
+        _lib.call("fj_case_factors_copy", C.byref(self.cfg), self.ws.data_ptr(), self.ws.numel(), lu.data_ptr(),
+                  piv.data_ptr(), self._stream())
+
     # -- outputs ----------------------------------------------------------------------
     def host_arrays(self, slots=None):
         """Numpy copies {field: (n_slots, total)} of the given slots (default all)."""

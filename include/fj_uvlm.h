@@ -195,8 +195,17 @@ FJ_API int fj_step_batched(const fj_batch_item* items, int n_items, void* d_batc
 FJ_API int fj_case_residual(const fj_case_config* cfg, void* d_ws, size_t ws_bytes, int i_ts,
                             double* h_out, fj_stream_t stream);
 
-/* Measured FP32 FMA throughput of the current device (TFLOP/s, an FMA counted as two),
- * from a register-resident FMA-chain kernel timed with CUDA events.  Synchronises. */
+/* Copies the getrf factors (row-major L\U, n x n) and 0-based pivots of the AIC that the
+ * last dynamic step of an FP64 case solved with, into caller buffers (stream-ordered).
+ * The adjoint keeps them per step to solve A^T mu = lam with fj_lu_solve_t instead of
+ * re-assembling and re-factorising; the reference has no counterpart (jax.vjp through
+ * jnp.linalg.solve recomputes, aero/uvlm.py:985). */
+FJ_API int fj_case_factors_copy(const fj_case_config* cfg, const void* d_ws, size_t ws_bytes, double* d_lu,
+                                int32_t* d_piv, fj_stream_t stream);
+
+/* Measured FP32 FMA throughput of the current device (TFLOP/s, an FMA counted as two):
+ * the larger of a scalar and a packed (f32x2) register-resident FMA-chain kernel, timed
+ * with CUDA events.  Synchronises. */
 FJ_API int fj_peak_fp32(double* tflops, fj_stream_t stream);
 
 /* ---------------------------------------------------------------------------------

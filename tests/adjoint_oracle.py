@@ -90,7 +90,7 @@ class OracleAdjoint(PrescribedAdjoint):
     def _static(self):
         return _Snap(self.uv.solve_static(), 0)
 
-    def _run_segment(self, init, hg_seg, hgd_seg):
+    def _run_segment(self, init, hg_seg, hgd_seg, keep_factors=False):
         return _Seg(self.uv.solve_prescribed_dynamic(init._case if init._i == 0 else _one(init), hg_seg, hgd_seg))
 
 

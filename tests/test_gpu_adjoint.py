@@ -153,3 +153,29 @@ def test_twist_gradient_matches_finite_differences(cuda, which):
         with R.real_type(np.longdouble):
             fd = float((forward_objective(c, zp, fw) - forward_objective(c, zm, fw)) / (2 * h))
         assert abs(fd - grad[k]) <= 1e-6 * max(abs(fd), 1e-2 * np.max(np.abs(grad))), (k, fd, grad[k])
+
+
+def test_case_factors_copy_matches_direct_factorisation(cuda):
+    """The factors an FP64 step solved with equal getrf of the AIC assembled directly
+    from that step's lattice."""
+    import torch
+
+    from flapjax_b200.adjoint import _Dev
+
+    c = cases.wing_pitch(m=4, n=6, m_star=5, n_steps=3, n_ctrl=3, seed=1)
+    uv, _ = device_uvlm(c, "fp64")
+    dc = uv.make_device_case(c.n_tstep)
+    uv.load_initial(dc, uv.solve_static())
+    dc.set_hg(c.hg_t, c.hg_dot_t)
+    nb = c.m * c.n
+    lu = torch.empty((nb, nb), dtype=torch.float64, device=cuda)
+    piv = torch.empty(nb, dtype=torch.int32, device=cuda)
+    for i in (1, 2):
+        dc.solve_dynamic(i, i + 1)
+        dc.copy_factors(lu, piv)
+        zb = uv._to_case(dc).zeta_b[0][i]
+        rhs = np.random.default_rng(i).normal(size=(c.m, c.n))
+        d = _Dev(cuda)
+        got = d.solve_t_factors(lu, piv, rhs)
+        want = d.solve_t(zb, None, rhs)
+        assert np.max(np.abs(got - want)) <= 1e-12 * np.max(np.abs(want))
