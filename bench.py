@@ -38,6 +38,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "UVLM time-steps/s (free wake 16x128, W=200)"
 UNIT = "steps/s"
 FLOPS_PER_PAIR = 70.0  # Biot-Savart convention: FMA = 2, rsqrt/div = 1 per (target, filament)
+VIND32_TRAFFIC_BYTES = 3.33e6  # DRAM bytes of one vind32 launch of this workload, from an ncu capture
 
 
 def parse():
@@ -339,8 +340,12 @@ def main():
     achieved = prof.vind_pairs * FLOPS_PER_PAIR / (prof.vind_ms * 1e-3) / 1e12 if prof.vind_ms > 0 else None
     roof = {"kernel": "vind32 (FP32 Biot-Savart sums)", "bound": "fp32", "achieved": achieved,
             "peak": peak, "unit": "TFLOP/s", "frac": (achieved / peak) if achieved and peak else None,
-            "traffic": None, "peak_source": "measured in-run (fj_peak_fp32: FP32 FMA chains); "
-                                             "MEASURED_PEAKS.json has no FP32 CUDA-core figure",
+            "traffic": VIND32_TRAFFIC_BYTES,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the convection launch of this "
+                              "workload (profiles/vind32_free_wake_16x128.md); the filament stream is the only "
+                              "DRAM traffic, the rest stays in L2",
+            "peak_source": "measured in-run (fj_peak_fp32: larger of scalar and packed FP32 FMA chains); "
+                           "MEASURED_PEAKS.json has no FP32 CUDA-core figure",
             "pairs_per_launch": prof.vind_pairs / max(prof.vind_launches, 1),
             "kernel_ms_per_step": prof.vind_ms / K, "share_of_step": prof.vind_ms / t_ms if t_ms else None,
             "pairs_per_s": prof.vind_pairs / (prof.vind_ms * 1e-3) if prof.vind_ms else None}
