@@ -137,6 +137,18 @@ _SIGS = {
     "fj_step_batched": (C.c_int, [C.POINTER(FjBatchItem), C.c_int, _P, C.c_size_t, _P]),
     "fj_case_residual": (C.c_int, [C.POINTER(FjCaseConfig), _P, C.c_size_t, C.c_int, C.POINTER(C.c_double), _P]),
     "fj_case_factors_copy": (C.c_int, [C.POINTER(FjCaseConfig), _P, C.c_size_t, _P, _P, _P]),
+    "fj_rhs_workspace_size": (C.c_int, [C.c_int64, _P, _P, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_size_t)]),
+    "fj_rhs": (C.c_int, [_P, _P, _P, C.c_int64, C.POINTER(FjFlowfield), C.c_double, _P, _P, _P, _P, C.c_int,
+                         _P, _P, C.c_int, C.c_double, C.c_int, _P, _P, C.c_size_t, _P]),
+    "fj_wake_shed_convect": (C.c_int, [_P, _P, _P, _P, _P, C.c_int, C.c_int, C.POINTER(FjFlowfield), C.c_double,
+                                       C.c_double, _P, _P, _P]),
+    "fj_forces_workspace_size": (C.c_int, [C.c_int, C.c_int, _P, _P, C.c_int, C.c_int, C.c_int,
+                                           C.POINTER(C.c_size_t)]),
+    "fj_forces": (C.c_int, [_P, _P, _P, _P, _P, C.c_int, C.c_int, C.POINTER(FjFlowfield), C.c_double, _P, _P, _P,
+                            _P, C.c_int, _P, _P, C.c_int, C.c_double, C.c_int, _P, _P, _P, C.c_size_t, _P]),
+    "fj_aic_vjp_workspace_size": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_size_t)]),
+    "fj_aic_vjp": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, C.c_int, _P, _P, C.c_size_t, _P]),
+    "fj_wake_vjp": (C.c_int, [_P, _P, C.c_int, C.c_int, _P, _P, _P, _P, _P]),
     "fj_launch_count": (C.c_int64, []),
     "fj_profile_begin": (C.c_int, []),
     "fj_profile_end": (C.c_int, [C.c_void_p]),

@@ -280,6 +280,61 @@ FJ_API int fj_lu_solve(const double* d_lu, int n, const int32_t* d_piv, double* 
 FJ_API int fj_lu_solve_t(const double* d_lu, int n, const int32_t* d_piv, double* d_b, void* d_ws,
                          size_t ws_bytes, fj_stream_t stream);
 
+/* ---- One surface's pieces of a step, as the reference calls them separately ---------
+ * Right-hand side of the dynamic solve, aero/uvlm.py:961-983: b_i = -(v_bc_i . nc_i) with
+ * v_bc = U(c, t) - c_dot + v_ind(c; wake lattices) -- the vector the reference passes to
+ * jnp.linalg.solve(aic, -rhs).  The static solve is n_wake = 0 and d_c_dot = NULL. */
+FJ_API int fj_rhs_workspace_size(int64_t n_pan, const int* rows_w, const int* cols_w, int n_wake,
+                                 int mirror, int precision, size_t* bytes);
+FJ_API int fj_rhs(const double* d_c, const double* d_nc, const double* d_c_dot, int64_t n_pan,
+                  const fj_flowfield* flow, double t, const double* const* d_zetas_w,
+                  const double* const* d_gammas_w, const int* rows_w, const int* cols_w, int n_wake,
+                  const double* mirror_point, const double* mirror_normal, int kernel, double r_cut,
+                  int precision, double* d_b, void* d_ws, size_t ws_bytes, fj_stream_t stream);
+
+/* propagate_surf_wake, uniform branch (aero/utils.py:400-450): zeta_w_n (m_star+1, n+1, 3)
+ * = [TE row of zeta_b_n; zeta_w_nm1[:-1] + dt (U(x, t) + v_conv)] and gamma_w_n (m_star, n)
+ * = [TE row of gamma_b_nm1; gamma_w_nm1[:-1]].  d_v_conv (m_star, n+1, 3): the free-wake
+ * induced velocity at zeta_w_nm1[:-1] (fj_vind over the lattices of step n-1), or NULL
+ * for a prescribed wake. */
+FJ_API int fj_wake_shed_convect(const double* d_zeta_te_n, const double* d_gamma_te_nm1,
+                                const double* d_zeta_w_nm1, const double* d_gamma_w_nm1,
+                                const double* d_v_conv, int n, int m_star, const fj_flowfield* flow,
+                                double t, double dt, double* d_zeta_w_n, double* d_gamma_w_n,
+                                fj_stream_t stream);
+
+/* calculate_steady_forcing (aero/utils.py:126-223) of one lattice zeta_b (m+1, n+1, 3):
+ * per filament rho G_eff (v_rel x r) at its midpoint, v_rel = U + v_ind(midpoint; the
+ * given lattices, normally bound + wake) - zeta_b_dot (averaged), the TE spanwise
+ * filament less gamma_w[0] (d_gamma_w0, n values, or NULL), split to the vertices; and
+ * with d_gamma_b_dot the unsteady force split_to_vertex(rho gamma_dot nc)
+ * (aero/uvlm.py:1086-1103) into d_f_unsteady (or NULL to skip). */
+FJ_API int fj_forces_workspace_size(int m, int n, const int* rows, const int* cols, int n_lat,
+                                    int mirror, int precision, size_t* bytes);
+FJ_API int fj_forces(const double* d_zeta_b, const double* d_zeta_b_dot, const double* d_gamma_b,
+                     const double* d_gamma_w0, const double* d_gamma_b_dot, int m, int n,
+                     const fj_flowfield* flow, double t, const double* const* d_zetas,
+                     const double* const* d_gammas, const int* rows, const int* cols, int n_lat,
+                     const double* mirror_point, const double* mirror_normal, int kernel, double r_cut,
+                     int precision, double* d_f_steady, double* d_f_unsteady, void* d_ws, size_t ws_bytes,
+                     fj_stream_t stream);
+
+/* Adjoint twin of the AIC (compute_aic_solve, aero/aic.py:11-187; the reference
+ * differentiates it with jax.vjp): ACCUMULATES into d_zeta_bar (m+1, n+1, 3) the lattice
+ * cotangent of s = mu^T A(zeta) Gamma for one surface's bound AIC (epsilon kernel, no
+ * mirror), through the filaments, the collocation points and the normals. */
+FJ_API int fj_aic_vjp_workspace_size(int m, int n, size_t* bytes);
+FJ_API int fj_aic_vjp(const double* d_zeta, int m, int n, const double* d_gamma, const double* d_mu,
+                      int kernel, double* d_zeta_bar, void* d_ws, size_t ws_bytes, fj_stream_t stream);
+
+/* Adjoint twin of the prescribed wake shift (aero/utils.py:427-450): given the cotangents
+ * of zeta_w_n and gamma_w_n, ACCUMULATES row 0 into the TE cotangents (of zeta_b_n's last
+ * row and gamma_b_nm1's last row) and rows 1.. into the cotangents of zeta_w_nm1[:-1] and
+ * gamma_w_nm1[:-1].  Any output may be NULL. */
+FJ_API int fj_wake_vjp(const double* d_zeta_w_bar_n, const double* d_gamma_w_bar_n, int n, int m_star,
+                       double* d_zeta_te_bar, double* d_gamma_te_bar, double* d_zeta_w_bar_nm1,
+                       double* d_gamma_w_bar_nm1, fj_stream_t stream);
+
 /* Mixed-precision solve of A x = b: FP32 factors of A (recomputed when refactor != 0)
  * kept in the workspace, then FP64 iterative refinement x += M (b - A x) with the FP64
  * residual.  Writes the final relative residual ||b-Ax||_inf / ||b||_inf to
