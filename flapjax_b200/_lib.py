@@ -70,6 +70,7 @@ class FjCaseConfig(C.Structure):
         ("gamma_dot_relaxation", C.c_double),
         ("flow", FjFlowfield),
         ("precision", C.c_int),
+        ("variable_wake", _I8),
     ]
 
 
@@ -82,6 +83,7 @@ class FjCaseBuffers(C.Structure):
         ("d_dof_mapping", _P),
         ("d_hg_t", _P),
         ("d_hg_dot_t", _P),
+        ("d_delta_w", _P),
         ("d_t", _P),
         ("d_zeta_b", _P),
         ("d_zeta_b_dot", _P),

@@ -41,7 +41,12 @@ struct Layout {
     int64_t so[FJ_MAX_SURF + 1];   // strips
     int64_t dofo[FJ_MAX_SURF + 1]; // dof mapping entries (n+1)
     int64_t fo[FJ_MAX_SURF + 1];   // bound filaments m(n+1) + (m+1)n
-    int64_t wto[FJ_MAX_SURF + 1];  // free-wake targets m_star(n+1)
+    int64_t wto[FJ_MAX_SURF + 1];  // free-wake targets (m_star + var)(n+1)
+    int64_t dwo[FJ_MAX_SURF + 1];  // delta_w entries m_star
+    int64_t xvo[FJ_MAX_SURF + 1];  // variable wake: vertices before re-discretisation (m_star+2)(n+1)
+    int64_t xpo[FJ_MAX_SURF + 1];  // variable wake: circulations before re-discretisation (m_star+1)n
+    int var[FJ_MAX_SURF];          // 1: variable wake discretisation (delta_w)
+    int any_var;
     int n_nodes;                   // beam nodes in the frame arrays
 };
 
@@ -62,7 +67,14 @@ static Layout make_layout(const fj_case_config& c) {
         L.so[s + 1] = L.so[s] + n;
         L.dofo[s + 1] = L.dofo[s] + n + 1;
         L.fo[s + 1] = L.fo[s] + (int64_t)m * (n + 1) + (int64_t)(m + 1) * n;
-        L.wto[s + 1] = L.wto[s] + (int64_t)ms * (n + 1);
+        const int var = c.variable_wake[s] ? 1 : 0;
+        L.var[s] = var;
+        L.any_var |= var;
+        // with delta_w every wake row is convected (aero/utils.py:431-436)
+        L.wto[s + 1] = L.wto[s] + (int64_t)(ms + var) * (n + 1);
+        L.dwo[s + 1] = L.dwo[s] + ms;
+        L.xvo[s + 1] = L.xvo[s] + (var ? (int64_t)(ms + 2) * (n + 1) : 0);
+        L.xpo[s + 1] = L.xpo[s] + (var ? (int64_t)(ms + 1) * n : 0);
     }
     return L;
 }
@@ -124,6 +136,10 @@ struct StepCase {
     double* ffil;
     double* rhs;
     const double* v_wake;   // free-wake convection velocities (null: prescribed wake)
+    const double* delta_w;  // variable wake segment lengths (Layout::dwo blocks)
+    double* zw_tmp;         // variable wake before re-discretisation (Layout::xvo blocks)
+    double* gw_tmp;         // (Layout::xpo blocks)
+    double* s_tmp;          // arc length along each wake column (Layout::xvo blocks)
     const double* v_rhs;    // wake velocity at collocation points (null: static solve)
     const double* zeta_ref; // mixed path: lattice of the cached AIC (null: no comparison)
     int* changed;           // mixed path: set to 1 when zb_n differs from zeta_ref
@@ -204,7 +220,8 @@ __global__ void k_geom_panels(const StepCase* __restrict__ T) {
 // initialise_wake (uvlm.py:662-689): TE + cumsum(dt |U|) along the freestream direction.
 // `hs_len` > 0 builds the 2-row horseshoe wake instead (uvlm.py:642-660).
 __global__ void init_wake_kernel(Layout L, const double* __restrict__ zeta_b, fj_flowfield f, double dt,
-                                 double hs_len, double* __restrict__ zeta_w, int rows_override) {
+                                 double hs_len, double* __restrict__ zeta_w, int rows_override,
+                                 const double* __restrict__ delta_w) {
     // rows_override > 0: that many rows for every surface that has a wake, 0 rows
     // (the TE only) for surfaces with m_star == 0 (uvlm.py:652-660)
     int64_t tot = 0;
@@ -230,6 +247,9 @@ __global__ void init_wake_kernel(Layout L, const double* __restrict__ zeta_b, fj
     double sdist;
     if (hs_len > 0.0) {
         sdist = r == 0 ? 0.0 : hs_len;
+    } else if (L.var[s] && delta_w != nullptr) {
+        sdist = 0.0;  // cumsum(delta_w), uvlm.py:672-683
+        for (int q = 0; q < r; ++q) sdist += delta_w[L.dwo[s] + q];
     } else {
         sdist = 0.0;  // cumsum of equal increments, summed in order as jnp.cumsum
         const double inc = 1.0 * dt * umag;
@@ -263,7 +283,9 @@ __global__ void k_wake_shed(const StepCase* __restrict__ T) {
         const int64_t lv = v - L.wvo[s];
         const int n = L.n[s];
         const int r = (int)(lv / (n + 1)), l = (int)(lv % (n + 1));
-        if (r == 0) {
+        if (L.var[s]) {
+            // variable wake: k_wake_shed_var and the re-discretisation write this surface
+        } else if (r == 0) {
             const double* te = C.zb_n + (L.vo[s] + (int64_t)L.m[s] * (n + 1) + l) * 3;
             for (int d = 0; d < 3; ++d) C.zw_n[v * 3 + d] = te[d];
         } else {
@@ -286,8 +308,129 @@ __global__ void k_wake_shed(const StepCase* __restrict__ T) {
         const int64_t lg = g - L.wpo[s];
         const int n = L.n[s];
         const int r = (int)(lg / n), l = (int)(lg % n);
-        C.gw_n[g] = r == 0 ? C.gb_nm1[L.po[s] + (int64_t)(L.m[s] - 1) * n + l]
-                           : C.gw_nm1[L.wpo[s] + (int64_t)(r - 1) * n + l];
+        if (!L.var[s])
+            C.gw_n[g] = r == 0 ? C.gb_nm1[L.po[s] + (int64_t)(L.m[s] - 1) * n + l]
+                               : C.gw_nm1[L.wpo[s] + (int64_t)(r - 1) * n + l];
+    }
+}
+
+// propagate_surf_wake with delta_w (aero/utils.py:427-491), part 1: shed the TE row and
+// convect EVERY row of the wake at n-1 (m_star+2 vertex rows, m_star+1 circulation rows).
+__global__ void k_wake_shed_var(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    const Layout& L = C.L;
+    if (!L.any_var || C.zw_tmp == nullptr) return;
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t nv = L.xvo[L.n_surf];
+    const double t = C.t[C.i];
+    if (v < nv) {
+        const int s = find_surf(L.xvo, L.n_surf, v);
+        const int64_t lv = v - L.xvo[s];
+        const int n = L.n[s];
+        const int r = (int)(lv / (n + 1)), l = (int)(lv % (n + 1));
+        if (r == 0) {
+            const double* te = C.zb_n + (L.vo[s] + (int64_t)L.m[s] * (n + 1) + l) * 3;
+            for (int d = 0; d < 3; ++d) C.zw_tmp[v * 3 + d] = te[d];
+        } else {
+            const int64_t src = L.wvo[s] + (int64_t)(r - 1) * (n + 1) + l;
+            const double x[3] = {C.zw_nm1[src * 3], C.zw_nm1[src * 3 + 1], C.zw_nm1[src * 3 + 2]};
+            double u[3];
+            flow_eval(C.flow, x, t, u);
+            if (C.v_wake != nullptr) {
+                const int64_t ti = L.wto[s] + (int64_t)(r - 1) * (n + 1) + l;
+                u[0] += C.v_wake[ti * 3];
+                u[1] += C.v_wake[ti * 3 + 1];
+                u[2] += C.v_wake[ti * 3 + 2];
+            }
+            for (int d = 0; d < 3; ++d) C.zw_tmp[v * 3 + d] = x[d] + C.dt * u[d];
+        }
+    }
+    const int64_t g = v - nv;
+    if (g >= 0 && g < L.xpo[L.n_surf]) {
+        const int s = find_surf(L.xpo, L.n_surf, g);
+        const int64_t lg = g - L.xpo[s];
+        const int n = L.n[s];
+        const int r = (int)(lg / n), l = (int)(lg % n);
+        C.gw_tmp[g] = r == 0 ? C.gb_nm1[L.po[s] + (int64_t)(L.m[s] - 1) * n + l]
+                             : C.gw_nm1[L.wpo[s] + (int64_t)(r - 1) * n + l];
+    }
+}
+
+// np.interp(x, xp, fp) for increasing xp of length np_ (strided by `st`): fp[0] left of
+// xp[0], fp[-1] right of xp[-1], else fp[j] + slope (x - xp[j]) on xp[j] <= x < xp[j+1].
+template <typename XP, typename FP>
+__device__ __forceinline__ double interp1(double x, int np_, XP xp, FP fp) {
+    if (!(x >= xp(0))) return fp(0);
+    if (x >= xp(np_ - 1)) return fp(np_ - 1);
+    int lo = 0, hi = np_ - 1;  // invariant xp(lo) <= x < xp(hi)
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (xp(mid) <= x) lo = mid; else hi = mid;
+    }
+    const double slope = (fp(hi) - fp(lo)) / (xp(hi) - xp(lo));
+    return slope * (x - xp(lo)) + fp(lo);
+}
+
+// Part 2: arc length along each vertex column of the convected wake, and the vertices
+// re-interpolated at the prescribed arc lengths [0, cumsum(delta_w)].  Thread per
+// (surface, column).
+__global__ void k_wake_redisc_z(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    const Layout& L = C.L;
+    if (!L.any_var || C.zw_tmp == nullptr) return;
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= L.dofo[L.n_surf]) return;
+    const int s = find_surf(L.dofo, L.n_surf, idx);
+    if (!L.var[s]) return;
+    const int n = L.n[s], ms = L.ms[s];
+    const int l = (int)(idx - L.dofo[s]);
+    const double* X = C.zw_tmp + L.xvo[s] * 3;
+    double* S = C.s_tmp + L.xvo[s];
+    const int np_ = ms + 2;
+    S[l] = 0.0;
+    for (int r = 1; r < np_; ++r) {
+        const double* a = X + ((int64_t)(r - 1) * (n + 1) + l) * 3;
+        const double* b = X + ((int64_t)r * (n + 1) + l) * 3;
+        const double dx = b[0] - a[0], dy = b[1] - a[1], dz = b[2] - a[2];
+        S[(int64_t)r * (n + 1) + l] = S[(int64_t)(r - 1) * (n + 1) + l] + sqrt(dx * dx + dy * dy + dz * dz);
+    }
+    auto xp = [&](int r) { return S[(int64_t)r * (n + 1) + l]; };
+    const double* dw = C.delta_w + L.dwo[s];
+    double sd = 0.0;
+    for (int q = 0; q <= ms; ++q) {
+        if (q > 0) sd += dw[q - 1];
+        double* out = C.zw_n + (L.wvo[s] + (int64_t)q * (n + 1) + l) * 3;
+        for (int d = 0; d < 3; ++d)
+            out[d] = interp1(sd, np_, xp, [&](int r) { return X[((int64_t)r * (n + 1) + l) * 3 + d]; });
+    }
+}
+
+// Part 3: circulations re-interpolated from the panel-centre arc lengths
+// (neighbour_average of the vertex arc lengths over both axes) at the midpoints of the
+// prescribed segments.  Thread per (surface, circulation column).
+__global__ void k_wake_redisc_g(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    const Layout& L = C.L;
+    if (!L.any_var || C.zw_tmp == nullptr) return;
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= L.so[L.n_surf]) return;
+    const int s = find_surf(L.so, L.n_surf, idx);
+    if (!L.var[s] || L.ms[s] == 0) return;
+    const int n = L.n[s], ms = L.ms[s];
+    const int l = (int)(idx - L.so[s]);
+    const double* S = C.s_tmp + L.xvo[s];
+    const double* G = C.gw_tmp + L.xpo[s];
+    auto sz = [&](int r, int c) { return S[(int64_t)r * (n + 1) + c]; };
+    auto xp = [&](int r) {
+        return 0.5 * (0.5 * (sz(r, l) + sz(r + 1, l)) + 0.5 * (sz(r, l + 1) + sz(r + 1, l + 1)));
+    };
+    auto fp = [&](int r) { return G[(int64_t)r * n + l]; };
+    const double* dw = C.delta_w + L.dwo[s];
+    double s0 = 0.0;
+    for (int q = 0; q < ms; ++q) {
+        const double s1 = s0 + dw[q];
+        C.gw_n[L.wpo[s] + (int64_t)q * n + l] = interp1(0.5 * (s0 + s1), ms + 1, xp, fp);
+        s0 = s1;
     }
 }
 
@@ -557,6 +700,9 @@ struct Plan {
     void* stream;
     double* hs_zw;       // horseshoe wake scratch
     double* hs_gw;
+    double* zw_tmp;      // variable wake scratch (null when no surface has delta_w)
+    double* gw_tmp;
+    double* s_tmp;
     double* a64;         // FP64 AIC (factored in place on the FP64 path)
     float* a32;          // FP32 LU factors (mixed)
     float* x32;          // FP32 inverse (mixed)
@@ -577,6 +723,9 @@ static int validate(const fj_case_config* c) {
         if (c->m[s] < 1 || c->n[s] < 1 || c->m_star[s] < 0)
             return fail(FJ_ERR_SHAPE, "surface %d: m=%d n=%d m_star=%d", s, c->m[s], c->n[s], c->m_star[s]);
     }
+    for (int s = 0; s < c->n_surf; ++s)
+        if (c->variable_wake[s] != 0 && c->variable_wake[s] != 1)
+            return fail(FJ_ERR_SHAPE, "variable_wake[%d]=%d must be 0 or 1", s, c->variable_wake[s]);
     if (c->n_tstep < 1) return fail(FJ_ERR_SHAPE, "n_tstep=%d", c->n_tstep);
     if (c->n_nodes < 1) return fail(FJ_ERR_SHAPE, "n_nodes=%d", c->n_nodes);
     if (!(c->dt > 0.0) || !std::isfinite(c->dt)) return fail(FJ_ERR_SHAPE, "dt=%g must be positive", c->dt);
@@ -666,6 +815,13 @@ static int make_plan(const fj_case_config* cfg, void* ws, size_t ws_bytes, Plan&
     }
     p.hs_zw = a.carve<double>(hs);
     p.hs_gw = a.carve<double>(hsg);
+    if (L.any_var) {
+        p.zw_tmp = a.carve<double>(L.xvo[ns] * 3);
+        p.gw_tmp = a.carve<double>(std::max<int64_t>(L.xpo[ns], 1));
+        p.s_tmp = a.carve<double>(L.xvo[ns]);
+    } else {
+        p.zw_tmp = p.gw_tmp = p.s_tmp = nullptr;
+    }
     p.a64 = a.carve<double>((int64_t)p.nb * p.nb);
     if (cfg->precision == FJ_PREC_MIXED) {
         p.a32 = a.carve<float>((int64_t)p.nb * p.nb);
@@ -858,9 +1014,10 @@ static int run_static(const Plan& p, const fj_case_buffers* B, const double* hg,
     if (horseshoe) {
         int64_t rows_tot = 0;
         for (int q = 0; q < L.n_surf; ++q) rows_tot += (int64_t)((L.ms[q] == 0 ? 0 : 1) + 1) * (L.n[q] + 1);
-        init_wake_kernel<<<nblk(rows_tot), 256, 0, s>>>(L, zb, c.flow, c.dt, 1e3, p.hs_zw, 1); note_launch();
+        init_wake_kernel<<<nblk(rows_tot), 256, 0, s>>>(L, zb, c.flow, c.dt, 1e3, p.hs_zw, 1, nullptr); note_launch();
     }
-    init_wake_kernel<<<nblk(L.wvo[L.n_surf]), 256, 0, s>>>(L, zb, c.flow, c.dt, 0.0, zw, 0); note_launch();
+    if (L.any_var && B->d_delta_w == nullptr) return fail(FJ_ERR_SHAPE, "variable_wake set but d_delta_w is NULL");
+    init_wake_kernel<<<nblk(L.wvo[L.n_surf]), 256, 0, s>>>(L, zb, c.flow, c.dt, 0.0, zw, 0, B->d_delta_w); note_launch();
     FJ_LAUNCH_CHECK("static geometry");
     AicArgs aa;
     fill_aic_args(p, aa, zb, B->d_c, B->d_nc, zw_solve, rows_solve);
@@ -962,7 +1119,8 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
     std::vector<RefineJob> ref;
     std::vector<int> free_idx;
     int64_t max_v = 0, max_p = 0, max_w = 0, max_wt = 0, max_f = 0, max_e_free = 0, max_e_wake = 0, max_e_bound = 0;
-    int max_n = 0, max_fil = 0, any_mirror = 0, any_free = 0, any_changed = 0;
+    int max_n = 0, max_fil = 0, any_mirror = 0, any_free = 0, any_changed = 0, any_var = 0;
+    int64_t max_xw = 0, max_cols = 0;
     for (int k = 0; k < K; ++k) {
         BatchItem& it = items[k];
         const Plan& p = it.p;
@@ -1011,6 +1169,15 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
         C.rhs = p.rhs;
         C.v_wake = C.free_wake ? p.v : nullptr;
         C.v_rhs = p.v;
+        if (L.any_var && B->d_delta_w == nullptr)
+            return fail(FJ_ERR_SHAPE, "variable_wake set but d_delta_w is NULL");
+        C.delta_w = B->d_delta_w;
+        C.zw_tmp = p.zw_tmp;
+        C.gw_tmp = p.gw_tmp;
+        C.s_tmp = p.s_tmp;
+        any_var |= L.any_var;
+        max_xw = std::max(max_xw, L.xvo[L.n_surf] + L.xpo[L.n_surf]);
+        max_cols = std::max(max_cols, L.dofo[L.n_surf]);
         C.zeta_ref = (mixed && !it.refactor) ? p.zeta_ref : nullptr;
         C.changed = (mixed && !it.refactor) ? p.flags + 1 : nullptr;
         any_changed |= C.changed != nullptr;
@@ -1135,6 +1302,11 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
         FJ_TRY(launch_sum(jf, cf, d_tab + tl.job_free, d_tab + tl.cta_free, precision, kernel, r_cut, s));
     }
     k_wake_shed<<<dim3(nblk(max_w), K), b, 0, s>>>(dC); note_launch();
+    if (any_var) {  // delta_w surfaces: convect all rows, then re-discretise (aero/utils.py:452-491)
+        k_wake_shed_var<<<dim3(nblk(max_xw), K), b, 0, s>>>(dC); note_launch();
+        k_wake_redisc_z<<<dim3(nblk(max_cols), K), b, 0, s>>>(dC); note_launch();
+        k_wake_redisc_g<<<dim3(nblk(max_cols), K), b, 0, s>>>(dC); note_launch();
+    }
     // 3. AIC (mixed: only where the lattice changed since the factorisation)
     if (any_changed) {
         k_clear_changed<<<dim3(1, K), 32, 0, s>>>(dC); note_launch();

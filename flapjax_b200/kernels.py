@@ -35,8 +35,8 @@ class KernelSpec:
         x = np.asarray(x, dtype=np.float64)
         y = np.asarray(y, dtype=np.float64)
         batch = np.broadcast_shapes(x.shape[:-1], y.shape[:-2])
-        xb = np.ascontiguousarray(np.broadcast_to(x, batch + (3,))).reshape(-1, 3)
-        yb = np.ascontiguousarray(np.broadcast_to(y, batch + (2, 3))).reshape(-1, 2, 3)
+        xb = np.array(np.broadcast_to(x, batch + (3,))).reshape(-1, 3)  # writable copies
+        yb = np.array(np.broadcast_to(y, batch + (2, 3))).reshape(-1, 2, 3)
         dev = device_of(None)
         tx = torch.from_numpy(xb).to(dev)
         ty = torch.from_numpy(yb).to(dev)

@@ -84,7 +84,7 @@ class DeviceCase:
     """Outputs, inputs and workspace of one case on one GPU."""
 
     def __init__(self, cfg: _lib.FjCaseConfig, layout: SurfaceLayout, zeta_b0: np.ndarray, dof_mapping: np.ndarray,
-                 device=None, stream=None):
+                 device=None, stream=None, delta_w: np.ndarray | None = None):
         import torch
 
         self.torch = torch
@@ -102,6 +102,8 @@ class DeviceCase:
         self.force_total = torch.zeros((self.n_tstep, 3), **f64)
         self.zeta_b0 = torch.from_numpy(np.ascontiguousarray(zeta_b0, dtype=np.float64)).to(self.dev)
         self.dof = torch.from_numpy(np.ascontiguousarray(dof_mapping, dtype=np.int32)).to(self.dev)
+        self.delta_w = None if delta_w is None else torch.from_numpy(
+            np.ascontiguousarray(delta_w, dtype=np.float64)).to(self.dev)
         self.hg_t = torch.zeros((self.n_tstep, cfg.n_nodes, 4, 4), **f64)
         self.hg_dot_t = torch.zeros((self.n_tstep, cfg.n_nodes, 4, 4), **f64)
         nbytes = C.c_size_t()
@@ -115,6 +117,7 @@ class DeviceCase:
         b.d_dof_mapping = self.dof.data_ptr()
         b.d_hg_t = self.hg_t.data_ptr()
         b.d_hg_dot_t = self.hg_dot_t.data_ptr()
+        b.d_delta_w = None if self.delta_w is None else self.delta_w.data_ptr()
         b.d_t = self.t.data_ptr()
         for name in FIELDS:
             setattr(b, "d_" + name, self.arrays[name].data_ptr())

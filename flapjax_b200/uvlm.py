@@ -2,10 +2,10 @@
 ``libfj_uvlm.so`` on a B200.
 
 Supported: any number of surfaces, the epsilon / cutoff / plain kernels, mirror images,
-prescribed and free wakes, static (regular or horseshoe wake) and prescribed-motion
-dynamic solves, single-step ``case_solve`` for fluid-structure loops, Constant and
-OneMinusCosine flows.  Not supported (they raise): control surfaces (``grid_func``),
-polar corrections, and the variable wake discretisation ``delta_w``.
+prescribed and free wakes, the variable wake discretisation ``delta_w``, static (regular
+or horseshoe wake) and prescribed-motion dynamic solves, single-step ``case_solve`` for
+fluid-structure loops, Constant and OneMinusCosine flows.  Not supported (they raise):
+control surfaces (``grid_func``) and polar corrections.
 
 ``precision="fp64"`` runs the reference's arithmetic in FP64; ``precision="mixed"`` runs
 the Biot-Savart sums in FP32 (FP64 accumulation) and solves with cached FP32 factors
@@ -154,10 +154,16 @@ class UVLM:
 
     def set_design_variables(self, dt, flowfield: FlowField, zeta_b0, hg0, delta_w=None, reference_cs_angles=None):
         """aero/uvlm.py:387-472."""
-        if delta_w is not None:
-            dws = [delta_w] if isinstance(delta_w, np.ndarray) else list(delta_w)
-            if any(d is not None for d in dws):
-                raise NotImplementedError("the variable wake discretisation (delta_w) is not part of the CUDA path")
+        if isinstance(delta_w, np.ndarray):
+            dws = [delta_w]
+        elif delta_w is None:
+            dws = [None] * self.n_surf
+        elif isinstance(delta_w, Sequence):
+            dws = list(delta_w)
+        else:
+            raise TypeError("Invalid delta_w type")
+        if len(dws) != self.n_surf:
+            raise ValueError(f"Expected {self.n_surf} delta_w entries, got {len(dws)}")
         if reference_cs_angles:
             raise NotImplementedError("control surfaces are not part of the CUDA path")
         if isinstance(zeta_b0, np.ndarray):
@@ -180,7 +186,14 @@ class UVLM:
             self._dt = float(dt)
         else:
             raise TypeError("dt must be either a float or an Array scalar")
-        self.delta_w = [None] * self.n_surf
+        self.delta_w = []
+        for i, dw in enumerate(dws):
+            if dw is None:
+                self.delta_w.append(None)
+            else:
+                dw = np.asarray(dw, dtype=np.float64)
+                check_arr_shape(dw, (self.grid_disc[i].m_star,), "delta_w")
+                self.delta_w.append(dw)
         self.zeta_w_ref = self.initialise_wake()
         self._step_case = None
 
@@ -195,7 +208,8 @@ class UVLM:
         out = ArrayList()
         for i in range(self.n_surf):
             zeta_te = zeta_b[i][-1, :, :]
-            dw = np.ones(self.grid_disc[i].m_star) * self.dt * self.flowfield.u_inf_mag
+            dw = self.delta_w[i] if self.delta_w and self.delta_w[i] is not None else (
+                np.ones(self.grid_disc[i].m_star) * self.dt * self.flowfield.u_inf_mag)
             grid_s = np.concatenate((np.zeros(1), np.cumsum(dw)))
             out.append(zeta_te[None, :, :] + np.outer(grid_s, self.flowfield.u_inf_dir)[:, None, :])
         return out
@@ -221,7 +235,16 @@ class UVLM:
         c.gamma_dot_relaxation = self.gamma_dot_relaxation
         c.flow = self.flowfield.to_c()
         c.precision = _PREC[self.precision]
+        for i, dw in enumerate(self.delta_w or []):
+            c.variable_wake[i] = int(dw is not None)
         return c
+
+    def _delta_w_flat(self):
+        """Concatenated delta_w of every surface (zeros where a surface is uniform), or
+        None when no surface has one."""
+        if not self.delta_w or all(d is None for d in self.delta_w):
+            return None
+        return np.concatenate([np.zeros(g.m_star) if d is None else d for d, g in zip(self.delta_w, self.grid_disc)])
 
     def _layout(self) -> SurfaceLayout:
         return SurfaceLayout(tuple(g.m for g in self.grid_disc), tuple(g.n for g in self.grid_disc),
@@ -237,7 +260,8 @@ class UVLM:
                 raise ValueError(f"dof_mapping[{i}] refers to nodes outside [0, {n_nodes})")
         zeta0 = np.concatenate([z.ravel() for z in self.zeta_b0])
         dof = np.concatenate([d.ravel() for d in self.dof_mapping])
-        return DeviceCase(self._config(n_tstep, n_nodes), self._layout(), zeta0, dof, self.device, stream)
+        return DeviceCase(self._config(n_tstep, n_nodes), self._layout(), zeta0, dof, self.device, stream,
+                          delta_w=self._delta_w_flat())
 
     def _to_case(self, dc: DeviceCase, slots=None, snapshot=False) -> AeroCase:
         h = dc.host_arrays(slots)

@@ -93,6 +93,9 @@ typedef struct fj_case_config {
     double gamma_dot_relaxation;
     fj_flowfield flow;
     int precision;           /* FJ_PREC_* */
+    /* 1: surface s uses the variable wake discretisation (propagate_surf_wake with
+     * delta_w, aero/utils.py:452-491): its segment lengths are d_delta_w's block */
+    int variable_wake[FJ_MAX_SURF];
 } fj_case_config;
 
 /* Device buffers of one case.  Surfaces are concatenated in the innermost extent of
@@ -105,6 +108,8 @@ typedef struct fj_case_buffers {
     const int32_t* d_dof_mapping; /* sum_s (n+1): spanwise vertex -> beam node */
     const double* d_hg_t;      /* (n_tstep, n_nodes, 4, 4) SE(3) node frames */
     const double* d_hg_dot_t;  /* (n_tstep, n_nodes, 4, 4) their time derivatives */
+    const double* d_delta_w;   /* sum_s m_star: wake segment lengths (UVLM.delta_w) of the
+                                  surfaces with variable_wake set; NULL when none is */
     /* outputs, time-major (n_tstep, ...) */
     double* d_t;               /* (n_tstep,) */
     double* d_zeta_b;          /* (m+1, n+1, 3) per surface */

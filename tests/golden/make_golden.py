@@ -91,8 +91,11 @@ def _flow_dict(kind, u_inf, rho, gust=None):
 
 
 def run_case(ref, name, surfaces, dt, flow, kernel="epsilon", r_cut=None, free_wake=False, mirror=None,
-             horseshoe=False, gamma_dot_relaxation=0.7, hg0=None, hg_t=None, hg_dot_t=None):
-    """surfaces: list of (m, n, m_star, zeta_b0, dof_mapping)."""
+             horseshoe=False, gamma_dot_relaxation=0.7, hg0=None, hg_t=None, hg_dot_t=None, delta_w=None):
+    """surfaces: list of (m, n, m_star, zeta_b0, dof_mapping); delta_w: per-surface segment
+    lengths (or None entries) of the variable wake discretisation."""
+    if ONLY and name not in ONLY:
+        return
     jnp = ref.jnp
     kern = {"epsilon": ref.utils.biot_savart_epsilon, "cutoff": ref.utils.biot_savart_cutoff,
             "plain": ref.utils.biot_savart}[kernel]
@@ -112,13 +115,16 @@ def run_case(ref, name, surfaces, dt, flow, kernel="epsilon", r_cut=None, free_w
             ff = ref.OneMinusCosine(jnp.array(flow["u_inf"]), flow["rho"], True,
                                     gust_length=float(flow["gust_length"]),
                                     gust_amplitude=float(flow["gust_amplitude"]))
+        dw_arg = None if delta_w is None else [None if d is None else jnp.array(d) for d in delta_w]
         uv.set_design_variables(dt=float(dt), flowfield=ff, zeta_b0=[jnp.array(z) for *_, z, _ in surfaces],
-                                hg0=jnp.array(hg0))
+                                hg0=jnp.array(hg0), delta_w=dw_arg)
         st = uv.solve_static(horseshoe=horseshoe)
         out = {"case_name": name, "kernel": kernel, "r_cut": r_cut if r_cut is not None else saved_r,
                "free_wake": free_wake, "horseshoe": horseshoe, "dt": dt, "gamma_dot_relaxation": gamma_dot_relaxation,
                "hg0": hg0, "n_surf": len(surfaces), **flow}
         for i, (m, n, ms, z, d) in enumerate(surfaces):
+            if delta_w is not None and delta_w[i] is not None:
+                out[f"surf{i}_delta_w"] = np.asarray(delta_w[i], float)
             out[f"surf{i}_dims"] = np.array([m, n, ms])
             out[f"surf{i}_zeta_b0"] = z
             out[f"surf{i}_dof"] = np.asarray(d)
@@ -143,7 +149,11 @@ def run_case(ref, name, surfaces, dt, flow, kernel="epsilon", r_cut=None, free_w
         ref.utils.R_CUTOFF = saved_r
 
 
+ONLY: set[str] = set()
+
+
 def main():
+    ONLY.update(sys.argv[1:])  # optional case names: regenerate only those
     sys.path.insert(0, str(ROOT))
     from flapjax_b200 import cases
 
@@ -195,6 +205,18 @@ def main():
     hg_dot_t = np.concatenate([wing.hg_dot_t, np.zeros((wing.hg_t.shape[0], 3, 4, 4))], axis=1)
     run_case(ref, "two_surfaces", [(3, 4, 4, wing.zeta_b0, np.arange(5)), (2, 2, 3, tail, np.arange(5, 8))],
              wing.dt, _flow_dict("constant", wing.u_inf, wing.rho), hg0=hg0, hg_t=hg_t, hg_dot_t=hg_dot_t)
+
+    # variable wake discretisation (delta_w): segments growing by 15 % per row, prescribed
+    # heave and free wake
+    c = cases.wing_heave(m=3, n=4, m_star=6, n_steps=5)
+    dw = c.dt * c.u_mag * 1.15 ** np.arange(c.m_star)
+    run_case(ref, "variable_wake_heave", [(c.m, c.n, c.m_star, c.zeta_b0, np.arange(c.n + 1))], c.dt,
+             _flow_dict("constant", c.u_inf, c.rho), hg0=c.hg0, hg_t=c.hg_t, hg_dot_t=c.hg_dot_t, delta_w=[dw])
+    c = cases.wing_free(m=2, n=4, m_star=5, n_steps=4)
+    dw = c.dt * c.u_mag * 1.2 ** np.arange(c.m_star)
+    run_case(ref, "variable_wake_free", [(c.m, c.n, c.m_star, c.zeta_b0, np.arange(c.n + 1))], c.dt,
+             _flow_dict("constant", c.u_inf, c.rho), free_wake=True, hg0=c.hg0, hg_t=c.hg_t, hg_dot_t=c.hg_dot_t,
+             delta_w=[dw])
 
 
 if __name__ == "__main__":

@@ -40,6 +40,11 @@ def _flow(fx, mod):
                               gust_amplitude=float(fx["gust_amplitude"]))
 
 
+def _delta_w(fx):
+    dws = [fx.get(f"surf{i}_delta_w") for i in range(int(fx["n_surf"]))]
+    return None if all(d is None for d in dws) else dws
+
+
 def _mirror(fx):
     return (fx["mirror_point"], fx["mirror_normal"]) if "mirror_point" in fx else (None, None)
 
@@ -55,7 +60,7 @@ def _compare(get, fx, prefix, tol, fields=FIELDS):
 
 
 def test_golden_cases_present():
-    assert len(CASES) >= 8
+    assert len(CASES) >= 10
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -66,7 +71,8 @@ def test_oracle_matches_reference_golden(name):
     uv = R.UVLMRef([(m, n, ms) for m, n, ms, _, _ in surfs], [d for *_, d in surfs], mirror_point=mp,
                    mirror_normal=mn, kernel=str(fx["kernel"]), r_cut=float(fx["r_cut"]),
                    free_wake=bool(fx["free_wake"]), gamma_dot_relaxation=float(fx["gamma_dot_relaxation"]))
-    uv.set_design_variables(float(fx["dt"]), _flow(fx, R), [z for *_, z, _ in surfs], fx["hg0"])
+    uv.set_design_variables(float(fx["dt"]), _flow(fx, R), [z for *_, z, _ in surfs], fx["hg0"],
+                            delta_w=_delta_w(fx))
     st = uv.solve_static(horseshoe=bool(fx["horseshoe"]))
     # most fields agree bit for bit; gamma_b_dot = dGamma / dt magnifies the last-digit
     # differences of the free-wake sums (NumPy einsum grouping), hence 1e-11
@@ -93,7 +99,7 @@ def test_cuda_matches_reference_golden(cuda, name, precision):
                  mirror_point=mp, mirror_normal=mn, kernel=kernel, free_wake=bool(fx["free_wake"]),
                  gamma_dot_relaxation=float(fx["gamma_dot_relaxation"]), precision=precision)
     uv.set_design_variables(dt=float(fx["dt"]), flowfield=_flow(fx, fj), zeta_b0=[z for *_, z, _ in surfs],
-                            hg0=fx["hg0"])
+                            hg0=fx["hg0"], delta_w=_delta_w(fx))
     tol_b = 1e-10 if precision == "fp64" else 1e-5
     st = uv.solve_static(horseshoe=bool(fx["horseshoe"]))
     _compare(lambda f: getattr(st, f), fx, "static", tol_b,

@@ -103,3 +103,35 @@ def test_serving_loop_results_match_alone(cuda):
         for f in FIELDS:
             for a, b in zip(getattr(got, f), getattr(want, f)):
                 assert rel_err(a, b) < 1e-6, (k, f, rel_err(a, b))
+
+
+def test_batched_variable_and_uniform_wakes(cuda):
+    """A delta_w case and a uniform-wake case in one batch (FP64): as alone."""
+    from flapjax_b200.serving import BatchStepper
+
+    mix = [cases.wing_heave(m=3, n=8, m_star=9, n_steps=5, seed=7), cases.wing_heave(m=4, n=6, m_star=7, n_steps=5)]
+    dws = [mix[0].dt * 1.1 ** np.arange(mix[0].m_star), None]
+    outs = []
+    for mode in ("alone", "batch"):
+        uvs, dcs, res = [], [], []
+        for c, dw in zip(mix, dws):
+            uv, ff = device_uvlm(c, "fp64")
+            uv.set_design_variables(dt=c.dt, flowfield=ff, zeta_b0=c.zeta_b0, hg0=c.hg0, delta_w=dw)
+            if mode == "alone":
+                res.append(uv.solve_prescribed_dynamic(uv.solve_static(), c.hg_t, c.hg_dot_t))
+            else:
+                dc = uv.make_device_case(c.n_tstep)
+                uv.load_initial(dc, uv.solve_static())
+                dc.set_hg(c.hg_t, c.hg_dot_t)
+                uvs.append(uv)
+                dcs.append(dc)
+        if mode == "batch":
+            st = BatchStepper(4, cuda)
+            for i in range(1, mix[0].n_tstep):
+                st.step(dcs, [i, i], [i > 1, i > 1])
+            res = [uv._to_case(dc) for uv, dc in zip(uvs, dcs)]
+        outs.append(res)
+    for got, want in zip(outs[1], outs[0]):
+        for f in FIELDS:
+            for a, b in zip(getattr(got, f), getattr(want, f)):
+                assert rel_err(a, b) < 1e-12, f

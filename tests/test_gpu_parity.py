@@ -323,3 +323,28 @@ def test_full_heave_config_fp64_and_mixed(cuda):
     assert np.max(np.abs(cdm - cd64)) / np.max(np.abs(cd64)) < 3e-6
     clr, _ = coefficients(oracle_force_total(want), c)
     assert np.max(np.abs(cl64 - clr) / np.abs(clr)) < TOL64
+
+
+@pytest.mark.parametrize("free", [False, True])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_variable_wake_matches_oracle(cuda, free, precision):
+    """delta_w (propagate_surf_wake's re-discretisation, aero/utils.py:452-491): wake
+    segments growing 12 % per row; FP64 within 1e-10 of the oracle, mixed within 1e-4."""
+    if free:
+        c = cases.wing_free(m=4, n=10, m_star=14, n_steps=8)
+    else:
+        c = cases.wing_heave(m=4, n=10, m_star=14, n_steps=8)
+    dw = c.dt * c.u_mag * 1.12 ** np.arange(c.m_star)
+    uv, ff = device_uvlm(c, precision)
+    uv.set_design_variables(dt=c.dt, flowfield=ff, zeta_b0=c.zeta_b0, hg0=c.hg0, delta_w=dw)
+    ur, ffr = oracle_uvlm(c)
+    ur.set_design_variables(c.dt, ffr, c.zeta_b0, c.hg0, delta_w=dw)
+    got = uv.solve_prescribed_dynamic(uv.solve_static(), c.hg_t, c.hg_dot_t)
+    want = ur.solve_prescribed_dynamic(ur.solve_static(), c.hg_t, c.hg_dot_t)
+    if precision == "fp64":
+        _compare_case(got, want, TOL64)
+    else:
+        _compare_case(got, want, 1e-4, fields=("gamma_b", "gamma_w", "zeta_w", "f_steady"))
+    # the wake really follows delta_w: first-column segment lengths at the last step
+    seg = np.linalg.norm(np.diff(got.zeta_w[0][-1][:, 0], axis=0), axis=-1)
+    assert np.all(seg[1:] > seg[:-1])
