@@ -340,7 +340,7 @@ int lu_solve_t64(const double* lu, int n, const int32_t* piv, double* b, double*
             trsv_t_update_kernel<<<(i0 + 127) / 128, 128, 0, s>>>(lu, n, i0, bw, 0, i0, work); note_launch();
         }
     }
-    FJ_CUDA(cudaFuncSetAttribute(unpermute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(n * sizeof(int))));
+    FJ_TRY(allow_dynamic_smem((const void*)unpermute_kernel, (size_t)(n * sizeof(int))));
     unpermute_kernel<<<1, 1024, n * sizeof(int), s>>>(piv, n, work, b); note_launch();
     FJ_LAUNCH_CHECK("lu_solve_t64");
     return FJ_OK;

@@ -148,15 +148,15 @@ int aic_launch_jobs(const AicArgs* d_tab, int n_jobs, int64_t max_rows, int max_
     dim3 g((unsigned)max_rows, (unsigned)n_jobs);
     switch (kernel) {
         case FJ_KERNEL_EPSILON:
-            FJ_CUDA(cudaFuncSetAttribute(aic_jobs_kernel<FJ_KERNEL_EPSILON>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            FJ_TRY(allow_dynamic_smem((const void*)aic_jobs_kernel<FJ_KERNEL_EPSILON>, (size_t)smem));
             aic_jobs_kernel<FJ_KERNEL_EPSILON><<<g, 256, smem, s>>>(d_tab); note_launch();
             break;
         case FJ_KERNEL_CUTOFF:
-            FJ_CUDA(cudaFuncSetAttribute(aic_jobs_kernel<FJ_KERNEL_CUTOFF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            FJ_TRY(allow_dynamic_smem((const void*)aic_jobs_kernel<FJ_KERNEL_CUTOFF>, (size_t)smem));
             aic_jobs_kernel<FJ_KERNEL_CUTOFF><<<g, 256, smem, s>>>(d_tab); note_launch();
             break;
         case FJ_KERNEL_PLAIN:
-            FJ_CUDA(cudaFuncSetAttribute(aic_jobs_kernel<FJ_KERNEL_PLAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            FJ_TRY(allow_dynamic_smem((const void*)aic_jobs_kernel<FJ_KERNEL_PLAIN>, (size_t)smem));
             aic_jobs_kernel<FJ_KERNEL_PLAIN><<<g, 256, smem, s>>>(d_tab); note_launch();
             break;
         default:
@@ -173,15 +173,15 @@ int aic_launch(const AicArgs& a, const int* d_run_flag, cudaStream_t s) {
     if (a.n_rows == 0) return FJ_OK;
     switch (a.kernel) {
         case FJ_KERNEL_EPSILON:
-            FJ_CUDA(cudaFuncSetAttribute(aic_kernel<FJ_KERNEL_EPSILON>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            FJ_TRY(allow_dynamic_smem((const void*)aic_kernel<FJ_KERNEL_EPSILON>, (size_t)smem));
             aic_kernel<FJ_KERNEL_EPSILON><<<(unsigned)a.n_rows, 256, smem, s>>>(a, d_run_flag); note_launch();
             break;
         case FJ_KERNEL_CUTOFF:
-            FJ_CUDA(cudaFuncSetAttribute(aic_kernel<FJ_KERNEL_CUTOFF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            FJ_TRY(allow_dynamic_smem((const void*)aic_kernel<FJ_KERNEL_CUTOFF>, (size_t)smem));
             aic_kernel<FJ_KERNEL_CUTOFF><<<(unsigned)a.n_rows, 256, smem, s>>>(a, d_run_flag); note_launch();
             break;
         case FJ_KERNEL_PLAIN:
-            FJ_CUDA(cudaFuncSetAttribute(aic_kernel<FJ_KERNEL_PLAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            FJ_TRY(allow_dynamic_smem((const void*)aic_kernel<FJ_KERNEL_PLAIN>, (size_t)smem));
             aic_kernel<FJ_KERNEL_PLAIN><<<(unsigned)a.n_rows, 256, smem, s>>>(a, d_run_flag); note_launch();
             break;
         default:

@@ -27,6 +27,11 @@ int fail(int code, const char* fmt, ...);
 // Count of kernels this library has launched (read through fj_launch_count).
 void note_launch(int n = 1);
 
+// Raise a kernel's dynamic shared-memory limit on the current device to at least
+// `bytes`.  The limit only ever grows, under a lock, so host threads launching the same
+// kernel on different streams never lower each other's limit between set and launch.
+int allow_dynamic_smem(const void* func, size_t bytes);
+
 // Opt-in timing of the Biot-Savart sum kernels with CUDA events on their stream
 // (fj_profile_begin / fj_profile_end).  prof_start returns -1 when profiling is off.
 int prof_start(cudaStream_t s);

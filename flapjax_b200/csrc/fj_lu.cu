@@ -176,7 +176,7 @@ static int lu_factor_impl(T* a, int n, int32_t* piv, int* d_info, cudaStream_t s
     if (n <= 0) return fail(FJ_ERR_SHAPE, "lu_factor: n=%d", n);
     const size_t smem = (size_t)n * (NB + 1) * sizeof(T);
     if (smem > 220 * 1024) return fail(FJ_ERR_UNSUPPORTED, "lu_factor: n=%d too large for the shared-memory panel", n);
-    FJ_CUDA(cudaFuncSetAttribute(lu_panel_kernel<T, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FJ_TRY(allow_dynamic_smem((const void*)lu_panel_kernel<T, NB>, (size_t)smem));
     FJ_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int), s));
     for (int k = 0; k < n; k += NB) {
         const int nb = min(NB, n - k);
@@ -277,8 +277,8 @@ int lu_solve64(const double* lu, int n, const int32_t* piv, double* b, double* w
     if (n <= 0) return fail(FJ_ERR_SHAPE, "lu_solve: n=%d", n);
     if ((size_t)n * sizeof(int) > 220 * 1024) return fail(FJ_ERR_UNSUPPORTED, "lu_solve: n=%d too large", n);
     const size_t dsm = (size_t)kTrsvBlk * (kTrsvBlk + 1) * sizeof(double);
-    FJ_CUDA(cudaFuncSetAttribute(permute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(n * sizeof(int))));
-    FJ_CUDA(cudaFuncSetAttribute(trsv_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
+    FJ_TRY(allow_dynamic_smem((const void*)permute_kernel, (size_t)(n * sizeof(int))));
+    FJ_TRY(allow_dynamic_smem((const void*)trsv_diag_kernel, (size_t)dsm));
     permute_kernel<<<1, 1024, n * sizeof(int), s>>>(piv, n, b, work); note_launch();
     const int wpb = 8;
     for (int i0 = 0; i0 < n; i0 += kTrsvBlk) {  // forward, unit lower
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(512) lu_inverse32_kernel(const float* __restri
 int lu_inverse32(const float* lu, int n, const int32_t* piv, float* x, cudaStream_t s) {
     const size_t smem = (size_t)n * kInvCols * sizeof(float);
     if (smem > 220 * 1024) return fail(FJ_ERR_UNSUPPORTED, "lu_inverse32: n=%d too large", n);
-    FJ_CUDA(cudaFuncSetAttribute(lu_inverse32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FJ_TRY(allow_dynamic_smem((const void*)lu_inverse32_kernel, (size_t)smem));
     lu_inverse32_kernel<<<(n + kInvCols - 1) / kInvCols, 512, smem, s>>>(lu, n, piv, x); note_launch();
     FJ_LAUNCH_CHECK("lu_inverse32_kernel");
     return FJ_OK;

@@ -15,6 +15,7 @@
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -44,6 +45,20 @@ const char* last_error() { return g_err; }
 
 static std::atomic<int64_t> g_launches{0};
 void note_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+int allow_dynamic_smem(const void* func, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> limit;
+    int dev = 0;
+    FJ_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> g(mu);
+    size_t& cur = limit[{dev, func}];
+    if (bytes > cur) {
+        FJ_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        cur = bytes;
+    }
+    return FJ_OK;
+}
 int64_t launch_count() { return g_launches.load(); }
 
 struct ProfState {
@@ -645,16 +660,20 @@ constexpr int kT32 = 2;
 // CTAs resident per SM for the sum kernels and the SM count, queried once.
 static int g_sms = 0, g_res64 = 0, g_res32 = 0;
 
+static std::once_flag g_occ_once;
+
 static void query_occupancy() {
-    if (g_sms > 0) return;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_res64, vind64_kernel<FJ_KERNEL_EPSILON, kT64>, kBlock, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_res32, vind32_kernel<FJ_KERNEL_CUTOFF, kT32>, kBlock, 0);
-    if (g_sms <= 0) g_sms = 148;
-    if (g_res64 <= 0) g_res64 = 1;
-    if (g_res32 <= 0) g_res32 = 1;
+    std::call_once(g_occ_once, [] {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        int sms = 0, r64 = 0, r32 = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r64, vind64_kernel<FJ_KERNEL_EPSILON, kT64>, kBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r32, vind32_kernel<FJ_KERNEL_CUTOFF, kT32>, kBlock, 0);
+        g_res64 = r64 > 0 ? r64 : 1;
+        g_res32 = r32 > 0 ? r32 : 1;
+        g_sms = sms > 0 ? sms : 148;
+    });
 }
 
 // Split the stream so that (target blocks) x (splits) fills whole waves: the smallest

@@ -6,10 +6,17 @@ loop advances every active case by one time step per iteration with a single set
 kernel launches (``fj_step_batched``), admits waiting cases as device memory frees up
 (admission by footprint), and retires finished cases.  Per-step latency is the device
 time of the batched iteration a case's step ran in, measured with CUDA events.
+
+With ``overlap_admission`` (the default) ``admission_workers`` host threads admit cases,
+each on its own CUDA stream -- static solve and first, factorising step, which are
+latency-bound LU panels -- while the batched steps of the active cases run on the main
+stream; a case joins the batch once its admission event has completed.
 """
 from __future__ import annotations
 
 import ctypes as C
+import queue
+import threading
 import time
 from dataclasses import dataclass, field
 
@@ -130,7 +137,7 @@ class ServingLoop:
     """
 
     def __init__(self, memory_budget: int, max_active: int = 256, device=None, keep_results=True,
-                 admit_per_iteration: int = 4):
+                 admit_per_iteration: int = 4, overlap_admission: bool = True, admission_workers: int = 4):
         import torch
 
         from .runtime import device_of
@@ -142,16 +149,21 @@ class ServingLoop:
         self.stepper = BatchStepper(max_active, self.dev)
         self.keep_results = keep_results
         self.admit_per_iteration = admit_per_iteration
+        self.overlap_admission = overlap_admission
+        self.admission_workers = max(1, int(admission_workers))
 
-    def _admit(self, req: Request, now: float) -> _Active:
+    def _admit(self, req: Request, now: float, stream=None) -> _Active:
         """Static solve and the first (factorising) step run for the case alone, so the
-        batched steps it joins reuse its cached factors and stay uniform."""
+        batched steps it joins reuse its cached factors and stay uniform.  The static
+        solve writes slot 0 of the case in place (the frames of the reference
+        configuration, ``UVLM.solve_static()``), so nothing crosses to the host."""
         uv = req.uvlm
         n_tstep = req.hg_t.shape[0]
-        init = uv.solve_static()
-        dc = uv.make_device_case(n_tstep, req.hg_t.shape[1])
-        uv.load_initial(dc, init)
+        dc = uv.make_device_case(n_tstep, req.hg_t.shape[1], stream=stream)
         dc.set_hg(req.hg_t, req.hg_dot_t)
+        dc.hg_t[0].copy_(self.torch.from_numpy(np.ascontiguousarray(uv.hg_ref, dtype=np.float64)))
+        dc.solve_static(False, 0.0)
+        dc.hg_t[0].copy_(self.torch.from_numpy(np.ascontiguousarray(req.hg_t[0], dtype=np.float64)))
         first = 1
         if n_tstep > 1:
             dc.solve_dynamic(1, 2)
@@ -164,6 +176,120 @@ class ServingLoop:
         a.dc = None
 
     def run(self, requests: list[Request], realtime: bool = True) -> ServeResult:
+        if self.overlap_admission:
+            return self._run_overlapped(requests, realtime)
+        return self._run_serial(requests, realtime)
+
+    def _run_overlapped(self, requests: list[Request], realtime: bool) -> ServeResult:
+        torch = self.torch
+        pending = sorted(requests, key=lambda r: r.arrival)
+        n_total = len(pending)
+        cond = threading.Condition()
+        state = {"used": 0, "inflight": 0, "error": None, "next": 0}
+        ready: queue.Queue = queue.Queue()
+        t0 = time.perf_counter()
+
+        def worker():
+            try:
+                torch.cuda.set_device(self.dev)
+                adm_stream = torch.cuda.Stream(self.dev)
+                while True:
+                    with cond:  # requests are taken in arrival order
+                        k = state["next"]
+                        if k >= n_total or state["error"] is not None:
+                            return
+                        state["next"] = k + 1
+                    req = pending[k]
+                    if realtime:
+                        wait = req.arrival - (time.perf_counter() - t0)
+                        if wait > 0:
+                            time.sleep(wait)
+                    est = case_footprint_bytes(req.uvlm, req.hg_t.shape[0])
+                    with cond:
+                        # footprint budget and batch width; an empty system always admits
+                        while state["inflight"] > 0 and (state["used"] + est > self.memory_budget
+                                                         or state["inflight"] >= self.max_active):
+                            cond.wait()
+                        state["used"] += est
+                        state["inflight"] += 1
+                    with torch.cuda.stream(adm_stream):
+                        a = self._admit(req, time.perf_counter() - t0, stream=adm_stream)
+                        a.footprint = est
+                        ev = torch.cuda.Event()
+                        ev.record(adm_stream)
+                    ready.put((a, ev, time.perf_counter() - t0))
+            except BaseException as e:  # surfaced by the stepping loop
+                state["error"] = e
+                ready.put(None)
+
+        threads = [threading.Thread(target=worker, daemon=True) for _ in range(self.admission_workers)]
+        for th in threads:
+            th.start()
+        active: list[_Active] = []
+        results = {}
+        lat, admit_lat = [], []
+        busy_s = 0.0
+        steps = 0
+        max_act = 0
+        received = 0
+        stream = torch.cuda.current_stream(self.dev)
+
+        def release(a):
+            with cond:
+                state["used"] -= a.footprint
+                state["inflight"] -= 1
+                cond.notify_all()
+
+        while received < n_total or active:
+            # take every admitted case; block only when nothing is running
+            while received < n_total:
+                try:
+                    item = ready.get(block=not active, timeout=None if not active else 0)
+                except queue.Empty:
+                    break
+                if item is None:
+                    raise state["error"]
+                a, ev, done_at = item
+                received += 1
+                stream.wait_event(ev)
+                a.dc.stream = None  # from here on the case lives on the stepping stream
+                if a.next_slot > 1:
+                    steps += 1
+                admit_lat.append(max(0.0, done_at - a.req.arrival) if realtime else 0.0)
+                if a.next_slot >= a.n_tstep:
+                    ev.synchronize()
+                    self._retire(a, results)
+                    release(a)
+                else:
+                    active.append(a)
+            if not active:
+                continue
+            max_act = max(max_act, len(active))
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            self.stepper.step([a.dc for a in active], [a.next_slot for a in active],
+                              [a.next_slot > 1 for a in active], stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            busy_s += ms * 1e-3
+            for a in active:
+                a.step_ms.append(ms)
+                lat.append(ms)
+                a.next_slot += 1
+                steps += 1
+            done = [a for a in active if a.next_slot >= a.n_tstep]
+            for a in done:
+                self._retire(a, results)
+                active.remove(a)
+                release(a)
+        for th in threads:
+            th.join()
+        wall = time.perf_counter() - t0
+        return ServeResult(results, np.asarray(lat), steps, wall, busy_s, np.asarray(admit_lat), max_act)
+
+    def _run_serial(self, requests: list[Request], realtime: bool) -> ServeResult:
         torch = self.torch
         pending = sorted(requests, key=lambda r: r.arrival)
         active: list[_Active] = []

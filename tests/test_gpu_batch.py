@@ -80,7 +80,8 @@ def test_batched_free_wake_and_mirror(cuda):
                 assert rel_err(a, b) < 1e-12, f
 
 
-def test_serving_loop_results_match_alone(cuda):
+@pytest.mark.parametrize("overlap", [True, False])
+def test_serving_loop_results_match_alone(cuda, overlap):
     from flapjax_b200.serving import Request, ServingLoop
 
     rng = np.random.default_rng(0)
@@ -92,12 +93,14 @@ def test_serving_loop_results_match_alone(cuda):
         alone[k] = uv.solve_prescribed_dynamic(uv.solve_static(), c.hg_t, c.hg_dot_t)
         uv2, _ = device_uvlm(c, "mixed")
         reqs.append(Request(uv2, c.hg_t, c.hg_dot_t, arrival=0.01 * k, tag=k))
-    loop = ServingLoop(memory_budget=1 << 30, max_active=4, device=cuda)
+    loop = ServingLoop(memory_budget=1 << 30, max_active=4, device=cuda, overlap_admission=overlap)
     out = loop.run(reqs, realtime=False)
     summ = out.summary()
     assert summ["case_steps"] == sum(r.hg_t.shape[0] - 1 for r in reqs)
     assert summ["p99_step_ms"] >= summ["p50_step_ms"] > 0
-    assert summ["max_active"] == 4
+    # serial admission fills the batch 4 at a time; overlapped admission lets cases join
+    # as the admission thread finishes them, so the batch may stay narrower
+    assert summ["max_active"] == 4 if not overlap else 1 <= summ["max_active"] <= 4
     for k, want in alone.items():
         got = out.results[k]
         for f in FIELDS:
