@@ -296,18 +296,19 @@ def main():
 
     from flapjax_b200 import _lib
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
+    from flapjax_b200 import replicas
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    rank, world, local = replicas.rank_env()
+    torch.cuda.set_device(local)
+    replicas.init("nccl")
     dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
     if args.only_serving:
-        print(json.dumps({"serving": serving_bench(args, torch)}))
+        serving = serving_bench(args, torch)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"serving": serving}))
         return 0
     assert args.warmup >= 3, "at least 3 warm-up steps"
     K, W = args.steps, args.warmup
@@ -326,11 +327,8 @@ def main():
         ms, prof = run_device_steps(dc, 1 + W, n_slots, flush, torch, profile=True)
     launches = _lib.load().fj_launch_count() - launches0
     torch.cuda.synchronize()
-    t_ms = sum(ms)
+    t_ms = replicas.max_over_ranks(sum(ms), dev)
     if world > 1:
-        tt = torch.tensor([t_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
         dist.barrier()
     value = world * K / (t_ms * 1e-3)
     ft_mixed = dc.force_total[1 + W:n_slots].cpu().numpy()
@@ -396,11 +394,7 @@ def main():
         if world > 1:
             dist.barrier()
         ms_e, bi, bo = e2e_run(uv2, dce, case, 1 + W, n_slots, torch)
-        te = sum(ms_e)
-        if world > 1:
-            tt = torch.tensor([te], device=dev, dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            te = float(tt.item())
+        te = replicas.max_over_ranks(sum(ms_e), dev)
         e2e = {"value": world * K / (te * 1e-3), "unit": UNIT, "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo}
         del dce
 
@@ -431,9 +425,11 @@ def main():
 def serving_bench(args, torch):
     """Config 5: Poisson arrivals (200/s) of heaving wings with M ~ U{4..16},
     N ~ U{16..128}, W ~ U{20..200}, AoA ~ U[0, 8] deg, 100 steps each, mixed precision,
-    continuously batched.  Reports whole-stream throughput and per-step latency."""
+    continuously batched.  Reports whole-stream throughput and per-step latency.  With
+    several ranks each serves every world-th arrival of the same stream (no collective
+    on the data path); rank 0 merges the summaries."""
     import flapjax_b200 as fj
-    from flapjax_b200 import cases
+    from flapjax_b200 import cases, replicas
     from flapjax_b200.serving import Request, ServingLoop
 
     n = args.serving_cases
@@ -447,12 +443,19 @@ def serving_bench(args, torch):
             out.append(Request(uv, c.hg_t, c.hg_dot_t, arrival=float(t), tag=k))
         return out
 
+    rank, world, _ = replicas.rank_env()
     free = torch.cuda.mem_get_info()[0]
     loop = ServingLoop(memory_budget=int(0.5 * free), max_active=512, keep_results=False)
     loop.run(requests()[:8], realtime=False)  # warm-up (module load, allocator)
     torch.cuda.synchronize()
-    res = loop.run(requests(), realtime=True)
-    summ = res.summary()
+    res = loop.run(replicas.shard(requests(), rank, world), realtime=True)
+    part = {"case_steps": res.case_steps, "wall_s": res.wall_s, "gpu_busy_s": res.gpu_busy_s,
+            "step_latency_ms": res.step_latency_ms.tolist(), "admit_latency_s": res.admit_latency_s.tolist(),
+            "max_active": res.max_active}
+    parts = replicas.gather_to_root(part)
+    if parts is None:
+        return None
+    summ = replicas.merge_serving(parts)
     summ.update({"cases": n, "arrival_rate_per_s": 200.0, "steps_per_case": 100,
                  "workload": "heaving wings, M~U{4..16}, N~U{16..128}, W~U{20..200}, AoA~U[0,8] deg, mixed precision",
                  "pairs_total": float(sum(c.pairs_per_step() * c.n_steps for c in stream))})
