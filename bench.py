@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--small", action="store_true", help="a reduced workload (for quick checks)")
     ap.add_argument("--serving-cases", type=int, default=512, help="cases in the serving stream (0: skip)")
     ap.add_argument("--only-serving", action="store_true")
+    ap.add_argument("--configs", action="store_true",
+                    help="the per-config table instead of the headline line: C1 heave 8x32/W64/50 steps, "
+                         "C2 free wake 16x128/W200, C3 pitch 12x64/W100 primal")
     return ap.parse_args()
 
 
@@ -302,6 +305,10 @@ def main():
     torch.cuda.set_device(local)
     replicas.init("nccl")
     dev = torch.device("cuda", local)
+    if args.configs:
+        if rank == 0:
+            print(json.dumps({"configs": config_table(args, torch)}))
+        return 0
     if args.only_serving:
         serving = serving_bench(args, torch)
         if world > 1:
@@ -420,6 +427,66 @@ def main():
     }
     print(json.dumps(line))
     return 0
+
+
+def config_table(args, torch):
+    """Steps/s of the mixed and plain FP64 GPU paths and of the C++ FP64 oracle (1 thread
+    and every host thread) on each single-case configuration, with the mixed path's CL/CD
+    error against the FP64 path.  Prescribed wakes: the error over the whole run; the
+    free wake (chaotic): the one-step error (FP64 state in, one mixed step)."""
+    from flapjax_b200 import cases
+
+    rows = {}
+    specs = [("C1", cases.wing_heave(), 50), ("C2", cases.wing_free(n_steps=60), 60),
+             ("C3", cases.wing_pitch(n_steps=200), 200)]
+    for name, case, n_steps in specs:
+        n_slots = n_steps + 1
+        res = {"m": case.m, "n": case.n, "m_star": case.m_star, "steps": n_steps, "free_wake": case.free_wake,
+               "pairs_per_step": case.pairs_per_step()}
+        for prec in ("mixed", "fp64"):
+            _, dc = make_case(case, prec, n_slots)
+            run_device_steps(dc, 1, 4, None, torch)  # warm-up and the first (factorising) step
+            ms, _ = run_device_steps(dc, 4, n_slots, None, torch)
+            res[f"{prec}_steps_per_s"] = (n_slots - 4) / (sum(ms) * 1e-3)
+            res[f"{prec}_ms_per_step"] = sum(ms) / (n_slots - 4)
+            res[f"_{prec}_dc"] = dc
+        dm, d64 = res.pop("_mixed_dc"), res.pop("_fp64_dc")
+        res["speedup_mixed_over_fp64"] = res["mixed_steps_per_s"] / res["fp64_steps_per_s"]
+        cl64, cd64 = coeffs(d64.force_total[1:].cpu().numpy(), case)
+        if case.free_wake:
+            errs = []
+            for i in np.linspace(2, n_slots - 1, 5).astype(int):
+                dm.copy_slot_from(d64, i - 1)
+                dm.solve_dynamic(i, i + 1, reuse_factors=True)
+                cl_i, cd_i = coeffs(dm.force_total[i].cpu().numpy()[None], case)
+                errs.append((abs(cl_i[0] - cl64[i - 1]) / abs(cl64[i - 1]),
+                             abs(cd_i[0] - cd64[i - 1]) / np.max(np.abs(cd64))))
+            res["cl_rel_err_one_step_max"] = max(e[0] for e in errs)
+            res["cd_rel_err_one_step_max"] = max(e[1] for e in errs)
+            res["cd_err_over_max_cl_one_step"] = res["cd_rel_err_one_step_max"] * float(
+                np.max(np.abs(cd64)) / np.max(np.abs(cl64)))
+        else:
+            clm, cdm = coeffs(dm.force_total[1:].cpu().numpy(), case)
+            res["cl_rel_err_max"] = float(np.max(np.abs(clm - cl64) / np.abs(cl64)))
+            res["cd_rel_err_max_of_max"] = float(np.max(np.abs(cdm - cd64)) / np.max(np.abs(cd64)))
+            # CD is a small projection of a force that is mostly lift: its error measured
+            # against the lift scale shows the force accuracy itself
+            res["cd_err_over_max_cl"] = float(np.max(np.abs(cdm - cd64)) / np.max(np.abs(cl64)))
+            res["max_cd_over_max_cl"] = float(np.max(np.abs(cd64)) / np.max(np.abs(cl64)))
+        del dm, d64
+        th = host_threads()
+        cpu_case = type(case)(**{**case.__dict__})
+        v_all, t_all = cpu_steps(cpu_case, th, 1, min(10, n_steps - 1), 10.0)
+        if case.free_wake:  # a free-wake step takes ~25 s on one core: sample its pair rate
+            v_one, t_one = cpu_single_thread(cpu_case, 5.0)["value"], []
+        else:
+            v_one, t_one = cpu_steps(cpu_case, 1, 1, min(3, n_steps - 1), 10.0)
+        res["cpu_all_threads_steps_per_s"] = v_all
+        res["cpu_threads"] = th
+        res["cpu_1_thread_steps_per_s"] = v_one
+        res["cpu_sample_steps"] = [len(t_all), len(t_one)]
+        rows[name] = res
+    return rows
 
 
 def serving_bench(args, torch):

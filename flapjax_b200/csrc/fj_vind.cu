@@ -399,6 +399,7 @@ constexpr int kDup = 6;  // float4 per staged element
 // Six resident CTAs per SM (registers capped at 80): the sum is FMA-pipe bound and the
 // extra warps hide the MUFU and FMA latencies better than the registers they cost.
 constexpr int kMinCtas32 = 6;
+constexpr int kFold = 16;  // elements per FP32 partial sum (even: the ping-pong takes pairs)
 
 __device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
 
@@ -528,41 +529,46 @@ __device__ __forceinline__ void vind32_body(const double* __restrict__ tgt, int6
             __syncthreads();
             for (int k = threadIdx.x; k <= cnt; k += kBlock) stage_dup(s4, c0 - 1 + k, sh + k * kDup);
             __syncthreads();
-            float2 accf[P][3];
+            // FP32 partial sums over kFold elements, folded into the FP64 accumulators:
+            // bounds the FP32 summation error to that of a 16-term sum
+            for (int f0 = 0; f0 < cnt; f0 += kFold) {
+                const int fend = min(cnt, f0 + kFold);
+                float2 accf[P][3];
 #pragma unroll
-            for (int p = 0; p < P; ++p) accf[p][0] = accf[p][1] = accf[p][2] = make_float2(0.f, 0.f);
-            // Chain breaks carry g = 0 and a q that keeps their (discarded) term finite,
-            // so every element is processed without a branch.
-            int i = 0;
-            for (; i + 2 <= cnt; i += 2) {
-                const float4* e = sh + i * kDup;  // slots i, i+1, i+2
+                for (int p = 0; p < P; ++p) accf[p][0] = accf[p][1] = accf[p][2] = make_float2(0.f, 0.f);
+                // Chain breaks carry g = 0 and a q that keeps their (discarded) term
+                // finite, so every element is processed without a branch.
+                int i = f0;
+                for (; i + 2 <= fend; i += 2) {
+                    const float4* e = sh + i * kDup;  // slots i, i+1, i+2
 #pragma unroll
-                for (int p = 0; p < P; ++p) {
-                    vtx32x2(xh[p], xl[p], e + kDup, B[p]);
-                    link32x2<KER>(A[p], B[p], e + 3, accf[p]);
+                    for (int p = 0; p < P; ++p) {
+                        vtx32x2(xh[p], xl[p], e + kDup, B[p]);
+                        link32x2<KER>(A[p], B[p], e + 3, accf[p]);
+                    }
+#pragma unroll
+                    for (int p = 0; p < P; ++p) {
+                        vtx32x2(xh[p], xl[p], e + 2 * kDup, A[p]);
+                        link32x2<KER>(B[p], A[p], e + kDup + 3, accf[p]);
+                    }
+                }
+                if (i < fend) {
+                    const float4* e = sh + i * kDup;
+#pragma unroll
+                    for (int p = 0; p < P; ++p) {
+                        vtx32x2(xh[p], xl[p], e + kDup, B[p]);
+                        link32x2<KER>(A[p], B[p], e + 3, accf[p]);
+                        A[p] = B[p];
+                    }
                 }
 #pragma unroll
-                for (int p = 0; p < P; ++p) {
-                    vtx32x2(xh[p], xl[p], e + 2 * kDup, A[p]);
-                    link32x2<KER>(B[p], A[p], e + kDup + 3, accf[p]);
-                }
+                for (int p = 0; p < P; ++p)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        acc[2 * p][c] += (double)accf[p][c].x;
+                        acc[2 * p + 1][c] += (double)accf[p][c].y;
+                    }
             }
-            if (i < cnt) {
-                const float4* e = sh + i * kDup;
-#pragma unroll
-                for (int p = 0; p < P; ++p) {
-                    vtx32x2(xh[p], xl[p], e + kDup, B[p]);
-                    link32x2<KER>(A[p], B[p], e + 3, accf[p]);
-                    A[p] = B[p];
-                }
-            }
-#pragma unroll
-            for (int p = 0; p < P; ++p)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    acc[2 * p][c] += (double)accf[p][c].x;
-                    acc[2 * p + 1][c] += (double)accf[p][c].y;
-                }
         }
     }
 #pragma unroll
