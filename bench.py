@@ -446,9 +446,19 @@ def config_table(args, torch):
         for prec in ("mixed", "fp64"):
             _, dc = make_case(case, prec, n_slots)
             run_device_steps(dc, 1, 4, None, torch)  # warm-up and the first (factorising) step
-            ms, _ = run_device_steps(dc, 4, n_slots, None, torch)
-            res[f"{prec}_steps_per_s"] = (n_slots - 4) / (sum(ms) * 1e-3)
-            res[f"{prec}_ms_per_step"] = sum(ms) / (n_slots - 4)
+            # steps 4.. as one call (UVLM.solve_prescribed_dynamic): launched step by step,
+            # then replayed from a captured step graph
+            for graph in (False, True):
+                st = torch.cuda.current_stream()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                dc.solve_dynamic(4, n_slots, reuse_factors=True, graph=graph)
+                e1.record(st)
+                e1.synchronize()
+                ms = e0.elapsed_time(e1)
+                key = prec if graph else f"{prec}_no_graph"
+                res[f"{key}_steps_per_s"] = (n_slots - 4) / (ms * 1e-3)
+                res[f"{key}_ms_per_step"] = ms / (n_slots - 4)
             res[f"_{prec}_dc"] = dc
         dm, d64 = res.pop("_mixed_dc"), res.pop("_fp64_dc")
         res["speedup_mixed_over_fp64"] = res["mixed_steps_per_s"] / res["fp64_steps_per_s"]

@@ -111,6 +111,7 @@ class FjProfile(C.Structure):
 
 
 FJ_REUSE_FACTORS = 1
+FJ_NO_GRAPH = 2
 
 
 class FjBatchItem(C.Structure):

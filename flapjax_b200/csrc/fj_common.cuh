@@ -26,6 +26,11 @@ int fail(int code, const char* fmt, ...);
 
 // Count of kernels this library has launched (read through fj_launch_count).
 void note_launch(int n = 1);
+int64_t launch_count();
+
+// True while fj_profile_begin/_end bracket a region (its event records cannot be
+// captured into a CUDA graph).
+bool prof_active();
 
 // Raise a kernel's dynamic shared-memory limit on the current device to at least
 // `bytes`.  The limit only ever grows, under a lock, so host threads launching the same

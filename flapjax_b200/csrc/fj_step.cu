@@ -714,6 +714,8 @@ struct Plan {
     double* ffil;
     char* tab;           // device table of a one-case step
     size_t tab_bytes;
+    char* tab_all;       // graph-replayed steps: the table of every slot (n_tstep x tab_bytes)
+    int* step_ctr;       // graph-replayed steps: slot whose table the next replay selects
 };
 
 static int validate(const fj_case_config* c) {
@@ -839,6 +841,8 @@ static int make_plan(const fj_case_config* cfg, void* ws, size_t ws_bytes, Plan&
     p.ffil = a.carve<double>(L.fo[ns] * 3);
     p.tab_bytes = table_layout(1).total;
     p.tab = a.carve<char>(p.tab_bytes);
+    p.tab_all = a.carve<char>((size_t)cfg->n_tstep * p.tab_bytes);
+    p.step_ctr = a.carve<int>(4);
     if (ws != nullptr && !a.fits())
         return fail(FJ_ERR_NOMEM, "workspace of %zu bytes is smaller than the %zu required", ws_bytes, a.used);
     p.ws_needed = a.used;
@@ -953,6 +957,33 @@ static void fill_aic_args(const Plan& p, AicArgs& a, const double* zeta, const d
 
 static int upload(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     return cuda_status(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "table upload");
+}
+
+// The solved circulations into the step's slot (the slot pointer comes from the table,
+// so a graph-replayed step writes the slot of its replay).
+__global__ void k_take_solution(const StepCase* __restrict__ C, const double* __restrict__ x, int nb) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nb) C->gb_n[i] = x[i];
+}
+
+// The lattice the cached factors belong to (mixed path).
+__global__ void k_keep_lattice(const StepCase* __restrict__ C, double* __restrict__ zeta_ref, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) zeta_ref[i] = C->zb_n[i];
+}
+
+// Graph-replayed steps: copy the table of slot *ctr into the fixed table area, and
+// advance *ctr after the step.
+__global__ void k_select_table(const char* __restrict__ all, size_t stride, const int* __restrict__ ctr,
+                               char* __restrict__ tab) {
+    const int4* src = reinterpret_cast<const int4*>(all + (size_t)(*ctr) * stride);
+    int4* dst = reinterpret_cast<int4*>(tab);
+    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < stride / 16; w += (size_t)gridDim.x * blockDim.x)
+        dst[w] = src[w];
+}
+
+__global__ void k_advance(int* ctr) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *ctr += 1;
 }
 
 // ------------------------------------------------------------------------------------
@@ -1099,7 +1130,13 @@ static int launch_sum(const std::vector<VindJob>& jobs, const std::vector<int64_
     return reduce_jobs((const VindJob*)d_jobs, (int)jobs.size(), max_t, s);
 }
 
-static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_bytes, cudaStream_t s) {
+// run_steps modes: build the table and launch (normal); only build the table into a
+// host buffer (build); launch with the table already in place on the device (launch:
+// the graph-replayed steps, whose table a select kernel copies in first).
+enum { kStepNormal = 0, kStepBuild = 1, kStepLaunch = 2 };
+
+static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_bytes, cudaStream_t s,
+                     int mode = kStepNormal, char* h_out = nullptr) {
     const int K = (int)items.size();
     if (K == 0) return FJ_OK;
     const int precision = items[0].p.cfg.precision;
@@ -1287,7 +1324,11 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
     memcpy(h.data() + tl.job_force, jfo.data(), jfo.size() * sizeof(VindJob));
     memcpy(h.data() + tl.aic, aic.data(), K * sizeof(AicArgs));
     if (!ref.empty()) memcpy(h.data() + tl.refine, ref.data(), ref.size() * sizeof(RefineJob));
-    FJ_TRY(upload(d_tab, h.data(), tl.total, s));
+    if (mode == kStepBuild) {
+        memcpy(h_out, h.data(), tl.total);
+        return FJ_OK;
+    }
+    if (mode == kStepNormal) FJ_TRY(upload(d_tab, h.data(), tl.total, s));
     const StepCase* dC = (const StepCase*)(d_tab + tl.step);
     const dim3 b(256);
 
@@ -1327,7 +1368,7 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
             const Plan& p = items[k].p;
             FJ_TRY(lu_factor64(p.a64, p.nb, p.piv, p.flags, s));
             FJ_TRY(lu_solve64(p.a64, p.nb, p.piv, p.rhs, p.r, s));
-            FJ_CUDA(cudaMemcpyAsync(hC[k].gb_n, p.rhs, p.nb * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            k_take_solution<<<nblk(p.nb), 256, 0, s>>>(dC + k, p.rhs, p.nb); note_launch();
         }
     } else {
         for (int k = 0; k < K; ++k) {
@@ -1336,7 +1377,7 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
             FJ_TRY(convert64to32(p.a64, p.a32, (int64_t)p.nb * p.nb, s));
             FJ_TRY(lu_factor32(p.a32, p.nb, p.piv, p.flags, s));
             FJ_TRY(lu_inverse32(p.a32, p.nb, p.piv, p.x32, s));
-            FJ_CUDA(cudaMemcpyAsync(p.zeta_ref, hC[k].zb_n, p.sz_zb * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            k_keep_lattice<<<nblk(p.sz_zb), 256, 0, s>>>(dC + k, p.zeta_ref, p.sz_zb); note_launch();
         }
         FJ_TRY(refine_jobs((const RefineJob*)(d_tab + tl.refine), (int)ref.size(), max_n, 3, s));
     }
@@ -1384,24 +1425,77 @@ static int check_buffers(const fj_case_buffers* B, bool dynamic) {
     return FJ_OK;
 }
 
-static int run_dynamic(const Plan& p, const fj_case_buffers* B, int i_first, int i_last, int flags, cudaStream_t s) {
+static BatchItem step_item(const Plan& p, const fj_case_buffers* B, int k, bool refactor) {
     const int64_t hs = (int64_t)p.cfg.n_nodes * 16;
+    BatchItem it;
+    it.p = p;
+    it.B = B;
+    it.i = k;
+    it.refactor = refactor;
+    it.hg_n = B->d_hg_t + (int64_t)k * hs;
+    it.hgd_n = B->d_hg_dot_t + (int64_t)k * hs;
+    it.hg_nm1 = B->d_hg_t + (int64_t)(k - 1) * hs;
+    return it;
+}
+
+// Steps g0..g1-1 (none refactorising) replayed from one captured step: every slot's
+// table is built on the host and uploaded once; the graph selects the table of slot
+// *step_ctr, runs the step's kernels on the fixed table area and advances the counter.
+// The capture runs on a private stream (the legacy default stream cannot be captured);
+// the replays go to the caller's stream.
+static int run_range_graph(const Plan& p, const fj_case_buffers* B, int g0, int g1, cudaStream_t s) {
+    std::vector<char> h((size_t)(g1 - g0) * p.tab_bytes);
+    for (int k = g0; k < g1; ++k) {
+        std::vector<BatchItem> one(1, step_item(p, B, k, false));
+        FJ_TRY(run_steps(one, p.tab, p.tab_bytes, s, kStepBuild, h.data() + (size_t)(k - g0) * p.tab_bytes));
+    }
+    FJ_TRY(upload(p.tab_all + (size_t)g0 * p.tab_bytes, h.data(), h.size(), s));
+    FJ_TRY(upload(p.step_ctr, &g0, sizeof(int), s));
+
+    cudaStream_t cs = nullptr;
+    FJ_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t graph = nullptr;
+    const int64_t launches0 = launch_count();
+    int st = cuda_status(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "step graph capture");
+    if (st == FJ_OK) {
+        k_select_table<<<32, 256, 0, cs>>>(p.tab_all, p.tab_bytes, p.step_ctr, p.tab); note_launch();
+        std::vector<BatchItem> one(1, step_item(p, B, g0, false));
+        st = run_steps(one, p.tab, p.tab_bytes, cs, kStepLaunch);
+        k_advance<<<1, 32, 0, cs>>>(p.step_ctr); note_launch();
+        const int st_end = cuda_status(cudaStreamEndCapture(cs, &graph), "step graph capture");
+        if (st == FJ_OK) st = st_end;
+    }
+    const int64_t per_step = launch_count() - launches0;
+    cudaGraphExec_t exec = nullptr;
+    if (st == FJ_OK) st = cuda_status(cudaGraphInstantiate(&exec, graph, 0), "step graph instantiate");
+    for (int k = g0; k < g1 && st == FJ_OK; ++k) st = cuda_status(cudaGraphLaunch(exec, s), "step graph launch");
+    if (st == FJ_OK) {
+        note_launch((int)(per_step * (g1 - g0 - 1)));  // kernels executed by the replays beyond the capture
+        st = cuda_status(cudaStreamSynchronize(s), "step graph replay");
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(cs);
+    return st;
+}
+
+static int run_dynamic(const Plan& p, const fj_case_buffers* B, int i_first, int i_last, int flags, cudaStream_t s) {
     const bool mixed = p.cfg.precision == FJ_PREC_MIXED;
+    const bool graphs = !(flags & FJ_NO_GRAPH) && !prof_active();
     bool refactor_all = false;
     int i = i_first;
     for (int attempt = 0; attempt < 2; ++attempt) {
-        for (int k = i; k < i_last; ++k) {
+        int k = i;
+        while (k < i_last) {
             const bool first = (k == i) && !(attempt == 0 && (flags & FJ_REUSE_FACTORS));
-            std::vector<BatchItem> one(1);
-            one[0].p = p;
-            one[0].B = B;
-            one[0].i = k;
-            one[0].refactor = mixed && (refactor_all || first);
-            one[0].hg_n = B->d_hg_t + (int64_t)k * hs;
-            one[0].hgd_n = B->d_hg_dot_t + (int64_t)k * hs;
-            one[0].hg_nm1 = B->d_hg_t + (int64_t)(k - 1) * hs;
+            const bool refactor = mixed && (refactor_all || first);
+            // the first step always runs directly (it also does the one-time set-up)
+            if (graphs && !refactor && k > i && i_last - k >= 2) break;
+            std::vector<BatchItem> one(1, step_item(p, B, k, refactor));
             FJ_TRY(run_steps(one, p.tab, p.tab_bytes, s));
+            ++k;
         }
+        if (k < i_last) FJ_TRY(run_range_graph(p, B, k, i_last, s));
         if (!mixed) break;
         // read the refinement residuals back once; re-run from the first failure with a
         // fresh factorisation every step if the cached factors were not good enough

@@ -94,6 +94,11 @@ void prof_stop(int slot, cudaStream_t s, double pairs) {
     g_prof.pairs[slot] = pairs;
 }
 
+bool prof_active() {
+    std::lock_guard<std::mutex> g(g_prof.mu);
+    return g_prof.on;
+}
+
 int prof_begin() {
     std::lock_guard<std::mutex> g(g_prof.mu);
     g_prof.on = true;

@@ -158,10 +158,11 @@ class DeviceCase:
         _lib.call("fj_solve_static", C.byref(self.cfg), C.byref(self._bufs), int(horseshoe), float(t0),
                   self.ws.data_ptr(), self.ws.numel(), self._stream())
 
-    def solve_dynamic(self, i_first: int, i_last: int, reuse_factors: bool = False):
+    def solve_dynamic(self, i_first: int, i_last: int, reuse_factors: bool = False, graph: bool = True):
         """Steps i_first..i_last-1.  ``reuse_factors``: keep the mixed path's cached
-        factors from the previous call on this case."""
-        flags = _lib.FJ_REUSE_FACTORS if reuse_factors else 0
+        factors from the previous call on this case.  ``graph``: replay runs of steps from
+        one captured CUDA graph (False: launch every step directly; same results)."""
+        flags = (_lib.FJ_REUSE_FACTORS if reuse_factors else 0) | (0 if graph else _lib.FJ_NO_GRAPH)
         _lib.call("fj_solve_prescribed_dynamic", C.byref(self.cfg), C.byref(self._bufs), int(i_first), int(i_last),
                   flags, self.ws.data_ptr(), self.ws.numel(), self._stream())
 

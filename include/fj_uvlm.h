@@ -166,8 +166,12 @@ FJ_API int fj_solve_static(const fj_case_config* cfg, const fj_case_buffers* buf
  * FJ_PREC_MIXED: the FP32 factors are computed at step i_first, unless flags has
  * FJ_REUSE_FACTORS and an earlier call on this workspace left factors there; the
  * refinement residuals are read back after the last step (one synchronisation) and
- * the steps from the first one above 1e-12 are re-run with fresh factors. */
+ * the steps from the first one above 1e-12 are re-run with fresh factors.
+ * Runs of three or more steps that reuse their factors (FP64: every step after the
+ * first) are replayed from one CUDA graph captured for a single step; FJ_NO_GRAPH
+ * launches every step directly instead (same arithmetic). */
 #define FJ_REUSE_FACTORS 1
+#define FJ_NO_GRAPH 2
 FJ_API int fj_solve_prescribed_dynamic(const fj_case_config* cfg, const fj_case_buffers* bufs,
                                 int i_first, int i_last, int flags, void* d_ws,
                                 size_t ws_bytes, fj_stream_t stream);

@@ -11,7 +11,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from flapjax_b200 import cases
+from flapjax_b200 import _lib, cases
 from oracle import uvlm_ref as R
 from tests.helpers import coefficients, device_uvlm, oracle_force_total, oracle_uvlm, rel_err
 
@@ -348,3 +348,28 @@ def test_variable_wake_matches_oracle(cuda, free, precision):
     # the wake really follows delta_w: first-column segment lengths at the last step
     seg = np.linalg.norm(np.diff(got.zeta_w[0][-1][:, 0], axis=0), axis=-1)
     assert np.all(seg[1:] > seg[:-1])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_graph_replayed_steps_match_direct_launches(cuda, precision):
+    """A run of steps replayed from one captured step graph gives the same slots,
+    bit for bit, as launching every step directly (free wake, so every kernel runs)."""
+    import torch
+
+    c = cases.wing_free(m=4, n=10, m_star=12, n_steps=9)
+    outs = []
+    for graph in (False, True):
+        uv, _ = device_uvlm(c, precision)
+        dc = uv.make_device_case(c.n_tstep)
+        uv.load_initial(dc, uv.solve_static())
+        dc.set_hg(c.hg_t, c.hg_dot_t)
+        launches0 = _lib.load().fj_launch_count()
+        dc.solve_dynamic(1, c.n_tstep, graph=graph)
+        torch.cuda.synchronize()
+        outs.append((dc.host_arrays(), _lib.load().fj_launch_count() - launches0))
+    (a, na), (b, nb) = outs
+    for f in ("gamma_b", "gamma_w", "zeta_w", "f_steady", "f_unsteady", "gamma_b_dot", "alpha"):
+        assert np.array_equal(a[f], b[f]), f
+    assert np.array_equal(a["t"], b["t"]) and np.array_equal(a["force_total"], b["force_total"])
+    # the launch counter counts the kernels the replays executed (plus the graph's two)
+    assert nb >= na
