@@ -1415,12 +1415,14 @@ __global__ void surface_c_nc_kernel(int m, int n, const double* __restrict__ zet
     nc[p * 3 + 2] = d1[0] * d2[1] - d1[1] * d2[0];
 }
 
-static int check_buffers(const fj_case_buffers* B, bool dynamic) {
+static int check_buffers(const Plan& p, const fj_case_buffers* B, bool dynamic) {
     if (B == nullptr) return fail(FJ_ERR_SHAPE, "buffers struct is NULL");
     if (!B->d_zeta_b0 || !B->d_dof_mapping || !B->d_t || !B->d_zeta_b || !B->d_zeta_b_dot || !B->d_zeta_w ||
-        !B->d_c || !B->d_nc || !B->d_gamma_b || !B->d_gamma_b_dot || !B->d_gamma_w || !B->d_f_steady ||
+        !B->d_c || !B->d_nc || !B->d_gamma_b || !B->d_gamma_b_dot || !B->d_f_steady ||
         !B->d_f_unsteady || !B->d_alpha || !B->d_force_total)
         return fail(FJ_ERR_SHAPE, "a required device buffer is NULL");
+    // gamma_w has no entries when no surface has a wake (m_star = 0 everywhere)
+    if (!B->d_gamma_w && p.sz_gw > 0) return fail(FJ_ERR_SHAPE, "d_gamma_w is NULL");
     if (dynamic && (!B->d_hg_t || !B->d_hg_dot_t)) return fail(FJ_ERR_SHAPE, "hg_t / hg_dot_t are NULL");
     return FJ_OK;
 }
@@ -1543,7 +1545,7 @@ int fj_solve_static(const fj_case_config* cfg, const fj_case_buffers* bufs, int 
                     size_t ws_bytes, fj_stream_t stream) {
     Plan p;
     FJ_TRY(make_plan(cfg, d_ws, ws_bytes, p));
-    FJ_TRY(check_buffers(bufs, false));
+    FJ_TRY(check_buffers(p, bufs, false));
     const double* hg = bufs->d_hg_t;
     if (hg == nullptr) return fail(FJ_ERR_SHAPE, "d_hg_t is NULL (slot 0 holds the static frames)");
     return run_static(p, bufs, hg, horseshoe, t0, (cudaStream_t)stream);
@@ -1553,7 +1555,7 @@ int fj_solve_prescribed_dynamic(const fj_case_config* cfg, const fj_case_buffers
                                 int flags, void* d_ws, size_t ws_bytes, fj_stream_t stream) {
     Plan p;
     FJ_TRY(make_plan(cfg, d_ws, ws_bytes, p));
-    FJ_TRY(check_buffers(bufs, true));
+    FJ_TRY(check_buffers(p, bufs, true));
     if (i_first < 1 || i_last > cfg->n_tstep || i_first > i_last)
         return fail(FJ_ERR_SHAPE, "step range [%d, %d) not within [1, %d)", i_first, i_last, cfg->n_tstep);
     if (i_first == i_last) return FJ_OK;
@@ -1579,7 +1581,7 @@ int fj_step_batched(const fj_batch_item* items, int n_items, void* d_batch_ws, s
     for (int k = 0; k < n_items; ++k) {
         const fj_batch_item& it = items[k];
         FJ_TRY(make_plan(it.cfg, it.d_ws, it.ws_bytes, v[k].p));
-        FJ_TRY(check_buffers(it.bufs, true));
+        FJ_TRY(check_buffers(v[k].p, it.bufs, true));
         if (it.i_ts < 1 || it.i_ts >= it.cfg->n_tstep)
             return fail(FJ_ERR_SHAPE, "item %d: slot %d not in [1, %d)", k, it.i_ts, it.cfg->n_tstep);
         const int64_t hs = (int64_t)it.cfg->n_nodes * 16;
