@@ -143,6 +143,7 @@ struct StepCase {
     const double* v_rhs;    // wake velocity at collocation points (null: static solve)
     const double* zeta_ref; // mixed path: lattice of the cached AIC (null: no comparison)
     int* changed;           // mixed path: set to 1 when zb_n differs from zeta_ref
+    int* nonfinite;         // lowest slot whose total force is not finite (sentinel: none)
 };
 
 __global__ void k_time(const StepCase* __restrict__ T) {
@@ -673,8 +674,12 @@ __global__ void k_force_total(const StepCase* __restrict__ T) {
             for (int d = 0; d < 3; ++d) sh[d][threadIdx.x] += sh[d][threadIdx.x + w];
         __syncthreads();
     }
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0) {
         for (int d = 0; d < 3; ++d) C.ft[d] = sh[d][0];
+        // every output of the step feeds the total force: a NaN/Inf anywhere shows here
+        if (C.nonfinite != nullptr && !(isfinite(sh[0][0]) && isfinite(sh[1][0]) && isfinite(sh[2][0])))
+            atomicMin(C.nonfinite, C.i);
+    }
 }
 
 static inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
@@ -1037,6 +1042,7 @@ static int run_static(const Plan& p, const fj_case_buffers* B, const double* hg,
     C.v = p.v;
     C.ffil = p.ffil;
     C.rhs = p.rhs;
+    C.nonfinite = p.flags + 2;
     const TableLayout tl = table_layout(1);
     StepCase* dC = (StepCase*)(p.tab + tl.step);
     FJ_TRY(upload(dC, &C, sizeof(C), s));
@@ -1204,6 +1210,7 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
         C.v = p.v;
         C.ffil = p.ffil;
         C.rhs = p.rhs;
+        C.nonfinite = p.flags + 2;
         C.v_wake = C.free_wake ? p.v : nullptr;
         C.v_rhs = p.v;
         if (L.any_var && B->d_delta_w == nullptr)
@@ -1427,6 +1434,23 @@ static int check_buffers(const Plan& p, const fj_case_buffers* B, bool dynamic) 
     return FJ_OK;
 }
 
+// Status words of a case-level call: flags[0] the LU info of the last factorisation
+// (first zero pivot + 1), flags[2] the lowest slot with a non-finite total force.
+static constexpr int kNoSlot = 0x7f7f7f7f;  // the byte pattern 0x7f repeated
+
+static int clear_status(const Plan& p, cudaStream_t s) {
+    return cuda_status(cudaMemsetAsync(p.flags + 2, 0x7f, sizeof(int), s), "status reset");
+}
+
+static int read_status(const Plan& p, cudaStream_t s) {
+    int w[3] = {0, 0, 0};
+    FJ_CUDA(cudaMemcpyAsync(w, p.flags, sizeof(w), cudaMemcpyDeviceToHost, s));
+    FJ_CUDA(cudaStreamSynchronize(s));
+    if (w[2] != kNoSlot) return fail(FJ_ERR_NONFINITE, "non-finite forces at time slot %d", w[2]);
+    if (w[0] != 0) return fail(FJ_ERR_SINGULAR, "zero pivot in column %d of the AIC factorisation", w[0] - 1);
+    return FJ_OK;
+}
+
 static BatchItem step_item(const Plan& p, const fj_case_buffers* B, int k, bool refactor) {
     const int64_t hs = (int64_t)p.cfg.n_nodes * 16;
     BatchItem it;
@@ -1503,7 +1527,7 @@ static int run_dynamic(const Plan& p, const fj_case_buffers* B, int i_first, int
         // fresh factorisation every step if the cached factors were not good enough
         std::vector<double> res(i_last - i);
         FJ_CUDA(cudaMemcpyAsync(res.data(), p.resid + i, res.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-        FJ_CUDA(cudaStreamSynchronize(s));
+        FJ_TRY(read_status(p, s));  // non-finite data is not a refinement failure
         int bad = -1;
         for (size_t q = 0; q < res.size(); ++q)
             if (!(res[q] <= 1e-12)) {
@@ -1548,7 +1572,10 @@ int fj_solve_static(const fj_case_config* cfg, const fj_case_buffers* bufs, int 
     FJ_TRY(check_buffers(p, bufs, false));
     const double* hg = bufs->d_hg_t;
     if (hg == nullptr) return fail(FJ_ERR_SHAPE, "d_hg_t is NULL (slot 0 holds the static frames)");
-    return run_static(p, bufs, hg, horseshoe, t0, (cudaStream_t)stream);
+    cudaStream_t s = (cudaStream_t)stream;
+    FJ_TRY(clear_status(p, s));
+    FJ_TRY(run_static(p, bufs, hg, horseshoe, t0, s));
+    return read_status(p, s);
 }
 
 int fj_solve_prescribed_dynamic(const fj_case_config* cfg, const fj_case_buffers* bufs, int i_first, int i_last,
@@ -1559,7 +1586,10 @@ int fj_solve_prescribed_dynamic(const fj_case_config* cfg, const fj_case_buffers
     if (i_first < 1 || i_last > cfg->n_tstep || i_first > i_last)
         return fail(FJ_ERR_SHAPE, "step range [%d, %d) not within [1, %d)", i_first, i_last, cfg->n_tstep);
     if (i_first == i_last) return FJ_OK;
-    return run_dynamic(p, bufs, i_first, i_last, flags, (cudaStream_t)stream);
+    cudaStream_t s = (cudaStream_t)stream;
+    FJ_TRY(clear_status(p, s));
+    FJ_TRY(run_dynamic(p, bufs, i_first, i_last, flags, s));
+    return read_status(p, s);
 }
 
 int fj_case_step(const fj_case_config* cfg, const fj_case_buffers* bufs, int i_ts, int flags, void* d_ws,

@@ -169,7 +169,11 @@ FJ_API int fj_solve_static(const fj_case_config* cfg, const fj_case_buffers* buf
  * the steps from the first one above 1e-12 are re-run with fresh factors.
  * Runs of three or more steps that reuse their factors (FP64: every step after the
  * first) are replayed from one CUDA graph captured for a single step; FJ_NO_GRAPH
- * launches every step directly instead (same arithmetic). */
+ * launches every step directly instead (same arithmetic).
+ * fj_solve_static and fj_solve_prescribed_dynamic synchronise the stream before
+ * returning and scan their slots: FJ_ERR_NONFINITE names the first slot whose total
+ * force is NaN/Inf (a NaN anywhere in the step reaches it), FJ_ERR_SINGULAR an exact
+ * zero pivot of the last factorisation. */
 #define FJ_REUSE_FACTORS 1
 #define FJ_NO_GRAPH 2
 FJ_API int fj_solve_prescribed_dynamic(const fj_case_config* cfg, const fj_case_buffers* bufs,

@@ -75,3 +75,28 @@ def test_rotation_invariance_and_no_wake_force(cuda):
         scale = np.abs(s.f_steady[0]).sum()
         assert np.max(np.abs(ft)) < 1e-10 * scale
     assert rel_err(out[1].gamma_b[0], out[0].gamma_b[0]) < 1e-10
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_nonfinite_inputs_return_an_error_status(cuda, precision):
+    """Malformed data injected on the host: a NaN in the lattice makes the static solve
+    return FJ_ERR_NONFINITE; a NaN node frame at slot 3 makes the dynamic solve name slot
+    3.  The device stays usable afterwards."""
+    from flapjax_b200._lib import FJ_ERR_NONFINITE, FjError
+
+    c = cases.wing_heave(m=4, n=8, m_star=8, n_steps=6)
+    bad = c.zeta_b0.copy()
+    bad[2, 3, 2] = np.nan
+    uv = fj.UVLM([fj.GridDiscretisation(c.m, c.n, c.m_star)], np.arange(c.n + 1), precision=precision)
+    uv.set_design_variables(dt=c.dt, flowfield=fj.Constant(c.u_inf, c.rho, True), zeta_b0=bad, hg0=c.hg0)
+    with pytest.raises(FjError) as e:
+        uv.solve_static()
+    assert e.value.code == FJ_ERR_NONFINITE
+    uv, _ = device_uvlm(c, precision)
+    hg = c.hg_t.copy()
+    hg[3, 0, 2, 3] = np.nan
+    with pytest.raises(FjError) as e:
+        uv.solve_prescribed_dynamic(uv.solve_static(), hg, c.hg_dot_t)
+    assert e.value.code == FJ_ERR_NONFINITE and "slot 3" in str(e.value)
+    good = uv.solve_prescribed_dynamic(uv.solve_static(), c.hg_t, c.hg_dot_t)
+    assert np.all(np.isfinite(good.gamma_b[0]))
