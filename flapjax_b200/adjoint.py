@@ -27,7 +27,8 @@ Forward states are recomputed from checkpoints every ``checkpoint`` steps (only 
 checkpoint slots are kept), so device memory is O(checkpoint) slots and O(checkpoint)
 factor matrices.
 
-Scope: one surface, epsilon kernel, Constant flow, prescribed wake, no mirror.
+Scope: one surface, epsilon kernel, Constant flow, prescribed wake (uniform or variable,
+``delta_w``, with gradients through the arc-length re-discretisation), no mirror.
 """
 from __future__ import annotations
 
@@ -167,6 +168,74 @@ def _normals_T(zeta, bar_nc):
     out[1:, :-1] += b2
     out[:-1, 1:] -= b2
     return out
+
+
+def _interp_T(x, xp, fp, fbar):
+    """Transpose of np.interp(x, xp, fp) per output (1-D xp increasing): returns
+    (xp_bar, fp_bar).  fp may carry trailing component axes; fbar matches x's shape plus
+    them.  Inside [xp[j], xp[j+1]): f = fp[j] + t (fp[j+1] - fp[j]), t = (x - xp[j]) / dx;
+    beyond the last node f = fp[-1] (no xp dependence); x is constant."""
+    xp_bar = np.zeros(xp.shape)
+    fp_bar = np.zeros(fp.shape)
+    last = xp.shape[0] - 1
+    for q in range(x.shape[0]):
+        xq = x[q]
+        if not xq >= xp[0]:
+            fp_bar[0] += fbar[q]
+            continue
+        if xq >= xp[last]:
+            fp_bar[last] += fbar[q]
+            continue
+        j = int(np.searchsorted(xp, xq, side="right")) - 1
+        dx = xp[j + 1] - xp[j]
+        t = (xq - xp[j]) / dx
+        fp_bar[j] += (1.0 - t) * fbar[q]
+        fp_bar[j + 1] += t * fbar[q]
+        tbar = np.sum(fbar[q] * (fp[j + 1] - fp[j]))
+        xp_bar[j] += tbar * (-(1.0 - t) / dx)
+        xp_bar[j + 1] += tbar * (-t / dx)
+    return xp_bar, fp_bar
+
+
+def _variable_wake_T(zw_nm1, te_n, gb_te_nm1, gw_nm1, dw, dt, U, Zw_bar, Gw_bar):
+    """Transpose of propagate_surf_wake with delta_w for a prescribed wake
+    (aero/utils.py:427-491, gradients through the arc lengths as the reference's default
+    linearise_variable_wake=False).  Returns the cotangents of zeta_w at n-1, of the
+    trailing-edge vertex row at n, of the trailing-edge circulation row at n-1 and of
+    gamma_w at n-1."""
+    W1, n1, _ = zw_nm1.shape          # W + 1 vertex rows, n + 1 columns
+    X = np.concatenate([te_n[None], zw_nm1 + dt * U], axis=0)  # (W + 2, n + 1, 3)
+    G = np.concatenate([gb_te_nm1[None], gw_nm1], axis=0)      # (W + 1, n)
+    seg = np.linalg.norm(X[1:] - X[:-1], axis=-1)              # (W + 1, n + 1)
+    S = np.concatenate([np.zeros((1, n1)), np.cumsum(seg, axis=0)], axis=0)
+    SG = 0.5 * (0.5 * (S[:-1, :-1] + S[1:, :-1]) + 0.5 * (S[:-1, 1:] + S[1:, 1:]))
+    s_disc = np.concatenate([np.zeros(1), np.cumsum(dw)])
+    sg_disc = 0.5 * (s_disc[:-1] + s_disc[1:])
+    X_bar = np.zeros_like(X)
+    S_bar = np.zeros_like(S)
+    for j in range(n1):
+        sb, xb = _interp_T(s_disc, S[:, j], X[:, j], Zw_bar[:, j])
+        S_bar[:, j] += sb
+        X_bar[:, j] += xb
+    G_bar = np.zeros_like(G)
+    SG_bar = np.zeros_like(SG)
+    if G.shape[0] > 1 or Gw_bar.size:
+        for j in range(G.shape[1]):
+            sgb, gb = _interp_T(sg_disc, SG[:, j], G[:, j], Gw_bar[:, j])
+            SG_bar[:, j] += sgb
+            G_bar[:, j] += gb
+    q = 0.25 * SG_bar
+    S_bar[:-1, :-1] += q
+    S_bar[1:, :-1] += q
+    S_bar[:-1, 1:] += q
+    S_bar[1:, 1:] += q
+    # S_r = sum_{p <= r} |X_p - X_{p-1}|
+    D_bar = np.cumsum(S_bar[::-1], axis=0)[::-1][1:]          # (W + 1, n + 1): sum_{r >= p} S_bar_r
+    d = X[1:] - X[:-1]
+    e = d / np.maximum(np.linalg.norm(d, axis=-1, keepdims=True), 1e-300)
+    X_bar[1:] += D_bar[..., None] * e
+    X_bar[:-1] -= D_bar[..., None] * e
+    return X_bar[1:], X_bar[0], G_bar[0], G_bar[1:]
 
 
 def _frames_T(bar_zb, bar_zbd, hg, hgd, dof):
@@ -362,13 +431,23 @@ class PrescribedAdjoint:
         Zb += _normals_T(zb, ncbar)
         Zbd += _avg4_T(cdotbar, zbd.shape)
         # 6. wake shedding transposes
-        Zb[-1] += Zw[0]
-        Zw_prev = np.zeros_like(Zw)
-        Zw_prev[:-1] += Zw[1:]
-        Gw_prev = np.zeros_like(Gw)
-        if W > 0:
-            Gb_prev[-1, :] += Gw[0, :]
-            Gw_prev[:-1] += Gw[1:]
+        dw = self.uv.delta_w[0] if getattr(self.uv, "delta_w", None) else None
+        if dw is not None:
+            zw_p, te_bar, gte_bar, gw_p = _variable_wake_T(
+                seg.zeta_w[0][loc - 1], zb[-1], seg.gamma_b[0][loc - 1][-1], seg.gamma_w[0][loc - 1],
+                np.asarray(dw, float), dt, U, Zw, Gw)
+            Zb[-1] += te_bar
+            Zw_prev = zw_p
+            Gw_prev = gw_p
+            Gb_prev[-1, :] += gte_bar
+        else:
+            Zb[-1] += Zw[0]
+            Zw_prev = np.zeros_like(Zw)
+            Zw_prev[:-1] += Zw[1:]
+            Gw_prev = np.zeros_like(Gw)
+            if W > 0:
+                Gb_prev[-1, :] += Gw[0, :]
+                Gw_prev[:-1] += Gw[1:]
         # 7. node frames
         zeta0_bar += _frames_T(Zb, Zbd, hg_n, hgd_n, dof)
         return Gb_prev, Gbd_prev, Gw_prev, Zw_prev

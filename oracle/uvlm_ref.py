@@ -414,6 +414,25 @@ class OneMinusCosine(Constant):
 # ----------------------------------------------------------------------------------
 # Wake, forces and strip angle, aero/utils.py.
 # ----------------------------------------------------------------------------------
+def _interp(x, xp, fp):
+    """np.interp in the arrays' own type: np.interp itself for float64 (the reference's
+    jnp.interp semantics as the goldens pin them), the same formula for extended precision
+    (np.interp accepts only float64)."""
+    if np.result_type(x, xp, fp) == np.float64:
+        return np.interp(x, xp, fp)
+    out = np.empty(np.shape(x), dtype=REAL)
+    last = xp.shape[0] - 1
+    for q, xq in enumerate(np.asarray(x)):
+        if xq < xp[0]:
+            out[q] = fp[0]
+        elif xq >= xp[last]:
+            out[q] = fp[last]
+        else:
+            j = int(np.searchsorted(xp, xq, side="right")) - 1
+            out[q] = (fp[j + 1] - fp[j]) / (xp[j + 1] - xp[j]) * (xq - xp[j]) + fp[j]
+    return out
+
+
 def propagate_surf_wake(gamma_b_nm1, gamma_w_nm1, zeta_b_n, zeta_w_nm1, delta_w, v_func, dt):
     """``propagate_surf_wake`` aero/utils.py:400-500 (uniform and ``delta_w`` branches)."""
     zeta_te = zeta_b_n[-1, ...]
@@ -433,13 +452,13 @@ def propagate_surf_wake(gamma_b_nm1, gamma_w_nm1, zeta_b_n, zeta_w_nm1, delta_w,
         s_gamma_w = neighbour_average(s_zeta_w, (0, 1))
         s_disc = np.concatenate((np.zeros(1), np.cumsum(delta_w)))
         s_gamma_disc = neighbour_average(s_disc, (0,))
-        zn = np.empty((s_disc.shape[0], zeta_w_n.shape[1], 3))
+        zn = np.empty((s_disc.shape[0], zeta_w_n.shape[1], 3), REAL)
         for j in range(zeta_w_n.shape[1]):
             for k in range(3):
-                zn[:, j, k] = np.interp(s_disc, s_zeta_w[:, j], zeta_w_n[:, j, k])
-        gn = np.empty((s_gamma_disc.shape[0], gamma_w_n.shape[1]))
+                zn[:, j, k] = _interp(s_disc, s_zeta_w[:, j], zeta_w_n[:, j, k])
+        gn = np.empty((s_gamma_disc.shape[0], gamma_w_n.shape[1]), REAL)
         for j in range(gamma_w_n.shape[1]):
-            gn[:, j] = np.interp(s_gamma_disc, s_gamma_w[:, j], gamma_w_n[:, j])
+            gn[:, j] = _interp(s_gamma_disc, s_gamma_w[:, j], gamma_w_n[:, j])
         zeta_w_n, gamma_w_n = zn, gn
     if gamma_w_nm1.size == 0:
         gamma_w_n = np.zeros_like(gamma_w_nm1)

@@ -101,19 +101,21 @@ def _one(snap):
     return out
 
 
-def forward_objective(case, zeta_b0, fw):
+def forward_objective(case, zeta_b0, fw, delta_w=None):
     """J = sum_{n>=1} fw[n] . F_n of the oracle forward at the lattice ``zeta_b0`` (in
-    the oracle's current floating type)."""
+    the oracle's current floating type), with an optional variable wake ``delta_w``."""
     from flapjax_b200 import cases
     from tests.helpers import oracle_uvlm
 
-    uv, _ = oracle_uvlm(cases.WingCase(**{**case.__dict__, "zeta_b0": zeta_b0}))
+    uv, ff = oracle_uvlm(cases.WingCase(**{**case.__dict__, "zeta_b0": zeta_b0}))
+    if delta_w is not None:
+        uv.set_design_variables(case.dt, ff, zeta_b0, case.hg0, delta_w=np.asarray(delta_w, float))
     out = uv.solve_prescribed_dynamic(uv.solve_static(), case.hg_t, case.hg_dot_t)
     ft = sum(fs.sum(axis=(1, 2)) + fu.sum(axis=(1, 2)) for fs, fu in zip(out.f_steady, out.f_unsteady))
     return np.sum(fw[1:] * ft[1:])
 
 
-def central_difference(case, direction, fw, h=1e-6):
+def central_difference(case, direction, fw, h=1e-6, delta_w=None):
     """(J(z + h d) - J(z - h d)) / 2h of the oracle forward run in 80-bit extended
     precision.  In float64 the forward carries ~1e-11 relative roundoff noise (the
     epsilon kernel evaluated at a filament's own midpoint divides roundoff by
@@ -121,8 +123,8 @@ def central_difference(case, direction, fw, h=1e-6):
     z = np.asarray(case.zeta_b0, np.longdouble)
     hh = np.longdouble(h)
     with R.real_type(np.longdouble):
-        jp = forward_objective(case, z + hh * direction, fw)
-        jm = forward_objective(case, z - hh * direction, fw)
+        jp = forward_objective(case, z + hh * direction, fw, delta_w)
+        jm = forward_objective(case, z - hh * direction, fw, delta_w)
     return float((jp - jm) / (2 * hh))
 
 

@@ -83,3 +83,21 @@ def test_twist_jacobian_finite_differences():
         fd = (cases.twisted_grid(m, n, 1.0, 0.25, np.interp(span_y, ctrl_y, tp), 0.03)
               - cases.twisted_grid(m, n, 1.0, 0.25, np.interp(span_y, ctrl_y, tm), 0.03)) / (2 * h)
         assert np.max(np.abs(fd - jac[k])) < 1e-9
+
+
+def test_reverse_sweep_variable_wake_matches_finite_differences():
+    """delta_w: the transpose of the arc-length re-discretisation (through the arc lengths,
+    as the reference differentiates it by default) against extended-precision central
+    differences."""
+    c = cases.wing_pitch(m=3, n=4, m_star=5, n_steps=5, n_ctrl=3, seed=3)
+    dw = c.dt * c.u_mag * 1.2 ** np.arange(c.m_star)
+    fw = coefficient_weights(c, "CL")
+    uv, ff = oracle_uvlm(c)
+    uv.set_design_variables(c.dt, ff, c.zeta_b0, c.hg0, delta_w=dw)
+    J, g = OracleAdjoint(uv).gradient(c.hg_t, c.hg_dot_t, fw, checkpoint=2)
+    assert abs(J - forward_objective(c, c.zeta_b0, fw, dw)) < 1e-13 * abs(J)
+    rng = np.random.default_rng(1)
+    for _ in range(2):
+        d = rng.normal(size=c.zeta_b0.shape) * 0.1
+        fd = central_difference(c, d, fw, delta_w=dw)
+        assert abs(fd - np.sum(g * d)) <= 1e-6 * abs(fd), (fd, np.sum(g * d))
