@@ -483,6 +483,28 @@ def config_table(args, torch):
             # against the lift scale shows the force accuracy itself
             res["cd_err_over_max_cl"] = float(np.max(np.abs(cdm - cd64)) / np.max(np.abs(cl64)))
             res["max_cd_over_max_cl"] = float(np.max(np.abs(cd64)) / np.max(np.abs(cl64)))
+        if case.free_wake:
+            # fluid-structure iterations: each step re-solved 3 times with new frames (a
+            # structural iterate); iterations 2-3 reuse the convection velocities
+            fsi = {}
+            for prec in ("mixed", "fp64"):
+                _, dc = make_case(case, prec, n_slots)
+                run_device_steps(dc, 1, 4, None, torch)
+                for reuse in (False, True):
+                    st = torch.cuda.current_stream()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    n_it = 0
+                    e0.record(st)
+                    for i in range(4, min(n_slots, 14)):
+                        for it in range(3):
+                            dc.hg_t[i, :, 2, 3] += 1e-4  # the structure's new iterate
+                            dc.solve_dynamic(i, i + 1, reuse_factors=True, reuse_convection=reuse and it > 0)
+                            n_it += 1
+                    e1.record(st)
+                    e1.synchronize()
+                    fsi[f"{prec}{'_reuse' if reuse else ''}_iterations_per_s"] = n_it / (e0.elapsed_time(e1) * 1e-3)
+                del dc
+            res["fsi_3_iterations_per_step"] = fsi
         del dm, d64
         th = host_threads()
         cpu_case = type(case)(**{**case.__dict__})

@@ -112,6 +112,7 @@ class FjProfile(C.Structure):
 
 FJ_REUSE_FACTORS = 1
 FJ_NO_GRAPH = 2
+FJ_REUSE_CONVECTION = 4
 
 
 class FjBatchItem(C.Structure):

@@ -705,6 +705,7 @@ struct Plan {
     void* stream;
     double* hs_zw;       // horseshoe wake scratch
     double* hs_gw;
+    double* v_conv;      // free-wake convection velocities of the last step solved (wake targets x 3)
     double* zw_tmp;      // variable wake scratch (null when no surface has delta_w)
     double* gw_tmp;
     double* s_tmp;
@@ -822,6 +823,7 @@ static int make_plan(const fj_case_config* cfg, void* ws, size_t ws_bytes, Plan&
     }
     p.hs_zw = a.carve<double>(hs);
     p.hs_gw = a.carve<double>(hsg);
+    p.v_conv = a.carve<double>(std::max<int64_t>(L.wto[ns], 1) * 3);
     if (L.any_var) {
         p.zw_tmp = a.carve<double>(L.xvo[ns] * 3);
         p.gw_tmp = a.carve<double>(std::max<int64_t>(L.xpo[ns], 1));
@@ -1102,6 +1104,7 @@ struct BatchItem {
     const double* hg_n;
     const double* hgd_n;
     const double* hg_nm1;
+    bool reuse_convection = false;  // free wake: the previous call's convection velocities hold
 };
 
 // Target CTAs for a batched sum; each job gets a share proportional to its pairs.
@@ -1176,7 +1179,10 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
         C.L = L;
         C.nb = p.nb;
         C.i = i;
-        C.free_wake = c.free_wake && L.wto[L.n_surf] > 0;
+        // convection velocities: computed into p.v_conv (kept for the next call), or
+        // reused from there when the caller says the step's n-1 state is the same
+        const bool fw = c.free_wake && L.wto[L.n_surf] > 0;
+        C.free_wake = fw && !it.reuse_convection;
         C.dt = c.dt;
         C.relax = c.gamma_dot_relaxation;
         C.flow = c.flow;
@@ -1211,7 +1217,7 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
         C.ffil = p.ffil;
         C.rhs = p.rhs;
         C.nonfinite = p.flags + 2;
-        C.v_wake = C.free_wake ? p.v : nullptr;
+        C.v_wake = fw ? p.v_conv : nullptr;
         C.v_rhs = p.v;
         if (L.any_var && B->d_delta_w == nullptr)
             return fail(FJ_ERR_SHAPE, "variable_wake set but d_delta_w is NULL");
@@ -1253,7 +1259,7 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
             j.n_elem = sb.len();
             j.part = p.part;
             j.n_links = sb.n_links;
-            j.out = p.v;
+            j.out = p.v_conv;
             jf.push_back(j);
         } else {
             memset(&pf[k], 0, sizeof(PackJob));  // empty job: offset[0] = 0 packs nothing
@@ -1518,6 +1524,9 @@ static int run_dynamic(const Plan& p, const fj_case_buffers* B, int i_first, int
             // the first step always runs directly (it also does the one-time set-up)
             if (graphs && !refactor && k > i && i_last - k >= 2) break;
             std::vector<BatchItem> one(1, step_item(p, B, k, refactor));
+            // the cached convection velocities belong to the previous call's step: only the
+            // first step of the first attempt may take them
+            one[0].reuse_convection = attempt == 0 && k == i_first && (flags & FJ_REUSE_CONVECTION);
             FJ_TRY(run_steps(one, p.tab, p.tab_bytes, s));
             ++k;
         }
@@ -1618,6 +1627,7 @@ int fj_step_batched(const fj_batch_item* items, int n_items, void* d_batch_ws, s
         v[k].B = it.bufs;
         v[k].i = it.i_ts;
         v[k].refactor = it.cfg->precision == FJ_PREC_MIXED && !(it.flags & FJ_REUSE_FACTORS);
+        v[k].reuse_convection = (it.flags & FJ_REUSE_CONVECTION) != 0;
         v[k].hg_n = it.bufs->d_hg_t + it.i_ts * hs;
         v[k].hgd_n = it.bufs->d_hg_dot_t + it.i_ts * hs;
         v[k].hg_nm1 = it.bufs->d_hg_t + (it.i_ts - 1) * hs;

@@ -158,11 +158,16 @@ class DeviceCase:
         _lib.call("fj_solve_static", C.byref(self.cfg), C.byref(self._bufs), int(horseshoe), float(t0),
                   self.ws.data_ptr(), self.ws.numel(), self._stream())
 
-    def solve_dynamic(self, i_first: int, i_last: int, reuse_factors: bool = False, graph: bool = True):
+    def solve_dynamic(self, i_first: int, i_last: int, reuse_factors: bool = False, graph: bool = True,
+                      reuse_convection: bool = False):
         """Steps i_first..i_last-1.  ``reuse_factors``: keep the mixed path's cached
         factors from the previous call on this case.  ``graph``: replay runs of steps from
-        one captured CUDA graph (False: launch every step directly; same results)."""
-        flags = (_lib.FJ_REUSE_FACTORS if reuse_factors else 0) | (0 if graph else _lib.FJ_NO_GRAPH)
+        one captured CUDA graph (False: launch every step directly; same results).
+        ``reuse_convection``: the previous call solved slot i_first from the same slot
+        i_first-1 and frames hg_t[i_first-1] (a fluid-structure iteration), so its free-wake
+        convection velocities are taken instead of recomputed."""
+        flags = ((_lib.FJ_REUSE_FACTORS if reuse_factors else 0) | (0 if graph else _lib.FJ_NO_GRAPH)
+                 | (_lib.FJ_REUSE_CONVECTION if reuse_convection else 0))
         _lib.call("fj_solve_prescribed_dynamic", C.byref(self.cfg), C.byref(self._bufs), int(i_first), int(i_last),
                   flags, self.ws.data_ptr(), self.ws.numel(), self._stream())
 

@@ -144,6 +144,8 @@ class UVLM:
         self.zeta_w_ref = None
         self.delta_w = None
         self._step_case = None
+        self._step_key = None
+        self._step_factored = False
 
     # ---------------------------------------------------------------------------------
     @property
@@ -196,6 +198,8 @@ class UVLM:
                 self.delta_w.append(dw)
         self.zeta_w_ref = self.initialise_wake()
         self._step_case = None
+        self._step_key = None
+        self._step_factored = False
 
     def hg_to_zeta_b(self, hg_n, cs_ang_n=None) -> ArrayList:
         """aero/uvlm.py:537-560 (host evaluation)."""
@@ -346,15 +350,30 @@ class UVLM:
                 case.set_arraylist_at_ts(k, getattr(snap, k), i_ts)
             return case
         hg_n = np.asarray(hg_n, dtype=np.float64)
+        hg_nm1 = np.asarray(hg_nm1, dtype=np.float64)
         n_nodes = hg_n.shape[0]
         dc = self._step_case
         if dc is None or dc.cfg.n_nodes != n_nodes:
             dc = self._step_case = self.make_device_case(2, n_nodes)
+            self._step_key = None
+            self._step_factored = False
         prev = case[i_ts - 1]
+        # A fluid-structure loop re-solves slot i_ts with new frames hg_n from the same
+        # converged slot i_ts-1: the free-wake convection (which depends on slot i_ts-1 and
+        # hg_nm1 only, uvlm.py:912-941) is then taken from the previous call.
+        key = (i_ts, hg_nm1, [np.asarray(a) for a in prev.gamma_b], [np.asarray(a) for a in prev.gamma_w],
+               [np.asarray(a) for a in prev.zeta_w])
+        old = self._step_key
+        reuse_conv = bool(self.free_wake and old is not None and old[0] == i_ts and np.array_equal(old[1], hg_nm1)
+                          and all(np.array_equal(a, b) for x, y in zip(old[2:], key[2:]) for a, b in zip(x, y)))
         self.load_initial(dc, prev)
-        dc.set_hg(np.stack([np.asarray(hg_nm1, dtype=np.float64), hg_n]),
-                  np.stack([np.zeros_like(hg_n), np.asarray(hg_dot_n, dtype=np.float64)]))
-        dc.solve_dynamic(1, 2)
+        dc.set_hg(np.stack([hg_nm1, hg_n]), np.stack([np.zeros_like(hg_n), np.asarray(hg_dot_n, dtype=np.float64)]))
+        # mixed: the FP32 factors of the previous call serve as the refinement's
+        # preconditioner; the residual check refactorises if they no longer do
+        dc.solve_dynamic(1, 2, reuse_factors=self._step_factored, reuse_convection=reuse_conv)
+        self._step_factored = self.precision == "mixed"
+        self._step_key = (key[0], key[1].copy(), [a.copy() for a in key[2]], [a.copy() for a in key[3]],
+                          [a.copy() for a in key[4]])
         out = self._to_case(dc, slots=slice(1, 2))
         for k in ("zeta_b", "zeta_b_dot", "zeta_w", "c", "nc", "gamma_b", "gamma_b_dot", "gamma_w", "f_steady",
                   "f_unsteady", "alpha"):

@@ -176,6 +176,12 @@ FJ_API int fj_solve_static(const fj_case_config* cfg, const fj_case_buffers* buf
  * zero pivot of the last factorisation. */
 #define FJ_REUSE_FACTORS 1
 #define FJ_NO_GRAPH 2
+/* Fluid-structure iterations re-solve one slot i with new frames hg_t[i] but the same
+ * converged slot i-1.  The free-wake convection velocity (aero/uvlm.py:912-941) depends
+ * only on slot i-1 and hg_t[i-1], so with FJ_REUSE_CONVECTION the first step of the call
+ * takes the velocities the previous call on this workspace computed for that slot instead
+ * of recomputing them (the caller guarantees slot i-1 and hg_t[i-1] are unchanged). */
+#define FJ_REUSE_CONVECTION 4
 FJ_API int fj_solve_prescribed_dynamic(const fj_case_config* cfg, const fj_case_buffers* bufs,
                                 int i_first, int i_last, int flags, void* d_ws,
                                 size_t ws_bytes, fj_stream_t stream);

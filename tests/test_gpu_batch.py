@@ -138,3 +138,32 @@ def test_batched_variable_and_uniform_wakes(cuda):
         for f in FIELDS:
             for a, b in zip(getattr(got, f), getattr(want, f)):
                 assert rel_err(a, b) < 1e-12, f
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 0.0), ("mixed", 1e-9)])
+def test_fsi_iterations_reuse_the_wake_convection(cuda, precision, tol):
+    """A fluid-structure loop re-solves one slot with new frames (UVLM.case_solve, as the
+    reference beam calls it).  The second and later iterations take the free-wake
+    convection (and, mixed, the factors) from the first: the final iterate equals a fresh
+    solve of that slot (FP64 bit for bit), with fewer kernel launches per iteration."""
+    from flapjax_b200 import _lib
+
+    c = cases.wing_free(m=4, n=10, m_star=12, n_steps=6, seed=2)
+    uv, _ = device_uvlm(c, precision)
+    case = uv.solve_prescribed_dynamic(uv.solve_static(), c.hg_t, c.hg_dot_t)
+    i = 4
+    rng = np.random.default_rng(0)
+    launches = []
+    for it in range(3):
+        hg_n = c.hg_t[i].copy()
+        hg_n[:, 2, 3] += 1e-3 * rng.normal(size=hg_n.shape[0])  # a structural iterate
+        l0 = _lib.load().fj_launch_count()
+        uv.case_solve(case, i, hg_n, c.hg_t[i - 1], c.hg_dot_t[i], static=False, horseshoe=False)
+        launches.append(_lib.load().fj_launch_count() - l0)
+    assert launches[1] < launches[0] and launches[2] == launches[1]
+    fresh, _ = device_uvlm(c, precision)
+    case2 = uv.solve_prescribed_dynamic(uv.solve_static(), c.hg_t, c.hg_dot_t)
+    fresh.case_solve(case2, i, hg_n, c.hg_t[i - 1], c.hg_dot_t[i], static=False, horseshoe=False)
+    for f in ("gamma_b", "gamma_w", "zeta_w", "f_steady", "f_unsteady"):
+        a, b = getattr(case, f)[0][i], getattr(case2, f)[0][i]
+        assert rel_err(a, b) <= tol, (f, rel_err(a, b))
