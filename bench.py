@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--small", action="store_true", help="a reduced workload (for quick checks)")
     ap.add_argument("--serving-cases", type=int, default=512, help="cases in the serving stream (0: skip)")
     ap.add_argument("--only-serving", action="store_true")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="config 3: twist gradient of time-mean CL and CD by the hand-written adjoint")
+    ap.add_argument("--adjoint-steps", type=int, default=1000)
     ap.add_argument("--configs", action="store_true",
                     help="the per-config table instead of the headline line: C1 heave 8x32/W64/50 steps, "
                          "C2 free wake 16x128/W200, C3 pitch 12x64/W100 primal")
@@ -309,6 +312,10 @@ def main():
         if rank == 0:
             print(json.dumps({"configs": config_table(args, torch)}))
         return 0
+    if args.adjoint:
+        if rank == 0:
+            print(json.dumps({"adjoint": adjoint_bench(args, torch)}))
+        return 0
     if args.only_serving:
         serving = serving_bench(args, torch)
         if world > 1:
@@ -519,6 +526,72 @@ def config_table(args, torch):
         res["cpu_sample_steps"] = [len(t_all), len(t_one)]
         rows[name] = res
     return rows
+
+
+def adjoint_bench(args, torch):
+    """Config 3: 12 x 64 wing, W = 100, 32 twist control angles ~ N(0, 1 deg), pitch 2 deg
+    at k = 0.3, checkpoints every 10 steps.  Gradient of time-mean CL and CD with respect
+    to the twist angles: FP64 forward, checkpointed recomputation, hand-written reverse
+    sweep.  Two twist angles are also checked by central differences of the FP64 GPU
+    forward (h = 1e-6; that forward's own roundoff limits such a difference to ~1e-4)."""
+    import flapjax_b200 as fj
+    from flapjax_b200 import cases
+    from flapjax_b200.adjoint import PrescribedAdjoint, twist_jacobian
+
+    c = cases.wing_pitch(n_steps=args.adjoint_steps)
+    theta = c.extra["twist_ctrl_rad"]
+    ctrl_y = np.linspace(0.0, c.span, len(theta))
+    span_y = np.linspace(0.0, c.span, c.n + 1)
+    jac = twist_jacobian(c.m, c.n, c.chord, 0.25, ctrl_y, span_y, np.interp(span_y, ctrl_y, theta))
+    a = np.deg2rad(c.alpha_deg)
+    q = 0.5 * c.rho * c.u_mag**2 * c.s_ref
+
+    def weights(e):
+        fw = np.zeros((c.n_tstep, 3))
+        fw[1:] = np.asarray(e) / (q * c.n_steps)
+        return fw
+
+    def uvlm(zeta_b0):
+        uv = fj.UVLM([fj.GridDiscretisation(c.m, c.n, c.m_star)], np.arange(c.n + 1), precision="fp64")
+        uv.set_design_variables(dt=c.dt, flowfield=fj.Constant(c.u_inf, c.rho, True), zeta_b0=zeta_b0, hg0=c.hg0)
+        return uv
+
+    def mean_coeffs(zeta_b0):
+        uv = uvlm(zeta_b0)
+        out = uv.solve_prescribed_dynamic(uv.solve_static(), c.hg_t, c.hg_dot_t)
+        return [float(np.sum(weights(e)[1:] * out.force_total[1:])) for e in (e_l, e_d)]
+
+    e_l, e_d = (-np.sin(a), 0.0, np.cos(a)), (np.cos(a), 0.0, np.sin(a))
+    uv = uvlm(c.zeta_b0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    uv.solve_prescribed_dynamic(uv.solve_static(), c.hg_t, c.hg_dot_t)
+    torch.cuda.synchronize()
+    t_fwd = time.perf_counter() - t0
+    res = {"workload": "12x64 wing, W=100, 32 twist angles, pitch 2 deg at k=0.3, checkpoint 10",
+           "steps": c.n_steps, "forward_s": t_fwd}
+    for name, e in (("CL", e_l), ("CD", e_d)):
+        t0 = time.perf_counter()
+        J, g = PrescribedAdjoint(uv).gradient(c.hg_t, c.hg_dot_t, weights(e), checkpoint=10)
+        torch.cuda.synchronize()
+        res[f"gradient_{name}_s"] = time.perf_counter() - t0
+        grad = np.einsum("kmjd,mjd->k", jac, g)
+        res[f"mean_{name}"] = J
+        res[f"d{name}_dtwist"] = grad.tolist()
+        checks = []
+        for k in (3, 17):
+            h = 1e-6
+            tp, tm = theta.copy(), theta.copy()
+            tp[k] += h
+            tm[k] -= h
+            jp = mean_coeffs(cases.twisted_grid(c.m, c.n, c.chord, 0.25, np.interp(span_y, ctrl_y, tp)))
+            jm = mean_coeffs(cases.twisted_grid(c.m, c.n, c.chord, 0.25, np.interp(span_y, ctrl_y, tm)))
+            idx = 0 if name == "CL" else 1
+            fd = (jp[idx] - jm[idx]) / (2 * h)
+            checks.append({"param": k, "adjoint": float(grad[k]), "central_fd_fp64_gpu": fd,
+                           "rel_diff": abs(fd - grad[k]) / max(abs(fd), 1e-30)})
+        res[f"fd_check_{name}"] = checks
+    return res
 
 
 def serving_bench(args, torch):
