@@ -27,8 +27,11 @@ Forward states are recomputed from checkpoints every ``checkpoint`` steps (only 
 checkpoint slots are kept), so device memory is O(checkpoint) slots and O(checkpoint)
 factor matrices.
 
-Scope: one surface, epsilon kernel, Constant flow, prescribed wake (uniform or variable,
-``delta_w``, with gradients through the arc-length re-discretisation), no mirror.
+Scope: one surface, epsilon or cutoff kernel, Constant flow, prescribed or free wake
+(uniform or variable, ``delta_w``, with gradients through the arc-length
+re-discretisation), no mirror.  The free wake adds, per step, the VJP of its convection
+velocity V(zeta_w_{n-1}; bound and wake of n-1): targets, both source lattices, both
+circulations; the bound lattice's share is carried to the reverse step of slot n-1.
 """
 from __future__ import annotations
 
@@ -46,11 +49,13 @@ FIELDS = ("zeta_b", "zeta_b_dot", "zeta_w", "c", "nc", "gamma_b", "gamma_b_dot",
 class _Dev:
     """Device helpers around the C ABI (FP64)."""
 
-    def __init__(self, device):
+    def __init__(self, device, kernel=None, r_cut=0.0):
         import torch
 
         self.torch = torch
         self.dev = device_of(device)
+        self.kernel = _lib.FJ_KERNEL_EPSILON if kernel is None else kernel
+        self.r_cut = float(r_cut)
         self._ws = {}
 
     def t(self, a):
@@ -81,7 +86,7 @@ class _Dev:
         ws = self.ws("vind", n.value)
         out = self.torch.empty_like(tt)
         _lib.call("fj_vind", tt.data_ptr(), tt.shape[0], zp, gp, rows, cols, len(lats), None, None,
-                  _lib.FJ_KERNEL_EPSILON, 0.0, _lib.FJ_PREC_FP64, out.data_ptr(), ws.data_ptr(), ws.numel(),
+                  self.kernel, self.r_cut, _lib.FJ_PREC_FP64, out.data_ptr(), ws.data_ptr(), ws.numel(),
                   self.stream())
         return out.cpu().numpy().reshape(targets.shape)
 
@@ -100,7 +105,7 @@ class _Dev:
         _lib.call("fj_vind_vjp_workspace_size", tt.shape[0], rows, cols, n, 0, C.byref(nb))
         ws = self.ws("vjp", nb.value)
         _lib.call("fj_vind_vjp", tt.data_ptr(), tt.shape[0], zp, gp, rows, cols, n, None, None,
-                  _lib.FJ_KERNEL_EPSILON, 0.0, tl.data_ptr(), tb.data_ptr(), zbp, gbp, ws.data_ptr(), ws.numel(),
+                  self.kernel, self.r_cut, tl.data_ptr(), tb.data_ptr(), zbp, gbp, ws.data_ptr(), ws.numel(),
                   self.stream())
         return (tb.cpu().numpy().reshape(targets.shape), [z.cpu().numpy() for z in zb],
                 [g.cpu().numpy() for g in gb])
@@ -134,7 +139,7 @@ class _Dev:
         _lib.call("fj_aic_workspace_size", mm, nn, 1, C.byref(w))
         ws = self.ws("aic", w.value)
         s = self.stream()
-        _lib.call("fj_aic_assemble", zp, mm, nn, 1, wp, ms, None, None, _lib.FJ_KERNEL_EPSILON, 0.0, a.data_ptr(),
+        _lib.call("fj_aic_assemble", zp, mm, nn, 1, wp, ms, None, None, self.kernel, self.r_cut, a.data_ptr(),
                   ws.data_ptr(), ws.numel(), s)
         piv = self.torch.empty(nb, dtype=self.torch.int32, device=self.dev)
         _lib.call("fj_lu_workspace_size", nb, C.byref(w))
@@ -197,14 +202,16 @@ def _interp_T(x, xp, fp, fbar):
     return xp_bar, fp_bar
 
 
-def _variable_wake_T(zw_nm1, te_n, gb_te_nm1, gw_nm1, dw, dt, U, Zw_bar, Gw_bar):
+def _variable_wake_T(zw_nm1, te_n, gb_te_nm1, gw_nm1, dw, dt, U, Zw_bar, Gw_bar, v_conv=None):
     """Transpose of propagate_surf_wake with delta_w for a prescribed wake
     (aero/utils.py:427-491, gradients through the arc lengths as the reference's default
     linearise_variable_wake=False).  Returns the cotangents of zeta_w at n-1, of the
     trailing-edge vertex row at n, of the trailing-edge circulation row at n-1 and of
-    gamma_w at n-1."""
+    gamma_w at n-1.  ``v_conv``: the free wake's induced velocity at zw_nm1 (its own VJP is
+    the caller's), so that the arc lengths are those of the convected rows."""
     W1, n1, _ = zw_nm1.shape          # W + 1 vertex rows, n + 1 columns
-    X = np.concatenate([te_n[None], zw_nm1 + dt * U], axis=0)  # (W + 2, n + 1, 3)
+    vel = U if v_conv is None else U + v_conv                  # free wake: + induced velocity
+    X = np.concatenate([te_n[None], zw_nm1 + dt * vel], axis=0)  # (W + 2, n + 1, 3)
     G = np.concatenate([gb_te_nm1[None], gw_nm1], axis=0)      # (W + 1, n)
     seg = np.linalg.norm(X[1:] - X[:-1], axis=-1)              # (W + 1, n + 1)
     S = np.concatenate([np.zeros((1, n1)), np.cumsum(seg, axis=0)], axis=0)
@@ -254,10 +261,10 @@ class PrescribedAdjoint:
     def __init__(self, uvlm, device=None):
         if uvlm.n_surf != 1:
             raise NotImplementedError("the adjoint handles one surface")
-        if uvlm.kernel.kernel_id != _lib.FJ_KERNEL_EPSILON:
-            raise NotImplementedError("the adjoint is written for the epsilon kernel")
-        if uvlm.mirror_point is not None or uvlm.free_wake:
-            raise NotImplementedError("the adjoint covers prescribed wakes without images")
+        if uvlm.kernel.kernel_id not in (_lib.FJ_KERNEL_EPSILON, _lib.FJ_KERNEL_CUTOFF):
+            raise NotImplementedError("the adjoint is written for the epsilon and cutoff kernels")
+        if uvlm.mirror_point is not None:
+            raise NotImplementedError("the adjoint covers wakes without images")
         if uvlm.precision != "fp64":
             raise NotImplementedError("the adjoint runs in FP64")
         from .flowfields import Constant
@@ -265,7 +272,7 @@ class PrescribedAdjoint:
         if not isinstance(uvlm.flowfield, Constant):
             raise NotImplementedError("the adjoint assumes a uniform (Constant) flow")
         self.uv = uvlm
-        self.d = _Dev(device)
+        self.d = _Dev(device, uvlm.kernel.kernel_id, uvlm.kernel.r_cut)
 
     # -- forward with checkpoints ------------------------------------------------------
     def _static(self):
@@ -323,22 +330,22 @@ class PrescribedAdjoint:
         Gbd_next = np.zeros((m, n_))
         Gw_next = np.zeros((W, n_))
         Zw_next = np.zeros((W + 1, n_ + 1, 3))
+        Zb_next = np.zeros((m + 1, n_ + 1, 3))  # free wake: cotangent of slot n's lattice from step n+1
         seg_starts = sorted(k for k in ckpt if k < N)
         for s0 in reversed(seg_starts):
             s1 = min(N, s0 + checkpoint)
             seg = self._run_segment(ckpt[s0], hg_t[s0:s1 + 1], hg_dot_t[s0:s1 + 1], keep_factors=True)
             for loc in range(s1 - s0, 0, -1):
                 nstep = s0 + loc
-                Gb_prev, Gbd_prev, Gw_prev, Zw_prev = self._reverse_step(
-                    seg, loc, fw[nstep], Gb_next, Gbd_next, Gw_next, Zw_next, zeta0_bar, hg_t[nstep],
+                Gb_next, Gbd_next, Gw_next, Zw_next, Zb_next = self._reverse_step(
+                    seg, loc, fw[nstep], Gb_next, Gbd_next, Gw_next, Zw_next, Zb_next, zeta0_bar, hg_t[nstep],
                     hg_dot_t[nstep], dof, m, n_, W, dt, relax, rho, U)
-                Gb_next, Gbd_next, Gw_next, Zw_next = Gb_prev, Gbd_prev, Gw_prev, Zw_prev
-        self._reverse_static(static, Gb_next, Gw_next, Zw_next, zeta0_bar, uv.hg_ref, dof, m, n_, W, U)
+        self._reverse_static(static, Gb_next, Gw_next, Zw_next, Zb_next, zeta0_bar, uv.hg_ref, dof, m, n_, W, U)
         return J, zeta0_bar
 
     # -- one dynamic reverse step ------------------------------------------------------
-    def _reverse_step(self, seg, loc, Fbar, Gb_n, Gbd_n, Gw_n, Zw_n, zeta0_bar, hg_n, hgd_n, dof, m, n_, W, dt,
-                      relax, rho, U):
+    def _reverse_step(self, seg, loc, Fbar, Gb_n, Gbd_n, Gw_n, Zw_n, Zb_n, zeta0_bar, hg_n, hgd_n, dof, m, n_, W,
+                      dt, relax, rho, U):
         d = self.d
         zb = seg.zeta_b[0][loc]
         zbd = seg.zeta_b_dot[0][loc]
@@ -348,7 +355,7 @@ class PrescribedAdjoint:
         gbd = seg.gamma_b_dot[0][loc]
         nc = seg.nc[0][loc]
         c = seg.c[0][loc]
-        Zb = np.zeros_like(zb)
+        Zb = Zb_n.copy()
         Zbd = np.zeros_like(zbd)
         Gb = Gb_n.copy()
         Gw = Gw_n.copy()
@@ -430,16 +437,22 @@ class PrescribedAdjoint:
         Zb += _avg4_T(cbar, zb.shape)
         Zb += _normals_T(zb, ncbar)
         Zbd += _avg4_T(cdotbar, zbd.shape)
-        # 6. wake shedding transposes
+        # 6. wake shedding transposes; the free wake's convection velocity
+        #    V(zw_{n-1}; bound n-1, wake n-1) adds its own VJP
+        zw_nm1, gw_nm1 = seg.zeta_w[0][loc - 1], seg.gamma_w[0][loc - 1]
+        zb_nm1, gb_nm1 = seg.zeta_b[0][loc - 1], seg.gamma_b[0][loc - 1]
+        free = bool(self.uv.free_wake) and W > 0
+        lats_nm1 = [(zb_nm1, gb_nm1), (zw_nm1, gw_nm1)]
         dw = self.uv.delta_w[0] if getattr(self.uv, "delta_w", None) else None
         if dw is not None:
+            v_conv = d.vind(zw_nm1, lats_nm1) if free else None
             zw_p, te_bar, gte_bar, gw_p = _variable_wake_T(
-                seg.zeta_w[0][loc - 1], zb[-1], seg.gamma_b[0][loc - 1][-1], seg.gamma_w[0][loc - 1],
-                np.asarray(dw, float), dt, U, Zw, Gw)
+                zw_nm1, zb[-1], gb_nm1[-1], gw_nm1, np.asarray(dw, float), dt, U, Zw, Gw, v_conv)
             Zb[-1] += te_bar
             Zw_prev = zw_p
             Gw_prev = gw_p
             Gb_prev[-1, :] += gte_bar
+            conv_rows, conv_bar = slice(None), zw_p  # every row of zw_{n-1} is convected
         else:
             Zb[-1] += Zw[0]
             Zw_prev = np.zeros_like(Zw)
@@ -448,11 +461,21 @@ class PrescribedAdjoint:
             if W > 0:
                 Gb_prev[-1, :] += Gw[0, :]
                 Gw_prev[:-1] += Gw[1:]
+            conv_rows, conv_bar = slice(0, W), Zw[1:]
+        Zb_prev = np.zeros_like(zb)
+        if free:
+            conv_bar = np.array(conv_bar)  # x_r = zw_{n-1,r} + dt (U + V(zw_{n-1,r})): lam = dt x_bar
+            tbar, zbar_c, gbar_c = d.vjp(zw_nm1[conv_rows], lats_nm1, dt * conv_bar)
+            Zw_prev[conv_rows] += tbar
+            Zb_prev += zbar_c[0]
+            Zw_prev += zbar_c[1]
+            Gb_prev += gbar_c[0]
+            Gw_prev += gbar_c[1]
         # 7. node frames
         zeta0_bar += _frames_T(Zb, Zbd, hg_n, hgd_n, dof)
-        return Gb_prev, Gbd_prev, Gw_prev, Zw_prev
+        return Gb_prev, Gbd_prev, Gw_prev, Zw_prev, Zb_prev
 
-    def _reverse_static(self, st, Gb0, Gw0, Zw0, zeta0_bar, hg0, dof, m, n_, W, U):
+    def _reverse_static(self, st, Gb0, Gw0, Zw0, Zb0, zeta0_bar, hg0, dof, m, n_, W, U):
         d = self.d
         zb = st.zeta_b[0]
         zw = st.zeta_w[0]
@@ -470,7 +493,7 @@ class PrescribedAdjoint:
         ncbar = -mu[..., None] * (U + Vtot)
         cbar, zbar, _ = d.vjp(c, lats, -mu[..., None] * nc)
         Zw += zbar[0]
-        Zb = zbar[1]
+        Zb = zbar[1] + Zb0
         Zb[-1] += Zw.sum(axis=0)  # every wake row = TE + s_r u_dir (uvlm.py:662-689)
         Zb += _avg4_T(cbar, zb.shape)
         Zb += _normals_T(zb, ncbar)

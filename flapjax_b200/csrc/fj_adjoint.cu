@@ -5,7 +5,9 @@
 // operators that carry the cost have hand-written adjoints:
 //   * the Biot-Savart sum v(x) = sum_s K(x; y0_s, y1_s) g_s (compute_v_ind,
 //     aero/aic.py:248-310) -- cotangent lam(x) -> x_bar, vertex adjoints of every source
-//     lattice, ring-circulation adjoints (FP64, epsilon kernel, aero/utils.py:606-623);
+//     lattice, ring-circulation adjoints (FP64; epsilon kernel aero/utils.py:606-623, and
+//     the cutoff kernel :626-648, whose D is |c|^2 and whose pairs within the cutoff
+//     radius of the filament line contribute nothing, derivative included);
 //   * the dense solve (aero/uvlm.py:985) -- A^T mu = lam with the getrf factors of A.
 // K's derivative: with r1 = x - y0, r2 = x - y1, r0 = y1 - y0, c = r1 x r2,
 // u_i = r_i / n_i, n_i = sqrt(|r_i|^2 + eps^2), dot = r0.(u1 - u2), D = |c|^2 + eps|r0|^4,
@@ -53,14 +55,27 @@ __device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
 }
 
 // d(lam . K)/dr1 -> g1, d(lam . K)/dr2 -> g2 (each scaled by g), and lam . K (unit g).
+// KER: FJ_KERNEL_EPSILON (D = |c|^2 + eps |r0|^4) or FJ_KERNEL_CUTOFF (D = |c|^2, zero
+// within rc2 of the filament line, aero/utils.py:637-648).
+template <int KER>
 __device__ __forceinline__ void link_vjp(const VtxA& A, const VtxA& B, const double r0[3], double g,
-                                         const double lam[3], double g1[3], double g2[3], double& lk) {
+                                         const double lam[3], double rc2, double g1[3], double g2[3], double& lk) {
     double c[3];
     cross3(A.d, B.d, c);
     const double du[3] = {A.u[0] - B.u[0], A.u[1] - B.u[1], A.u[2] - B.u[2]};
     const double dot = dot3(r0, du);
     const double r0sq = dot3(r0, r0);
-    const double D = dot3(c, c) + kEps * r0sq * r0sq;
+    if (KER == FJ_KERNEL_CUTOFF) {
+        const double sm = dot3(r0, A.d) / r0sq;
+        const double mx = A.d[0] - sm * r0[0], my = A.d[1] - sm * r0[1], mz = A.d[2] - sm * r0[2];
+        if (!(mx * mx + my * my + mz * mz > rc2)) {
+            g1[0] = g1[1] = g1[2] = g2[0] = g2[1] = g2[2] = 0.0;
+            lk = 0.0;
+            return;
+        }
+    }
+    const double eps_term = KER == FJ_KERNEL_EPSILON ? kEps * r0sq * r0sq : 0.0;
+    const double D = dot3(c, c) + eps_term;
     const double inv = 1.0 / (kFourPi * D);
     const double s = dot * inv;
     const double a = dot3(lam, c);
@@ -72,9 +87,10 @@ __device__ __forceinline__ void link_vjp(const VtxA& A, const VtxA& B, const dou
     double r2c[3], cr1[3];
     cross3(B.d, c, r2c);
     cross3(c, A.d, cr1);
+    const double e4 = KER == FJ_KERNEL_EPSILON ? 4.0 * kEps * r0sq : 0.0;
     for (int k = 0; k < 3; ++k) {
-        dD1[k] = 2.0 * r2c[k] + 4.0 * kEps * r0sq * r0[k];
-        dD2[k] = 2.0 * cr1[k] - 4.0 * kEps * r0sq * r0[k];
+        dD1[k] = 2.0 * r2c[k] + e4 * r0[k];
+        dD2[k] = 2.0 * cr1[k] - e4 * r0[k];
     }
     const double q = dot / D;
     for (int k = 0; k < 3; ++k) {
@@ -86,10 +102,11 @@ __device__ __forceinline__ void link_vjp(const VtxA& A, const VtxA& B, const dou
 }
 
 // Pass 1: target adjoints.  Walks the stream as the forward sum does.
+template <int KER>
 __global__ void __launch_bounds__(kAdjBlock) vjp_targets_kernel(const double* __restrict__ tgt,
                                                                 const double* __restrict__ lam, int64_t n_t,
                                                                 const Elem64* __restrict__ st, int64_t n_elem,
-                                                                int n_split, double* __restrict__ part) {
+                                                                int n_split, double rc2, double* __restrict__ part) {
     __shared__ Elem64 sh[kAdjBlock];
     const int split = blockIdx.y;
     const int64_t per = (n_elem + n_split - 1) / n_split;
@@ -117,7 +134,7 @@ __global__ void __launch_bounds__(kAdjBlock) vjp_targets_kernel(const double* __
                 if (pl.q >= 0.0) {
                     const double r0[3] = {pl.r0x, pl.r0y, pl.r0z};
                     double g1[3], g2[3], lk;
-                    link_vjp(prev, v, r0, pl.g, lm, g1, g2, lk);
+                    link_vjp<KER>(prev, v, r0, pl.g, lm, rc2, g1, g2, lk);
                     acc[0] += g1[0] + g2[0];
                     acc[1] += g1[1] + g2[1];
                     acc[2] += g1[2] + g2[2];
@@ -138,10 +155,11 @@ __global__ void __launch_bounds__(kAdjBlock) vjp_targets_kernel(const double* __
 // Pass 2: filament adjoints.  Thread per stream element e (the link e -> e+1); targets
 // of this CTA's split staged through shared memory.  Output per element and split:
 // [y0_bar(3), y1_bar(3), g_bar].
+template <int KER>
 __global__ void __launch_bounds__(kAdjBlock) vjp_links_kernel(const double* __restrict__ tgt,
                                                               const double* __restrict__ lam, int64_t n_t,
                                                               const Elem64* __restrict__ st, int64_t n_elem,
-                                                              int n_split, double* __restrict__ part) {
+                                                              int n_split, double rc2, double* __restrict__ part) {
     __shared__ double sx[kAdjBlock][6];
     const int split = blockIdx.y;
     const int64_t per = (n_t + n_split - 1) / n_split;
@@ -178,7 +196,7 @@ __global__ void __launch_bounds__(kAdjBlock) vjp_links_kernel(const double* __re
                 vtxa(x, a.x, a.y, a.z, A);
                 vtxa(x, b.x, b.y, b.z, B);
                 double g1[3], g2[3], lk;
-                link_vjp(A, B, r0, a.g, lm, g1, g2, lk);
+                link_vjp<KER>(A, B, r0, a.g, lm, rc2, g1, g2, lk);
                 for (int k = 0; k < 3; ++k) {
                     y0b[k] -= g1[k];
                     y1b[k] -= g2[k];
@@ -385,9 +403,9 @@ int fj_vind_vjp(const double* d_targets, int64_t n_targets, const double* const*
                 const double* d_lam, double* d_targets_bar, double* const* d_zetas_bar, double* const* d_gammas_bar,
                 void* d_ws, size_t ws_bytes, fj_stream_t stream) {
     cudaStream_t s = (cudaStream_t)stream;
-    if (kernel != FJ_KERNEL_EPSILON)
-        return fail(FJ_ERR_UNSUPPORTED, "fj_vind_vjp: only the epsilon kernel has a hand-written adjoint");
-    (void)r_cut;
+    if (kernel != FJ_KERNEL_EPSILON && kernel != FJ_KERNEL_CUTOFF)
+        return fail(FJ_ERR_UNSUPPORTED, "fj_vind_vjp: the epsilon and cutoff kernels have hand-written adjoints");
+    const double rc2 = r_cut * r_cut;
     const int mirror = mirror_point != nullptr && mirror_normal != nullptr;
     const int img = mirror ? 2 : 1;
     size_t need;
@@ -438,13 +456,25 @@ int fj_vind_vjp(const double* d_targets, int64_t n_targets, const double* const*
     FJ_TRY(pack_stream64(pa, st, s));
     if (d_targets_bar) {
         dim3 g((unsigned)((n_targets + kAdjBlock - 1) / kAdjBlock), (unsigned)st_split);
-        vjp_targets_kernel<<<g, kAdjBlock, 0, s>>>(d_targets, d_lam, n_targets, st, ne, st_split, part_t); note_launch();
+        if (kernel == FJ_KERNEL_EPSILON)
+            vjp_targets_kernel<FJ_KERNEL_EPSILON><<<g, kAdjBlock, 0, s>>>(d_targets, d_lam, n_targets, st, ne,
+                                                                          st_split, rc2, part_t);
+        else
+            vjp_targets_kernel<FJ_KERNEL_CUTOFF><<<g, kAdjBlock, 0, s>>>(d_targets, d_lam, n_targets, st, ne,
+                                                                         st_split, rc2, part_t);
+        note_launch();
         sum_splits_kernel<<<(unsigned)((n_targets * 3 + 255) / 256), 256, 0, s>>>(part_t, st_split, n_targets * 3,
                                                                                  d_targets_bar, 1); note_launch();
     }
     if (d_zetas_bar || d_gammas_bar) {
         dim3 g((unsigned)((ne + kAdjBlock - 1) / kAdjBlock), (unsigned)l_split);
-        vjp_links_kernel<<<g, kAdjBlock, 0, s>>>(d_targets, d_lam, n_targets, st, ne, l_split, part_l); note_launch();
+        if (kernel == FJ_KERNEL_EPSILON)
+            vjp_links_kernel<FJ_KERNEL_EPSILON><<<g, kAdjBlock, 0, s>>>(d_targets, d_lam, n_targets, st, ne, l_split,
+                                                                        rc2, part_l);
+        else
+            vjp_links_kernel<FJ_KERNEL_CUTOFF><<<g, kAdjBlock, 0, s>>>(d_targets, d_lam, n_targets, st, ne, l_split,
+                                                                       rc2, part_l);
+        note_launch();
         sum_splits_kernel<<<(unsigned)((ne * 7 + 255) / 256), 256, 0, s>>>(part_l, l_split, ne * 7, el, 0); note_launch();
         for (int li = 0; li < n; ++li) {
             const int64_t nv = (int64_t)(ua.lat[li].rows + 1) * (ua.lat[li].cols + 1);

@@ -9,7 +9,7 @@ import numpy as np
 
 from flapjax_b200.adjoint import PrescribedAdjoint
 from oracle import uvlm_ref as R
-from oracle.uvlm_vjp import bs_epsilon_vjp
+from oracle.uvlm_vjp import bs_vjp
 
 _KEYS = ("zeta_b", "zeta_b_dot", "zeta_w", "c", "nc", "gamma_b", "gamma_b_dot", "gamma_w", "f_steady", "f_unsteady",
          "alpha")
@@ -38,8 +38,12 @@ class _Seg:
 
 
 class OracleDev:
+    def __init__(self, kernel=R.KERNEL_EPSILON, r_cut=R.R_CUTOFF):
+        self.kernel = kernel
+        self.r_cut = r_cut
+
     def vind(self, targets, lats):
-        return R.compute_v_ind(targets, [z for z, _ in lats], [g for _, g in lats], R.KERNEL_EPSILON)
+        return R.compute_v_ind(targets, [z for z, _ in lats], [g for _, g in lats], self.kernel, None, self.r_cut)
 
     def vjp(self, targets, lats, lam):
         t = targets.reshape(-1, 3)
@@ -54,10 +58,10 @@ class OracleDev:
             for segs, gs, gbar, kind in ((R.chordwise_segments(z), g_m, gbar_m, "m"),
                                           (R.spanwise_segments(z), g_n, gbar_n, "n")):
                 y0, y1 = segs[..., 0, :], segs[..., 1, :]
-                kv = R.bs_epsilon(t[:, None, None, :], y0[None], y1[None])
+                kv = R.kernel_eval(self.kernel, t[:, None, None, :], y0[None], y1[None], self.r_cut)
                 gbar += np.einsum("tijk,tk->ij", kv, lm)
-                xb, y0b, y1b = bs_epsilon_vjp(t[:, None, None, :], y0[None], y1[None],
-                                              lm[:, None, None, :] * gs[None, ..., None])
+                xb, y0b, y1b = bs_vjp(t[:, None, None, :], y0[None], y1[None],
+                                      lm[:, None, None, :] * gs[None, ..., None], self.kernel, self.r_cut)
                 tb += xb.sum(axis=(1, 2))
                 y0b, y1b = y0b.sum(0), y1b.sum(0)
                 if kind == "m":      # chordwise filament (k,l): zeta[k,l] -> zeta[k+1,l]
@@ -76,7 +80,7 @@ class OracleDev:
         c = R.compute_surf_c(zeta_b)
         nc = R.compute_surf_nc(zeta_b)
         a = R.compute_aic_solve([c], [nc], [zeta_b], None if zeta_w_static is None else [zeta_w_static],
-                                R.KERNEL_EPSILON)
+                                self.kernel, None, self.r_cut)
         return np.linalg.solve(a.T, rhs.ravel()).reshape(rhs.shape)
 
 
@@ -85,7 +89,7 @@ class OracleAdjoint(PrescribedAdjoint):
 
     def __init__(self, ref):
         self.uv = ref
-        self.d = OracleDev()
+        self.d = OracleDev(ref.kernel, ref.r_cut)
 
     def _static(self):
         return _Snap(self.uv.solve_static(), 0)

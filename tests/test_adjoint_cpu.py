@@ -101,3 +101,43 @@ def test_reverse_sweep_variable_wake_matches_finite_differences():
         d = rng.normal(size=c.zeta_b0.shape) * 0.1
         fd = central_difference(c, d, fw, delta_w=dw)
         assert abs(fd - np.sum(g * d)) <= 1e-6 * abs(fd), (fd, np.sum(g * d))
+
+
+@pytest.mark.parametrize("kernel,dw_growth", [("cutoff", None), ("epsilon", None), ("cutoff", 1.15)])
+def test_reverse_sweep_free_wake_matches_finite_differences(kernel, dw_growth):
+    """Free wake (the convection velocity's VJP, whose bound-lattice share is carried to
+    the previous step), with the epsilon or the cutoff kernel and optionally delta_w,
+    against extended-precision central differences."""
+    c = cases.wing_free(m=3, n=4, m_star=4, n_steps=4, seed=1)
+    c = cases.WingCase(**{**c.__dict__, "kernel": kernel, "r_cut": 1e-3 if kernel == "cutoff" else 1e-4})
+    dw = None if dw_growth is None else c.dt * c.u_mag * dw_growth ** np.arange(c.m_star)
+    fw = coefficient_weights(c, "CL")
+    uv, ff = oracle_uvlm(c)
+    if dw is not None:
+        uv.set_design_variables(c.dt, ff, c.zeta_b0, c.hg0, delta_w=dw)
+    J, g = OracleAdjoint(uv).gradient(c.hg_t, c.hg_dot_t, fw, checkpoint=2)
+    assert abs(J - forward_objective(c, c.zeta_b0, fw, dw)) < 1e-13 * abs(J)
+    rng = np.random.default_rng(1)
+    for _ in range(2):
+        d = rng.normal(size=c.zeta_b0.shape) * 0.1
+        fd = central_difference(c, d, fw, delta_w=dw)
+        assert abs(fd - np.sum(g * d)) <= 1e-6 * abs(fd), (fd, np.sum(g * d))
+
+
+def test_cutoff_vjp_finite_differences():
+    from oracle.uvlm_vjp import bs_vjp
+
+    rng = np.random.default_rng(4)
+    x = rng.normal(size=(64, 3))
+    y0 = rng.normal(size=(64, 3))
+    y1 = y0 + rng.normal(size=(64, 3))
+    lam = rng.normal(size=(64, 3))
+    xb, y0b, y1b = bs_vjp(x, y0, y1, lam, R.KERNEL_CUTOFF, 1e-3)
+    h = 1e-6
+    for arg, bar in ((0, xb), (1, y0b), (2, y1b)):
+        for k in range(3):
+            p, m = [x.copy(), y0.copy(), y1.copy()], [x.copy(), y0.copy(), y1.copy()]
+            p[arg][:, k] += h
+            m[arg][:, k] -= h
+            fd = np.sum(lam * (R.bs_cutoff(*p, 1e-3) - R.bs_cutoff(*m, 1e-3)), axis=-1) / (2 * h)
+            assert np.max(np.abs(fd - bar[:, k])) <= 1e-7 * max(1.0, np.max(np.abs(bar[:, k])))

@@ -200,3 +200,37 @@ def test_device_sweep_variable_wake(cuda):
     d = np.random.default_rng(2).normal(size=c.zeta_b0.shape) * 0.1
     fd = central_difference(c, d, fw, delta_w=dw)
     assert abs(fd - np.sum(g * d)) <= 1e-6 * abs(fd)
+
+
+def test_cutoff_vind_vjp_matches_oracle(cuda):
+    from flapjax_b200 import _lib
+    from flapjax_b200.adjoint import _Dev
+
+    rng = np.random.default_rng(7)
+    lats = _lattices(rng)
+    tg = rng.normal(size=(40, 3)) * [1.0, 1.5, 0.4] + [0.8, 1.0, 0.0]
+    lam = rng.normal(size=(40, 3))
+    got = _Dev(cuda, _lib.FJ_KERNEL_CUTOFF, 1e-3).vjp(tg, lats, lam)
+    want = OracleDev(R.KERNEL_CUTOFF, 1e-3).vjp(tg, lats, lam)
+    for a, b in [(got[0], want[0])] + list(zip(got[1], want[1])) + list(zip(got[2], want[2])):
+        assert np.max(np.abs(a - b)) <= 1e-10 * np.max(np.abs(b))
+
+
+@pytest.mark.parametrize("kernel", ["cutoff", "epsilon"])
+def test_device_sweep_free_wake(cuda, kernel):
+    """Free wake (the headline workload's kernel: cutoff 1e-3): device sweep against the
+    oracle sweep and against extended-precision central differences."""
+    from flapjax_b200.adjoint import PrescribedAdjoint
+
+    c = cases.wing_free(m=3, n=5, m_star=5, n_steps=5, seed=2)
+    c = cases.WingCase(**{**c.__dict__, "kernel": kernel, "r_cut": 1e-3 if kernel == "cutoff" else 1e-4})
+    fw = coefficient_weights(c, "CL")
+    uv, _ = device_uvlm(c, "fp64")
+    J, g = PrescribedAdjoint(uv, cuda).gradient(c.hg_t, c.hg_dot_t, fw, checkpoint=2)
+    ref, _ = oracle_uvlm(c)
+    J_o, g_o = OracleAdjoint(ref).gradient(c.hg_t, c.hg_dot_t, fw, checkpoint=2)
+    assert abs(J - J_o) <= 1e-10 * abs(J_o)
+    assert np.max(np.abs(g - g_o)) <= 1e-8 * np.max(np.abs(g_o))
+    d = np.random.default_rng(3).normal(size=c.zeta_b0.shape) * 0.1
+    fd = central_difference(c, d, fw)
+    assert abs(fd - np.sum(g * d)) <= 1e-6 * abs(fd)
