@@ -27,9 +27,9 @@ Forward states are recomputed from checkpoints every ``checkpoint`` steps (only 
 checkpoint slots are kept), so device memory is O(checkpoint) slots and O(checkpoint)
 factor matrices.
 
-Scope: one surface, epsilon or cutoff kernel, Constant flow, prescribed or free wake
-(uniform or variable, ``delta_w``, with gradients through the arc-length
-re-discretisation), no mirror.  The free wake adds, per step, the VJP of its convection
+Scope: one surface (with or without a mirror image), epsilon or cutoff kernel, Constant
+flow, prescribed or free wake (uniform or variable, ``delta_w``, with gradients through
+the arc-length re-discretisation).  The free wake adds, per step, the VJP of its convection
 velocity V(zeta_w_{n-1}; bound and wake of n-1): targets, both source lattices, both
 circulations; the bound lattice's share is carried to the reverse step of slot n-1.
 """
@@ -49,13 +49,16 @@ FIELDS = ("zeta_b", "zeta_b_dot", "zeta_w", "c", "nc", "gamma_b", "gamma_b_dot",
 class _Dev:
     """Device helpers around the C ABI (FP64)."""
 
-    def __init__(self, device, kernel=None, r_cut=0.0):
+    def __init__(self, device, kernel=None, r_cut=0.0, mirror=None):
         import torch
 
         self.torch = torch
         self.dev = device_of(device)
         self.kernel = _lib.FJ_KERNEL_EPSILON if kernel is None else kernel
         self.r_cut = float(r_cut)
+        # image system across the plane (point, unit normal): host arrays for the C ABI
+        self._mir = None if mirror is None else tuple(
+            (C.c_double * 3)(*np.asarray(v, dtype=np.float64).tolist()) for v in mirror)
         self._ws = {}
 
     def t(self, a):
@@ -82,10 +85,12 @@ class _Dev:
         tt = self.t(targets.reshape(-1, 3))
         zs, gs, zp, gp, rows, cols = self._lat(lats)
         n = C.c_size_t()
-        _lib.call("fj_vind_workspace_size", tt.shape[0], rows, cols, len(lats), 0, _lib.FJ_PREC_FP64, C.byref(n))
+        mir = int(self._mir is not None)
+        mp, mn = self._mir if mir else (None, None)
+        _lib.call("fj_vind_workspace_size", tt.shape[0], rows, cols, len(lats), mir, _lib.FJ_PREC_FP64, C.byref(n))
         ws = self.ws("vind", n.value)
         out = self.torch.empty_like(tt)
-        _lib.call("fj_vind", tt.data_ptr(), tt.shape[0], zp, gp, rows, cols, len(lats), None, None,
+        _lib.call("fj_vind", tt.data_ptr(), tt.shape[0], zp, gp, rows, cols, len(lats), mp, mn,
                   self.kernel, self.r_cut, _lib.FJ_PREC_FP64, out.data_ptr(), ws.data_ptr(), ws.numel(),
                   self.stream())
         return out.cpu().numpy().reshape(targets.shape)
@@ -102,9 +107,11 @@ class _Dev:
         zbp = (C.c_void_p * n)(*[z.data_ptr() for z in zb])
         gbp = (C.c_void_p * n)(*[g.data_ptr() for g in gb])
         nb = C.c_size_t()
-        _lib.call("fj_vind_vjp_workspace_size", tt.shape[0], rows, cols, n, 0, C.byref(nb))
+        mir = int(self._mir is not None)
+        mp, mn = self._mir if mir else (None, None)
+        _lib.call("fj_vind_vjp_workspace_size", tt.shape[0], rows, cols, n, mir, C.byref(nb))
         ws = self.ws("vjp", nb.value)
-        _lib.call("fj_vind_vjp", tt.data_ptr(), tt.shape[0], zp, gp, rows, cols, n, None, None,
+        _lib.call("fj_vind_vjp", tt.data_ptr(), tt.shape[0], zp, gp, rows, cols, n, mp, mn,
                   self.kernel, self.r_cut, tl.data_ptr(), tb.data_ptr(), zbp, gbp, ws.data_ptr(), ws.numel(),
                   self.stream())
         return (tb.cpu().numpy().reshape(targets.shape), [z.cpu().numpy() for z in zb],
@@ -139,7 +146,8 @@ class _Dev:
         _lib.call("fj_aic_workspace_size", mm, nn, 1, C.byref(w))
         ws = self.ws("aic", w.value)
         s = self.stream()
-        _lib.call("fj_aic_assemble", zp, mm, nn, 1, wp, ms, None, None, self.kernel, self.r_cut, a.data_ptr(),
+        mp, mn = self._mir if self._mir is not None else (None, None)
+        _lib.call("fj_aic_assemble", zp, mm, nn, 1, wp, ms, mp, mn, self.kernel, self.r_cut, a.data_ptr(),
                   ws.data_ptr(), ws.numel(), s)
         piv = self.torch.empty(nb, dtype=self.torch.int32, device=self.dev)
         _lib.call("fj_lu_workspace_size", nb, C.byref(w))
@@ -263,8 +271,6 @@ class PrescribedAdjoint:
             raise NotImplementedError("the adjoint handles one surface")
         if uvlm.kernel.kernel_id not in (_lib.FJ_KERNEL_EPSILON, _lib.FJ_KERNEL_CUTOFF):
             raise NotImplementedError("the adjoint is written for the epsilon and cutoff kernels")
-        if uvlm.mirror_point is not None:
-            raise NotImplementedError("the adjoint covers wakes without images")
         if uvlm.precision != "fp64":
             raise NotImplementedError("the adjoint runs in FP64")
         from .flowfields import Constant
@@ -272,7 +278,8 @@ class PrescribedAdjoint:
         if not isinstance(uvlm.flowfield, Constant):
             raise NotImplementedError("the adjoint assumes a uniform (Constant) flow")
         self.uv = uvlm
-        self.d = _Dev(device, uvlm.kernel.kernel_id, uvlm.kernel.r_cut)
+        mirror = None if uvlm.mirror_point is None else (uvlm.mirror_point, uvlm.mirror_normal)
+        self.d = _Dev(device, uvlm.kernel.kernel_id, uvlm.kernel.r_cut, mirror)
 
     # -- forward with checkpoints ------------------------------------------------------
     def _static(self):

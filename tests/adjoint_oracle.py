@@ -38,14 +38,27 @@ class _Seg:
 
 
 class OracleDev:
-    def __init__(self, kernel=R.KERNEL_EPSILON, r_cut=R.R_CUTOFF):
+    def __init__(self, kernel=R.KERNEL_EPSILON, r_cut=R.R_CUTOFF, mirror=None):
         self.kernel = kernel
         self.r_cut = r_cut
+        self.mirror = mirror
 
     def vind(self, targets, lats):
-        return R.compute_v_ind(targets, [z for z, _ in lats], [g for _, g in lats], self.kernel, None, self.r_cut)
+        return R.compute_v_ind(targets, [z for z, _ in lats], [g for _, g in lats], self.kernel, self.mirror,
+                               self.r_cut)
 
     def vjp(self, targets, lats, lam):
+        """With a mirror plane the image lattice (reflected vertices, strengths negated)
+        adds its VJP, reflected back onto the original vertices."""
+        tb, zb, gb = self._vjp(targets, lats, lam)
+        if self.mirror is None:
+            return tb, zb, gb
+        p, nrm = (np.asarray(v, float) for v in self.mirror)
+        refl = np.eye(3) - 2.0 * np.outer(nrm, nrm)
+        tb2, zb2, gb2 = self._vjp(targets, [(R.mirror_grid(z, p, nrm), -g) for z, g in lats], lam)
+        return (tb + tb2, [a + b @ refl.T for a, b in zip(zb, zb2)], [a - b for a, b in zip(gb, gb2)])
+
+    def _vjp(self, targets, lats, lam):
         t = targets.reshape(-1, 3)
         lm = lam.reshape(-1, 3)
         tb = np.zeros_like(t)
@@ -80,7 +93,7 @@ class OracleDev:
         c = R.compute_surf_c(zeta_b)
         nc = R.compute_surf_nc(zeta_b)
         a = R.compute_aic_solve([c], [nc], [zeta_b], None if zeta_w_static is None else [zeta_w_static],
-                                self.kernel, None, self.r_cut)
+                                self.kernel, self.mirror, self.r_cut)
         return np.linalg.solve(a.T, rhs.ravel()).reshape(rhs.shape)
 
 
@@ -89,7 +102,7 @@ class OracleAdjoint(PrescribedAdjoint):
 
     def __init__(self, ref):
         self.uv = ref
-        self.d = OracleDev(ref.kernel, ref.r_cut)
+        self.d = OracleDev(ref.kernel, ref.r_cut, ref.mirror)
 
     def _static(self):
         return _Snap(self.uv.solve_static(), 0)
