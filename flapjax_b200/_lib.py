@@ -180,6 +180,8 @@ _SIGS = {
     "fj_lu_solve": (C.c_int, [_P, C.c_int, _P, _P, _P, C.c_size_t, _P]),
     "fj_solve_mixed_workspace_size": (C.c_int, [C.c_int, C.POINTER(C.c_size_t)]),
     "fj_solve_mixed": (C.c_int, [_P, C.c_int, _P, _P, C.c_int, _P, _P, C.c_size_t, _P]),
+    "fj_gemm_tf32": (C.c_int, [_P, C.c_int, _P, C.c_int, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                               C.c_float, C.c_int, _P, _P]),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -11,8 +11,11 @@
 // explicit inverse X once per factorisation; every solve is then GEMVs over all SMs:
 // x = X b, r = b - A x in FP64, x += X r.
 #include <climits>
+#include <cstdlib>
+#include <cstring>
 
 #include "fj_lu.cuh"
+#include "fj_tc.cuh"
 
 namespace fj {
 
@@ -107,8 +110,10 @@ __global__ void __launch_bounds__(1024) lu_panel_kernel(T* __restrict__ a, int n
     }
 }
 
+// Row swaps of the panel at column k for every other column; U12 = L11^-1 A12 for the
+// columns [k + nb, c_end).
 template <typename T, int NB>
-__global__ void lu_swap_trsm_kernel(T* __restrict__ a, int n, int k, const int32_t* __restrict__ piv) {
+__global__ void lu_swap_trsm_kernel(T* __restrict__ a, int n, int k, const int32_t* __restrict__ piv, int c_end) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int nb = min(NB, n - k);
     if (c >= n || (c >= k && c < k + nb)) return;
@@ -120,7 +125,7 @@ __global__ void lu_swap_trsm_kernel(T* __restrict__ a, int n, int k, const int32
             a[(int64_t)p * n + c] = t;
         }
     }
-    if (c >= k + nb) {
+    if (c >= k + nb && c < c_end) {
         T u[NB];
 #pragma unroll
         for (int j = 0; j < NB; ++j)
@@ -140,28 +145,29 @@ __global__ void lu_swap_trsm_kernel(T* __restrict__ a, int n, int k, const int32
     }
 }
 
+// A[r0.., c0..] -= L[., k..k+NB) U[k..k+NB, .] on one 64 x 64 tile, rows < r_end and
+// columns < c_end.
 template <typename T, int NB>
-__global__ void __launch_bounds__(256) lu_update_kernel(T* __restrict__ a, int n, int k) {
+__device__ __forceinline__ void lu_update_tile(T* __restrict__ a, int n, int k, int r0, int c0, int r_end,
+                                               int c_end) {
     __shared__ T Ls[64][NB + 1];
     __shared__ T Us[NB][64];
-    const int k2 = k + NB;
-    const int r0 = k2 + blockIdx.y * 64, c0 = k2 + blockIdx.x * 64;
     for (int idx = threadIdx.x; idx < 64 * NB; idx += blockDim.x) {
         const int r = idx / NB, j = idx % NB;
-        Ls[r][j] = (r0 + r < n) ? a[(int64_t)(r0 + r) * n + k + j] : T(0);
+        Ls[r][j] = (r0 + r < r_end) ? a[(int64_t)(r0 + r) * n + k + j] : T(0);
         const int jj = idx / 64, c = idx % 64;
-        Us[jj][c] = (c0 + c < n) ? a[(int64_t)(k + jj) * n + c0 + c] : T(0);
+        Us[jj][c] = (c0 + c < c_end) ? a[(int64_t)(k + jj) * n + c0 + c] : T(0);
     }
     __syncthreads();
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
         const int r = ty + 16 * p;
-        if (r0 + r >= n) continue;
+        if (r0 + r >= r_end) continue;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int c = tx + 16 * q;
-            if (c0 + c >= n) continue;
+            if (c0 + c >= c_end) continue;
             T* dst = a + (int64_t)(r0 + r) * n + c0 + c;
             T acc = *dst;
 #pragma unroll
@@ -169,6 +175,13 @@ __global__ void __launch_bounds__(256) lu_update_kernel(T* __restrict__ a, int n
             *dst = acc;
         }
     }
+}
+
+// A22 -= L21 U12 over rows [k + NB, n) and columns [k + NB, c_end).
+template <typename T, int NB>
+__global__ void __launch_bounds__(256) lu_update_kernel(T* __restrict__ a, int n, int k, int c_end) {
+    const int k2 = k + NB;
+    lu_update_tile<T, NB>(a, n, k, k2 + blockIdx.y * 64, k2 + blockIdx.x * 64, n, c_end);
 }
 
 template <typename T, int NB>
@@ -182,12 +195,12 @@ static int lu_factor_impl(T* a, int n, int32_t* piv, int* d_info, cudaStream_t s
         const int nb = min(NB, n - k);
         lu_panel_kernel<T, NB><<<1, 1024, (size_t)(n - k) * (NB + 1) * sizeof(T), s>>>(a, n, k, piv, d_info); note_launch();
         if (n > nb) {
-            lu_swap_trsm_kernel<T, NB><<<(n + 255) / 256, 256, 0, s>>>(a, n, k, piv); note_launch();
+            lu_swap_trsm_kernel<T, NB><<<(n + 255) / 256, 256, 0, s>>>(a, n, k, piv, n); note_launch();
         }
         const int rem = n - k - nb;
         if (rem > 0) {
             dim3 g((rem + 63) / 64, (rem + 63) / 64);
-            lu_update_kernel<T, NB><<<g, 256, 0, s>>>(a, n, k); note_launch();
+            lu_update_kernel<T, NB><<<g, 256, 0, s>>>(a, n, k, n); note_launch();
         }
     }
     FJ_LAUNCH_CHECK("lu_factor");
@@ -387,6 +400,141 @@ int lu_inverse32(const float* lu, int n, const int32_t* piv, float* x, cudaStrea
     lu_inverse32_kernel<<<(n + kInvCols - 1) / kInvCols, 512, smem, s>>>(lu, n, piv, x); note_launch();
     FJ_LAUNCH_CHECK("lu_inverse32_kernel");
     return FJ_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Tensor-core factorisation and inverse (mixed path, n >= kTcMinN).
+//
+// lu_factor32_tc: the same partial-pivoting LU, blocked twice.  Inside an outer panel of
+// 128 columns the 16-column panels run as above (row swaps over all columns), with their
+// U rows and updates confined to the outer panel.  The columns to its right receive only
+// the row swaps until the outer panel is done; then, with L11^-1 (tri_inverse32_blocks),
+//   U12 = L11^-1 A12        (tensor cores; in place, one 128-row tile)
+//   A22 -= L21 U12          (tensor cores, K = 128)
+// L11^-1 of every outer panel is kept for the inverse.
+//
+// lu_inverse32_tc: X = U^-1 L^-1 P by blocked substitution on the n x n right-hand side
+// P (the getrf row swaps applied to the identity), 128 rows at a time:
+//   forward   Y_i = L_ii^-1 Y_i,  Y_below -= L_below,i Y_i
+//   backward  X_i = U_ii^-1 Y_i,  Y_above -= U_above,i X_i
+// Every product is a tensor-core GEMM; 2 n^3 flop in all.
+constexpr int kTcBlk = 128;
+
+size_t tc_tri_floats(int n) {
+    return (size_t)2 * ((n + kTcBlk - 1) / kTcBlk) * kTcBlk * kTcBlk;
+}
+
+int lu_factor32_tc(float* a, int n, int32_t* piv, int* d_info, int* d_err, float* tri_l, int passes,
+                   cudaStream_t s) {
+    constexpr int NB = 16;
+    if (n <= 0) return fail(FJ_ERR_SHAPE, "lu_factor: n=%d", n);
+    const size_t smem = (size_t)n * (NB + 1) * sizeof(float);
+    if (smem > 220 * 1024) return fail(FJ_ERR_UNSUPPORTED, "lu_factor: n=%d too large for the shared-memory panel", n);
+    FJ_TRY(allow_dynamic_smem((const void*)lu_panel_kernel<float, NB>, smem));
+    FJ_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int), s));
+    for (int k = 0; k < n; k += kTcBlk) {
+        const int kb = min(kTcBlk, n - k), ke = k + kb;
+        for (int j = k; j < ke; j += NB) {
+            const int nb = min(NB, n - j);
+            lu_panel_kernel<float, NB><<<1, 1024, (size_t)(n - j) * (NB + 1) * sizeof(float), s>>>(a, n, j, piv, d_info);
+            note_launch();
+            if (n > nb) {
+                lu_swap_trsm_kernel<float, NB><<<(n + 255) / 256, 256, 0, s>>>(a, n, j, piv, ke);
+                note_launch();
+            }
+            const int rows = n - j - nb, cols = ke - j - nb;
+            if (nb == NB && rows > 0 && cols > 0) {
+                lu_update_kernel<float, NB><<<dim3((cols + 63) / 64, (rows + 63) / 64), 256, 0, s>>>(a, n, j, ke);
+                note_launch();
+            }
+        }
+        const int b = k / kTcBlk;
+        float* linv = tri_l + (size_t)b * kTcBlk * kTcBlk;
+        FJ_TRY(tri_inverse32_blocks(a, n, b, 1, false, tri_l, s));
+        const int rest = n - ke;
+        if (rest > 0) {
+            float* a12 = a + (int64_t)k * n + ke;
+            FJ_TRY(tc_gemm_tf32(linv, kTcBlk, a12, n, a12, n, kb, rest, kb, 1.0f, 0.0f, passes, d_err, s));
+            FJ_TRY(tc_gemm_tf32(a + (int64_t)ke * n + k, n, a12, n, a + (int64_t)ke * n + ke, n, rest, rest, kb,
+                                -1.0f, 1.0f, passes, d_err, s));
+        }
+    }
+    FJ_LAUNCH_CHECK("lu_factor32_tc");
+    return FJ_OK;
+}
+
+// Y = P I: row i holds a one in column perm[i].  Y must be zero on entry.
+__global__ void __launch_bounds__(1024) perm_identity_kernel(const int32_t* __restrict__ piv, int n,
+                                                             float* __restrict__ y) {
+    extern __shared__ int perm_sm[];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) perm_sm[i] = i;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < n; ++i) {
+            const int p = piv[i];
+            if (p != i) {
+                const int t = perm_sm[i];
+                perm_sm[i] = perm_sm[p];
+                perm_sm[p] = t;
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) y[(int64_t)i * n + perm_sm[i]] = 1.0f;
+}
+
+int lu_inverse32_tc(const float* lu, int n, const int32_t* piv, float* x, float* tri, int passes, int* d_err,
+                    cudaStream_t s) {
+    const int nblk = (n + kTcBlk - 1) / kTcBlk;
+    const float* tri_l = tri;  // from the factorisation
+    float* tri_u = tri + (size_t)nblk * kTcBlk * kTcBlk;
+    FJ_TRY(tri_inverse32_blocks(lu, n, 0, nblk, true, tri_u, s));
+    FJ_CUDA(cudaMemsetAsync(x, 0, (size_t)n * n * sizeof(float), s));
+    FJ_TRY(allow_dynamic_smem((const void*)perm_identity_kernel, (size_t)n * sizeof(int)));
+    perm_identity_kernel<<<1, 1024, (size_t)n * sizeof(int), s>>>(piv, n, x);
+    note_launch();
+    FJ_LAUNCH_CHECK("perm_identity_kernel");
+    for (int b = 0; b < nblk; ++b) {  // forward: unit lower
+        const int i0 = b * kTcBlk, ib = min(kTcBlk, n - i0), below = n - i0 - ib;
+        float* yi = x + (int64_t)i0 * n;
+        FJ_TRY(tc_gemm_tf32(tri_l + (size_t)b * kTcBlk * kTcBlk, kTcBlk, yi, n, yi, n, ib, n, ib, 1.0f, 0.0f, passes,
+                            d_err, s));
+        if (below > 0)
+            FJ_TRY(tc_gemm_tf32(lu + (int64_t)(i0 + ib) * n + i0, n, yi, n, yi + (int64_t)ib * n, n, below, n, ib,
+                                -1.0f, 1.0f, passes, d_err, s));
+    }
+    for (int b = nblk - 1; b >= 0; --b) {  // backward: upper
+        const int i0 = b * kTcBlk, ib = min(kTcBlk, n - i0);
+        float* yi = x + (int64_t)i0 * n;
+        FJ_TRY(tc_gemm_tf32(tri_u + (size_t)b * kTcBlk * kTcBlk, kTcBlk, yi, n, yi, n, ib, n, ib, 1.0f, 0.0f, passes,
+                            d_err, s));
+        if (i0 > 0)
+            FJ_TRY(tc_gemm_tf32(lu + i0, n, yi, n, x, n, i0, n, ib, -1.0f, 1.0f, passes, d_err, s));
+    }
+    return FJ_OK;
+}
+
+// Factor path of the mixed solve.  FJ_MIXED_FACTOR selects it: "cuda" (FP32 CUDA cores),
+// "tf32" (tensor cores, one TF32 pass) or the default "tf32x3" (three-pass split); the
+// tensor-core paths apply from n >= kTcMinN.
+constexpr int kTcMinN = 256;
+
+int factor_inverse32(const double* a64, int n, float* a32, int32_t* piv, int* flags, float* x32, float* tri,
+                     cudaStream_t s) {
+    int passes = 3;
+    if (const char* e = getenv("FJ_MIXED_FACTOR")) {
+        if (!strcmp(e, "cuda")) passes = 0;
+        else if (!strcmp(e, "tf32")) passes = 1;
+        else if (strcmp(e, "tf32x3") != 0) return fail(FJ_ERR_SHAPE, "FJ_MIXED_FACTOR=%s (cuda, tf32 or tf32x3)", e);
+    }
+    FJ_TRY(convert64to32(a64, a32, (int64_t)n * n, s));
+    if (passes == 0 || n < kTcMinN) {
+        FJ_TRY(lu_factor32(a32, n, piv, flags, s));
+        return lu_inverse32(a32, n, piv, x32, s);
+    }
+    FJ_CUDA(cudaMemsetAsync(flags + 3, 0, sizeof(int), s));
+    FJ_TRY(lu_factor32_tc(a32, n, piv, flags, flags + 3, tri, passes, s));
+    return lu_inverse32_tc(a32, n, piv, x32, tri, passes, flags + 3, s);
 }
 
 __global__ void convert64to32_kernel(const double* __restrict__ a, float* __restrict__ b, int64_t count) {

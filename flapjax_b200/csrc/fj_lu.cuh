@@ -17,6 +17,14 @@ int lu_solve64(const double* lu, int n, const int32_t* piv, double* b, double* w
 // X <- A^-1 (row-major n x n) from FP32 factors.
 int lu_inverse32(const float* lu, int n, const int32_t* piv, float* x, cudaStream_t s);
 
+// The factorisation behind the mixed solve: a32 <- FP32 LU of a64 (pivots in piv,
+// zero-pivot info in flags[0]) and x32 <- the FP32 inverse.  From n = 256 on the
+// products run on the tensor cores (flags[3] <- 1 if one of their bounded waits expired).
+// tri: tc_tri_floats(n) floats of scratch.
+size_t tc_tri_floats(int n);
+int factor_inverse32(const double* a64, int n, float* a32, int32_t* piv, int* flags, float* x32, float* tri,
+                     cudaStream_t s);
+
 // Round an FP64 matrix to FP32.
 int convert64to32(const double* a, float* b, int64_t count, cudaStream_t s);
 

@@ -712,6 +712,7 @@ struct Plan {
     double* a64;         // FP64 AIC (factored in place on the FP64 path)
     float* a32;          // FP32 LU factors (mixed)
     float* x32;          // FP32 inverse (mixed)
+    float* tri32;        // triangular-block inverses of the tensor-core factorisation (mixed)
     double* zeta_ref;    // lattice of the cached AIC (mixed)
     int32_t* piv;
     double* rhs;
@@ -835,10 +836,12 @@ static int make_plan(const fj_case_config* cfg, void* ws, size_t ws_bytes, Plan&
     if (cfg->precision == FJ_PREC_MIXED) {
         p.a32 = a.carve<float>((int64_t)p.nb * p.nb);
         p.x32 = a.carve<float>((int64_t)p.nb * p.nb);
+        p.tri32 = a.carve<float>(tc_tri_floats(p.nb));
         p.zeta_ref = a.carve<double>(p.sz_zb);
     } else {
         p.a32 = nullptr;
         p.x32 = nullptr;
+        p.tri32 = nullptr;
         p.zeta_ref = nullptr;
     }
     p.piv = a.carve<int32_t>(p.nb);
@@ -1387,9 +1390,7 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
         for (int k = 0; k < K; ++k) {
             if (!items[k].refactor) continue;
             const Plan& p = items[k].p;
-            FJ_TRY(convert64to32(p.a64, p.a32, (int64_t)p.nb * p.nb, s));
-            FJ_TRY(lu_factor32(p.a32, p.nb, p.piv, p.flags, s));
-            FJ_TRY(lu_inverse32(p.a32, p.nb, p.piv, p.x32, s));
+            FJ_TRY(factor_inverse32(p.a64, p.nb, p.a32, p.piv, p.flags, p.x32, p.tri32, s));
             k_keep_lattice<<<nblk(p.sz_zb), 256, 0, s>>>(dC + k, p.zeta_ref, p.sz_zb); note_launch();
         }
         FJ_TRY(refine_jobs((const RefineJob*)(d_tab + tl.refine), (int)ref.size(), max_n, 3, s));
@@ -1441,17 +1442,20 @@ static int check_buffers(const Plan& p, const fj_case_buffers* B, bool dynamic) 
 }
 
 // Status words of a case-level call: flags[0] the LU info of the last factorisation
-// (first zero pivot + 1), flags[2] the lowest slot with a non-finite total force.
+// (first zero pivot + 1), flags[2] the lowest slot with a non-finite total force,
+// flags[3] set when a bounded wait of the tensor-core factorisation expired.
 static constexpr int kNoSlot = 0x7f7f7f7f;  // the byte pattern 0x7f repeated
 
 static int clear_status(const Plan& p, cudaStream_t s) {
+    FJ_CUDA(cudaMemsetAsync(p.flags + 3, 0, sizeof(int), s));
     return cuda_status(cudaMemsetAsync(p.flags + 2, 0x7f, sizeof(int), s), "status reset");
 }
 
 static int read_status(const Plan& p, cudaStream_t s) {
-    int w[3] = {0, 0, 0};
+    int w[4] = {0, 0, 0, 0};
     FJ_CUDA(cudaMemcpyAsync(w, p.flags, sizeof(w), cudaMemcpyDeviceToHost, s));
     FJ_CUDA(cudaStreamSynchronize(s));
+    if (w[3] != 0) return fail(FJ_ERR_TIMEOUT, "a tensor-core wait of the AIC factorisation expired");
     if (w[2] != kNoSlot) return fail(FJ_ERR_NONFINITE, "non-finite forces at time slot %d", w[2]);
     if (w[0] != 0) return fail(FJ_ERR_SINGULAR, "zero pivot in column %d of the AIC factorisation", w[0] - 1);
     return FJ_OK;
@@ -1847,6 +1851,7 @@ int fj_solve_mixed_workspace_size(int n, size_t* bytes) {
     a.carve<int32_t>(n);
     a.carve<double>(n);
     a.carve<int>(4);
+    a.carve<float>(tc_tri_floats(n));
     *bytes = a.used + 256;
     return FJ_OK;
 }
@@ -1863,10 +1868,9 @@ int fj_solve_mixed(const double* d_a, int n, const double* d_b, double* d_x, int
     int32_t* piv = a.carve<int32_t>(n);
     double* r = a.carve<double>(n);
     int* info = a.carve<int>(4);
+    float* tri = a.carve<float>(tc_tri_floats(n));
     if (refactor) {
-        FJ_TRY(convert64to32(d_a, a32, (int64_t)n * n, s));
-        FJ_TRY(lu_factor32(a32, n, piv, info, s));
-        FJ_TRY(lu_inverse32(a32, n, piv, x32, s));
+        FJ_TRY(factor_inverse32(d_a, n, a32, piv, info, x32, tri, s));
     }
     return refine_solve(d_a, x32, n, d_b, d_x, r, d_resid, 3, s);
 }

@@ -354,13 +354,26 @@ FJ_API int fj_wake_vjp(const double* d_zeta_w_bar_n, const double* d_gamma_w_bar
                        double* d_zeta_te_bar, double* d_gamma_te_bar, double* d_zeta_w_bar_nm1,
                        double* d_gamma_w_bar_nm1, fj_stream_t stream);
 
-/* Mixed-precision solve of A x = b: FP32 factors of A (recomputed when refactor != 0)
- * kept in the workspace, then FP64 iterative refinement x += M (b - A x) with the FP64
- * residual.  Writes the final relative residual ||b-Ax||_inf / ||b||_inf to
- * *d_resid (device, 1 double). */
+/* Mixed-precision solve of A x = b (jnp.linalg.solve, aero/uvlm.py:985): FP32 factors
+ * of A and the FP32 inverse M (recomputed when refactor != 0) kept in the workspace, then
+ * FP64 iterative refinement x += M (b - A x) with the FP64 residual.  Writes the final
+ * relative residual ||b-Ax||_inf / ||b||_inf to *d_resid (device, 1 double).  From
+ * n = 256 the factorisation's and the inverse's products run on the tensor cores
+ * (fj_gemm_tf32, three-pass split); the environment variable FJ_MIXED_FACTOR = "cuda" |
+ * "tf32" | "tf32x3" selects the FP32 CUDA-core path, a single TF32 pass or the default. */
 FJ_API int fj_solve_mixed_workspace_size(int n, size_t* bytes);
 FJ_API int fj_solve_mixed(const double* d_a, int n, const double* d_b, double* d_x, int refactor,
                    double* d_resid, void* d_ws, size_t ws_bytes, fj_stream_t stream);
+
+/* C <- alpha A B + beta C on the tensor cores (tcgen05, TF32 operands, FP32 accumulation
+ * in tensor memory): A (m x k, lda), B (k x n, ldb), C (m x n, ldc), row-major FP32
+ * device arrays.  passes = 1 multiplies the TF32-rounded operands; passes = 3 adds the
+ * products with the operands' rounding remainders (hi*hi + hi*lo + lo*hi), close to
+ * FP32 accuracy.  beta = 0 does not read C.  *d_err (device int) is set to 1 if a bounded
+ * device wait expired.  The product building block of the mixed factorisation (the
+ * reference's solve runs inside jnp.linalg.solve, aero/uvlm.py:985). */
+FJ_API int fj_gemm_tf32(const float* d_a, int lda, const float* d_b, int ldb, float* d_c, int ldc, int m, int n,
+                        int k, float alpha, float beta, int passes, int* d_err, fj_stream_t stream);
 
 #ifdef __cplusplus
 }

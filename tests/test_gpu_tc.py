@@ -1,0 +1,164 @@
+"""Tensor-core products (fj_gemm_tf32) and the tensor-core factorisation behind the mixed
+solve (jnp.linalg.solve, aero/uvlm.py:985).
+
+The GEMM is checked elementwise against the FP64 product, with error bounds scaled by
+|A| |B|: three-pass split within 1e-5 (FP32-class), one TF32 pass within 3e-3.  The mixed
+solve must reach the same refined answer whichever factor path made its inverse.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from tests.helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _f32(a, dev):
+    import torch
+
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32)).to(dev)
+
+
+def _gemm(cuda, a, b, c, m, n, k, alpha, beta, passes):
+    """C <- alpha A B + beta C on the device; a, b, c are 2-D float32 host arrays whose
+    leading (m x k), (k x n), (m x n) blocks are the operands (row strides = their widths)."""
+    import torch
+
+    from flapjax_b200 import _lib
+
+    ta, tb, tc = _f32(a, cuda), _f32(b, cuda), _f32(c, cuda)
+    err = torch.zeros(1, dtype=torch.int32, device=cuda)
+    s = torch.cuda.current_stream(cuda).cuda_stream
+    _lib.call("fj_gemm_tf32", ta.data_ptr(), a.shape[1], tb.data_ptr(), b.shape[1], tc.data_ptr(), c.shape[1], m, n,
+              k, C.c_float(alpha), C.c_float(beta), passes, err.data_ptr(), s)
+    out = tc.cpu().numpy()
+    assert int(err.cpu()) == 0
+    return out
+
+
+@pytest.mark.parametrize("m,n,k,lda,ldb,ldc", [(128, 128, 32, 32, 128, 128), (200, 300, 100, 103, 301, 305),
+                                               (5, 7, 3, 3, 7, 7), (384, 256, 128, 131, 257, 256)])
+@pytest.mark.parametrize("passes", [1, 3])
+def test_gemm_matches_fp64_product(cuda, m, n, k, lda, ldb, ldc, passes):
+    rng = np.random.default_rng(m + n + k + passes)
+    a = rng.normal(size=(m, lda)).astype(np.float32)
+    b = rng.normal(size=(k, ldb)).astype(np.float32)
+    c = rng.normal(size=(m, ldc)).astype(np.float32)
+    alpha, beta = -1.0, 1.0
+    got = _gemm(cuda, a, b, c, m, n, k, alpha, beta, passes)
+    A, B = a[:, :k].astype(np.float64), b[:, :n].astype(np.float64)
+    want = alpha * A @ B + beta * c[:, :n].astype(np.float64)
+    scale = np.abs(A) @ np.abs(B) + np.abs(c[:, :n])
+    tol = 1e-5 if passes == 3 else 3e-3
+    assert np.all(np.abs(got[:, :n] - want) <= tol * scale)
+    # columns past n and the padding of every row stay untouched
+    assert np.array_equal(got[:, n:], c[:, n:])
+
+
+def test_gemm_split_beats_single_pass_and_beta_zero_ignores_c(cuda):
+    rng = np.random.default_rng(9)
+    m, n, k = 256, 256, 128
+    a = rng.normal(size=(m, k)).astype(np.float32)
+    b = rng.normal(size=(k, n)).astype(np.float32)
+    c = np.full((m, n), np.nan, np.float32)  # beta = 0 must not read C
+    want = a.astype(np.float64) @ b.astype(np.float64)
+    e1 = rel_err(_gemm(cuda, a, b, c, m, n, k, 1.0, 0.0, 1), want)
+    e3 = rel_err(_gemm(cuda, a, b, c, m, n, k, 1.0, 0.0, 3), want)
+    assert e3 < 5e-6 and 100 * e3 < e1 < 1e-2
+
+
+def test_gemm_in_place_on_b(cuda):
+    """U12 = L11^-1 A12 runs in place (C is B's memory, m <= 128)."""
+    import torch
+
+    from flapjax_b200 import _lib
+
+    rng = np.random.default_rng(3)
+    m = k = 128
+    n = 500
+    a = rng.normal(size=(m, k)).astype(np.float32)
+    b = rng.normal(size=(k, n)).astype(np.float32)
+    ta, tb = _f32(a, cuda), _f32(b, cuda)
+    err = torch.zeros(1, dtype=torch.int32, device=cuda)
+    s = torch.cuda.current_stream(cuda).cuda_stream
+    _lib.call("fj_gemm_tf32", ta.data_ptr(), k, tb.data_ptr(), n, tb.data_ptr(), n, m, n, k, C.c_float(1.0),
+              C.c_float(0.0), 3, err.data_ptr(), s)
+    want = a.astype(np.float64) @ b.astype(np.float64)
+    assert rel_err(tb.cpu().numpy(), want) < 5e-6
+
+
+def _solve_mixed(cuda, a, b):
+    import torch
+
+    from flapjax_b200 import _lib
+
+    n = a.shape[0]
+    nbytes = C.c_size_t()
+    _lib.call("fj_solve_mixed_workspace_size", n, C.byref(nbytes))
+    ws = torch.empty(nbytes.value, dtype=torch.uint8, device=cuda)
+    ta = torch.as_tensor(a).to(cuda)
+    tb = torch.as_tensor(b).to(cuda)
+    tx = torch.empty(n, dtype=torch.float64, device=cuda)
+    res = torch.empty(1, dtype=torch.float64, device=cuda)
+    s = torch.cuda.current_stream(cuda).cuda_stream
+    _lib.call("fj_solve_mixed", ta.data_ptr(), n, tb.data_ptr(), tx.data_ptr(), 1, res.data_ptr(), ws.data_ptr(),
+              ws.numel(), s)
+    return tx.cpu().numpy(), float(res.cpu())
+
+
+@pytest.mark.parametrize("n", [256, 300, 777, 1500])
+def test_mixed_solve_through_tensor_core_factors(cuda, n, monkeypatch):
+    rng = np.random.default_rng(n)
+    a = rng.normal(size=(n, n)) + n * 0.05 * np.eye(n)
+    b = rng.normal(size=n)
+    want = np.linalg.solve(a, b)
+    monkeypatch.setenv("FJ_MIXED_FACTOR", "tf32x3")
+    x3, r3 = _solve_mixed(cuda, a, b)
+    assert r3 < 1e-12 and rel_err(x3, want) < 1e-11
+    monkeypatch.setenv("FJ_MIXED_FACTOR", "cuda")
+    xc, rc = _solve_mixed(cuda, a, b)
+    assert rc < 1e-12 and rel_err(xc, want) < 1e-11
+    # one TF32 pass: a coarser inverse, so three refinement sweeps leave more behind
+    monkeypatch.setenv("FJ_MIXED_FACTOR", "tf32")
+    x1, r1 = _solve_mixed(cuda, a, b)
+    assert r1 < 1e-2
+
+
+@pytest.mark.parametrize("n", [300, 520])
+def test_mixed_solve_heavy_pivoting(cuda, n, monkeypatch):
+    """No diagonal dominance: pivot rows come from far below the outer panel, so the row
+    swaps must reach the columns to its right before their updates.  Such a matrix
+    (condition number ~1e3) converges more slowly in three refinement sweeps; the
+    tensor-core inverse must do as well as the FP32 CUDA-core one."""
+    rng = np.random.default_rng(100 + n)
+    a = rng.normal(size=(n, n))
+    b = rng.normal(size=n)
+    want = np.linalg.solve(a, b)
+    monkeypatch.setenv("FJ_MIXED_FACTOR", "cuda")
+    xc, rc = _solve_mixed(cuda, a, b)
+    monkeypatch.setenv("FJ_MIXED_FACTOR", "tf32x3")
+    x, r = _solve_mixed(cuda, a, b)
+    assert r < max(1e-12, 10 * rc) and rel_err(x, want) < max(1e-11, 10 * rel_err(xc, want))
+
+
+def test_mixed_solve_of_an_aic(cuda):
+    """The static AIC of a 16 x 32 wing with a 20-row wake (n = 512): tensor-core factors
+    through the refinement to the FP64 solution."""
+    from oracle import uvlm_ref as R
+
+    m, n = 16, 32
+    z = np.zeros((m + 1, n + 1, 3))
+    z[..., 0] = np.linspace(-0.25, 0.75, m + 1)[:, None]
+    z[..., 1] = np.linspace(0.0, 8.0, n + 1)[None, :]
+    z[..., 2] = 0.05 * z[..., 0] ** 2  # a little camber
+    zw = z[-1][None] + np.arange(21)[:, None, None] * np.array([0.125, 0.0, 0.0])  # a straight static wake
+    cs, ns = [R.compute_surf_c(z)], [R.compute_surf_nc(z)]
+    a = R.compute_aic_solve(cs, ns, [z], [zw], R.KERNEL_EPSILON, None)
+    b = np.random.default_rng(0).normal(size=a.shape[0])
+    want = np.linalg.solve(a, b)
+    x, r = _solve_mixed(cuda, a, b)
+    assert r < 1e-12 and rel_err(x, want) < 1e-10
