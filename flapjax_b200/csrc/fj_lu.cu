@@ -32,15 +32,21 @@ __global__ void __launch_bounds__(1024) lu_panel_kernel(T* __restrict__ a, int n
     constexpr int LDP = NB + 1;
     __shared__ T s_val[32];
     __shared__ int s_idx[32];
-    __shared__ int s_piv;
     const int rows = n - k;
     const int nb = min(NB, rows);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nwarps = (blockDim.x + 31) >> 5;
+    // asynchronous copies of the panel: every element in flight at once (columns past nb
+    // zero-filled)
     for (int idx = threadIdx.x; idx < rows * NB; idx += blockDim.x) {
         const int r = idx / NB, c = idx % NB;
-        P[r * LDP + c] = c < nb ? a[(int64_t)(k + r) * n + k + c] : T(0);
+        const T* src = a + (int64_t)(k + r) * n + k + min(c, nb - 1);
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(P + r * LDP + c);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(src), "n"(sizeof(T)),
+                     "r"(c < nb ? (int)sizeof(T) : 0)
+                     : "memory");
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
     for (int j = 0; j < nb; ++j) {
         T best = T(-1);
@@ -66,26 +72,20 @@ __global__ void __launch_bounds__(1024) lu_panel_kernel(T* __restrict__ a, int n
             s_idx[warp] = bi;
         }
         __syncthreads();
-        if (warp == 0) {
-            best = lane < nwarps ? s_val[lane] : T(-1);
-            bi = lane < nwarps ? s_idx[lane] : INT_MAX;
+        // every warp reduces the partials itself: no second barrier
+        best = lane < nwarps ? s_val[lane] : T(-1);
+        bi = lane < nwarps ? s_idx[lane] : INT_MAX;
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const T ov = __shfl_down_sync(0xffffffffu, best, off);
-                const int oi = __shfl_down_sync(0xffffffffu, bi, off);
-                if (ov > best || (ov == best && oi < bi)) {
-                    best = ov;
-                    bi = oi;
-                }
-            }
-            if (lane == 0) {
-                const int p = (bi == INT_MAX) ? j : bi;  // all-NaN column: keep the diagonal
-                s_piv = p;
-                piv[k + j] = k + p;
+        for (int off = 16; off > 0; off >>= 1) {
+            const T ov = __shfl_xor_sync(0xffffffffu, best, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+            if (ov > best || (ov == best && oi < bi)) {
+                best = ov;
+                bi = oi;
             }
         }
-        __syncthreads();
-        const int p = s_piv;
+        const int p = (bi == INT_MAX) ? j : bi;  // all-NaN column: keep the diagonal
+        if (threadIdx.x == 0) piv[k + j] = k + p;
         if (p != j && threadIdx.x < NB) {
             const T t = P[j * LDP + threadIdx.x];
             P[j * LDP + threadIdx.x] = P[p * LDP + threadIdx.x];
@@ -104,6 +104,7 @@ __global__ void __launch_bounds__(1024) lu_panel_kernel(T* __restrict__ a, int n
         }
         __syncthreads();
     }
+#pragma unroll 8
     for (int idx = threadIdx.x; idx < rows * NB; idx += blockDim.x) {
         const int r = idx / NB, c = idx % NB;
         if (c < nb) a[(int64_t)(k + r) * n + k + c] = P[r * LDP + c];
@@ -111,20 +112,59 @@ __global__ void __launch_bounds__(1024) lu_panel_kernel(T* __restrict__ a, int n
 }
 
 // Row swaps of the panel at column k for every other column; U12 = L11^-1 A12 for the
-// columns [k + nb, c_end).
+// columns [k + nb, c_end).  The panel's swaps (applied in order, as getrf) compose to one
+// permutation of the at most 2 NB rows they touch; thread 0 works it out in shared memory,
+// then each column thread loads all the touched values before storing any, one memory
+// round trip instead of one per swap.
 template <typename T, int NB>
 __global__ void lu_swap_trsm_kernel(T* __restrict__ a, int n, int k, const int32_t* __restrict__ piv, int c_end) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ int s_dst[2 * NB], s_src[2 * NB], s_piv[NB];
+    __shared__ int s_cnt;
+    __shared__ T s_l[NB][NB];  // the panel's unit-lower diagonal block, for the triangular solve
     const int nb = min(NB, n - k);
-    if (c >= n || (c >= k && c < k + nb)) return;
-    for (int j = 0; j < nb; ++j) {
-        const int p = piv[k + j];
-        if (p != k + j) {
-            const T t = a[(int64_t)(k + j) * n + c];
-            a[(int64_t)(k + j) * n + c] = a[(int64_t)p * n + c];
-            a[(int64_t)p * n + c] = t;
-        }
+    if (threadIdx.x < nb) s_piv[threadIdx.x] = piv[k + threadIdx.x];
+    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
+        const int r = idx / NB, c = idx % NB;
+        s_l[r][c] = (r < nb && c < r) ? a[(int64_t)(k + r) * n + k + c] : T(0);
     }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int cnt = 0;
+        for (int jj = 0; jj < nb; ++jj) {
+            const int r1 = k + jj, r2 = s_piv[jj];
+            if (r1 == r2) continue;
+            int i1 = -1, i2 = -1;
+            for (int e = 0; e < cnt; ++e) {
+                if (s_dst[e] == r1) i1 = e;
+                if (s_dst[e] == r2) i2 = e;
+            }
+            if (i1 < 0) {
+                i1 = cnt++;
+                s_dst[i1] = r1;
+                s_src[i1] = r1;
+            }
+            if (i2 < 0) {
+                i2 = cnt++;
+                s_dst[i2] = r2;
+                s_src[i2] = r2;
+            }
+            const int tmp = s_src[i1];
+            s_src[i1] = s_src[i2];
+            s_src[i2] = tmp;
+        }
+        s_cnt = cnt;
+    }
+    __syncthreads();
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n || (c >= k && c < k + nb)) return;
+    const int cnt = s_cnt;
+    T val[2 * NB];
+#pragma unroll
+    for (int e = 0; e < 2 * NB; ++e)
+        if (e < cnt) val[e] = a[(int64_t)s_src[e] * n + c];
+#pragma unroll
+    for (int e = 0; e < 2 * NB; ++e)
+        if (e < cnt) a[(int64_t)s_dst[e] * n + c] = val[e];
     if (c >= k + nb && c < c_end) {
         T u[NB];
 #pragma unroll
@@ -135,7 +175,7 @@ __global__ void lu_swap_trsm_kernel(T* __restrict__ a, int n, int k, const int32
             if (j < nb) {
                 T s = u[j];
 #pragma unroll
-                for (int jj = 0; jj < j; ++jj) s -= a[(int64_t)(k + j) * n + k + jj] * u[jj];
+                for (int jj = 0; jj < j; ++jj) s -= s_l[j][jj] * u[jj];
                 u[j] = s;
             }
         }
@@ -158,23 +198,33 @@ __device__ __forceinline__ void lu_update_tile(T* __restrict__ a, int n, int k, 
         const int jj = idx / 64, c = idx % 64;
         Us[jj][c] = (c0 + c < c_end) ? a[(int64_t)(k + jj) * n + c0 + c] : T(0);
     }
-    __syncthreads();
+    // the 16 elements of this thread are loaded before any is computed: one memory round
+    // trip per tile
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    T acc[4][4];
 #pragma unroll
-    for (int p = 0; p < 4; ++p) {
-        const int r = ty + 16 * p;
-        if (r0 + r >= r_end) continue;
+    for (int p = 0; p < 4; ++p)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const int c = tx + 16 * q;
-            if (c0 + c >= c_end) continue;
-            T* dst = a + (int64_t)(r0 + r) * n + c0 + c;
-            T acc = *dst;
-#pragma unroll
-            for (int j = 0; j < NB; ++j) acc -= Ls[r][j] * Us[j][c];
-            *dst = acc;
+            const int r = ty + 16 * p, c = tx + 16 * q;
+            acc[p][q] = (r0 + r < r_end && c0 + c < c_end) ? a[(int64_t)(r0 + r) * n + c0 + c] : T(0);
         }
-    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = ty + 16 * p, c = tx + 16 * q;
+#pragma unroll
+            for (int j = 0; j < NB; ++j) acc[p][q] -= Ls[r][j] * Us[j][c];
+        }
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = ty + 16 * p, c = tx + 16 * q;
+            if (r0 + r < r_end && c0 + c < c_end) a[(int64_t)(r0 + r) * n + c0 + c] = acc[p][q];
+        }
 }
 
 // A22 -= L21 U12 over rows [k + NB, n) and columns [k + NB, c_end).
@@ -223,12 +273,16 @@ constexpr int kTrsvBlk = 128;
 // x[i] = b[perm[i]], perm from the getrf row swaps applied in order to the identity.
 __global__ void __launch_bounds__(1024) permute_kernel(const int32_t* __restrict__ piv, int n,
                                                        const double* __restrict__ b, double* __restrict__ x) {
-    extern __shared__ int perm[];
-    for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = i;
+    extern __shared__ int perm[];  // n permutation entries, then n pivots
+    int* sp = perm + n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        perm[i] = i;
+        sp[i] = piv[i];
+    }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0) {  // the swaps compose in order; from shared memory only
         for (int i = 0; i < n; ++i) {
-            const int p = piv[i];
+            const int p = sp[i];
             if (p != i) {
                 const int t = perm[i];
                 perm[i] = perm[p];
@@ -290,9 +344,9 @@ int lu_solve64(const double* lu, int n, const int32_t* piv, double* b, double* w
     if (n <= 0) return fail(FJ_ERR_SHAPE, "lu_solve: n=%d", n);
     if ((size_t)n * sizeof(int) > 220 * 1024) return fail(FJ_ERR_UNSUPPORTED, "lu_solve: n=%d too large", n);
     const size_t dsm = (size_t)kTrsvBlk * (kTrsvBlk + 1) * sizeof(double);
-    FJ_TRY(allow_dynamic_smem((const void*)permute_kernel, (size_t)(n * sizeof(int))));
+    FJ_TRY(allow_dynamic_smem((const void*)permute_kernel, (size_t)(2 * n * sizeof(int))));
     FJ_TRY(allow_dynamic_smem((const void*)trsv_diag_kernel, (size_t)dsm));
-    permute_kernel<<<1, 1024, n * sizeof(int), s>>>(piv, n, b, work); note_launch();
+    permute_kernel<<<1, 1024, 2 * n * sizeof(int), s>>>(piv, n, b, work); note_launch();
     const int wpb = 8;
     for (int i0 = 0; i0 < n; i0 += kTrsvBlk) {  // forward, unit lower
         const int bw = min(kTrsvBlk, n - i0);
@@ -466,12 +520,16 @@ int lu_factor32_tc(float* a, int n, int32_t* piv, int* d_info, int* d_err, float
 // Y = P I: row i holds a one in column perm[i].  Y must be zero on entry.
 __global__ void __launch_bounds__(1024) perm_identity_kernel(const int32_t* __restrict__ piv, int n,
                                                              float* __restrict__ y) {
-    extern __shared__ int perm_sm[];
-    for (int i = threadIdx.x; i < n; i += blockDim.x) perm_sm[i] = i;
+    extern __shared__ int perm_sm[];  // n permutation entries, then n pivots
+    int* sp = perm_sm + n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        perm_sm[i] = i;
+        sp[i] = piv[i];
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int i = 0; i < n; ++i) {
-            const int p = piv[i];
+            const int p = sp[i];
             if (p != i) {
                 const int t = perm_sm[i];
                 perm_sm[i] = perm_sm[p];
@@ -490,8 +548,8 @@ int lu_inverse32_tc(const float* lu, int n, const int32_t* piv, float* x, float*
     float* tri_u = tri + (size_t)nblk * kTcBlk * kTcBlk;
     FJ_TRY(tri_inverse32_blocks(lu, n, 0, nblk, true, tri_u, s));
     FJ_CUDA(cudaMemsetAsync(x, 0, (size_t)n * n * sizeof(float), s));
-    FJ_TRY(allow_dynamic_smem((const void*)perm_identity_kernel, (size_t)n * sizeof(int)));
-    perm_identity_kernel<<<1, 1024, (size_t)n * sizeof(int), s>>>(piv, n, x);
+    FJ_TRY(allow_dynamic_smem((const void*)perm_identity_kernel, (size_t)2 * n * sizeof(int)));
+    perm_identity_kernel<<<1, 1024, (size_t)2 * n * sizeof(int), s>>>(piv, n, x);
     note_launch();
     FJ_LAUNCH_CHECK("perm_identity_kernel");
     for (int b = 0; b < nblk; ++b) {  // forward: unit lower

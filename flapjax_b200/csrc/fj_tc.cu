@@ -218,6 +218,21 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         issued = ks + 1;
     }
+    // this thread's C values for the epilogue, loaded while the last MMAs run: rows
+    // m0 + 32 (w%4) + r, column n0 + 64 (w/4) + 32 cc + lane
+    const int q = warp & 3, h = warp >> 2;
+    float cpre[2][32];
+    if (beta != 0.0f) {
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+            const int col = n0 + 64 * h + 32 * cc + lane;
+#pragma unroll
+            for (int r = 0; r < 32; ++r) {
+                const int row = m0 + 32 * q + r;
+                cpre[cc][r] = (row < m && col < n) ? c[(int64_t)row * ldc + col] : 0.0f;
+            }
+        }
+    }
     if (issued > 0) {  // all MMAs done: the last commit covers every earlier one
         const int last = issued - 1;
         const bool w = bar_wait(&bars[last & 1], (uint32_t)((last >> 1) & 1));
@@ -229,9 +244,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         // warp w reads TMEM lanes 32*(w%4).. (tile rows) and columns 64*(w/4)..+63; each
         // 32 x 32 block goes through the warp's own padded shared-memory square (the
         // operand buffers are idle now) so that C is read and written row by row, coalesced
-        const int q = warp & 3, h = warp >> 2;
         float* sq = reinterpret_cast<float*>(smem) + warp * (32 * 33);
-#pragma unroll 1
+#pragma unroll
         for (int cc = 0; cc < 2; ++cc) {
             const int col0 = 64 * h + 32 * cc;
             uint32_t v[32];
@@ -250,13 +264,12 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int j = 0; j < 32; ++j) sq[lane * 33 + j] = __uint_as_float(v[j]);  // row lane, column j
             __syncwarp();
             const int col = n0 + col0 + lane;
-#pragma unroll 4
+#pragma unroll
             for (int r = 0; r < 32; ++r) {
                 const int row = m0 + 32 * q + r;
                 if (row < m && col < n) {
-                    float* dst = c + (int64_t)row * ldc + col;
                     const float acc = alpha * sq[r * 33 + lane];
-                    *dst = beta != 0.0f ? acc + beta * *dst : acc;
+                    c[(int64_t)row * ldc + col] = beta != 0.0f ? acc + beta * cpre[cc][r] : acc;
                 }
             }
             __syncwarp();
@@ -293,6 +306,7 @@ __global__ void __launch_bounds__(512) tri_inv_kernel(const float* __restrict__ 
     const int b = b0 + blockIdx.x;
     const int i0 = b * 128, ib = min(128, n - i0);
     float* out = out_all + (size_t)b * 128 * 128;
+#pragma unroll 16
     for (int idx = threadIdx.x; idx < 128 * 128; idx += blockDim.x) {
         const int r = idx >> 7, c = idx & 127;
         float v = (r == c) ? 1.0f : 0.0f;
