@@ -14,6 +14,10 @@ e2e     the same metric through the C ABI with host buffers: every step copies i
         step's solution slot back to pinned host memory.
 fp64_gpu  the plain FP64 path on the same steps, and the mixed path's CL/CD error
         against it.
+factorisation  the mixed solve's FP32 LU + FP32 inverse of this workload's AIC through the
+        tensor-core path (tcgen05 TF32, three-pass split; the default) and through the FP32
+        CUDA-core path, and the tensor-core GEMM alone at the LU's trailing-update shape
+        (--factor runs only this leg).
 
 --impl reference  times the FP64 oracle (the reference's arithmetic restated; the
         reference itself is JAX, which is not installed) with its pair sums in C++/OpenMP on
@@ -56,6 +60,8 @@ def parse():
     ap.add_argument("--adjoint", action="store_true",
                     help="config 3: twist gradient of time-mean CL and CD by the hand-written adjoint")
     ap.add_argument("--adjoint-steps", type=int, default=1000)
+    ap.add_argument("--factor", action="store_true",
+                    help="only the factorisation leg (mixed solve's FP32 LU + inverse, tensor cores vs CUDA cores)")
     ap.add_argument("--configs", action="store_true",
                     help="the per-config table instead of the headline line: C1 heave 8x32/W64/50 steps, "
                          "C2 free wake 16x128/W200, C3 pitch 12x64/W100 primal")
@@ -316,6 +322,12 @@ def main():
         if rank == 0:
             print(json.dumps({"adjoint": adjoint_bench(args, torch)}))
         return 0
+    if args.factor:
+        case = workload(args, 2)
+        _, dcf = make_case(case, "mixed", 2)
+        if rank == 0:
+            print(json.dumps({"factorisation": factor_bench(dcf, case, torch)}))
+        return 0
     if args.only_serving:
         serving = serving_bench(args, torch)
         if world > 1:
@@ -398,6 +410,7 @@ def main():
                 "cd_rel_err_traj_max": float(np.max(np.abs(cdm - cd64)) / np.max(np.abs(cd64))),
                 "fp64_cl_change_from_1e-13_input_perturbation": float(np.max(np.abs(clp - cl64) / np.abs(cl64)))}
         del d64, dpp
+    factor = factor_bench(dc, case, torch) if not args.small else None
     del dc
 
     # -- e2e through the C ABI with host buffers -------------------------------------------
@@ -429,11 +442,98 @@ def main():
                    "precision": "mixed (FP32 Biot-Savart, FP32 factors + FP64 refinement)",
                    "l2": "flushed between steps (256 MB write outside the timed events)",
                    "parallelism": f"independent case replica per GPU x{world}", "seed": case.seed},
-        "e2e": e2e, "fp64_gpu": fp64, "roofline": roof, "cpu_baseline": cpu,
+        "e2e": e2e, "fp64_gpu": fp64, "roofline": roof, "cpu_baseline": cpu, "factorisation": factor,
         "gpu_launches": int(launches), "clocks": clk.summary(), "serving": serving,
     }
     print(json.dumps(line))
     return 0
+
+
+def factor_bench(dc, case, torch):
+    """The factorisation behind the mixed solve on this workload's own AIC (the bound
+    lattice at slot 0, fj_aic_assemble): FP32 LU + FP32 inverse through each path
+    (FJ_MIXED_FACTOR), device-timed per call with CUDA events, then the FP64-refined
+    residual.  Beside it, the tensor-core GEMM alone at the LU's trailing-update shape
+    (m = n = N - 128, k = 128, three passes) against the dense TF32 rate, taken as half the
+    measured cuBLAS bf16 peak."""
+    import ctypes as C
+
+    from flapjax_b200 import _lib
+
+    s = torch.cuda.current_stream().cuda_stream
+    dev = torch.device("cuda", torch.cuda.current_device())
+    m, n = case.m, case.n
+    z = dc.arrays["zeta_b"][0].clone()
+    nb = m * n
+    zp = (C.c_void_p * 1)(z.data_ptr())
+    mm, nn, ms = (C.c_int * 1)(m), (C.c_int * 1)(n), (C.c_int * 1)(0)
+    nbytes = C.c_size_t()
+    _lib.call("fj_aic_workspace_size", mm, nn, 1, C.byref(nbytes))
+    ws = torch.empty(nbytes.value, dtype=torch.uint8, device=dev)
+    a = torch.empty((nb, nb), dtype=torch.float64, device=dev)
+    kern = _lib.FJ_KERNEL_CUTOFF if case.kernel == "cutoff" else _lib.FJ_KERNEL_EPSILON
+    _lib.call("fj_aic_assemble", zp, mm, nn, 1, None, ms, None, None, kern, case.r_cut, a.data_ptr(), ws.data_ptr(),
+              ws.numel(), s)
+    b = torch.randn(nb, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(0))
+    _lib.call("fj_solve_mixed_workspace_size", nb, C.byref(nbytes))
+    wsm = torch.empty(nbytes.value, dtype=torch.uint8, device=dev)
+    x = torch.empty(nb, dtype=torch.float64, device=dev)
+    res = torch.empty(1, dtype=torch.float64, device=dev)
+    out = {"n": nb, "matrix": "AIC of the workload's bound lattice (slot 0)"}
+    old = os.environ.get("FJ_MIXED_FACTOR")
+    try:
+        for mode in ("tf32x3", "tf32", "cuda"):
+            os.environ["FJ_MIXED_FACTOR"] = mode
+            times = []
+            for it in range(6):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                _lib.call("fj_solve_mixed", a.data_ptr(), nb, b.data_ptr(), x.data_ptr(), 1, res.data_ptr(),
+                          wsm.data_ptr(), wsm.numel(), s)
+                e1.record()
+                torch.cuda.synchronize()
+                if it >= 2:
+                    times.append(e0.elapsed_time(e1))
+            out[mode] = {"factor_inverse_solve_ms": float(np.median(times)), "refined_rel_residual": float(res.item())}
+    finally:
+        if old is None:
+            os.environ.pop("FJ_MIXED_FACTOR", None)
+        else:
+            os.environ["FJ_MIXED_FACTOR"] = old
+    out["tensor_core_speedup_over_cuda_cores"] = (out["cuda"]["factor_inverse_solve_ms"] /
+                                                   out["tf32x3"]["factor_inverse_solve_ms"])
+    # the GEMM alone
+    g = max(nb - 128, 128)
+    A = torch.randn((g, 128), dtype=torch.float32, device=dev)
+    B = torch.randn((128, g), dtype=torch.float32, device=dev)
+    Cm = torch.randn((g, g), dtype=torch.float32, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    times = []
+    for it in range(8):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.call("fj_gemm_tf32", A.data_ptr(), 128, B.data_ptr(), g, Cm.data_ptr(), g, g, g, 128, C.c_float(-1.0),
+                  C.c_float(1.0), 3, err.data_ptr(), s)
+        e1.record()
+        torch.cuda.synchronize()
+        if it >= 3:
+            times.append(e0.elapsed_time(e1))
+    t = float(np.median(times))
+    tf32_peak = measured_peaks().get("bf16_tflops", 1590.0) / 2
+    achieved = 3 * 2.0 * g * g * 128 / (t * 1e-3) / 1e12
+    out["gemm"] = {"shape": [g, g, 128], "passes": 3, "ms": t, "tflops_tf32_issued": achieved,
+                   "tf32_peak_tflops": tf32_peak, "frac": achieved / tf32_peak,
+                   "peak_source": "half of MEASURED_PEAKS.json bf16_tflops (dense TF32 runs at half the bf16 rate)"}
+    return out
+
+
+def measured_peaks():
+    p = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
 
 
 def config_table(args, torch):
