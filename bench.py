@@ -14,6 +14,9 @@ e2e     the same metric through the C ABI with host buffers: every step copies i
         step's solution slot back to pinned host memory.
 fp64_gpu  the plain FP64 path on the same steps, and the mixed path's CL/CD error
         against it.
+autotune  the split counts of the step's three Biot-Savart sums, timed on the device before
+        the timed regions (fj_autotune_vind) for both precisions, against the wave-filling
+        rule the launches use untuned.
 factorisation  the mixed solve's FP32 LU + FP32 inverse of this workload's AIC through the
         tensor-core path (tcgen05 TF32, three-pass split; the default) and through the FP32
         CUDA-core path, and the tensor-core GEMM alone at the LU's trailing-update shape
@@ -342,6 +345,14 @@ def main():
     case = workload(args, n_slots - 1)
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    # -- autotuning of the sum launches (outside every timed region) ----------------------
+    from flapjax_b200 import tuning
+
+    t_tune = time.perf_counter()
+    kern = _lib.FJ_KERNEL_CUTOFF if case.kernel == "cutoff" else _lib.FJ_KERNEL_EPSILON
+    shapes = tuning.step_shapes(case.m, case.n, case.m_star, case.free_wake)
+    autotune = {p: tuning.autotune(shapes, p, kern, case.r_cut) for p in ("mixed", "fp64")}
+    autotune["seconds"] = time.perf_counter() - t_tune
     # -- mixed path: value ---------------------------------------------------------------
     uv, dc = make_case(case, "mixed", n_slots)
     run_device_steps(dc, 1, 1 + W, flush, torch)
@@ -443,7 +454,7 @@ def main():
                    "l2": "flushed between steps (256 MB write outside the timed events)",
                    "parallelism": f"independent case replica per GPU x{world}", "seed": case.seed},
         "e2e": e2e, "fp64_gpu": fp64, "roofline": roof, "cpu_baseline": cpu, "factorisation": factor,
-        "gpu_launches": int(launches), "clocks": clk.summary(), "serving": serving,
+        "gpu_launches": int(launches), "clocks": clk.summary(), "serving": serving, "autotune": autotune,
     }
     print(json.dumps(line))
     return 0

@@ -182,6 +182,12 @@ _SIGS = {
     "fj_solve_mixed": (C.c_int, [_P, C.c_int, _P, _P, C.c_int, _P, _P, C.c_size_t, _P]),
     "fj_gemm_tf32": (C.c_int, [_P, C.c_int, _P, C.c_int, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
                                C.c_float, C.c_int, _P, _P]),
+    "fj_autotune_vind_workspace_size": (C.c_int, [C.c_int, _P, _P, C.c_int, C.POINTER(C.c_size_t)]),
+    "fj_autotune_vind": (C.c_int, [C.c_int, C.c_int, C.c_double, _P, _P, C.c_int, _P, _P, _P, _P, _P, C.c_size_t,
+                                   _P]),
+    "fj_autotune_table_size": (C.c_int, [C.POINTER(C.c_int)]),
+    "fj_autotune_get": (C.c_int, [_P, C.c_int]),
+    "fj_autotune_set": (C.c_int, [_P, C.c_int]),
 }
 
 EXPORTED = tuple(_SIGS)

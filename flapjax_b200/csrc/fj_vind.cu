@@ -699,7 +699,35 @@ int split_bound(int64_t n_targets, int64_t n_elem_max, int precision) {
     return (int)std::max<int64_t>(1, std::min<int64_t>({1024, cap, std::max<int64_t>(1, n_elem_max / 256)}));
 }
 
+// Autotuned splits (fj_autotune_vind): published once per tuning as a whole new table,
+// never modified after publication; choose_split reads it lock-free.
+static std::atomic<const TuneTable*> g_tune{nullptr};
+
+const TuneTable* tune_table() { return g_tune.load(std::memory_order_acquire); }
+
+void tune_publish(const TuneTable* t) { g_tune.store(t, std::memory_order_release); }
+
+int tune_bucket_targets(int64_t n_targets) {
+    int b = 0;
+    while (b + 1 < kTuneTargetBuckets && (1ll << (b + 1)) <= n_targets) ++b;
+    return b;
+}
+
+int tune_bucket_elem(int64_t n_elem) {
+    int b = 0;
+    while (b + 1 < kTuneElemBuckets && (1ll << (b + 1)) <= n_elem) ++b;
+    return b;
+}
+
 int choose_split(int64_t n_targets, int64_t n_elem, int precision) {
+    if (const TuneTable* t = tune_table()) {
+        const int v = t->split[precision == FJ_PREC_FP64 ? 0 : 1][tune_bucket_targets(n_targets)][tune_bucket_elem(n_elem)];
+        if (v > 0) return std::min(v, split_bound(n_targets, n_elem, precision));
+    }
+    return heuristic_split(n_targets, n_elem, precision);
+}
+
+int heuristic_split(int64_t n_targets, int64_t n_elem, int precision) {
     query_occupancy();
     const int T = precision == FJ_PREC_FP64 ? kT64 : kT32;
     const int64_t ctas = (n_targets + (int64_t)kBlock * T - 1) / ((int64_t)kBlock * T);

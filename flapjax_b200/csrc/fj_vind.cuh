@@ -106,6 +106,19 @@ int vind_launch(const VindJob& job, int precision, int kernel, double r_cut, cud
 int reduce_partials(const double* part, int n_split, int64_t n_targets, double* out,
                     int accumulate, double scale, cudaStream_t s);
 int choose_split(int64_t n_targets, int64_t n_elem, int precision);
+// The wave-filling rule choose_split falls back to where no tuned entry exists.
+int heuristic_split(int64_t n_targets, int64_t n_elem, int precision);
+
+// Tuned split counts, by precision (0 FP64, 1 FP32), log2 of the target count and log2 of
+// the stream length; 0 = not tuned.  A published table is immutable.
+constexpr int kTuneTargetBuckets = 24, kTuneElemBuckets = 28;
+struct TuneTable {
+    int16_t split[2][kTuneTargetBuckets][kTuneElemBuckets];
+};
+const TuneTable* tune_table();
+void tune_publish(const TuneTable* t);
+int tune_bucket_targets(int64_t n_targets);
+int tune_bucket_elem(int64_t n_elem);
 int split_bound(int64_t n_targets, int64_t n_elem_max, int precision);
 
 }  // namespace fj

@@ -375,6 +375,26 @@ FJ_API int fj_solve_mixed(const double* d_a, int n, const double* d_b, double* d
 FJ_API int fj_gemm_tf32(const float* d_a, int lda, const float* d_b, int ldb, float* d_c, int ldc, int m, int n,
                         int k, float alpha, float beta, int passes, int* d_err, fj_stream_t stream);
 
+/* Autotuner of the Biot-Savart sum launches (the reference's vmap/lax.map chunking,
+ * aero/aic.py:47-63, 237-245, has no tunable).  A sum of n_targets points over a stream of
+ * n_elem filament elements runs as target tiles x splits CTAs; for each shape this times
+ * the sum and its reduction at candidate split counts on a synthetic lattice of that
+ * stream length (CUDA events; synchronises) and publishes the fastest into a new
+ * immutable table, by precision, log2 n_targets and log2 stream length, that every later
+ * launch consults.  Per shape it reports the split chosen, the rule's split and both
+ * times (ms); any of those arrays may be NULL.  precision: FJ_PREC_FP64 or
+ * FJ_PREC_MIXED (the FP32 sums). */
+FJ_API int fj_autotune_vind_workspace_size(int precision, const int64_t* n_targets, const int64_t* n_elem,
+                                           int n_shapes, size_t* bytes);
+FJ_API int fj_autotune_vind(int precision, int kernel, double r_cut, const int64_t* n_targets,
+                            const int64_t* n_elem, int n_shapes, int* chosen, int* heuristic, double* chosen_ms,
+                            double* heuristic_ms, void* d_ws, size_t ws_bytes, fj_stream_t stream);
+/* The published table as int16 entries (fj_autotune_table_size of them; 0 = not tuned),
+ * to save it and load it into another process; fj_autotune_set(NULL, 0) drops it. */
+FJ_API int fj_autotune_table_size(int* n_entries);
+FJ_API int fj_autotune_get(int16_t* entries, int n_entries);
+FJ_API int fj_autotune_set(const int16_t* entries, int n_entries);
+
 #ifdef __cplusplus
 }
 #endif

@@ -100,3 +100,19 @@ def test_struct_layouts_match_header(tmp_path):
     assert int(out["fj_flowfield.gust_x0"]) == _lib.FjFlowfield.gust_x0.offset
     assert int(out["fj_case_buffers.d_force_total"]) == _lib.FjCaseBuffers.d_force_total.offset
     assert int(out["fj_profile.vind_pairs"]) == _lib.FjProfile.vind_pairs.offset
+
+
+def test_autograd_module_imports_without_a_gpu():
+    from flapjax_b200 import autograd
+
+    assert callable(autograd.induced_velocity) and callable(autograd.dense_solve)
+
+
+def test_tuning_shapes_of_a_step():
+    from flapjax_b200 import tuning
+
+    s = tuning.step_shapes(16, 128, 200, True)
+    assert s[0] == (16 * 128, 2 * 201 * 129)
+    assert s[1] == (16 * 129 + 17 * 128, 2 * 17 * 129 + 2 * 201 * 129)
+    assert s[2] == (201 * 129, 2 * 17 * 129 + 2 * 201 * 129)
+    assert len(tuning.step_shapes(4, 8, 10, False)) == 2

@@ -250,3 +250,31 @@ def test_device_sweep_mirror(cuda):
     J_o, g_o = OracleAdjoint(ref).gradient(c.hg_t, c.hg_dot_t, fw, checkpoint=2)
     assert abs(J - J_o) <= 1e-10 * abs(J_o)
     assert np.max(np.abs(g - g_o)) <= 1e-8 * np.max(np.abs(g_o))
+
+
+def test_autograd_wrappers_pass_gradcheck(cuda):
+    """The hand-written VJPs behind torch.autograd.Function (fj_vind -> fj_vind_vjp,
+    fj_lu_factor/solve -> fj_lu_solve_t) against torch's central differences."""
+    import torch
+
+    from flapjax_b200 import _lib
+    from flapjax_b200.autograd import dense_solve, induced_velocity
+
+    g = torch.Generator().manual_seed(5)
+    R, Cn = 3, 4
+    zeta = torch.zeros((R + 1, Cn + 1, 3), dtype=torch.float64)
+    zeta[..., 0] = torch.linspace(0.0, 1.0, R + 1)[:, None]
+    zeta[..., 1] = torch.linspace(0.0, 2.0, Cn + 1)[None, :]
+    zeta += 0.02 * torch.randn(zeta.shape, generator=g, dtype=torch.float64)
+    gamma = torch.randn((R, Cn), generator=g, dtype=torch.float64)
+    targets = torch.tensor([[0.3, 0.7, 0.4], [1.5, -0.2, 0.3], [0.5, 1.1, -0.6], [-0.4, 2.3, 0.2]],
+                           dtype=torch.float64)
+    args = [t.to(cuda).requires_grad_(True) for t in (targets, zeta, gamma)]
+    for kern, rc in ((_lib.FJ_KERNEL_EPSILON, 0.0), (_lib.FJ_KERNEL_CUTOFF, 1e-3)):
+        assert torch.autograd.gradcheck(lambda t, z, gm: induced_velocity(t, z, gm, kern, rc), args, eps=1e-6,
+                                        atol=1e-8, rtol=1e-6)
+    n = 12
+    a = (torch.randn((n, n), generator=g, dtype=torch.float64) + 4 * torch.eye(n, dtype=torch.float64)).to(cuda)
+    b = torch.randn(n, generator=g, dtype=torch.float64).to(cuda)
+    assert torch.autograd.gradcheck(dense_solve, (a.requires_grad_(True), b.requires_grad_(True)), eps=1e-6,
+                                    atol=1e-8, rtol=1e-6)
