@@ -128,34 +128,37 @@ class _Dev:
                   self.stream())
         return b.cpu().numpy().reshape(rhs.shape)
 
-    def solve_t(self, zeta_b, zeta_w_static, rhs):
-        """mu with A^T mu = rhs, A the AIC of zeta_b (with the wake lumped onto the TE
-        column when zeta_w_static is given: the static solve)."""
-        m, n = zeta_b.shape[0] - 1, zeta_b.shape[1] - 1
-        nb = m * n
-        tz = self.t(zeta_b)
-        zp = (C.c_void_p * 1)(tz.data_ptr())
-        mm, nn = (C.c_int * 1)(m), (C.c_int * 1)(n)
-        wp, ms = None, (C.c_int * 1)(0)
-        if zeta_w_static is not None:
-            tw = self.t(zeta_w_static)
-            wp = (C.c_void_p * 1)(tw.data_ptr())
-            ms = (C.c_int * 1)(zeta_w_static.shape[0] - 1)
+    def solve_t(self, zetas_b, zetas_w_static, rhs):
+        """mu with A^T mu = rhs (flat, all surfaces), A the AIC of the bound lattices
+        zetas_b (with each surface's wake lumped onto its TE column when zetas_w_static is
+        given: the static solve)."""
+        k = len(zetas_b)
+        ms = [z.shape[0] - 1 for z in zetas_b]
+        ns = [z.shape[1] - 1 for z in zetas_b]
+        nb = sum(m * n for m, n in zip(ms, ns))
+        tz = [self.t(z) for z in zetas_b]
+        zp = (C.c_void_p * k)(*[z.data_ptr() for z in tz])
+        mm, nn = (C.c_int * k)(*ms), (C.c_int * k)(*ns)
+        wp, mstar = None, (C.c_int * k)(*([0] * k))
+        if zetas_w_static is not None:
+            tw = [self.t(z) for z in zetas_w_static]
+            wp = (C.c_void_p * k)(*[z.data_ptr() for z in tw])
+            mstar = (C.c_int * k)(*[z.shape[0] - 1 for z in zetas_w_static])
         a = self.torch.empty((nb, nb), dtype=self.torch.float64, device=self.dev)
         w = C.c_size_t()
-        _lib.call("fj_aic_workspace_size", mm, nn, 1, C.byref(w))
+        _lib.call("fj_aic_workspace_size", mm, nn, k, C.byref(w))
         ws = self.ws("aic", w.value)
         s = self.stream()
         mp, mn = self._mir if self._mir is not None else (None, None)
-        _lib.call("fj_aic_assemble", zp, mm, nn, 1, wp, ms, mp, mn, self.kernel, self.r_cut, a.data_ptr(),
+        _lib.call("fj_aic_assemble", zp, mm, nn, k, wp, mstar, mp, mn, self.kernel, self.r_cut, a.data_ptr(),
                   ws.data_ptr(), ws.numel(), s)
         piv = self.torch.empty(nb, dtype=self.torch.int32, device=self.dev)
         _lib.call("fj_lu_workspace_size", nb, C.byref(w))
         wl = self.ws("lu", w.value)
         _lib.call("fj_lu_factor", a.data_ptr(), nb, piv.data_ptr(), wl.data_ptr(), wl.numel(), s)
-        b = self.t(rhs.ravel())
+        b = self.t(np.ravel(rhs))
         _lib.call("fj_lu_solve_t", a.data_ptr(), nb, piv.data_ptr(), b.data_ptr(), wl.data_ptr(), wl.numel(), s)
-        return b.cpu().numpy().reshape(rhs.shape)
+        return b.cpu().numpy().reshape(np.shape(rhs))
 
 
 def _avg4_T(bar_c, shape):
@@ -253,6 +256,26 @@ def _variable_wake_T(zw_nm1, te_n, gb_te_nm1, gw_nm1, dw, dt, U, Zw_bar, Gw_bar,
     return X_bar[1:], X_bar[0], G_bar[0], G_bar[1:]
 
 
+def _flow_T(ff, x, t, ubar):
+    """x-cotangent of u = ff(x, t) (aero/flowfields.py:87-181).  Zero for a Constant
+    field.  For the 1-cos gust u = a (A/2)(1 - cos(pi g / L)) on 0 < g < 2L, with
+    g = (x - x0 - U t) . d (U t only with relative motion), so
+    x_bar = (ubar . a) (A/2)(pi/L) sin(pi g / L) d inside the gust, 0 outside (the
+    reference's jax.vjp through jnp.where differentiates the taken branch)."""
+    x = np.asarray(x)
+    if not hasattr(ff, "gust_length"):
+        return np.zeros_like(x)
+    d, a = ff.gust_travel_direction, ff.gust_amplitude_direction
+    L, A = ff.gust_length, ff.gust_amplitude
+    rel = x - ff.gust_x0
+    if ff.relative_motion:
+        rel = rel - ff.u_inf * t
+    g = rel @ d
+    inside = (g > 0) & (g < 2.0 * L)
+    coef = np.where(inside, 0.5 * A * (np.pi / L) * np.sin(np.pi * g / L), 0.0) * (np.asarray(ubar) @ a)
+    return coef[..., None] * d
+
+
 def _frames_T(bar_zb, bar_zbd, hg, hgd, dof):
     """zeta_b0 cotangent of zeta_b = R zeta_b0 + t and zeta_b_dot = Rdot zeta_b0 + tdot."""
     R = hg[dof][:, :3, :3]          # (n+1, 3, 3) per spanwise vertex column
@@ -267,16 +290,10 @@ class PrescribedAdjoint:
     """Forward + reverse sweep for one FP64 UVLM case (flapjax_b200.UVLM)."""
 
     def __init__(self, uvlm, device=None):
-        if uvlm.n_surf != 1:
-            raise NotImplementedError("the adjoint handles one surface")
         if uvlm.kernel.kernel_id not in (_lib.FJ_KERNEL_EPSILON, _lib.FJ_KERNEL_CUTOFF):
             raise NotImplementedError("the adjoint is written for the epsilon and cutoff kernels")
         if uvlm.precision != "fp64":
             raise NotImplementedError("the adjoint runs in FP64")
-        from .flowfields import Constant
-
-        if not isinstance(uvlm.flowfield, Constant):
-            raise NotImplementedError("the adjoint assumes a uniform (Constant) flow")
         self.uv = uvlm
         mirror = None if uvlm.mirror_point is None else (uvlm.mirror_point, uvlm.mirror_normal)
         self.d = _Dev(device, uvlm.kernel.kernel_id, uvlm.kernel.r_cut, mirror)
@@ -308,7 +325,9 @@ class PrescribedAdjoint:
         return seg
 
     def gradient(self, hg_t, hg_dot_t, force_weights, checkpoint=10):
-        """Return (J, dJ/dzeta_b0) for J = sum_{n>=1} force_weights[n] . F_n."""
+        """Return (J, dJ/dzeta_b0) for J = sum_{n>=1} force_weights[n] . F_n, F_n the total
+        force on all surfaces at slot n; dJ/dzeta_b0 is an array for one surface and a
+        list (one per surface) otherwise."""
         uv = self.uv
         hg_t = np.asarray(hg_t, float)
         hg_dot_t = np.asarray(hg_dot_t, float)
@@ -326,18 +345,14 @@ class PrescribedAdjoint:
                 J += float(fw[s0 + n] @ seg.force_total[n])
             cur = seg[s1 - s0]
             ckpt[s1] = cur
-        # reverse
-        g = uv.grid_disc[0]
-        m, n_, W = g.m, g.n, g.m_star
-        dt, relax, rho = uv.dt, uv.gamma_dot_relaxation, uv.flowfield.rho
-        U = uv.flowfield.u_inf
-        dof = uv.dof_mapping[0]
-        zeta0_bar = np.zeros_like(uv.zeta_b0[0])
-        Gb_next = np.zeros((m, n_))      # cotangent of Gamma_b at slot n (being completed)
-        Gbd_next = np.zeros((m, n_))
-        Gw_next = np.zeros((W, n_))
-        Zw_next = np.zeros((W + 1, n_ + 1, 3))
-        Zb_next = np.zeros((m + 1, n_ + 1, 3))  # free wake: cotangent of slot n's lattice from step n+1
+        # reverse: per surface, the cotangents of slot n's state flowing into step n
+        dims = [(g.m, g.n, g.m_star) for g in uv.grid_disc]
+        zeta0_bar = [np.zeros_like(np.asarray(z, float)) for z in uv.zeta_b0]
+        Gb_next = [np.zeros((m, n)) for m, n, _ in dims]
+        Gbd_next = [np.zeros((m, n)) for m, n, _ in dims]
+        Gw_next = [np.zeros((W, n)) for _, n, W in dims]
+        Zw_next = [np.zeros((W + 1, n + 1, 3)) for _, n, W in dims]
+        Zb_next = [np.zeros((m + 1, n + 1, 3)) for m, n, _ in dims]  # free wake: from step n+1
         seg_starts = sorted(k for k in ckpt if k < N)
         for s0 in reversed(seg_starts):
             s1 = min(N, s0 + checkpoint)
@@ -346,165 +361,225 @@ class PrescribedAdjoint:
                 nstep = s0 + loc
                 Gb_next, Gbd_next, Gw_next, Zw_next, Zb_next = self._reverse_step(
                     seg, loc, fw[nstep], Gb_next, Gbd_next, Gw_next, Zw_next, Zb_next, zeta0_bar, hg_t[nstep],
-                    hg_dot_t[nstep], dof, m, n_, W, dt, relax, rho, U)
-        self._reverse_static(static, Gb_next, Gw_next, Zw_next, Zb_next, zeta0_bar, uv.hg_ref, dof, m, n_, W, U)
-        return J, zeta0_bar
+                    hg_dot_t[nstep])
+        self._reverse_static(static, Gb_next, Gw_next, Zw_next, Zb_next, zeta0_bar, uv.hg_ref)
+        return J, (zeta0_bar[0] if len(zeta0_bar) == 1 else zeta0_bar)
 
     # -- one dynamic reverse step ------------------------------------------------------
-    def _reverse_step(self, seg, loc, Fbar, Gb_n, Gbd_n, Gw_n, Zw_n, Zb_n, zeta0_bar, hg_n, hgd_n, dof, m, n_, W,
-                      dt, relax, rho, U):
-        d = self.d
-        zb = seg.zeta_b[0][loc]
-        zbd = seg.zeta_b_dot[0][loc]
-        zw = seg.zeta_w[0][loc]
-        gb = seg.gamma_b[0][loc]
-        gw = seg.gamma_w[0][loc]
-        gbd = seg.gamma_b_dot[0][loc]
-        nc = seg.nc[0][loc]
-        c = seg.c[0][loc]
-        Zb = Zb_n.copy()
-        Zbd = np.zeros_like(zbd)
-        Gb = Gb_n.copy()
-        Gw = Gw_n.copy()
-        Zw = Zw_n.copy()
-        Gbd = Gbd_n.copy()
-        # 1. forces
-        mp_c = 0.5 * (zb[:-1] + zb[1:])
-        mp_s = 0.5 * (zb[:, :-1] + zb[:, 1:])
-        targets = np.concatenate([mp_c.reshape(-1, 3), mp_s.reshape(-1, 3)])
-        lats = [(zw, gw), (zb, gb)]
+    def _reverse_step(self, seg, loc, Fbar, Gb_n, Gbd_n, Gw_n, Zw_n, Zb_n, zeta0_bar, hg_n, hgd_n):
+        d, uv = self.d, self.uv
+        ff = uv.flowfield
+        dt, relax, rho = uv.dt, uv.gamma_dot_relaxation, ff.rho
+        t_n = float(np.ravel(seg.t)[loc]) if np.ndim(seg.t) else float(seg.t)
+        S = len(Gb_n)
+        sl = range(S)
+        zb = [seg.zeta_b[s][loc] for s in sl]
+        zbd = [seg.zeta_b_dot[s][loc] for s in sl]
+        zw = [seg.zeta_w[s][loc] for s in sl]
+        gb = [seg.gamma_b[s][loc] for s in sl]
+        gw = [seg.gamma_w[s][loc] for s in sl]
+        gbd = [seg.gamma_b_dot[s][loc] for s in sl]
+        nc = [seg.nc[s][loc] for s in sl]
+        c = [seg.c[s][loc] for s in sl]
+        Zb = [a.copy() for a in Zb_n]
+        Zbd = [np.zeros_like(a) for a in zbd]
+        Gb = [a.copy() for a in Gb_n]
+        Gw = [a.copy() for a in Gw_n]
+        Zw = [a.copy() for a in Zw_n]
+        Gbd = [a.copy() for a in Gbd_n]
+        lats = [(zw[s], gw[s]) for s in sl] + [(zb[s], gb[s]) for s in sl]  # lattice i: wake i, bound S + i
+        # 1. forces: f = rho Gamma_eff (v_rel x r) per filament, v_rel = u + V - zeta_dot (midpoints)
+        mp_c = [0.5 * (z[:-1] + z[1:]) for z in zb]
+        mp_s = [0.5 * (z[:, :-1] + z[:, 1:]) for z in zb]
+        parts = []
+        for s in sl:
+            parts += [mp_c[s].reshape(-1, 3), mp_s[s].reshape(-1, 3)]
+        sizes = [p.shape[0] for p in parts]
+        offs = np.concatenate([[0], np.cumsum(sizes)])
+        targets = np.concatenate(parts)
         v = d.vind(targets, lats)
-        nc_ = mp_c.shape[0] * mp_c.shape[1]
-        v_c, v_s = v[:nc_].reshape(mp_c.shape), v[nc_:].reshape(mp_s.shape)
-        mpd_c = 0.5 * (zbd[:-1] + zbd[1:])
-        mpd_s = 0.5 * (zbd[:, :-1] + zbd[:, 1:])
-        vr_c, vr_s = U + v_c - mpd_c, U + v_s - mpd_s
-        g_c = np.zeros((m, n_ + 1))
-        g_c[:, :-1] = gb
-        g_c[:, 1:] += -gb
-        g_s = np.zeros((m + 1, n_))
-        g_s[:-1, :] = -gb
-        g_s[1:, :] += gb
-        if W > 0:
-            g_s[-1, :] += -gw[0, :]
-        r_c = zb[1:] - zb[:-1]
-        r_s = zb[:, 1:] - zb[:, :-1]
-        gbar_c = rho * np.einsum("ijk,k->ij", np.cross(vr_c, r_c), Fbar)
-        gbar_s = rho * np.einsum("ijk,k->ij", np.cross(vr_s, r_s), Fbar)
-        vbar_c = rho * g_c[..., None] * np.cross(r_c, Fbar)
-        vbar_s = rho * g_s[..., None] * np.cross(r_s, Fbar)
-        rbar_c = rho * g_c[..., None] * np.cross(Fbar, vr_c)
-        rbar_s = rho * g_s[..., None] * np.cross(Fbar, vr_s)
-        Zb[1:] += rbar_c
-        Zb[:-1] -= rbar_c
-        Zb[:, 1:] += rbar_s
-        Zb[:, :-1] -= rbar_s
-        Zbd[:-1] += -0.5 * vbar_c
-        Zbd[1:] += -0.5 * vbar_c
-        Zbd[:, :-1] += -0.5 * vbar_s
-        Zbd[:, 1:] += -0.5 * vbar_s
-        Gb += gbar_c[:, :-1]      # g_c[k,l] = G[k,l] (l < n) - G[k,l-1] (l >= 1)
-        Gb -= gbar_c[:, 1:]
-        Gb -= gbar_s[:-1, :]      # g_s[k,l] = -G[k,l] (k < m) + G[k-1,l] (k >= 1)
-        Gb += gbar_s[1:, :]
-        if W > 0:
-            Gw[0, :] -= gbar_s[-1, :]
-        lam = np.concatenate([vbar_c.reshape(-1, 3), vbar_s.reshape(-1, 3)])
+        lam = np.zeros_like(targets)
+        vbar = []
+        for s in sl:
+            m, n_ = gb[s].shape
+            v_c = v[offs[2 * s]:offs[2 * s + 1]].reshape(mp_c[s].shape)
+            v_s = v[offs[2 * s + 1]:offs[2 * s + 2]].reshape(mp_s[s].shape)
+            mpd_c = 0.5 * (zbd[s][:-1] + zbd[s][1:])
+            mpd_s = 0.5 * (zbd[s][:, :-1] + zbd[s][:, 1:])
+            vr_c, vr_s = ff(mp_c[s], t_n) + v_c - mpd_c, ff(mp_s[s], t_n) + v_s - mpd_s
+            g_c = np.zeros((m, n_ + 1))
+            g_c[:, :-1] = gb[s]
+            g_c[:, 1:] += -gb[s]
+            g_s = np.zeros((m + 1, n_))
+            g_s[:-1, :] = -gb[s]
+            g_s[1:, :] += gb[s]
+            if gw[s].shape[0] > 0:
+                g_s[-1, :] += -gw[s][0, :]
+            r_c = zb[s][1:] - zb[s][:-1]
+            r_s = zb[s][:, 1:] - zb[s][:, :-1]
+            gbar_c = rho * np.einsum("ijk,k->ij", np.cross(vr_c, r_c), Fbar)
+            gbar_s = rho * np.einsum("ijk,k->ij", np.cross(vr_s, r_s), Fbar)
+            vbar_c = rho * g_c[..., None] * np.cross(r_c, Fbar)
+            vbar_s = rho * g_s[..., None] * np.cross(r_s, Fbar)
+            rbar_c = rho * g_c[..., None] * np.cross(Fbar, vr_c)
+            rbar_s = rho * g_s[..., None] * np.cross(Fbar, vr_s)
+            Zb[s][1:] += rbar_c
+            Zb[s][:-1] -= rbar_c
+            Zb[s][:, 1:] += rbar_s
+            Zb[s][:, :-1] -= rbar_s
+            Zbd[s][:-1] += -0.5 * vbar_c
+            Zbd[s][1:] += -0.5 * vbar_c
+            Zbd[s][:, :-1] += -0.5 * vbar_s
+            Zbd[s][:, 1:] += -0.5 * vbar_s
+            Gb[s] += gbar_c[:, :-1]      # g_c[k,l] = G[k,l] (l < n) - G[k,l-1] (l >= 1)
+            Gb[s] -= gbar_c[:, 1:]
+            Gb[s] -= gbar_s[:-1, :]      # g_s[k,l] = -G[k,l] (k < m) + G[k-1,l] (k >= 1)
+            Gb[s] += gbar_s[1:, :]
+            if gw[s].shape[0] > 0:
+                Gw[s][0, :] -= gbar_s[-1, :]
+            lam[offs[2 * s]:offs[2 * s + 1]] = vbar_c.reshape(-1, 3)
+            lam[offs[2 * s + 1]:offs[2 * s + 2]] = vbar_s.reshape(-1, 3)
+            vbar.append((vbar_c, vbar_s))
         tbar, zbar, gbars = d.vjp(targets, lats, lam)
-        mpbar_c, mpbar_s = tbar[:nc_].reshape(mp_c.shape), tbar[nc_:].reshape(mp_s.shape)
-        Zb[:-1] += 0.5 * mpbar_c
-        Zb[1:] += 0.5 * mpbar_c
-        Zb[:, :-1] += 0.5 * mpbar_s
-        Zb[:, 1:] += 0.5 * mpbar_s
-        Zw += zbar[0]
-        Zb += zbar[1]
-        Gw += gbars[0]
-        Gb += gbars[1]
-        # unsteady force rho * gamma_dot * nc
-        Gbd += rho * np.einsum("ijk,k->ij", nc, Fbar)
-        ncbar = rho * gbd[..., None] * Fbar
-        # 2. gamma_dot filter
-        Gb += (relax / dt) * Gbd
-        Gb_prev = -(relax / dt) * Gbd
-        Gbd_prev = (1.0 - relax) * Gbd
-        # 3. transpose solve with A_n
+        for s in sl:
+            mpbar_c = tbar[offs[2 * s]:offs[2 * s + 1]].reshape(mp_c[s].shape) + _flow_T(ff, mp_c[s], t_n, vbar[s][0])
+            mpbar_s = tbar[offs[2 * s + 1]:offs[2 * s + 2]].reshape(mp_s[s].shape) + _flow_T(ff, mp_s[s], t_n,
+                                                                                            vbar[s][1])
+            Zb[s][:-1] += 0.5 * mpbar_c
+            Zb[s][1:] += 0.5 * mpbar_c
+            Zb[s][:, :-1] += 0.5 * mpbar_s
+            Zb[s][:, 1:] += 0.5 * mpbar_s
+            Zw[s] += zbar[s]
+            Zb[s] += zbar[S + s]
+            Gw[s] += gbars[s]
+            Gb[s] += gbars[S + s]
+        # unsteady force rho * gamma_dot * nc; 2. gamma_dot filter
+        ncbar, Gb_prev, Gbd_prev = [], [], []
+        for s in sl:
+            Gbd[s] += rho * np.einsum("ijk,k->ij", nc[s], Fbar)
+            ncbar.append(rho * gbd[s][..., None] * Fbar)
+            Gb[s] += (relax / dt) * Gbd[s]
+            Gb_prev.append(-(relax / dt) * Gbd[s])
+            Gbd_prev.append((1.0 - relax) * Gbd[s])
+        # 3. transpose solve with A_n (all surfaces)
+        rhs = np.concatenate([g.ravel() for g in Gb])
         factors = getattr(seg, "factors", None)
-        mu = d.solve_t(zb, None, Gb) if factors is None else d.solve_t_factors(factors[0][loc], factors[1][loc], Gb)
-        # 4. RHS + AIC geometry: b = -(U - c_dot + V_w(c)) . nc and A Gamma = nc . V_b(c)
-        cdot = 0.5 * (0.5 * (zbd[:-1, :-1] + zbd[1:, :-1]) + 0.5 * (zbd[:-1, 1:] + zbd[1:, 1:]))
-        Vtot = d.vind(c, [(zw, gw), (zb, gb)])
-        ncbar += -mu[..., None] * (U - cdot + Vtot)
-        cdotbar = mu[..., None] * nc
-        lam_c = -mu[..., None] * nc
-        cbar, zbar2, gbar2 = d.vjp(c, [(zw, gw), (zb, gb)], lam_c)
-        Zw += zbar2[0]
-        Zb += zbar2[1]
-        Gw += gbar2[0]   # the bound part belongs to the solve's linearity in Gamma
-        # 5. geometry
-        Zb += _avg4_T(cbar, zb.shape)
-        Zb += _normals_T(zb, ncbar)
-        Zbd += _avg4_T(cdotbar, zbd.shape)
+        mu_flat = (d.solve_t(zb, None, rhs) if factors is None
+                   else d.solve_t_factors(factors[0][loc], factors[1][loc], rhs))
+        po = np.concatenate([[0], np.cumsum([g.size for g in gb])])
+        mu = [mu_flat[po[s]:po[s + 1]].reshape(gb[s].shape) for s in sl]
+        # 4. RHS + AIC geometry: b = -(u - c_dot + V_w(c)) . nc and A Gamma = nc . V_b(c)
+        cdot = [0.5 * (0.5 * (z[:-1, :-1] + z[1:, :-1]) + 0.5 * (z[:-1, 1:] + z[1:, 1:])) for z in zbd]
+        co = np.concatenate([[0], np.cumsum([x.shape[0] * x.shape[1] for x in c])])
+        c_all = np.concatenate([x.reshape(-1, 3) for x in c])
+        Vtot = d.vind(c_all, lats)
+        lam_c = [-mu[s][..., None] * nc[s] for s in sl]
+        cdotbar = []
+        for s in sl:
+            Vs = Vtot[co[s]:co[s + 1]].reshape(c[s].shape)
+            ncbar[s] += -mu[s][..., None] * (ff(c[s], t_n) - cdot[s] + Vs)
+            cdotbar.append(mu[s][..., None] * nc[s])
+        cbar_all, zbar2, gbar2 = d.vjp(c_all, lats, np.concatenate([x.reshape(-1, 3) for x in lam_c]))
+        for s in sl:
+            cbar = cbar_all[co[s]:co[s + 1]].reshape(c[s].shape) + _flow_T(ff, c[s], t_n, lam_c[s])
+            Zw[s] += zbar2[s]
+            Zb[s] += zbar2[S + s]
+            Gw[s] += gbar2[s]   # the bound part belongs to the solve's linearity in Gamma
+            # 5. geometry
+            Zb[s] += _avg4_T(cbar, zb[s].shape)
+            Zb[s] += _normals_T(zb[s], ncbar[s])
+            Zbd[s] += _avg4_T(cdotbar[s], zbd[s].shape)
         # 6. wake shedding transposes; the free wake's convection velocity
-        #    V(zw_{n-1}; bound n-1, wake n-1) adds its own VJP
-        zw_nm1, gw_nm1 = seg.zeta_w[0][loc - 1], seg.gamma_w[0][loc - 1]
-        zb_nm1, gb_nm1 = seg.zeta_b[0][loc - 1], seg.gamma_b[0][loc - 1]
-        free = bool(self.uv.free_wake) and W > 0
-        lats_nm1 = [(zb_nm1, gb_nm1), (zw_nm1, gw_nm1)]
-        dw = self.uv.delta_w[0] if getattr(self.uv, "delta_w", None) else None
-        if dw is not None:
-            v_conv = d.vind(zw_nm1, lats_nm1) if free else None
-            zw_p, te_bar, gte_bar, gw_p = _variable_wake_T(
-                zw_nm1, zb[-1], gb_nm1[-1], gw_nm1, np.asarray(dw, float), dt, U, Zw, Gw, v_conv)
-            Zb[-1] += te_bar
-            Zw_prev = zw_p
-            Gw_prev = gw_p
-            Gb_prev[-1, :] += gte_bar
-            conv_rows, conv_bar = slice(None), zw_p  # every row of zw_{n-1} is convected
-        else:
-            Zb[-1] += Zw[0]
-            Zw_prev = np.zeros_like(Zw)
-            Zw_prev[:-1] += Zw[1:]
-            Gw_prev = np.zeros_like(Gw)
-            if W > 0:
-                Gb_prev[-1, :] += Gw[0, :]
-                Gw_prev[:-1] += Gw[1:]
-            conv_rows, conv_bar = slice(0, W), Zw[1:]
-        Zb_prev = np.zeros_like(zb)
+        #    V(zw_{n-1}; all lattices of n-1) adds its own VJP
+        zw_nm1 = [seg.zeta_w[s][loc - 1] for s in sl]
+        gw_nm1 = [seg.gamma_w[s][loc - 1] for s in sl]
+        zb_nm1 = [seg.zeta_b[s][loc - 1] for s in sl]
+        gb_nm1 = [seg.gamma_b[s][loc - 1] for s in sl]
+        lats_nm1 = [(zb_nm1[s], gb_nm1[s]) for s in sl] + [(zw_nm1[s], gw_nm1[s]) for s in sl]
+        dws = getattr(uv, "delta_w", None) or [None] * S
+        free = bool(uv.free_wake)
+        Zw_prev, Gw_prev, Zb_prev = [], [], [np.zeros_like(z) for z in zb]
+        conv = []  # per surface: (rows of zw_{n-1} convected, their cotangent)
+        for s in sl:
+            W = gw[s].shape[0]
+            if dws[s] is not None:
+                v_conv = d.vind(zw_nm1[s], lats_nm1) if (free and W > 0) else None
+                zw_p, te_bar, gte_bar, gw_p = _variable_wake_T(
+                    zw_nm1[s], zb[s][-1], gb_nm1[s][-1], gw_nm1[s], np.asarray(dws[s], float), dt,
+                    ff(zw_nm1[s], t_n), Zw[s], Gw[s], v_conv)
+                Zb[s][-1] += te_bar
+                Zw_prev.append(zw_p)
+                Gw_prev.append(gw_p)
+                Gb_prev[s][-1, :] += gte_bar
+                rows, cb = slice(None), np.array(zw_p)  # every row of zw_{n-1} is convected
+            else:
+                Zb[s][-1] += Zw[s][0]
+                zp = np.zeros_like(Zw[s])
+                zp[:-1] += Zw[s][1:]
+                gp = np.zeros_like(Gw[s])
+                if W > 0:
+                    Gb_prev[s][-1, :] += Gw[s][0, :]
+                    gp[:-1] += Gw[s][1:]
+                Zw_prev.append(zp)
+                Gw_prev.append(gp)
+                rows, cb = slice(0, W), np.array(Zw[s][1:])
+            # x_r = zw_{n-1,r} + dt (u(zw_{n-1,r}, t_n) + ...): the flow's own dependence on x
+            Zw_prev[s][rows] += dt * _flow_T(ff, zw_nm1[s][rows], t_n, cb)
+            conv.append((rows, cb))
         if free:
-            conv_bar = np.array(conv_bar)  # x_r = zw_{n-1,r} + dt (U + V(zw_{n-1,r})): lam = dt x_bar
-            tbar, zbar_c, gbar_c = d.vjp(zw_nm1[conv_rows], lats_nm1, dt * conv_bar)
-            Zw_prev[conv_rows] += tbar
-            Zb_prev += zbar_c[0]
-            Zw_prev += zbar_c[1]
-            Gb_prev += gbar_c[0]
-            Gw_prev += gbar_c[1]
+            tparts = [zw_nm1[s][conv[s][0]].reshape(-1, 3) for s in sl]
+            lparts = [dt * conv[s][1].reshape(-1, 3) for s in sl]
+            to = np.concatenate([[0], np.cumsum([p.shape[0] for p in tparts])])
+            if to[-1] > 0:
+                tbar, zbar_c, gbar_c = d.vjp(np.concatenate(tparts), lats_nm1, np.concatenate(lparts))
+                for s in sl:
+                    Zw_prev[s][conv[s][0]] += tbar[to[s]:to[s + 1]].reshape(zw_nm1[s][conv[s][0]].shape)
+                    Zb_prev[s] += zbar_c[s]
+                    Zw_prev[s] += zbar_c[S + s]
+                    Gb_prev[s] += gbar_c[s]
+                    Gw_prev[s] += gbar_c[S + s]
         # 7. node frames
-        zeta0_bar += _frames_T(Zb, Zbd, hg_n, hgd_n, dof)
+        for s in sl:
+            zeta0_bar[s] += _frames_T(Zb[s], Zbd[s], hg_n, hgd_n, uv.dof_mapping[s])
         return Gb_prev, Gbd_prev, Gw_prev, Zw_prev, Zb_prev
 
-    def _reverse_static(self, st, Gb0, Gw0, Zw0, Zb0, zeta0_bar, hg0, dof, m, n_, W, U):
-        d = self.d
-        zb = st.zeta_b[0]
-        zw = st.zeta_w[0]
-        gb = st.gamma_b[0]
-        gw = st.gamma_w[0]
-        nc = st.nc[0]
-        c = st.c[0]
-        Gb = Gb0.copy()
-        Zw = Zw0.copy()
-        if W > 0:
-            Gb[-1, :] += Gw0.sum(axis=0)  # gamma_w = broadcast of the TE row (uvlm.py:995-1012)
-        mu = d.solve_t(zb, zw if W > 0 else None, Gb)
-        lats = [(zw, gw), (zb, gb)]
-        Vtot = d.vind(c, lats)
-        ncbar = -mu[..., None] * (U + Vtot)
-        cbar, zbar, _ = d.vjp(c, lats, -mu[..., None] * nc)
-        Zw += zbar[0]
-        Zb = zbar[1] + Zb0
-        Zb[-1] += Zw.sum(axis=0)  # every wake row = TE + s_r u_dir (uvlm.py:662-689)
-        Zb += _avg4_T(cbar, zb.shape)
-        Zb += _normals_T(zb, ncbar)
-        zeta0_bar += _frames_T(Zb, None, hg0, None, dof)
+    def _reverse_static(self, st, Gb0, Gw0, Zw0, Zb0, zeta0_bar, hg0):
+        d, uv = self.d, self.uv
+        ff = uv.flowfield
+        t0 = float(np.ravel(st.t)[0]) if np.ndim(st.t) else float(st.t)
+        S = len(Gb0)
+        sl = range(S)
+        zb = [st.zeta_b[s] for s in sl]
+        zw = [st.zeta_w[s] for s in sl]
+        gb = [st.gamma_b[s] for s in sl]
+        gw = [st.gamma_w[s] for s in sl]
+        nc = [st.nc[s] for s in sl]
+        c = [st.c[s] for s in sl]
+        Gb = [g.copy() for g in Gb0]
+        Zw = [z.copy() for z in Zw0]
+        for s in sl:
+            if Gw0[s].shape[0] > 0:
+                Gb[s][-1, :] += Gw0[s].sum(axis=0)  # gamma_w = broadcast of the TE row (uvlm.py:995-1012)
+        lumped = [z if g.shape[0] > 0 else None for z, g in zip(zw, Gw0)]
+        rhs = np.concatenate([g.ravel() for g in Gb])
+        mu_flat = d.solve_t(zb, None if all(x is None for x in lumped) else zw, rhs)
+        po = np.concatenate([[0], np.cumsum([g.size for g in gb])])
+        mu = [mu_flat[po[s]:po[s + 1]].reshape(gb[s].shape) for s in sl]
+        lats = [(zw[s], gw[s]) for s in sl] + [(zb[s], gb[s]) for s in sl]
+        co = np.concatenate([[0], np.cumsum([x.shape[0] * x.shape[1] for x in c])])
+        c_all = np.concatenate([x.reshape(-1, 3) for x in c])
+        Vtot = d.vind(c_all, lats)
+        lam_c = [-mu[s][..., None] * nc[s] for s in sl]
+        cbar_all, zbar, _ = d.vjp(c_all, lats, np.concatenate([x.reshape(-1, 3) for x in lam_c]))
+        for s in sl:
+            ncbar = -mu[s][..., None] * (ff(c[s], t0) + Vtot[co[s]:co[s + 1]].reshape(c[s].shape))
+            cbar = cbar_all[co[s]:co[s + 1]].reshape(c[s].shape) + _flow_T(ff, c[s], t0, lam_c[s])
+            Zw[s] += zbar[s]
+            Zb = zbar[S + s] + Zb0[s]
+            Zb[-1] += Zw[s].sum(axis=0)  # every wake row = TE + s_r u_dir (uvlm.py:662-689)
+            Zb += _avg4_T(cbar, zb[s].shape)
+            Zb += _normals_T(zb[s], ncbar)
+            zeta0_bar[s] += _frames_T(Zb, None, hg0, None, uv.dof_mapping[s])
 
 
 def twist_jacobian(m, n, chord, ea, ctrl_y, span_y, twist, camber=0.0):

@@ -7,6 +7,7 @@ from __future__ import annotations
 
 import numpy as np
 
+from flapjax_b200 import cases
 from flapjax_b200.adjoint import PrescribedAdjoint
 from oracle import uvlm_ref as R
 from oracle.uvlm_vjp import bs_vjp
@@ -31,6 +32,7 @@ class _Seg:
             setattr(self, k, getattr(case, k))
         self.force_total = sum(fs.sum(axis=(1, 2)) + fu.sum(axis=(1, 2))
                                for fs, fu in zip(case.f_steady, case.f_unsteady))
+        self.t = case.t
         self._case = case
 
     def __getitem__(self, i):
@@ -89,12 +91,12 @@ class OracleDev:
             gb.append(Gb)
         return tb.reshape(targets.shape), zb, gb
 
-    def solve_t(self, zeta_b, zeta_w_static, rhs):
-        c = R.compute_surf_c(zeta_b)
-        nc = R.compute_surf_nc(zeta_b)
-        a = R.compute_aic_solve([c], [nc], [zeta_b], None if zeta_w_static is None else [zeta_w_static],
+    def solve_t(self, zetas_b, zetas_w_static, rhs):
+        cs = [R.compute_surf_c(z) for z in zetas_b]
+        ns = [R.compute_surf_nc(z) for z in zetas_b]
+        a = R.compute_aic_solve(cs, ns, list(zetas_b), None if zetas_w_static is None else list(zetas_w_static),
                                 self.kernel, self.mirror, self.r_cut)
-        return np.linalg.solve(a.T, rhs.ravel()).reshape(rhs.shape)
+        return np.linalg.solve(a.T, np.ravel(rhs)).reshape(np.shape(rhs))
 
 
 class OracleAdjoint(PrescribedAdjoint):
@@ -153,3 +155,30 @@ def coefficient_weights(case, which):
     fw = np.zeros((case.n_tstep, 3))
     fw[1:] = e / (q * case.n_steps)
     return fw
+
+
+def two_surface_case(free_wake=False, n_steps=3):
+    """A 3 x 4 heaving wing and a 2 x 2 tail 3 chords behind it on their own nodes (the
+    layout of the two-surface golden case), as (surfaces, hg0, hg_t, hg_dot_t, wing)."""
+    wing = (cases.wing_free(m=3, n=4, m_star=4, n_steps=n_steps, seed=1) if free_wake
+            else cases.wing_heave(m=3, n=4, m_star=4, n_steps=n_steps))
+    tail = np.zeros((3, 3, 3))
+    tail[..., 0] = (np.linspace(0.0, 0.5, 3) - 0.125)[:, None] + 3.0
+    tail[..., 2] = 0.2
+    hg_tail = np.zeros((3, 4, 4))
+    hg_tail[:, :3, :3] = np.eye(3)
+    hg_tail[:, 1, 3] = np.linspace(0.0, 1.5, 3)
+    hg_tail[:, 3, 3] = 1.0
+    hg0 = np.concatenate([wing.hg0, hg_tail])
+    hg_t = np.concatenate([wing.hg_t, np.repeat(hg_tail[None], wing.hg_t.shape[0], 0)], axis=1)
+    hg_dot_t = np.concatenate([wing.hg_dot_t, np.zeros((wing.hg_t.shape[0], 3, 4, 4))], axis=1)
+    surfs = [(3, 4, 4, np.asarray(wing.zeta_b0, float), np.arange(5)), (2, 2, 3, tail, np.arange(5, 8))]
+    return surfs, hg0, hg_t, hg_dot_t, wing
+
+
+def two_surface_oracle(surfs, hg0, wing, zetas=None):
+    uv = R.UVLMRef([(m, n, ms) for m, n, ms, _, _ in surfs], [d for *_, d in surfs], kernel=wing.kernel,
+                   r_cut=wing.r_cut, free_wake=wing.free_wake)
+    uv.set_design_variables(wing.dt, R.Constant(wing.u_inf, wing.rho, True),
+                            [z for *_, z, _ in surfs] if zetas is None else zetas, hg0)
+    return uv

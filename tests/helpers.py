@@ -15,25 +15,29 @@ def rel_err(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-def oracle_uvlm(case: cases.WingCase, mirror=None, **kw):
+def oracle_uvlm(case: cases.WingCase, mirror=None, gust=None, **kw):
+    """``gust``: keyword arguments of a OneMinusCosine flow (gust_length, gust_amplitude,
+    ...) in place of the Constant one."""
     from oracle import uvlm_ref as R
 
     mp, mn = (None, None) if mirror is None else mirror
     uv = R.UVLMRef([(case.m, case.n, case.m_star)], np.arange(case.n + 1), mirror_point=mp, mirror_normal=mn,
                    kernel=case.kernel, r_cut=case.r_cut, free_wake=case.free_wake, **kw)
-    ff = R.Constant(case.u_inf, case.rho, True)
+    ff = R.Constant(case.u_inf, case.rho, True) if gust is None else R.OneMinusCosine(case.u_inf, case.rho, True,
+                                                                                     **gust)
     uv.set_design_variables(case.dt, ff, case.zeta_b0, case.hg0)
     return uv, ff
 
 
-def device_uvlm(case: cases.WingCase, precision="fp64", mirror=None, **kw):
+def device_uvlm(case: cases.WingCase, precision="fp64", mirror=None, gust=None, **kw):
     import flapjax_b200 as fj
 
     kernel = fj.cutoff_kernel(case.r_cut) if case.kernel == "cutoff" else fj.biot_savart_epsilon
     mp, mn = (None, None) if mirror is None else mirror
     uv = fj.UVLM([fj.GridDiscretisation(case.m, case.n, case.m_star)], np.arange(case.n + 1), kernel=kernel,
                  free_wake=case.free_wake, precision=precision, mirror_point=mp, mirror_normal=mn, **kw)
-    ff = fj.Constant(case.u_inf, case.rho, True)
+    ff = fj.Constant(case.u_inf, case.rho, True) if gust is None else fj.OneMinusCosine(case.u_inf, case.rho, True,
+                                                                                       **gust)
     uv.set_design_variables(dt=case.dt, flowfield=ff, zeta_b0=case.zeta_b0, hg0=case.hg0)
     return uv, ff
 
