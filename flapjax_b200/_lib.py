@@ -71,6 +71,8 @@ class FjCaseConfig(C.Structure):
         ("flow", FjFlowfield),
         ("precision", C.c_int),
         ("variable_wake", _I8),
+        ("polar_points", _I8),
+        ("polar_circulation_scale", C.c_double),
     ]
 
 
@@ -97,6 +99,7 @@ class FjCaseBuffers(C.Structure):
         ("d_f_unsteady", _P),
         ("d_alpha", _P),
         ("d_force_total", _P),
+        ("d_polars", _P),
     ]
 
 

@@ -294,6 +294,8 @@ class PrescribedAdjoint:
             raise NotImplementedError("the adjoint is written for the epsilon and cutoff kernels")
         if uvlm.precision != "fp64":
             raise NotImplementedError("the adjoint runs in FP64")
+        if any(p is not None for p in getattr(uvlm, "polars", ())):
+            raise NotImplementedError("the adjoint does not differentiate the polar correction")
         self.uv = uvlm
         mirror = None if uvlm.mirror_point is None else (uvlm.mirror_point, uvlm.mirror_normal)
         self.d = _Dev(device, uvlm.kernel.kernel_id, uvlm.kernel.r_cut, mirror)

@@ -48,6 +48,9 @@ struct Layout {
     int var[FJ_MAX_SURF];          // 1: variable wake discretisation (delta_w)
     int any_var;
     int n_nodes;                   // beam nodes in the frame arrays
+    int pp[FJ_MAX_SURF];           // polar table points per strip (0: no polar correction)
+    int64_t plo[FJ_MAX_SURF + 1];  // polar tables: doubles before surface s (n * pp * 4 each)
+    int any_polar;
 };
 
 static Layout make_layout(const fj_case_config& c) {
@@ -75,6 +78,9 @@ static Layout make_layout(const fj_case_config& c) {
         L.dwo[s + 1] = L.dwo[s] + ms;
         L.xvo[s + 1] = L.xvo[s] + (var ? (int64_t)(ms + 2) * (n + 1) : 0);
         L.xpo[s + 1] = L.xpo[s] + (var ? (int64_t)(ms + 1) * n : 0);
+        L.pp[s] = c.polar_points[s];
+        L.plo[s + 1] = L.plo[s] + (int64_t)n * c.polar_points[s] * 4;
+        L.any_polar |= c.polar_points[s] > 0 ? 1 : 0;
     }
     return L;
 }
@@ -144,6 +150,9 @@ struct StepCase {
     const double* zeta_ref; // mixed path: lattice of the cached AIC (null: no comparison)
     int* changed;           // mixed path: set to 1 when zb_n differs from zeta_ref
     int* nonfinite;         // lowest slot whose total force is not finite (sentinel: none)
+    const double* polars;   // polar tables (Layout::plo blocks; null: no polar correction)
+    double* polar_tmp;      // per strip: sectional force (3), couple (3), lift scale
+    double polar_scale;     // polar_circulation_scale
 };
 
 __global__ void k_time(const StepCase* __restrict__ T) {
@@ -574,7 +583,8 @@ __global__ void k_gamma_dot(const StepCase* __restrict__ T) {
 
 // split_to_vertex of the filament forces (aero/utils.py:220-222) and of
 // rho * gamma_dot * n (uvlm.py:1093-1103), algebra/array_utils.py:332-367.
-__global__ void k_vertex_forces(const StepCase* __restrict__ T) {
+// parts: 1 the steady forces, 2 the unsteady ones, 3 both.
+__global__ void k_vertex_forces(const StepCase* __restrict__ T, int parts) {
     const StepCase& C = T[blockIdx.y];
     const Layout& L = C.L;
     const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -586,7 +596,7 @@ __global__ void k_vertex_forces(const StepCase* __restrict__ T) {
     const double* fc = C.ffil + L.fo[s] * 3;                          // (m, n+1, 3)
     const double* fsp = C.ffil + (L.fo[s] + (int64_t)m * (n + 1)) * 3;  // (m+1, n, 3)
     const double rho = C.flow.rho;
-    for (int d = 0; d < 3; ++d) {
+    for (int d = 0; d < 3 && (parts & 1); ++d) {
         double a = 0.0;  // split_to_vertex(f_chordwise, 0)
         if (k < m) a = 0.5 * fc[((int64_t)k * (n + 1) + l) * 3 + d];
         if (k >= 1) a += 0.5 * fc[((int64_t)(k - 1) * (n + 1) + l) * 3 + d];
@@ -596,7 +606,7 @@ __global__ void k_vertex_forces(const StepCase* __restrict__ T) {
         C.fs[v * 3 + d] = a + b;
     }
     const bool has_gd = C.gbd_nm1 != nullptr;
-    for (int d = 0; d < 3; ++d) {
+    for (int d = 0; d < 3 && (parts & 2); ++d) {
         double out = 0.0;
         if (has_gd) {
             const double* g = C.gbd_n + L.po[s];
@@ -659,6 +669,133 @@ __global__ void k_strip_alpha(const StepCase* __restrict__ T) {
     C.alpha[j] = cl / (2.0 * kPi);
 }
 
+// apply_polar_correction (aero/utils.py:276-397), per strip of a surface with polars:
+// strip frame (e_c, e_s, e_n), freestream at the strip centre, polar(alpha) by linear
+// interpolation in the strip's table with the end values held (np.interp), the lift
+// scale cl / (2 pi alpha), the sectional force q c b (cl e_l + cd e_d) and couple
+// q c b cm e_n into polar_tmp.
+__device__ __forceinline__ void polar_lookup(const double* tab, int np_, double a, double out[3]) {
+    // tab: np_ rows of (alpha, cl, cd, cm), alpha ascending
+    if (!(a > tab[0])) {  // below the table (and NaN, which np.interp maps to the end too)
+        for (int q = 0; q < 3; ++q) out[q] = tab[1 + q];
+        if (a != a)
+            for (int q = 0; q < 3; ++q) out[q] = a;
+        return;
+    }
+    if (a >= tab[(int64_t)(np_ - 1) * 4]) {
+        for (int q = 0; q < 3; ++q) out[q] = tab[(int64_t)(np_ - 1) * 4 + 1 + q];
+        return;
+    }
+    int lo = 0, hi = np_ - 1;  // tab[lo].alpha <= a < tab[hi].alpha
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (tab[(int64_t)mid * 4] <= a) lo = mid;
+        else hi = mid;
+    }
+    const double* r0 = tab + (int64_t)lo * 4;
+    const double* r1 = tab + (int64_t)hi * 4;
+    for (int q = 0; q < 3; ++q) {
+        const double slope = (r1[1 + q] - r0[1 + q]) / (r1[0] - r0[0]);
+        out[q] = r0[1 + q] + slope * (a - r0[0]);
+    }
+}
+
+__global__ void k_polar_strips(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    const Layout& L = C.L;
+    if (C.polars == nullptr) return;
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= L.so[L.n_surf]) return;
+    const int s = find_surf(L.so, L.n_surf, j);
+    if (L.pp[s] == 0) return;
+    const double t = C.t[C.i];
+    const int l = (int)(j - L.so[s]);
+    const int m = L.m[s], n = L.n[s];
+    const double* z = C.zb_n + L.vo[s] * 3;
+    const double* le0 = z + (int64_t)l * 3;
+    const double* le1 = le0 + 3;
+    const double* te0 = z + ((int64_t)m * (n + 1) + l) * 3;
+    const double* te1 = te0 + 3;
+    double le[3], te[3], chord[3], span[3], mid[3];
+    for (int d = 0; d < 3; ++d) {
+        le[d] = 0.5 * (le0[d] + le1[d]);
+        te[d] = 0.5 * (te0[d] + te1[d]);
+        chord[d] = te[d] - le[d];
+        span[d] = 0.5 * ((le1[d] + te1[d]) - (le0[d] + te0[d]));
+        mid[d] = 0.5 * (le[d] + te[d]);
+    }
+    const double c_len = sqrt(chord[0] * chord[0] + chord[1] * chord[1] + chord[2] * chord[2]);
+    const double b_len = sqrt(span[0] * span[0] + span[1] * span[1] + span[2] * span[2]);
+    const double ec[3] = {chord[0] / c_len, chord[1] / c_len, chord[2] / c_len};
+    const double es[3] = {span[0] / b_len, span[1] / b_len, span[2] / b_len};
+    double en[3] = {ec[1] * es[2] - ec[2] * es[1], ec[2] * es[0] - ec[0] * es[2], ec[0] * es[1] - ec[1] * es[0]};
+    const double enn = sqrt(en[0] * en[0] + en[1] * en[1] + en[2] * en[2]);
+    for (int d = 0; d < 3; ++d) en[d] /= enn;
+    double vr[3];
+    flow_eval(C.flow, mid, t, vr);
+    const double vmag2 = vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2];
+    const double vmag = sqrt(vmag2);
+    const double q = 0.5 * C.flow.rho * vmag2;
+    double el[3] = {vr[1] * es[2] - vr[2] * es[1], vr[2] * es[0] - vr[0] * es[2], vr[0] * es[1] - vr[1] * es[0]};
+    const double eln = sqrt(el[0] * el[0] + el[1] * el[1] + el[2] * el[2]);
+    for (int d = 0; d < 3; ++d) el[d] /= eln;
+    const double ed[3] = {vr[0] / vmag, vr[1] / vmag, vr[2] / vmag};
+    const double a = C.alpha[j];
+    double cf[3];
+    polar_lookup(C.polars + L.plo[s] + (int64_t)l * L.pp[s] * 4, L.pp[s], a, cf);
+    const double cl_uvlm = 2.0 * kPi * a;
+    const double qcb = q * c_len * b_len;
+    double* o = C.polar_tmp + j * 7;
+    for (int d = 0; d < 3; ++d) {
+        o[d] = qcb * (cf[0] * el[d] + cf[1] * ed[d]);
+        o[3 + d] = (qcb * cf[2]) * en[d];
+    }
+    o[6] = fabs(cl_uvlm) > kEps ? cf[0] / cl_uvlm : 1.0;
+}
+
+// The corrected steady forces of a surface with polars, one thread per vertex: the
+// sectional force at c/4 by the triangular chordwise weights, half to each of the strip's
+// two vertex columns, and the couple as opposing leading/trailing-edge forces.
+__global__ void k_polar_vertices(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    const Layout& L = C.L;
+    if (C.polars == nullptr) return;
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= L.vo[L.n_surf]) return;
+    const int s = find_surf(L.vo, L.n_surf, v);
+    if (L.pp[s] == 0) return;
+    const int64_t lv = v - L.vo[s];
+    const int m = L.m[s], n = L.n[s];
+    const int k = (int)(lv / (n + 1)), l = (int)(lv % (n + 1));
+    const double frac = (double)k / (double)m;  // linspace(0, 1, m + 1)
+    const double w = fmin(fmax(1.0 - fabs(frac - 0.25) * m, 0.0), 1.0);
+    double f[3] = {0.0, 0.0, 0.0};
+    for (int sj = l - 1; sj <= l; ++sj) {
+        if (sj < 0 || sj >= n) continue;
+        const double* o = C.polar_tmp + (L.so[s] + sj) * 7;
+        for (int d = 0; d < 3; ++d) {
+            f[d] += 0.5 * w * o[d];
+            if (k == 0) f[d] += 0.5 * o[3 + d];
+            if (k == m) f[d] -= 0.5 * o[3 + d];
+        }
+    }
+    for (int d = 0; d < 3; ++d) C.fs[v * 3 + d] = f[d];
+}
+
+// Blend Gamma_b towards the polar lift: gamma *= 1 + scale (lift_scale - 1) per strip
+// (uvlm.py:1066-1075).
+__global__ void k_polar_gamma(const StepCase* __restrict__ T) {
+    const StepCase& C = T[blockIdx.y];
+    const Layout& L = C.L;
+    if (C.polars == nullptr || C.polar_scale == 0.0) return;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= L.po[L.n_surf]) return;
+    const int s = find_surf(L.po, L.n_surf, p);
+    if (L.pp[s] == 0) return;
+    const int l = (int)((p - L.po[s]) % L.n[s]);
+    C.gb_n[p] *= 1.0 + C.polar_scale * (C.polar_tmp[(L.so[s] + l) * 7 + 6] - 1.0);
+}
+
 // Sum over vertices of f_steady + f_unsteady (one CTA per case, fixed order).
 __global__ void k_force_total(const StepCase* __restrict__ T) {
     const StepCase& C = T[blockIdx.y];
@@ -719,6 +856,7 @@ struct Plan {
     double* r;
     double* resid;       // per-slot refinement residual (mixed)
     double* ffil;
+    double* polar_tmp;   // polar correction: 7 doubles per strip (null without polars)
     char* tab;           // device table of a one-case step
     size_t tab_bytes;
     char* tab_all;       // graph-replayed steps: the table of every slot (n_tstep x tab_bytes)
@@ -735,6 +873,10 @@ static int validate(const fj_case_config* c) {
     for (int s = 0; s < c->n_surf; ++s)
         if (c->variable_wake[s] != 0 && c->variable_wake[s] != 1)
             return fail(FJ_ERR_SHAPE, "variable_wake[%d]=%d must be 0 or 1", s, c->variable_wake[s]);
+    for (int s = 0; s < c->n_surf; ++s)
+        if (c->polar_points[s] < 0) return fail(FJ_ERR_SHAPE, "polar_points[%d]=%d", s, c->polar_points[s]);
+    if (!(c->polar_circulation_scale >= 0.0 && c->polar_circulation_scale <= 1.0))
+        return fail(FJ_ERR_SHAPE, "polar_circulation_scale=%g not in [0, 1]", c->polar_circulation_scale);
     if (c->n_tstep < 1) return fail(FJ_ERR_SHAPE, "n_tstep=%d", c->n_tstep);
     if (c->n_nodes < 1) return fail(FJ_ERR_SHAPE, "n_nodes=%d", c->n_nodes);
     if (!(c->dt > 0.0) || !std::isfinite(c->dt)) return fail(FJ_ERR_SHAPE, "dt=%g must be positive", c->dt);
@@ -849,6 +991,7 @@ static int make_plan(const fj_case_config* cfg, void* ws, size_t ws_bytes, Plan&
     p.r = a.carve<double>(p.nb);
     p.resid = a.carve<double>(cfg->n_tstep);
     p.ffil = a.carve<double>(L.fo[ns] * 3);
+    p.polar_tmp = L.any_polar ? a.carve<double>(L.so[ns] * 7) : nullptr;
     p.tab_bytes = table_layout(1).total;
     p.tab = a.carve<char>(p.tab_bytes);
     p.tab_all = a.carve<char>((size_t)cfg->n_tstep * p.tab_bytes);
@@ -1048,6 +1191,9 @@ static int run_static(const Plan& p, const fj_case_buffers* B, const double* hg,
     C.ffil = p.ffil;
     C.rhs = p.rhs;
     C.nonfinite = p.flags + 2;
+    C.polars = L.any_polar ? B->d_polars : nullptr;
+    C.polar_tmp = p.polar_tmp;
+    C.polar_scale = c.polar_circulation_scale;
     const TableLayout tl = table_layout(1);
     StepCase* dC = (StepCase*)(p.tab + tl.step);
     FJ_TRY(upload(dC, &C, sizeof(C), s));
@@ -1088,8 +1234,16 @@ static int run_static(const Plan& p, const fj_case_buffers* B, const double* hg,
     k_force_targets<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(dC); note_launch();
     FJ_TRY(vind_sum(p, p.targets, L.fo[L.n_surf], sb.len(), sb.n_links, p.v, s));
     k_force_filament<<<nblk(L.fo[L.n_surf]), 256, 0, s>>>(dC); note_launch();
-    k_vertex_forces<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(dC); note_launch();
+    k_vertex_forces<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(dC, 3); note_launch();
     k_strip_alpha<<<nblk(p.sz_strip), 256, 0, s>>>(dC); note_launch();
+    if (L.any_polar) {  // uvlm.py:1055-1075: forces, then the circulations and the static wake
+        k_polar_strips<<<nblk(p.sz_strip), 256, 0, s>>>(dC); note_launch();
+        k_polar_vertices<<<nblk(L.vo[L.n_surf]), 256, 0, s>>>(dC); note_launch();
+        if (c.polar_circulation_scale != 0.0) {
+            k_polar_gamma<<<nblk(p.sz_pan), 256, 0, s>>>(dC); note_launch();
+            static_gamma_w_kernel<<<nblk(p.sz_gw + 1), 256, 0, s>>>(L, gb, gw, -1); note_launch();
+        }
+    }
     FJ_CUDA(cudaMemsetAsync(B->d_gamma_b_dot, 0, p.sz_pan * sizeof(double), s));
     k_force_total<<<1, 256, 0, s>>>(dC); note_launch();
     FJ_LAUNCH_CHECK("static solve");
@@ -1168,7 +1322,7 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
     std::vector<RefineJob> ref;
     std::vector<int> free_idx;
     int64_t max_v = 0, max_p = 0, max_w = 0, max_wt = 0, max_f = 0, max_e_free = 0, max_e_wake = 0, max_e_bound = 0;
-    int max_n = 0, max_fil = 0, any_mirror = 0, any_free = 0, any_changed = 0, any_var = 0;
+    int max_n = 0, max_fil = 0, any_mirror = 0, any_free = 0, any_changed = 0, any_var = 0, any_polar = 0;
     int64_t max_xw = 0, max_cols = 0;
     for (int k = 0; k < K; ++k) {
         BatchItem& it = items[k];
@@ -1233,6 +1387,10 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
         max_cols = std::max(max_cols, L.dofo[L.n_surf]);
         C.zeta_ref = (mixed && !it.refactor) ? p.zeta_ref : nullptr;
         C.changed = (mixed && !it.refactor) ? p.flags + 1 : nullptr;
+        C.polars = L.any_polar ? B->d_polars : nullptr;
+        C.polar_tmp = p.polar_tmp;
+        C.polar_scale = c.polar_circulation_scale;
+        any_polar |= L.any_polar;
         any_changed |= C.changed != nullptr;
         max_v = std::max(max_v, L.vo[L.n_surf]);
         max_p = std::max(max_p, L.po[L.n_surf]);
@@ -1401,11 +1559,28 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
     FJ_TRY(launch_sum(jfo, cfo, d_tab + tl.job_force, d_tab + tl.cta_force, precision, kernel, r_cut, s));
     k_force_filament<<<dim3(nblk(max_f), K), b, 0, s>>>(dC); note_launch();
     // 7. gamma_dot, vertex forces, strip alpha, totals
-    k_gamma_dot<<<dim3(nblk(max_n), K), b, 0, s>>>(dC); note_launch();
-    k_vertex_forces<<<dim3(nblk(max_v), K), b, 0, s>>>(dC); note_launch();
-    int64_t max_strip = 0;
-    for (const BatchItem& it : items) max_strip = std::max(max_strip, it.p.sz_strip);
-    k_strip_alpha<<<dim3(nblk(max_strip), K), b, 0, s>>>(dC); note_launch();
+    if (!any_polar) {
+        k_gamma_dot<<<dim3(nblk(max_n), K), b, 0, s>>>(dC); note_launch();
+        k_vertex_forces<<<dim3(nblk(max_v), K), b, 0, s>>>(dC, 3); note_launch();
+    } else {
+        // uvlm.py:1055-1103: steady forces and strip alpha from the solved Gamma, the polar
+        // forces and circulation blend, then gamma_dot and the unsteady forces from the
+        // blended Gamma (the same kernels; a case without polars skips the polar ones)
+        int64_t max_s = 0;
+        for (const BatchItem& it : items) max_s = std::max(max_s, it.p.sz_strip);
+        k_vertex_forces<<<dim3(nblk(max_v), K), b, 0, s>>>(dC, 1); note_launch();
+        k_strip_alpha<<<dim3(nblk(max_s), K), b, 0, s>>>(dC); note_launch();
+        k_polar_strips<<<dim3(nblk(max_s), K), b, 0, s>>>(dC); note_launch();
+        k_polar_vertices<<<dim3(nblk(max_v), K), b, 0, s>>>(dC); note_launch();
+        k_polar_gamma<<<dim3(nblk(max_n), K), b, 0, s>>>(dC); note_launch();
+        k_gamma_dot<<<dim3(nblk(max_n), K), b, 0, s>>>(dC); note_launch();
+        k_vertex_forces<<<dim3(nblk(max_v), K), b, 0, s>>>(dC, 2); note_launch();
+    }
+    if (!any_polar) {
+        int64_t max_strip = 0;
+        for (const BatchItem& it : items) max_strip = std::max(max_strip, it.p.sz_strip);
+        k_strip_alpha<<<dim3(nblk(max_strip), K), b, 0, s>>>(dC); note_launch();
+    }
     k_force_total<<<dim3(1, K), b, 0, s>>>(dC); note_launch();
     FJ_LAUNCH_CHECK("step: forces");
     return FJ_OK;
@@ -1438,6 +1613,7 @@ static int check_buffers(const Plan& p, const fj_case_buffers* B, bool dynamic) 
     // gamma_w has no entries when no surface has a wake (m_star = 0 everywhere)
     if (!B->d_gamma_w && p.sz_gw > 0) return fail(FJ_ERR_SHAPE, "d_gamma_w is NULL");
     if (dynamic && (!B->d_hg_t || !B->d_hg_dot_t)) return fail(FJ_ERR_SHAPE, "hg_t / hg_dot_t are NULL");
+    if (p.L.any_polar && !B->d_polars) return fail(FJ_ERR_SHAPE, "polar_points set but d_polars is NULL");
     return FJ_OK;
 }
 

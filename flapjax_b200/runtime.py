@@ -84,7 +84,7 @@ class DeviceCase:
     """Outputs, inputs and workspace of one case on one GPU."""
 
     def __init__(self, cfg: _lib.FjCaseConfig, layout: SurfaceLayout, zeta_b0: np.ndarray, dof_mapping: np.ndarray,
-                 device=None, stream=None, delta_w: np.ndarray | None = None):
+                 device=None, stream=None, delta_w: np.ndarray | None = None, polars: np.ndarray | None = None):
         import torch
 
         self.torch = torch
@@ -104,6 +104,8 @@ class DeviceCase:
         self.dof = torch.from_numpy(np.ascontiguousarray(dof_mapping, dtype=np.int32)).to(self.dev)
         self.delta_w = None if delta_w is None else torch.from_numpy(
             np.ascontiguousarray(delta_w, dtype=np.float64)).to(self.dev)
+        self.polars = None if polars is None else torch.from_numpy(
+            np.ascontiguousarray(polars, dtype=np.float64)).to(self.dev)
         self.hg_t = torch.zeros((self.n_tstep, cfg.n_nodes, 4, 4), **f64)
         self.hg_dot_t = torch.zeros((self.n_tstep, cfg.n_nodes, 4, 4), **f64)
         nbytes = C.c_size_t()
@@ -122,6 +124,7 @@ class DeviceCase:
         for name in FIELDS:
             setattr(b, "d_" + name, self.arrays[name].data_ptr())
         b.d_force_total = self.force_total.data_ptr()
+        b.d_polars = None if self.polars is None else self.polars.data_ptr()
         return b
 
     def _stream(self):

@@ -21,6 +21,7 @@ from . import _lib
 from .data_structures import AeroCase, ArrayList, GridDiscretisation
 from .flowfields import FlowField
 from .kernels import resolve
+from .polars import pack_surface, tabulate
 from .runtime import DeviceCase, SurfaceLayout
 
 HORSESHOE_LENGTH = 1e3  # utils/constants.py:13
@@ -110,10 +111,16 @@ class UVLM:
             self.dof_mapping.append(arr.astype(np.int32))
         if grid_func is not None:
             raise NotImplementedError("control surfaces (grid_func) are not part of the CUDA path")
-        if polars is not None and any(p is not None for p in polars):
-            raise NotImplementedError("polar corrections are not part of the CUDA path")
+        # uvlm.py:294-303: per surface None or n strip polars (tables on the device)
+        if polars is None:
+            self.polars = tuple([None] * self.n_surf)
+        else:
+            if len(polars) != self.n_surf:
+                raise ValueError(f"Expected {self.n_surf} polar entries, got {len(polars)}")
+            self.polars = tuple(None if p is None else tuple(tabulate(f) for f in p) for p in polars)
         if not 0.0 <= polar_circulation_scale <= 1.0:
             raise ValueError(f"polar_circulation_scale must be in [0, 1], got {polar_circulation_scale}.")
+        self.polar_circulation_scale = float(polar_circulation_scale)
         if (mirror_point is None) != (mirror_normal is None):
             raise ValueError("Both mirror_point and mirror_normal must be provided to apply mirroring, or both must be "
                              "None to apply no mirroring.")
@@ -241,7 +248,18 @@ class UVLM:
         c.precision = _PREC[self.precision]
         for i, dw in enumerate(self.delta_w or []):
             c.variable_wake[i] = int(dw is not None)
+        for i, (P, _) in enumerate(self._polar_blocks()):
+            c.polar_points[i] = P
+        c.polar_circulation_scale = self.polar_circulation_scale
         return c
+
+    def _polar_blocks(self):
+        """(points per strip, table block) per surface; (0, None) without polars."""
+        return [(0, None) if p is None else pack_surface(p, gd.n) for p, gd in zip(self.polars, self.grid_disc)]
+
+    def _polars_flat(self):
+        blocks = [b for P, b in self._polar_blocks() if P > 0]
+        return None if not blocks else np.concatenate([b.ravel() for b in blocks])
 
     def _delta_w_flat(self):
         """Concatenated delta_w of every surface (zeros where a surface is uniform), or
@@ -265,7 +283,7 @@ class UVLM:
         zeta0 = np.concatenate([z.ravel() for z in self.zeta_b0])
         dof = np.concatenate([d.ravel() for d in self.dof_mapping])
         return DeviceCase(self._config(n_tstep, n_nodes), self._layout(), zeta0, dof, self.device, stream,
-                          delta_w=self._delta_w_flat())
+                          delta_w=self._delta_w_flat(), polars=self._polars_flat())
 
     def _to_case(self, dc: DeviceCase, slots=None, snapshot=False) -> AeroCase:
         h = dc.host_arrays(slots)

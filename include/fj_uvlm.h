@@ -96,6 +96,11 @@ typedef struct fj_case_config {
     /* 1: surface s uses the variable wake discretisation (propagate_surf_wake with
      * delta_w, aero/utils.py:452-491): its segment lengths are d_delta_w's block */
     int variable_wake[FJ_MAX_SURF];
+    /* polar correction (apply_polar_correction, aero/utils.py:276-397, applied as
+     * uvlm.py:1055-1075): table points per strip of surface s in d_polars, 0 = none */
+    int polar_points[FJ_MAX_SURF];
+    /* 0..1: Gamma_b (and a static solve's Gamma_w) blended towards the polar lift scale */
+    double polar_circulation_scale;
 } fj_case_config;
 
 /* Device buffers of one case.  Surfaces are concatenated in the innermost extent of
@@ -124,6 +129,10 @@ typedef struct fj_case_buffers {
     double* d_f_unsteady;      /* (m+1, n+1, 3) */
     double* d_alpha;           /* (n,) strip angle of attack */
     double* d_force_total;     /* (3,) per slot: sum over vertices of f_steady+f_unsteady */
+    /* polar tables of the surfaces with polar_points > 0, in surface order: per strip
+     * polar_points rows of (alpha, cl, cd, cm), alpha ascending (linear interpolation,
+     * end values held outside); NULL when no surface has polars */
+    const double* d_polars;
 } fj_case_buffers;
 
 /* ---------------------------------------------------------------------------------

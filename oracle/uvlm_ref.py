@@ -515,6 +515,77 @@ def strip_alpha(zeta_b, f_steady, v_func, rho):
     return alphas
 
 
+def apply_polar_correction(zeta_b, f_steady, v_func, rho, polars, alpha):
+    """``apply_polar_correction`` aero/utils.py:276-397: per strip of a surface with polars,
+    the sectional force q c b (cl e_l + cd e_d) placed at c/4 by triangular chordwise
+    weights and split onto the strip's two vertex columns, plus the couple q c b cm e_n as
+    opposing leading/trailing-edge forces; cl, cd, cm = polar(alpha).  Returns the corrected
+    steady forces and the per-strip lift scale cl / (2 pi alpha) (1 where |2 pi alpha| <=
+    EPSILON)."""
+    f_out, scale_out = [], []
+    for zs, fs, pol, al in zip(zeta_b, f_steady, polars, alpha):
+        n = zs.shape[1] - 1
+        if pol is None:
+            f_out.append(fs)
+            scale_out.append(np.ones(n, REAL))
+            continue
+        m = zs.shape[0] - 1
+        if len(pol) != n:
+            raise ValueError(f"Expected {n} polar callables, got {len(pol)}")
+        zle, zte = zs[0], zs[-1]
+        le_j = 0.5 * (zle[:-1] + zle[1:])
+        te_j = 0.5 * (zte[:-1] + zte[1:])
+        chord = te_j - le_j
+        c_len = np.linalg.norm(chord, axis=-1)
+        e_c = chord / c_len[:, None]
+        span_vec = 0.5 * ((zle[1:] + zte[1:]) - (zle[:-1] + zte[:-1]))
+        b_len = np.linalg.norm(span_vec, axis=-1)
+        e_s = span_vec / b_len[:, None]
+        e_n = np.cross(e_c, e_s)
+        e_n = e_n / np.linalg.norm(e_n, axis=-1, keepdims=True)
+        v_ref = v_func(0.5 * (le_j + te_j))
+        v_mag2 = np.sum(v_ref * v_ref, axis=-1)
+        v_mag = np.sqrt(v_mag2)
+        q = 0.5 * rho * v_mag2
+        e_l = np.cross(v_ref, e_s)
+        e_l = e_l / np.linalg.norm(e_l, axis=-1, keepdims=True)
+        e_d = v_ref / v_mag[:, None]
+        coeffs = [pol[j](al[j]) for j in range(n)]
+        cl_p = np.array([cf[0] for cf in coeffs], REAL)
+        cd_p = np.array([cf[1] for cf in coeffs], REAL)
+        cm_p = np.array([cf[2] for cf in coeffs], REAL)
+        cl_uvlm = 2.0 * np.pi * al
+        with np.errstate(divide="ignore", invalid="ignore"):
+            scale_out.append(np.where(np.abs(cl_uvlm) > EPSILON, cl_p / cl_uvlm, 1.0))
+        qcb = q * c_len * b_len
+        f_lump = qcb[:, None] * (cl_p[:, None] * e_l + cd_p[:, None] * e_d)
+        f_couple = (qcb * cm_p)[:, None] * e_n
+        w_chord = np.clip(1.0 - np.abs(np.linspace(0.0, 1.0, m + 1) - 0.25) * m, 0.0, 1.0)
+        fc = np.zeros_like(fs)
+        lump = 0.5 * w_chord[:, None, None] * f_lump[None]
+        fc[:, :-1] += lump
+        fc[:, 1:] += lump
+        cp = 0.5 * f_couple
+        fc[0, :-1] += cp
+        fc[0, 1:] += cp
+        fc[-1, :-1] -= cp
+        fc[-1, 1:] -= cp
+        f_out.append(fc)
+    return f_out, scale_out
+
+
+class TabulatedPolar:
+    """A strip polar from tables: alpha (ascending, rad) -> (cl, cd, cm) by linear
+    interpolation with the end values held outside the table (np.interp)."""
+
+    def __init__(self, alpha, cl, cd, cm):
+        self.alpha = np.asarray(alpha, float)
+        self.cl, self.cd, self.cm = (np.asarray(v, float) for v in (cl, cd, cm))
+
+    def __call__(self, a):
+        return tuple(_interp(np.asarray(a).reshape(1), self.alpha, v)[0] for v in (self.cl, self.cd, self.cm))
+
+
 def se3_vect_product(hg, x):
     """``se3.vect_product`` algebra/se3.py:209-216 for hg (..., 4, 4), x (..., 3)."""
     return np.einsum("...ij,...j->...i", hg[..., :3, :3], x) + hg[..., :3, 3]
@@ -553,11 +624,11 @@ class Case:
 
 class UVLMRef:
     """FP64 restatement of ``UVLM`` aero/uvlm.py:80-1406 for the configurations the CUDA
-    path supports (no control surfaces, no polar correction)."""
+    path supports (no control surfaces)."""
 
     def __init__(self, grid_shapes, dof_mapping, mirror_point=None, mirror_normal=None,
                  kernel=KERNEL_EPSILON, r_cut=R_CUTOFF, free_wake=False,
-                 gamma_dot_relaxation=0.7, variable_wake_disc=False):
+                 gamma_dot_relaxation=0.7, variable_wake_disc=False, polars=None, polar_circulation_scale=0.0):
         self.grid_disc = [g if isinstance(g, GridDiscretisation) else GridDiscretisation(*g)
                           for g in grid_shapes]
         self.n_surf = len(self.grid_disc)
@@ -574,6 +645,14 @@ class UVLMRef:
         self.free_wake = free_wake
         self.gamma_dot_relaxation = gamma_dot_relaxation
         self.variable_wake_disc = variable_wake_disc
+        # uvlm.py:294-303: per surface None or a sequence of n strip polars
+        if polars is None:
+            self.polars = [None] * self.n_surf
+        else:
+            if len(polars) != self.n_surf:
+                raise ValueError(f"Expected {self.n_surf} polar entries, got {len(polars)}")
+            self.polars = [None if p is None else list(p) for p in polars]
+        self.polar_circulation_scale = float(polar_circulation_scale)
 
     # uvlm.py:387-472
     def set_design_variables(self, dt, flowfield, zeta_b0, hg0, delta_w=None):
@@ -683,6 +762,15 @@ class UVLMRef:
 
         f_steady = calculate_steady_forcing(zeta_b_n, zdf, gamma_b_n, gamma_w_n, ff.rho, v_total)
         alpha_n = strip_alpha(zeta_b_n, f_steady, lambda x_: ff(x_, t_n), ff.rho)
+        if any(p is not None for p in self.polars):  # uvlm.py:1055-1075
+            f_steady, lift_scale = apply_polar_correction(zeta_b_n, f_steady, lambda x_: ff(x_, t_n), ff.rho,
+                                                          self.polars, alpha_n)
+            if self.polar_circulation_scale != 0.0:
+                sc = self.polar_circulation_scale
+                gamma_b_n = [gb * (1.0 + sc * (ls[None, :] - 1.0)) for gb, ls in zip(gamma_b_n, lift_scale)]
+                if static:
+                    gamma_w_n = [np.broadcast_to(gb[[-1], ...], gw.shape).copy()
+                                 for gb, gw in zip(gamma_b_n, gamma_w_n)]
         if static:
             gamma_b_dot_n = None
             f_unsteady = None
