@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--adjoint", action="store_true",
                     help="config 3: twist gradient of time-mean CL and CD by the hand-written adjoint")
     ap.add_argument("--adjoint-steps", type=int, default=1000)
+    ap.add_argument("--residual", action="store_true",
+                    help="only the time-step residual VJP (timestep_residual, config-3 wing) on the device")
     ap.add_argument("--factor", action="store_true",
                     help="only the factorisation leg (mixed solve's FP32 LU + inverse, tensor cores vs CUDA cores)")
     ap.add_argument("--configs", action="store_true",
@@ -325,6 +327,10 @@ def main():
         if rank == 0:
             print(json.dumps({"adjoint": adjoint_bench(args, torch)}))
         return 0
+    if args.residual:
+        if rank == 0:
+            print(json.dumps({"residual_vjp": residual_bench(torch)}))
+        return 0
     if args.factor:
         case = workload(args, 2)
         _, dcf = make_case(case, "mixed", 2)
@@ -536,6 +542,39 @@ def factor_bench(dc, case, torch):
                    "tf32_peak_tflops": tf32_peak, "frac": achieved / tf32_peak,
                    "peak_source": "half of MEASURED_PEAKS.json bf16_tflops (dense TF32 runs at half the bf16 rate)"}
     return out
+
+
+def residual_bench(torch):
+    """Device time of one residual VJP (AeroResidual.vjp: the residual of the reference's
+    timestep_residual and the cotangents of all its inputs) on the config-3 wing (12 x 64,
+    W = 100, prescribed pitch) at slot 2, wall clock around the call (host algebra, transfers
+    and device work), after one warm-up call."""
+    import flapjax_b200 as fj
+    from flapjax_b200 import cases
+    from flapjax_b200.residual import AeroResidual
+
+    c = cases.wing_pitch(m=12, n=64, m_star=100, n_steps=3)
+    uv = fj.UVLM([fj.GridDiscretisation(c.m, c.n, c.m_star)], np.arange(c.n + 1), kernel=fj.biot_savart_epsilon,
+                 precision="fp64")
+    uv.set_design_variables(dt=c.dt, flowfield=fj.Constant(c.u_inf, c.rho, True), zeta_b0=c.zeta_b0, hg0=c.hg0)
+    out = uv.solve_prescribed_dynamic(uv.solve_static(), c.hg_t, c.hg_dot_t)
+    keys = ("gamma_b", "gamma_w", "gamma_b_dot", "zeta_w")
+    q = lambda i: {k: [np.array(a[i]) for a in getattr(out, k)] for k in keys}
+    ar = AeroResidual(uv)
+    rng = np.random.default_rng(0)
+    fb = rng.normal(size=(c.hg0.shape[0], 6))
+    rbar = rng.normal(size=AeroResidual.ravel(q(2)).size + fb.size)
+    args = (float(out.t[2]), c.hg_t[2], c.hg_dot_t[2], c.hg_t[1], q(2), q(1), fb, rbar)
+    ar.vjp(*args)
+    times = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r, _ = ar.vjp(*args)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    return {"workload": "config-3 wing 12x64, W=100, epsilon kernel, slot 2", "residual_size": int(r.size),
+            "ms_per_vjp": 1e3 * float(np.median(times))}
 
 
 def measured_peaks():

@@ -128,6 +128,34 @@ class _Dev:
                   self.stream())
         return b.cpu().numpy().reshape(rhs.shape)
 
+    def solve_pair(self, zetas_b, rhs, rhs_t):
+        """(x, mu) with A x = rhs and A^T mu = rhs_t, A the dynamic AIC of the bound
+        lattices zetas_b, from one factorisation."""
+        k = len(zetas_b)
+        ms = [z.shape[0] - 1 for z in zetas_b]
+        ns = [z.shape[1] - 1 for z in zetas_b]
+        nb = sum(m * n for m, n in zip(ms, ns))
+        tz = [self.t(z) for z in zetas_b]
+        zp = (C.c_void_p * k)(*[z.data_ptr() for z in tz])
+        mm, nn = (C.c_int * k)(*ms), (C.c_int * k)(*ns)
+        a = self.torch.empty((nb, nb), dtype=self.torch.float64, device=self.dev)
+        w = C.c_size_t()
+        _lib.call("fj_aic_workspace_size", mm, nn, k, C.byref(w))
+        ws = self.ws("aic", w.value)
+        s = self.stream()
+        mp, mn = self._mir if self._mir is not None else (None, None)
+        _lib.call("fj_aic_assemble", zp, mm, nn, k, None, (C.c_int * k)(*([0] * k)), mp, mn, self.kernel, self.r_cut,
+                  a.data_ptr(), ws.data_ptr(), ws.numel(), s)
+        piv = self.torch.empty(nb, dtype=self.torch.int32, device=self.dev)
+        _lib.call("fj_lu_workspace_size", nb, C.byref(w))
+        wl = self.ws("lu", w.value)
+        _lib.call("fj_lu_factor", a.data_ptr(), nb, piv.data_ptr(), wl.data_ptr(), wl.numel(), s)
+        x = self.t(np.ravel(rhs))
+        _lib.call("fj_lu_solve", a.data_ptr(), nb, piv.data_ptr(), x.data_ptr(), wl.data_ptr(), wl.numel(), s)
+        mu = self.t(np.ravel(rhs_t))
+        _lib.call("fj_lu_solve_t", a.data_ptr(), nb, piv.data_ptr(), mu.data_ptr(), wl.data_ptr(), wl.numel(), s)
+        return x.cpu().numpy(), mu.cpu().numpy()
+
     def solve_t(self, zetas_b, zetas_w_static, rhs):
         """mu with A^T mu = rhs (flat, all surfaces), A the AIC of the bound lattices
         zetas_b (with each surface's wake lumped onto its TE column when zetas_w_static is

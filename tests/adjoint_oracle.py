@@ -91,6 +91,12 @@ class OracleDev:
             gb.append(Gb)
         return tb.reshape(targets.shape), zb, gb
 
+    def solve_pair(self, zetas_b, rhs, rhs_t):
+        cs = [R.compute_surf_c(z) for z in zetas_b]
+        ns = [R.compute_surf_nc(z) for z in zetas_b]
+        a = R.compute_aic_solve(cs, ns, list(zetas_b), None, self.kernel, self.mirror, self.r_cut)
+        return R._solve(a, np.ravel(rhs)), np.linalg.solve(a.T, np.ravel(rhs_t))
+
     def solve_t(self, zetas_b, zetas_w_static, rhs):
         cs = [R.compute_surf_c(z) for z in zetas_b]
         ns = [R.compute_surf_nc(z) for z in zetas_b]
