@@ -91,9 +91,12 @@ def _flow_dict(kind, u_inf, rho, gust=None):
 
 
 def run_case(ref, name, surfaces, dt, flow, kernel="epsilon", r_cut=None, free_wake=False, mirror=None,
-             horseshoe=False, gamma_dot_relaxation=0.7, hg0=None, hg_t=None, hg_dot_t=None, delta_w=None):
+             horseshoe=False, gamma_dot_relaxation=0.7, hg0=None, hg_t=None, hg_dot_t=None, delta_w=None,
+             polars=None, polar_circulation_scale=0.0):
     """surfaces: list of (m, n, m_star, zeta_b0, dof_mapping); delta_w: per-surface segment
-    lengths (or None entries) of the variable wake discretisation."""
+    lengths (or None entries) of the variable wake discretisation; polars: per-surface
+    (n, P, 4) tables of (alpha, cl, cd, cm) (or None entries), handed to the reference as
+    jnp.interp callables."""
     if ONLY and name not in ONLY:
         return
     jnp = ref.jnp
@@ -106,6 +109,12 @@ def run_case(ref, name, surfaces, dt, flow, kernel="epsilon", r_cut=None, free_w
         kw = {}
         if mirror is not None:
             kw = dict(mirror_point=jnp.array(mirror[0]), mirror_normal=jnp.array(mirror[1]))
+        if polars is not None:
+            def _callable(tab):
+                return lambda a: tuple(jnp.interp(a, tab[:, 0], tab[:, q]) for q in (1, 2, 3))
+
+            kw["polars"] = [None if p is None else [_callable(np.asarray(t, float)) for t in p] for p in polars]
+            kw["polar_circulation_scale"] = polar_circulation_scale
         uv = ref.UVLM(grid_shapes=[ref.GridDiscretisation(m, n, ms) for m, n, ms, _, _ in surfaces],
                       dof_mapping=[jnp.array(d) for *_, d in surfaces], kernel=kern, free_wake=free_wake,
                       gamma_dot_relaxation=gamma_dot_relaxation, **kw)
@@ -128,6 +137,11 @@ def run_case(ref, name, surfaces, dt, flow, kernel="epsilon", r_cut=None, free_w
             out[f"surf{i}_dims"] = np.array([m, n, ms])
             out[f"surf{i}_zeta_b0"] = z
             out[f"surf{i}_dof"] = np.asarray(d)
+        if polars is not None:
+            out["polar_circulation_scale"] = float(polar_circulation_scale)
+            for i, p in enumerate(polars):
+                if p is not None:
+                    out[f"surf{i}_polars"] = np.asarray(p, float)
         if mirror is not None:
             out["mirror_point"] = np.asarray(mirror[0], float)
             out["mirror_normal"] = np.asarray(mirror[1], float)
@@ -212,6 +226,18 @@ def main():
     dw = c.dt * c.u_mag * 1.15 ** np.arange(c.m_star)
     run_case(ref, "variable_wake_heave", [(c.m, c.n, c.m_star, c.zeta_b0, np.arange(c.n + 1))], c.dt,
              _flow_dict("constant", c.u_inf, c.rho), hg0=c.hg0, hg_t=c.hg_t, hg_dot_t=c.hg_dot_t, delta_w=[dw])
+    # polar correction (aero/utils.py:276-397): per-strip tables, circulation blend 0.5
+    c = cases.wing_heave(m=3, n=4, m_star=4, n_steps=3)
+    rng = np.random.default_rng(5)
+    tabs = []
+    for _ in range(c.n):
+        al = np.sort(rng.uniform(-0.2, 0.3, 7))
+        tabs.append(np.stack([al, 5.5 * al + rng.normal(0, 0.05, 7), 0.01 + 0.3 * al ** 2,
+                              -0.04 + 0.02 * rng.normal(size=7)], axis=1))
+    run_case(ref, "polar_heave", [(c.m, c.n, c.m_star, c.zeta_b0, np.arange(c.n + 1))], c.dt,
+             _flow_dict("constant", c.u_inf, c.rho), hg0=c.hg0, hg_t=c.hg_t, hg_dot_t=c.hg_dot_t,
+             polars=[np.stack(tabs)], polar_circulation_scale=0.5)
+
     c = cases.wing_free(m=2, n=4, m_star=5, n_steps=4)
     dw = c.dt * c.u_mag * 1.2 ** np.arange(c.m_star)
     run_case(ref, "variable_wake_free", [(c.m, c.n, c.m_star, c.zeta_b0, np.arange(c.n + 1))], c.dt,

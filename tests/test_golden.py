@@ -45,6 +45,19 @@ def _delta_w(fx):
     return None if all(d is None for d in dws) else dws
 
 
+def _polars(fx, make):
+    """Per-surface strip polars from the fixture's tables (None where a surface has none),
+    built with ``make(alpha, cl, cd, cm)``; (polars, circulation scale)."""
+    n_surf = int(fx["n_surf"])
+    if not any(f"surf{i}_polars" in fx for i in range(n_surf)):
+        return None, 0.0
+    out = []
+    for i in range(n_surf):
+        t = fx.get(f"surf{i}_polars")
+        out.append(None if t is None else [make(r[:, 0], r[:, 1], r[:, 2], r[:, 3]) for r in t])
+    return out, float(fx["polar_circulation_scale"])
+
+
 def _mirror(fx):
     return (fx["mirror_point"], fx["mirror_normal"]) if "mirror_point" in fx else (None, None)
 
@@ -68,9 +81,11 @@ def test_oracle_matches_reference_golden(name):
     fx = load(name)
     surfs = _surfaces(fx)
     mp, mn = _mirror(fx)
+    pol, pscale = _polars(fx, R.TabulatedPolar)
     uv = R.UVLMRef([(m, n, ms) for m, n, ms, _, _ in surfs], [d for *_, d in surfs], mirror_point=mp,
                    mirror_normal=mn, kernel=str(fx["kernel"]), r_cut=float(fx["r_cut"]),
-                   free_wake=bool(fx["free_wake"]), gamma_dot_relaxation=float(fx["gamma_dot_relaxation"]))
+                   free_wake=bool(fx["free_wake"]), gamma_dot_relaxation=float(fx["gamma_dot_relaxation"]),
+                   polars=pol, polar_circulation_scale=pscale)
     uv.set_design_variables(float(fx["dt"]), _flow(fx, R), [z for *_, z, _ in surfs], fx["hg0"],
                             delta_w=_delta_w(fx))
     st = uv.solve_static(horseshoe=bool(fx["horseshoe"]))
@@ -95,9 +110,11 @@ def test_cuda_matches_reference_golden(cuda, name, precision):
     mp, mn = _mirror(fx)
     kernel = {"epsilon": fj.biot_savart_epsilon, "plain": fj.biot_savart,
               "cutoff": fj.cutoff_kernel(float(fx["r_cut"]))}[str(fx["kernel"])]
+    pol, pscale = _polars(fx, fj.TabulatedPolar)
     uv = fj.UVLM([fj.GridDiscretisation(m, n, ms) for m, n, ms, _, _ in surfs], [d for *_, d in surfs],
                  mirror_point=mp, mirror_normal=mn, kernel=kernel, free_wake=bool(fx["free_wake"]),
-                 gamma_dot_relaxation=float(fx["gamma_dot_relaxation"]), precision=precision)
+                 gamma_dot_relaxation=float(fx["gamma_dot_relaxation"]), precision=precision, polars=pol,
+                 polar_circulation_scale=pscale)
     uv.set_design_variables(dt=float(fx["dt"]), flowfield=_flow(fx, fj), zeta_b0=[z for *_, z, _ in surfs],
                             hg0=fx["hg0"], delta_w=_delta_w(fx))
     tol_b = 1e-10 if precision == "fp64" else 1e-5
