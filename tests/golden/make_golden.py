@@ -163,6 +163,78 @@ def run_case(ref, name, surfaces, dt, flow, kernel="epsilon", r_cut=None, free_w
         ref.utils.R_CUTOFF = saved_r
 
 
+def run_residual_case(ref, name, c, free_wake=False, kernel="epsilon", r_cut=None, gust=None, slot=2, seed=0):
+    """The reference's own UVLM.timestep_residual (aero/uvlm.py:1942-2047) at slot ``slot``
+    of a prescribed run, with the states of slot n moved off the solution by seeded noise
+    and seeded beam forces.  The beam is not part of this path: a stand-in structure
+    object hands the residual the run's node frames for varphi_n / varphi_nm1 (told apart
+    by their fill value) and the frame velocities for v_n; the design variables carry no
+    overrides and no control surfaces."""
+    if ONLY and name not in ONLY:
+        return
+    jnp = ref.jnp
+    from flapjax.algebra.array_utils import ArrayList
+
+    kern = {"epsilon": ref.utils.biot_savart_epsilon, "cutoff": ref.utils.biot_savart_cutoff}[kernel]
+    saved_r = ref.utils.R_CUTOFF
+    if r_cut is not None:
+        ref.utils.R_CUTOFF = r_cut
+    try:
+        uv = ref.UVLM(grid_shapes=[ref.GridDiscretisation(c.m, c.n, c.m_star)], dof_mapping=[jnp.arange(c.n + 1)],
+                      kernel=kern, free_wake=free_wake)
+        if gust is None:
+            ff = ref.Constant(jnp.array(c.u_inf), c.rho, True)
+        else:
+            ff = ref.OneMinusCosine(jnp.array(c.u_inf), c.rho, True, gust_length=gust["length"],
+                                    gust_amplitude=gust["amplitude"], gust_x0=jnp.array(gust["x0"]))
+        uv.set_design_variables(dt=float(c.dt), flowfield=ff, zeta_b0=[jnp.array(c.zeta_b0)], hg0=jnp.array(c.hg0))
+        st = uv.solve_static()
+        dy = uv.solve_prescribed_dynamic(init_case=st, hg_t=jnp.array(c.hg_t), hg_dot_t=jnp.array(c.hg_dot_t))
+        rng = np.random.default_rng(seed)
+        keys = ("gamma_b", "gamma_w", "gamma_b_dot", "zeta_w")
+        qn = {k: np.asarray(getattr(dy, k)[0][slot]) + 0.01 * rng.normal(size=np.shape(getattr(dy, k)[0][slot]))
+              for k in keys}
+        qm = {k: np.asarray(getattr(dy, k)[0][slot - 1]) for k in keys}
+        n_nodes = c.hg0.shape[0]
+        f_beam = rng.normal(size=(n_nodes, 6))
+        frames = {1.0: np.asarray(c.hg_t[slot]), 2.0: np.asarray(c.hg_t[slot - 1])}
+
+        class _Beam:
+            n_dof = n_nodes * 6
+
+            def case_from_dv(self, dv):
+                return self
+
+            def calculate_hg_from_varphi(self, varphi):
+                return jnp.array(frames[float(np.asarray(varphi).ravel()[0])])
+
+            def make_hg_dot(self, hg, v):
+                return jnp.array(c.hg_dot_t[slot])
+
+        aero_dv = types.SimpleNamespace(flowfield=None, cs_ang_t=None, zeta_b0=None,
+                                        get_cs_n=lambda i_ts, dv_full: ({}, {}))
+        dv = types.SimpleNamespace(structure=None, aero=aero_dv)
+        to_states = lambda q: types.SimpleNamespace(**{k: ArrayList([jnp.array(q[k])]) for k in keys})
+        r = uv.timestep_residual(i_ts=slot, varphi_nm1=jnp.full((n_nodes, 6), 2.0),
+                                 varphi_n=jnp.full((n_nodes, 6), 1.0), v_n=jnp.zeros((n_nodes, 6)),
+                                 t_n=dy.t[slot], q_n=to_states(qn), q_nm1=to_states(qm), dv=dv, dv_full=dv,
+                                 f_aero_beam_n=jnp.array(f_beam), struct_obj=_Beam(), approx_grads=False)
+        out = {"case_name": name, "kernel": kernel, "r_cut": r_cut if r_cut is not None else saved_r,
+               "free_wake": free_wake, "dt": c.dt, "u_inf": c.u_inf, "rho": c.rho, "zeta_b0": c.zeta_b0,
+               "hg0": c.hg0, "hg_n": c.hg_t[slot], "hg_dot_n": c.hg_dot_t[slot], "hg_nm1": c.hg_t[slot - 1],
+               "t_n": np.asarray(dy.t[slot]), "f_beam_n": f_beam, "dims": np.array([c.m, c.n, c.m_star]),
+               "residual": np.asarray(r)}
+        if gust is not None:
+            out.update(gust_length=gust["length"], gust_amplitude=gust["amplitude"], gust_x0=np.asarray(gust["x0"]))
+        for k in keys:
+            out[f"q_n_{k}"] = qn[k]
+            out[f"q_nm1_{k}"] = qm[k]
+        np.savez_compressed(HERE / "residual" / f"{name}.npz", **{k: np.asarray(v) for k, v in out.items()})
+        print("wrote residual", name)
+    finally:
+        ref.utils.R_CUTOFF = saved_r
+
+
 ONLY: set[str] = set()
 
 
@@ -243,6 +315,16 @@ def main():
     run_case(ref, "variable_wake_free", [(c.m, c.n, c.m_star, c.zeta_b0, np.arange(c.n + 1))], c.dt,
              _flow_dict("constant", c.u_inf, c.rho), free_wake=True, hg0=c.hg0, hg_t=c.hg_t, hg_dot_t=c.hg_dot_t,
              delta_w=[dw])
+
+
+    # the time-step residual of the coupled adjoint (aero side)
+    (HERE / "residual").mkdir(exist_ok=True)
+    c = cases.wing_heave(m=3, n=4, m_star=4, n_steps=3)
+    run_residual_case(ref, "residual_heave", c)
+    c = cases.wing_free(m=3, n=4, m_star=4, n_steps=3, seed=1)
+    run_residual_case(ref, "residual_free_cutoff", c, free_wake=True, kernel="cutoff", r_cut=1e-3)
+    run_residual_case(ref, "residual_free_gust", c, free_wake=True, kernel="cutoff", r_cut=1e-3,
+                      gust={"length": 2.0, "amplitude": 0.1, "x0": [-3.0, 0.0, 0.0]})
 
 
 if __name__ == "__main__":
