@@ -235,6 +235,55 @@ def run_residual_case(ref, name, c, free_wake=False, kernel="epsilon", r_cut=Non
         ref.utils.R_CUTOFF = saved_r
 
 
+def run_gradient_case(ref, name, c, free_wake=False, kernel="epsilon", r_cut=None, gust=None, delta_w=None,
+                      n_dir=2, h=1e-6, seed=0):
+    """Directional derivatives of the reference's own forward: J(zeta_b0) = time-mean CL over
+    steps 1..N (sum_n fw_n . F_n, F_n the total vertex force of UVLM.solve_prescribed_dynamic
+    from the static solve), and (J(z + h d) - J(z - h d)) / 2h for ``n_dir`` seeded unit-scale
+    directions d.  With h = 1e-6 in float64 the truncation error is O(h^2) and the rounding
+    error about 1e-16 |J| / h, both far below the 1e-6 the adjoint is held to."""
+    if ONLY and name not in ONLY:
+        return
+    jnp = ref.jnp
+    kern = {"epsilon": ref.utils.biot_savart_epsilon, "cutoff": ref.utils.biot_savart_cutoff}[kernel]
+    saved_r = ref.utils.R_CUTOFF
+    if r_cut is not None:
+        ref.utils.R_CUTOFF = r_cut
+    a = np.deg2rad(c.alpha_deg)
+    e_l = np.array((-np.sin(a), 0.0, np.cos(a)))
+    q = 0.5 * c.rho * c.u_mag ** 2 * c.s_ref
+
+    def objective(z0):
+        uv = ref.UVLM(grid_shapes=[ref.GridDiscretisation(c.m, c.n, c.m_star)], dof_mapping=[jnp.arange(c.n + 1)],
+                      kernel=kern, free_wake=free_wake)
+        ff = (ref.Constant(jnp.array(c.u_inf), c.rho, True) if gust is None else
+              ref.OneMinusCosine(jnp.array(c.u_inf), c.rho, True, gust_length=gust["length"],
+                                 gust_amplitude=gust["amplitude"], gust_x0=jnp.array(gust["x0"])))
+        uv.set_design_variables(dt=float(c.dt), flowfield=ff, zeta_b0=[jnp.array(z0)], hg0=jnp.array(c.hg0),
+                                delta_w=None if delta_w is None else [jnp.array(delta_w)])
+        dy = uv.solve_prescribed_dynamic(init_case=uv.solve_static(), hg_t=jnp.array(c.hg_t),
+                                         hg_dot_t=jnp.array(c.hg_dot_t))
+        ft = np.asarray(dy.f_steady[0]).sum(axis=(1, 2)) + np.asarray(dy.f_unsteady[0]).sum(axis=(1, 2))
+        return float(np.sum(ft[1:] @ e_l) / (q * c.n_steps))
+
+    try:
+        z0 = np.asarray(c.zeta_b0, float)
+        rng = np.random.default_rng(seed)
+        dirs = rng.normal(size=(n_dir,) + z0.shape) * 0.1
+        J = objective(z0)
+        dJ = np.array([(objective(z0 + h * d) - objective(z0 - h * d)) / (2 * h) for d in dirs])
+        out = {"case_name": name, "kernel": kernel, "r_cut": r_cut if r_cut is not None else saved_r,
+               "free_wake": free_wake, "J": J, "dJ": dJ, "directions": dirs, "h": h}
+        if gust is not None:
+            out.update(gust_length=gust["length"], gust_amplitude=gust["amplitude"], gust_x0=np.asarray(gust["x0"]))
+        if delta_w is not None:
+            out["delta_w"] = np.asarray(delta_w, float)
+        np.savez_compressed(HERE / "gradient" / f"{name}.npz", **{k: np.asarray(v) for k, v in out.items()})
+        print("wrote gradient", name, J, dJ)
+    finally:
+        ref.utils.R_CUTOFF = saved_r
+
+
 ONLY: set[str] = set()
 
 
@@ -325,6 +374,17 @@ def main():
     run_residual_case(ref, "residual_free_cutoff", c, free_wake=True, kernel="cutoff", r_cut=1e-3)
     run_residual_case(ref, "residual_free_gust", c, free_wake=True, kernel="cutoff", r_cut=1e-3,
                       gust={"length": 2.0, "amplitude": 0.1, "x0": [-3.0, 0.0, 0.0]})
+
+
+    # directional derivatives of the reference's own forward, for the adjoint
+    (HERE / "gradient").mkdir(exist_ok=True)
+    run_gradient_case(ref, "gradient_pitch", cases.wing_pitch(m=3, n=4, m_star=4, n_steps=4, n_ctrl=3, seed=3))
+    c = cases.wing_free(m=3, n=4, m_star=4, n_steps=3, seed=1)
+    run_gradient_case(ref, "gradient_free_cutoff", c, free_wake=True, kernel="cutoff", r_cut=1e-3)
+    run_gradient_case(ref, "gradient_free_gust", c, free_wake=True, kernel="cutoff", r_cut=1e-3,
+                      gust={"length": 2.0, "amplitude": 0.1, "x0": [-3.0, 0.0, 0.0]})
+    c = cases.wing_pitch(m=3, n=4, m_star=5, n_steps=4, n_ctrl=3, seed=3)
+    run_gradient_case(ref, "gradient_pitch_delta_w", c, delta_w=c.dt * c.u_mag * 1.2 ** np.arange(c.m_star))
 
 
 if __name__ == "__main__":
