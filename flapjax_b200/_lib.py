@@ -191,6 +191,7 @@ _SIGS = {
     "fj_autotune_table_size": (C.c_int, [C.POINTER(C.c_int)]),
     "fj_autotune_get": (C.c_int, [_P, C.c_int]),
     "fj_autotune_set": (C.c_int, [_P, C.c_int]),
+    "fj_tc_wait_selftest": (C.c_int, [_P, _P, _P]),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         __syncthreads();
         // the next slab's loads are in flight while this slab's MMAs run
         if (ks + 1 < n_slab) load_slab(regs, a, lda, b, ldb, m, n, k, m0, n0, (ks + 1) * kBK);
-        if (threadIdx.x == 0) {
+        if (threadIdx.x == 0 && passes != 0) {  // passes = 0: the wait self-test issues nothing
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t sa = smem_u32(base), sb = smem_u32(base + 2 * kSlabBytes);
 #pragma unroll
@@ -380,6 +380,23 @@ int tri_inverse32_blocks(const float* lu, int n, int b0, int nb, bool upper, flo
 }
 
 }  // namespace fj
+
+// Failure-detection self-test: the GEMM kernel with its MMAs and commits withheld, so
+// that nothing ever completes the mbarrier it waits on.  Its bounded wait expires (about
+// a second), it records the failure, waits (bounded) once more, frees its tensor memory
+// and returns; the context stays usable.
+extern "C" int fj_tc_wait_selftest(int* d_err, float* d_scratch, fj_stream_t stream) {
+    if (!d_err || !d_scratch) return fj::fail(FJ_ERR_SHAPE, "tc_wait_selftest: null pointer");
+    float* buf = d_scratch;  // a, b, c of a 1 x 1 x 1 product
+    cudaStream_t s = (cudaStream_t)stream;
+    FJ_CUDA(cudaMemsetAsync(buf, 0, 4 * sizeof(float), s));
+    FJ_TRY(fj::allow_dynamic_smem((const void*)fj::tc_gemm_tf32_kernel, fj::kGemmSmem));
+    fj::tc_gemm_tf32_kernel<<<1, fj::kThreads, fj::kGemmSmem, s>>>(buf, 1, buf + 1, 1, buf + 2, 1, 1, 1, 1, 1.0f, 0.0f,
+                                                                   0, d_err);
+    fj::note_launch();
+    FJ_LAUNCH_CHECK("tc_gemm_tf32_kernel (wait self-test)");
+    return FJ_OK;
+}
 
 extern "C" int fj_gemm_tf32(const float* d_a, int lda, const float* d_b, int ldb, float* d_c, int ldc, int m, int n,
                             int k, float alpha, float beta, int passes, int* d_err, fj_stream_t stream) {

@@ -384,6 +384,13 @@ FJ_API int fj_solve_mixed(const double* d_a, int n, const double* d_b, double* d
 FJ_API int fj_gemm_tf32(const float* d_a, int lda, const float* d_b, int ldb, float* d_c, int ldc, int m, int n,
                         int k, float alpha, float beta, int passes, int* d_err, fj_stream_t stream);
 
+/* Failure-detection self-test of the tensor-core kernel's bounded waits: launches
+ * fj_gemm_tf32's kernel with its MMAs and commits withheld, so that the mbarrier it waits
+ * on never completes.  After about two seconds (the wait and a bounded drain) the kernel
+ * has set *d_err (device int) to 1, freed its tensor memory and returned; the context
+ * stays usable.  d_scratch: 4 device floats. */
+FJ_API int fj_tc_wait_selftest(int* d_err, float* d_scratch, fj_stream_t stream);
+
 /* Autotuner of the Biot-Savart sum launches (the reference's vmap/lax.map chunking,
  * aero/aic.py:47-63, 237-245, has no tunable).  A sum of n_targets points over a stream of
  * n_elem filament elements runs as target tiles x splits CTAs; for each shape this times

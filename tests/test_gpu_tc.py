@@ -162,3 +162,28 @@ def test_mixed_solve_of_an_aic(cuda):
     want = np.linalg.solve(a, b)
     x, r = _solve_mixed(cuda, a, b)
     assert r < 1e-12 and rel_err(x, want) < 1e-10
+
+
+def test_bounded_wait_expires_and_context_survives(cuda):
+    """Failure detection without a fault: the GEMM kernel with its MMAs withheld waits on
+    an mbarrier that nothing completes; the bounded wait gives up (about 2 s), the kernel
+    reports it in the status word and returns, and the next product is correct."""
+    import time
+
+    import torch
+
+    from flapjax_b200 import _lib
+
+    err = torch.zeros(1, dtype=torch.int32, device=cuda)
+    scratch = torch.zeros(4, dtype=torch.float32, device=cuda)
+    s = torch.cuda.current_stream(cuda).cuda_stream
+    t0 = time.perf_counter()
+    _lib.call("fj_tc_wait_selftest", err.data_ptr(), scratch.data_ptr(), s)
+    torch.cuda.synchronize()
+    assert int(err.cpu()) == 1
+    assert time.perf_counter() - t0 < 30.0
+    rng = np.random.default_rng(1)
+    a = rng.normal(size=(64, 32)).astype(np.float32)
+    b = rng.normal(size=(32, 48)).astype(np.float32)
+    got = _gemm(cuda, a, b, np.zeros((64, 48), np.float32), 64, 48, 32, 1.0, 0.0, 3)
+    assert rel_err(got, a.astype(np.float64) @ b.astype(np.float64)) < 5e-6
