@@ -257,11 +257,21 @@ static int lu_factor_impl(T* a, int n, int32_t* piv, int* d_info, cudaStream_t s
     return FJ_OK;
 }
 
+// Panel width: the widest whose (n x (NB + 1)) panel fits the shared-memory budget, so that
+// the largest validated AIC order (6144) factors too.
+template <typename T>
+static bool panel_fits(int n, int nb) {
+    return (size_t)n * (nb + 1) * sizeof(T) <= (size_t)220 * 1024;
+}
+
 int lu_factor64(double* a, int n, int32_t* piv, int* d_info, cudaStream_t s) {
-    return lu_factor_impl<double, 8>(a, n, piv, d_info, s);
+    if (panel_fits<double>(n, 8)) return lu_factor_impl<double, 8>(a, n, piv, d_info, s);
+    if (panel_fits<double>(n, 4)) return lu_factor_impl<double, 4>(a, n, piv, d_info, s);
+    return lu_factor_impl<double, 2>(a, n, piv, d_info, s);
 }
 int lu_factor32(float* a, int n, int32_t* piv, int* d_info, cudaStream_t s) {
-    return lu_factor_impl<float, 16>(a, n, piv, d_info, s);
+    if (panel_fits<float>(n, 16)) return lu_factor_impl<float, 16>(a, n, piv, d_info, s);
+    return lu_factor_impl<float, 8>(a, n, piv, d_info, s);
 }
 
 // ---------------------------------------------------------------------------------
@@ -478,9 +488,10 @@ size_t tc_tri_floats(int n) {
     return (size_t)2 * ((n + kTcBlk - 1) / kTcBlk) * kTcBlk * kTcBlk;
 }
 
-int lu_factor32_tc(float* a, int n, int32_t* piv, int* d_info, int* d_err, float* tri_l, int passes,
-                   cudaStream_t s) {
-    constexpr int NB = 16;
+template <int NB>
+static int lu_factor32_tc_impl(float* a, int n, int32_t* piv, int* d_info, int* d_err, float* tri_l, int passes,
+                               cudaStream_t s) {
+    static_assert(kTcBlk % NB == 0, "inner panels tile the outer one");
     if (n <= 0) return fail(FJ_ERR_SHAPE, "lu_factor: n=%d", n);
     const size_t smem = (size_t)n * (NB + 1) * sizeof(float);
     if (smem > 220 * 1024) return fail(FJ_ERR_UNSUPPORTED, "lu_factor: n=%d too large for the shared-memory panel", n);
@@ -515,6 +526,12 @@ int lu_factor32_tc(float* a, int n, int32_t* piv, int* d_info, int* d_err, float
     }
     FJ_LAUNCH_CHECK("lu_factor32_tc");
     return FJ_OK;
+}
+
+int lu_factor32_tc(float* a, int n, int32_t* piv, int* d_info, int* d_err, float* tri_l, int passes,
+                   cudaStream_t s) {
+    if (panel_fits<float>(n, 16)) return lu_factor32_tc_impl<16>(a, n, piv, d_info, d_err, tri_l, passes, s);
+    return lu_factor32_tc_impl<8>(a, n, piv, d_info, d_err, tri_l, passes, s);
 }
 
 // Y = P I: row i holds a one in column perm[i].  Y must be zero on entry.

@@ -187,3 +187,44 @@ def test_bounded_wait_expires_and_context_survives(cuda):
     b = rng.normal(size=(32, 48)).astype(np.float32)
     got = _gemm(cuda, a, b, np.zeros((64, 48), np.float32), 64, 48, 32, 1.0, 0.0, 3)
     assert rel_err(got, a.astype(np.float64) @ b.astype(np.float64)) < 5e-6
+
+
+@pytest.mark.parametrize("n", [3200, 6144])
+def test_largest_orders_factor(cuda, n):
+    """AIC orders up to the validated 6144: the FP64 LU (panel width 8, 4 or 2 by order)
+    and the mixed solve (inner panels 16 or 8) both factor and solve."""
+    import torch
+
+    from flapjax_b200 import _lib
+
+    rng = np.random.default_rng(n)
+    a = rng.normal(size=(n, n)) + n * 0.05 * np.eye(n)
+    b = rng.normal(size=n)
+    want = np.linalg.solve(a, b)
+    ta = torch.as_tensor(a).to(cuda)
+    piv = torch.empty(n, dtype=torch.int32, device=cuda)
+    nb_ = C.c_size_t()
+    _lib.call("fj_lu_workspace_size", n, C.byref(nb_))
+    ws = torch.empty(nb_.value, dtype=torch.uint8, device=cuda)
+    s = torch.cuda.current_stream(cuda).cuda_stream
+    _lib.call("fj_lu_factor", ta.data_ptr(), n, piv.data_ptr(), ws.data_ptr(), ws.numel(), s)
+    tb = torch.as_tensor(b).to(cuda)
+    _lib.call("fj_lu_solve", ta.data_ptr(), n, piv.data_ptr(), tb.data_ptr(), ws.data_ptr(), ws.numel(), s)
+    assert rel_err(tb.cpu().numpy(), want) < 1e-10
+    x, r = _solve_mixed(cuda, a, b)
+    assert r < 1e-12 and rel_err(x, want) < 1e-11
+
+
+def test_largest_wing_solves(cuda):
+    """A 16 x 384 wing (AIC order 6144, the largest accepted): static and dynamic steps in
+    FP64 and mixed agree."""
+    from flapjax_b200 import cases
+    from tests.helpers import device_uvlm
+
+    c = cases.wing_heave(m=16, n=384, m_star=4, n_steps=2, span=24.0)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        uv, _ = device_uvlm(c, prec)
+        out[prec] = uv.solve_prescribed_dynamic(uv.solve_static(), c.hg_t, c.hg_dot_t)
+    for i in range(c.n_tstep):
+        assert rel_err(out["mixed"].gamma_b[0][i], out["fp64"].gamma_b[0][i]) < 1e-5
