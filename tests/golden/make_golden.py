@@ -236,7 +236,7 @@ def run_residual_case(ref, name, c, free_wake=False, kernel="epsilon", r_cut=Non
 
 
 def run_gradient_case(ref, name, c, free_wake=False, kernel="epsilon", r_cut=None, gust=None, delta_w=None,
-                      n_dir=2, h=1e-6, seed=0):
+                      mirror=None, n_dir=2, h=1e-6, seed=0):
     """Directional derivatives of the reference's own forward: J(zeta_b0) = time-mean CL over
     steps 1..N (sum_n fw_n . F_n, F_n the total vertex force of UVLM.solve_prescribed_dynamic
     from the static solve), and (J(z + h d) - J(z - h d)) / 2h for ``n_dir`` seeded unit-scale
@@ -254,8 +254,9 @@ def run_gradient_case(ref, name, c, free_wake=False, kernel="epsilon", r_cut=Non
     q = 0.5 * c.rho * c.u_mag ** 2 * c.s_ref
 
     def objective(z0):
+        kw = {} if mirror is None else dict(mirror_point=jnp.array(mirror[0]), mirror_normal=jnp.array(mirror[1]))
         uv = ref.UVLM(grid_shapes=[ref.GridDiscretisation(c.m, c.n, c.m_star)], dof_mapping=[jnp.arange(c.n + 1)],
-                      kernel=kern, free_wake=free_wake)
+                      kernel=kern, free_wake=free_wake, **kw)
         ff = (ref.Constant(jnp.array(c.u_inf), c.rho, True) if gust is None else
               ref.OneMinusCosine(jnp.array(c.u_inf), c.rho, True, gust_length=gust["length"],
                                  gust_amplitude=gust["amplitude"], gust_x0=jnp.array(gust["x0"])))
@@ -278,6 +279,9 @@ def run_gradient_case(ref, name, c, free_wake=False, kernel="epsilon", r_cut=Non
             out.update(gust_length=gust["length"], gust_amplitude=gust["amplitude"], gust_x0=np.asarray(gust["x0"]))
         if delta_w is not None:
             out["delta_w"] = np.asarray(delta_w, float)
+        if mirror is not None:
+            out["mirror_point"] = np.asarray(mirror[0], float)
+            out["mirror_normal"] = np.asarray(mirror[1], float)
         np.savez_compressed(HERE / "gradient" / f"{name}.npz", **{k: np.asarray(v) for k, v in out.items()})
         print("wrote gradient", name, J, dJ)
     finally:
@@ -385,6 +389,9 @@ def main():
                       gust={"length": 2.0, "amplitude": 0.1, "x0": [-3.0, 0.0, 0.0]})
     c = cases.wing_pitch(m=3, n=4, m_star=5, n_steps=4, n_ctrl=3, seed=3)
     run_gradient_case(ref, "gradient_pitch_delta_w", c, delta_w=c.dt * c.u_mag * 1.2 ** np.arange(c.m_star))
+    c = cases.wing_free(m=3, n=4, m_star=4, n_steps=3, seed=1)
+    run_gradient_case(ref, "gradient_free_mirror", c, free_wake=True, kernel="cutoff", r_cut=1e-3,
+                      mirror=([0.0, 0.0, 0.0], [0.0, 1.0, 0.0]))
 
 
 if __name__ == "__main__":

@@ -24,6 +24,7 @@ _BUILD = {
     "gradient_free_cutoff": lambda: cases.wing_free(m=3, n=4, m_star=4, n_steps=3, seed=1),
     "gradient_free_gust": lambda: cases.wing_free(m=3, n=4, m_star=4, n_steps=3, seed=1),
     "gradient_pitch_delta_w": lambda: cases.wing_pitch(m=3, n=4, m_star=5, n_steps=4, n_ctrl=3, seed=3),
+    "gradient_free_mirror": lambda: cases.wing_free(m=3, n=4, m_star=4, n_steps=3, seed=1),
 }
 
 
@@ -43,17 +44,18 @@ def _setup(name):
         gust = dict(gust_length=float(fx["gust_length"]), gust_amplitude=float(fx["gust_amplitude"]),
                     gust_x0=fx["gust_x0"])
     dw = fx.get("delta_w")
-    return fx, c, gust, dw
+    mirror = (fx["mirror_point"], fx["mirror_normal"]) if "mirror_point" in fx else None
+    return fx, c, gust, dw, mirror
 
 
 def test_gradient_golden_cases_present():
-    assert len(CASES) >= 4
+    assert len(CASES) >= 5
 
 
 @pytest.mark.parametrize("name", CASES)
 def test_oracle_adjoint_matches_reference_differences(name):
-    fx, c, gust, dw = _setup(name)
-    uv, ff = oracle_uvlm(c, gust=gust)
+    fx, c, gust, dw, mirror = _setup(name)
+    uv, ff = oracle_uvlm(c, gust=gust, mirror=mirror)
     if dw is not None:
         uv.set_design_variables(c.dt, ff, c.zeta_b0, c.hg0, delta_w=[dw])
     J, g = OracleAdjoint(uv).gradient(c.hg_t, c.hg_dot_t, coefficient_weights(c, "CL"), checkpoint=2)
@@ -67,8 +69,8 @@ def test_oracle_adjoint_matches_reference_differences(name):
 def test_device_adjoint_matches_reference_differences(cuda, name):
     from flapjax_b200.adjoint import PrescribedAdjoint
 
-    fx, c, gust, dw = _setup(name)
-    uv, ff = device_uvlm(c, "fp64", gust=gust)
+    fx, c, gust, dw, mirror = _setup(name)
+    uv, ff = device_uvlm(c, "fp64", gust=gust, mirror=mirror)
     if dw is not None:
         uv.set_design_variables(dt=c.dt, flowfield=ff, zeta_b0=c.zeta_b0, hg0=c.hg0, delta_w=[dw])
     J, g = PrescribedAdjoint(uv, cuda).gradient(c.hg_t, c.hg_dot_t, coefficient_weights(c, "CL"), checkpoint=2)
