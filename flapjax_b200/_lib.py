@@ -174,6 +174,12 @@ _SIGS = {
                               C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, C.c_double, _P, _P,
                               C.POINTER(_P), C.POINTER(_P), _P, C.c_size_t, _P]),
     "fj_lu_solve_t": (C.c_int, [_P, C.c_int, _P, _P, _P, C.c_size_t, _P]),
+    "fj_ring_influence": (C.c_int, [_P, C.c_int64, _P, _P, C.c_int, C.c_int, C.POINTER(C.c_double),
+                                    C.POINTER(C.c_double), C.c_int, C.c_double, _P, C.c_int64, _P]),
+    "fj_vertex_jacobian": (C.c_int, [_P, C.c_int64, _P, _P, _P, C.c_int, C.c_int, C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double), C.c_int, C.c_double, _P, C.c_int64, _P]),
+    "fj_lu_solve_many_workspace_size": (C.c_int, [C.c_int, C.c_int64, C.POINTER(C.c_size_t)]),
+    "fj_lu_solve_many": (C.c_int, [_P, C.c_int, _P, _P, C.c_int64, C.c_int64, _P, C.c_size_t, _P]),
     "fj_aic_workspace_size": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_size_t)]),
     "fj_aic_assemble": (C.c_int, [C.POINTER(_P), C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.POINTER(_P),
                                   C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int,

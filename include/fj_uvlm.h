@@ -270,6 +270,32 @@ FJ_API int fj_vind_vjp(const double* d_targets, int64_t n_targets, const double*
                        double* const* d_zetas_bar, double* const* d_gammas_bar, void* d_ws,
                        size_t ws_bytes, fj_stream_t stream);
 
+/* Dense influence Jacobians of compute_v_ind (aero/aic.py:248-310) for one source lattice
+ * zeta (rows+1, cols+1, 3), for the linearised UVLM (aero/linear/linear_uvlm.py forms its
+ * state-space matrices by jax.jacrev of one step).  FP64, epsilon or cutoff kernel, the
+ * mirror image subtracted when mirror_point/mirror_normal are given.  Each writes a
+ * row-major block with leading dimension ld_out (overwritten, not accumulated):
+ *   fj_ring_influence:  d v(x_t) / d gamma_r, the velocity of unit circulation on ring
+ *     r = k*cols + l;  (n_targets, ld_out) projected on d_normals (n_targets, 3) when given,
+ *     else (3 n_targets, ld_out) with rows t*3 + {x, y, z};  ld_out >= rows*cols.
+ *   fj_vertex_jacobian: d v(x_t) / d zeta_v for circulations d_gamma (rows, cols), column
+ *     v*3 + {x, y, z} for vertex v = k*(cols+1) + l;  rows as above;  ld_out >= 3 vertices. */
+FJ_API int fj_ring_influence(const double* d_targets, int64_t n_targets, const double* d_normals,
+                             const double* d_zeta, int rows, int cols, const double* mirror_point,
+                             const double* mirror_normal, int kernel, double r_cut, double* d_out,
+                             int64_t ld_out, fj_stream_t stream);
+FJ_API int fj_vertex_jacobian(const double* d_targets, int64_t n_targets, const double* d_normals,
+                              const double* d_zeta, const double* d_gamma, int rows, int cols,
+                              const double* mirror_point, const double* mirror_normal, int kernel,
+                              double r_cut, double* d_out, int64_t ld_out, fj_stream_t stream);
+
+/* B <- A^-1 B for nrhs right-hand sides, the columns of the row-major (n, ldb) d_b, from the
+ * factors of fj_lu_factor (jax.scipy.linalg.lu_solve / jnp.linalg.solve with a matrix
+ * right-hand side, as the linear model's Jacobians need). */
+FJ_API int fj_lu_solve_many_workspace_size(int n, int64_t nrhs, size_t* bytes);
+FJ_API int fj_lu_solve_many(const double* d_lu, int n, const int32_t* d_piv, double* d_b, int64_t nrhs,
+                            int64_t ldb, void* d_ws, size_t ws_bytes, fj_stream_t stream);
+
 /* fj_vind without a caller workspace, for callers that cannot allocate device memory
  * (a plugin host that owns the device memory pool, a real-time loop that may not block in
  * cudaMalloc).  No counterpart in the reference.  Its scratch is a fixed 8 MiB array in

@@ -465,16 +465,22 @@ def propagate_surf_wake(gamma_b_nm1, gamma_w_nm1, zeta_b_n, zeta_w_nm1, delta_w,
     return zeta_w_n, gamma_w_n
 
 
-def calculate_steady_forcing(zeta_b, zeta_dot_b, gamma_b, gamma_w, rho, v_func):
-    """``calculate_steady_forcing`` aero/utils.py:126-223 for a list of surfaces."""
+def calculate_steady_forcing(zeta_b, zeta_dot_b, gamma_b, gamma_w, rho, v_func, v_inputs=None):
+    """``calculate_steady_forcing`` aero/utils.py:126-223 for a list of surfaces;
+    ``v_inputs`` (vertex velocities added at the filament midpoints, :179-181) is the
+    linear model's bound upwash."""
     out = []
-    for zb, zd, gb, gw in zip(zeta_b, zeta_dot_b, gamma_b, gamma_w):
+    v_in = v_inputs if v_inputs is not None else [None] * len(zeta_b)
+    for zb, zd, gb, gw, vi in zip(zeta_b, zeta_dot_b, gamma_b, gamma_w, v_in):
         mp_c = neighbour_average(zb, 0)
         mp_s = neighbour_average(zb, 1)
         mpd_c = neighbour_average(zd, 0)
         mpd_s = neighbour_average(zd, 1)
         v_rel_c = v_func(mp_c) - mpd_c
         v_rel_s = v_func(mp_s) - mpd_s
+        if vi is not None:
+            v_rel_c = v_rel_c + neighbour_average(vi, 0)
+            v_rel_s = v_rel_s + neighbour_average(vi, 1)
         g_c = np.zeros(v_rel_c.shape[:-1], REAL)
         g_c[:, :-1] = gb
         g_c[:, 1:] += -gb
@@ -710,9 +716,10 @@ class UVLMRef:
     def aic_solve(self, cs, ns, zetas_b, zetas_w):
         return compute_aic_solve(cs, ns, zetas_b, zetas_w, self.kernel, self.mirror, self.r_cut)
 
-    # uvlm.py:824-1117
+    # uvlm.py:824-1117; nu_b / nu_w are the linear model's bound and wake upwash inputs
+    # (uvlm.py:943-946, 979-981, and calculate_steady_forcing's v_inputs)
     def base_solve_from_grid(self, q_nm1, t_n, zeta_b_n, zeta_b_nm1, zeta_b_dot_n, static,
-                             horseshoe=False):
+                             horseshoe=False, nu_b=None, nu_w=None):
         ff = self.flowfield
         c_n = [compute_surf_c(z) for z in zeta_b_n]
         nc_n = [compute_surf_nc(z) for z in zeta_b_n]
@@ -740,12 +747,16 @@ class UVLMRef:
                                              self.delta_w[i], v_wake_prop, self.dt)
                 zeta_w_n.append(zw)
                 gamma_w_n.append(gw)
+            if nu_w is not None:
+                zeta_w_n = [zw + nw * self.dt for zw, nw in zip(zeta_w_n, nu_w)]
 
         aic = self.aic_solve(c_n, nc_n, zeta_b_n, zeta_w_n if static else None)
         v_bc = [ff(c, t_n) for c in c_n]
         if not static:
             v_bc = [v - cd for v, cd in zip(v_bc, c_dot_n)]
             v_bc = [v + self.v_ind(c, zeta_w_n, gamma_w_n) for v, c in zip(v_bc, c_n)]
+        if nu_b is not None:
+            v_bc = [v + compute_surf_c(nb) for v, nb in zip(v_bc, nu_b)]
         rhs = np.concatenate([np.einsum("ijk,ijk->ij", v, n).ravel() for v, n in zip(v_bc, nc_n)])
         gamma_vec = _solve(aic, -rhs)
         gamma_b_n, off = [], 0
@@ -760,7 +771,7 @@ class UVLMRef:
         def v_total(x_):
             return ff(x_, t_n) + self.v_ind(x_, [*zeta_b_n, *zeta_w_n], [*gamma_b_n, *gamma_w_n])
 
-        f_steady = calculate_steady_forcing(zeta_b_n, zdf, gamma_b_n, gamma_w_n, ff.rho, v_total)
+        f_steady = calculate_steady_forcing(zeta_b_n, zdf, gamma_b_n, gamma_w_n, ff.rho, v_total, nu_b)
         alpha_n = strip_alpha(zeta_b_n, f_steady, lambda x_: ff(x_, t_n), ff.rho)
         if any(p is not None for p in self.polars):  # uvlm.py:1055-1075
             f_steady, lift_scale = apply_polar_correction(zeta_b_n, f_steady, lambda x_: ff(x_, t_n), ff.rho,

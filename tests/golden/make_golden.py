@@ -288,6 +288,124 @@ def run_gradient_case(ref, name, c, free_wake=False, kernel="epsilon", r_cut=Non
         ref.utils.R_CUTOFF = saved_r
 
 
+def run_linear_case(ref, name, c, wake_type, free_wake=False, kernel="epsilon", r_cut=None, gust=None, mirror=None,
+                    n_run=6, h=1e-6, seed=0):
+    """The reference's own linearised UVLM (aero/linear/linear_uvlm.py) about the static
+    solution of case ``c``.  ``LinearUVLM.compute_jacobians`` supplies, per residual, the
+    step function, its arguments and the arguments it differentiates; jax.jacrev is
+    replaced by central differences of those same step functions (h = 1e-6 in float64:
+    truncation O(h^2), rounding about 1e-16 / h), and the blocks are assembled into A, B,
+    C, D by the reference's ``construct_named_block_jacobian`` in ``linearise``'s order.
+    The reference's ``LinearSystem.run`` then marches those matrices over ``n_run`` seeded
+    input perturbations.  Also stored: the step's packed outputs at the reference point
+    and at one seeded perturbation of every input and state."""
+    if ONLY and name not in ONLY:
+        return
+    jnp = ref.jnp
+    from flapjax.aero.linear.linear_uvlm import LinearUVLM
+    from flapjax.algebra.array_utils import construct_named_block_jacobian
+    from flapjax.utils.linear import LinearSystem
+
+    kern = {"epsilon": ref.utils.biot_savart_epsilon, "cutoff": ref.utils.biot_savart_cutoff}[kernel]
+    saved_r = ref.utils.R_CUTOFF
+    if r_cut is not None:
+        ref.utils.R_CUTOFF = r_cut
+    try:
+        kw = {} if mirror is None else dict(mirror_point=jnp.array(mirror[0]), mirror_normal=jnp.array(mirror[1]))
+        uv = ref.UVLM(grid_shapes=[ref.GridDiscretisation(c.m, c.n, c.m_star)], dof_mapping=[jnp.arange(c.n + 1)],
+                      kernel=kern, free_wake=free_wake, **kw)
+        ff = (ref.Constant(jnp.array(c.u_inf), c.rho, True) if gust is None else
+              ref.OneMinusCosine(jnp.array(c.u_inf), c.rho, True, gust_length=gust["length"],
+                                 gust_amplitude=gust["amplitude"], gust_x0=jnp.array(gust["x0"])))
+        uv.set_design_variables(dt=float(c.dt), flowfield=ff, zeta_b0=[jnp.array(c.zeta_b0)], hg0=jnp.array(c.hg0))
+        st = uv.solve_static()
+        lin = LinearUVLM(uv, st, wake_type=wake_type, skip_linearisation=True)
+        residuals = lin.compute_jacobians()
+
+        def full_step(**kwargs):
+            x1, y0 = lin._step_from_vecs(**kwargs)
+            return np.asarray(lin.pack_state_vector(x1)), np.asarray(lin.pack_output_vector(y0))
+
+        # every differentiated argument, each perturbed once per column and sign; all
+        # other arguments stay at the reference, as in the residual functions' defaults
+        ref_args = {}
+        for _, args, diff in residuals.values():
+            for k in diff:
+                ref_args[k] = np.asarray(args[k], float)
+        x_ref, y_ref = full_step()
+        cols = {}
+        for k, v in ref_args.items():
+            jx = np.zeros((x_ref.size, v.size))
+            jy = np.zeros((y_ref.size, v.size))
+            for j in range(v.size):
+                vp, vm = v.copy(), v.copy()
+                vp[j] += h
+                vm[j] -= h
+                xp, yp = full_step(**{k: jnp.array(vp)})
+                xm, ym = full_step(**{k: jnp.array(vm)})
+                jx[:, j] = (xp - xm) / (2 * h)
+                jy[:, j] = (yp - ym) / (2 * h)
+            cols[k] = (jx, jy)
+            print(" ", name, k, v.size)
+
+        def rows(slices, nm):
+            comp = slices[nm]
+            sl = comp.slices if isinstance(comp.slices, slice) else comp.slices[0]
+            return sl
+
+        jac = {}
+        for res, (_, _, diff) in residuals.items():
+            is_out = res in ("f_steady", "f_unsteady")
+            sl = rows(lin.output_slices if is_out else lin.state_slices, res)
+            jac[res] = {k: jnp.array(cols[k][1 if is_out else 0][sl]) for k in diff}
+        state_specs = [("gamma_b", "gamma_b_n_vec"), ("gamma_w", "gamma_w_n_vec"), ("gamma_b_nm1", "gamma_b_nm1_vec"),
+                       ("zeta_w", "zeta_w_n_vec"), ("zeta_b", "zeta_b_n_vec")]
+        state_specs = [(a, b) for a, b in state_specs if lin.state_slices[a].enabled]
+        sizes = {"gamma_b": st.gamma_b.size, "gamma_w": st.gamma_w.size, "gamma_b_nm1": st.gamma_b.size,
+                 "zeta_w": st.zeta_w.size, "zeta_b": st.zeta_b.size}
+        input_specs = [("zeta_b_np1_vec", st.zeta_b.size), ("zeta_b_dot_np1_vec", st.zeta_b.size),
+                       ("nu_b_np1_vec", st.zeta_b.size), ("nu_w_np1_vec", st.zeta_w.size)]
+        output_specs = [("f_steady", st.zeta_b.size * 1), ("f_unsteady", st.zeta_b.size)]
+        s_names = [a for a, _ in state_specs]
+        s_keys = [b for _, b in state_specs]
+        s_sizes = [sizes[a] for a in s_names]
+        a_ = construct_named_block_jacobian(tuple(jac[k] for k in s_names), s_keys, s_sizes, s_sizes)
+        b_ = construct_named_block_jacobian(tuple(jac[k] for k in s_names), [k for k, _ in input_specs],
+                                            [v for _, v in input_specs], s_sizes)
+        c_ = construct_named_block_jacobian(tuple(jac[k] for k, _ in output_specs), s_keys, s_sizes,
+                                            [v for _, v in output_specs])
+        d_ = construct_named_block_jacobian(tuple(jac[k] for k, _ in output_specs), [k for k, _ in input_specs],
+                                            [v for _, v in input_specs], [v for _, v in output_specs])
+        sys_ = LinearSystem(a=a_, b=b_, c=c_, d=d_, dt=float(c.dt))
+        rng = np.random.default_rng(seed)
+        u_run = 1e-3 * rng.normal(size=(n_run, lin.n_inputs))
+        x0 = 1e-3 * rng.normal(size=lin.n_states)
+        x_run, y_run = sys_.run(jnp.array(u_run), jnp.array(x0))
+        # the nonlinear step at one seeded perturbation of every argument
+        pert = {k: v + 1e-3 * rng.normal(size=v.shape) for k, v in ref_args.items()}
+        x_p, y_p = full_step(**{k: jnp.array(v) for k, v in pert.items()})
+        out = {"case_name": name, "wake_type": wake_type, "kernel": kernel,
+               "r_cut": r_cut if r_cut is not None else saved_r, "free_wake": free_wake, "dt": c.dt,
+               "u_inf": c.u_inf, "rho": c.rho, "zeta_b0": c.zeta_b0, "hg0": c.hg0,
+               "dims": np.array([c.m, c.n, c.m_star]), "h": h,
+               "a": np.asarray(a_), "b": np.asarray(b_), "c": np.asarray(c_), "d": np.asarray(d_),
+               "u_run": u_run, "x0_run": x0, "x_run": np.asarray(x_run), "y_run": np.asarray(y_run),
+               "x_ref": x_ref, "y_ref": y_ref, "x_pert": x_p, "y_pert": y_p}
+        for k, v in pert.items():
+            out[f"pert_{k}"] = v
+        for f in ("zeta_b", "zeta_w", "gamma_b", "gamma_w", "f_steady"):
+            out[f"ref_{f}"] = np.asarray(getattr(st, f)[0])
+        if gust is not None:
+            out.update(gust_length=gust["length"], gust_amplitude=gust["amplitude"], gust_x0=np.asarray(gust["x0"]))
+        if mirror is not None:
+            out["mirror_point"] = np.asarray(mirror[0], float)
+            out["mirror_normal"] = np.asarray(mirror[1], float)
+        np.savez_compressed(HERE / "linear" / f"{name}.npz", **{k: np.asarray(v) for k, v in out.items()})
+        print("wrote linear", name)
+    finally:
+        ref.utils.R_CUTOFF = saved_r
+
+
 ONLY: set[str] = set()
 
 
@@ -392,6 +510,17 @@ def main():
     c = cases.wing_free(m=3, n=4, m_star=4, n_steps=3, seed=1)
     run_gradient_case(ref, "gradient_free_mirror", c, free_wake=True, kernel="cutoff", r_cut=1e-3,
                       mirror=([0.0, 0.0, 0.0], [0.0, 1.0, 0.0]))
+
+    # the linearised UVLM about a static solution: A, B, C, D by central differences of the
+    # reference's own step functions, and its LinearSystem.run
+    (HERE / "linear").mkdir(exist_ok=True)
+    run_linear_case(ref, "linear_frozen", cases.wing_heave(m=2, n=3, m_star=3, n_steps=1), "frozen")
+    c = cases.wing_free(m=2, n=3, m_star=3, n_steps=1, seed=2)
+    run_linear_case(ref, "linear_free_gust_mirror", c, "free", free_wake=True, kernel="cutoff", r_cut=1e-3,
+                    gust={"length": 2.0, "amplitude": 0.1, "x0": [-1.5, 0.0, 0.0]},
+                    mirror=([0.0, -0.5, 0.0], [0.0, 1.0, 0.0]))
+    c = cases.wing_pitch(m=2, n=3, m_star=3, n_steps=1, n_ctrl=3, seed=4)
+    run_linear_case(ref, "linear_prescribed", c, "prescribed")
 
 
 if __name__ == "__main__":
