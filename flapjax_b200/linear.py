@@ -1,0 +1,831 @@
+"""The linearised UVLM (aero/linear/linear_uvlm.py) and its discrete state-space system
+(utils/linear.py:673-822), assembled on the device.
+
+The reference linearises one UVLM step (``LinearUVLM.step``, :324-429: the nonlinear
+step from states x_n to x_{n+1} with the inputs of step n+1) about a steady reference
+solution by ``jax.jacrev`` of each residual with respect to the arguments listed in
+``compute_jacobians`` (:499-621), and assembles A, B, C, D from the blocks
+(``linearise``, :727-829).  Here the same blocks come from the chain rule written out,
+with every pairwise Biot-Savart term on the GPU:
+
+* the bound circulation of step n+1 is Gamma_b = A(zeta_b)^-1 Phi, Phi = -n . V(c) with
+  V the total velocity at the collocation points (free stream, -c_dot, induced velocity
+  of the new wake and the bound upwash input).  Holding Gamma_b at its value the
+  derivative of A Gamma_b folds into the bound lattice's share of V, so
+  dGamma_b = A^-1 dPhi, and dPhi needs
+    - the ring influence of the wake at c (fj_ring_influence, normals): the wake
+      circulation shifted from the states;
+    - the vertex Jacobians of the wake and bound lattices at c (fj_vertex_jacobian,
+      normals): the trailing-edge row of the new wake is the input lattice's, the
+      wake upwash moves every wake vertex, the bound lattice moves its own sources;
+    - n^T grad V at c (fj_vind_vjp with cotangent n) and the normals' derivative;
+    - for a free wake, the convection velocity's ring and vertex Jacobians and its
+      gradient at the convected vertices;
+  and A^-1 is applied to all columns at once (fj_lu_factor, fj_lu_solve_many);
+* the wake rows shift and convect (aero/utils.py:400-500, uniform wake);
+* the steady force f = rho g (v_rel x r) per filament (aero/utils.py:126-223, the linear
+  model's own cutoff kernel :155-160) is differentiated through its strength g, the
+  relative velocity at the midpoint (ring and vertex Jacobians of the bound and wake
+  lattices at the midpoints, 3 rows each; the velocity gradient there) and the filament
+  vector, then split to the vertices; the unsteady force through Gamma_dot.
+
+Blocks the reference does not differentiate stay zero.  Vectors follow the reference's
+slice order, each block the concatenation of its surfaces:
+
+* inputs  u = [zeta_b, zeta_b_dot, nu_b, nu_w]
+* states  x = [gamma_b, gamma_w, gamma_b_nm1, zeta_w, zeta_b]  (zeta_w, zeta_b only for
+  the prescribed and free wake types; gamma_b_nm1 only with the unsteady force)
+* outputs y = [f_steady, f_unsteady]
+
+Scope: FP64, epsilon or cutoff kernel for the UVLM's own sums, any number of surfaces,
+mirror images, Constant or 1-cos gust flow, uniform wake (``delta_w`` raises).  The
+reference point is a steady solution (the static solve), so Gamma_dot there is zero and
+the unsteady force has no geometric derivative.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import warnings
+
+import numpy as np
+
+from . import _lib
+from .adjoint import _flow_T
+from .kernels import R_CUTOFF
+from .runtime import device_of
+
+WAKE_TYPES = ("frozen", "prescribed", "free")
+
+
+# ---------------------------------------------------------------------------------------
+# the state-space system
+# ---------------------------------------------------------------------------------------
+class LinearSystem:
+    """x_n = A x_{n-1} + B u_n, y_n = C x_n + D u_n (utils/linear.py:673-822), device
+    tensors (FP64)."""
+
+    def __init__(self, a, b, c, d, dt, removed_u_np1: bool = False):
+        self.a, self.b, self.c, self.d = a, b, c, d
+        self.dt = float(dt)
+        self.n_inputs = int(b.shape[1])
+        self.n_states = int(a.shape[0])
+        self.n_outputs = int(c.shape[0])
+        self.continuous_time = False
+        self.removed_u_np1 = bool(removed_u_np1)
+
+    def remove_u_np1(self) -> None:
+        """:714-724: D <- C B + D and B <- A B (inputs of step n instead of n+1)."""
+        if self.removed_u_np1:
+            warnings.warn("u_np1 has already been removed from the system. Skipping.")
+            return
+        self.d = self.c @ self.b + self.d
+        self.b = self.a @ self.b
+        self.removed_u_np1 = True
+
+    def run(self, u, x0=None):
+        """:775-822: state and output histories for the input history u (n_tstep, n_inputs),
+        from x0 (zero if None).  Returns device tensors (n_tstep, n_states), (n_tstep,
+        n_outputs)."""
+        import torch
+
+        dev = self.a.device
+        u = torch.as_tensor(np.asarray(u) if not torch.is_tensor(u) else u, dtype=torch.float64).to(dev)
+        if u.ndim != 2 or u.shape[1] != self.n_inputs:
+            raise ValueError(f"Expected shape (None, {self.n_inputs}), but got shape {tuple(u.shape)}.Issue with "
+                             f"input 'u'")
+        n_t = u.shape[0]
+        x = torch.zeros((n_t, self.n_states), dtype=torch.float64, device=dev)
+        if x0 is not None:
+            x0 = torch.as_tensor(np.asarray(x0) if not torch.is_tensor(x0) else x0, dtype=torch.float64).to(dev)
+            if tuple(x0.shape) != (self.n_states,):
+                raise ValueError(f"Expected shape ({self.n_states},), but got shape {tuple(x0.shape)}.Issue with "
+                                 f"input 'x0'")
+            x[0] = x0
+        bu = u @ self.b.T  # every step's input term in one product
+        for i in range(1, n_t):
+            x[i] = self.a @ x[i - 1] + (bu[i - 1] if self.removed_u_np1 else bu[i])
+        y = x @ self.c.T + u @ self.d.T
+        return x, y
+
+
+# ---------------------------------------------------------------------------------------
+# device operations (the C ABI)
+# ---------------------------------------------------------------------------------------
+class _CudaOps:
+    """The pairwise sums, Jacobians and solves of the assembly, on the GPU (FP64)."""
+
+    def __init__(self, device, mirror):
+        import torch
+
+        self.torch = torch
+        self.dev = device_of(device)
+        self._mir = None if mirror is None else tuple(
+            (C.c_double * 3)(*np.asarray(v, dtype=np.float64).tolist()) for v in mirror)
+        self._ws = {}
+
+    def tensor(self, a):
+        return self.torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).to(self.dev)
+
+    def zeros(self, *shape):
+        return self.torch.zeros(shape, dtype=self.torch.float64, device=self.dev)
+
+    def _wsb(self, key, nbytes):
+        w = self._ws.get(key)
+        if w is None or w.numel() < nbytes:
+            w = self.torch.empty(max(int(nbytes), 1), dtype=self.torch.uint8, device=self.dev)
+            self._ws[key] = w
+        return w
+
+    def _stream(self):
+        return self.torch.cuda.current_stream(self.dev).cuda_stream
+
+    def _mirror(self):
+        return self._mir if self._mir is not None else (None, None)
+
+    def ring(self, out, col0, targets, normals, zeta, kernel, r_cut):
+        """out[:, col0 + r] <- d v(targets) / d gamma_r of lattice zeta (rows: 1 per target
+        with normals, else 3)."""
+        mp, mn = self._mirror()
+        _lib.call("fj_ring_influence", targets.data_ptr(), targets.shape[0],
+                  None if normals is None else normals.data_ptr(), zeta.data_ptr(), zeta.shape[0] - 1,
+                  zeta.shape[1] - 1, mp, mn, kernel, r_cut, out.data_ptr() + 8 * col0, out.stride(0),
+                  self._stream())
+
+    def vertex(self, out, col0, targets, normals, zeta, gamma, kernel, r_cut):
+        """out[:, col0 + 3v + b] <- d v(targets) / d zeta_vb for circulations gamma."""
+        mp, mn = self._mirror()
+        _lib.call("fj_vertex_jacobian", targets.data_ptr(), targets.shape[0],
+                  None if normals is None else normals.data_ptr(), zeta.data_ptr(), gamma.data_ptr(),
+                  zeta.shape[0] - 1, zeta.shape[1] - 1, mp, mn, kernel, r_cut, out.data_ptr() + 8 * col0,
+                  out.stride(0), self._stream())
+
+    def _lats(self, lats):
+        n = len(lats)
+        return ((C.c_void_p * n)(*[z.data_ptr() for z, _ in lats]), (C.c_void_p * n)(*[g.data_ptr() for _, g in lats]),
+                (C.c_int * n)(*[z.shape[0] - 1 for z, _ in lats]), (C.c_int * n)(*[z.shape[1] - 1 for z, _ in lats]))
+
+    def vind(self, targets, lats, kernel, r_cut):
+        zp, gp, rows, cols = self._lats(lats)
+        mp, mn = self._mirror()
+        nb = C.c_size_t()
+        _lib.call("fj_vind_workspace_size", targets.shape[0], rows, cols, len(lats), int(self._mir is not None),
+                  _lib.FJ_PREC_FP64, C.byref(nb))
+        ws = self._wsb("vind", nb.value)
+        out = self.torch.empty_like(targets)
+        _lib.call("fj_vind", targets.data_ptr(), targets.shape[0], zp, gp, rows, cols, len(lats), mp, mn, kernel,
+                  r_cut, _lib.FJ_PREC_FP64, out.data_ptr(), ws.data_ptr(), ws.numel(), self._stream())
+        return out
+
+    def vind_grad_t(self, targets, lats, kernel, r_cut, lam):
+        """sum_s d(lam_t . v(x_t))/dx_t per target (the target share of fj_vind_vjp)."""
+        zp, gp, rows, cols = self._lats(lats)
+        mp, mn = self._mirror()
+        nb = C.c_size_t()
+        _lib.call("fj_vind_vjp_workspace_size", targets.shape[0], rows, cols, len(lats), int(self._mir is not None),
+                  C.byref(nb))
+        ws = self._wsb("vjp", nb.value)
+        out = self.torch.zeros_like(targets)
+        _lib.call("fj_vind_vjp", targets.data_ptr(), targets.shape[0], zp, gp, rows, cols, len(lats), mp, mn,
+                  kernel, r_cut, lam.data_ptr(), out.data_ptr(), None, None, ws.data_ptr(), ws.numel(),
+                  self._stream())
+        return out
+
+    def aic_factor(self, zetas_b, kernel, r_cut):
+        k = len(zetas_b)
+        zp = (C.c_void_p * k)(*[z.data_ptr() for z in zetas_b])
+        ms = (C.c_int * k)(*[z.shape[0] - 1 for z in zetas_b])
+        ns = (C.c_int * k)(*[z.shape[1] - 1 for z in zetas_b])
+        nb = sum((z.shape[0] - 1) * (z.shape[1] - 1) for z in zetas_b)
+        a = self.torch.empty((nb, nb), dtype=self.torch.float64, device=self.dev)
+        w = C.c_size_t()
+        _lib.call("fj_aic_workspace_size", ms, ns, k, C.byref(w))
+        ws = self._wsb("aic", w.value)
+        mp, mn = self._mirror()
+        s = self._stream()
+        _lib.call("fj_aic_assemble", zp, ms, ns, k, None, (C.c_int * k)(*([0] * k)), mp, mn, kernel, r_cut,
+                  a.data_ptr(), ws.data_ptr(), ws.numel(), s)
+        piv = self.torch.empty(nb, dtype=self.torch.int32, device=self.dev)
+        _lib.call("fj_lu_workspace_size", nb, C.byref(w))
+        wl = self._wsb("lu", w.value)
+        _lib.call("fj_lu_factor", a.data_ptr(), nb, piv.data_ptr(), wl.data_ptr(), wl.numel(), s)
+        return a, piv
+
+    def solve(self, lu, piv, b):
+        n = piv.numel()
+        w = C.c_size_t()
+        _lib.call("fj_lu_workspace_size", n, C.byref(w))
+        wl = self._wsb("lu", w.value)
+        x = b.clone().contiguous()
+        _lib.call("fj_lu_solve", lu.data_ptr(), n, piv.data_ptr(), x.data_ptr(), wl.data_ptr(), wl.numel(),
+                  self._stream())
+        return x
+
+    def solve_many(self, lu, piv, b):
+        """b <- A^-1 b in place for the columns of the row-major (n, m) b."""
+        n = piv.numel()
+        w = C.c_size_t()
+        _lib.call("fj_lu_solve_many_workspace_size", n, b.shape[1], C.byref(w))
+        ws = self._wsb("many", w.value)
+        _lib.call("fj_lu_solve_many", lu.data_ptr(), n, piv.data_ptr(), b.data_ptr(), b.shape[1], b.stride(0),
+                  ws.data_ptr(), ws.numel(), self._stream())
+
+
+# ---------------------------------------------------------------------------------------
+# geometry bookkeeping (host)
+# ---------------------------------------------------------------------------------------
+def _skew(v):
+    """[v]x per row: (..., 3) -> (..., 3, 3) with [v]x w = v x w."""
+    o = np.zeros(v.shape[:-1] + (3, 3))
+    o[..., 0, 1], o[..., 0, 2] = -v[..., 2], v[..., 1]
+    o[..., 1, 0], o[..., 1, 2] = v[..., 2], -v[..., 0]
+    o[..., 2, 0], o[..., 2, 1] = -v[..., 1], v[..., 0]
+    return o
+
+
+def _flow_grad(ff, x, t):
+    """d u_a / d x_b of the flow field at points x (..., 3) -> (..., 3, 3)."""
+    x = np.asarray(x, dtype=np.float64)
+    out = np.zeros(x.shape + (3,))
+    for a in range(3):
+        e = np.zeros(3)
+        e[a] = 1.0
+        out[..., a, :] = _flow_T(ff, x, t, np.broadcast_to(e, x.shape))
+    return out
+
+
+class _Layout:
+    """Offsets of every block of the state, input and output vectors."""
+
+    def __init__(self, dims, wake_type, bound_upwash, wake_upwash, unsteady_force):
+        self.dims = dims  # per surface (m, n, m_star)
+        self.nb = [m * n for m, n, _ in dims]
+        self.nw = [w * n for _, n, w in dims]
+        self.nvb = [(m + 1) * (n + 1) for m, n, _ in dims]
+        self.nvw = [(w + 1) * (n + 1) for _, n, w in dims]
+        cum = lambda v: np.concatenate([[0], np.cumsum(v)]).astype(np.int64)
+        self.o_gb, self.o_gw, self.o_vb, self.o_vw = cum(self.nb), cum(self.nw), cum(self.nvb), cum(self.nvw)
+        NB, NW, NVB, NVW = int(self.o_gb[-1]), int(self.o_gw[-1]), int(self.o_vb[-1]), int(self.o_vw[-1])
+        self.NB, self.NW, self.NVB, self.NVW = NB, NW, NVB, NVW
+        prescribed = wake_type in ("prescribed", "free")
+        x = [("gamma_b", NB), ("gamma_w", NW)]
+        if unsteady_force:
+            x.append(("gamma_b_nm1", NB))
+        if prescribed:
+            x += [("zeta_w", 3 * NVW), ("zeta_b", 3 * NVB)]
+        u = [("zeta_b", 3 * NVB), ("zeta_b_dot", 3 * NVB)]
+        if bound_upwash:
+            u.append(("nu_b", 3 * NVB))
+        if wake_upwash:
+            u.append(("nu_w", 3 * NVW))
+        y = [("f_steady", 3 * NVB)]
+        if unsteady_force:
+            y.append(("f_unsteady", 3 * NVB))
+
+        def offs(blocks):
+            o, d = 0, {}
+            for k, n in blocks:
+                d[k] = (o, o + n)
+                o += n
+            return d, o
+
+        self.x, self.n_states = offs(x)
+        self.u, self.n_inputs = offs(u)
+        self.y, self.n_outputs = offs(y)
+        self.x_blocks, self.u_blocks, self.y_blocks = x, u, y
+
+    # columns of [states | inputs]
+    def col(self, kind, name):
+        if kind == "x":
+            return self.x.get(name)
+        r = self.u.get(name)
+        return None if r is None else (self.n_states + r[0], self.n_states + r[1])
+
+
+def _diff_lists(wake_type, bound_upwash, wake_upwash, unsteady_force):
+    """compute_jacobians (:499-621): residual -> differentiated arguments."""
+    prescribed = wake_type in ("prescribed", "free")
+    g_b = ["x:gamma_b", "x:gamma_w", "u:zeta_b", "u:zeta_b_dot"] + (["x:zeta_w", "x:zeta_b"] if prescribed else [])
+    g_b += (["u:nu_b"] if bound_upwash else []) + (["u:nu_w"] if wake_upwash else [])
+    out = {"gamma_b": g_b, "gamma_w": ["x:gamma_b", "x:gamma_w"]}
+    if prescribed:
+        out["zeta_w"] = ["x:zeta_w", "u:zeta_b"] + (["u:nu_w"] if wake_upwash else []) + (
+            ["x:gamma_b", "x:gamma_w"] if wake_type == "free" else [])
+    if unsteady_force:
+        out["gamma_b_nm1"] = ["x:gamma_b"]
+    if prescribed:
+        out["zeta_b"] = ["u:zeta_b"]
+    out["f_steady"] = ["x:gamma_b", "x:gamma_w", "u:zeta_b", "u:zeta_b_dot"] + (
+        ["x:zeta_w"] if prescribed else []) + (["u:nu_b"] if bound_upwash else [])
+    if unsteady_force:
+        out["f_unsteady"] = ["x:gamma_b", "x:gamma_b_nm1", "u:zeta_b"]
+    return out
+
+
+# ---------------------------------------------------------------------------------------
+# assembly
+# ---------------------------------------------------------------------------------------
+def _assemble(ops, lay, ref, cfg):
+    """Jacobian rows of every residual over the columns [states | inputs].
+
+    ref: host arrays per surface (zeta_b, zeta_w, gamma_b, gamma_w); cfg: wake_type,
+    free_wake, kernel, r_cut, force_r_cut, dt, rho, flowfield, t, bound_upwash,
+    wake_upwash, unsteady_force.  Returns (R_state, R_out), the Jacobians of the next
+    states and of the outputs, each (rows, n_states + n_inputs), on the ops' device."""
+    torch = ops.torch
+    S = len(lay.dims)
+    ff, t, dt, rho = cfg["flowfield"], cfg["t"], cfg["dt"], cfg["rho"]
+    K, RC, FK, FRC = cfg["kernel"], cfg["r_cut"], _lib.FJ_KERNEL_CUTOFF, cfg["force_r_cut"]
+    free = cfg["free_wake"]
+    wt = cfg["wake_type"]
+    prescribed = wt in ("prescribed", "free")
+    ncol = lay.n_states + lay.n_inputs
+    lists = _diff_lists(wt, cfg["bound_upwash"], cfg["wake_upwash"], cfg["unsteady_force"])
+    Zb = [np.asarray(z, np.float64) for z in ref["zeta_b"]]
+    Zw = [np.asarray(z, np.float64) for z in ref["zeta_w"]]
+    gb = [np.asarray(g, np.float64) for g in ref["gamma_b"]]
+    gw = [np.asarray(g, np.float64) for g in ref["gamma_w"]]
+    tZb, tZw = [ops.tensor(z) for z in Zb], [ops.tensor(z) for z in Zw]
+    tgb, tgw = [ops.tensor(g) for g in gb], [ops.tensor(g) for g in gw]
+
+    def cols(kind, name):
+        return lay.col(kind, name)
+
+    # ---- forward at the reference point -------------------------------------------------
+    conv_pts = [z[:-1] for z in Zw]                    # wake vertices convected (rows 0..W-1)
+    n_conv = [p.shape[0] * p.shape[1] for p in conv_pts]
+    o_conv = np.concatenate([[0], np.cumsum(n_conv)]).astype(np.int64)
+    NC = int(o_conv[-1])
+    conv_flat = np.concatenate([p.reshape(-1, 3) for p in conv_pts]) if NC else np.zeros((0, 3))
+    t_conv = ops.tensor(conv_flat)
+    vc = ff(conv_flat, t)
+    if free and NC:
+        vc = vc + ops.vind(t_conv, list(zip(tZb, tgb)) + list(zip(tZw, tgw)), K, RC).cpu().numpy()
+    zw1, gw1 = [], []
+    for s, (m, n, w) in enumerate(lay.dims):
+        conv = conv_pts[s] + dt * vc[o_conv[s]:o_conv[s + 1]].reshape(conv_pts[s].shape)
+        zw1.append(np.concatenate([Zb[s][-1][None], conv], axis=0))
+        gw1.append(np.concatenate([gb[s][-1][None], gw[s][:-1]], axis=0) if w > 0 else gw[s].copy())
+    tzw1, tgw1 = [ops.tensor(z) for z in zw1], [ops.tensor(g) for g in gw1]
+    c = [0.25 * (z[:-1, :-1] + z[1:, :-1] + z[:-1, 1:] + z[1:, 1:]) for z in Zb]
+    d1 = [z[1:, 1:] - z[:-1, :-1] for z in Zb]
+    d2 = [z[1:, :-1] - z[:-1, 1:] for z in Zb]
+    nc = [np.cross(a, b) for a, b in zip(d1, d2)]
+    c_flat = np.concatenate([x.reshape(-1, 3) for x in c])
+    n_flat = np.concatenate([x.reshape(-1, 3) for x in nc])
+    tc, tn = ops.tensor(c_flat), ops.tensor(n_flat)
+    lu, piv = ops.aic_factor(tZb, K, RC)
+    wake_lats = [(z, g) for z, g in zip(tzw1, tgw1) if z.shape[0] > 1]
+    v_w = ops.vind(tc, wake_lats, K, RC) if wake_lats else torch.zeros_like(tc)
+    u_c = ff(c_flat, t)
+    rhs = -np.einsum("ij,ij->i", u_c + v_w.cpu().numpy(), n_flat)
+    gb1 = ops.solve(lu, piv, ops.tensor(rhs)).cpu().numpy()
+    gb1_s = [gb1[lay.o_gb[s]:lay.o_gb[s + 1]].reshape(m, n) for s, (m, n, _) in enumerate(lay.dims)]
+    tgb1 = [ops.tensor(g) for g in gb1_s]
+    all_lats = list(zip(tZb, tgb1)) + wake_lats
+    v_tot = u_c + ops.vind(tc, all_lats, K, RC).cpu().numpy()            # V(c) at the reference point
+    g_c = ops.vind_grad_t(tc, all_lats, K, RC, tn).cpu().numpy()         # n^T grad_x V(c)
+    g_c += np.einsum("ia,iab->ib", n_flat, _flow_grad(ff, c_flat, t))
+
+    # ---- gamma_b rows: dPhi over all columns, then A^-1 ----------------------------------
+    NB = lay.NB
+    phi = ops.zeros(NB, ncol)
+    rows, cl, vals = [], [], []                                          # local (sparse) terms
+
+    def add(r, cc, v):
+        rows.append(np.asarray(r, np.int64).ravel())
+        cl.append(np.asarray(cc, np.int64).ravel())
+        vals.append(np.asarray(v, np.float64).ravel())
+
+    pw = None
+    if wake_lats and any(k in lists["gamma_b"] for k in ("u:zeta_b", "u:nu_w", "x:zeta_w", "x:zeta_b",
+                                                         "x:gamma_b", "x:gamma_w")):
+        pw = ops.zeros(NB, 3 * lay.NVW)                                   # n . dV(c)/d zeta_w1
+        for s in range(S):
+            if Zw[s].shape[0] > 1:
+                ops.vertex(pw, 3 * int(lay.o_vw[s]), tc, tn, tzw1[s], tgw1[s], K, RC)
+    for s, (m, n, w) in enumerate(lay.dims):
+        k_, l_ = np.meshgrid(np.arange(m), np.arange(n), indexing="ij")
+        i_row = lay.o_gb[s] + k_ * n + l_                                 # (m, n) panel rows
+        vb = lay.o_vb[s]
+        corner = {"00": vb + k_ * (n + 1) + l_, "01": vb + k_ * (n + 1) + l_ + 1,
+                  "10": vb + (k_ + 1) * (n + 1) + l_, "11": vb + (k_ + 1) * (n + 1) + l_ + 1}
+        ii = i_row.ravel()
+        w_i = v_tot[ii]                                                   # V at c_i
+        gi = g_c[ii]
+        D1, D2 = d1[s].reshape(-1, 3), d2[s].reshape(-1, 3)
+        dn = {"11": np.cross(D2, w_i), "00": -np.cross(D2, w_i), "10": np.cross(w_i, D1), "01": -np.cross(w_i, D1)}
+        nrm = n_flat[ii]
+        zb_c, zbd_c = cols("u", "zeta_b"), cols("u", "zeta_b_dot")
+        nub_c = cols("u", "nu_b")
+        for key, vv in corner.items():
+            vv = vv.ravel()
+            for b in range(3):
+                # Phi = -n . V(c): normal and collocation point move with the corner
+                add(ii, zb_c[0] + 3 * vv + b, -dn[key][:, b] - 0.25 * gi[:, b])
+                add(ii, zbd_c[0] + 3 * vv + b, 0.25 * nrm[:, b])          # -n . (-c_dot)
+                if nub_c is not None:
+                    add(ii, nub_c[0] + 3 * vv + b, -0.25 * nrm[:, b])     # -n . avg4(nu_b)
+        # the bound lattice's own sources (circulation held at Gamma_b of step n+1)
+        ops.vertex(phi, zb_c[0] + 3 * int(vb), tc, tn, tZb[s], tgb1[s], K, RC)
+    phi[:, zb_c[0]:zb_c[1]] *= -1.0
+    if pw is not None:
+        for s, (m, n, w) in enumerate(lay.dims):
+            if w == 0:
+                continue
+            te_w = 3 * (int(lay.o_vw[s]) + np.arange(n + 1))              # wake row 0 = input TE row
+            te_b = zb_c[0] + 3 * (int(lay.o_vb[s]) + m * (n + 1) + np.arange(n + 1))
+            for b in range(3):
+                phi[:, te_b + b] -= pw[:, te_w + b]
+        if cols("u", "nu_w") is not None:
+            c0, c1 = cols("u", "nu_w")
+            phi[:, c0:c1] -= dt * pw
+    # wake circulation: gamma_w1[0] = gamma_b[-1], gamma_w1[r+1] = gamma_w[r]
+    if wake_lats:
+        qw = ops.zeros(NB, lay.NW)
+        for s in range(S):
+            if Zw[s].shape[0] > 1:
+                ops.ring(qw, int(lay.o_gw[s]), tc, tn, tzw1[s], K, RC)
+        gbc, gwc = cols("x", "gamma_b"), cols("x", "gamma_w")
+        for s, (m, n, w) in enumerate(lay.dims):
+            if w == 0:
+                continue
+            ow, ob = int(lay.o_gw[s]), int(lay.o_gb[s])
+            phi[:, gbc[0] + ob + (m - 1) * n:gbc[0] + ob + m * n] -= qw[:, ow:ow + n]
+            if w > 1:
+                phi[:, gwc[0] + ow:gwc[0] + ow + (w - 1) * n] -= qw[:, ow + n:ow + w * n]
+    # convection of the wake rows 1..W of step n+1 from rows 0..W-1 of step n
+    need_conv = pw is not None and NC > 0 and (free or prescribed)
+    if need_conv:
+        # P_w restricted to the convected rows, in conv-target order (3 columns each)
+        conv_cols = np.concatenate([3 * (int(lay.o_vw[s]) + (lay.dims[s][1] + 1) + np.arange(n_conv[s]))
+                                    for s in range(S)]) if NC else np.zeros(0, np.int64)
+        cc3 = (conv_cols[:, None] + np.arange(3)[None, :]).ravel()
+        pw_conv = pw[:, torch.as_tensor(cc3, device=pw.device)]           # (NB, 3 NC)
+        if free:
+            jc_gb = ops.zeros(3 * NC, lay.NB)
+            jc_gw = ops.zeros(3 * NC, lay.NW)
+            for s in range(S):
+                ops.ring(jc_gb, int(lay.o_gb[s]), t_conv, None, tZb[s], K, RC)
+                if Zw[s].shape[0] > 1:
+                    ops.ring(jc_gw, int(lay.o_gw[s]), t_conv, None, tZw[s], K, RC)
+            gbc, gwc = cols("x", "gamma_b"), cols("x", "gamma_w")
+            phi[:, gbc[0]:gbc[1]] -= dt * (pw_conv @ jc_gb)
+            phi[:, gwc[0]:gwc[1]] -= dt * (pw_conv @ jc_gw)
+        if prescribed:
+            # d zw1[r+1] / d zw0[r] = I + dt grad(U + V_conv) at the convected vertex
+            gconv = _flow_grad(ff, conv_flat, t)
+            if free:
+                lats0 = list(zip(tZb, tgb)) + [(z, g) for z, g in zip(tZw, tgw) if z.shape[0] > 1]
+                for a in range(3):
+                    lam = np.zeros((NC, 3))
+                    lam[:, a] = 1.0
+                    gconv[:, a, :] += ops.vind_grad_t(t_conv, lats0, K, RC, ops.tensor(lam)).cpu().numpy()
+            blk = np.eye(3)[None] + dt * gconv                               # (NC, 3, 3)
+            zwc = cols("x", "zeta_w")
+            tblk = ops.tensor(blk)
+            # -P_w[:, conv cols of zw1] . blk on the zw0 columns of the same vertex
+            src_cols = np.concatenate([3 * (int(lay.o_vw[s]) + np.arange(n_conv[s])) for s in range(S)])
+            pc = pw_conv.reshape(NB, NC, 3)
+            contrib = -torch.einsum("iva,vab->ivb", pc, tblk)              # (NB, NC, 3)
+            idx = torch.as_tensor((zwc[0] + src_cols[:, None] + np.arange(3)[None, :]).ravel(), device=pw.device)
+            phi.index_add_(1, idx, contrib.reshape(NB, 3 * NC))
+            if free:
+                jc_zw = ops.zeros(3 * NC, 3 * lay.NVW)
+                jc_zb = ops.zeros(3 * NC, 3 * lay.NVB)
+                for s in range(S):
+                    if Zw[s].shape[0] > 1:
+                        ops.vertex(jc_zw, 3 * int(lay.o_vw[s]), t_conv, None, tZw[s], tgw[s], K, RC)
+                    ops.vertex(jc_zb, 3 * int(lay.o_vb[s]), t_conv, None, tZb[s], tgb[s], K, RC)
+                zbs = cols("x", "zeta_b")
+                phi[:, zwc[0]:zwc[1]] -= dt * (pw_conv @ jc_zw)
+                phi[:, zbs[0]:zbs[1]] -= dt * (pw_conv @ jc_zb)
+    if rows:
+        r_, c_, v_ = (np.concatenate(a) for a in (rows, cl, vals))
+        phi.index_put_((torch.as_tensor(r_, device=phi.device), torch.as_tensor(c_, device=phi.device)),
+                       torch.as_tensor(v_, device=phi.device), accumulate=True)
+    _mask(phi, lay, lists["gamma_b"])
+    ops.solve_many(lu, piv, phi)                                          # dGamma_b = A^-1 dPhi
+
+    # ---- next-state rows ------------------------------------------------------------------
+    R_state = ops.zeros(lay.n_states, ncol)
+    r0, r1 = lay.x["gamma_b"]
+    R_state[r0:r1] = phi
+    gbc, gwc = cols("x", "gamma_b"), cols("x", "gamma_w")
+    gw_r = lay.x["gamma_w"][0]
+    ones_r, ones_c = [], []                                               # unit entries of R_state
+    for s, (m, n, w) in enumerate(lay.dims):
+        ow, ob = int(lay.o_gw[s]), int(lay.o_gb[s])
+        if w > 0:
+            ones_r.append(gw_r + ow + np.arange(n))
+            ones_c.append(gbc[0] + ob + (m - 1) * n + np.arange(n))
+        if w > 1:
+            ones_r.append(gw_r + ow + n + np.arange((w - 1) * n))
+            ones_c.append(gwc[0] + ow + np.arange((w - 1) * n))
+    if "gamma_b_nm1" in lay.x:
+        q0 = lay.x["gamma_b_nm1"][0]
+        ones_r.append(q0 + np.arange(NB))
+        ones_c.append(gbc[0] + np.arange(NB))
+    if prescribed:
+        zr = lay.x["zeta_w"][0]
+        zwc, zbi = cols("x", "zeta_w"), cols("u", "zeta_b")
+        for s, (m, n, w) in enumerate(lay.dims):
+            ones_r.append(zr + 3 * int(lay.o_vw[s]) + np.arange(3 * (n + 1)))       # wake row 0 = TE row
+            ones_c.append(zbi[0] + 3 * (int(lay.o_vb[s]) + m * (n + 1)) + np.arange(3 * (n + 1)))
+        if NC:
+            gconv = _flow_grad(ff, conv_flat, t)
+            if free:
+                lats0 = list(zip(tZb, tgb)) + [(z, g) for z, g in zip(tZw, tgw) if z.shape[0] > 1]
+                for a in range(3):
+                    lam = np.zeros((NC, 3))
+                    lam[:, a] = 1.0
+                    gconv[:, a, :] += ops.vind_grad_t(t_conv, lats0, K, RC, ops.tensor(lam)).cpu().numpy()
+            dst = np.concatenate([3 * (int(lay.o_vw[s]) + (lay.dims[s][1] + 1) + np.arange(n_conv[s]))
+                                  for s in range(S)])
+            src = np.concatenate([3 * (int(lay.o_vw[s]) + np.arange(n_conv[s])) for s in range(S)])
+            blk = np.eye(3)[None] + dt * gconv
+            rr = (zr + dst[:, None, None] + np.arange(3)[None, :, None]).repeat(3, axis=2)
+            cc = (zwc[0] + src[:, None, None] + np.arange(3)[None, None, :]).repeat(3, axis=1)
+            R_state.index_put_((torch.as_tensor(rr.ravel(), device=R_state.device),
+                                torch.as_tensor(cc.ravel(), device=R_state.device)),
+                               ops.tensor(blk.ravel()), accumulate=True)
+            if free:
+                dst3 = torch.as_tensor((zr + dst[:, None] + np.arange(3)[None, :]).ravel(), device=R_state.device)
+                R_state[dst3, zwc[0]:zwc[1]] += dt * jc_zw
+                if wt == "free":
+                    R_state[dst3, gbc[0]:gbc[1]] += dt * jc_gb
+                    R_state[dst3, gwc[0]:gwc[1]] += dt * jc_gw
+        if cols("u", "nu_w") is not None:
+            c0, _ = cols("u", "nu_w")
+            R_state.index_put_((torch.as_tensor(zr + np.arange(3 * lay.NVW), device=R_state.device),
+                                torch.as_tensor(c0 + np.arange(3 * lay.NVW), device=R_state.device)),
+                               ops.tensor(np.full(3 * lay.NVW, dt)), accumulate=True)
+        zbr = lay.x["zeta_b"][0]
+        ones_r.append(zbr + np.arange(3 * lay.NVB))
+        ones_c.append(zbi[0] + np.arange(3 * lay.NVB))
+    if ones_r:
+        r_, c_ = np.concatenate(ones_r), np.concatenate(ones_c)
+        R_state.index_put_((torch.as_tensor(r_, device=R_state.device), torch.as_tensor(c_, device=R_state.device)),
+                           ops.tensor(np.ones(r_.size)), accumulate=True)
+
+    # ---- output rows ----------------------------------------------------------------------
+    R_out = ops.zeros(lay.n_outputs, ncol)
+    fs0 = lay.y["f_steady"][0]
+    R_out[fs0:fs0 + 3 * lay.NVB] = _steady_force_rows(ops, lay, cfg, Zb, Zw, gb, gw, tZb, tZw, tgb, tgw, lists)
+    if "f_unsteady" in lay.y:
+        fu0 = lay.y["f_unsteady"][0]
+        gbm = cols("x", "gamma_b_nm1")
+        rr, cc, vv = [], [], []
+        for s, (m, n, w) in enumerate(lay.dims):
+            k_, l_ = np.meshgrid(np.arange(m), np.arange(n), indexing="ij")
+            i = (int(lay.o_gb[s]) + k_ * n + l_).ravel()
+            for dk in (0, 1):
+                for dl in (0, 1):
+                    v = (int(lay.o_vb[s]) + (k_ + dk) * (n + 1) + l_ + dl).ravel()
+                    for b in range(3):
+                        val = 0.25 * rho / dt * n_flat[i, b]   # split_to_vertex over both axes: a quarter each
+                        rr += [fu0 + 3 * v + b, fu0 + 3 * v + b]
+                        cc += [gbc[0] + i, gbm[0] + i]
+                        vv += [val, -val]
+        R_out.index_put_((torch.as_tensor(np.concatenate(rr), device=R_out.device),
+                          torch.as_tensor(np.concatenate(cc), device=R_out.device)),
+                         ops.tensor(np.concatenate(vv)), accumulate=True)
+        # d f_unsteady / d zeta_b = rho Gamma_dot split(dn): Gamma_dot is zero at the
+        # reference point (gamma_b_n = gamma_b_nm1 = the reference circulation)
+    return R_state, R_out
+
+
+def _mask(mat, lay, diff):
+    """Zero the column blocks a residual does not differentiate."""
+    keep = set(diff)
+    for kind, blocks in (("x", lay.x_blocks), ("u", lay.u_blocks)):
+        for name, _ in blocks:
+            if f"{kind}:{name}" not in keep:
+                c0, c1 = lay.col(kind, name)
+                mat[:, c0:c1] = 0.0
+
+
+def _steady_force_rows(ops, lay, cfg, Zb, Zw, gb, gw, tZb, tZw, tgb, tgw, lists):
+    """d f_steady over [states | inputs]: f = rho g (v_rel x r) per filament, split to the
+    vertices (aero/utils.py:126-223), v_rel from the linear model's cutoff kernel."""
+    torch = ops.torch
+    S = len(lay.dims)
+    ff, t, rho = cfg["flowfield"], cfg["t"], cfg["rho"]
+    FK, FRC = _lib.FJ_KERNEL_CUTOFF, cfg["force_r_cut"]
+    prescribed = cfg["wake_type"] in ("prescribed", "free")
+    ncol = lay.n_states + lay.n_inputs
+    # filaments of every surface: start, end vertex (global), strength coefficients
+    fa, fb, mids, rvec, gval = [], [], [], [], []
+    gcoef = []   # list of (filament, column-in-gamma_b or -1-(gamma_w col), coefficient)
+    nf = 0
+    for s, (m, n, w) in enumerate(lay.dims):
+        z = Zb[s]
+        vb, ob, ow = int(lay.o_vb[s]), int(lay.o_gb[s]), int(lay.o_gw[s])
+        G = gb[s]
+        for k in range(m):          # chordwise (k,l)->(k+1,l), g = G[k,l] - G[k,l-1]
+            for l in range(n + 1):
+                fa.append(vb + k * (n + 1) + l)
+                fb.append(vb + (k + 1) * (n + 1) + l)
+                g = (G[k, l] if l < n else 0.0) - (G[k, l - 1] if l >= 1 else 0.0)
+                if l < n:
+                    gcoef.append((nf, ob + k * n + l, 1.0))
+                if l >= 1:
+                    gcoef.append((nf, ob + k * n + l - 1, -1.0))
+                gval.append(g)
+                nf += 1
+        for k in range(m + 1):      # spanwise (k,l)->(k,l+1), g = G[k-1,l] - G[k,l] (- G_w[0,l] at the TE)
+            for l in range(n):
+                fa.append(vb + k * (n + 1) + l)
+                fb.append(vb + k * (n + 1) + l + 1)
+                g = (G[k - 1, l] if k >= 1 else 0.0) - (G[k, l] if k < m else 0.0)
+                if k >= 1:
+                    gcoef.append((nf, ob + (k - 1) * n + l, 1.0))
+                if k < m:
+                    gcoef.append((nf, ob + k * n + l, -1.0))
+                if k == m and w > 0:
+                    g -= gw[s][0, l]
+                    gcoef.append((nf, -1 - (ow + l), -1.0))
+                gval.append(g)
+                nf += 1
+    fa, fb = np.asarray(fa), np.asarray(fb)
+    zflat = np.concatenate([z.reshape(-1, 3) for z in Zb])
+    mid = 0.5 * (zflat[fa] + zflat[fb])
+    rv = zflat[fb] - zflat[fa]
+    gval = np.asarray(gval)
+    tmid = ops.tensor(mid)
+    wake_lats = [(z, g) for z, g in zip(tZw, tgw) if z.shape[0] > 1]
+    lats = list(zip(tZb, tgb)) + wake_lats
+    v = ff(mid, t) + ops.vind(tmid, lats, FK, FRC).cpu().numpy()          # v_rel at the reference
+    grad = _flow_grad(ff, mid, t)
+    for a in range(3):
+        lam = np.zeros((nf, 3))
+        lam[:, a] = 1.0
+        grad[:, a, :] += ops.vind_grad_t(tmid, lats, FK, FRC, ops.tensor(lam)).cpu().numpy()
+    # dv (velocity at the midpoints) per column, 3 rows per filament
+    dv = ops.zeros(3 * nf, ncol)
+    gbc, gwc = lay.col("x", "gamma_b"), lay.col("x", "gamma_w")
+    for s in range(S):
+        ops.ring(dv, gbc[0] + int(lay.o_gb[s]), tmid, None, tZb[s], FK, FRC)
+        if Zw[s].shape[0] > 1:
+            ops.ring(dv, gwc[0] + int(lay.o_gw[s]), tmid, None, tZw[s], FK, FRC)
+    zbc = lay.col("u", "zeta_b")
+    for s in range(S):
+        ops.vertex(dv, zbc[0] + 3 * int(lay.o_vb[s]), tmid, None, tZb[s], tgb[s], FK, FRC)
+    if prescribed:
+        zwc = lay.col("x", "zeta_w")
+        for s in range(S):
+            if Zw[s].shape[0] > 1:
+                ops.vertex(dv, zwc[0] + 3 * int(lay.o_vw[s]), tmid, None, tZw[s], tgw[s], FK, FRC)
+    rows, cl, vals = [], [], []
+    fi = np.arange(nf)
+    for end in (fa, fb):
+        for a in range(3):
+            for b in range(3):
+                # the midpoint moves with both ends: grad v . 0.5 d zeta
+                rows.append(3 * fi + a)
+                cl.append(zbc[0] + 3 * end + b)
+                vals.append(0.5 * grad[:, a, b])
+            # - 0.5 zeta_dot (relative velocity) and + 0.5 nu_b (bound upwash input)
+            rows.append(3 * fi + a)
+            cl.append(lay.col("u", "zeta_b_dot")[0] + 3 * end + a)
+            vals.append(np.full(nf, -0.5))
+            if lay.col("u", "nu_b") is not None:
+                rows.append(3 * fi + a)
+                cl.append(lay.col("u", "nu_b")[0] + 3 * end + a)
+                vals.append(np.full(nf, 0.5))
+    r_, c_, v_ = (np.concatenate(x) for x in (rows, cl, vals))
+    dev = dv.device
+    dv.index_put_((torch.as_tensor(r_, device=dev), torch.as_tensor(c_, device=dev)), torch.as_tensor(v_, device=dev),
+                  accumulate=True)
+    # per filament: rho g (dv x r) + rho g (v x dr) + rho dg (v x r)
+    dv3 = dv.reshape(nf, 3, ncol)
+    r_t = ops.tensor(rv)[:, :, None].expand(nf, 3, ncol)
+    df = torch.linalg.cross(dv3, r_t, dim=1) * ops.tensor(rho * gval)[:, None, None]
+    rows, cl, vals = [], [], []
+    vx = _skew(v) * (rho * gval)[:, None, None]                           # rho g [v]x
+    for sign, end in ((1.0, fb), (-1.0, fa)):
+        for a in range(3):
+            for b in range(3):
+                rows.append(3 * fi + a)
+                cl.append(zbc[0] + 3 * end + b)
+                vals.append(sign * vx[:, a, b])
+    vxr = rho * np.cross(v, rv)                                           # rho (v x r)
+    for f, col, coef in gcoef:
+        colg = gbc[0] + col if col >= 0 else gwc[0] + (-1 - col)
+        for a in range(3):
+            rows.append([3 * f + a])
+            cl.append([colg])
+            vals.append([coef * vxr[f, a]])
+    r_, c_, v_ = (np.concatenate([np.ravel(x) for x in y]) for y in (rows, cl, vals))
+    df = df.reshape(3 * nf, ncol)
+    df.index_put_((torch.as_tensor(r_, device=dev), torch.as_tensor(c_, device=dev)), torch.as_tensor(v_, device=dev),
+                  accumulate=True)
+    # split to the vertices: each filament's force half to either end
+    out = ops.zeros(3 * lay.NVB, ncol)
+    for end in (fa, fb):
+        idx = torch.as_tensor((3 * end[:, None] + np.arange(3)[None, :]).ravel(), device=dev)
+        out.index_add_(0, idx, 0.5 * df)
+    _mask(out, lay, lists["f_steady"])
+    return out
+
+
+# ---------------------------------------------------------------------------------------
+# the public class
+# ---------------------------------------------------------------------------------------
+class LinearUVLM:
+    """Linearised UVLM about a steady reference solution (aero/linear/linear_uvlm.py:81-).
+
+    ``LinearUVLM(uvlm, reference, wake_type)`` with ``reference`` the snapshot of
+    ``uvlm.solve_static()``; ``.sys`` is the ``LinearSystem`` (A, B, C, D on the device),
+    ``.run(u, x0)`` marches it over input perturbations and returns the totals."""
+
+    def __init__(self, case, reference, wake_type: str = "frozen", bound_upwash: bool = True,
+                 wake_upwash: bool = True, unsteady_force: bool = True, *, skip_checks: bool = False,
+                 skip_linearisation: bool = False, device=None):
+        if wake_type not in WAKE_TYPES:
+            raise ValueError(f"wake_type must be one of {WAKE_TYPES}, got {wake_type!r}")
+        if case.kernel.kernel_id not in (_lib.FJ_KERNEL_EPSILON, _lib.FJ_KERNEL_CUTOFF):
+            raise NotImplementedError("the linearisation is written for the epsilon and cutoff kernels")
+        if any(d is not None for d in (case.delta_w or [])):
+            raise NotImplementedError("the linearisation is written for the uniform wake (delta_w = None)")
+        if any(p is not None for p in case.polars):
+            raise NotImplementedError("polar corrections are not part of the linear model")
+        self.case = case
+        self.wake_type = wake_type
+        self.prescribed_wake, self.free_wake = {"frozen": (False, False), "prescribed": (True, False),
+                                                "free": (True, True)}[wake_type]
+        self.bound_upwash, self.wake_upwash, self.unsteady_force = bound_upwash, wake_upwash, unsteady_force
+        self.dt = float(case.dt)
+        self._reference = reference
+        g = lambda name: [np.asarray(a, np.float64) for a in getattr(reference, name)]
+        self._ref = {"zeta_b": g("zeta_b"), "zeta_w": g("zeta_w"), "gamma_b": g("gamma_b"), "gamma_w": g("gamma_w"),
+                     "zeta_b_dot": g("zeta_b_dot"), "f_steady": g("f_steady")}
+        gbd = getattr(reference, "gamma_b_dot", None)
+        self._ref["gamma_b_dot"] = ([np.zeros_like(a) for a in self._ref["gamma_b"]] if gbd is None else
+                                    [np.asarray(a, np.float64) for a in gbd])
+        fu = getattr(reference, "f_unsteady", None)
+        self._ref["f_unsteady"] = ([np.zeros_like(a) for a in self._ref["f_steady"]] if fu is None else
+                                   [np.asarray(a, np.float64) for a in fu])
+        if not skip_checks:
+            if max(np.abs(z).max() for z in self._ref["zeta_b_dot"]) > 1e-6:
+                warnings.warn("Reference bound surface velocities are non-zero. Ensure that the reference state is "
+                              "steady for linearisation.")
+            if max(np.abs(z).max() for z in self._ref["gamma_b_dot"]) > 1e-6:
+                warnings.warn("Reference bound circulation time derivative is non-zero. Ensure that the reference "
+                              "state is steady for linearisation.")
+        dims = [(gd.m, gd.n, gd.m_star) for gd in case.grid_disc]
+        self.layout = _Layout(dims, wake_type, bound_upwash, wake_upwash, unsteady_force)
+        self.n_inputs, self.n_states, self.n_outputs = (self.layout.n_inputs, self.layout.n_states,
+                                                        self.layout.n_outputs)
+        mirror = None if case.mirror_point is None else (case.mirror_point, case.mirror_normal)
+        self._ops = _CudaOps(device, mirror)
+        self._sys = None
+        if not skip_linearisation:
+            self._sys = self.linearise()
+
+    @property
+    def sys(self) -> LinearSystem:
+        if self._sys is None:
+            raise ValueError("System not linearised")
+        return self._sys
+
+    @property
+    def reference(self):
+        return self._reference
+
+    def _config(self):
+        kid = self.case.kernel.kernel_id
+        return {"wake_type": self.wake_type, "free_wake": bool(self.case.free_wake), "kernel": kid,
+                "r_cut": self.case.kernel.r_cut,
+                # the linear model's force kernel is the cutoff kernel at the module radius
+                # (aero/utils.py:648), the UVLM's own radius when it uses the cutoff kernel
+                "force_r_cut": self.case.kernel.r_cut if kid == _lib.FJ_KERNEL_CUTOFF else R_CUTOFF,
+                "dt": self.dt, "rho": self.case.flowfield.rho, "flowfield": self.case.flowfield,
+                "t": float(np.asarray(self._reference.t).ravel()[0]), "bound_upwash": self.bound_upwash,
+                "wake_upwash": self.wake_upwash, "unsteady_force": self.unsteady_force}
+
+    def linearise(self) -> LinearSystem:
+        """A, B, C, D about the reference (:727-829)."""
+        lay = self.layout
+        r_state, r_out = _assemble(self._ops, lay, self._ref, self._config())
+        ns = lay.n_states
+        return LinearSystem(r_state[:, :ns].contiguous(), r_state[:, ns:].contiguous(), r_out[:, :ns].contiguous(),
+                            r_out[:, ns:].contiguous(), self.dt)
+
+    # -- vectors ------------------------------------------------------------------------
+    def reference_states(self) -> np.ndarray:
+        r = self._ref
+        d = {"gamma_b": r["gamma_b"], "gamma_w": r["gamma_w"], "gamma_b_nm1": r["gamma_b"], "zeta_w": r["zeta_w"],
+             "zeta_b": r["zeta_b"]}
+        return np.concatenate([np.concatenate([np.ravel(a) for a in d[k]]) for k, _ in self.layout.x_blocks])
+
+    def reference_outputs(self) -> np.ndarray:
+        r = self._ref
+        return np.concatenate([np.concatenate([np.ravel(a) for a in r[k]]) for k, _ in self.layout.y_blocks])
+
+    def run(self, u, x0=None):
+        """Perturbation histories (x, y) of the linear system for input perturbations u
+        (n_tstep, n_inputs) from x0, and the totals (reference + perturbation) as numpy
+        arrays: returns (x, y, x_total, y_total)."""
+        x, y = self.sys.run(u, x0)
+        x, y = x.cpu().numpy(), y.cpu().numpy()
+        return x, y, x + self.reference_states()[None], y + self.reference_outputs()[None]

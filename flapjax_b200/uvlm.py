@@ -311,6 +311,15 @@ class UVLM:
         dc.solve_static(horseshoe, float(t))
         return self._to_case(dc, snapshot=True)
 
+    def linearise(self, reference: AeroCase, wake_type: str, bound_upwash: bool = True, wake_upwash: bool = True,
+                  unsteady_force: bool = True):
+        """aero/uvlm.py:356-385: the linearised model about ``reference`` (a steady snapshot,
+        e.g. ``solve_static()``), with A, B, C, D assembled on the device."""
+        from .linear import LinearUVLM
+
+        return LinearUVLM(self, reference=reference, wake_type=wake_type, bound_upwash=bound_upwash,
+                          wake_upwash=wake_upwash, unsteady_force=unsteady_force, device=self.device)
+
     def reference_configuration(self) -> AeroCase:
         """aero/uvlm.py:1408-1446: the undisturbed snapshot with zero circulation."""
         gds = self.grid_disc

@@ -1,0 +1,62 @@
+"""Loading of the linear-model golden cases (tests/golden/linear/*.npz, written by
+tests/golden/make_golden.py from the reference's own LinearUVLM)."""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+
+GOLDEN = Path(__file__).resolve().parent / "golden" / "linear"
+CASES = ("linear_frozen", "linear_free_gust_mirror", "linear_prescribed")
+
+
+def load(name):
+    return dict(np.load(GOLDEN / f"{name}.npz", allow_pickle=False))
+
+
+def mirror_of(g):
+    return None if "mirror_point" not in g else (g["mirror_point"], g["mirror_normal"])
+
+
+def flow_oracle(g):
+    from oracle import uvlm_ref as R
+
+    if "gust_length" in g:
+        return R.OneMinusCosine(g["u_inf"], float(g["rho"]), True, float(g["gust_length"]),
+                                float(g["gust_amplitude"]), gust_x0=g["gust_x0"])
+    return R.Constant(g["u_inf"], float(g["rho"]))
+
+
+def flow_product(g):
+    from flapjax_b200 import Constant, OneMinusCosine
+
+    if "gust_length" in g:
+        return OneMinusCosine(g["u_inf"], float(g["rho"]), True, gust_length=float(g["gust_length"]),
+                              gust_amplitude=float(g["gust_amplitude"]), gust_x0=g["gust_x0"])
+    return Constant(g["u_inf"], float(g["rho"]), True)
+
+
+def kernel_id(g):
+    from flapjax_b200 import _lib
+
+    return {"epsilon": _lib.FJ_KERNEL_EPSILON, "cutoff": _lib.FJ_KERNEL_CUTOFF}[str(g["kernel"])]
+
+
+def config(g, flowfield):
+    from flapjax_b200 import _lib
+
+    kid = kernel_id(g)
+    return {"wake_type": str(g["wake_type"]), "free_wake": bool(g["free_wake"]), "kernel": kid,
+            "r_cut": float(g["r_cut"]), "force_r_cut": float(g["r_cut"]) if kid == _lib.FJ_KERNEL_CUTOFF else 1e-4,
+            "dt": float(g["dt"]), "rho": float(g["rho"]), "flowfield": flowfield, "t": 0.0, "bound_upwash": True,
+            "wake_upwash": True, "unsteady_force": True}
+
+
+def reference(g):
+    return {"zeta_b": [g["ref_zeta_b"]], "zeta_w": [g["ref_zeta_w"]], "gamma_b": [g["ref_gamma_b"]],
+            "gamma_w": [g["ref_gamma_w"]]}
+
+
+def dims(g):
+    m, n, w = (int(v) for v in g["dims"])
+    return [(m, n, w)]

@@ -1,0 +1,185 @@
+"""The linearised UVLM on the GPU (aero/linear/linear_uvlm.py): the influence-Jacobian
+and many-right-hand-side kernels against the oracle, A, B, C, D against the reference's
+own linear model (tests/golden/linear) and against the oracle at larger sizes, and the
+linear system against the nonlinear solver for a small heave."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from tests import linear_golden as LG
+from tests.helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _lattice(rows, cols, seed):
+    rng = np.random.default_rng(seed)
+    z = np.zeros((rows + 1, cols + 1, 3))
+    z[..., 0] = np.linspace(0.0, 1.0, rows + 1)[:, None]
+    z[..., 1] = np.linspace(0.0, 2.0, cols + 1)[None, :]
+    z += 0.02 * rng.normal(size=z.shape)
+    return z, rng.normal(size=(rows, cols))
+
+
+@pytest.mark.parametrize("kernel", ["epsilon", "cutoff"])
+@pytest.mark.parametrize("mirror", [False, True])
+def test_influence_kernels_match_oracle(cuda, kernel, mirror):
+    import torch
+
+    from flapjax_b200 import _lib
+    from flapjax_b200.linear import _CudaOps
+    from tests.linear_cpu_ops import OracleOps
+
+    kid = {"epsilon": _lib.FJ_KERNEL_EPSILON, "cutoff": _lib.FJ_KERNEL_CUTOFF}[kernel]
+    rc = 1e-3
+    mir = (np.array([0.0, -0.4, 0.0]), np.array([0.0, 1.0, 0.0])) if mirror else None
+    z, g = _lattice(3, 4, 1)
+    rng = np.random.default_rng(2)
+    x = np.stack([rng.uniform(-0.2, 1.2, 7), rng.uniform(-0.2, 2.2, 7), rng.uniform(0.1, 0.6, 7)], axis=1)
+    nrm = rng.normal(size=(7, 3))
+    gpu, cpu = _CudaOps(cuda, mir), OracleOps(mir)
+    for normals in (None, nrm):
+        rows = 7 if normals is not None else 21
+        for what, width in (("ring", 12), ("vertex", 60)):
+            ld, c0 = width + 5, 2
+            out = torch.full((rows, ld), float("nan"), dtype=torch.float64, device=cuda)
+            want = torch.zeros((rows, ld), dtype=torch.float64)
+            tn = None if normals is None else gpu.tensor(normals)
+            if what == "ring":
+                gpu.ring(out, c0, gpu.tensor(x), tn, gpu.tensor(z), kid, rc)
+                cpu.ring(want, c0, cpu.tensor(x), None if normals is None else cpu.tensor(normals), cpu.tensor(z),
+                         kid, rc)
+            else:
+                gpu.vertex(out, c0, gpu.tensor(x), tn, gpu.tensor(z), gpu.tensor(g), kid, rc)
+                cpu.vertex(want, c0, cpu.tensor(x), None if normals is None else cpu.tensor(normals), cpu.tensor(z),
+                           cpu.tensor(g), kid, rc)
+            o = out.cpu().numpy()
+            assert np.isnan(o[:, :c0]).all() and np.isnan(o[:, c0 + width:]).all()  # only its block written
+            w = want.numpy()[:, c0:c0 + width]
+            tol = 1e-12 if what == "ring" else 1e-7  # the oracle's vertex Jacobian is a central difference
+            assert rel_err(o[:, c0:c0 + width], w) < tol, (what, normals is None)
+
+
+def test_lu_solve_many(cuda):
+    import torch
+
+    from flapjax_b200 import _lib
+
+    rng = np.random.default_rng(0)
+    n, m, ldb = 300, 257, 261
+    a = rng.normal(size=(n, n)) + 0.2 * n * np.eye(n)
+    b = rng.normal(size=(n, ldb))
+    ta = torch.as_tensor(a).to(cuda)
+    piv = torch.empty(n, dtype=torch.int32, device=cuda)
+    w = C.c_size_t()
+    _lib.call("fj_lu_workspace_size", n, C.byref(w))
+    wl = torch.empty(w.value, dtype=torch.uint8, device=cuda)
+    s = torch.cuda.current_stream(cuda).cuda_stream
+    _lib.call("fj_lu_factor", ta.data_ptr(), n, piv.data_ptr(), wl.data_ptr(), wl.numel(), s)
+    tb = torch.as_tensor(b).to(cuda)
+    _lib.call("fj_lu_solve_many_workspace_size", n, m, C.byref(w))
+    ws = torch.empty(w.value, dtype=torch.uint8, device=cuda)
+    _lib.call("fj_lu_solve_many", ta.data_ptr(), n, piv.data_ptr(), tb.data_ptr(), m, ldb, ws.data_ptr(), ws.numel(),
+              s)
+    got = tb.cpu().numpy()
+    assert rel_err(got[:, :m], np.linalg.solve(a, b[:, :m])) < 1e-12
+    assert np.array_equal(got[:, m:], b[:, m:])
+    with pytest.raises(Exception):
+        _lib.call("fj_lu_solve_many", ta.data_ptr(), n, piv.data_ptr(), tb.data_ptr(), m, m - 1, ws.data_ptr(),
+                  ws.numel(), s)
+
+
+def _product_uvlm(g, **kw):
+    import flapjax_b200 as fj
+
+    m, n, w = (int(v) for v in g["dims"])
+    kernel = fj.cutoff_kernel(float(g["r_cut"])) if str(g["kernel"]) == "cutoff" else fj.biot_savart_epsilon
+    mir = LG.mirror_of(g)
+    mkw = {} if mir is None else dict(mirror_point=mir[0], mirror_normal=mir[1])
+    uv = fj.UVLM([fj.GridDiscretisation(m, n, w)], np.arange(n + 1), kernel=kernel, free_wake=bool(g["free_wake"]),
+                 **mkw, **kw)
+    uv.set_design_variables(dt=float(g["dt"]), flowfield=LG.flow_product(g), zeta_b0=g["zeta_b0"], hg0=g["hg0"])
+    return uv
+
+
+@pytest.mark.parametrize("name", LG.CASES)
+def test_linear_model_matches_reference(cuda, name):
+    """A, B, C, D of the reference's own LinearUVLM (central differences of its step
+    functions, h = 1e-6) and its LinearSystem.run over seeded inputs."""
+    from flapjax_b200.linear import LinearUVLM
+
+    g = LG.load(name)
+    uv = _product_uvlm(g)
+    lin = LinearUVLM(uv, uv.solve_static(), str(g["wake_type"]), device=cuda)
+    for k in "abcd":
+        got = getattr(lin.sys, k).cpu().numpy()
+        assert got.shape == g[k].shape, k
+        assert np.abs(got - g[k]).max() <= 1e-8 * max(1.0, np.abs(g[k]).max()), k
+    x, y, _, _ = lin.run(g["u_run"], g["x0_run"])
+    assert np.allclose(x, g["x_run"], rtol=0, atol=1e-10) and np.allclose(y, g["y_run"], rtol=0, atol=1e-10)
+
+
+@pytest.mark.parametrize("wake_type,free,kernel,mirror", [("frozen", False, "epsilon", False),
+                                                           ("free", True, "cutoff", True)])
+def test_linear_model_matches_oracle_larger(cuda, wake_type, free, kernel, mirror):
+    """A 4 x 8 wing with a 6-row wake against central differences of the oracle's step."""
+    import flapjax_b200 as fj
+    from flapjax_b200 import cases
+    from flapjax_b200.linear import LinearUVLM
+    from oracle import uvlm_linear as OL
+    from oracle import uvlm_ref as R
+
+    c = cases.wing_free(m=4, n=8, m_star=6, n_steps=1, seed=3)
+    mir = (np.array([0.0, -0.3, 0.0]), np.array([0.0, 1.0, 0.0])) if mirror else None
+    rc = 1e-3
+    kw = {} if mir is None else dict(mirror_point=mir[0], mirror_normal=mir[1])
+    uv = fj.UVLM([fj.GridDiscretisation(c.m, c.n, c.m_star)], np.arange(c.n + 1), free_wake=free,
+                 kernel=fj.cutoff_kernel(rc) if kernel == "cutoff" else fj.biot_savart_epsilon, **kw)
+    uv.set_design_variables(dt=c.dt, flowfield=fj.Constant(c.u_inf, c.rho, True), zeta_b0=c.zeta_b0, hg0=c.hg0)
+    lin = LinearUVLM(uv, uv.solve_static(), wake_type, device=cuda)
+    ro = R.UVLMRef([(c.m, c.n, c.m_star)], np.arange(c.n + 1), kernel=kernel, r_cut=rc, free_wake=free, **kw)
+    ro.set_design_variables(c.dt, R.Constant(c.u_inf, c.rho), c.zeta_b0, c.hg0)
+    want = OL.LinearUVLMRef(ro, ro.solve_static(), wake_type).linearise()
+    for k in "abcd":
+        got = getattr(lin.sys, k).cpu().numpy()
+        w = getattr(want, k)
+        assert np.abs(got - w).max() <= 1e-7 * max(1.0, np.abs(w).max()), k
+
+
+def test_linear_model_follows_nonlinear_heave(cuda):
+    """A heave of 1e-4 chords: the force perturbations of the linear system equal those of
+    the nonlinear prescribed-motion solve to second order in the amplitude (cutoff kernel,
+    as the linear model's forces; no Gamma_dot filter, as the linear model has none)."""
+    import flapjax_b200 as fj
+    from flapjax_b200 import cases
+    from flapjax_b200.linear import LinearUVLM
+
+    c = cases.wing_heave(m=4, n=8, m_star=12, n_steps=24, amp=1e-4, k=0.4)
+    uv = fj.UVLM([fj.GridDiscretisation(c.m, c.n, c.m_star)], np.arange(c.n + 1), kernel=fj.cutoff_kernel(1e-4),
+                 gamma_dot_relaxation=1.0)
+    uv.set_design_variables(dt=c.dt, flowfield=fj.Constant(c.u_inf, c.rho, True), zeta_b0=c.zeta_b0, hg0=c.hg0)
+    st = uv.solve_static()
+    dy = uv.solve_prescribed_dynamic(st, c.hg_t, c.hg_dot_t)
+    lin = LinearUVLM(uv, st, "prescribed", device=cuda)
+    lay = lin.layout
+    n_t = c.hg_t.shape[0]
+    u = np.zeros((n_t, lin.n_inputs))
+    zb = lay.u["zeta_b"]
+    zbd = lay.u["zeta_b_dot"]
+    z0 = np.asarray(st.zeta_b[0])
+    for i in range(n_t):
+        zi = np.einsum("jab,ijb->ija", c.hg_t[i][:, :3, :3], c.zeta_b0) + c.hg_t[i][None, :, :3, 3]
+        zdi = np.einsum("jab,ijb->ija", c.hg_dot_t[i][:, :3, :3], c.zeta_b0) + c.hg_dot_t[i][None, :, :3, 3]
+        u[i, zb[0]:zb[1]] = (zi - z0).ravel()
+        u[i, zbd[0]:zbd[1]] = zdi.ravel()
+    _, y, _, _ = lin.run(u)
+    nv = (c.m + 1) * (c.n + 1) * 3
+    f_lin = (y[:, :nv] + y[:, nv:2 * nv]).reshape(n_t, -1, 3).sum(axis=1)
+    f_ref = np.asarray(st.f_steady[0]).sum(axis=(0, 1))
+    f_nl = (np.asarray(dy.f_steady[0]) + np.asarray(dy.f_unsteady[0])).sum(axis=(1, 2)) - f_ref
+    dz = f_nl[1:, 2]
+    assert np.abs(dz).max() > 1e-6  # the heave does load the wing
+    assert np.abs(f_lin[1:] - f_nl[1:]).max() < 1e-3 * np.abs(dz).max()

@@ -1,0 +1,141 @@
+"""The linearised UVLM on the CPU: the oracle against the reference's own linear model
+(tests/golden/linear, FD Jacobians of the reference's LinearUVLM step functions), and the
+device assembly's chain rule and block bookkeeping with CPU stand-ins for its device
+operations (tests/linear_cpu_ops.py)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from tests import linear_golden as LG
+
+
+def _oracle(g):
+    from oracle import uvlm_linear as OL
+    from oracle import uvlm_ref as R
+
+    m, n, w = (int(v) for v in g["dims"])
+    kern = {"epsilon": R.KERNEL_EPSILON, "cutoff": R.KERNEL_CUTOFF}[str(g["kernel"])]
+    mir = LG.mirror_of(g)
+    kw = {} if mir is None else dict(mirror_point=mir[0], mirror_normal=mir[1])
+    uv = R.UVLMRef([(m, n, w)], np.arange(n + 1), kernel=kern, r_cut=float(g["r_cut"]),
+                   free_wake=bool(g["free_wake"]), **kw)
+    uv.set_design_variables(float(g["dt"]), LG.flow_oracle(g), g["zeta_b0"], g["hg0"])
+    return OL.LinearUVLMRef(uv, uv.solve_static(), str(g["wake_type"]))
+
+
+@pytest.mark.parametrize("name", LG.CASES)
+def test_oracle_step_matches_reference(name):
+    g = LG.load(name)
+    lin = _oracle(g)
+    u0, x0 = lin.reference_vectors()
+    x1, y0 = lin.step(u0, x0)
+    assert np.allclose(x1, g["x_ref"], rtol=0, atol=1e-13)
+    assert np.allclose(y0, g["y_ref"], rtol=0, atol=1e-13)
+    # the nonlinear step away from the reference point
+    up, xp = u0.copy(), x0.copy()
+    for blocks, vec, kind in ((lin.u_blocks, up, "u"), (lin.x_blocks, xp, "x")):
+        off = 0
+        for k, tmpl in blocks:
+            size = sum(a.size for a in tmpl)
+            key = {"u": {"zeta_b": "zeta_b_np1_vec", "zeta_b_dot": "zeta_b_dot_np1_vec", "nu_b": "nu_b_np1_vec",
+                         "nu_w": "nu_w_np1_vec"},
+                   "x": {"gamma_b": "gamma_b_n_vec", "gamma_w": "gamma_w_n_vec", "gamma_b_nm1": "gamma_b_nm1_vec",
+                         "zeta_w": "zeta_w_n_vec", "zeta_b": "zeta_b_n_vec"}}[kind][k]
+            if f"pert_{key}" in g:
+                vec[off:off + size] = g[f"pert_{key}"]
+            off += size
+    x1p, y0p = lin.step(up, xp)
+    assert np.allclose(x1p, g["x_pert"], rtol=0, atol=1e-12)
+    assert np.allclose(y0p, g["y_pert"], rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", LG.CASES)
+def test_oracle_jacobians_match_reference(name):
+    """Central differences of the oracle's step against those of the reference's step (both
+    h = 1e-6): agreement to the differencing noise."""
+    g = LG.load(name)
+    sys_ = _oracle(g).linearise()
+    for k in "abcd":
+        assert np.abs(getattr(sys_, k) - g[k]).max() <= 1e-8 * max(1.0, np.abs(g[k]).max()), k
+    x, y = sys_.run(g["u_run"], g["x0_run"])
+    assert np.allclose(x, g["x_run"], rtol=0, atol=1e-10)
+    assert np.allclose(y, g["y_run"], rtol=0, atol=1e-10)
+
+
+@pytest.mark.parametrize("name", LG.CASES)
+def test_assembly_chain_rule_matches_reference(name):
+    """The device assembly's chain rule with the oracle standing in for the device
+    operations: A, B, C, D equal the reference's Jacobians, every block (zero blocks
+    included: the reference does not differentiate them)."""
+    from flapjax_b200 import linear as L
+    from tests.linear_cpu_ops import OracleOps
+
+    g = LG.load(name)
+    cfg = LG.config(g, LG.flow_product(g))
+    lay = L._Layout(LG.dims(g), cfg["wake_type"], True, True, True)
+    rs, ro = L._assemble(OracleOps(LG.mirror_of(g)), lay, LG.reference(g), cfg)
+    ns = lay.n_states
+    got = {"a": rs[:, :ns], "b": rs[:, ns:], "c": ro[:, :ns], "d": ro[:, ns:]}
+    for k in "abcd":
+        want = g[k]
+        assert got[k].shape == want.shape, k
+        assert np.abs(got[k].numpy() - want).max() <= 1e-8 * max(1.0, np.abs(want).max()), k
+
+
+def test_layout_follows_reference_slices():
+    from flapjax_b200 import linear as L
+
+    lay = L._Layout([(2, 3, 4), (1, 2, 2)], "prescribed", True, False, True)
+    nb, nw, nvb, nvw = 6 + 2, 12 + 4, 12 + 6, 20 + 9
+    assert [k for k, _ in lay.x_blocks] == ["gamma_b", "gamma_w", "gamma_b_nm1", "zeta_w", "zeta_b"]
+    assert lay.x["zeta_w"] == (nb + nw + nb, nb + nw + nb + 3 * nvw)
+    assert [k for k, _ in lay.u_blocks] == ["zeta_b", "zeta_b_dot", "nu_b"]
+    assert lay.n_inputs == 9 * nvb and lay.n_outputs == 6 * nvb
+    frozen = L._Layout([(2, 3, 4)], "frozen", False, False, False)
+    assert [k for k, _ in frozen.x_blocks] == ["gamma_b", "gamma_w"]
+    assert [k for k, _ in frozen.y_blocks] == ["f_steady"]
+
+
+def test_diff_lists_follow_compute_jacobians():
+    """The differentiated arguments per residual, as the reference's compute_jacobians
+    lists them (the golden generator records the reference's own lists)."""
+    from flapjax_b200 import linear as L
+    from oracle import uvlm_linear as OL
+
+    for wt in ("frozen", "prescribed", "free"):
+        for flags in ((True, True, True), (False, True, False), (True, False, True)):
+            assert L._diff_lists(wt, *flags) == OL.diff_lists(wt, *flags)
+    assert "x:zeta_b" not in L._diff_lists("free", True, True, True)["zeta_w"]
+    assert "x:gamma_b" in L._diff_lists("free", True, True, True)["zeta_w"]
+    assert "x:gamma_b" not in L._diff_lists("prescribed", True, True, True)["zeta_w"]
+
+
+def test_linear_system_run_and_remove_u_np1():
+    """LinearSystem.run / remove_u_np1 (utils/linear.py:714-822) against the oracle's
+    restatement, on CPU tensors."""
+    from flapjax_b200.linear import LinearSystem
+    from oracle.uvlm_linear import LinearSystemRef
+
+    rng = np.random.default_rng(0)
+    a = 0.3 * rng.normal(size=(7, 7))
+    b, c, d = rng.normal(size=(7, 4)), rng.normal(size=(5, 7)), rng.normal(size=(5, 4))
+    u, x0 = rng.normal(size=(9, 4)), rng.normal(size=7)
+    t = lambda z: torch.as_tensor(z)
+    ours = LinearSystem(t(a), t(b), t(c), t(d), 0.1)
+    ref = LinearSystemRef(a, b, c, d, 0.1)
+    for removed in (False, True):
+        if removed:
+            ours.remove_u_np1()
+            ref.remove_u_np1()
+        x, y = ours.run(u, x0)
+        xr, yr = ref.run(u, x0)
+        assert np.allclose(x.numpy(), xr, rtol=1e-13, atol=1e-13) and np.allclose(y.numpy(), yr, rtol=1e-13,
+                                                                                   atol=1e-13)
+    with pytest.warns(UserWarning):
+        ours.remove_u_np1()
+    with pytest.raises(ValueError):
+        ours.run(u[:, :3])
+    with pytest.raises(ValueError):
+        ours.run(u, x0[:3])
