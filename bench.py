@@ -17,6 +17,8 @@ fp64_gpu  the plain FP64 path on the same steps, and the mixed path's CL/CD erro
 autotune  the split counts of the step's three Biot-Savart sums, timed on the device before
         the timed regions (fj_autotune_vind) for both precisions, against the wave-filling
         rule the launches use untuned.
+--linear  the linearised UVLM: assembly time of A, B, C, D on the device and the linear
+        system's time march (C1 and C3 wings).
 factorisation  the mixed solve's FP32 LU + FP32 inverse of this workload's AIC through the
         tensor-core path (tcgen05 TF32, three-pass split; the default) and through the FP32
         CUDA-core path, and the tensor-core GEMM alone at the LU's trailing-update shape
@@ -65,6 +67,9 @@ def parse():
     ap.add_argument("--adjoint-steps", type=int, default=1000)
     ap.add_argument("--residual", action="store_true",
                     help="only the time-step residual VJP (timestep_residual, config-3 wing) on the device")
+    ap.add_argument("--linear", action="store_true",
+                    help="only the linearised UVLM leg: A, B, C, D about the static solution (C1 and C3 wings, "
+                         "frozen and prescribed wakes) and the linear system's time march")
     ap.add_argument("--factor", action="store_true",
                     help="only the factorisation leg (mixed solve's FP32 LU + inverse, tensor cores vs CUDA cores)")
     ap.add_argument("--configs", action="store_true",
@@ -331,6 +336,10 @@ def main():
         if rank == 0:
             print(json.dumps({"residual_vjp": residual_bench(torch)}))
         return 0
+    if args.linear:
+        if rank == 0:
+            print(json.dumps({"linear": linear_bench(torch, small=args.small)}))
+        return 0
     if args.factor:
         case = workload(args, 2)
         _, dcf = make_case(case, "mixed", 2)
@@ -536,11 +545,16 @@ def factor_bench(dc, case, torch):
         if it >= 3:
             times.append(e0.elapsed_time(e1))
     t = float(np.median(times))
-    tf32_peak = measured_peaks().get("bf16_tflops", 1590.0) / 2
+    peaks = measured_peaks()
+    if "bf16_tflops" in peaks:
+        tf32_peak = peaks["bf16_tflops"] / 2
+        src = "half of measured MEASURED_PEAKS.json bf16_tflops (dense TF32 runs at half the bf16 rate)"
+    else:
+        tf32_peak = 1590.0 / 2
+        src = "half of the fallback 1590 TFLOP/s bf16 (MEASURED_PEAKS.json absent; dense TF32 is half bf16)"
     achieved = 3 * 2.0 * g * g * 128 / (t * 1e-3) / 1e12
     out["gemm"] = {"shape": [g, g, 128], "passes": 3, "ms": t, "tflops_tf32_issued": achieved,
-                   "tf32_peak_tflops": tf32_peak, "frac": achieved / tf32_peak,
-                   "peak_source": "half of MEASURED_PEAKS.json bf16_tflops (dense TF32 runs at half the bf16 rate)"}
+                   "tf32_peak_tflops": tf32_peak, "frac": achieved / tf32_peak, "peak_source": src}
     return out
 
 
@@ -575,6 +589,51 @@ def residual_bench(torch):
         times.append(time.perf_counter() - t0)
     return {"workload": "config-3 wing 12x64, W=100, epsilon kernel, slot 2", "residual_size": int(r.size),
             "ms_per_vjp": 1e3 * float(np.median(times))}
+
+
+def linear_bench(torch, small=False):
+    """The linearised UVLM (aero/linear/linear_uvlm.py) about the static solution: wall time
+    of the assembly of A, B, C, D on the device (after one warm-up assembly), and the linear
+    system's time march (x_n = A x_{n-1} + B u_n, y_n = C x_n + D u_n) over 1000 steps of
+    seeded input perturbations, device-timed with CUDA events.  small: the C1 frozen-wake
+    line only, with a 20-step march (the case the launch-list profile captures)."""
+    import flapjax_b200 as fj
+    from flapjax_b200 import cases
+    from flapjax_b200.linear import LinearUVLM
+
+    out = []
+    lines = (("C1 wing 8x32, W=64", (8, 32, 64), "frozen"), ("C1 wing 8x32, W=64", (8, 32, 64), "prescribed"),
+             ("C3 wing 12x64, W=100", (12, 64, 100), "frozen"))
+    for label, (m, n, w), wt in lines[:1] if small else lines:
+        c = cases.wing_heave(m=m, n=n, m_star=w, n_steps=1)
+        uv = fj.UVLM([fj.GridDiscretisation(m, n, w)], np.arange(n + 1), kernel=fj.biot_savart_epsilon)
+        uv.set_design_variables(dt=c.dt, flowfield=fj.Constant(c.u_inf, c.rho, True), zeta_b0=c.zeta_b0, hg0=c.hg0)
+        st = uv.solve_static()
+        lin = LinearUVLM(uv, st, wt)
+        times = []
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            sys_ = lin.linearise()
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        rng = np.random.default_rng(0)
+        n_t = 20 if small else 1000
+        u = torch.as_tensor(1e-4 * rng.normal(size=(n_t, lin.n_inputs))).cuda()
+        sys_.run(u[:10])
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sys_.run(u)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out.append({"workload": f"{label}, {wt} wake, epsilon kernel", "n_states": lin.n_states,
+                    "n_inputs": lin.n_inputs, "n_outputs": lin.n_outputs, "linearise_s": min(times),
+                    "matrix_bytes": 8 * (lin.n_states + lin.n_outputs) * (lin.n_states + lin.n_inputs),
+                    "run_steps_per_s": n_t / (ms * 1e-3)})
+        del lin, sys_, u
+        torch.cuda.empty_cache()
+    return out
 
 
 def measured_peaks():

@@ -19,8 +19,8 @@
 // the warp so the stores coalesce.
 //
 // fj_lu_solve_many: B <- A^-1 B for many right-hand sides (columns of a row-major B) from
-// the getrf factors of fj_lu_factor: thread per column, forward and backward substitution
-// with the factor rows read uniformly across the warp.
+// the getrf factors of fj_lu_factor: blocked forward and backward substitution, 32-column
+// tiles per CTA, the off-diagonal updates as shared-memory tile products.
 #include <algorithm>
 
 #include "fj_bs.cuh"
@@ -225,26 +225,118 @@ __global__ void perm_from_piv_kernel(const int32_t* __restrict__ piv, int n, int
     }
 }
 
-__global__ void __launch_bounds__(kJacBlock) lu_solve_many_kernel(const double* __restrict__ lu, int n,
-                                                                  const int32_t* __restrict__ perm,
-                                                                  double* __restrict__ b, int64_t nrhs, int64_t ldb,
-                                                                  double* __restrict__ w) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nrhs) return;
-    for (int i = 0; i < n; ++i) w[(int64_t)i * nrhs + c] = b[(int64_t)perm[i] * ldb + c];
-    for (int i = 1; i < n; ++i) {  // unit lower
-        const double* li = lu + (int64_t)i * n;
-        double acc = w[(int64_t)i * nrhs + c];
-        for (int j = 0; j < i; ++j) acc -= li[j] * w[(int64_t)j * nrhs + c];
-        w[(int64_t)i * nrhs + c] = acc;
+// Blocked substitution for many right-hand sides.  CTA = 256 threads on a tile of 32
+// columns; rows in blocks of 32.  For each row block: subtract the already-solved rows
+// (a 32 x 32 x k0 product, staged through shared memory in 32 x 32 chunks of the factor
+// and of the solved rows), then solve the block's own triangle in shared memory.  Thread
+// (c = lane, y = warp) owns rows y, y+8, y+16, y+24 of the block in column c.
+constexpr int kSolveCols = 32, kSolveRows = 32, kSolveThreads = 256;
+
+__device__ __forceinline__ void tile_update(const double* __restrict__ lu, int n, const double* __restrict__ w,
+                                            int64_t nrhs, int64_t col, bool col_ok, int i0, int k0, int k1,
+                                            double (*ls)[kSolveRows + 1], double (*ws)[kSolveCols + 1],
+                                            double acc[4]) {
+    const int c = threadIdx.x & 31, y = threadIdx.x >> 5;
+    for (int kb = k0; kb < k1; kb += kSolveRows) {
+        const int kw = min(kSolveRows, k1 - kb);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = y + 8 * q;
+            ls[r][c] = (i0 + r < n && c < kw) ? lu[(int64_t)(i0 + r) * n + kb + c] : 0.0;
+            ws[r][c] = (r < kw && col_ok) ? w[(int64_t)(kb + r) * nrhs + col] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int kk = 0; kk < kSolveRows; ++kk) {
+            const double x = ws[kk][c];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[q] -= ls[y + 8 * q][kk] * x;
+        }
+        __syncthreads();
     }
-    for (int i = n - 1; i >= 0; --i) {  // upper
-        const double* ui = lu + (int64_t)i * n;
-        double acc = w[(int64_t)i * nrhs + c];
-        for (int j = i + 1; j < n; ++j) acc -= ui[j] * w[(int64_t)j * nrhs + c];
-        acc /= ui[i];
-        w[(int64_t)i * nrhs + c] = acc;
-        b[(int64_t)i * ldb + c] = acc;
+}
+
+__global__ void __launch_bounds__(kSolveThreads) lu_solve_many_kernel(const double* __restrict__ lu, int n,
+                                                                      const int32_t* __restrict__ perm,
+                                                                      double* __restrict__ b, int64_t nrhs,
+                                                                      int64_t ldb, double* __restrict__ w) {
+    __shared__ double ls[kSolveRows][kSolveRows + 1];
+    __shared__ double ws[kSolveRows][kSolveCols + 1];
+    const int c = threadIdx.x & 31, y = threadIdx.x >> 5;
+    const int64_t col = (int64_t)blockIdx.x * kSolveCols + c;
+    const bool col_ok = col < nrhs;
+    // gather the permuted right-hand sides: w[i] = b[perm[i]]
+    if (col_ok)
+        for (int i = y; i < n; i += 8) w[(int64_t)i * nrhs + col] = b[(int64_t)perm[i] * ldb + col];
+    __syncthreads();
+    // forward: unit lower
+    for (int i0 = 0; i0 < n; i0 += kSolveRows) {
+        const int rb = min(kSolveRows, n - i0);
+        double acc[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = y + 8 * q;
+            acc[q] = (r < rb && col_ok) ? w[(int64_t)(i0 + r) * nrhs + col] : 0.0;
+        }
+        tile_update(lu, n, w, nrhs, col, col_ok, i0, 0, i0, ls, ws, acc);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = y + 8 * q;
+            ws[r][c] = acc[q];
+            ls[r][c] = (r < rb && c < rb) ? lu[(int64_t)(i0 + r) * n + i0 + c] : 0.0;
+        }
+        __syncthreads();
+        for (int rr = 0; rr + 1 < rb; ++rr) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = y + 8 * q;
+                if (r > rr && r < rb) ws[r][c] -= ls[r][rr] * ws[rr][c];
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = y + 8 * q;
+            if (r < rb && col_ok) w[(int64_t)(i0 + r) * nrhs + col] = ws[r][c];
+        }
+        __syncthreads();
+    }
+    // backward: upper, with the diagonal
+    for (int i0 = ((n - 1) / kSolveRows) * kSolveRows; i0 >= 0; i0 -= kSolveRows) {
+        const int rb = min(kSolveRows, n - i0);
+        double acc[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = y + 8 * q;
+            acc[q] = (r < rb && col_ok) ? w[(int64_t)(i0 + r) * nrhs + col] : 0.0;
+        }
+        tile_update(lu, n, w, nrhs, col, col_ok, i0, i0 + rb, n, ls, ws, acc);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = y + 8 * q;
+            ws[r][c] = acc[q];
+            ls[r][c] = (r < rb && c < rb) ? lu[(int64_t)(i0 + r) * n + i0 + c] : 1.0;
+        }
+        __syncthreads();
+        for (int rr = rb - 1; rr >= 0; --rr) {
+            if (y == (rr & 7)) ws[rr][c] /= ls[rr][rr];
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = y + 8 * q;
+                if (r < rr) ws[r][c] -= ls[r][rr] * ws[rr][c];
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = y + 8 * q;
+            if (r < rb && col_ok) {
+                w[(int64_t)(i0 + r) * nrhs + col] = ws[r][c];
+                b[(int64_t)(i0 + r) * ldb + col] = ws[r][c];
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -369,7 +461,7 @@ int fj_lu_solve_many(const double* d_lu, int n, const int32_t* d_piv, double* d_
     int32_t* perm = (int32_t*)base;
     double* w = (double*)(base + ((size_t)n * sizeof(int32_t) + 255) / 256 * 256);
     perm_from_piv_kernel<<<1, 32, 0, s>>>(d_piv, n, perm);
-    lu_solve_many_kernel<<<(unsigned)((nrhs + kJacBlock - 1) / kJacBlock), kJacBlock, 0, s>>>(d_lu, n, perm, d_b,
+    lu_solve_many_kernel<<<(unsigned)((nrhs + kSolveCols - 1) / kSolveCols), kSolveThreads, 0, s>>>(d_lu, n, perm, d_b,
                                                                                              nrhs, ldb, w);
     note_launch(2);
     FJ_LAUNCH_CHECK("fj_lu_solve_many");

@@ -60,3 +60,31 @@ def reference(g):
 def dims(g):
     m, n, w = (int(v) for v in g["dims"])
     return [(m, n, w)]
+
+
+def two_surfaces():
+    """A wing (2 x 3, 3 wake rows) and a tail (2 x 2, 2 wake rows) on separate node sets:
+    (dims, zeta_b0 per surface, dof mappings, hg0, wing case)."""
+    from flapjax_b200 import cases
+
+    wing = cases.wing_heave(m=2, n=3, m_star=3, n_steps=1)
+    tail = np.zeros((3, 3, 3))
+    tail[..., 0] = (np.linspace(0.0, 0.5, 3) - 0.125)[:, None] + 3.0
+    tail[..., 2] = 0.2
+    hg_tail = np.zeros((3, 4, 4))
+    hg_tail[:, :3, :3] = np.eye(3)
+    hg_tail[:, 1, 3] = np.linspace(0.0, 1.5, 3)
+    hg_tail[:, 3, 3] = 1.0
+    hg0 = np.concatenate([wing.hg0, hg_tail])
+    return [(2, 3, 3), (2, 2, 2)], [wing.zeta_b0, tail], [np.arange(4), np.arange(4, 7)], hg0, wing
+
+
+def two_surface_oracle(wake_type, free, kernel, r_cut=1e-3):
+    from oracle import uvlm_linear as OL
+    from oracle import uvlm_ref as R
+
+    dims, z0, dofs, hg0, wing = two_surfaces()
+    uv = R.UVLMRef(dims, dofs, kernel=kernel, r_cut=r_cut, free_wake=free)
+    uv.set_design_variables(wing.dt, R.Constant(wing.u_inf, wing.rho), z0, hg0)
+    st = uv.solve_static()
+    return uv, st, OL.LinearUVLMRef(uv, st, wake_type)

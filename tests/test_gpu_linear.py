@@ -149,6 +149,26 @@ def test_linear_model_matches_oracle_larger(cuda, wake_type, free, kernel, mirro
         assert np.abs(got - w).max() <= 1e-7 * max(1.0, np.abs(w).max()), k
 
 
+@pytest.mark.parametrize("wake_type,free,kernel", [("frozen", False, "epsilon"), ("free", True, "cutoff")])
+def test_linear_model_two_surfaces(cuda, wake_type, free, kernel):
+    """A wing and a tail: cross-surface blocks and offsets against the oracle."""
+    import flapjax_b200 as fj
+    from flapjax_b200.linear import LinearUVLM
+
+    _, _, lin_ref = LG.two_surface_oracle(wake_type, free, kernel)
+    want = lin_ref.linearise()
+    dims, z0, dofs, hg0, wing = LG.two_surfaces()
+    uv = fj.UVLM([fj.GridDiscretisation(*d) for d in dims], dofs, free_wake=free,
+                 kernel=fj.cutoff_kernel(1e-3) if kernel == "cutoff" else fj.biot_savart_epsilon)
+    uv.set_design_variables(dt=wing.dt, flowfield=fj.Constant(wing.u_inf, wing.rho, True), zeta_b0=z0, hg0=hg0)
+    lin = uv.linearise(uv.solve_static(), wake_type)
+    assert isinstance(lin, LinearUVLM)
+    for k in "abcd":
+        got = getattr(lin.sys, k).cpu().numpy()
+        w = getattr(want, k)
+        assert np.abs(got - w).max() <= 1e-7 * max(1.0, np.abs(w).max()), k
+
+
 def test_linear_model_follows_nonlinear_heave(cuda):
     """A heave of 1e-4 chords: the force perturbations of the linear system equal those of
     the nonlinear prescribed-motion solve to second order in the amplitude (cutoff kernel,

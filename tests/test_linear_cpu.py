@@ -84,6 +84,30 @@ def test_assembly_chain_rule_matches_reference(name):
         assert np.abs(got[k].numpy() - want).max() <= 1e-8 * max(1.0, np.abs(want).max()), k
 
 
+def test_assembly_two_surfaces_against_oracle():
+    """Two surfaces (free wake, cutoff kernel): the cross-surface blocks and every offset
+    of the assembly against central differences of the oracle's step."""
+    from flapjax_b200 import _lib
+    from flapjax_b200 import linear as L
+    from flapjax_b200.flowfields import Constant
+    from tests.linear_cpu_ops import OracleOps
+
+    uv, st, lin = LG.two_surface_oracle("free", True, "cutoff")
+    want = lin.linearise()
+    dims, *_, wing = LG.two_surfaces()
+    ref = {k: [a[0] for a in getattr(st, k)] for k in ("zeta_b", "zeta_w", "gamma_b", "gamma_w")}
+    cfg = {"wake_type": "free", "free_wake": True, "kernel": _lib.FJ_KERNEL_CUTOFF, "r_cut": 1e-3,
+           "force_r_cut": 1e-3, "dt": wing.dt, "rho": wing.rho, "flowfield": Constant(wing.u_inf, wing.rho, True),
+           "t": 0.0, "bound_upwash": True, "wake_upwash": True, "unsteady_force": True}
+    lay = L._Layout(dims, "free", True, True, True)
+    rs, ro = L._assemble(OracleOps(None), lay, ref, cfg)
+    ns = lay.n_states
+    got = {"a": rs[:, :ns], "b": rs[:, ns:], "c": ro[:, :ns], "d": ro[:, ns:]}
+    for k in "abcd":
+        w = getattr(want, k)
+        assert np.abs(got[k].numpy() - w).max() <= 1e-8 * max(1.0, np.abs(w).max()), k
+
+
 def test_layout_follows_reference_slices():
     from flapjax_b200 import linear as L
 
