@@ -169,6 +169,30 @@ def test_linear_model_two_surfaces(cuda, wake_type, free, kernel):
         assert np.abs(got - w).max() <= 1e-7 * max(1.0, np.abs(w).max()), k
 
 
+@pytest.mark.parametrize("wake_type,bound_upwash,wake_upwash,unsteady,m_star",
+                         [("frozen", True, True, True, 0), ("prescribed", False, True, False, 2)])
+def test_linear_model_options(cuda, wake_type, bound_upwash, wake_upwash, unsteady, m_star):
+    """No wake rows, and the upwash inputs / unsteady force switched off, against the oracle."""
+    import flapjax_b200 as fj
+    from flapjax_b200 import cases
+    from flapjax_b200.linear import LinearUVLM
+    from oracle import uvlm_linear as OL
+    from oracle import uvlm_ref as R
+
+    c = cases.wing_heave(m=3, n=4, m_star=m_star, n_steps=1)
+    uv = fj.UVLM([fj.GridDiscretisation(c.m, c.n, c.m_star)], np.arange(c.n + 1), kernel=fj.biot_savart_epsilon)
+    uv.set_design_variables(dt=c.dt, flowfield=fj.Constant(c.u_inf, c.rho, True), zeta_b0=c.zeta_b0, hg0=c.hg0)
+    lin = LinearUVLM(uv, uv.solve_static(), wake_type, bound_upwash, wake_upwash, unsteady, device=cuda)
+    ro = R.UVLMRef([(c.m, c.n, c.m_star)], np.arange(c.n + 1))
+    ro.set_design_variables(c.dt, R.Constant(c.u_inf, c.rho), c.zeta_b0, c.hg0)
+    want = OL.LinearUVLMRef(ro, ro.solve_static(), wake_type, bound_upwash, wake_upwash, unsteady).linearise()
+    for k in "abcd":
+        got = getattr(lin.sys, k).cpu().numpy()
+        w = getattr(want, k)
+        assert got.shape == w.shape, k
+        assert np.abs(got - w).max() <= 1e-7 * max(1.0, np.abs(w).max()), k
+
+
 def test_linear_model_follows_nonlinear_heave(cuda):
     """A heave of 1e-4 chords: the force perturbations of the linear system equal those of
     the nonlinear prescribed-motion solve to second order in the amplitude (cutoff kernel,

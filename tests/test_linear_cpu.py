@@ -108,6 +108,39 @@ def test_assembly_two_surfaces_against_oracle():
         assert np.abs(got[k].numpy() - w).max() <= 1e-8 * max(1.0, np.abs(w).max()), k
 
 
+@pytest.mark.parametrize("wake_type,bound_upwash,wake_upwash,unsteady,m_star",
+                         [("frozen", False, False, False, 3), ("prescribed", True, False, True, 3),
+                          ("frozen", True, True, True, 0), ("prescribed", False, True, False, 0),
+                          ("free", True, True, True, 1)])
+def test_assembly_options_against_oracle(wake_type, bound_upwash, wake_upwash, unsteady, m_star):
+    """The upwash inputs and the unsteady force switched off, and wakes of zero and one
+    row: the assembly against central differences of the oracle's step (2 x 2 wing)."""
+    from flapjax_b200 import _lib, cases
+    from flapjax_b200 import linear as L
+    from flapjax_b200.flowfields import Constant
+    from oracle import uvlm_linear as OL
+    from oracle import uvlm_ref as R
+    from tests.linear_cpu_ops import OracleOps
+
+    c = cases.wing_heave(m=2, n=2, m_star=m_star, n_steps=1)
+    uv = R.UVLMRef([(c.m, c.n, c.m_star)], np.arange(c.n + 1))
+    uv.set_design_variables(c.dt, R.Constant(c.u_inf, c.rho), c.zeta_b0, c.hg0)
+    st = uv.solve_static()
+    want = OL.LinearUVLMRef(uv, st, wake_type, bound_upwash, wake_upwash, unsteady).linearise()
+    ref = {k: [a[0] for a in getattr(st, k)] for k in ("zeta_b", "zeta_w", "gamma_b", "gamma_w")}
+    cfg = {"wake_type": wake_type, "free_wake": False, "kernel": _lib.FJ_KERNEL_EPSILON, "r_cut": 1e-4,
+           "force_r_cut": 1e-4, "dt": c.dt, "rho": c.rho, "flowfield": Constant(c.u_inf, c.rho, True), "t": 0.0,
+           "bound_upwash": bound_upwash, "wake_upwash": wake_upwash, "unsteady_force": unsteady}
+    lay = L._Layout([(c.m, c.n, c.m_star)], wake_type, bound_upwash, wake_upwash, unsteady)
+    rs, ro = L._assemble(OracleOps(None), lay, ref, cfg)
+    ns = lay.n_states
+    got = {"a": rs[:, :ns], "b": rs[:, ns:], "c": ro[:, :ns], "d": ro[:, ns:]}
+    for k in "abcd":
+        w = getattr(want, k)
+        assert got[k].shape == w.shape, k
+        assert np.abs(got[k].numpy() - w).max() <= 1e-8 * max(1.0, np.abs(w).max()), k
+
+
 def test_layout_follows_reference_slices():
     from flapjax_b200 import linear as L
 
