@@ -46,6 +46,8 @@ from __future__ import annotations
 
 import ctypes as C
 import warnings
+from collections.abc import Callable
+from dataclasses import dataclass
 
 import numpy as np
 
@@ -55,6 +57,55 @@ from .kernels import R_CUTOFF
 from .runtime import device_of
 
 WAKE_TYPES = ("frozen", "prescribed", "free")
+
+
+@dataclass
+class LinearInputProjection:
+    """Lattice coordinates and velocities from a lower-dimensional input space, e.g. beam
+    coordinates (aero/linear/linear_uvlm.py:48-63).  ``to_zeta(**{name: vec})`` returns
+    the total ``(zeta_b_vec, zeta_b_dot_vec)`` (surfaces concatenated, raveled).  The
+    reference differentiates ``to_zeta`` with jax; here ``jacobian(**{name: vec})`` gives
+    ``(d zeta_b / d q, d zeta_b_dot / d q)`` over the concatenated arguments q when it is
+    supplied, else central differences of ``to_zeta`` (step ``fd_step``) at ``arg_refs``."""
+
+    arg_names: tuple
+    arg_sizes: tuple
+    arg_refs: tuple
+    to_zeta: Callable
+    jacobian: Callable | None = None
+    fd_step: float = 1e-6
+
+
+@dataclass
+class LinearOutputProjection:
+    """Forces onto one output space (aero/linear/linear_uvlm.py:65-78):
+    ``to_output(f_steady_vec, f_unsteady_vec | None) -> vector of length size``.  Its
+    Jacobian is ``jacobian(f_steady_vec, f_unsteady_vec)`` -> ``(d out / d f_steady,
+    d out / d f_unsteady or None)`` when supplied, else central differences (step
+    ``fd_step``) at the reference forces."""
+
+    name: str
+    size: int
+    to_output: Callable
+    jacobian: Callable | None = None
+    fd_step: float = 1e-6
+
+
+def _fd_columns(fun, x0, h):
+    """Central-difference Jacobian of fun (vector -> tuple of vectors) at x0: one matrix
+    per output."""
+    x0 = np.asarray(x0, np.float64)
+    cols = None
+    for j in range(x0.size):
+        xp, xm = x0.copy(), x0.copy()
+        xp[j] += h
+        xm[j] -= h
+        fp, fm = fun(xp), fun(xm)
+        if cols is None:
+            cols = [np.zeros((np.size(a), x0.size)) for a in fp]
+        for c, a, b in zip(cols, fp, fm):
+            c[:, j] = (np.ravel(a) - np.ravel(b)) / (2 * h)
+    return cols
 
 
 # ---------------------------------------------------------------------------------------
@@ -728,6 +779,84 @@ def _steady_force_rows(ops, lay, cfg, Zb, Zw, gb, gw, tZb, tZw, tgb, tgw, lists)
     return out
 
 
+def _input_jacobians(proj: LinearInputProjection, nz: int):
+    """(d zeta_b / d q, d zeta_b_dot / d q), each (nz, len q), of an input projection."""
+    sizes = [int(v) for v in proj.arg_sizes]
+    if len(proj.arg_names) != len(sizes) or len(proj.arg_refs) != len(sizes):
+        raise ValueError("input projection: arg_names, arg_sizes and arg_refs must have the same length")
+    q0 = np.concatenate([np.ravel(np.asarray(r, np.float64)) for r in proj.arg_refs])
+    if q0.size != sum(sizes):
+        raise ValueError(f"input projection: arg_refs hold {q0.size} values, arg_sizes sum to {sum(sizes)}")
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+
+    def split(q):
+        return {n: q[offs[i]:offs[i + 1]] for i, n in enumerate(proj.arg_names)}
+
+    if proj.jacobian is not None:
+        jzb, jzbd = (np.asarray(j, np.float64) for j in proj.jacobian(**split(q0)))
+    else:
+        jzb, jzbd = _fd_columns(lambda q: proj.to_zeta(**split(q)), q0, proj.fd_step)
+    if jzb.shape != (nz, q0.size) or jzbd.shape != (nz, q0.size):
+        raise ValueError(f"input projection: Jacobians must be ({nz}, {q0.size}), got {jzb.shape}, {jzbd.shape}")
+    return jzb, jzbd
+
+
+def _output_jacobians(proj: LinearOutputProjection, fs0, fu0):
+    """(d out / d f_steady, d out / d f_unsteady or None) of an output projection at the
+    reference forces fs0, fu0 (fu0 None without the unsteady force)."""
+    if proj.jacobian is not None:
+        jfs, jfu = proj.jacobian(fs0, fu0)
+        jfs = np.asarray(jfs, np.float64)
+        jfu = None if jfu is None else np.asarray(jfu, np.float64)
+    else:
+        n = fs0.size
+        if fu0 is None:
+            (jfs,) = _fd_columns(lambda f: (proj.to_output(f, None),), fs0, proj.fd_step)
+            jfu = None
+        else:
+            (j,) = _fd_columns(lambda f: (proj.to_output(f[:n], f[n:]),), np.concatenate([fs0, fu0]), proj.fd_step)
+            jfs, jfu = j[:, :n], j[:, n:]
+    if jfs.shape != (int(proj.size), fs0.size):
+        raise ValueError(f"output projection: Jacobian must be ({proj.size}, {fs0.size}), got {jfs.shape}")
+    return jfs, jfu
+
+
+def _project(torch, lay, a, b, c, d, jin=None, jout=None):
+    """The reference's projections (:631-725) applied to the unprojected A, B, C, D.
+
+    Input (jin = (J_zeta_b, J_zeta_b_dot)): the inputs become [q, nu_b, nu_w]; every
+    derivative with respect to zeta_b and zeta_b_dot of step n+1 chains through J, and so
+    does the bound circulation's derivative with respect to zeta_b of step n (a state of
+    the prescribed and free wake types, which the projection also sets); those state
+    columns of A become zero.  Output (jout = (J_f_steady, J_f_unsteady)): the outputs
+    become J_fs f_steady + J_fu f_unsteady."""
+    if jin is not None:
+        jzb, jzbd = jin
+        zb, zbd = lay.u["zeta_b"], lay.u["zeta_b_dot"]
+
+        def project(m_state, m_in):
+            q = m_in[:, zb[0]:zb[1]] @ jzb + m_in[:, zbd[0]:zbd[1]] @ jzbd
+            if "zeta_b" in lay.x:
+                z0, z1 = lay.x["zeta_b"]
+                q = q + m_state[:, z0:z1] @ jzb
+                m_state[:, z0:z1] = 0.0
+            rest = [m_in[:, lay.u[k][0]:lay.u[k][1]] for k in ("nu_b", "nu_w") if k in lay.u]
+            return torch.cat([q, *rest], dim=1)
+
+        a, c = a.clone(), c.clone()
+        b = project(a, b)
+        d = project(c, d)
+    if jout is not None:
+        jfs, jfu = jout
+        fs, fu = lay.y["f_steady"], lay.y.get("f_unsteady")
+        c_new, d_new = jfs @ c[fs[0]:fs[1]], jfs @ d[fs[0]:fs[1]]
+        if fu is not None and jfu is not None:
+            c_new = c_new + jfu @ c[fu[0]:fu[1]]
+            d_new = d_new + jfu @ d[fu[0]:fu[1]]
+        c, d = c_new, d_new
+    return a, b, c, d
+
+
 # ---------------------------------------------------------------------------------------
 # the public class
 # ---------------------------------------------------------------------------------------
@@ -803,13 +932,29 @@ class LinearUVLM:
                 "t": float(np.asarray(self._reference.t).ravel()[0]), "bound_upwash": self.bound_upwash,
                 "wake_upwash": self.wake_upwash, "unsteady_force": self.unsteady_force}
 
-    def linearise(self) -> LinearSystem:
-        """A, B, C, D about the reference (:727-829)."""
+    def linearise(self, batch_size=None, *, input_projection: LinearInputProjection | None = None,
+                  output_projection: LinearOutputProjection | None = None) -> LinearSystem:
+        """A, B, C, D about the reference (:727-829).  With an input projection the inputs
+        are [projected arguments, nu_b, nu_w]: every residual's derivatives with respect to
+        zeta_b and zeta_b_dot of step n+1 (and, for the bound circulation of the prescribed
+        and free wake types, zeta_b of step n, which the projection also sets) chain
+        through the projection's Jacobian, and the zeta_b state columns of A are zero
+        (:631-698).  With an output projection the outputs are the projected forces
+        (:700-725).  ``batch_size`` is accepted for the reference's signature."""
         lay = self.layout
         r_state, r_out = _assemble(self._ops, lay, self._ref, self._config())
         ns = lay.n_states
-        return LinearSystem(r_state[:, :ns].contiguous(), r_state[:, ns:].contiguous(), r_out[:, :ns].contiguous(),
-                            r_out[:, ns:].contiguous(), self.dt)
+        jin = jout = None
+        if input_projection is not None:
+            jin = tuple(self._ops.tensor(j) for j in _input_jacobians(input_projection, 3 * lay.NVB))
+        if output_projection is not None:
+            fs0 = np.concatenate([np.ravel(x) for x in self._ref["f_steady"]])
+            fu0 = np.concatenate([np.ravel(x) for x in self._ref["f_unsteady"]]) if self.unsteady_force else None
+            jout = tuple(None if j is None else self._ops.tensor(j)
+                         for j in _output_jacobians(output_projection, fs0, fu0))
+        a, b, c, d = _project(self._ops.torch, lay, r_state[:, :ns], r_state[:, ns:], r_out[:, :ns], r_out[:, ns:],
+                              jin, jout)
+        return LinearSystem(a.contiguous(), b.contiguous(), c.contiguous(), d.contiguous(), self.dt)
 
     # -- vectors ------------------------------------------------------------------------
     def reference_states(self) -> np.ndarray:

@@ -406,6 +406,73 @@ def run_linear_case(ref, name, c, wake_type, free_wake=False, kernel="epsilon", 
         ref.utils.R_CUTOFF = saved_r
 
 
+def run_linear_projected_case(ref, name, c, wake_type, ea_x=0.0, h=1e-6, seed=0):
+    """The reference's linear model with an input projection (rigid heave and pitch) and an
+    output projection (lift and pitching moment): compute_jacobians(input_projection=,
+    output_projection=) supplies the projected residual functions and their arguments;
+    central differences of those functions (h = 1e-6) in place of jacrev, assembled as
+    linearise does with projections (aero/linear/linear_uvlm.py:727-829)."""
+    if ONLY and name not in ONLY:
+        return
+    jnp = ref.jnp
+    from flapjax.aero.linear.linear_uvlm import LinearInputProjection, LinearOutputProjection, LinearUVLM
+    from flapjax.algebra.array_utils import construct_named_block_jacobian
+
+    uv = ref.UVLM(grid_shapes=[ref.GridDiscretisation(c.m, c.n, c.m_star)], dof_mapping=[jnp.arange(c.n + 1)],
+                  kernel=ref.utils.biot_savart_epsilon)
+    uv.set_design_variables(dt=float(c.dt), flowfield=ref.Constant(jnp.array(c.u_inf), c.rho, True),
+                            zeta_b0=[jnp.array(c.zeta_b0)], hg0=jnp.array(c.hg0))
+    st = uv.solve_static()
+    lin = LinearUVLM(uv, st, wake_type=wake_type, skip_linearisation=True)
+    from tests.linear_golden import rigid_projections
+
+    names, sizes, to_zeta, out_size, to_output = rigid_projections(jnp, np.asarray(st.zeta_b[0]), ea_x)
+    refs = (jnp.zeros(2), jnp.zeros(2))
+    ip = LinearInputProjection(arg_names=names, arg_sizes=sizes, arg_refs=refs, to_zeta=to_zeta)
+    op = LinearOutputProjection(name="lift_moment", size=out_size, to_output=to_output)
+    residuals = lin.compute_jacobians(input_projection=ip, output_projection=op)
+    jac = {}
+    for res, (func, args, diff) in residuals.items():
+        f0 = np.asarray(func(**args)).ravel()
+        jac[res] = {}
+        for k in diff:
+            v = np.asarray(args[k], float)
+            blk = np.zeros((f0.size, v.size))
+            for j in range(v.size):
+                vp, vm = v.copy(), v.copy()
+                vp[j] += h
+                vm[j] -= h
+                fp = np.asarray(func(**{**args, k: jnp.array(vp)})).ravel()
+                fm = np.asarray(func(**{**args, k: jnp.array(vm)})).ravel()
+                blk[:, j] = (fp - fm) / (2 * h)
+            jac[res][k] = jnp.array(blk)
+        print(" ", name, res, diff)
+    state_specs = [("gamma_b", "gamma_b_n_vec"), ("gamma_w", "gamma_w_n_vec"), ("gamma_b_nm1", "gamma_b_nm1_vec"),
+                   ("zeta_w", "zeta_w_n_vec"), ("zeta_b", "zeta_b_n_vec")]
+    state_specs = [(a, b) for a, b in state_specs if lin.state_slices[a].enabled]
+    sizes_s = {"gamma_b": st.gamma_b.size, "gamma_w": st.gamma_w.size, "gamma_b_nm1": st.gamma_b.size,
+               "zeta_w": st.zeta_w.size, "zeta_b": st.zeta_b.size}
+    input_specs = list(zip(names, sizes)) + [("nu_b_np1_vec", st.zeta_b.size), ("nu_w_np1_vec", st.zeta_w.size)]
+    s_names = [a for a, _ in state_specs]
+    s_keys = [b for _, b in state_specs]
+    s_sz = [sizes_s[a] for a in s_names]
+    a_ = construct_named_block_jacobian(tuple(jac[k] for k in s_names), s_keys, s_sz, s_sz)
+    b_ = construct_named_block_jacobian(tuple(jac[k] for k in s_names), [k for k, _ in input_specs],
+                                        [v for _, v in input_specs], s_sz)
+    c_ = construct_named_block_jacobian((jac["lift_moment"],), s_keys, s_sz, [out_size])
+    d_ = construct_named_block_jacobian((jac["lift_moment"],), [k for k, _ in input_specs],
+                                        [v for _, v in input_specs], [out_size])
+    out = {"case_name": name, "wake_type": wake_type, "kernel": "epsilon", "r_cut": ref.utils.R_CUTOFF,
+           "free_wake": False, "dt": c.dt, "u_inf": c.u_inf, "rho": c.rho, "zeta_b0": c.zeta_b0, "hg0": c.hg0,
+           "dims": np.array([c.m, c.n, c.m_star]), "h": h, "ea_x": ea_x,
+           "a": np.asarray(a_), "b": np.asarray(b_), "c": np.asarray(c_), "d": np.asarray(d_)}
+    for f in ("zeta_b", "zeta_w", "gamma_b", "gamma_w", "f_steady"):
+        out[f"ref_{f}"] = np.asarray(getattr(st, f)[0])
+    np.savez_compressed(HERE / "linear" / f"{name}.npz", **{k: np.asarray(v) for k, v in out.items()})
+    print("wrote linear", name)
+
+
+ONLY: set[str] = set()
 ONLY: set[str] = set()
 
 
@@ -521,6 +588,9 @@ def main():
                     mirror=([0.0, -0.5, 0.0], [0.0, 1.0, 0.0]))
     c = cases.wing_pitch(m=2, n=3, m_star=3, n_steps=1, n_ctrl=3, seed=4)
     run_linear_case(ref, "linear_prescribed", c, "prescribed")
+    c = cases.wing_heave(m=2, n=3, m_star=3, n_steps=1)
+    run_linear_projected_case(ref, "linear_projected_frozen", c, "frozen")
+    run_linear_projected_case(ref, "linear_projected_prescribed", c, "prescribed", ea_x=0.1)
 
 
 if __name__ == "__main__":

@@ -8,6 +8,7 @@ import numpy as np
 
 GOLDEN = Path(__file__).resolve().parent / "golden" / "linear"
 CASES = ("linear_frozen", "linear_free_gust_mirror", "linear_prescribed")
+PROJECTED = ("linear_projected_frozen", "linear_projected_prescribed")
 
 
 def load(name):
@@ -88,3 +89,45 @@ def two_surface_oracle(wake_type, free, kernel, r_cut=1e-3):
     uv.set_design_variables(wing.dt, R.Constant(wing.u_inf, wing.rho), z0, hg0)
     st = uv.solve_static()
     return uv, st, OL.LinearUVLMRef(uv, st, wake_type)
+
+
+def rigid_projections(xp, zeta_ref, ea_x):
+    """A rigid heave h and pitch theta (about the y axis through x = ea_x) of the reference
+    lattice as the linear model's input projection, and the total lift and the pitching
+    moment about that axis as its output projection, written against an array module xp
+    (jax.numpy for the reference, numpy for the product's tests).  Returns (arg_names, arg_sizes, to_zeta,
+    out_size, to_output)."""
+    z = np.asarray(zeta_ref, float)
+
+    def to_zeta(hp_vec, hp_dot_vec):
+        h, th = hp_vec[0], hp_vec[1]
+        hd, thd = hp_dot_vec[0], hp_dot_vec[1]
+        dx, dz = z[..., 0] - ea_x, z[..., 2]
+        c, s_ = xp.cos(th), xp.sin(th)
+        x = ea_x + c * dx + s_ * dz
+        zz = -s_ * dx + c * dz + h
+        zeta = xp.stack([x, xp.asarray(z[..., 1]), zz], axis=-1)
+        xd = thd * (-s_ * dx + c * dz)
+        zd = hd + thd * (-c * dx - s_ * dz)
+        zeta_dot = xp.stack([xd, xp.zeros_like(xd), zd], axis=-1)
+        return zeta.ravel(), zeta_dot.ravel()
+
+    def to_output(fs, fu):
+        f = fs if fu is None else fs + fu
+        f = f.reshape(-1, 3)
+        arm = z.reshape(-1, 3)[:, 0] - ea_x
+        return xp.stack([xp.sum(f[:, 2]), -xp.sum(arm * f[:, 2])])
+
+    return ("hp_vec", "hp_dot_vec"), (2, 2), to_zeta, 2, to_output
+
+
+def projections(g):
+    """The product's LinearInputProjection / LinearOutputProjection of a projected golden
+    case (the same rigid heave-pitch and lift-moment maps, in numpy)."""
+    from flapjax_b200.linear import LinearInputProjection, LinearOutputProjection
+
+    names, sizes, to_zeta, out_size, to_output = rigid_projections(np, g["ref_zeta_b"], float(g["ea_x"]))
+    ip = LinearInputProjection(arg_names=names, arg_sizes=sizes, arg_refs=(np.zeros(2), np.zeros(2)),
+                               to_zeta=to_zeta)
+    op = LinearOutputProjection(name="lift_moment", size=out_size, to_output=to_output)
+    return ip, op

@@ -193,6 +193,23 @@ def test_linear_model_options(cuda, wake_type, bound_upwash, wake_upwash, unstea
         assert np.abs(got - w).max() <= 1e-7 * max(1.0, np.abs(w).max()), k
 
 
+@pytest.mark.parametrize("name", LG.PROJECTED)
+def test_linear_model_projections(cuda, name):
+    """linearise(input_projection=, output_projection=) against the reference's projected
+    linear model (rigid heave-pitch inputs, lift-moment outputs)."""
+    from flapjax_b200.linear import LinearUVLM
+
+    g = LG.load(name)
+    uv = _product_uvlm(g)
+    lin = LinearUVLM(uv, uv.solve_static(), str(g["wake_type"]), device=cuda, skip_linearisation=True)
+    ip, op = LG.projections(g)
+    sys_ = lin.linearise(input_projection=ip, output_projection=op)
+    for k in "abcd":
+        got = getattr(sys_, k).cpu().numpy()
+        assert got.shape == g[k].shape, k
+        assert np.abs(got - g[k]).max() <= 1e-8 * max(1.0, np.abs(g[k]).max()), k
+
+
 def test_linear_model_follows_nonlinear_heave(cuda):
     """A heave of 1e-4 chords: the force perturbations of the linear system equal those of
     the nonlinear prescribed-motion solve to second order in the amplitude (cutoff kernel,

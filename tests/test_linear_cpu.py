@@ -141,6 +141,52 @@ def test_assembly_options_against_oracle(wake_type, bound_upwash, wake_upwash, u
         assert np.abs(got[k].numpy() - w).max() <= 1e-8 * max(1.0, np.abs(w).max()), k
 
 
+@pytest.mark.parametrize("name", LG.PROJECTED)
+def test_projections_match_reference(name):
+    """Input projection (rigid heave and pitch) and output projection (lift and pitching
+    moment) against the reference's own projected linear model; the assembly with the
+    oracle's operations, the projections as the product applies them."""
+    from flapjax_b200 import linear as L
+    from tests.linear_cpu_ops import OracleOps
+
+    g = LG.load(name)
+    cfg = LG.config(g, LG.flow_product(g))
+    lay = L._Layout(LG.dims(g), cfg["wake_type"], True, True, True)
+    rs, ro = L._assemble(OracleOps(None), lay, LG.reference(g), cfg)
+    ip, op = LG.projections(g)
+    t = lambda x: None if x is None else torch.as_tensor(x)
+    jin = tuple(t(j) for j in L._input_jacobians(ip, 3 * lay.NVB))
+    fs0 = g["ref_f_steady"].ravel()
+    jout = tuple(t(j) for j in L._output_jacobians(op, fs0, np.zeros_like(fs0)))
+    ns = lay.n_states
+    a, b, c, d = L._project(torch, lay, rs[:, :ns], rs[:, ns:], ro[:, :ns], ro[:, ns:], jin, jout)
+    for k, got in zip("abcd", (a, b, c, d)):
+        want = g[k]
+        assert got.shape == want.shape, k
+        assert np.abs(got.numpy() - want).max() <= 1e-8 * max(1.0, np.abs(want).max()), k
+
+
+def test_projection_argument_checks():
+    from flapjax_b200 import linear as L
+
+    ip = L.LinearInputProjection(arg_names=("q",), arg_sizes=(2,), arg_refs=(np.zeros(3),),
+                                 to_zeta=lambda q: (np.zeros(6), np.zeros(6)))
+    with pytest.raises(ValueError):
+        L._input_jacobians(ip, 6)
+    ip = L.LinearInputProjection(arg_names=("q",), arg_sizes=(2,), arg_refs=(np.zeros(2),),
+                                 to_zeta=lambda q: (np.zeros(5), np.zeros(5)))
+    with pytest.raises(ValueError):
+        L._input_jacobians(ip, 6)
+    jz = np.arange(12.0).reshape(6, 2)
+    ip = L.LinearInputProjection(arg_names=("q",), arg_sizes=(2,), arg_refs=(np.zeros(2),),
+                                 to_zeta=lambda q: (jz @ q, 2 * jz @ q))
+    a, b = L._input_jacobians(ip, 6)
+    assert np.allclose(a, jz, atol=1e-8) and np.allclose(b, 2 * jz, atol=1e-8)
+    op = L.LinearOutputProjection(name="o", size=1, to_output=lambda fs, fu: np.array([fs.sum() + fu.sum()]))
+    jfs, jfu = L._output_jacobians(op, np.ones(6), np.ones(6))
+    assert np.allclose(jfs, 1.0) and np.allclose(jfu, 1.0)
+
+
 def test_layout_follows_reference_slices():
     from flapjax_b200 import linear as L
 
