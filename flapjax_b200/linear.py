@@ -22,7 +22,8 @@ with every pairwise Biot-Savart term on the GPU:
     - for a free wake, the convection velocity's ring and vertex Jacobians and its
       gradient at the convected vertices;
   and A^-1 is applied to all columns at once (fj_lu_factor, fj_lu_solve_many);
-* the wake rows shift and convect (aero/utils.py:400-500, uniform wake);
+* the wake rows shift and convect, and a variable wake is re-discretised with fixed
+  interpolation weights (aero/utils.py:400-500, ``_WakeMap``);
 * the steady force f = rho g (v_rel x r) per filament (aero/utils.py:126-223, the linear
   model's own cutoff kernel :155-160) is differentiated through its strength g, the
   relative velocity at the midpoint (ring and vertex Jacobians of the bound and wake
@@ -38,7 +39,9 @@ slice order, each block the concatenation of its surfaces:
 * outputs y = [f_steady, f_unsteady]
 
 Scope: FP64, epsilon or cutoff kernel for the UVLM's own sums, any number of surfaces,
-mirror images, Constant or 1-cos gust flow, uniform wake (``delta_w`` raises).  The
+mirror images, Constant or 1-cos gust flow, uniform or variable wake (``delta_w``: the
+re-discretisation with its arc lengths held at the reference point, as the reference's
+``linearise_variable_wake`` holds them).  The
 reference point is a steady solution (the static solve), so Gamma_dot there is zero and
 the unsteady force has no geometric derivative.
 """
@@ -375,6 +378,62 @@ def _diff_lists(wake_type, bound_upwash, wake_upwash, unsteady_force):
 # ---------------------------------------------------------------------------------------
 # assembly
 # ---------------------------------------------------------------------------------------
+def _interp_weights(xq, xp):
+    """W with W @ fp = interp(xq, xp, fp) for increasing xp (jnp.interp, as
+    aero/utils.py:480-491 calls it): end values held outside [xp[0], xp[-1]], linear
+    between the bracketing nodes inside."""
+    w = np.zeros((len(xq), len(xp)))
+    last = len(xp) - 1
+    for q, x in enumerate(xq):
+        if not x >= xp[0]:
+            w[q, 0] = 1.0
+        elif x >= xp[last]:
+            w[q, last] = 1.0
+        else:
+            j = int(np.searchsorted(xp, x, side="right")) - 1
+            t = (x - xp[j]) / (xp[j + 1] - xp[j])
+            w[q, j] += 1.0 - t
+            w[q, j + 1] += t
+    return w
+
+
+class _WakeMap:
+    """The wake of step n+1 from step n for one surface (aero/utils.py:400-500), per
+    spanwise column: zeta_w1 = Wz X and gamma_w1 = Wg G, with X = [trailing edge of step
+    n+1; convected vertex rows of step n] and G = [trailing-edge circulation of step n;
+    wake circulation rows of step n].  Uniform wake: rows 0..W-1 convect, G holds rows
+    0..W-2, and Wz, Wg are identities.  Variable wake (delta_w): every row convects, G
+    holds every row, and Wz, Wg re-discretise onto delta_w with the arc lengths of the
+    reference point, held as the linear model's stop_gradient holds them
+    (``linearise_variable_wake``, :465-468)."""
+
+    def __init__(self, n, w, delta_w, x_ref=None):
+        var = delta_w is not None and w > 0
+        self.n_conv_rows = w + 1 if var else w
+        self.n_x = self.n_conv_rows + 1
+        self.n_g = w + 1 if var else w
+        if not var:
+            self.wz = np.broadcast_to(np.eye(w + 1), (n + 1, w + 1, w + 1))
+            self.wg = np.broadcast_to(np.eye(w), (n, w, w))
+            return
+        if x_ref is None:  # row counts only
+            return
+        seg = np.linalg.norm(x_ref[1:] - x_ref[:-1], axis=-1)
+        arc = np.concatenate([np.zeros((1, n + 1)), np.cumsum(seg, axis=0)], axis=0)       # (W+2, n+1)
+        arc_g = 0.5 * (0.5 * (arc[:-1, :-1] + arc[1:, :-1]) + 0.5 * (arc[:-1, 1:] + arc[1:, 1:]))
+        s_disc = np.concatenate([np.zeros(1), np.cumsum(np.asarray(delta_w, np.float64))])
+        sg_disc = 0.5 * (s_disc[:-1] + s_disc[1:])
+        self.wz = np.stack([_interp_weights(s_disc, arc[:, j]) for j in range(n + 1)])       # (n+1, W+1, W+2)
+        self.wg = np.stack([_interp_weights(sg_disc, arc_g[:, j]) for j in range(n)])         # (n, W, W+1)
+
+    def apply_z(self, x):
+        """(n_x, n+1, ...) -> (W+1, n+1, ...)."""
+        return np.einsum("jrs,sj...->rj...", self.wz, x)
+
+    def apply_g(self, g):
+        return np.einsum("jrs,sj->rj", self.wg, g)
+
+
 def _assemble(ops, lay, ref, cfg):
     """Jacobian rows of every residual over the columns [states | inputs].
 
@@ -402,7 +461,9 @@ def _assemble(ops, lay, ref, cfg):
         return lay.col(kind, name)
 
     # ---- forward at the reference point -------------------------------------------------
-    conv_pts = [z[:-1] for z in Zw]                    # wake vertices convected (rows 0..W-1)
+    dws = cfg.get("delta_w") or [None] * S
+    maps0 = [_WakeMap(n, w, dw if w > 0 else None) for (m, n, w), dw in zip(lay.dims, dws)]
+    conv_pts = [z[:mp.n_conv_rows] for z, mp in zip(Zw, maps0)]          # wake vertex rows that convect
     n_conv = [p.shape[0] * p.shape[1] for p in conv_pts]
     o_conv = np.concatenate([[0], np.cumsum(n_conv)]).astype(np.int64)
     NC = int(o_conv[-1])
@@ -411,11 +472,15 @@ def _assemble(ops, lay, ref, cfg):
     vc = ff(conv_flat, t)
     if free and NC:
         vc = vc + ops.vind(t_conv, list(zip(tZb, tgb)) + list(zip(tZw, tgw)), K, RC).cpu().numpy()
-    zw1, gw1 = [], []
+    zw1, gw1, maps = [], [], []
     for s, (m, n, w) in enumerate(lay.dims):
         conv = conv_pts[s] + dt * vc[o_conv[s]:o_conv[s + 1]].reshape(conv_pts[s].shape)
-        zw1.append(np.concatenate([Zb[s][-1][None], conv], axis=0))
-        gw1.append(np.concatenate([gb[s][-1][None], gw[s][:-1]], axis=0) if w > 0 else gw[s].copy())
+        x_ref = np.concatenate([Zb[s][-1][None], conv], axis=0)
+        g_ref = np.concatenate([gb[s][-1][None], gw[s]], axis=0)[:maps0[s].n_g]
+        mp = _WakeMap(n, w, dws[s] if w > 0 else None, x_ref)
+        maps.append(mp)
+        zw1.append(mp.apply_z(x_ref))
+        gw1.append(mp.apply_g(g_ref) if w > 0 else gw[s].copy())
     tzw1, tgw1 = [ops.tensor(z) for z in zw1], [ops.tensor(g) for g in gw1]
     c = [0.25 * (z[:-1, :-1] + z[1:, :-1] + z[:-1, 1:] + z[1:, 1:]) for z in Zb]
     d1 = [z[1:, 1:] - z[:-1, :-1] for z in Zb]
@@ -479,39 +544,38 @@ def _assemble(ops, lay, ref, cfg):
         # the bound lattice's own sources (circulation held at Gamma_b of step n+1)
         ops.vertex(phi, zb_c[0] + 3 * int(vb), tc, tn, tZb[s], tgb1[s], K, RC)
     phi[:, zb_c[0]:zb_c[1]] *= -1.0
+    pw_conv = None
     if pw is not None:
-        for s, (m, n, w) in enumerate(lay.dims):
-            if w == 0:
-                continue
-            te_w = 3 * (int(lay.o_vw[s]) + np.arange(n + 1))              # wake row 0 = input TE row
-            te_b = zb_c[0] + 3 * (int(lay.o_vb[s]) + m * (n + 1) + np.arange(n + 1))
-            for b in range(3):
-                phi[:, te_b + b] -= pw[:, te_w + b]
-        if cols("u", "nu_w") is not None:
-            c0, c1 = cols("u", "nu_w")
-            phi[:, c0:c1] -= dt * pw
-    # wake circulation: gamma_w1[0] = gamma_b[-1], gamma_w1[r+1] = gamma_w[r]
-    if wake_lats:
-        qw = ops.zeros(NB, lay.NW)
+        zb_c = cols("u", "zeta_b")
+        gbc, gwc = cols("x", "gamma_b"), cols("x", "gamma_w")
+        qw = ops.zeros(NB, lay.NW)                                        # n . dV(c)/d gamma_w1
         for s in range(S):
             if Zw[s].shape[0] > 1:
                 ops.ring(qw, int(lay.o_gw[s]), tc, tn, tzw1[s], K, RC)
-        gbc, gwc = cols("x", "gamma_b"), cols("x", "gamma_w")
+        conv_parts = []
         for s, (m, n, w) in enumerate(lay.dims):
             if w == 0:
                 continue
-            ow, ob = int(lay.o_gw[s]), int(lay.o_gb[s])
-            phi[:, gbc[0] + ob + (m - 1) * n:gbc[0] + ob + m * n] -= qw[:, ow:ow + n]
-            if w > 1:
-                phi[:, gwc[0] + ow:gwc[0] + ow + (w - 1) * n] -= qw[:, ow + n:ow + w * n]
-    # convection of the wake rows 1..W of step n+1 from rows 0..W-1 of step n
-    need_conv = pw is not None and NC > 0 and (free or prescribed)
+            mp = maps[s]
+            ov, ow, ob = int(lay.o_vw[s]), int(lay.o_gw[s]), int(lay.o_gb[s])
+            # through the wake map: columns of X (trailing edge, convected rows) and of G
+            px = torch.einsum("irjk,jrs->isjk", pw[:, 3 * ov:3 * (ov + (w + 1) * (n + 1))].reshape(NB, w + 1, n + 1, 3),
+                              ops.tensor(mp.wz))
+            qg = torch.einsum("irj,jrs->isj", qw[:, ow:ow + w * n].reshape(NB, w, n), ops.tensor(mp.wg))
+            te_b = zb_c[0] + 3 * (int(lay.o_vb[s]) + m * (n + 1))
+            phi[:, te_b:te_b + 3 * (n + 1)] -= px[:, 0].reshape(NB, 3 * (n + 1))   # X row 0: the input's TE row
+            phi[:, gbc[0] + ob + (m - 1) * n:gbc[0] + ob + m * n] -= qg[:, 0]      # G row 0: gamma_b TE row
+            if mp.n_g > 1:
+                phi[:, gwc[0] + ow:gwc[0] + ow + (mp.n_g - 1) * n] -= qg[:, 1:].reshape(NB, (mp.n_g - 1) * n)
+            conv_parts.append(px[:, 1:].reshape(NB, 3 * n_conv[s]))
+        if cols("u", "nu_w") is not None:
+            c0, c1 = cols("u", "nu_w")
+            phi[:, c0:c1] -= dt * pw                                      # nu_w moves the new wake itself
+        if conv_parts:
+            pw_conv = torch.cat(conv_parts, dim=1)                        # (NB, 3 NC) in conv-target order
+    # convection of the wake rows of step n (into the X rows of step n+1)
+    need_conv = pw_conv is not None and NC > 0 and (free or prescribed)
     if need_conv:
-        # P_w restricted to the convected rows, in conv-target order (3 columns each)
-        conv_cols = np.concatenate([3 * (int(lay.o_vw[s]) + (lay.dims[s][1] + 1) + np.arange(n_conv[s]))
-                                    for s in range(S)]) if NC else np.zeros(0, np.int64)
-        cc3 = (conv_cols[:, None] + np.arange(3)[None, :]).ravel()
-        pw_conv = pw[:, torch.as_tensor(cc3, device=pw.device)]           # (NB, 3 NC)
         if free:
             jc_gb = ops.zeros(3 * NC, lay.NB)
             jc_gw = ops.zeros(3 * NC, lay.NW)
@@ -563,25 +627,24 @@ def _assemble(ops, lay, ref, cfg):
     R_state[r0:r1] = phi
     gbc, gwc = cols("x", "gamma_b"), cols("x", "gamma_w")
     gw_r = lay.x["gamma_w"][0]
-    ones_r, ones_c = [], []                                               # unit entries of R_state
+    ones_r, ones_c, ones_v = [], [], []                                   # sparse entries of R_state
     for s, (m, n, w) in enumerate(lay.dims):
+        if w == 0:
+            continue
         ow, ob = int(lay.o_gw[s]), int(lay.o_gb[s])
-        if w > 0:
-            ones_r.append(gw_r + ow + np.arange(n))
-            ones_c.append(gbc[0] + ob + (m - 1) * n + np.arange(n))
-        if w > 1:
-            ones_r.append(gw_r + ow + n + np.arange((w - 1) * n))
-            ones_c.append(gwc[0] + ow + np.arange((w - 1) * n))
+        j_, r_, g_ = np.nonzero(maps[s].wg)                               # gamma_w1[r, j] <- G[g, j]
+        ones_r.append(gw_r + ow + r_ * n + j_)
+        ones_c.append(np.where(g_ == 0, gbc[0] + ob + (m - 1) * n + j_, gwc[0] + ow + (g_ - 1) * n + j_))
+        ones_v.append(maps[s].wg[j_, r_, g_])
     if "gamma_b_nm1" in lay.x:
         q0 = lay.x["gamma_b_nm1"][0]
         ones_r.append(q0 + np.arange(NB))
         ones_c.append(gbc[0] + np.arange(NB))
+        ones_v.append(np.ones(NB))
     if prescribed:
         zr = lay.x["zeta_w"][0]
         zwc, zbi = cols("x", "zeta_w"), cols("u", "zeta_b")
-        for s, (m, n, w) in enumerate(lay.dims):
-            ones_r.append(zr + 3 * int(lay.o_vw[s]) + np.arange(3 * (n + 1)))       # wake row 0 = TE row
-            ones_c.append(zbi[0] + 3 * (int(lay.o_vb[s]) + m * (n + 1)) + np.arange(3 * (n + 1)))
+        blk = np.zeros((0, 3, 3))
         if NC:
             gconv = _flow_grad(ff, conv_flat, t)
             if free:
@@ -590,21 +653,36 @@ def _assemble(ops, lay, ref, cfg):
                     lam = np.zeros((NC, 3))
                     lam[:, a] = 1.0
                     gconv[:, a, :] += ops.vind_grad_t(t_conv, lats0, K, RC, ops.tensor(lam)).cpu().numpy()
-            dst = np.concatenate([3 * (int(lay.o_vw[s]) + (lay.dims[s][1] + 1) + np.arange(n_conv[s]))
-                                  for s in range(S)])
-            src = np.concatenate([3 * (int(lay.o_vw[s]) + np.arange(n_conv[s])) for s in range(S)])
-            blk = np.eye(3)[None] + dt * gconv
-            rr = (zr + dst[:, None, None] + np.arange(3)[None, :, None]).repeat(3, axis=2)
-            cc = (zwc[0] + src[:, None, None] + np.arange(3)[None, None, :]).repeat(3, axis=1)
-            R_state.index_put_((torch.as_tensor(rr.ravel(), device=R_state.device),
-                                torch.as_tensor(cc.ravel(), device=R_state.device)),
-                               ops.tensor(blk.ravel()), accumulate=True)
-            if free:
-                dst3 = torch.as_tensor((zr + dst[:, None] + np.arange(3)[None, :]).ravel(), device=R_state.device)
-                R_state[dst3, zwc[0]:zwc[1]] += dt * jc_zw
-                if wt == "free":
-                    R_state[dst3, gbc[0]:gbc[1]] += dt * jc_gb
-                    R_state[dst3, gwc[0]:gwc[1]] += dt * jc_gw
+            blk = np.eye(3)[None] + dt * gconv                           # d X[conv] / d zeta_w0 per vertex
+        for s, (m, n, w) in enumerate(lay.dims):
+            ov = int(lay.o_vw[s])
+            j_, r_, x_ = np.nonzero(maps[s].wz)                           # zeta_w1[r, j] <- X[x, j]
+            wv = maps[s].wz[j_, r_, x_]
+            te = x_ == 0                                                  # X row 0: the input's TE row
+            for k in range(3):
+                ones_r.append(zr + 3 * (ov + r_[te] * (n + 1) + j_[te]) + k)
+                ones_c.append(zbi[0] + 3 * (int(lay.o_vb[s]) + m * (n + 1) + j_[te]) + k)
+                ones_v.append(wv[te])
+            cv = ~te                                                      # convected rows of step n
+            tgt = o_conv[s] + (x_[cv] - 1) * (n + 1) + j_[cv]
+            for k in range(3):
+                for b in range(3):
+                    ones_r.append(zr + 3 * (ov + r_[cv] * (n + 1) + j_[cv]) + k)
+                    ones_c.append(zwc[0] + 3 * (ov + (x_[cv] - 1) * (n + 1) + j_[cv]) + b)
+                    ones_v.append(wv[cv] * blk[tgt, k, b])
+        if NC and free:
+            # the free convection's dense terms, through the wake map
+            dense = [(zwc, jc_zw)] + ([(gbc, jc_gb), (gwc, jc_gw)] if wt == "free" else [])
+            for s, (m, n, w) in enumerate(lay.dims):
+                if w == 0:
+                    continue
+                mp, ov = maps[s], int(lay.o_vw[s])
+                wz = ops.tensor(mp.wz)
+                for cc_, jc in dense:
+                    part = jc[3 * int(o_conv[s]):3 * int(o_conv[s + 1])].reshape(mp.n_conv_rows, n + 1, 3, -1)
+                    x_part = torch.cat([torch.zeros_like(part[:1]), part], dim=0)   # X row 0 does not convect
+                    rows_ = torch.einsum("jrs,sjkc->rjkc", wz, x_part).reshape(3 * (w + 1) * (n + 1), -1)
+                    R_state[zr + 3 * ov:zr + 3 * (ov + (w + 1) * (n + 1)), cc_[0]:cc_[1]] += dt * rows_
         if cols("u", "nu_w") is not None:
             c0, _ = cols("u", "nu_w")
             R_state.index_put_((torch.as_tensor(zr + np.arange(3 * lay.NVW), device=R_state.device),
@@ -613,10 +691,11 @@ def _assemble(ops, lay, ref, cfg):
         zbr = lay.x["zeta_b"][0]
         ones_r.append(zbr + np.arange(3 * lay.NVB))
         ones_c.append(zbi[0] + np.arange(3 * lay.NVB))
+        ones_v.append(np.ones(3 * lay.NVB))
     if ones_r:
-        r_, c_ = np.concatenate(ones_r), np.concatenate(ones_c)
+        r_, c_, v_ = np.concatenate(ones_r), np.concatenate(ones_c), np.concatenate(ones_v)
         R_state.index_put_((torch.as_tensor(r_, device=R_state.device), torch.as_tensor(c_, device=R_state.device)),
-                           ops.tensor(np.ones(r_.size)), accumulate=True)
+                           ops.tensor(v_), accumulate=True)
 
     # ---- output rows ----------------------------------------------------------------------
     R_out = ops.zeros(lay.n_outputs, ncol)
@@ -874,8 +953,6 @@ class LinearUVLM:
             raise ValueError(f"wake_type must be one of {WAKE_TYPES}, got {wake_type!r}")
         if case.kernel.kernel_id not in (_lib.FJ_KERNEL_EPSILON, _lib.FJ_KERNEL_CUTOFF):
             raise NotImplementedError("the linearisation is written for the epsilon and cutoff kernels")
-        if any(d is not None for d in (case.delta_w or [])):
-            raise NotImplementedError("the linearisation is written for the uniform wake (delta_w = None)")
         if any(p is not None for p in case.polars):
             raise NotImplementedError("polar corrections are not part of the linear model")
         self.case = case
@@ -930,7 +1007,9 @@ class LinearUVLM:
                 "force_r_cut": self.case.kernel.r_cut if kid == _lib.FJ_KERNEL_CUTOFF else R_CUTOFF,
                 "dt": self.dt, "rho": self.case.flowfield.rho, "flowfield": self.case.flowfield,
                 "t": float(np.asarray(self._reference.t).ravel()[0]), "bound_upwash": self.bound_upwash,
-                "wake_upwash": self.wake_upwash, "unsteady_force": self.unsteady_force}
+                "wake_upwash": self.wake_upwash, "unsteady_force": self.unsteady_force,
+                "delta_w": [None if d is None else np.asarray(d, np.float64) for d in (self.case.delta_w or [])]
+                or None}
 
     def linearise(self, batch_size=None, *, input_projection: LinearInputProjection | None = None,
                   output_projection: LinearOutputProjection | None = None) -> LinearSystem:

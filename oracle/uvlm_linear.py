@@ -98,8 +98,6 @@ class LinearUVLMRef:
                  unsteady_force=True):
         if wake_type not in ("frozen", "prescribed", "free"):
             raise ValueError(f"wake_type {wake_type!r}")
-        if any(d is not None for d in uv.delta_w):
-            raise NotImplementedError("the linear model here is written for the uniform wake")
         self.uv = uv
         self.wake_type = wake_type
         self.prescribed = wake_type in ("prescribed", "free")
@@ -168,7 +166,10 @@ class LinearUVLMRef:
         return self.pack(self.u_blocks, u), self.pack(self.x_blocks, x)
 
     # -- the nonlinear step (:324-429) ---------------------------------------------------
-    def step(self, u_vec, x_vec):
+    def step(self, u_vec, x_vec, arc_held=None, arc_record=None):
+        """One nonlinear step; with a variable wake, ``arc_held`` (one array per surface
+        with delta_w, in surface order) stands for the arc lengths that the reference's
+        stop_gradient holds, and ``arc_record`` receives the arc lengths used."""
         uv, ref = self.uv, self.ref
         u = self.unpack(self.u_blocks, u_vec)
         x = self.unpack(self.x_blocks, x_vec)
@@ -185,7 +186,12 @@ class LinearUVLMRef:
         else:
             zb_n, zw_n = ref["zeta_b"], ref["zeta_w"]
         q_n = (gb_n, gw_n, ref["gamma_b_dot"], zw_n)
-        out = uv.base_solve_from_grid(q_n, self.t, zb1, zb_n, zbd1, False, nu_b=nu_b, nu_w=nu_w)
+        held = None
+        if arc_held is not None:
+            it = iter(arc_held)
+            held = [None if d is None else next(it) for d in uv.delta_w]
+        out = uv.base_solve_from_grid(q_n, self.t, zb1, zb_n, zbd1, False, nu_b=nu_b, nu_w=nu_w, arc_held=held,
+                                      arc_record=arc_record)
         ff = uv.flowfield
 
         def v_out(x_):
@@ -213,6 +219,9 @@ class LinearUVLMRef:
     def linearise(self, h=1e-6):
         """(A, B, C, D) with the reference's differentiated blocks only."""
         u0, x0 = self.reference_vectors()
+        arcs = []
+        self.step(u0, x0, arc_record=arcs)  # the variable wake's arc lengths at the reference point
+        held = arcs if arcs else None
         xo, uo, yo = self._offsets(self.x_blocks), self._offsets(self.u_blocks), self._offsets(self.y_blocks)
         lists = diff_lists(self.wake_type, self.bound_upwash, self.wake_upwash, self.unsteady_force)
         args = sorted({a for v in lists.values() for a in v})
@@ -230,8 +239,8 @@ class LinearUVLMRef:
                 else:
                     up[lo + j] += h
                     um[lo + j] -= h
-                sxp, syp = self.step(up, xp)
-                sxm, sym = self.step(um, xm)
+                sxp, syp = self.step(up, xp, held)
+                sxm, sym = self.step(um, xm, held)
                 jx[:, j] = (sxp - sxm) / (2 * h)
                 jy[:, j] = (syp - sym) / (2 * h)
             col[a] = (jx, jy)

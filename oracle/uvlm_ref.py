@@ -433,8 +433,12 @@ def _interp(x, xp, fp):
     return out
 
 
-def propagate_surf_wake(gamma_b_nm1, gamma_w_nm1, zeta_b_n, zeta_w_nm1, delta_w, v_func, dt):
-    """``propagate_surf_wake`` aero/utils.py:400-500 (uniform and ``delta_w`` branches)."""
+def propagate_surf_wake(gamma_b_nm1, gamma_w_nm1, zeta_b_n, zeta_w_nm1, delta_w, v_func, dt, arc_held=None,
+                        arc_record=None):
+    """``propagate_surf_wake`` aero/utils.py:400-500 (uniform and ``delta_w`` branches).
+    ``arc_held``: arc lengths to use in place of the convected wake's own (the linear
+    model's ``linearise_variable_wake``, whose stop_gradient holds them at the reference
+    point, :465-468); ``arc_record``: a list that receives the arc lengths used."""
     zeta_te = zeta_b_n[-1, ...]
     gamma_te = gamma_b_nm1[-1, ...]
     if delta_w is not None:
@@ -449,6 +453,10 @@ def propagate_surf_wake(gamma_b_nm1, gamma_w_nm1, zeta_b_n, zeta_w_nm1, delta_w,
     if delta_w is not None:
         seg = np.linalg.norm(zeta_w_n[1:, ...] - zeta_w_n[:-1, ...], axis=-1)
         s_zeta_w = np.concatenate((np.zeros((1, zeta_te.shape[0])), np.cumsum(seg, axis=0)), axis=0)
+        if arc_held is not None:
+            s_zeta_w = np.asarray(arc_held, dtype=s_zeta_w.dtype)
+        if arc_record is not None:
+            arc_record.append(s_zeta_w.copy())
         s_gamma_w = neighbour_average(s_zeta_w, (0, 1))
         s_disc = np.concatenate((np.zeros(1), np.cumsum(delta_w)))
         s_gamma_disc = neighbour_average(s_disc, (0,))
@@ -719,7 +727,7 @@ class UVLMRef:
     # uvlm.py:824-1117; nu_b / nu_w are the linear model's bound and wake upwash inputs
     # (uvlm.py:943-946, 979-981, and calculate_steady_forcing's v_inputs)
     def base_solve_from_grid(self, q_nm1, t_n, zeta_b_n, zeta_b_nm1, zeta_b_dot_n, static,
-                             horseshoe=False, nu_b=None, nu_w=None):
+                             horseshoe=False, nu_b=None, nu_w=None, arc_held=None, arc_record=None):
         ff = self.flowfield
         c_n = [compute_surf_c(z) for z in zeta_b_n]
         nc_n = [compute_surf_nc(z) for z in zeta_b_n]
@@ -744,7 +752,8 @@ class UVLMRef:
             zeta_w_n, gamma_w_n = [], []
             for i in range(self.n_surf):
                 zw, gw = propagate_surf_wake(gb_nm1[i], gw_nm1[i], zeta_b_n[i], zw_nm1[i],
-                                             self.delta_w[i], v_wake_prop, self.dt)
+                                             self.delta_w[i], v_wake_prop, self.dt,
+                                             None if arc_held is None else arc_held[i], arc_record)
                 zeta_w_n.append(zw)
                 gamma_w_n.append(gw)
             if nu_w is not None:

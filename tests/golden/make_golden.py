@@ -289,7 +289,7 @@ def run_gradient_case(ref, name, c, free_wake=False, kernel="epsilon", r_cut=Non
 
 
 def run_linear_case(ref, name, c, wake_type, free_wake=False, kernel="epsilon", r_cut=None, gust=None, mirror=None,
-                    n_run=6, h=1e-6, seed=0):
+                    n_run=6, h=1e-6, seed=0, delta_w=None):
     """The reference's own linearised UVLM (aero/linear/linear_uvlm.py) about the static
     solution of case ``c``.  ``LinearUVLM.compute_jacobians`` supplies, per residual, the
     step function, its arguments and the arguments it differentiates; jax.jacrev is
@@ -298,7 +298,13 @@ def run_linear_case(ref, name, c, wake_type, free_wake=False, kernel="epsilon", 
     C, D by the reference's ``construct_named_block_jacobian`` in ``linearise``'s order.
     The reference's ``LinearSystem.run`` then marches those matrices over ``n_run`` seeded
     input perturbations.  Also stored: the step's packed outputs at the reference point
-    and at one seeded perturbation of every input and state."""
+    and at one seeded perturbation of every input and state.
+
+    With a variable wake (``delta_w``) the linear model's step holds the wake's arc lengths
+    with jax.lax.stop_gradient (``linearise_variable_wake``, aero/utils.py:465-468), so
+    jacrev differentiates with the arc lengths fixed at the reference point.  The stand-in's
+    stop_gradient is the identity; here it records the arc lengths of the reference-point
+    step and hands those back to every differenced step, which is what jacrev sees."""
     if ONLY and name not in ONLY:
         return
     jnp = ref.jnp
@@ -317,12 +323,29 @@ def run_linear_case(ref, name, c, wake_type, free_wake=False, kernel="epsilon", 
         ff = (ref.Constant(jnp.array(c.u_inf), c.rho, True) if gust is None else
               ref.OneMinusCosine(jnp.array(c.u_inf), c.rho, True, gust_length=gust["length"],
                                  gust_amplitude=gust["amplitude"], gust_x0=jnp.array(gust["x0"])))
-        uv.set_design_variables(dt=float(c.dt), flowfield=ff, zeta_b0=[jnp.array(c.zeta_b0)], hg0=jnp.array(c.hg0))
+        uv.set_design_variables(dt=float(c.dt), flowfield=ff, zeta_b0=[jnp.array(c.zeta_b0)], hg0=jnp.array(c.hg0),
+                                delta_w=None if delta_w is None else [jnp.array(delta_w)])
         st = uv.solve_static()
         lin = LinearUVLM(uv, st, wake_type=wake_type, skip_linearisation=True)
         residuals = lin.compute_jacobians()
+        import jax.lax as shim_lax
 
-        def full_step(**kwargs):
+        held = {"mode": "off", "vals": [], "k": 0}
+
+        def held_stop_gradient(x):
+            if held["mode"] == "record":
+                held["vals"].append(np.array(x))
+                return x
+            if held["mode"] == "replay":
+                v = held["vals"][held["k"]]
+                held["k"] += 1
+                return jnp.array(v)
+            return x
+
+        shim_lax.stop_gradient = held_stop_gradient
+
+        def full_step(mode="replay", **kwargs):
+            held["mode"], held["k"] = mode, 0
             x1, y0 = lin._step_from_vecs(**kwargs)
             return np.asarray(lin.pack_state_vector(x1)), np.asarray(lin.pack_output_vector(y0))
 
@@ -332,7 +355,7 @@ def run_linear_case(ref, name, c, wake_type, free_wake=False, kernel="epsilon", 
         for _, args, diff in residuals.values():
             for k in diff:
                 ref_args[k] = np.asarray(args[k], float)
-        x_ref, y_ref = full_step()
+        x_ref, y_ref = full_step(mode="record")
         cols = {}
         for k, v in ref_args.items():
             jx = np.zeros((x_ref.size, v.size))
@@ -383,7 +406,7 @@ def run_linear_case(ref, name, c, wake_type, free_wake=False, kernel="epsilon", 
         x_run, y_run = sys_.run(jnp.array(u_run), jnp.array(x0))
         # the nonlinear step at one seeded perturbation of every argument
         pert = {k: v + 1e-3 * rng.normal(size=v.shape) for k, v in ref_args.items()}
-        x_p, y_p = full_step(**{k: jnp.array(v) for k, v in pert.items()})
+        x_p, y_p = full_step(mode="off", **{k: jnp.array(v) for k, v in pert.items()})
         out = {"case_name": name, "wake_type": wake_type, "kernel": kernel,
                "r_cut": r_cut if r_cut is not None else saved_r, "free_wake": free_wake, "dt": c.dt,
                "u_inf": c.u_inf, "rho": c.rho, "zeta_b0": c.zeta_b0, "hg0": c.hg0,
@@ -400,10 +423,15 @@ def run_linear_case(ref, name, c, wake_type, free_wake=False, kernel="epsilon", 
         if mirror is not None:
             out["mirror_point"] = np.asarray(mirror[0], float)
             out["mirror_normal"] = np.asarray(mirror[1], float)
+        if delta_w is not None:
+            out["delta_w"] = np.asarray(delta_w, float)
         np.savez_compressed(HERE / "linear" / f"{name}.npz", **{k: np.asarray(v) for k, v in out.items()})
         print("wrote linear", name)
     finally:
         ref.utils.R_CUTOFF = saved_r
+        import jax.lax as shim_lax
+
+        shim_lax.stop_gradient = lambda x: x
 
 
 def run_linear_projected_case(ref, name, c, wake_type, ea_x=0.0, h=1e-6, seed=0):
@@ -588,6 +616,11 @@ def main():
                     mirror=([0.0, -0.5, 0.0], [0.0, 1.0, 0.0]))
     c = cases.wing_pitch(m=2, n=3, m_star=3, n_steps=1, n_ctrl=3, seed=4)
     run_linear_case(ref, "linear_prescribed", c, "prescribed")
+    c = cases.wing_heave(m=2, n=3, m_star=3, n_steps=1)
+    run_linear_case(ref, "linear_delta_w_frozen", c, "frozen", delta_w=c.dt * c.u_mag * 1.2 ** np.arange(c.m_star))
+    c = cases.wing_free(m=2, n=3, m_star=3, n_steps=1, seed=5)
+    run_linear_case(ref, "linear_delta_w_free", c, "free", free_wake=True, kernel="cutoff", r_cut=1e-3,
+                    delta_w=c.dt * c.u_mag * 1.15 ** np.arange(c.m_star))
     c = cases.wing_heave(m=2, n=3, m_star=3, n_steps=1)
     run_linear_projected_case(ref, "linear_projected_frozen", c, "frozen")
     run_linear_projected_case(ref, "linear_projected_prescribed", c, "prescribed", ea_x=0.1)

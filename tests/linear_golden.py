@@ -9,6 +9,7 @@ import numpy as np
 GOLDEN = Path(__file__).resolve().parent / "golden" / "linear"
 CASES = ("linear_frozen", "linear_free_gust_mirror", "linear_prescribed")
 PROJECTED = ("linear_projected_frozen", "linear_projected_prescribed")
+VARIABLE = ("linear_delta_w_frozen", "linear_delta_w_free")
 
 
 def load(name):
@@ -50,7 +51,7 @@ def config(g, flowfield):
     return {"wake_type": str(g["wake_type"]), "free_wake": bool(g["free_wake"]), "kernel": kid,
             "r_cut": float(g["r_cut"]), "force_r_cut": float(g["r_cut"]) if kid == _lib.FJ_KERNEL_CUTOFF else 1e-4,
             "dt": float(g["dt"]), "rho": float(g["rho"]), "flowfield": flowfield, "t": 0.0, "bound_upwash": True,
-            "wake_upwash": True, "unsteady_force": True}
+            "wake_upwash": True, "unsteady_force": True, "delta_w": [g["delta_w"]] if "delta_w" in g else None}
 
 
 def reference(g):

@@ -101,11 +101,12 @@ def _product_uvlm(g, **kw):
     mkw = {} if mir is None else dict(mirror_point=mir[0], mirror_normal=mir[1])
     uv = fj.UVLM([fj.GridDiscretisation(m, n, w)], np.arange(n + 1), kernel=kernel, free_wake=bool(g["free_wake"]),
                  **mkw, **kw)
-    uv.set_design_variables(dt=float(g["dt"]), flowfield=LG.flow_product(g), zeta_b0=g["zeta_b0"], hg0=g["hg0"])
+    uv.set_design_variables(dt=float(g["dt"]), flowfield=LG.flow_product(g), zeta_b0=g["zeta_b0"], hg0=g["hg0"],
+                            delta_w=g["delta_w"] if "delta_w" in g else None)
     return uv
 
 
-@pytest.mark.parametrize("name", LG.CASES)
+@pytest.mark.parametrize("name", LG.CASES + LG.VARIABLE)
 def test_linear_model_matches_reference(cuda, name):
     """A, B, C, D of the reference's own LinearUVLM (central differences of its step
     functions, h = 1e-6) and its LinearSystem.run over seeded inputs."""

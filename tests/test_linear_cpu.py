@@ -21,11 +21,12 @@ def _oracle(g):
     kw = {} if mir is None else dict(mirror_point=mir[0], mirror_normal=mir[1])
     uv = R.UVLMRef([(m, n, w)], np.arange(n + 1), kernel=kern, r_cut=float(g["r_cut"]),
                    free_wake=bool(g["free_wake"]), **kw)
-    uv.set_design_variables(float(g["dt"]), LG.flow_oracle(g), g["zeta_b0"], g["hg0"])
+    uv.set_design_variables(float(g["dt"]), LG.flow_oracle(g), g["zeta_b0"], g["hg0"],
+                            delta_w=g["delta_w"] if "delta_w" in g else None)
     return OL.LinearUVLMRef(uv, uv.solve_static(), str(g["wake_type"]))
 
 
-@pytest.mark.parametrize("name", LG.CASES)
+@pytest.mark.parametrize("name", LG.CASES + LG.VARIABLE)
 def test_oracle_step_matches_reference(name):
     g = LG.load(name)
     lin = _oracle(g)
@@ -51,7 +52,7 @@ def test_oracle_step_matches_reference(name):
     assert np.allclose(y0p, g["y_pert"], rtol=0, atol=1e-12)
 
 
-@pytest.mark.parametrize("name", LG.CASES)
+@pytest.mark.parametrize("name", LG.CASES + LG.VARIABLE)
 def test_oracle_jacobians_match_reference(name):
     """Central differences of the oracle's step against those of the reference's step (both
     h = 1e-6): agreement to the differencing noise."""
@@ -64,7 +65,7 @@ def test_oracle_jacobians_match_reference(name):
     assert np.allclose(y, g["y_run"], rtol=0, atol=1e-10)
 
 
-@pytest.mark.parametrize("name", LG.CASES)
+@pytest.mark.parametrize("name", LG.CASES + LG.VARIABLE)
 def test_assembly_chain_rule_matches_reference(name):
     """The device assembly's chain rule with the oracle standing in for the device
     operations: A, B, C, D equal the reference's Jacobians, every block (zero blocks
