@@ -17,8 +17,9 @@ fp64_gpu  the plain FP64 path on the same steps, and the mixed path's CL/CD erro
 autotune  the split counts of the step's three Biot-Savart sums, timed on the device before
         the timed regions (fj_autotune_vind) for both precisions, against the wave-filling
         rule the launches use untuned.
---linear  the linearised UVLM: assembly time of A, B, C, D on the device and the linear
-        system's time march (C1 and C3 wings).
+linear  the linearised UVLM at C1 size (8x32, W=64, frozen wake): assembly time of A, B, C,
+        D on the device and a short march (--linear runs only this leg, with C1 prescribed
+        and C3 as well, and a 1000-step march).
 factorisation  the mixed solve's FP32 LU + FP32 inverse of this workload's AIC through the
         tensor-core path (tcgen05 TF32, three-pass split; the default) and through the FP32
         CUDA-core path, and the tensor-core GEMM alone at the LU's trailing-update shape
@@ -476,6 +477,12 @@ def main():
         del dce
 
     serving = serving_bench(args, torch) if args.serving_cases > 0 else None
+    linear = None
+    if rank == 0 and not args.small:
+        try:  # the linearised UVLM at C1 size (its own leg: --linear)
+            linear = linear_bench(torch, small=True)
+        except Exception as e:  # keep the headline line if this leg fails
+            linear = {"error": f"{type(e).__name__}: {e}"}
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -494,6 +501,7 @@ def main():
                    "parallelism": f"independent case replica per GPU x{world}", "seed": case.seed},
         "e2e": e2e, "fp64_gpu": fp64, "roofline": roof, "cpu_baseline": cpu, "factorisation": factor,
         "gpu_launches": int(launches), "clocks": clk.summary(), "serving": serving, "autotune": autotune,
+        "linear": linear,
     }
     print(json.dumps(line))
     return 0

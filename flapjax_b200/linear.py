@@ -439,7 +439,7 @@ def _assemble(ops, lay, ref, cfg):
 
     ref: host arrays per surface (zeta_b, zeta_w, gamma_b, gamma_w); cfg: wake_type,
     free_wake, kernel, r_cut, force_r_cut, dt, rho, flowfield, t, bound_upwash,
-    wake_upwash, unsteady_force.  Returns (R_state, R_out), the Jacobians of the next
+    wake_upwash, unsteady_force, delta_w (per surface or None).  Returns (R_state, R_out), the Jacobians of the next
     states and of the outputs, each (rows, n_states + n_inputs), on the ops' device."""
     torch = ops.torch
     S = len(lay.dims)
