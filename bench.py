@@ -625,47 +625,57 @@ def residual_bench(torch):
 
 def linear_bench(torch, small=False):
     """The linearised UVLM (aero/linear/linear_uvlm.py) about the static solution: wall time
-    of the assembly of A, B, C, D on the device (after one warm-up assembly), and the linear
-    system's time march (x_n = A x_{n-1} + B u_n, y_n = C x_n + D u_n) over 1000 steps of
-    seeded input perturbations, device-timed with CUDA events.  small: the C1 frozen-wake
-    line only, with a 20-step march (the case the launch-list profile captures)."""
+    of the assembly of A, B, C, D on the device (the faster of two assemblies), the peak
+    device memory, and the linear system's time march (x_n = A x_{n-1} + B u_n,
+    y_n = C x_n + D u_n) over 1000 steps of seeded input perturbations, device-timed with
+    CUDA events.  small: the C1 frozen-wake line only, with a 20-step march (the case the
+    launch-list profile captures).  A line that runs out of device memory is recorded as
+    such and the others still run."""
+    out = []
+    lines = (("C1 wing 8x32, W=64", (8, 32, 64), "frozen"), ("C1 wing 8x32, W=64", (8, 32, 64), "prescribed"),
+             ("C3 wing 12x64, W=100", (12, 64, 100), "frozen"), ("C2 wing 16x128, W=200", (16, 128, 200), "frozen"))
+    for label, (m, n, w), wt in lines[:1] if small else lines:
+        torch.cuda.empty_cache()
+        torch.cuda.reset_peak_memory_stats()
+        try:
+            out.append(_linear_line(torch, label, m, n, w, wt, 20 if small else 1000))
+        except torch.cuda.OutOfMemoryError as e:
+            out.append({"workload": f"{label}, {wt} wake", "error": f"OutOfMemoryError: {str(e)[:200]}"})
+    torch.cuda.empty_cache()
+    return out
+
+
+def _linear_line(torch, label, m, n, w, wt, n_t):
     import flapjax_b200 as fj
     from flapjax_b200 import cases
     from flapjax_b200.linear import LinearUVLM
 
-    out = []
-    lines = (("C1 wing 8x32, W=64", (8, 32, 64), "frozen"), ("C1 wing 8x32, W=64", (8, 32, 64), "prescribed"),
-             ("C3 wing 12x64, W=100", (12, 64, 100), "frozen"))
-    for label, (m, n, w), wt in lines[:1] if small else lines:
-        c = cases.wing_heave(m=m, n=n, m_star=w, n_steps=1)
-        uv = fj.UVLM([fj.GridDiscretisation(m, n, w)], np.arange(n + 1), kernel=fj.biot_savart_epsilon)
-        uv.set_design_variables(dt=c.dt, flowfield=fj.Constant(c.u_inf, c.rho, True), zeta_b0=c.zeta_b0, hg0=c.hg0)
-        st = uv.solve_static()
-        lin = LinearUVLM(uv, st, wt)
-        times = []
-        for _ in range(2):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            sys_ = lin.linearise()
-            torch.cuda.synchronize()
-            times.append(time.perf_counter() - t0)
-        rng = np.random.default_rng(0)
-        n_t = 20 if small else 1000
-        u = torch.as_tensor(1e-4 * rng.normal(size=(n_t, lin.n_inputs))).cuda()
-        sys_.run(u[:10])
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        sys_.run(u)
-        e1.record()
+    c = cases.wing_heave(m=m, n=n, m_star=w, n_steps=1)
+    uv = fj.UVLM([fj.GridDiscretisation(m, n, w)], np.arange(n + 1), kernel=fj.biot_savart_epsilon)
+    uv.set_design_variables(dt=c.dt, flowfield=fj.Constant(c.u_inf, c.rho, True), zeta_b0=c.zeta_b0, hg0=c.hg0)
+    lin = LinearUVLM(uv, uv.solve_static(), wt, skip_linearisation=True)
+    times, sys_ = [], None
+    for _ in range(2):
+        sys_ = None  # one system alive at a time
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        out.append({"workload": f"{label}, {wt} wake, epsilon kernel", "n_states": lin.n_states,
-                    "n_inputs": lin.n_inputs, "n_outputs": lin.n_outputs, "linearise_s": min(times),
-                    "matrix_bytes": 8 * (lin.n_states + lin.n_outputs) * (lin.n_states + lin.n_inputs),
-                    "run_steps_per_s": n_t / (ms * 1e-3)})
-        del lin, sys_, u
-        torch.cuda.empty_cache()
-    return out
+        t0 = time.perf_counter()
+        sys_ = lin.linearise()
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    peak = torch.cuda.max_memory_allocated() / 1e9
+    rng = np.random.default_rng(0)
+    u = torch.as_tensor(1e-4 * rng.normal(size=(n_t, lin.n_inputs))).cuda()
+    sys_.run(u[:10])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    sys_.run(u)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"workload": f"{label}, {wt} wake, epsilon kernel", "n_states": lin.n_states, "n_inputs": lin.n_inputs,
+            "n_outputs": lin.n_outputs, "linearise_s": min(times),
+            "matrix_bytes": 8 * (lin.n_states + lin.n_outputs) * (lin.n_states + lin.n_inputs),
+            "peak_device_gb_assembly": peak, "run_steps_per_s": n_t / (ms * 1e-3)}
 
 
 def measured_peaks():

@@ -829,7 +829,9 @@ def _steady_force_rows(ops, lay, cfg, Zb, Zw, gb, gw, tZb, tZw, tgb, tgw, lists)
     # per filament: rho g (dv x r) + rho g (v x dr) + rho dg (v x r)
     dv3 = dv.reshape(nf, 3, ncol)
     r_t = ops.tensor(rv)[:, :, None].expand(nf, 3, ncol)
-    df = torch.linalg.cross(dv3, r_t, dim=1) * ops.tensor(rho * gval)[:, None, None]
+    df = torch.linalg.cross(dv3, r_t, dim=1)
+    del dv, dv3, r_t
+    df *= ops.tensor(rho * gval)[:, None, None]
     rows, cl, vals = [], [], []
     vx = _skew(v) * (rho * gval)[:, None, None]                           # rho g [v]x
     for sign, end in ((1.0, fb), (-1.0, fa)):
@@ -851,9 +853,11 @@ def _steady_force_rows(ops, lay, cfg, Zb, Zw, gb, gw, tZb, tZw, tgb, tgw, lists)
                   accumulate=True)
     # split to the vertices: each filament's force half to either end
     out = ops.zeros(3 * lay.NVB, ncol)
+    df *= 0.5
     for end in (fa, fb):
         idx = torch.as_tensor((3 * end[:, None] + np.arange(3)[None, :]).ravel(), device=dev)
-        out.index_add_(0, idx, 0.5 * df)
+        out.index_add_(0, idx, df)
+    del df
     _mask(out, lay, lists["f_steady"])
     return out
 
@@ -1033,7 +1037,9 @@ class LinearUVLM:
                          for j in _output_jacobians(output_projection, fs0, fu0))
         a, b, c, d = _project(self._ops.torch, lay, r_state[:, :ns], r_state[:, ns:], r_out[:, :ns], r_out[:, ns:],
                               jin, jout)
-        return LinearSystem(a.contiguous(), b.contiguous(), c.contiguous(), d.contiguous(), self.dt)
+        # A | B and C | D stay views of the two assembled blocks (row stride n_states +
+        # n_inputs): the products take strided operands, and no second copy is made
+        return LinearSystem(a, b, c, d, self.dt)
 
     # -- vectors ------------------------------------------------------------------------
     def reference_states(self) -> np.ndarray:
