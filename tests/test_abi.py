@@ -49,6 +49,34 @@ def test_error_string_without_gpu():
         _lib.check(st)
 
 
+def test_influence_jacobian_arguments_are_checked_on_cpu():
+    """The linear model's entry points reject bad arguments before any CUDA call."""
+    lib = _lib.load()
+    buf = (C.c_double * 64)()
+    p = C.cast(buf, C.c_void_p)
+    # the unregularised kernel has no hand-written derivatives
+    st = lib.fj_vertex_jacobian(p, 2, None, p, p, 1, 1, None, None, _lib.FJ_KERNEL_PLAIN, 0.0, p, 12, None)
+    assert st == _lib.FJ_ERR_UNSUPPORTED and b"epsilon and cutoff" in lib.fj_last_error_string()
+    st = lib.fj_ring_influence(p, 2, None, p, 1, 1, None, None, _lib.FJ_KERNEL_PLAIN, 0.0, p, 1, None)
+    assert st == _lib.FJ_ERR_UNSUPPORTED
+    # leading dimension below the block width; negative sizes; null outputs
+    assert lib.fj_ring_influence(p, 2, None, p, 2, 3, None, None, _lib.FJ_KERNEL_EPSILON, 0.0, p, 5,
+                                 None) == _lib.FJ_ERR_SHAPE
+    assert lib.fj_vertex_jacobian(p, 2, None, p, p, 1, 1, None, None, _lib.FJ_KERNEL_EPSILON, 0.0, p, 11,
+                                  None) == _lib.FJ_ERR_SHAPE
+    assert lib.fj_vertex_jacobian(p, -1, None, p, p, 1, 1, None, None, _lib.FJ_KERNEL_EPSILON, 0.0, p, 12,
+                                  None) == _lib.FJ_ERR_SHAPE
+    assert lib.fj_ring_influence(p, 2, None, p, 1, 1, None, None, _lib.FJ_KERNEL_EPSILON, 0.0, None, 1,
+                                 None) == _lib.FJ_ERR_SHAPE
+    # the many-right-hand-side solve: workspace, leading dimension
+    nb = C.c_size_t()
+    assert lib.fj_lu_solve_many_workspace_size(100, 300, C.byref(nb)) == _lib.FJ_OK
+    assert nb.value >= 100 * 300 * 8 + 100 * 4
+    assert lib.fj_lu_solve_many(p, 100, p, p, 300, 300, p, nb.value - 1, None) == _lib.FJ_ERR_NOMEM
+    assert lib.fj_lu_solve_many(p, 100, p, p, 300, 299, p, nb.value, None) == _lib.FJ_ERR_SHAPE
+    assert lib.fj_lu_solve_many_workspace_size(0, 3, C.byref(nb)) == _lib.FJ_ERR_SHAPE
+
+
 def test_workspace_size_is_computable_on_cpu():
     cfg = _lib.FjCaseConfig()
     cfg.n_surf = 1
