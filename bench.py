@@ -196,51 +196,55 @@ def C_byref(x):
     return ctypes.byref(x)
 
 
-def e2e_run(uv, dc, case, first, last, torch):
+def e2e_run(uv, dc, case, first, last, torch, chunk=8):
     """Per step: H2D of the step's frames (pinned), the step through the C ABI, D2H of the
-    step's solution slot (pinned).  The copies run on a second stream: step i+1's frames
-    go up while step i computes, and step i's slot comes back while step i+1 computes
-    (results double-buffered in pinned memory).  The compute stream waits on each upload
-    before its step and on the last read-back before the closing event, so the one timed
-    region (two events around the loop) holds every step's copies and compute.  Returns
-    ([ms of the loop], bytes in per step, bytes out per step)."""
+    step's solution slot (pinned).  The C ABI call advances `chunk` steps at a time (it
+    synchronises once per call to report a zero pivot, a NaN or a failed refinement of
+    any of its steps).  The copies run on a second stream: the next chunk's frames go up
+    while a chunk computes, and its slots come back while the next chunk computes
+    (results double-buffered in pinned memory).  The compute stream waits on the uploads
+    before each call and on the last read-back before the closing event, so the one
+    timed region (two events around the loop) holds every step's copies and compute.
+    Returns ([ms of the loop], bytes in per step, bytes out per step)."""
     n_nodes = case.hg0.shape[0]
     hg = torch.from_numpy(np.ascontiguousarray(case.hg_t)).pin_memory()
     hgd = torch.from_numpy(np.ascontiguousarray(case.hg_dot_t)).pin_memory()
     fields = list(dc.arrays)
     outs = [{k: torch.empty(dc.arrays[k].shape[1], dtype=torch.float64).pin_memory() for k in fields}
-            for _ in range(2)]
-    out_ft = [torch.empty(3, dtype=torch.float64).pin_memory() for _ in range(2)]
+            for _ in range(2 * chunk)]
+    out_ft = [torch.empty(3, dtype=torch.float64).pin_memory() for _ in range(2 * chunk)]
     main = torch.cuda.current_stream()
     copy = torch.cuda.Stream()
     bytes_in = 2 * n_nodes * 16 * 8
     bytes_out = sum(v.numel() * 8 for v in outs[0].values()) + 3 * 8
     up = {i: torch.cuda.Event() for i in range(first, last)}
-    done = {i: torch.cuda.Event() for i in range(first, last)}
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(main)
     copy.wait_event(e0)
 
-    def upload(i):
+    def upload(i0, i1):
         with torch.cuda.stream(copy):
-            dc.hg_t[i].copy_(hg[i], non_blocking=True)
-            dc.hg_dot_t[i].copy_(hgd[i], non_blocking=True)
-            up[i].record(copy)
+            for i in range(i0, i1):
+                dc.hg_t[i].copy_(hg[i], non_blocking=True)
+                dc.hg_dot_t[i].copy_(hgd[i], non_blocking=True)
+                up[i].record(copy)
 
-    upload(first)
-    for i in range(first, last):
-        main.wait_event(up[i])
-        dc.solve_dynamic(i, i + 1, reuse_factors=i > 1)
-        done[i].record(main)
-        if i + 1 < last:
-            upload(i + 1)
+    upload(first, min(first + chunk, last))
+    for c0 in range(first, last, chunk):
+        c1 = min(c0 + chunk, last)
+        main.wait_event(up[c1 - 1])  # the copy stream uploads in order
+        dc.solve_dynamic(c0, c1, reuse_factors=c0 > 1)
+        done = torch.cuda.Event()
+        done.record(main)
+        upload(c1, min(c1 + chunk, last))
         with torch.cuda.stream(copy):
-            copy.wait_event(done[i])
-            o = outs[i % 2]
-            for k in fields:
-                o[k].copy_(dc.arrays[k][i], non_blocking=True)
-            out_ft[i % 2].copy_(dc.force_total[i], non_blocking=True)
+            copy.wait_event(done)
+            for i in range(c0, c1):
+                o = outs[(i - first) % (2 * chunk)]
+                for k in fields:
+                    o[k].copy_(dc.arrays[k][i], non_blocking=True)
+                out_ft[(i - first) % (2 * chunk)].copy_(dc.force_total[i], non_blocking=True)
     main.wait_stream(copy)
     e1.record(main)
     torch.cuda.synchronize()
@@ -473,7 +477,8 @@ def main():
         te = replicas.max_over_ranks(sum(ms_e), dev)
         e2e = {"value": world * K / (te * 1e-3), "unit": UNIT, "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
                "copies": "each step's frames H2D and solution slot D2H (pinned) on a copy stream overlapping the "
-                         "neighbouring steps' compute; one event pair around the whole loop"}
+                         "neighbouring chunk's compute; one event pair around the whole loop",
+               "steps_per_call": 8}
         del dce
 
     serving = serving_bench(args, torch) if args.serving_cases > 0 else None
