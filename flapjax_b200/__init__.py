@@ -6,7 +6,8 @@ The computation lives in ``libfj_uvlm.so`` (CUDA, C ABI declared in
 from .data_structures import AeroCase, ArrayList, GridDiscretisation
 from .flowfields import Constant, FlowField, OneMinusCosine
 from .kernels import biot_savart, biot_savart_cutoff, biot_savart_epsilon, cutoff_kernel
-from .linear import LinearInputProjection, LinearOutputProjection, LinearSystem, LinearUVLM
+from .linear import (AeroInputUnflattened, AeroLinearResult, AeroOutputUnflattened, AeroStateUnflattened,
+                     LinearInputProjection, LinearOutputProjection, LinearSystem, LinearUVLM)
 from .polars import TabulatedPolar, tabulate
 from .uvlm import UVLM, make_rectangular_grid
 
@@ -14,4 +15,5 @@ __all__ = [
     "AeroCase", "ArrayList", "GridDiscretisation", "Constant", "FlowField", "OneMinusCosine", "biot_savart",
     "biot_savart_cutoff", "biot_savart_epsilon", "cutoff_kernel", "UVLM", "make_rectangular_grid", "TabulatedPolar",
     "tabulate", "LinearUVLM", "LinearSystem", "LinearInputProjection", "LinearOutputProjection",
+    "AeroInputUnflattened", "AeroStateUnflattened", "AeroOutputUnflattened", "AeroLinearResult",
 ]

@@ -94,6 +94,54 @@ class LinearOutputProjection:
     fd_step: float = 1e-6
 
 
+@dataclass
+class AeroInputUnflattened:
+    """Inputs per surface, time-batched in ``run`` (aero/linear/data_structures.py:16-22):
+    zeta_b and zeta_b_dot (n_tstep, m+1, n+1, 3), nu_b the same or None, nu_w
+    (n_tstep, m_star+1, n+1, 3) or None."""
+
+    zeta_b: list
+    zeta_b_dot: list
+    nu_b: list | None = None
+    nu_w: list | None = None
+
+
+@dataclass
+class AeroStateUnflattened:
+    """States per surface (aero/linear/data_structures.py:24-31)."""
+
+    gamma_b: list
+    gamma_w: list
+    gamma_b_nm1: list | None = None
+    zeta_w: list | None = None
+    zeta_b: list | None = None
+
+
+@dataclass
+class AeroOutputUnflattened:
+    """Outputs per surface (aero/linear/data_structures.py:33-36)."""
+
+    f_steady: list
+    f_unsteady: list | None = None
+
+
+@dataclass
+class AeroLinearResult:
+    """A linear run (aero/linear/data_structures.py:39-): perturbations u_t, x_t, y_t and
+    totals (reference + perturbation), per surface with a leading time axis."""
+
+    reference: object
+    u_t: AeroInputUnflattened
+    x_t: AeroStateUnflattened
+    y_t: AeroOutputUnflattened
+    u_t_tot: AeroInputUnflattened
+    x_t_tot: AeroStateUnflattened
+    y_t_tot: AeroOutputUnflattened
+    n_tstep: int
+    n_surf: int
+    t: np.ndarray
+
+
 def _fd_columns(fun, x0, h):
     """Central-difference Jacobian of fun (vector -> tuple of vectors) at x0: one matrix
     per output."""
@@ -1052,10 +1100,79 @@ class LinearUVLM:
         r = self._ref
         return np.concatenate([np.concatenate([np.ravel(a) for a in r[k]]) for k, _ in self.layout.y_blocks])
 
-    def run(self, u, x0=None):
-        """Perturbation histories (x, y) of the linear system for input perturbations u
-        (n_tstep, n_inputs) from x0, and the totals (reference + perturbation) as numpy
-        arrays: returns (x, y, x_total, y_total)."""
+    def run_vectors(self, u, x0=None):
+        """The linear system over packed input perturbations u (n_tstep, n_inputs) from the
+        packed state perturbation x0: (x, y, x_total, y_total) as numpy arrays."""
         x, y = self.sys.run(u, x0)
         x, y = x.cpu().numpy(), y.cpu().numpy()
         return x, y, x + self.reference_states()[None], y + self.reference_outputs()[None]
+
+    def _blocks_t(self, blocks, vec_t):
+        """(n_tstep, size) -> {name: [per surface (n_tstep, *shape)]} in the blocks' order."""
+        out, off = {}, 0
+        n_t = vec_t.shape[0]
+        for name, _ in blocks:
+            tmpl = self._template(name)
+            out[name] = []
+            for a in tmpl:
+                out[name].append(vec_t[:, off:off + a.size].reshape((n_t,) + a.shape))
+                off += a.size
+        return out
+
+    def _template(self, name):
+        r = self._ref
+        return {"zeta_b": r["zeta_b"], "zeta_b_dot": r["zeta_b"], "nu_b": r["zeta_b"], "nu_w": r["zeta_w"],
+                "gamma_b": r["gamma_b"], "gamma_w": r["gamma_w"], "gamma_b_nm1": r["gamma_b"],
+                "zeta_w": r["zeta_w"], "f_steady": r["f_steady"], "f_unsteady": r["f_steady"]}[name]
+
+    def _reference_value(self, name):
+        r = self._ref
+        if name in ("nu_b", "nu_w"):
+            return [np.zeros_like(a) for a in self._template(name)]
+        key = {"gamma_b_nm1": "gamma_b"}.get(name, name)
+        return r[key]
+
+    def run(self, u: AeroInputUnflattened, x0: AeroStateUnflattened | None = None, flowfield=None):
+        """aero/linear/linear_uvlm.py:869-972: march the linear system over the input
+        perturbations u (per surface, time-batched), from the state perturbation x0 (zero
+        if None).  A flow field adds the bound and wake upwash perturbations
+        U(zeta, t) - U(zeta, t_0) at the reference lattices, t = t_ref + i dt."""
+        if self.prescribed_wake and self.sys.removed_u_np1:
+            warnings.warn("Wake perturbations coordinates at the trailing edge are zero when removing u_np1 from the "
+                          "system.")
+        n_t = int(np.shape(u.zeta_b[0])[0])
+        t0 = float(np.asarray(self._reference.t).ravel()[0])
+        t = t0 + np.arange(n_t) * self.dt
+        nu = {"nu_b": None if u.nu_b is None else [np.asarray(a, np.float64) for a in u.nu_b],
+              "nu_w": None if u.nu_w is None else [np.asarray(a, np.float64) for a in u.nu_w]}
+        for name, flag, lat in (("nu_b", self.bound_upwash, self._ref["zeta_b"]),
+                                ("nu_w", self.wake_upwash, self._ref["zeta_w"])):
+            if not flag:
+                continue
+            if flowfield is None and nu[name] is None:
+                warnings.warn(f"No flowfield or {'bound' if name == 'nu_b' else 'wake'} upwash perturbations provided. "
+                              f"Assuming zero {'bound' if name == 'nu_b' else 'wake'} upwash perturbations.")
+                nu[name] = [np.zeros((n_t,) + z.shape) for z in lat]
+            if flowfield is not None:
+                flow = [np.stack([flowfield(z, ti) - flowfield(z, t[0]) for ti in t]) for z in lat]
+                nu[name] = flow if nu[name] is None else [a + b for a, b in zip(nu[name], flow)]
+        given = {"zeta_b": u.zeta_b, "zeta_b_dot": u.zeta_b_dot, **nu}
+        u_vec = np.concatenate([np.concatenate([np.asarray(a, np.float64).reshape(n_t, -1) for a in given[k]], axis=1)
+                                for k, _ in self.layout.u_blocks], axis=1)
+        x0_vec = None
+        if x0 is not None:
+            x0_vec = np.concatenate([np.concatenate([np.ravel(a) for a in getattr(x0, k)])
+                                     for k, _ in self.layout.x_blocks])
+        x, y, _, _ = self.run_vectors(u_vec, x0_vec)
+        ud = self._blocks_t(self.layout.u_blocks, u_vec)
+        xd = self._blocks_t(self.layout.x_blocks, x)
+        yd = self._blocks_t(self.layout.y_blocks, y)
+
+        def total(d):
+            return {k: [a + r[None] for a, r in zip(v, self._reference_value(k))] for k, v in d.items()}
+
+        return AeroLinearResult(reference=self._reference, u_t=AeroInputUnflattened(**ud),
+                                x_t=AeroStateUnflattened(**xd), y_t=AeroOutputUnflattened(**yd),
+                                u_t_tot=AeroInputUnflattened(**total(ud)), x_t_tot=AeroStateUnflattened(**total(xd)),
+                                y_t_tot=AeroOutputUnflattened(**total(yd)), n_tstep=n_t,
+                                n_surf=len(self.layout.dims), t=t)

@@ -119,7 +119,7 @@ def test_linear_model_matches_reference(cuda, name):
         got = getattr(lin.sys, k).cpu().numpy()
         assert got.shape == g[k].shape, k
         assert np.abs(got - g[k]).max() <= 1e-8 * max(1.0, np.abs(g[k]).max()), k
-    x, y, _, _ = lin.run(g["u_run"], g["x0_run"])
+    x, y, _, _ = lin.run_vectors(g["u_run"], g["x0_run"])
     assert np.allclose(x, g["x_run"], rtol=0, atol=1e-10) and np.allclose(y, g["y_run"], rtol=0, atol=1e-10)
 
 
@@ -211,6 +211,40 @@ def test_linear_model_projections(cuda, name):
         assert np.abs(got - g[k]).max() <= 1e-8 * max(1.0, np.abs(g[k]).max()), k
 
 
+def test_run_with_unflattened_inputs(cuda):
+    """LinearUVLM.run as the reference calls it (aero/linear/linear_uvlm.py:869-972):
+    per-surface time-batched inputs, a gust flow field turned into upwash perturbations,
+    per-surface results and totals; equal to the packed march."""
+    import flapjax_b200 as fj
+    from flapjax_b200.linear import AeroInputUnflattened, LinearUVLM
+
+    g = LG.load("linear_frozen")
+    uv = _product_uvlm(g)
+    lin = LinearUVLM(uv, uv.solve_static(), "frozen", device=cuda)
+    lay, n_t = lin.layout, 5
+    rng = np.random.default_rng(3)
+    zb = [1e-3 * rng.normal(size=(n_t,) + np.shape(a)) for a in lin._ref["zeta_b"]]
+    zbd = [1e-3 * rng.normal(size=(n_t,) + np.shape(a)) for a in lin._ref["zeta_b"]]
+    gust = fj.OneMinusCosine(g["u_inf"], float(g["rho"]), True, gust_length=1.0, gust_amplitude=0.1,
+                             gust_x0=np.array([-1.0, 0.0, 0.0]))
+    res = lin.run(AeroInputUnflattened(zeta_b=zb, zeta_b_dot=zbd), flowfield=gust)
+    t = np.arange(n_t) * lin.dt
+    nu_b = [np.stack([gust(z, ti) - gust(z, 0.0) for ti in t]) for z in lin._ref["zeta_b"]]
+    nu_w = [np.stack([gust(z, ti) - gust(z, 0.0) for ti in t]) for z in lin._ref["zeta_w"]]
+    u = np.concatenate([np.concatenate([a.reshape(n_t, -1) for a in blk], axis=1) for blk in (zb, zbd, nu_b, nu_w)],
+                       axis=1)
+    x, y, xt, yt = lin.run_vectors(u)
+    assert res.n_tstep == n_t and np.allclose(res.t, t)
+    assert np.abs(np.concatenate([a.reshape(n_t, -1) for a in res.u_t.nu_w], axis=1) - u[:, -nu_w[0][0].size:]).max() == 0
+    got_x = np.concatenate([a.reshape(n_t, -1) for k, _ in lay.x_blocks for a in getattr(res.x_t, k)], axis=1)
+    got_y = np.concatenate([a.reshape(n_t, -1) for k, _ in lay.y_blocks for a in getattr(res.y_t, k)], axis=1)
+    assert np.array_equal(got_x, x) and np.array_equal(got_y, y)
+    tot_y = np.concatenate([a.reshape(n_t, -1) for k, _ in lay.y_blocks for a in getattr(res.y_t_tot, k)], axis=1)
+    assert np.allclose(tot_y, yt, rtol=0, atol=1e-14)
+    assert np.allclose(res.u_t_tot.zeta_b[0], lin._ref["zeta_b"][0][None] + zb[0], rtol=0, atol=1e-15)
+    assert np.abs(res.y_t.f_steady[0]).max() > 0
+
+
 def test_linear_model_follows_nonlinear_heave(cuda):
     """A heave of 1e-4 chords: the force perturbations of the linear system equal those of
     the nonlinear prescribed-motion solve to second order in the amplitude (cutoff kernel,
@@ -237,7 +271,7 @@ def test_linear_model_follows_nonlinear_heave(cuda):
         zdi = np.einsum("jab,ijb->ija", c.hg_dot_t[i][:, :3, :3], c.zeta_b0) + c.hg_dot_t[i][None, :, :3, 3]
         u[i, zb[0]:zb[1]] = (zi - z0).ravel()
         u[i, zbd[0]:zbd[1]] = zdi.ravel()
-    _, y, _, _ = lin.run(u)
+    _, y, _, _ = lin.run_vectors(u)
     nv = (c.m + 1) * (c.n + 1) * 3
     f_lin = (y[:, :nv] + y[:, nv:2 * nv]).reshape(n_t, -1, 3).sum(axis=1)
     f_ref = np.asarray(st.f_steady[0]).sum(axis=(0, 1))
