@@ -204,8 +204,8 @@ class LinearSystem:
                                  f"input 'x0'")
             x[0] = x0
         bu = u @ self.b.T  # every step's input term in one product
-        for i in range(1, n_t):
-            x[i] = self.a @ x[i - 1] + (bu[i - 1] if self.removed_u_np1 else bu[i])
+        for i in range(1, n_t):  # one GEMV-with-add per step
+            torch.addmv(bu[i - 1] if self.removed_u_np1 else bu[i], self.a, x[i - 1], out=x[i])
         y = x @ self.c.T + u @ self.d.T
         return x, y
 
