@@ -9,7 +9,10 @@
 //
 // Host code cannot use the array's name as a device address (on the host it names a
 // stand-in object), so the address is fetched with cudaGetSymbolAddress, once per device,
-// with that device current, on the first call made on that device.
+// with that device current, on the first call made on that device.  The fetched address
+// is kept for the life of the process: it does not survive cudaDeviceReset (which
+// reloads this module), so a caller that resets a device must not call this entry point
+// on that device afterwards.
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -64,12 +67,19 @@ extern "C" FJ_API int fj_vind_noalloc(const double* d_targets, int64_t n_targets
     const int img = mirror ? 2 : 1;
     int64_t n_elem = 0, n_links = 0;
     for (int i = 0; i < n_lattices; ++i) {
-        if (rows[i] < 0 || cols[i] < 0)
+        if (rows[i] < 0 || cols[i] < 0 || rows[i] >= (1 << 24) || cols[i] >= (1 << 24))
             return fail(FJ_ERR_SHAPE, "fj_vind_noalloc: lattice %d has rows=%d cols=%d", i, rows[i], cols[i]);
         n_elem += img * stream_len(rows[i], cols[i]);
         n_links += img * lattice_links(rows[i], cols[i]);
     }
-    // scratch = [stream][partials]; refuse sizes the fixed array cannot hold
+    // scratch = [stream][partials]; refuse sizes the fixed array cannot hold (the target
+    // count first, so that the byte counts below cannot wrap)
+    if (n_targets > (int64_t)(kNoAllocScratchBytes / (3 * sizeof(double))) ||
+        n_elem > (int64_t)(kNoAllocScratchBytes / sizeof(Elem32)))
+        return fail(FJ_ERR_SHAPE,
+                    "fj_vind_noalloc: %lld targets and %lld filament-stream elements exceed its fixed %zu-byte "
+                    "array; use fj_vind with a caller workspace",
+                    (long long)n_targets, (long long)n_elem, kNoAllocScratchBytes);
     const size_t elem_bytes = precision == FJ_PREC_FP64 ? sizeof(Elem64) : sizeof(Elem32);
     const size_t stream_bytes = align_up((size_t)n_elem * elem_bytes, 256);
     const size_t part_per_split = (size_t)std::max<int64_t>(n_targets, 1) * 3 * sizeof(double);

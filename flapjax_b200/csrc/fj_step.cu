@@ -1932,7 +1932,7 @@ int fj_vind(const double* d_targets, int64_t n_targets, const double* const* d_z
     j.n_links = 0;
     for (int i = 0; i < n_lattices; ++i) j.n_links += (mirror ? 2 : 1) * lattice_links(rows[i], cols[i]);
     FJ_TRY(vind_launch(j, precision, kernel, r_cut, s));
-    return reduce_partials(part, sp, n_targets, d_v_out, 0, 1.0, s);
+    return reduce_partials(part, j.n_split, n_targets, d_v_out, 0, 1.0, s);
 }
 
 int fj_aic_workspace_size(const int* m, const int* n, int n_surf, size_t* bytes) {

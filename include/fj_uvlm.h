@@ -302,8 +302,9 @@ FJ_API int fj_lu_solve_many(const double* d_lu, int n, const int32_t* d_piv, dou
  * the library's device memory, reserved on every GPU that loads the library; sizes whose
  * filament stream plus one set of partial velocities exceed it are refused with
  * FJ_ERR_SHAPE.  The first call on a device looks the array up (cudaGetSymbolAddress) and
- * should come before any stream capture.  All calls share the array: calls that overlap
- * on the GPU (other streams, other host threads) race and must be serialised. */
+ * should come before any stream capture; the address it keeps does not survive a
+ * cudaDeviceReset of that device.  All calls share the array: calls that overlap on the
+ * GPU (other streams, other host threads) race and must be serialised. */
 FJ_API int fj_vind_noalloc(const double* d_targets, int64_t n_targets, const double* const* d_zetas,
                            const double* const* d_gammas, const int* rows, const int* cols,
                            int n_lattices, const double* mirror_point, const double* mirror_normal,

@@ -76,7 +76,7 @@ def _lattices(rng, shapes):
     return out
 
 
-def _fj_vind(dev, targets, lats, kernel, r_cut, precision, mirror=None):
+def _fj_vind(dev, targets, lats, kernel, r_cut, precision, mirror=None, ws_fill=None):
     import torch
 
     from flapjax_b200 import _lib
@@ -97,6 +97,8 @@ def _fj_vind(dev, targets, lats, kernel, r_cut, precision, mirror=None):
     _lib.call("fj_vind_workspace_size", targets.shape[0], rows, cols, n, int(mirror is not None), precision,
               C.byref(nbytes))
     ws = torch.empty(nbytes.value, dtype=torch.uint8, device=dev)
+    if ws_fill is not None:
+        ws.fill_(ws_fill)
     out = torch.empty_like(tt)
     _lib.call("fj_vind", tt.data_ptr(), targets.shape[0], zp, gp, rows, cols, n, mp, mn, kernel, r_cut, precision,
               out.data_ptr(), ws.data_ptr(), ws.numel(), torch.cuda.current_stream(dev).cuda_stream)
@@ -125,6 +127,25 @@ def test_vind_matches_oracle(cuda, kernel, mirror):
     assert rel_err(got64, want) < TOL64
     got32 = _fj_vind(cuda, targets, lats, kid, r_cut, _lib.FJ_PREC_MIXED, mir)
     assert rel_err(got32, want) < TOL_MIXED_V
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_vind_split_below_workspace_bound(cuda, precision):
+    """The workspace is sized for the largest split count a shape allows, and the sum
+    usually runs with fewer (20 000 targets against a 60 x 200 lattice: about 22 FP64 or
+    33 FP32 splits against a bound of 95).  Only the splits that ran may be reduced: the
+    workspace starts as NaN bytes (0xFF), so reading an unwritten slab shows."""
+    from flapjax_b200 import _lib
+
+    rng = np.random.default_rng(17)
+    lats = _lattices(rng, [(60, 200)])
+    targets = rng.normal(size=(20000, 3)) * [1.0, 2.0, 0.3] + [0.5, 1.5, 0.0]
+    prec = _lib.FJ_PREC_FP64 if precision == "fp64" else _lib.FJ_PREC_MIXED
+    got = _fj_vind(cuda, targets, lats, _lib.FJ_KERNEL_EPSILON, 0.0, prec, ws_fill=0xFF)
+    assert np.all(np.isfinite(got))
+    sub = rng.choice(targets.shape[0], 256, replace=False)
+    want = R.compute_v_ind(targets[sub], [lats[0][0]], [lats[0][1]], "epsilon")
+    assert rel_err(got[sub], want) < (TOL64 if precision == "fp64" else TOL_MIXED_V)
 
 
 def test_vind_plain_kernel_fp64(cuda):
@@ -318,9 +339,7 @@ def test_full_heave_config_fp64_and_mixed(cuda):
     cl64, cd64 = coefficients(got.force_total, c)
     clm, cdm = coefficients(gm.force_total, c)
     assert np.max(np.abs(clm - cl64) / np.abs(cl64)) < 1e-6
-    # CD is ~30x smaller than CL here, so the same absolute force error is ~30x larger
-    # relative to CD; measured 1.2e-6 of max|CD|
-    assert np.max(np.abs(cdm - cd64)) / np.max(np.abs(cd64)) < 3e-6
+    assert np.max(np.abs(cdm - cd64)) / np.max(np.abs(cd64)) < 1e-6
     clr, _ = coefficients(oracle_force_total(want), c)
     assert np.max(np.abs(cl64 - clr) / np.abs(clr)) < TOL64
 

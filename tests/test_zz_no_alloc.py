@@ -3,9 +3,10 @@
 Such callers (a plugin host that owns the device memory pool, a real-time loop that may
 not block in cudaMalloc) cannot provide fj_vind's workspace; fj_vind_noalloc uses a fixed
 8 MiB array inside the library instead.  Checked against fj_vind (which takes a caller
-workspace) on two consecutive calls with different inputs, in FP64 (1e-10 normwise, the
-FP64 bar of the other tests) and in the mixed path (2e-6, the FP32 velocity bar), and its
-refusal of sizes beyond the array.
+workspace) and against the FP64 oracle on two consecutive calls with different inputs, in
+FP64 (1e-10 normwise, the FP64 bar of the other tests) and in the mixed path (2e-6, the
+FP32 velocity bar); with a mirror plane; with so many targets that fewer splits fit in the
+array than fj_vind would use; and its refusal of sizes beyond the array.
 """
 from __future__ import annotations
 
@@ -13,6 +14,8 @@ import ctypes as C
 
 import numpy as np
 import pytest
+
+from oracle import uvlm_ref as R
 
 pytestmark = pytest.mark.gpu
 
@@ -34,6 +37,12 @@ def _lattices(rng, shapes):
     return out
 
 
+def _mirror_args(mirror):
+    if mirror is None:
+        return None, None
+    return (C.c_double * 3)(*mirror[0]), (C.c_double * 3)(*mirror[1])
+
+
 def _args(dev, targets, lats):
     zs = [_t(z, dev) for z, _ in lats]
     gs = [_t(g, dev) for _, g in lats]
@@ -49,27 +58,30 @@ def _args(dev, targets, lats):
     )
 
 
-def _with_workspace(dev, a, n_t, kernel, r_cut, precision):
+def _with_workspace(dev, a, n_t, kernel, r_cut, precision, mirror=None):
     import torch
 
     from flapjax_b200 import _lib
 
+    mp, mn = _mirror_args(mirror)
     nbytes = C.c_size_t()
-    _lib.call("fj_vind_workspace_size", n_t, a["rows"], a["cols"], a["n"], 0, precision, C.byref(nbytes))
+    _lib.call("fj_vind_workspace_size", n_t, a["rows"], a["cols"], a["n"], int(mirror is not None), precision,
+              C.byref(nbytes))
     ws = torch.empty(nbytes.value, dtype=torch.uint8, device=dev)
     out = torch.empty((n_t, 3), dtype=torch.float64, device=dev)
-    _lib.call("fj_vind", a["tt"].data_ptr(), n_t, a["zp"], a["gp"], a["rows"], a["cols"], a["n"], None, None, kernel,
+    _lib.call("fj_vind", a["tt"].data_ptr(), n_t, a["zp"], a["gp"], a["rows"], a["cols"], a["n"], mp, mn, kernel,
               r_cut, precision, out.data_ptr(), ws.data_ptr(), ws.numel(), torch.cuda.current_stream(dev).cuda_stream)
     return out.cpu().numpy()
 
 
-def _no_alloc(dev, a, n_t, kernel, r_cut, precision):
+def _no_alloc(dev, a, n_t, kernel, r_cut, precision, mirror=None):
     import torch
 
     from flapjax_b200 import _lib
 
+    mp, mn = _mirror_args(mirror)
     out = torch.empty((n_t, 3), dtype=torch.float64, device=dev)
-    _lib.call("fj_vind_noalloc", a["tt"].data_ptr(), n_t, a["zp"], a["gp"], a["rows"], a["cols"], a["n"], None, None,
+    _lib.call("fj_vind_noalloc", a["tt"].data_ptr(), n_t, a["zp"], a["gp"], a["rows"], a["cols"], a["n"], mp, mn,
               kernel, r_cut, precision, out.data_ptr(), torch.cuda.current_stream(dev).cuda_stream)
     return out.cpu().numpy()
 
@@ -82,15 +94,41 @@ def _rel(a, b):
 def test_noalloc_matches_workspace_version_twice(cuda, precision, tol):
     from flapjax_b200 import _lib
 
-    for call, (seed, shapes, n_t, kernel) in enumerate([(1, [(6, 9), (20, 9)], 500, _lib.FJ_KERNEL_EPSILON),
-                                                        (2, [(12, 30)], 1500, _lib.FJ_KERNEL_CUTOFF)]):
+    mir = (np.array([0.0, -0.2, 0.0]), np.array([0.0, 1.0, 0.0]))
+    for call, (seed, shapes, n_t, kernel, mirror) in enumerate([
+            (1, [(6, 9), (20, 9)], 500, _lib.FJ_KERNEL_EPSILON, None),
+            (2, [(12, 30)], 1500, _lib.FJ_KERNEL_CUTOFF, None),
+            (4, [(5, 8), (15, 8)], 700, _lib.FJ_KERNEL_EPSILON, mir)]):
         rng = np.random.default_rng(seed)
         lats = _lattices(rng, shapes)
         targets = rng.normal(size=(n_t, 3)) * [1.0, 2.0, 0.3] + [0.5, 1.5, 0.0]
         a = _args(cuda, targets, lats)
-        want = _with_workspace(cuda, a, n_t, kernel, 1e-3, precision)
-        got = _no_alloc(cuda, a, n_t, kernel, 1e-3, precision)
+        want = _with_workspace(cuda, a, n_t, kernel, 1e-3, precision, mirror)
+        got = _no_alloc(cuda, a, n_t, kernel, 1e-3, precision, mirror)
         assert _rel(got, want) < tol, (call, _rel(got, want))
+        kname = "epsilon" if kernel == _lib.FJ_KERNEL_EPSILON else "cutoff"
+        ref = R.compute_v_ind(targets, [z for z, _ in lats], [g for _, g in lats], kname, mirror, 1e-3)
+        assert _rel(got, ref) < tol, (call, _rel(got, ref))
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-10), (1, 2e-6)])
+def test_noalloc_caps_splits_to_its_array(cuda, precision, tol):
+    """20 000 targets against a 60 x 200 lattice: one set of partial velocities is 480 kB,
+    so about 14 splits fit beside the filament stream, fewer than the 22 (FP64) or 33
+    (FP32) that fj_vind picks; the result must not depend on the split count."""
+    from flapjax_b200 import _lib
+
+    rng = np.random.default_rng(9)
+    lats = _lattices(rng, [(60, 200)])
+    n_t = 20000
+    targets = rng.normal(size=(n_t, 3)) * [1.0, 2.0, 0.3] + [0.5, 1.5, 0.0]
+    a = _args(cuda, targets, lats)
+    got = _no_alloc(cuda, a, n_t, _lib.FJ_KERNEL_EPSILON, 0.0, precision)
+    want = _with_workspace(cuda, a, n_t, _lib.FJ_KERNEL_EPSILON, 0.0, precision)
+    assert _rel(got, want) < tol
+    sub = rng.choice(n_t, 256, replace=False)
+    ref = R.compute_v_ind(targets[sub], [lats[0][0]], [lats[0][1]], "epsilon")
+    assert _rel(got[sub], ref) < tol
 
 
 def test_noalloc_refuses_sizes_beyond_its_array(cuda):
