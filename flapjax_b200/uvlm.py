@@ -4,8 +4,8 @@
 Supported: any number of surfaces, the epsilon / cutoff / plain kernels, mirror images,
 prescribed and free wakes, the variable wake discretisation ``delta_w``, static (regular
 or horseshoe wake) and prescribed-motion dynamic solves, single-step ``case_solve`` for
-fluid-structure loops, Constant and OneMinusCosine flows.  Not supported (they raise):
-control surfaces (``grid_func``) and polar corrections.
+fluid-structure loops, Constant and OneMinusCosine flows, tabulated strip polars with the
+circulation blend.  Not supported (it raises): control surfaces (``grid_func``).
 
 ``precision="fp64"`` runs the reference's arithmetic in FP64; ``precision="mixed"`` runs
 the Biot-Savart sums in FP32 (FP64 accumulation) and solves with cached FP32 factors
@@ -153,6 +153,7 @@ class UVLM:
         self._step_case = None
         self._step_key = None
         self._step_factored = False
+        self._vind_dev = None
 
     # ---------------------------------------------------------------------------------
     @property
@@ -296,7 +297,22 @@ class UVLM:
         else:
             t, i_ts, ft = h["t"], np.arange(h["t"].shape[0]), h["force_total"]
         f["n"] = f.pop("nc")
-        return AeroCase(**f, t=t, i_ts=i_ts, force_total=ft, flowfield=self.flowfield)
+        return AeroCase(**f, t=t, i_ts=i_ts, force_total=ft, **self._case_meta())
+
+    def _case_meta(self) -> dict:
+        """What an AeroCase needs from its solver: the flow, the vertex-column -> node map
+        (project_forcing_to_beam) and an FP64 induced-velocity sum with this solver's kernel
+        and mirror plane (get_v_ind)."""
+        return dict(flowfield=self.flowfield, dof_mapping=self.dof_mapping, induced=self._induced)
+
+    def _induced(self, targets, zetas, gammas):
+        if self._vind_dev is None:
+            from .adjoint import _Dev
+
+            mirror = None if self.mirror_point is None else (self.mirror_point, self.mirror_normal)
+            self._vind_dev = _Dev(self.device, self.kernel.kernel_id, self.kernel.r_cut, mirror)
+        lats = [(np.asarray(z, float), np.asarray(g, float)) for z, g in zip(zetas, gammas)]
+        return self._vind_dev.vind(np.asarray(targets, float), lats)
 
     @staticmethod
     def _flat(case_field, idx=None):
@@ -330,7 +346,7 @@ class UVLM:
             gamma_b_dot=[np.zeros((g.m, g.n)) for g in gds], gamma_w=[np.zeros((g.m_star, g.n)) for g in gds],
             f_steady=[np.zeros((g.m + 1, g.n + 1, 3)) for g in gds],
             f_unsteady=[np.zeros((g.m + 1, g.n + 1, 3)) for g in gds], alpha=[np.zeros((g.n,)) for g in gds],
-            t=0.0, i_ts=-1, force_total=np.zeros(3), flowfield=self.flowfield)
+            t=0.0, i_ts=-1, force_total=np.zeros(3), **self._case_meta())
 
     def _check_motion(self, hg_t, hg_dot_t):
         check_arr_shape(hg_t, (None, None, 4, 4), "hg_n")

@@ -11,14 +11,16 @@ data_structures.py, algebra/*) runs unmodified.
 Each case is written to ``tests/golden/<name>.npz`` with its inputs and the reference's
 time-batched outputs.  Run from the repository root in this container:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case names]
 
-The GPU box has no /root/reference; only the .npz files travel.
+The reference's ``src`` directory defaults to /root/reference/src; set FLAPJAX_REF_SRC to
+read it from elsewhere.  The GPU box has no reference checkout; only the .npz files travel.
 """
 from __future__ import annotations
 
 import importlib.abc
 import importlib.machinery
+import os
 import sys
 import types
 from pathlib import Path
@@ -27,7 +29,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REF_SRC = Path("/root/reference/src")
+REF_SRC = Path(os.environ.get("FLAPJAX_REF_SRC", "/root/reference/src"))
 
 
 class _Stub(types.ModuleType):
@@ -500,7 +502,69 @@ def run_linear_projected_case(ref, name, c, wake_type, ea_x=0.0, h=1e-6, seed=0)
     print("wrote linear", name)
 
 
-ONLY: set[str] = set()
+def run_fsi_case(ref, name, c, free_wake=False, kernel="epsilon", r_cut=None, n_iter=3):
+    """A fluid-structure loop with the shape of the reference's fsi_convergence_loop
+    (structure/beam.py:2612-2697): the reference's own UVLM.case_solve, then the solved
+    slot's AeroCase.project_forcing_to_beam, then a structural update, ``n_iter`` times per
+    step (tests/fsi_standin.py, a typical-section stand-in for the beam).  Stored per call:
+    the frames, their rates and the projected loads; at the end the case's slots, the
+    structural history, and the reference's get_states / gamma_full / zeta_full of one slot
+    and its projection with and without the unsteady forces."""
+    if ONLY and name not in ONLY:
+        return
+    jnp = ref.jnp
+    from flapjax.aero.data_structures import AeroCase as RefAeroCase
+
+    from tests.fsi_standin import TypicalSection, run_fsi
+
+    kern = {"epsilon": ref.utils.biot_savart_epsilon, "cutoff": ref.utils.biot_savart_cutoff}[kernel]
+    saved_r = ref.utils.R_CUTOFF
+    if r_cut is not None:
+        ref.utils.R_CUTOFF = r_cut
+    try:
+        uv = ref.UVLM(grid_shapes=[ref.GridDiscretisation(c.m, c.n, c.m_star)], dof_mapping=[jnp.arange(c.n + 1)],
+                      kernel=kern, free_wake=free_wake)
+        uv.set_design_variables(dt=float(c.dt), flowfield=ref.Constant(jnp.array(c.u_inf), c.rho, True),
+                                zeta_b0=[jnp.array(c.zeta_b0)], hg0=jnp.array(c.hg0))
+        st = uv.solve_static()
+        case = RefAeroCase.initialise(st, c.n_tstep)
+        struct = TypicalSection(c.hg0[:, 1, 3])
+        rec = []
+        case, (x, v, a) = run_fsi(uv, struct, case, c.n_tstep, c.dt, n_iter=n_iter, record=rec)
+        out = {"case_name": name, "kernel": kernel, "r_cut": r_cut if r_cut is not None else saved_r,
+               "free_wake": free_wake, "dt": c.dt, "u_inf": c.u_inf, "rho": c.rho, "zeta_b0": c.zeta_b0,
+               "hg0": c.hg0, "dims": np.array([c.m, c.n, c.m_star]), "n_tstep": c.n_tstep, "n_iter": n_iter,
+               "rec_i": np.array([r[0] for r in rec]), "rec_it": np.array([r[1] for r in rec]),
+               "rec_hg": np.stack([r[2] for r in rec]), "rec_hg_dot": np.stack([r[3] for r in rec]),
+               "rec_f": np.stack([r[4] for r in rec]), "x": x, "v": v, "a": a}
+        for f in FIELDS:
+            out[f"dyn_{f}"] = np.asarray(getattr(case, f)[0])
+        out["dyn_t"] = np.asarray(case.t)
+        slot = c.n_tstep - 1
+        out["states_slot"] = slot
+        out["states_ravel"] = np.asarray(case.get_states(slot).ravel())
+        out["gamma_full"] = np.concatenate([np.ravel(g) for g in case.gamma_full(slot)])
+        out["zeta_full"] = np.concatenate([np.ravel(z) for z in case.zeta_full(slot)])
+        rng = np.random.default_rng(11)
+        th = rng.normal(size=(c.n + 1, 3)) * 0.2
+        rmat = np.stack([_rot(t) for t in th])
+        out["proj_rmat"] = rmat
+        out["proj_unsteady"] = np.asarray(case.project_forcing_to_beam(slot, jnp.array(rmat), uv.zeta_b0, True))
+        out["proj_steady"] = np.asarray(case.project_forcing_to_beam(slot, jnp.array(rmat), uv.zeta_b0, False))
+        np.savez_compressed(HERE / "fsi" / f"{name}.npz", **{k: np.asarray(v_) for k, v_ in out.items()})
+        print("wrote fsi", name, len(rec), "calls")
+    finally:
+        ref.utils.R_CUTOFF = saved_r
+
+
+def _rot(t):
+    """Rotation matrix of the rotation vector t (Rodrigues)."""
+    a = float(np.linalg.norm(t))
+    k = t / a
+    kx = np.array([[0.0, -k[2], k[1]], [k[2], 0.0, -k[0]], [-k[1], k[0], 0.0]])
+    return np.eye(3) + np.sin(a) * kx + (1.0 - np.cos(a)) * kx @ kx
+
+
 ONLY: set[str] = set()
 
 
@@ -624,6 +688,13 @@ def main():
     c = cases.wing_heave(m=2, n=3, m_star=3, n_steps=1)
     run_linear_projected_case(ref, "linear_projected_frozen", c, "frozen")
     run_linear_projected_case(ref, "linear_projected_prescribed", c, "prescribed", ea_x=0.1)
+
+    # fluid-structure loops: the reference's case_solve + project_forcing_to_beam driven by
+    # a typical-section stand-in for the beam (prescribed and free wake)
+    (HERE / "fsi").mkdir(exist_ok=True)
+    run_fsi_case(ref, "fsi_heave", cases.wing_heave(m=3, n=6, m_star=6, n_steps=6))
+    run_fsi_case(ref, "fsi_free_cutoff", cases.wing_free(m=3, n=6, m_star=5, n_steps=5, seed=2), free_wake=True,
+                 kernel="cutoff", r_cut=1e-3)
 
 
 if __name__ == "__main__":
