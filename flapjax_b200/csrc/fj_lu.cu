@@ -26,7 +26,9 @@ __device__ __forceinline__ T absval(T v) {
 
 template <typename T, int NB>
 __global__ void __launch_bounds__(1024) lu_panel_kernel(T* __restrict__ a, int n, int k,
-                                                        int32_t* __restrict__ piv, int* __restrict__ info) {
+                                                        int32_t* __restrict__ piv, int* __restrict__ info,
+                                                        const int* __restrict__ run_flag) {
+    if (run_flag != nullptr && *run_flag == 0) return;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* P = reinterpret_cast<T*>(smraw);  // (n-k) x LDP, row-major; odd stride avoids bank conflicts
     constexpr int LDP = NB + 1;
@@ -117,7 +119,9 @@ __global__ void __launch_bounds__(1024) lu_panel_kernel(T* __restrict__ a, int n
 // then each column thread loads all the touched values before storing any, one memory
 // round trip instead of one per swap.
 template <typename T, int NB>
-__global__ void lu_swap_trsm_kernel(T* __restrict__ a, int n, int k, const int32_t* __restrict__ piv, int c_end) {
+__global__ void lu_swap_trsm_kernel(T* __restrict__ a, int n, int k, const int32_t* __restrict__ piv, int c_end,
+                                    const int* __restrict__ run_flag) {
+    if (run_flag != nullptr && *run_flag == 0) return;
     __shared__ int s_dst[2 * NB], s_src[2 * NB], s_piv[NB];
     __shared__ int s_cnt;
     __shared__ T s_l[NB][NB];  // the panel's unit-lower diagonal block, for the triangular solve
@@ -229,13 +233,15 @@ __device__ __forceinline__ void lu_update_tile(T* __restrict__ a, int n, int k, 
 
 // A22 -= L21 U12 over rows [k + NB, n) and columns [k + NB, c_end).
 template <typename T, int NB>
-__global__ void __launch_bounds__(256) lu_update_kernel(T* __restrict__ a, int n, int k, int c_end) {
+__global__ void __launch_bounds__(256) lu_update_kernel(T* __restrict__ a, int n, int k, int c_end,
+                                                        const int* __restrict__ run_flag) {
+    if (run_flag != nullptr && *run_flag == 0) return;
     const int k2 = k + NB;
     lu_update_tile<T, NB>(a, n, k, k2 + blockIdx.y * 64, k2 + blockIdx.x * 64, n, c_end);
 }
 
 template <typename T, int NB>
-static int lu_factor_impl(T* a, int n, int32_t* piv, int* d_info, cudaStream_t s) {
+static int lu_factor_impl(T* a, int n, int32_t* piv, int* d_info, cudaStream_t s, const int* run_flag) {
     if (n <= 0) return fail(FJ_ERR_SHAPE, "lu_factor: n=%d", n);
     const size_t smem = (size_t)n * (NB + 1) * sizeof(T);
     if (smem > 220 * 1024) return fail(FJ_ERR_UNSUPPORTED, "lu_factor: n=%d too large for the shared-memory panel", n);
@@ -243,14 +249,15 @@ static int lu_factor_impl(T* a, int n, int32_t* piv, int* d_info, cudaStream_t s
     FJ_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int), s));
     for (int k = 0; k < n; k += NB) {
         const int nb = min(NB, n - k);
-        lu_panel_kernel<T, NB><<<1, 1024, (size_t)(n - k) * (NB + 1) * sizeof(T), s>>>(a, n, k, piv, d_info); note_launch();
+        lu_panel_kernel<T, NB><<<1, 1024, (size_t)(n - k) * (NB + 1) * sizeof(T), s>>>(a, n, k, piv, d_info,
+                                                                                         run_flag); note_launch();
         if (n > nb) {
-            lu_swap_trsm_kernel<T, NB><<<(n + 255) / 256, 256, 0, s>>>(a, n, k, piv, n); note_launch();
+            lu_swap_trsm_kernel<T, NB><<<(n + 255) / 256, 256, 0, s>>>(a, n, k, piv, n, run_flag); note_launch();
         }
         const int rem = n - k - nb;
         if (rem > 0) {
             dim3 g((rem + 63) / 64, (rem + 63) / 64);
-            lu_update_kernel<T, NB><<<g, 256, 0, s>>>(a, n, k, n); note_launch();
+            lu_update_kernel<T, NB><<<g, 256, 0, s>>>(a, n, k, n, run_flag); note_launch();
         }
     }
     FJ_LAUNCH_CHECK("lu_factor");
@@ -264,14 +271,14 @@ static bool panel_fits(int n, int nb) {
     return (size_t)n * (nb + 1) * sizeof(T) <= (size_t)220 * 1024;
 }
 
-int lu_factor64(double* a, int n, int32_t* piv, int* d_info, cudaStream_t s) {
-    if (panel_fits<double>(n, 8)) return lu_factor_impl<double, 8>(a, n, piv, d_info, s);
-    if (panel_fits<double>(n, 4)) return lu_factor_impl<double, 4>(a, n, piv, d_info, s);
-    return lu_factor_impl<double, 2>(a, n, piv, d_info, s);
+int lu_factor64(double* a, int n, int32_t* piv, int* d_info, cudaStream_t s, const int* run_flag) {
+    if (panel_fits<double>(n, 8)) return lu_factor_impl<double, 8>(a, n, piv, d_info, s, run_flag);
+    if (panel_fits<double>(n, 4)) return lu_factor_impl<double, 4>(a, n, piv, d_info, s, run_flag);
+    return lu_factor_impl<double, 2>(a, n, piv, d_info, s, run_flag);
 }
 int lu_factor32(float* a, int n, int32_t* piv, int* d_info, cudaStream_t s) {
-    if (panel_fits<float>(n, 16)) return lu_factor_impl<float, 16>(a, n, piv, d_info, s);
-    return lu_factor_impl<float, 8>(a, n, piv, d_info, s);
+    if (panel_fits<float>(n, 16)) return lu_factor_impl<float, 16>(a, n, piv, d_info, s, nullptr);
+    return lu_factor_impl<float, 8>(a, n, piv, d_info, s, nullptr);
 }
 
 // ---------------------------------------------------------------------------------
@@ -501,15 +508,16 @@ static int lu_factor32_tc_impl(float* a, int n, int32_t* piv, int* d_info, int* 
         const int kb = min(kTcBlk, n - k), ke = k + kb;
         for (int j = k; j < ke; j += NB) {
             const int nb = min(NB, n - j);
-            lu_panel_kernel<float, NB><<<1, 1024, (size_t)(n - j) * (NB + 1) * sizeof(float), s>>>(a, n, j, piv, d_info);
+            lu_panel_kernel<float, NB><<<1, 1024, (size_t)(n - j) * (NB + 1) * sizeof(float), s>>>(a, n, j, piv, d_info,
+                                                                                              nullptr);
             note_launch();
             if (n > nb) {
-                lu_swap_trsm_kernel<float, NB><<<(n + 255) / 256, 256, 0, s>>>(a, n, j, piv, ke);
+                lu_swap_trsm_kernel<float, NB><<<(n + 255) / 256, 256, 0, s>>>(a, n, j, piv, ke, nullptr);
                 note_launch();
             }
             const int rows = n - j - nb, cols = ke - j - nb;
             if (nb == NB && rows > 0 && cols > 0) {
-                lu_update_kernel<float, NB><<<dim3((cols + 63) / 64, (rows + 63) / 64), 256, 0, s>>>(a, n, j, ke);
+                lu_update_kernel<float, NB><<<dim3((cols + 63) / 64, (rows + 63) / 64), 256, 0, s>>>(a, n, j, ke, nullptr);
                 note_launch();
             }
         }

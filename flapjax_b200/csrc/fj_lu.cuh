@@ -8,7 +8,8 @@ namespace fj {
 // Row-major n x n, in place (L unit-lower below the diagonal, U on and above), 0-based
 // pivot rows in piv (row i was swapped with piv[i], applied in increasing i, as LAPACK
 // getrf).  *d_info (device int) receives 0 or 1 + the first zero-pivot column.
-int lu_factor64(double* a, int n, int32_t* piv, int* d_info, cudaStream_t s);
+// run_flag (device, may be null): the factor kernels return at once when *run_flag == 0
+int lu_factor64(double* a, int n, int32_t* piv, int* d_info, cudaStream_t s, const int* run_flag = nullptr);
 int lu_factor32(float* a, int n, int32_t* piv, int* d_info, cudaStream_t s);
 
 // getrs: b <- A^-1 b using the factors (single right-hand side, in place); work: n doubles.

@@ -824,6 +824,15 @@ static inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)((n + b -
 // ------------------------------------------------------------------------------------
 // Case plan: layout, workspace carve-up, validation
 // ------------------------------------------------------------------------------------
+// Mixed path: the RHS sums the first kNearWakeRows wake rows in FP64 and the rest in FP32.
+// Row 0's leading filament lies on the trailing edge, a quarter panel from the last row of
+// collocation points, where one filament's term is several times the whole normalwash: its
+// FP32 rounding alone moved Gamma by ~2e-7 relative, and the unsteady force
+// rho (dGamma/dt) A n turns that into ~2e-6 of the drag.  With four rows in FP64 the rest
+// of the wake moves Gamma by ~1e-8 (16 x 128 wing, W = 200); the FP64 part is 2 % of the
+// wake's links.  The force and convection sums stay FP32 whole.
+constexpr int kNearWakeRows = 4;
+
 struct Plan {
     fj_case_config cfg;
     Layout L;
@@ -840,6 +849,7 @@ struct Plan {
     double* v;
     double* part;
     void* stream;
+    Elem64* stream_near; // mixed path: FP64 stream of the near-wake rows for the RHS (null on FP64)
     double* hs_zw;       // horseshoe wake scratch
     double* hs_gw;
     double* v_conv;      // free-wake convection velocities of the last step solved (wake targets x 3)
@@ -850,7 +860,7 @@ struct Plan {
     float* a32;          // FP32 LU factors (mixed)
     float* x32;          // FP32 inverse (mixed)
     float* tri32;        // triangular-block inverses of the tensor-core factorisation (mixed)
-    double* zeta_ref;    // lattice of the cached AIC (mixed)
+    double* zeta_ref;    // lattice of the cached AIC (mixed) or of the cached FP64 factors
     int32_t* piv;
     double* rhs;
     double* r;
@@ -895,8 +905,8 @@ static int validate(const fj_case_config* c) {
 }
 
 struct TableLayout {
-    size_t step, pack_free, pack_wake, pack_bound, job_free, job_rhs, job_force, cta_free, cta_rhs, cta_force, aic,
-        refine, total;
+    size_t step, pack_free, pack_wake, pack_bound, pack_near, job_free, job_rhs, job_force, job_near, cta_free,
+        cta_rhs, cta_force, cta_near, aic, refine, total;
 };
 
 static TableLayout table_layout(int k) {
@@ -912,12 +922,15 @@ static TableLayout table_layout(int k) {
     t.pack_free = take(k * sizeof(PackJob));
     t.pack_wake = take(k * sizeof(PackJob));
     t.pack_bound = take(k * sizeof(PackJob));
+    t.pack_near = take(k * sizeof(PackJob));
     t.job_free = take(k * sizeof(VindJob));
     t.job_rhs = take(k * sizeof(VindJob));
     t.job_force = take(k * sizeof(VindJob));
+    t.job_near = take(k * sizeof(VindJob));
     t.cta_free = take((k + 1) * sizeof(int64_t));
     t.cta_rhs = take((k + 1) * sizeof(int64_t));
     t.cta_force = take((k + 1) * sizeof(int64_t));
+    t.cta_near = take((k + 1) * sizeof(int64_t));
     t.aic = take(k * sizeof(AicArgs));
     t.refine = take(k * sizeof(RefineJob));
     t.total = align_up(o, 256);
@@ -959,6 +972,14 @@ static int make_plan(const fj_case_config* cfg, void* ws, size_t ws_bytes, Plan&
     p.v = a.carve<double>(p.max_targets * 3);
     p.part = a.carve<double>(std::max<int64_t>(part, 1));
     p.stream = a.carve<Elem64>(stream);
+    if (cfg->precision == FJ_PREC_MIXED) {
+        int64_t near = 0;
+        for (int s = 0; s < ns; ++s)
+            if (L.ms[s] > 0) near += img * stream_len(std::min(L.ms[s], kNearWakeRows), L.n[s]);
+        p.stream_near = a.carve<Elem64>(std::max<int64_t>(near, 1));
+    } else {
+        p.stream_near = nullptr;
+    }
     int64_t hs = 0, hsg = 0;
     for (int s = 0; s < ns; ++s) {
         hs += 2ll * (L.n[s] + 1) * 3;
@@ -979,13 +1000,12 @@ static int make_plan(const fj_case_config* cfg, void* ws, size_t ws_bytes, Plan&
         p.a32 = a.carve<float>((int64_t)p.nb * p.nb);
         p.x32 = a.carve<float>((int64_t)p.nb * p.nb);
         p.tri32 = a.carve<float>(tc_tri_floats(p.nb));
-        p.zeta_ref = a.carve<double>(p.sz_zb);
     } else {
         p.a32 = nullptr;
         p.x32 = nullptr;
         p.tri32 = nullptr;
-        p.zeta_ref = nullptr;
     }
+    p.zeta_ref = a.carve<double>(p.sz_zb);
     p.piv = a.carve<int32_t>(p.nb);
     p.rhs = a.carve<double>(p.nb);
     p.r = a.carve<double>(p.nb);
@@ -1214,6 +1234,9 @@ static int run_static(const Plan& p, const fj_case_buffers* B, const double* hg,
     FJ_TRY(lu_factor64(p.a64, p.nb, p.piv, p.flags, s));
     FJ_TRY(lu_solve64(p.a64, p.nb, p.piv, p.rhs, p.r, s));
     FJ_CUDA(cudaMemcpyAsync(gb, p.rhs, p.nb * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    // the static AIC (with the wake lumped in) now occupies the AIC buffer: a NaN in the
+    // cached lattice makes the next dynamic step that compares lattices rebuild it
+    FJ_CUDA(cudaMemsetAsync(p.zeta_ref, 0xFF, sizeof(double), s));
     // wake circulation of the solve (horseshoe: one row) and of the stored slot
     if (horseshoe) {
         static_gamma_w_kernel<<<nblk(p.sz_strip), 256, 0, s>>>(L, gb, p.hs_gw, 1); note_launch();
@@ -1316,12 +1339,14 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
 
     std::vector<char> h(tl.total, 0);
     StepCase* hC = (StepCase*)(h.data() + tl.step);
-    std::vector<VindJob> jf, jr, jfo;
-    std::vector<PackJob> pf(K), pw(K), pb(K);
+    std::vector<VindJob> jf, jr, jfo, jrn;
+    std::vector<PackJob> pf(K), pw(K), pb(K), pwn(K);
+    std::vector<int64_t> rhs_far(K, 0), near_cap;
     std::vector<AicArgs> aic(K);
     std::vector<RefineJob> ref;
     std::vector<int> free_idx;
-    int64_t max_v = 0, max_p = 0, max_w = 0, max_wt = 0, max_f = 0, max_e_free = 0, max_e_wake = 0, max_e_bound = 0;
+    int64_t max_v = 0, max_p = 0, max_w = 0, max_wt = 0, max_f = 0, max_e_free = 0, max_e_wake = 0, max_e_bound = 0,
+            max_e_near = 0;
     int max_n = 0, max_fil = 0, any_mirror = 0, any_free = 0, any_changed = 0, any_var = 0, any_polar = 0;
     int64_t max_xw = 0, max_cols = 0;
     for (int k = 0; k < K; ++k) {
@@ -1385,8 +1410,10 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
         any_var |= L.any_var;
         max_xw = std::max(max_xw, L.xvo[L.n_surf] + L.xpo[L.n_surf]);
         max_cols = std::max(max_cols, L.dofo[L.n_surf]);
-        C.zeta_ref = (mixed && !it.refactor) ? p.zeta_ref : nullptr;
-        C.changed = (mixed && !it.refactor) ? p.flags + 1 : nullptr;
+        // a step that does not refactorise compares its lattice with the one of the cached
+        // AIC (mixed) or FP64 factors and rebuilds them only where it changed
+        C.zeta_ref = !it.refactor ? p.zeta_ref : nullptr;
+        C.changed = !it.refactor ? p.flags + 1 : nullptr;
         C.polars = L.any_polar ? B->d_polars : nullptr;
         C.polar_tmp = p.polar_tmp;
         C.polar_scale = c.polar_circulation_scale;
@@ -1425,10 +1452,37 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
         } else {
             memset(&pf[k], 0, sizeof(PackJob));  // empty job: offset[0] = 0 packs nothing
         }
-        // wake(n) stream, then bound(n) appended
-        StreamBuilder sw;
+        // wake(n) stream, then bound(n) appended.  Mixed: each wake goes in as two lattices,
+        // rows [kNearWakeRows, m_star) first and rows [0, kNearWakeRows) after them (the two
+        // together carry the same filaments as the whole wake), so that the RHS sums the
+        // stream's leading far part in FP32 and takes the near rows, in FP64, from their own
+        // stream; the force sum reads the whole wake part.
+        StreamBuilder sw, swn;
         sw.init(p);
-        for (int q = 0; q < L.n_surf; ++q) sw.add(p, C.zw_n + L.wvo[q] * 3, C.gw_n + L.wpo[q], L.ms[q], L.n[q]);
+        swn.init(p);
+        if (!mixed) {
+            for (int q = 0; q < L.n_surf; ++q) sw.add(p, C.zw_n + L.wvo[q] * 3, C.gw_n + L.wpo[q], L.ms[q], L.n[q]);
+        } else {
+            for (int q = 0; q < L.n_surf; ++q) {
+                const int kn = std::min(L.ms[q], kNearWakeRows);
+                if (L.ms[q] > kn)
+                    sw.add(p, C.zw_n + (L.wvo[q] + (int64_t)kn * (L.n[q] + 1)) * 3, C.gw_n + L.wpo[q] + (int64_t)kn * L.n[q],
+                           L.ms[q] - kn, L.n[q]);
+            }
+        }
+        rhs_far[k] = sw.len();
+        const int64_t far_links = sw.n_links;
+        if (mixed) {
+            for (int q = 0; q < L.n_surf; ++q) {
+                const int kn = std::min(L.ms[q], kNearWakeRows);
+                if (kn == 0) continue;
+                sw.add(p, C.zw_n + L.wvo[q] * 3, C.gw_n + L.wpo[q], kn, L.n[q]);
+                swn.add(p, C.zw_n + L.wvo[q] * 3, C.gw_n + L.wpo[q], kn, L.n[q]);
+            }
+        }
+        pwn[k].a = swn.a;
+        pwn[k].out = p.stream_near;
+        max_e_near = std::max(max_e_near, swn.len());
         pw[k].a = sw.a;
         pw[k].out = stream_at(p, 0);
         max_e_wake = std::max(max_e_wake, sw.len());
@@ -1444,11 +1498,25 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
             j.targets = C.c;
             j.n_targets = p.nb;
             j.stream = p.stream;
-            j.n_elem = sw.len();
+            j.n_elem = rhs_far[k];
             j.part = p.part;
-            j.n_links = sw.n_links;
+            j.n_links = far_links;
             j.out = p.v;
             if (j.n_elem > 0) jr.push_back(j);
+        }
+        if (p.nb > 0 && swn.len() > 0) {  // the near rows in FP64, added to the far sum
+            VindJob j;
+            memset(&j, 0, sizeof(j));
+            j.targets = C.c;
+            j.n_targets = p.nb;
+            j.stream = p.stream_near;
+            j.n_elem = swn.len();
+            j.part = p.part;
+            j.n_links = swn.n_links;
+            j.out = p.v;
+            j.accumulate = 1;
+            jrn.push_back(j);
+            near_cap.push_back(p.part_elems / ((int64_t)p.nb * 3));
         }
         {
             VindJob j;
@@ -1482,20 +1550,26 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
     assign_splits(jf, precision);
     assign_splits(jr, precision);
     assign_splits(jfo, precision);
-    auto fill_cta = [&](const std::vector<VindJob>& jobs, size_t off) {
+    assign_splits(jrn, FJ_PREC_FP64);
+    for (size_t q = 0; q < jrn.size(); ++q)  // the near sum reuses the case's partial buffer
+        jrn[q].n_split = (int)std::max<int64_t>(1, std::min<int64_t>(jrn[q].n_split, near_cap[q]));
+    auto fill_cta = [&](const std::vector<VindJob>& jobs, size_t off, int prec) {
         int64_t* c0 = (int64_t*)(h.data() + off);
         c0[0] = 0;
-        for (size_t q = 0; q < jobs.size(); ++q) c0[q + 1] = c0[q] + vind_ctas(jobs[q].n_targets, jobs[q].n_split, precision);
+        for (size_t q = 0; q < jobs.size(); ++q) c0[q + 1] = c0[q] + vind_ctas(jobs[q].n_targets, jobs[q].n_split, prec);
         return std::vector<int64_t>(c0, c0 + jobs.size() + 1);
     };
-    const std::vector<int64_t> cf = fill_cta(jf, tl.cta_free), cr = fill_cta(jr, tl.cta_rhs),
-                               cfo = fill_cta(jfo, tl.cta_force);
+    const std::vector<int64_t> cf = fill_cta(jf, tl.cta_free, precision), cr = fill_cta(jr, tl.cta_rhs, precision),
+                               cfo = fill_cta(jfo, tl.cta_force, precision),
+                               crn = fill_cta(jrn, tl.cta_near, FJ_PREC_FP64);
     memcpy(h.data() + tl.pack_free, pf.data(), K * sizeof(PackJob));
     memcpy(h.data() + tl.pack_wake, pw.data(), K * sizeof(PackJob));
     memcpy(h.data() + tl.pack_bound, pb.data(), K * sizeof(PackJob));
+    memcpy(h.data() + tl.pack_near, pwn.data(), K * sizeof(PackJob));
     if (!jf.empty()) memcpy(h.data() + tl.job_free, jf.data(), jf.size() * sizeof(VindJob));
     if (!jr.empty()) memcpy(h.data() + tl.job_rhs, jr.data(), jr.size() * sizeof(VindJob));
     memcpy(h.data() + tl.job_force, jfo.data(), jfo.size() * sizeof(VindJob));
+    if (!jrn.empty()) memcpy(h.data() + tl.job_near, jrn.data(), jrn.size() * sizeof(VindJob));
     memcpy(h.data() + tl.aic, aic.data(), K * sizeof(AicArgs));
     if (!ref.empty()) memcpy(h.data() + tl.refine, ref.data(), ref.size() * sizeof(RefineJob));
     if (mode == kStepBuild) {
@@ -1530,19 +1604,24 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
     FJ_TRY(aic_launch_jobs((const AicArgs*)(d_tab + tl.aic), K, max_n, max_fil, any_mirror, kernel, s));
     // 4. RHS
     FJ_TRY(pack_jobs((const PackJob*)(d_tab + tl.pack_wake), K, max_e_wake, precision, s));
-    for (int k = 0; k < K; ++k)  // cases without wake filaments see no wake velocity
-        if (pw[k].a.offset[pw[k].a.n_lat] == 0 && items[k].p.nb > 0)
+    if (!jrn.empty()) FJ_TRY(pack_jobs((const PackJob*)(d_tab + tl.pack_near), K, max_e_near, FJ_PREC_FP64, s));
+    for (int k = 0; k < K; ++k)  // cases without (far) wake filaments: zero, then the near rows add
+        if (rhs_far[k] == 0 && items[k].p.nb > 0)
             FJ_CUDA(cudaMemsetAsync(items[k].p.v, 0, items[k].p.nb * 3 * sizeof(double), s));
     FJ_TRY(launch_sum(jr, cr, d_tab + tl.job_rhs, d_tab + tl.cta_rhs, precision, kernel, r_cut, s));
+    FJ_TRY(launch_sum(jrn, crn, d_tab + tl.job_near, d_tab + tl.cta_near, FJ_PREC_FP64, kernel, r_cut, s));
     k_rhs<<<dim3(nblk(max_n), K), b, 0, s>>>(dC); note_launch();
     FJ_LAUNCH_CHECK("step: geometry, wake, RHS");
     // 5. solve
     if (precision == FJ_PREC_FP64) {
         for (int k = 0; k < K; ++k) {
             const Plan& p = items[k].p;
-            FJ_TRY(lu_factor64(p.a64, p.nb, p.piv, p.flags, s));
+            // factor only when the lattice changed since the cached factors (the factor
+            // kernels read the flag and return at once when it is clear)
+            FJ_TRY(lu_factor64(p.a64, p.nb, p.piv, p.flags, s, hC[k].changed));
             FJ_TRY(lu_solve64(p.a64, p.nb, p.piv, p.rhs, p.r, s));
             k_take_solution<<<nblk(p.nb), 256, 0, s>>>(dC + k, p.rhs, p.nb); note_launch();
+            k_keep_lattice<<<nblk(p.sz_zb), 256, 0, s>>>(dC + k, p.zeta_ref, p.sz_zb); note_launch();
         }
     } else {
         for (int k = 0; k < K; ++k) {
@@ -1700,7 +1779,7 @@ static int run_dynamic(const Plan& p, const fj_case_buffers* B, int i_first, int
         int k = i;
         while (k < i_last) {
             const bool first = (k == i) && !(attempt == 0 && (flags & FJ_REUSE_FACTORS));
-            const bool refactor = mixed && (refactor_all || first);
+            const bool refactor = refactor_all || first;
             // the first step always runs directly (it also does the one-time set-up)
             if (graphs && !refactor && k > i && i_last - k >= 2) break;
             std::vector<BatchItem> one(1, step_item(p, B, k, refactor));
@@ -1806,7 +1885,7 @@ int fj_step_batched(const fj_batch_item* items, int n_items, void* d_batch_ws, s
         const int64_t hs = (int64_t)it.cfg->n_nodes * 16;
         v[k].B = it.bufs;
         v[k].i = it.i_ts;
-        v[k].refactor = it.cfg->precision == FJ_PREC_MIXED && !(it.flags & FJ_REUSE_FACTORS);
+        v[k].refactor = !(it.flags & FJ_REUSE_FACTORS);
         v[k].reuse_convection = (it.flags & FJ_REUSE_CONVECTION) != 0;
         v[k].hg_n = it.bufs->d_hg_t + it.i_ts * hs;
         v[k].hgd_n = it.bufs->d_hg_dot_t + it.i_ts * hs;

@@ -387,20 +387,35 @@ __global__ void __launch_bounds__(kBlock) vind64_kernel(VindJob job, double rc2)
 // Packed form: two targets ride in one float2 and every FP32 add/mul/fma of the pair is
 // one f32x2 instruction (sm_100: __fadd2_rn / __fmul2_rn / __ffma2_rn), halving the
 // issue slots per pair of the scalar form.  The staged element is stored duplicated in
-// shared memory ({v, v} pairs, 6 float4), so the broadcast loads give packed operands
+// shared memory ({v, v} pairs, 4 float4), so the broadcast loads give packed operands
 // directly.  Subtractions are fma(b, -1, a), which is exact.  The filament cross product
 // stays r1 x r2: a target that coincides with a filament end (r2 = 0 exactly, as the
 // free-wake vertices do) then contributes exactly zero, as in FP64.  T = 2 P targets per
 // thread.
+//
+// Cancellation-free strength.  The reference's factor r0 . (r1/|r1| - r2/|r2|) subtracts
+// two nearly equal unit vectors whenever the target is far from the filament compared with
+// its length; in FP32 (and with the approximate MUFU rsqrt) that difference keeps only
+// about eps * d / |r0| relative accuracy, so the far field carries an error that decays
+// like 1/d instead of 1/d^2 and sums to several 1e-6 of the induced drag.  With
+// P = |r1||r2| and D = r1 . r2 the same factor is
+//     r0 . (r1/|r1| - r2/|r2|) = (|r1| + |r2|) (P - D) / P,
+// and P - D = |r1 x r2|^2 / (P + D).  The kernel takes the second form where D > 0 (the
+// far side, where P - D cancels and P + D does not) and the first where D <= 0, so
+//     coef = g (|r1| + |r2|) N / (P M (|r1 x r2|^2 + q)),
+//     N = |r1 x r2|^2, M = P + D   (D > 0),      N = P - D, M = 1   (D <= 0),
+// every term of which is well conditioned.  The product in the denominator is of degree
+// 8 in the lattice's lengths: FP32 keeps it in range for filament lengths and target
+// distances between about 1e-4 and 1e4 in the lattice's units.
 struct Vtx32x2 {
     float2 d[3];
-    float2 u[3];
+    float2 n;  // ||d||_eps
     float2 s;  // kCollinearSin * ||d||_eps^2
 };
 
 // Staged element: vertex part v[0..2] = {hx,hx,hy,hy}, {hz,hz,lx,lx}, {ly,ly,lz,lz} and
-// link part l[0..2] = {g,g,q,q}, {r0x,r0x,r0y,r0y}, {r0z,r0z,0,0}.
-constexpr int kDup = 6;  // float4 per staged element
+// link part l[0] = {g,g,q,q} (the strength form above needs no filament vector).
+constexpr int kDup = 4;  // float4 per staged element
 // Six resident CTAs per SM (registers capped at 80): the sum is FMA-pipe bound and the
 // extra warps hide the MUFU and FMA latencies better than the registers they cost.
 constexpr int kMinCtas32 = 6;
@@ -436,9 +451,7 @@ __device__ __forceinline__ void vtx32x2(const float2 xh[3], const float2 xl[3], 
     const float2 n2 = __ffma2_rn(o.d[2], o.d[2],
                                  __ffma2_rn(o.d[1], o.d[1], __ffma2_rn(o.d[0], o.d[0], dup2((float)(kEps * kEps)))));
     const float2 inv = make_float2(rsqrt_ftz(n2.x), rsqrt_ftz(n2.y));
-    o.u[0] = __fmul2_rn(o.d[0], inv);
-    o.u[1] = __fmul2_rn(o.d[1], inv);
-    o.u[2] = __fmul2_rn(o.d[2], inv);
+    o.n = __fmul2_rn(n2, inv);
     o.s = __fmul2_rn(n2, dup2(kCollinearSin));
 }
 
@@ -447,28 +460,31 @@ template <int KER>
 __device__ __forceinline__ void link32x2(const Vtx32x2& a, const Vtx32x2& b, const float4* __restrict__ l,
                                          float2 acc[3]) {
     const float2 neg1 = dup2(-1.0f);
-    const float4 l0 = l[0], l1 = l[1], l2 = l[2];
+    const float4 l0 = l[0];
     const float2 g = make_float2(l0.x, l0.y), q = make_float2(l0.z, l0.w);
-    const float2 r0x = make_float2(l1.x, l1.y), r0y = make_float2(l1.z, l1.w), r0z = make_float2(l2.x, l2.y);
     const float2 nax = __fmul2_rn(a.d[0], neg1), nay = __fmul2_rn(a.d[1], neg1), naz = __fmul2_rn(a.d[2], neg1);
     const float2 cx = __ffma2_rn(a.d[1], b.d[2], __fmul2_rn(naz, b.d[1]));
     const float2 cy = __ffma2_rn(a.d[2], b.d[0], __fmul2_rn(nax, b.d[2]));
     const float2 cz = __ffma2_rn(a.d[0], b.d[1], __fmul2_rn(nay, b.d[0]));
     const float2 c2 = __ffma2_rn(cz, cz, __ffma2_rn(cy, cy, __fmul2_rn(cx, cx)));
-    const float2 dux = __ffma2_rn(b.u[0], neg1, a.u[0]);
-    const float2 duy = __ffma2_rn(b.u[1], neg1, a.u[1]);
-    const float2 duz = __ffma2_rn(b.u[2], neg1, a.u[2]);
-    const float2 dot = __ffma2_rn(r0z, duz, __ffma2_rn(r0y, duy, __fmul2_rn(r0x, dux)));
+    const float2 D = __ffma2_rn(a.d[2], b.d[2], __ffma2_rn(a.d[1], b.d[1], __fmul2_rn(a.d[0], b.d[0])));
+    const float2 P = __fmul2_rn(a.n, b.n);
+    const float2 PpD = __fadd2_rn(P, D);
+    const float2 PmD = __ffma2_rn(D, neg1, P);
+    const float2 N = make_float2(D.x > 0.0f ? c2.x : PmD.x, D.y > 0.0f ? c2.y : PmD.y);
+    const float2 M = make_float2(D.x > 0.0f ? PpD.x : 1.0f, D.y > 0.0f ? PpD.y : 1.0f);
     const float2 t = __fmul2_rn(a.s, b.s);
-    const float2 num = __fmul2_rn(g, dot);
+    const float2 num = __fmul2_rn(__fmul2_rn(g, __fadd2_rn(a.n, b.n)), N);
+    const float2 pm = __fmul2_rn(P, M);
     float2 coef;
     if (KER == FJ_KERNEL_EPSILON) {
-        const float2 den = __fadd2_rn(c2, q);
+        const float2 den = __fmul2_rn(pm, __fadd2_rn(c2, q));
         coef = __fmul2_rn(num, make_float2(rcp_ftz(den.x), rcp_ftz(den.y)));
         coef.x = c2.x > t.x ? coef.x : 0.0f;
         coef.y = c2.y > t.y ? coef.y : 0.0f;
     } else {
-        coef = __fmul2_rn(num, make_float2(rcp_ftz(c2.x), rcp_ftz(c2.y)));
+        const float2 den = __fmul2_rn(pm, c2);
+        coef = __fmul2_rn(num, make_float2(rcp_ftz(den.x), rcp_ftz(den.y)));
         coef.x = c2.x > fmaxf(q.x, t.x) ? coef.x : 0.0f;
         coef.y = c2.y > fmaxf(q.y, t.y) ? coef.y : 0.0f;
     }
@@ -478,13 +494,11 @@ __device__ __forceinline__ void link32x2(const Vtx32x2& a, const Vtx32x2& b, con
 }
 
 __device__ __forceinline__ void stage_dup(const float4* __restrict__ s4, int64_t e, float4* __restrict__ o) {
-    const float4 a = s4[e * 3 + 0], b = s4[e * 3 + 1], c = s4[e * 3 + 2];  // {xh,yh,zh,g} {xl,yl,zl,q} {r0,pad}
+    const float4 a = s4[e * 3 + 0], b = s4[e * 3 + 1];  // {xh,yh,zh,g} {xl,yl,zl,q}
     o[0] = make_float4(a.x, a.x, a.y, a.y);
     o[1] = make_float4(a.z, a.z, b.x, b.x);
     o[2] = make_float4(b.y, b.y, b.z, b.z);
     o[3] = make_float4(a.w, a.w, b.w, b.w);
-    o[4] = make_float4(c.x, c.x, c.y, c.y);
-    o[5] = make_float4(c.z, c.z, 0.0f, 0.0f);
 }
 
 template <int KER, int T>
@@ -644,7 +658,7 @@ __global__ void reduce_jobs_kernel(const VindJob* __restrict__ jobs) {
     if (i >= n3) return;
     double sacc = 0.0;
     for (int k = 0; k < J.n_split; ++k) sacc += J.part[(int64_t)k * n3 + i];
-    J.out[i] = sacc;
+    J.out[i] = J.accumulate ? J.out[i] + sacc : sacc;
 }
 
 int reduce_jobs(const VindJob* d_jobs, int n_jobs, int64_t max_targets, cudaStream_t s) {

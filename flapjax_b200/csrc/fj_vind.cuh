@@ -79,6 +79,7 @@ struct VindJob {
     double* part;           // (n_split, n_targets, 3)
     int64_t n_links;        // filaments in the stream (for pair counting)
     double* out;            // (n_targets, 3) result of the reduction (batched launches)
+    int accumulate;         // batched reduction: 1 adds the sum to out, 0 overwrites out
 };
 
 // A stream-packing job of a batched launch: lattices -> elements at `out`.
