@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--small", action="store_true", help="a reduced workload (for quick checks)")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="only the timed mixed steps, no autotuning or other legs (for profiler runs)")
     ap.add_argument("--serving-cases", type=int, default=512, help="cases in the serving stream (0: skip)")
     ap.add_argument("--only-serving", action="store_true")
     ap.add_argument("--adjoint", action="store_true",
@@ -393,8 +395,10 @@ def main():
     t_tune = time.perf_counter()
     kern = _lib.FJ_KERNEL_CUTOFF if case.kernel == "cutoff" else _lib.FJ_KERNEL_EPSILON
     shapes = tuning.step_shapes(case.m, case.n, case.m_star, case.free_wake)
-    autotune = {p: tuning.autotune(shapes, p, kern, case.r_cut) for p in ("mixed", "fp64")}
-    autotune["seconds"] = time.perf_counter() - t_tune
+    autotune = None
+    if not args.kernels_only:
+        autotune = {p: tuning.autotune(shapes, p, kern, case.r_cut) for p in ("mixed", "fp64")}
+        autotune["seconds"] = time.perf_counter() - t_tune
     # -- mixed path: value ---------------------------------------------------------------
     uv, dc = make_case(case, "mixed", n_slots)
     run_device_steps(dc, 1, 1 + W, flush, torch)
@@ -414,7 +418,9 @@ def main():
 
     # -- roofline of the dominant kernel (Biot-Savart sums) -------------------------------
     peak = ctypes_peak(torch)
-    achieved = prof.vind_pairs * FLOPS_PER_PAIR / (prof.vind_ms * 1e-3) / 1e12 if prof.vind_ms > 0 else None
+    # the FP32 sums only: the RHS's near-wake rows run in FP64 and are reported beside them
+    v32_ms, v32_pairs = prof.vind_ms - prof.vind64_ms, prof.vind_pairs - prof.vind64_pairs
+    achieved = v32_pairs * FLOPS_PER_PAIR / (v32_ms * 1e-3) / 1e12 if v32_ms > 0 else None
     roof = {"kernel": "vind32 (FP32 Biot-Savart sums)", "bound": "fp32", "achieved": achieved,
             "peak": peak, "unit": "TFLOP/s", "frac": (achieved / peak) if achieved and peak else None,
             "traffic": VIND32_TRAFFIC_BYTES,
@@ -423,9 +429,20 @@ def main():
                               "DRAM traffic, the rest stays in L2",
             "peak_source": "measured in-run (fj_peak_fp32: larger of scalar and packed FP32 FMA chains); "
                            "MEASURED_PEAKS.json has no FP32 CUDA-core figure",
-            "pairs_per_launch": prof.vind_pairs / max(prof.vind_launches, 1),
-            "kernel_ms_per_step": prof.vind_ms / K, "share_of_step": prof.vind_ms / t_ms if t_ms else None,
-            "pairs_per_s": prof.vind_pairs / (prof.vind_ms * 1e-3) if prof.vind_ms else None}
+            "pairs_per_launch": v32_pairs / max(prof.vind_launches - prof.vind64_launches, 1),
+            "kernel_ms_per_step": v32_ms / K, "share_of_step": v32_ms / t_ms if t_ms else None,
+            "pairs_per_s": v32_pairs / (v32_ms * 1e-3) if v32_ms > 0 else None,
+            "fp64_near_wake_sums": {"ms_per_step": prof.vind64_ms / K, "pairs_per_step": prof.vind64_pairs / K,
+                                    "share_of_step": prof.vind64_ms / t_ms if t_ms else None}}
+
+    if args.kernels_only:
+        if world > 1:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "ms_per_step": t_ms / K,
+                              "steps": K, "warmup": W, "roofline": roof, "gpu_launches": int(launches),
+                              "note": "kernels only: heuristic sum splits, no other legs"}))
+        return 0
 
     # -- plain FP64 path and the mixed path's force-coefficient error -------------------
     # The free wake is chaotic: the FP64 path's own CL moves by many orders of magnitude
@@ -441,13 +458,14 @@ def main():
         cl64, cd64 = coeffs(ft64, case)
         clm, cdm = coeffs(ft_mixed, case)
         # one-step error at sampled steps: mixed step from the FP64 state of slot i-1
-        local = []
+        local, local_cd = [], []
         for i in np.linspace(1 + W, n_slots - 1, 5).astype(int):
             dc.copy_slot_from(d64, i - 1)
             dc.solve_dynamic(i, i + 1, reuse_factors=True)
-            cl_i, _ = coeffs(dc.force_total[i].cpu().numpy()[None], case)
-            cl_r, _ = coeffs(d64.force_total[i].cpu().numpy()[None], case)
+            cl_i, cd_i = coeffs(dc.force_total[i].cpu().numpy()[None], case)
+            cl_r, cd_r = coeffs(d64.force_total[i].cpu().numpy()[None], case)
             local.append(float(abs(cl_i[0] - cl_r[0]) / abs(cl_r[0])))
+            local_cd.append(float(abs(cd_i[0] - cd_r[0]) / np.max(np.abs(cd64))))
         # FP64 self-sensitivity: the same run with zeta_b0 scaled by (1 + 1e-13)
         import copy as _copy
 
@@ -459,6 +477,7 @@ def main():
         fp64 = {"value": K / (sum(ms64) * 1e-3), "unit": UNIT, "ms_per_step": sum(ms64) / K,
                 "speedup_mixed_over_fp64": (sum(ms64) / t_ms) if t_ms else None,
                 "cl_rel_err_one_step_max": max(local),
+                "cd_err_one_step_of_max_cd": max(local_cd),
                 "cl_rel_err_traj_max": float(np.max(np.abs(clm - cl64) / np.abs(cl64))),
                 "cd_rel_err_traj_max": float(np.max(np.abs(cdm - cd64)) / np.max(np.abs(cd64))),
                 "fp64_cl_change_from_1e-13_input_perturbation": float(np.max(np.abs(clp - cl64) / np.abs(cl64)))}
@@ -498,12 +517,9 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32+fp64", "data": "synthetic (seeded wing geometry, no dataset)",
-        "config": {"workload": "free-wake UVLM 16x128 bound, W=200 wake rows, cutoff kernel r=1e-3c, twist+camber "
-                               "seeded, static-solve start" + (" [SMALL]" if args.small else ""),
-                   "m": case.m, "n": case.n, "m_star": case.m_star, "pairs_per_step": case.pairs_per_step(),
-                   "precision": "mixed (FP32 Biot-Savart, FP32 factors + FP64 refinement)",
-                   "l2": "flushed between steps (256 MB write outside the timed events)",
-                   "parallelism": f"independent case replica per GPU x{world}", "seed": case.seed},
+        "config": bench_config(case, args, world),
+        "precision": "mixed (FP32 Biot-Savart with the first 4 wake rows of the RHS in FP64, FP32 factors + FP64 "
+                     "refinement)",
         "e2e": e2e, "fp64_gpu": fp64, "roofline": roof, "cpu_baseline": cpu, "factorisation": factor,
         "gpu_launches": int(launches), "clocks": clk.summary(), "serving": serving, "autotune": autotune,
         "linear": linear,
@@ -890,6 +906,15 @@ def serving_bench(args, torch):
     return summ
 
 
+def bench_config(case, args, world):
+    """The workload's description, the same on both arms."""
+    return {"workload": "free-wake UVLM 16x128 bound, W=200 wake rows, cutoff kernel r=1e-3c, twist+camber seeded, "
+                        "static-solve start" + (" [SMALL]" if args.small else ""),
+            "m": case.m, "n": case.n, "m_star": case.m_star, "pairs_per_step": case.pairs_per_step(),
+            "l2": "flushed between steps (256 MB write outside the timed events)",
+            "parallelism": f"independent case replica per GPU x{world}", "seed": case.seed}
+
+
 def ctypes_peak(torch):
     import ctypes
 
@@ -918,9 +943,8 @@ def reference_arm(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
             "steps": len(times), "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
             "higher_is_better": True, "scaling": "weak", "dtype": "fp64", "data": "synthetic",
-            "config": {"workload": "free-wake UVLM 16x128 bound, W=200 wake rows, cutoff kernel r=1e-3c, twist+camber "
-                                   "seeded, static-solve start" + (" [SMALL]" if args.small else ""),
-                       "seed": case.seed},
+            "config": bench_config(case, args, int(os.environ.get("WORLD_SIZE", "1"))),
+            "precision": "fp64",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": th, "kind": "port",
                              "sample": f"C++/OpenMP FP64 oracle, {args.warmup} untimed + {len(times)} timed full "
                                        f"time steps on {th} threads ({sum(times):.1f} s)"},

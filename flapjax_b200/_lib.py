@@ -110,6 +110,9 @@ class FjProfile(C.Structure):
         ("vind_ms", C.c_double),
         ("vind_ms_max", C.c_double),
         ("vind_pairs", C.c_double),
+        ("vind64_launches", C.c_int64),
+        ("vind64_ms", C.c_double),
+        ("vind64_pairs", C.c_double),
     ]
 
 

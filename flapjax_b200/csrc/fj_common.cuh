@@ -40,7 +40,7 @@ int allow_dynamic_smem(const void* func, size_t bytes);
 // Opt-in timing of the Biot-Savart sum kernels with CUDA events on their stream
 // (fj_profile_begin / fj_profile_end).  prof_start returns -1 when profiling is off.
 int prof_start(cudaStream_t s);
-void prof_stop(int slot, cudaStream_t s, double pairs);
+void prof_stop(int slot, cudaStream_t s, double pairs, bool fp64);
 
 inline int cuda_status(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return FJ_OK;

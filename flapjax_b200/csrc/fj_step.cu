@@ -1550,9 +1550,11 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
     assign_splits(jf, precision);
     assign_splits(jr, precision);
     assign_splits(jfo, precision);
-    assign_splits(jrn, FJ_PREC_FP64);
-    for (size_t q = 0; q < jrn.size(); ++q)  // the near sum reuses the case's partial buffer
-        jrn[q].n_split = (int)std::max<int64_t>(1, std::min<int64_t>(jrn[q].n_split, near_cap[q]));
+    // The near-row sums are short (a few rows of links): 32 elements per split so that they
+    // spread over the GPU instead of running as a handful of long FP64 CTAs; each reuses
+    // its case's partial buffer.
+    for (size_t q = 0; q < jrn.size(); ++q)
+        jrn[q].n_split = (int)std::max<int64_t>(1, std::min<int64_t>({(jrn[q].n_elem + 31) / 32, 1024, near_cap[q]}));
     auto fill_cta = [&](const std::vector<VindJob>& jobs, size_t off, int prec) {
         int64_t* c0 = (int64_t*)(h.data() + off);
         c0[0] = 0;

@@ -66,6 +66,7 @@ struct ProfState {
     bool on = false;
     std::vector<cudaEvent_t> ev;  // 2 per slot
     std::vector<double> pairs;
+    std::vector<char> fp64;
     int used = 0;
     int64_t launches0 = 0;
 };
@@ -81,17 +82,21 @@ int prof_start(cudaStream_t s) {
         if (cudaEventCreate(&e) != cudaSuccess) return -1;
         g_prof.ev.push_back(e);
     }
-    if ((int)g_prof.pairs.size() <= slot) g_prof.pairs.resize(slot + 1);
+    if ((int)g_prof.pairs.size() <= slot) {
+        g_prof.pairs.resize(slot + 1);
+        g_prof.fp64.resize(slot + 1);
+    }
     cudaEventRecord(g_prof.ev[2 * slot], s);
     g_prof.used = slot + 1;
     return slot;
 }
 
-void prof_stop(int slot, cudaStream_t s, double pairs) {
+void prof_stop(int slot, cudaStream_t s, double pairs, bool fp64) {
     if (slot < 0) return;
     std::lock_guard<std::mutex> g(g_prof.mu);
     cudaEventRecord(g_prof.ev[2 * slot + 1], s);
     g_prof.pairs[slot] = pairs;
+    g_prof.fp64[slot] = fp64;
 }
 
 bool prof_active() {
@@ -120,6 +125,11 @@ int prof_end(fj_profile* out) {
         r.vind_ms += ms;
         r.vind_ms_max = std::max(r.vind_ms_max, (double)ms);
         r.vind_pairs += g_prof.pairs[i];
+        if (g_prof.fp64[i]) {
+            r.vind64_launches += 1;
+            r.vind64_ms += ms;
+            r.vind64_pairs += g_prof.pairs[i];
+        }
     }
     r.vind_launches = g_prof.used;
     if (out) *out = r;
@@ -387,11 +397,8 @@ __global__ void __launch_bounds__(kBlock) vind64_kernel(VindJob job, double rc2)
 // Packed form: two targets ride in one float2 and every FP32 add/mul/fma of the pair is
 // one f32x2 instruction (sm_100: __fadd2_rn / __fmul2_rn / __ffma2_rn), halving the
 // issue slots per pair of the scalar form.  The staged element is stored duplicated in
-// shared memory ({v, v} pairs, 4 float4), so the broadcast loads give packed operands
-// directly.  Subtractions are fma(b, -1, a), which is exact.  The filament cross product
-// stays r1 x r2: a target that coincides with a filament end (r2 = 0 exactly, as the
-// free-wake vertices do) then contributes exactly zero, as in FP64.  T = 2 P targets per
-// thread.
+// shared memory ({v, v} pairs, 7 float4), so the broadcast loads give packed operands
+// directly.  Subtractions are fma(b, -1, a), which is exact.  T = 2 P targets per thread.
 //
 // Cancellation-free strength.  The reference's factor r0 . (r1/|r1| - r2/|r2|) subtracts
 // two nearly equal unit vectors whenever the target is far from the filament compared with
@@ -401,21 +408,28 @@ __global__ void __launch_bounds__(kBlock) vind64_kernel(VindJob job, double rc2)
 // P = |r1||r2| and D = r1 . r2 the same factor is
 //     r0 . (r1/|r1| - r2/|r2|) = (|r1| + |r2|) (P - D) / P,
 // and P - D = |r1 x r2|^2 / (P + D).  The kernel takes the second form where D > 0 (the
-// far side, where P - D cancels and P + D does not) and the first where D <= 0, so
-//     coef = g (|r1| + |r2|) N / (P M (|r1 x r2|^2 + q)),
-//     N = |r1 x r2|^2, M = P + D   (D > 0),      N = P - D, M = 1   (D <= 0),
-// every term of which is well conditioned.  The product in the denominator is of degree
-// 8 in the lattice's lengths: FP32 keeps it in range for filament lengths and target
-// distances between about 1e-4 and 1e4 in the lattice's units.
+// far side, where P - D cancels and P + D does not) and the first where D <= 0:
+//     epsilon: coef = g S N / (P M (|c|^2 + q)),  N = |c|^2, M = P + D (D > 0); N = P - D, M = 1
+//     cutoff:  coef = g S X / (P Y),              X = 1, Y = P + D (D > 0);   X = P - D, Y = |c|^2
+// with S = |r1| + |r2|; every term is well conditioned.  The products in the denominators
+// are of degree 8 (epsilon) and 4 (cutoff) in the lattice's lengths: FP32 keeps them in
+// range for filament lengths and target distances between about 1e-4 and 1e4.
+//
+// Cross product.  c = r1 x r2 = r0 x r1 (r2 = r1 - r0), formed from the staged filament
+// vector r0 and its negation, two instructions per component.  A target on the link's
+// start (r1 = 0 exactly, as free-wake vertices are) gives c = 0 exactly; a target on its
+// end (r2 = 0 exactly) leaves a rounding residue in r0 x r1, so a vertex whose distance
+// is exactly zero carries an infinite collinearity scale s, and the test |c|^2 > s_a s_b
+// drops every link that ends there -- the exact zero of the reference's r1 x r2.
 struct Vtx32x2 {
     float2 d[3];
     float2 n;  // ||d||_eps
-    float2 s;  // kCollinearSin * ||d||_eps^2
+    float2 s;  // kCollinearSin * ||d||_eps^2, or +inf where d = 0
 };
 
-// Staged element: vertex part v[0..2] = {hx,hx,hy,hy}, {hz,hz,lx,lx}, {ly,ly,lz,lz} and
-// link part l[0] = {g,g,q,q} (the strength form above needs no filament vector).
-constexpr int kDup = 4;  // float4 per staged element
+// Staged element: vertex part v[0..2] = {hx,hx,hy,hy}, {hz,hz,lx,lx}, {ly,ly,lz,lz}; link
+// part l[0..3] = {g,g,q,q}, {r0x,r0x,r0y,r0y}, {r0z,r0z,-r0x,-r0x}, {-r0y,-r0y,-r0z,-r0z}.
+constexpr int kDup = 7;  // float4 per staged element
 // Six resident CTAs per SM (registers capped at 80): the sum is FMA-pipe bound and the
 // extra warps hide the MUFU and FMA latencies better than the registers they cost.
 constexpr int kMinCtas32 = 6;
@@ -448,11 +462,12 @@ __device__ __forceinline__ void vtx32x2(const float2 xh[3], const float2 xl[3], 
     o.d[0] = __fadd2_rn(__ffma2_rn(hx, neg1, xh[0]), __ffma2_rn(lx, neg1, xl[0]));
     o.d[1] = __fadd2_rn(__ffma2_rn(hy, neg1, xh[1]), __ffma2_rn(ly, neg1, xl[1]));
     o.d[2] = __fadd2_rn(__ffma2_rn(hz, neg1, xh[2]), __ffma2_rn(lz, neg1, xl[2]));
-    const float2 n2 = __ffma2_rn(o.d[2], o.d[2],
-                                 __ffma2_rn(o.d[1], o.d[1], __ffma2_rn(o.d[0], o.d[0], dup2((float)(kEps * kEps)))));
+    constexpr float e2 = (float)(kEps * kEps);
+    const float2 n2 = __ffma2_rn(o.d[2], o.d[2], __ffma2_rn(o.d[1], o.d[1], __ffma2_rn(o.d[0], o.d[0], dup2(e2))));
     const float2 inv = make_float2(rsqrt_ftz(n2.x), rsqrt_ftz(n2.y));
     o.n = __fmul2_rn(n2, inv);
-    o.s = __fmul2_rn(n2, dup2(kCollinearSin));
+    const float2 s = __fmul2_rn(n2, dup2(kCollinearSin));
+    o.s = make_float2(n2.x > e2 ? s.x : __int_as_float(0x7f800000), n2.y > e2 ? s.y : __int_as_float(0x7f800000));
 }
 
 // The link from vertex a (element e) to vertex b (element e+1) with element e's link part l.
@@ -460,31 +475,33 @@ template <int KER>
 __device__ __forceinline__ void link32x2(const Vtx32x2& a, const Vtx32x2& b, const float4* __restrict__ l,
                                          float2 acc[3]) {
     const float2 neg1 = dup2(-1.0f);
-    const float4 l0 = l[0];
+    const float4 l0 = l[0], l1 = l[1], l2 = l[2], l3 = l[3];
     const float2 g = make_float2(l0.x, l0.y), q = make_float2(l0.z, l0.w);
-    const float2 nax = __fmul2_rn(a.d[0], neg1), nay = __fmul2_rn(a.d[1], neg1), naz = __fmul2_rn(a.d[2], neg1);
-    const float2 cx = __ffma2_rn(a.d[1], b.d[2], __fmul2_rn(naz, b.d[1]));
-    const float2 cy = __ffma2_rn(a.d[2], b.d[0], __fmul2_rn(nax, b.d[2]));
-    const float2 cz = __ffma2_rn(a.d[0], b.d[1], __fmul2_rn(nay, b.d[0]));
+    const float2 r0x = make_float2(l1.x, l1.y), r0y = make_float2(l1.z, l1.w), r0z = make_float2(l2.x, l2.y);
+    const float2 nx = make_float2(l2.z, l2.w), ny = make_float2(l3.x, l3.y), nz = make_float2(l3.z, l3.w);
+    const float2 cx = __ffma2_rn(r0y, a.d[2], __fmul2_rn(nz, a.d[1]));
+    const float2 cy = __ffma2_rn(r0z, a.d[0], __fmul2_rn(nx, a.d[2]));
+    const float2 cz = __ffma2_rn(r0x, a.d[1], __fmul2_rn(ny, a.d[0]));
     const float2 c2 = __ffma2_rn(cz, cz, __ffma2_rn(cy, cy, __fmul2_rn(cx, cx)));
     const float2 D = __ffma2_rn(a.d[2], b.d[2], __ffma2_rn(a.d[1], b.d[1], __fmul2_rn(a.d[0], b.d[0])));
     const float2 P = __fmul2_rn(a.n, b.n);
     const float2 PpD = __fadd2_rn(P, D);
     const float2 PmD = __ffma2_rn(D, neg1, P);
-    const float2 N = make_float2(D.x > 0.0f ? c2.x : PmD.x, D.y > 0.0f ? c2.y : PmD.y);
-    const float2 M = make_float2(D.x > 0.0f ? PpD.x : 1.0f, D.y > 0.0f ? PpD.y : 1.0f);
     const float2 t = __fmul2_rn(a.s, b.s);
-    const float2 num = __fmul2_rn(__fmul2_rn(g, __fadd2_rn(a.n, b.n)), N);
-    const float2 pm = __fmul2_rn(P, M);
+    const float2 gS = __fmul2_rn(g, __fadd2_rn(a.n, b.n));
     float2 coef;
     if (KER == FJ_KERNEL_EPSILON) {
-        const float2 den = __fmul2_rn(pm, __fadd2_rn(c2, q));
-        coef = __fmul2_rn(num, make_float2(rcp_ftz(den.x), rcp_ftz(den.y)));
+        const float2 N = make_float2(D.x > 0.0f ? c2.x : PmD.x, D.y > 0.0f ? c2.y : PmD.y);
+        const float2 M = make_float2(D.x > 0.0f ? PpD.x : 1.0f, D.y > 0.0f ? PpD.y : 1.0f);
+        const float2 den = __fmul2_rn(__fmul2_rn(P, M), __fadd2_rn(c2, q));
+        coef = __fmul2_rn(__fmul2_rn(gS, N), make_float2(rcp_ftz(den.x), rcp_ftz(den.y)));
         coef.x = c2.x > t.x ? coef.x : 0.0f;
         coef.y = c2.y > t.y ? coef.y : 0.0f;
     } else {
-        const float2 den = __fmul2_rn(pm, c2);
-        coef = __fmul2_rn(num, make_float2(rcp_ftz(den.x), rcp_ftz(den.y)));
+        const float2 X = make_float2(D.x > 0.0f ? 1.0f : PmD.x, D.y > 0.0f ? 1.0f : PmD.y);
+        const float2 Y = make_float2(D.x > 0.0f ? PpD.x : c2.x, D.y > 0.0f ? PpD.y : c2.y);
+        const float2 den = __fmul2_rn(P, Y);
+        coef = __fmul2_rn(__fmul2_rn(gS, X), make_float2(rcp_ftz(den.x), rcp_ftz(den.y)));
         coef.x = c2.x > fmaxf(q.x, t.x) ? coef.x : 0.0f;
         coef.y = c2.y > fmaxf(q.y, t.y) ? coef.y : 0.0f;
     }
@@ -494,11 +511,14 @@ __device__ __forceinline__ void link32x2(const Vtx32x2& a, const Vtx32x2& b, con
 }
 
 __device__ __forceinline__ void stage_dup(const float4* __restrict__ s4, int64_t e, float4* __restrict__ o) {
-    const float4 a = s4[e * 3 + 0], b = s4[e * 3 + 1];  // {xh,yh,zh,g} {xl,yl,zl,q}
+    const float4 a = s4[e * 3 + 0], b = s4[e * 3 + 1], c = s4[e * 3 + 2];  // {xh,yh,zh,g} {xl,yl,zl,q} {r0,pad}
     o[0] = make_float4(a.x, a.x, a.y, a.y);
     o[1] = make_float4(a.z, a.z, b.x, b.x);
     o[2] = make_float4(b.y, b.y, b.z, b.z);
     o[3] = make_float4(a.w, a.w, b.w, b.w);
+    o[4] = make_float4(c.x, c.x, c.y, c.y);
+    o[5] = make_float4(c.z, c.z, -c.x, -c.x);
+    o[6] = make_float4(-c.y, -c.y, -c.z, -c.z);
 }
 
 template <int KER, int T>
@@ -802,7 +822,7 @@ int vind_launch(const VindJob& job, int precision, int kernel, double r_cut, cud
                 return fail(FJ_ERR_UNSUPPORTED, "vind: kernel %d has no FP32 variant (use FJ_PREC_FP64)", kernel);
         }
     }
-    prof_stop(prof, s, (double)job.n_targets * (double)job.n_links);
+    prof_stop(prof, s, (double)job.n_targets * (double)job.n_links, precision == FJ_PREC_FP64);
     FJ_LAUNCH_CHECK("vind kernel");
     return FJ_OK;
 }
@@ -846,7 +866,7 @@ int vind_launch_jobs(const VindJob* d_jobs, const int64_t* d_cta0, int n_jobs, i
                 return fail(FJ_ERR_UNSUPPORTED, "vind: kernel %d has no FP32 variant (use FJ_PREC_FP64)", kernel);
         }
     }
-    prof_stop(prof, s, pairs);
+    prof_stop(prof, s, pairs, precision == FJ_PREC_FP64);
     FJ_LAUNCH_CHECK("vind jobs kernel");
     return FJ_OK;
 }

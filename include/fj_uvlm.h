@@ -151,6 +151,9 @@ typedef struct fj_profile {
     double vind_ms;        /* their summed device time */
     double vind_ms_max;    /* longest single launch */
     double vind_pairs;     /* (target, filament) pairs they evaluated */
+    int64_t vind64_launches; /* the FP64 sums among them (the FP32 ones are the rest) */
+    double vind64_ms;
+    double vind64_pairs;
 } fj_profile;
 FJ_API int64_t fj_launch_count(void);
 FJ_API int fj_profile_begin(void);

@@ -103,6 +103,7 @@ int main(void) {
          sizeof(fj_flowfield), sizeof(fj_case_config), sizeof(fj_case_buffers), sizeof(fj_profile));
   P(fj_case_config, flow) P(fj_case_config, precision) P(fj_case_config, dt) P(fj_case_config, mirror_normal)
   P(fj_flowfield, gust_x0) P(fj_case_buffers, d_force_total) P(fj_profile, vind_pairs)
+  P(fj_profile, vind64_pairs)
   return 0;
 }
 '''
@@ -128,6 +129,7 @@ def test_struct_layouts_match_header(tmp_path):
     assert int(out["fj_flowfield.gust_x0"]) == _lib.FjFlowfield.gust_x0.offset
     assert int(out["fj_case_buffers.d_force_total"]) == _lib.FjCaseBuffers.d_force_total.offset
     assert int(out["fj_profile.vind_pairs"]) == _lib.FjProfile.vind_pairs.offset
+    assert int(out["fj_profile.vind64_pairs"]) == _lib.FjProfile.vind64_pairs.offset
 
 
 def test_autograd_module_imports_without_a_gpu():
