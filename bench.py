@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--small", action="store_true", help="a reduced workload (for quick checks)")
     ap.add_argument("--kernels-only", action="store_true",
-                    help="only the timed mixed steps, no autotuning or other legs (for profiler runs)")
+                    help="only the autotuned, timed mixed steps, no other legs (for profiler runs)")
     ap.add_argument("--serving-cases", type=int, default=512, help="cases in the serving stream (0: skip)")
     ap.add_argument("--only-serving", action="store_true")
     ap.add_argument("--adjoint", action="store_true",
@@ -395,10 +395,9 @@ def main():
     t_tune = time.perf_counter()
     kern = _lib.FJ_KERNEL_CUTOFF if case.kernel == "cutoff" else _lib.FJ_KERNEL_EPSILON
     shapes = tuning.step_shapes(case.m, case.n, case.m_star, case.free_wake)
-    autotune = None
-    if not args.kernels_only:
-        autotune = {p: tuning.autotune(shapes, p, kern, case.r_cut) for p in ("mixed", "fp64")}
-        autotune["seconds"] = time.perf_counter() - t_tune
+    precs = ("mixed",) if args.kernels_only else ("mixed", "fp64")
+    autotune = {p: tuning.autotune(shapes, p, kern, case.r_cut) for p in precs}
+    autotune["seconds"] = time.perf_counter() - t_tune
     # -- mixed path: value ---------------------------------------------------------------
     uv, dc = make_case(case, "mixed", n_slots)
     run_device_steps(dc, 1, 1 + W, flush, torch)
@@ -441,7 +440,7 @@ def main():
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "ms_per_step": t_ms / K,
                               "steps": K, "warmup": W, "roofline": roof, "gpu_launches": int(launches),
-                              "note": "kernels only: heuristic sum splits, no other legs"}))
+                              "note": "kernels only: no other legs"}))
         return 0
 
     # -- plain FP64 path and the mixed path's force-coefficient error -------------------

@@ -84,5 +84,34 @@ def build(verbose: bool = False) -> Path:
     return LIB
 
 
+def xla_include_dir() -> Path | None:
+    """jaxlib's FFI header directory (jax.ffi.include_dir()), or None without JAX."""
+    try:
+        import jax.ffi
+    except ImportError:
+        return None
+    return Path(jax.ffi.include_dir())
+
+
+def build_xla(verbose: bool = False) -> Path:
+    """libfj_xla.so: the XLA FFI handlers of xla/fj_xla.cc, linked against libfj_uvlm.so."""
+    inc = xla_include_dir()
+    if inc is None:
+        raise RuntimeError("the XLA FFI handlers need jaxlib's headers (jax.ffi.include_dir()); JAX is not installed")
+    lib = build(verbose)
+    out = LIB_DIR / "libfj_xla.so"
+    cmd = [nvcc(), *ARCH, "-shared", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "-I", str(inc), "-I", str(INCLUDE),
+           str(PKG / "xla" / "fj_xla.cc"), "-o", str(out), "-L", str(LIB_DIR), "-lfj_uvlm", "-lcudart",
+           "-Xlinker", "-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"fj_xla.cc failed:\n{r.stdout}\n{r.stderr}")
+    return out
+
+
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv))
+    if "--xla" in sys.argv:
+        print(build_xla(verbose="-v" in sys.argv))

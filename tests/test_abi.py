@@ -146,3 +146,24 @@ def test_tuning_shapes_of_a_step():
     assert s[1] == (16 * 129 + 17 * 128, 2 * 17 * 129 + 2 * 201 * 129)
     assert s[2] == (201 * 129, 2 * 17 * 129 + 2 * 201 * 129)
     assert len(tuning.step_shapes(4, 8, 10, False)) == 2
+
+
+def test_jax_binding_is_import_guarded():
+    """flapjax_b200.fj_jax (the jax.ffi / custom_vjp binding) imports without JAX, reports
+    itself unavailable and refuses to register; its handler source names only exported
+    entry points."""
+    import re
+
+    from flapjax_b200 import build, fj_jax
+
+    if fj_jax.jax is None:
+        assert not fj_jax.available()
+        with pytest.raises(RuntimeError, match="needs JAX"):
+            fj_jax.register()
+        assert build.xla_include_dir() is None
+    src = (ROOT / "flapjax_b200" / "xla" / "fj_xla.cc").read_text()
+    header = (ROOT / "include" / "fj_uvlm.h").read_text()
+    for name in set(re.findall(r"\b(fj_[a-z0-9_]+)\(", src)):
+        assert f"FJ_API int {name}(" in header or f"FJ_API const char* {name}(" in header, name
+    for sym in fj_jax._TARGETS.values():
+        assert f"XLA_FFI_DEFINE_HANDLER_SYMBOL({sym}," in src
