@@ -500,6 +500,9 @@ def main():
         del dce
 
     serving = serving_bench(args, torch) if args.serving_cases > 0 else None
+    # below capacity (about a sixth of what one GPU serves), so that latency is the step's
+    # and not the queue's
+    serving_low = serving_bench(args, torch, n=64, rate=10.0) if args.serving_cases > 0 else None
     linear = None
     if rank == 0 and not args.small:
         try:  # the linearised UVLM at C1 size (its own leg: --linear)
@@ -520,7 +523,8 @@ def main():
         "precision": "mixed (FP32 Biot-Savart with the first 4 wake rows of the RHS in FP64, FP32 factors + FP64 "
                      "refinement)",
         "e2e": e2e, "fp64_gpu": fp64, "roofline": roof, "cpu_baseline": cpu, "factorisation": factor,
-        "gpu_launches": int(launches), "clocks": clk.summary(), "serving": serving, "autotune": autotune,
+        "gpu_launches": int(launches), "clocks": clk.summary(), "serving": serving,
+        "serving_below_capacity": serving_low, "autotune": autotune,
         "linear": linear,
     }
     print(json.dumps(line))
@@ -865,18 +869,19 @@ def adjoint_bench(args, torch):
     return res
 
 
-def serving_bench(args, torch):
+def serving_bench(args, torch, n=None, rate=200.0):
     """Config 5: Poisson arrivals (200/s) of heaving wings with M ~ U{4..16},
     N ~ U{16..128}, W ~ U{20..200}, AoA ~ U[0, 8] deg, 100 steps each, mixed precision,
-    continuously batched.  Reports whole-stream throughput and per-step latency.  With
-    several ranks each serves every world-th arrival of the same stream (no collective
-    on the data path); rank 0 merges the summaries."""
+    continuously batched.  Reports whole-stream throughput and per-step latency, and the
+    batched-step graph replays and captures.  With several ranks each serves every
+    world-th arrival of the same stream (no collective on the data path); rank 0 merges
+    the summaries."""
     import flapjax_b200 as fj
     from flapjax_b200 import cases, replicas
-    from flapjax_b200.serving import Request, ServingLoop
+    from flapjax_b200.serving import Request, ServingLoop, graph_stats
 
-    n = args.serving_cases
-    stream, arrivals = cases.serving_stream(n_cases=n, rate=200.0, n_steps=100, seed=0)
+    n = args.serving_cases if n is None else n
+    stream, arrivals = cases.serving_stream(n_cases=n, rate=rate, n_steps=100, seed=0)
 
     def requests():
         out = []
@@ -891,15 +896,20 @@ def serving_bench(args, torch):
     loop = ServingLoop(memory_budget=int(0.5 * free), max_active=512, keep_results=False)
     loop.run(requests()[:8], realtime=False)  # warm-up (module load, allocator)
     torch.cuda.synchronize()
+    g0 = graph_stats()
     res = loop.run(replicas.shard(requests(), rank, world), realtime=True)
+    g1 = graph_stats()
     part = {"case_steps": res.case_steps, "wall_s": res.wall_s, "gpu_busy_s": res.gpu_busy_s,
             "step_latency_ms": res.step_latency_ms.tolist(), "admit_latency_s": res.admit_latency_s.tolist(),
-            "max_active": res.max_active}
+            "max_active": res.max_active, "graph_replays": g1["replays"] - g0["replays"],
+            "graph_captures": g1["captures"] - g0["captures"]}
     parts = replicas.gather_to_root(part)
     if parts is None:
         return None
     summ = replicas.merge_serving(parts)
-    summ.update({"cases": n, "arrival_rate_per_s": 200.0, "steps_per_case": 100,
+    summ.update({"cases": n, "arrival_rate_per_s": rate, "steps_per_case": 100,
+                 "graph_replays": sum(p["graph_replays"] for p in parts),
+                 "graph_captures": sum(p["graph_captures"] for p in parts),
                  "workload": "heaving wings, M~U{4..16}, N~U{16..128}, W~U{20..200}, AoA~U[0,8] deg, mixed precision",
                  "pairs_total": float(sum(c.pairs_per_step() * c.n_steps for c in stream))})
     return summ

@@ -15,6 +15,9 @@
 #include <cmath>
 #include <cstring>
 #include <algorithm>
+#include <atomic>
+#include <mutex>
+#include <unordered_map>
 #include <vector>
 
 #include "fj_aic.cuh"
@@ -951,8 +954,13 @@ static int make_plan(const fj_case_config* cfg, void* ws, size_t ws_bytes, Plan&
     p.sz_strip = L.so[ns];
     const int img = cfg->mirror ? 2 : 1;
     int64_t stream = 0;
-    for (int s = 0; s < ns; ++s)
+    for (int s = 0; s < ns; ++s) {
         stream += img * (stream_len(L.m[s], L.n[s]) + stream_len(std::max(L.ms[s], 1), L.n[s]));
+        // mixed: a wake longer than the near rows goes in as two lattices that both hold the
+        // split row: one more spanwise chain (n+1 elements) and one more element in each of
+        // the n+1 chordwise chains
+        if (cfg->precision == FJ_PREC_MIXED && L.ms[s] > kNearWakeRows) stream += img * 2ll * (L.n[s] + 1);
+    }
     p.max_stream = stream;
     p.max_targets = std::max<int64_t>(std::max<int64_t>(L.wto[ns], L.fo[ns]), L.po[ns]);
     // partial buffers for each of the three target sets at the full stream length
@@ -1306,7 +1314,7 @@ static void assign_splits(std::vector<VindJob>& jobs, int precision) {
 }
 
 static int launch_sum(const std::vector<VindJob>& jobs, const std::vector<int64_t>& cta0, char* d_jobs, char* d_cta0,
-                      int precision, int kernel, double r_cut, cudaStream_t s) {
+                      int precision, int kernel, double r_cut, cudaStream_t s, bool persistent) {
     if (jobs.empty()) return FJ_OK;
     double pairs = 0.0;
     int64_t max_t = 0;
@@ -1315,7 +1323,7 @@ static int launch_sum(const std::vector<VindJob>& jobs, const std::vector<int64_
         max_t = std::max(max_t, j.n_targets);
     }
     FJ_TRY(vind_launch_jobs((const VindJob*)d_jobs, (const int64_t*)d_cta0, (int)jobs.size(), cta0.back(), pairs,
-                            precision, kernel, r_cut, s));
+                            precision, kernel, r_cut, s, persistent));
     return reduce_jobs((const VindJob*)d_jobs, (int)jobs.size(), max_t, s);
 }
 
@@ -1325,7 +1333,8 @@ static int launch_sum(const std::vector<VindJob>& jobs, const std::vector<int64_
 enum { kStepNormal = 0, kStepBuild = 1, kStepLaunch = 2 };
 
 static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_bytes, cudaStream_t s,
-                     int mode = kStepNormal, char* h_out = nullptr) {
+                     int mode = kStepNormal, char* h_out = nullptr, std::vector<int64_t>* sig = nullptr,
+                     bool persistent_sums = false) {
     const int K = (int)items.size();
     if (K == 0) return FJ_OK;
     const int precision = items[0].p.cfg.precision;
@@ -1555,6 +1564,15 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
     // its case's partial buffer.
     for (size_t q = 0; q < jrn.size(); ++q)
         jrn[q].n_split = (int)std::max<int64_t>(1, std::min<int64_t>({(jrn[q].n_elem + 31) / 32, 1024, near_cap[q]}));
+    // every job's partials must fit its case's partial buffer (the kernels take any split)
+    std::unordered_map<const double*, int64_t> part_elems;
+    for (const BatchItem& it : items) part_elems[it.p.part] = it.p.part_elems;
+    for (std::vector<VindJob>* jobs : {&jf, &jr, &jfo, &jrn})
+        for (VindJob& j : *jobs) {
+            const int64_t cap = part_elems[j.part] / std::max<int64_t>(1, j.n_targets * 3);
+            if (cap < 1) return fail(FJ_ERR_NOMEM, "partial buffer too small for %lld targets", (long long)j.n_targets);
+            j.n_split = (int)std::min<int64_t>(j.n_split, cap);
+        }
     auto fill_cta = [&](const std::vector<VindJob>& jobs, size_t off, int prec) {
         int64_t* c0 = (int64_t*)(h.data() + off);
         c0[0] = 0;
@@ -1574,6 +1592,45 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
     if (!jrn.empty()) memcpy(h.data() + tl.job_near, jrn.data(), jrn.size() * sizeof(VindJob));
     memcpy(h.data() + tl.aic, aic.data(), K * sizeof(AicArgs));
     if (!ref.empty()) memcpy(h.data() + tl.refine, ref.data(), ref.size() * sizeof(RefineJob));
+    if (sig != nullptr) {
+        // Every host value the launches below take outside the table: grid extents, job
+        // counts, and the per-case pointers of the launches that are not table-driven (the
+        // FP64 and refactorising solves, the zeroing of cases without far-wake rows).  Two
+        // builds with equal signatures launch the same kernels with the same arguments, so
+        // a graph captured for one replays the other once its table is in place.
+        std::vector<int64_t>& g = *sig;
+        double rc = r_cut;
+        int64_t rc_bits = 0;
+        memcpy(&rc_bits, &rc, sizeof(rc_bits));
+        auto sum_sig = [&](const std::vector<VindJob>& jobs) {
+            int64_t mt = 0;
+            for (const VindJob& j : jobs) mt = std::max(mt, j.n_targets);
+            g.push_back((int64_t)jobs.size());
+            g.push_back(mt);
+        };
+        g = {precision, kernel, rc_bits, K, max_v, max_p, max_w, max_wt, max_f, max_n, max_fil, any_mirror, any_free,
+             any_changed, any_var, any_polar, max_xw, max_cols, max_e_free, max_e_wake, max_e_bound, max_e_near,
+             (int64_t)ref.size()};
+        sum_sig(jf);
+        sum_sig(jr);
+        sum_sig(jrn);
+        sum_sig(jfo);
+        for (int k = 0; k < K; ++k) {
+            const Plan& p = items[k].p;
+            g.push_back(p.sz_strip);
+            if (rhs_far[k] == 0) g.push_back((int64_t)(uintptr_t)p.v);
+            if (precision == FJ_PREC_FP64 || items[k].refactor) {
+                g.push_back(items[k].refactor);
+                for (const void* ptr : {(const void*)p.a64, (const void*)p.piv, (const void*)p.flags,
+                                        (const void*)p.rhs, (const void*)p.r, (const void*)p.a32, (const void*)p.x32,
+                                        (const void*)p.tri32, (const void*)p.zeta_ref})
+                    g.push_back((int64_t)(uintptr_t)ptr);
+                g.push_back((int64_t)(uintptr_t)hC[k].changed);
+                g.push_back(p.nb);
+                g.push_back(p.sz_zb);
+            }
+        }
+    }
     if (mode == kStepBuild) {
         memcpy(h_out, h.data(), tl.total);
         return FJ_OK;
@@ -1590,7 +1647,7 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
     if (any_free) {
         FJ_TRY(pack_jobs((const PackJob*)(d_tab + tl.pack_free), K, max_e_free, precision, s));
         k_gather_wake_targets<<<dim3(nblk(max_wt), K), b, 0, s>>>(dC); note_launch();
-        FJ_TRY(launch_sum(jf, cf, d_tab + tl.job_free, d_tab + tl.cta_free, precision, kernel, r_cut, s));
+        FJ_TRY(launch_sum(jf, cf, d_tab + tl.job_free, d_tab + tl.cta_free, precision, kernel, r_cut, s, persistent_sums));
     }
     k_wake_shed<<<dim3(nblk(max_w), K), b, 0, s>>>(dC); note_launch();
     if (any_var) {  // delta_w surfaces: convect all rows, then re-discretise (aero/utils.py:452-491)
@@ -1610,8 +1667,8 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
     for (int k = 0; k < K; ++k)  // cases without (far) wake filaments: zero, then the near rows add
         if (rhs_far[k] == 0 && items[k].p.nb > 0)
             FJ_CUDA(cudaMemsetAsync(items[k].p.v, 0, items[k].p.nb * 3 * sizeof(double), s));
-    FJ_TRY(launch_sum(jr, cr, d_tab + tl.job_rhs, d_tab + tl.cta_rhs, precision, kernel, r_cut, s));
-    FJ_TRY(launch_sum(jrn, crn, d_tab + tl.job_near, d_tab + tl.cta_near, FJ_PREC_FP64, kernel, r_cut, s));
+    FJ_TRY(launch_sum(jr, cr, d_tab + tl.job_rhs, d_tab + tl.cta_rhs, precision, kernel, r_cut, s, persistent_sums));
+    FJ_TRY(launch_sum(jrn, crn, d_tab + tl.job_near, d_tab + tl.cta_near, FJ_PREC_FP64, kernel, r_cut, s, persistent_sums));
     k_rhs<<<dim3(nblk(max_n), K), b, 0, s>>>(dC); note_launch();
     FJ_LAUNCH_CHECK("step: geometry, wake, RHS");
     // 5. solve
@@ -1637,7 +1694,7 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
     // 6. forces with bound(n) + wake(n)
     FJ_TRY(pack_jobs((const PackJob*)(d_tab + tl.pack_bound), K, max_e_bound, precision, s));
     k_force_targets<<<dim3(nblk(max_f), K), b, 0, s>>>(dC); note_launch();
-    FJ_TRY(launch_sum(jfo, cfo, d_tab + tl.job_force, d_tab + tl.cta_force, precision, kernel, r_cut, s));
+    FJ_TRY(launch_sum(jfo, cfo, d_tab + tl.job_force, d_tab + tl.cta_force, precision, kernel, r_cut, s, persistent_sums));
     k_force_filament<<<dim3(nblk(max_f), K), b, 0, s>>>(dC); note_launch();
     // 7. gamma_dot, vertex forces, strip alpha, totals
     if (!any_polar) {
@@ -1873,10 +1930,94 @@ int fj_batch_workspace_size(int max_items, size_t* bytes) {
     return FJ_OK;
 }
 
+}  // extern "C"
+
+namespace fj {
+
+// Captured batched steps, one per batch workspace.  A batch whose launch signature (the
+// grid extents, job counts and out-of-table pointers run_steps reports) equals that of the
+// last capture on its workspace uploads its table and replays the graph; any other batch
+// re-captures (updating the executable graph in place where CUDA allows).  The sum kernels
+// are persistent, so the cases' sizes enter only through the grid maxima.
+struct BatchGraph {
+    std::vector<int64_t> sig;
+    cudaGraphExec_t exec = nullptr;
+    int64_t kernels = 0;
+};
+static std::mutex g_bg_mu;
+static std::unordered_map<const void*, BatchGraph> g_bg;
+static std::atomic<int64_t> g_bg_replays{0}, g_bg_captures{0};
+
+static int step_batched_graph(std::vector<BatchItem>& v, char* d_tab, size_t tab_bytes, cudaStream_t s) {
+    std::vector<char> h(table_layout((int)v.size()).total);
+    std::vector<int64_t> sig;
+    FJ_TRY(run_steps(v, d_tab, tab_bytes, s, kStepBuild, h.data(), &sig));
+    FJ_TRY(upload(d_tab, h.data(), h.size(), s));
+    std::lock_guard<std::mutex> lk(g_bg_mu);
+    BatchGraph& bg = g_bg[d_tab];
+    if (bg.exec != nullptr && bg.sig == sig) {
+        note_launch((int)bg.kernels);  // the replay runs the captured kernels once more
+        g_bg_replays.fetch_add(1);
+        return cuda_status(cudaGraphLaunch(bg.exec, s), "batched step graph launch");
+    }
+    cudaStream_t cs = nullptr;
+    FJ_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t graph = nullptr;
+    const int64_t launches0 = launch_count();
+    int st = cuda_status(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "batched step capture");
+    if (st == FJ_OK) {
+        st = run_steps(v, d_tab, tab_bytes, cs, kStepLaunch, nullptr, nullptr, true);
+        const int st_end = cuda_status(cudaStreamEndCapture(cs, &graph), "batched step capture");
+        if (st == FJ_OK) st = st_end;
+    }
+    cudaStreamDestroy(cs);
+    if (st == FJ_OK) {
+        cudaGraphExecUpdateResultInfo info;
+        if (bg.exec != nullptr && cudaGraphExecUpdate(bg.exec, graph, &info) != cudaSuccess) {
+            cudaGetLastError();  // an update that does not apply is not an error: instantiate anew
+            cudaGraphExecDestroy(bg.exec);
+            bg.exec = nullptr;
+        }
+        if (bg.exec == nullptr) st = cuda_status(cudaGraphInstantiate(&bg.exec, graph, 0), "batched step instantiate");
+    }
+    if (graph) cudaGraphDestroy(graph);
+    if (st != FJ_OK) {
+        if (bg.exec) cudaGraphExecDestroy(bg.exec);
+        g_bg.erase(d_tab);
+        return st;
+    }
+    bg.sig.swap(sig);
+    bg.kernels = launch_count() - launches0;
+    g_bg_captures.fetch_add(1);
+    return cuda_status(cudaGraphLaunch(bg.exec, s), "batched step graph launch");
+}
+
+}  // namespace fj
+
+extern "C" {
+
+int fj_batch_release(void* d_batch_ws) {
+    std::lock_guard<std::mutex> lk(g_bg_mu);
+    auto it = g_bg.find(d_batch_ws);
+    if (it == g_bg.end()) return FJ_OK;
+    if (it->second.exec) FJ_CUDA(cudaGraphExecDestroy(it->second.exec));
+    g_bg.erase(it);
+    return FJ_OK;
+}
+
+int fj_batch_graph_stats(int64_t* replays, int64_t* captures) {
+    if (replays) *replays = g_bg_replays.load();
+    if (captures) *captures = g_bg_captures.load();
+    return FJ_OK;
+}
+
 int fj_step_batched(const fj_batch_item* items, int n_items, void* d_batch_ws, size_t batch_ws_bytes,
                     fj_stream_t stream) {
     if (n_items < 0 || (n_items > 0 && items == nullptr)) return fail(FJ_ERR_SHAPE, "n_items=%d", n_items);
     if (n_items == 0) return FJ_OK;
+    // graph replay unless a caller opts out, a case refactorises (its factorisation is
+    // direct launches) or the event profiler is recording launch times
+    bool graphs = !prof_active();
     std::vector<BatchItem> v(n_items);
     for (int k = 0; k < n_items; ++k) {
         const fj_batch_item& it = items[k];
@@ -1892,8 +2033,10 @@ int fj_step_batched(const fj_batch_item* items, int n_items, void* d_batch_ws, s
         v[k].hg_n = it.bufs->d_hg_t + it.i_ts * hs;
         v[k].hgd_n = it.bufs->d_hg_dot_t + it.i_ts * hs;
         v[k].hg_nm1 = it.bufs->d_hg_t + (it.i_ts - 1) * hs;
+        graphs = graphs && !(it.flags & FJ_NO_GRAPH) && !v[k].refactor;
     }
-    return run_steps(v, (char*)d_batch_ws, batch_ws_bytes, (cudaStream_t)stream);
+    if (!graphs) return run_steps(v, (char*)d_batch_ws, batch_ws_bytes, (cudaStream_t)stream);
+    return step_batched_graph(v, (char*)d_batch_ws, batch_ws_bytes, (cudaStream_t)stream);
 }
 
 int fj_case_residual(const fj_case_config* cfg, void* d_ws, size_t ws_bytes, int i_ts, double* h_out,

@@ -92,7 +92,7 @@ struct PackJob {
 //  vind: CTAs of job j are cta0[j] .. cta0[j+1]-1 (ctas_x(j) * n_split(j) of them);
 //  all jobs of one launch share precision and kernel.
 int vind_launch_jobs(const VindJob* d_jobs, const int64_t* d_cta0, int n_jobs, int64_t total_ctas, double pairs,
-                     int precision, int kernel, double r_cut, cudaStream_t s);
+                     int precision, int kernel, double r_cut, cudaStream_t s, bool persistent = false);
 int pack_jobs(const PackJob* d_jobs, int n_jobs, int64_t max_elem, int precision, cudaStream_t s);
 int reduce_jobs(const VindJob* d_jobs, int n_jobs, int64_t max_targets, cudaStream_t s);
 // CTAs of one sum (target tiles x splits), for building cta0.

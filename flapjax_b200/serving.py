@@ -41,7 +41,10 @@ class BatchStepper:
         _lib.call("fj_batch_workspace_size", max_items, C.byref(n))
         self.ws = torch.empty(n.value, dtype=torch.uint8, device=self.dev)
 
-    def step(self, cases: list[DeviceCase], slots: list[int], reuse: list[bool], stream=None):
+    def step(self, cases: list[DeviceCase], slots: list[int], reuse: list[bool], stream=None, graph: bool = True):
+        """One step of each case.  ``graph``: replay the batch's captured CUDA graph when the
+        batch has the launch signature of the last call (fj_step_batched); False launches
+        every kernel directly (same results)."""
         if not cases:
             return
         if len(cases) > self.max_items:
@@ -53,9 +56,29 @@ class BatchStepper:
             items[k].d_ws = dc.ws.data_ptr()
             items[k].ws_bytes = dc.ws.numel()
             items[k].i_ts = int(i)
-            items[k].flags = _lib.FJ_REUSE_FACTORS if r else 0
+            items[k].flags = (_lib.FJ_REUSE_FACTORS if r else 0) | (0 if graph else _lib.FJ_NO_GRAPH)
         s = (stream or self.torch.cuda.current_stream(self.dev)).cuda_stream
         _lib.call("fj_step_batched", items, len(cases), self.ws.data_ptr(), self.ws.numel(), s)
+
+    def close(self):
+        """Drops the captured graph of this stepper's batch workspace."""
+        if self.ws is not None:
+            self.torch.cuda.synchronize(self.dev)
+            _lib.call("fj_batch_release", self.ws.data_ptr())
+            self.ws = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the process releases everything
+            pass
+
+
+def graph_stats() -> dict:
+    """Batched-step graph replays and captures since the library was loaded."""
+    r, c = C.c_int64(), C.c_int64()
+    _lib.call("fj_batch_graph_stats", C.byref(r), C.byref(c))
+    return {"replays": int(r.value), "captures": int(c.value)}
 
 
 def residual(dc: DeviceCase, i: int) -> float:

@@ -220,8 +220,18 @@ typedef struct fj_batch_item {
     int flags;
 } fj_batch_item;
 FJ_API int fj_batch_workspace_size(int max_items, size_t* bytes);
+/* Unless an item has FJ_NO_GRAPH or factorises (no FJ_REUSE_FACTORS), the step runs as a
+ * CUDA graph captured on the first call for its batch workspace and replayed by later calls
+ * whose batch has the same launch signature: the same number of cases, the same grid
+ * maxima and the same sum-job counts (the per-case data travel in the uploaded table; the
+ * Biot-Savart sums are persistent kernels whose grid is fixed).  A different signature
+ * re-captures.  Calls that share a batch workspace must not overlap. */
 FJ_API int fj_step_batched(const fj_batch_item* items, int n_items, void* d_batch_ws,
                            size_t batch_ws_bytes, fj_stream_t stream);
+/* Drops the captured graph held for a batch workspace (call before freeing it). */
+FJ_API int fj_batch_release(void* d_batch_ws);
+/* Replays and captures of batched-step graphs since the library was loaded. */
+FJ_API int fj_batch_graph_stats(int64_t* replays, int64_t* captures);
 /* Relative refinement residual of slot i_ts of a mixed-precision case (synchronises). */
 FJ_API int fj_case_residual(const fj_case_config* cfg, void* d_ws, size_t ws_bytes, int i_ts,
                             double* h_out, fj_stream_t stream);

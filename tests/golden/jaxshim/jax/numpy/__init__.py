@@ -40,6 +40,12 @@ def broadcast_to(a, shape):
     return wrap(_np.array(_np.broadcast_to(a, shape)))
 
 
+def bincount(x, weights=None, minlength=0, *, length=None):
+    n = length if length is not None else minlength
+    out = _np.bincount(_np.asarray(x).ravel(), weights=weights, minlength=n)
+    return wrap(out[:length] if length is not None else out)
+
+
 acos = _np.arccos
 asin = _np.arcsin
 atan = _np.arctan

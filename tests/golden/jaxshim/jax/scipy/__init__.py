@@ -1,1 +1,1 @@
-from . import linalg, special  # noqa: F401
+from . import linalg, special, spatial  # noqa: F401

@@ -167,3 +167,44 @@ def test_fsi_iterations_reuse_the_wake_convection(cuda, precision, tol):
     for f in ("gamma_b", "gamma_w", "zeta_w", "f_steady", "f_unsteady"):
         a, b = getattr(case, f)[0][i], getattr(case2, f)[0][i]
         assert rel_err(a, b) <= tol, (f, rel_err(a, b))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batched_graph_replay_equals_direct_launches(cuda, precision):
+    """fj_step_batched replays a captured graph while the batch's launch signature holds
+    and re-captures when it changes (a case leaves the batch, here after step 3); the
+    results are bit-identical to direct launches of every kernel."""
+    import torch
+
+    from flapjax_b200.serving import BatchStepper, graph_stats
+
+    mix = _mix()
+    outs = {}
+    for graph in (False, True):
+        uvs, dcs = [], []
+        for c in mix:
+            uv, _ = device_uvlm(c, precision)
+            dc = uv.make_device_case(c.n_tstep)
+            uv.load_initial(dc, uv.solve_static())
+            dc.set_hg(c.hg_t, c.hg_dot_t)
+            dc.solve_dynamic(1, 2)  # the factorising first step, outside the batch
+            uvs.append(uv)
+            dcs.append(dc)
+        st = BatchStepper(8, cuda)
+        before = graph_stats()
+        for i in range(2, mix[0].n_tstep):
+            k = len(dcs) if i <= 3 else len(dcs) - 1
+            st.step(dcs[:k], [i] * k, [True] * k, graph=graph)
+        torch.cuda.synchronize()
+        after = graph_stats()
+        if graph:
+            assert after["captures"] - before["captures"] == 2, (before, after)
+            assert after["replays"] - before["replays"] == mix[0].n_tstep - 2 - 2
+        else:
+            assert after == before
+        st.close()
+        outs[graph] = [uv._to_case(dc) for uv, dc in zip(uvs, dcs)]
+    for a, b in zip(outs[False], outs[True]):
+        for f in FIELDS:
+            for x, y in zip(getattr(a, f), getattr(b, f)):
+                assert np.array_equal(x, y), f

@@ -96,3 +96,23 @@ def test_fp64_reuses_factors_only_for_an_unchanged_lattice(cuda):
         torch.cuda.synchronize()
         ga, gb = a.arrays["gamma_b"].cpu().numpy(), b.arrays["gamma_b"].cpu().numpy()
         assert np.max(np.abs(ga - gb)) <= 1e-12 * np.max(np.abs(gb))
+
+
+@pytest.mark.parametrize("m,n,m_star", [(13, 53, 25), (4, 16, 5), (6, 20, 4)])
+def test_mixed_near_far_wake_split_shapes(cuda, m, n, m_star):
+    """The mixed path puts a wake longer than its four FP64 rows into the FP32 stream as two
+    lattices that both hold the split row; the workspace must size the stream and the
+    partial sums for that (13 x 53 with 25 rows once overran them and left NaN forces).
+    Wakes of 5 and 4 rows: one far row, and no far rows at all."""
+    c = cases.wing_heave(m=m, n=n, m_star=m_star, n_steps=4)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        dc = _device_case(c, prec, c.n_tstep)
+        dc.solve_dynamic(1, c.n_tstep)
+        out[prec] = (dc.arrays["gamma_b"][1:].cpu().numpy(), dc.force_total[1:].cpu().numpy())
+    assert np.all(np.isfinite(out["mixed"][1]))
+    g64, gm = out["fp64"][0], out["mixed"][0]
+    assert np.max(np.abs(gm - g64)) < TOL * np.max(np.abs(g64))
+    cl64, _ = _coeffs(out["fp64"][1], c)
+    clm, _ = _coeffs(out["mixed"][1], c)
+    assert np.max(np.abs(clm - cl64)) < TOL * np.max(np.abs(cl64))
