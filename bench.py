@@ -509,6 +509,12 @@ def main():
             linear = linear_bench(torch, small=True)
         except Exception as e:  # keep the headline line if this leg fails
             linear = {"error": f"{type(e).__name__}: {e}"}
+    adjoint = None
+    if rank == 0 and world == 1 and not args.small and args.adjoint_steps > 0:
+        try:  # config 3's gradient on one GPU (its own leg: --adjoint)
+            adjoint = adjoint_bench(args, torch)
+        except Exception as e:  # keep the headline line if this leg fails
+            adjoint = {"error": f"{type(e).__name__}: {e}"}
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -524,7 +530,7 @@ def main():
                      "refinement)",
         "e2e": e2e, "fp64_gpu": fp64, "roofline": roof, "cpu_baseline": cpu, "factorisation": factor,
         "gpu_launches": int(launches), "clocks": clk.summary(), "serving": serving,
-        "serving_below_capacity": serving_low, "autotune": autotune,
+        "serving_below_capacity": serving_low, "adjoint": adjoint, "autotune": autotune,
         "linear": linear,
     }
     print(json.dumps(line))
@@ -845,7 +851,18 @@ def adjoint_bench(args, torch):
     t_fwd = time.perf_counter() - t0
     res = {"workload": "12x64 wing, W=100, 32 twist angles, pitch 2 deg at k=0.3, checkpoint 10",
            "steps": c.n_steps, "forward_s": t_fwd}
-    for name, e in (("CL", e_l), ("CD", e_d)):
+    # central differences of the FP64 GPU forward for two twist angles (both coefficients
+    # from the same pair of runs)
+    fd = {}
+    for k in (3, 17):
+        h = 1e-6
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += h
+        tm[k] -= h
+        jp = mean_coeffs(cases.twisted_grid(c.m, c.n, c.chord, 0.25, np.interp(span_y, ctrl_y, tp)))
+        jm = mean_coeffs(cases.twisted_grid(c.m, c.n, c.chord, 0.25, np.interp(span_y, ctrl_y, tm)))
+        fd[k] = [(jp[i] - jm[i]) / (2 * h) for i in (0, 1)]
+    for idx, (name, e) in enumerate((("CL", e_l), ("CD", e_d))):
         t0 = time.perf_counter()
         J, g = PrescribedAdjoint(uv).gradient(c.hg_t, c.hg_dot_t, weights(e), checkpoint=10)
         torch.cuda.synchronize()
@@ -853,19 +870,9 @@ def adjoint_bench(args, torch):
         grad = np.einsum("kmjd,mjd->k", jac, g)
         res[f"mean_{name}"] = J
         res[f"d{name}_dtwist"] = grad.tolist()
-        checks = []
-        for k in (3, 17):
-            h = 1e-6
-            tp, tm = theta.copy(), theta.copy()
-            tp[k] += h
-            tm[k] -= h
-            jp = mean_coeffs(cases.twisted_grid(c.m, c.n, c.chord, 0.25, np.interp(span_y, ctrl_y, tp)))
-            jm = mean_coeffs(cases.twisted_grid(c.m, c.n, c.chord, 0.25, np.interp(span_y, ctrl_y, tm)))
-            idx = 0 if name == "CL" else 1
-            fd = (jp[idx] - jm[idx]) / (2 * h)
-            checks.append({"param": k, "adjoint": float(grad[k]), "central_fd_fp64_gpu": fd,
-                           "rel_diff": abs(fd - grad[k]) / max(abs(fd), 1e-30)})
-        res[f"fd_check_{name}"] = checks
+        res[f"fd_check_{name}"] = [{"param": k, "adjoint": float(grad[k]), "central_fd_fp64_gpu": fd[k][idx],
+                                    "rel_diff": abs(fd[k][idx] - grad[k]) / max(abs(fd[k][idx]), 1e-30)}
+                                   for k in (3, 17)]
     return res
 
 
