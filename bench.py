@@ -705,7 +705,11 @@ def _linear_line(torch, label, m, n, w, wt, n_t):
     return {"workload": f"{label}, {wt} wake, epsilon kernel", "n_states": lin.n_states, "n_inputs": lin.n_inputs,
             "n_outputs": lin.n_outputs, "linearise_s": min(times),
             "matrix_bytes": 8 * (lin.n_states + lin.n_outputs) * (lin.n_states + lin.n_inputs),
-            "peak_device_gb_assembly": peak, "run_steps_per_s": n_t / (ms * 1e-3)}
+            "peak_device_gb_assembly": peak, "run_steps_per_s": n_t / (ms * 1e-3),
+            # the march reads A once per step (fj_lti_march); run() also does the B u, C x and D u
+            # products, so this lower-bounds the march's own bandwidth
+            "march_a_gbs": 8.0 * lin.n_states ** 2 * (n_t - 1) / (ms * 1e-3) / 1e9,
+            "a_fits_l2": 8 * lin.n_states ** 2 < 126e6}
 
 
 def measured_peaks():

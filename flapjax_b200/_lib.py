@@ -146,6 +146,7 @@ _SIGS = {
     "fj_batch_workspace_size": (C.c_int, [C.c_int, C.POINTER(C.c_size_t)]),
     "fj_step_batched": (C.c_int, [C.POINTER(FjBatchItem), C.c_int, _P, C.c_size_t, _P]),
     "fj_batch_release": (C.c_int, [_P]),
+    "fj_lti_march": (C.c_int, [_P, C.c_int, _P, C.c_int64, _P, C.c_int64, C.c_int, _P]),
     "fj_batch_graph_stats": (C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "fj_case_residual": (C.c_int, [C.POINTER(FjCaseConfig), _P, C.c_size_t, C.c_int, C.POINTER(C.c_double), _P]),
     "fj_case_factors_copy": (C.c_int, [C.POINTER(FjCaseConfig), _P, C.c_size_t, _P, _P, _P]),

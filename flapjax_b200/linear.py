@@ -203,9 +203,10 @@ class LinearSystem:
                 raise ValueError(f"Expected shape ({self.n_states},), but got shape {tuple(x0.shape)}.Issue with "
                                  f"input 'x0'")
             x[0] = x0
-        bu = u @ self.b.T  # every step's input term in one product
-        for i in range(1, n_t):  # one GEMV-with-add per step
-            torch.addmv(bu[i - 1] if self.removed_u_np1 else bu[i], self.a, x[i - 1], out=x[i])
+        bu = (u @ self.b.T).contiguous()  # every step's input term in one product
+        a = self.a.contiguous()
+        _lib.call("fj_lti_march", a.data_ptr(), self.n_states, bu.data_ptr(), bu.stride(0), x.data_ptr(), n_t,
+                  1 if self.removed_u_np1 else 0, torch.cuda.current_stream(dev).cuda_stream)
         y = x @ self.c.T + u @ self.d.T
         return x, y
 

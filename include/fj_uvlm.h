@@ -309,6 +309,14 @@ FJ_API int fj_lu_solve_many_workspace_size(int n, int64_t nrhs, size_t* bytes);
 FJ_API int fj_lu_solve_many(const double* d_lu, int n, const int32_t* d_piv, double* d_b, int64_t nrhs,
                             int64_t ldb, void* d_ws, size_t ws_bytes, fj_stream_t stream);
 
+/* The state march of LinearSystem.run (utils/linear.py:775-822): for i = 1 .. n_tstep-1,
+ * x_i = A x_{i-1} + bu_{i-shift}, with A (n, n) row-major, the input terms bu (n_tstep rows
+ * of leading dimension ld_bu, bu_i = B u_i) and x (n_tstep, n) whose row 0 holds x_0.
+ * shift = 1 after remove_u_np1 (the system takes the input of step i-1), else 0.  One
+ * GEMV-with-add launch per step on the caller's stream; FP64. */
+FJ_API int fj_lti_march(const double* d_a, int n, const double* d_bu, int64_t ld_bu, double* d_x,
+                        int64_t n_tstep, int shift, fj_stream_t stream);
+
 /* fj_vind without a caller workspace, for callers that cannot allocate device memory
  * (a plugin host that owns the device memory pool, a real-time loop that may not block in
  * cudaMalloc).  No counterpart in the reference.  Its scratch is a fixed 8 MiB array in

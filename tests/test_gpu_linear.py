@@ -92,6 +92,32 @@ def test_lu_solve_many(cuda):
                   ws.numel(), s)
 
 
+@pytest.mark.parametrize("n,shift", [(300, 0), (257, 1)])
+def test_lti_march_matches_numpy(cuda, n, shift):
+    """fj_lti_march (LinearSystem.run's state march): x_i = A x_{i-1} + bu_{i-shift} against
+    the same recurrence in NumPy FP64, an even order (16-byte row loads) and an odd one,
+    with the input rows strided; a bad shift is refused."""
+    import torch
+
+    from flapjax_b200 import _lib
+
+    rng = np.random.default_rng(1)
+    nt, ld = 40, n + 3
+    a = rng.normal(size=(n, n)) * (0.9 / np.sqrt(n))
+    bu = rng.normal(size=(nt, ld))
+    x = np.zeros((nt, n))
+    x[0] = rng.normal(size=n)
+    want = x.copy()
+    for i in range(1, nt):
+        want[i] = a @ want[i - 1] + bu[i - shift, :n]
+    ta, tb, tx = (torch.as_tensor(v).to(cuda) for v in (a, bu, x))
+    s = torch.cuda.current_stream(cuda).cuda_stream
+    _lib.call("fj_lti_march", ta.data_ptr(), n, tb.data_ptr(), ld, tx.data_ptr(), nt, shift, s)
+    assert rel_err(tx.cpu().numpy(), want) < 1e-13
+    with pytest.raises(Exception):
+        _lib.call("fj_lti_march", ta.data_ptr(), n, tb.data_ptr(), ld, tx.data_ptr(), nt, 2, s)
+
+
 def _product_uvlm(g, **kw):
     import flapjax_b200 as fj
 
