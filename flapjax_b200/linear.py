@@ -191,6 +191,9 @@ class LinearSystem:
         import torch
 
         dev = self.a.device
+        if dev.type != "cuda":
+            raise RuntimeError("LinearSystem.run marches on the GPU (fj_lti_march): its matrices must be CUDA "
+                               "tensors")
         u = torch.as_tensor(np.asarray(u) if not torch.is_tensor(u) else u, dtype=torch.float64).to(dev)
         if u.ndim != 2 or u.shape[1] != self.n_inputs:
             raise ValueError(f"Expected shape (None, {self.n_inputs}), but got shape {tuple(u.shape)}.Issue with "

@@ -118,6 +118,34 @@ def test_lti_march_matches_numpy(cuda, n, shift):
         _lib.call("fj_lti_march", ta.data_ptr(), n, tb.data_ptr(), ld, tx.data_ptr(), nt, 2, s)
 
 
+def test_linear_system_run_matches_oracle(cuda):
+    """LinearSystem.run (utils/linear.py:775-822) on the device against the oracle's
+    restatement, before and after remove_u_np1."""
+    import torch
+
+    from flapjax_b200.linear import LinearSystem
+    from oracle.uvlm_linear import LinearSystemRef
+
+    rng = np.random.default_rng(0)
+    a = 0.3 * rng.normal(size=(7, 7))
+    b, c, d = rng.normal(size=(7, 4)), rng.normal(size=(5, 7)), rng.normal(size=(5, 4))
+    u, x0 = rng.normal(size=(9, 4)), rng.normal(size=7)
+    ours = LinearSystem(*(torch.as_tensor(z).to(cuda) for z in (a, b, c, d)), 0.1)
+    ref = LinearSystemRef(a, b, c, d, 0.1)
+    for removed in (False, True):
+        if removed:
+            ours.remove_u_np1()
+            ref.remove_u_np1()
+        x, y = ours.run(u, x0)
+        xr, yr = ref.run(u, x0)
+        assert np.allclose(x.cpu().numpy(), xr, rtol=1e-13, atol=1e-13)
+        assert np.allclose(y.cpu().numpy(), yr, rtol=1e-13, atol=1e-13)
+    with pytest.raises(ValueError):
+        ours.run(u[:, :3])
+    with pytest.raises(ValueError):
+        ours.run(u, x0[:3])
+
+
 def _product_uvlm(g, **kw):
     import flapjax_b200 as fj
 
