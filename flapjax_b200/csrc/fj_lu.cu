@@ -113,6 +113,162 @@ __global__ void __launch_bounds__(1024) lu_panel_kernel(T* __restrict__ a, int n
     }
 }
 
+// The same panel with its rows in registers, for panels of at most RPT * 1024 rows.  The
+// panel comes in and goes out through shared memory (coalesced cp.async loads and row-
+// contiguous stores, as lu_panel_kernel); between, thread t owns rows t + 1024 i (i < RPT)
+// in registers, and a column costs two barriers: one to combine the warps' pivot
+// candidates, one to exchange the pivot row and row j.  Pivots (first maximum, as getrf)
+// and every arithmetic operation are those of lu_panel_kernel, so the factors are bitwise
+// the same.
+template <typename T, int NB, int RPT>
+__global__ void __launch_bounds__(1024) lu_panel_reg_kernel(T* __restrict__ a, int n, int k,
+                                                            int32_t* __restrict__ piv, int* __restrict__ info,
+                                                            const int* __restrict__ run_flag) {
+    if (run_flag != nullptr && *run_flag == 0) return;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* P = reinterpret_cast<T*>(smraw);  // (n-k) x LDP staging
+    constexpr int LDP = NB + 1;
+    __shared__ T s_val[32];
+    __shared__ int s_idx[32];
+    __shared__ T s_rowp[NB], s_rowj[NB];
+    const int rows = n - k;
+    const int nb = min(NB, rows);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nwarps = blockDim.x >> 5;
+    for (int idx = tid; idx < rows * NB; idx += blockDim.x) {
+        const int r = idx / NB, c = idx % NB;
+        const T* src = a + (int64_t)(k + r) * n + k + min(c, nb - 1);
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(P + r * LDP + c);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(src), "n"(sizeof(T)),
+                     "r"(c < nb ? (int)sizeof(T) : 0)
+                     : "memory");
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    T v[RPT][NB];
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+        const int r = tid + i * (int)blockDim.x;
+#pragma unroll
+        for (int c = 0; c < NB; ++c) v[i][c] = r < rows ? P[r * LDP + c] : T(0);
+    }
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        if (j >= nb) break;  // uniform over the CTA
+        T best = T(-1);
+        int bi = INT_MAX;
+#pragma unroll
+        for (int i = 0; i < RPT; ++i) {
+            const int r = tid + i * (int)blockDim.x;
+            if (r >= j && r < rows) {
+                const T x = absval(v[i][j]);
+                if (x > best) {
+                    best = x;
+                    bi = r;
+                }
+            }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const T ov = __shfl_down_sync(0xffffffffu, best, off);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+            if (ov > best || (ov == best && oi < bi)) {
+                best = ov;
+                bi = oi;
+            }
+        }
+        if (lane == 0) {
+            s_val[warp] = best;
+            s_idx[warp] = bi;
+        }
+        __syncthreads();
+        best = lane < nwarps ? s_val[lane] : T(-1);
+        bi = lane < nwarps ? s_idx[lane] : INT_MAX;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const T ov = __shfl_xor_sync(0xffffffffu, best, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+            if (ov > best || (ov == best && oi < bi)) {
+                best = ov;
+                bi = oi;
+            }
+        }
+        const int p = (bi == INT_MAX) ? j : bi;  // all-NaN column: keep the diagonal
+        if (tid == 0) piv[k + j] = k + p;
+#pragma unroll
+        for (int i = 0; i < RPT; ++i) {  // the owners of rows p and j publish them
+            const int r = tid + i * (int)blockDim.x;
+            if (r == p) {
+#pragma unroll
+                for (int c = 0; c < NB; ++c) s_rowp[c] = v[i][c];
+            }
+            if (r == j) {
+#pragma unroll
+                for (int c = 0; c < NB; ++c) s_rowj[c] = v[i][c];
+            }
+        }
+        __syncthreads();
+        if (p != j) {  // the swap: row j takes the pivot row, row p takes row j
+#pragma unroll
+            for (int i = 0; i < RPT; ++i) {
+                const int r = tid + i * (int)blockDim.x;
+                if (r == j) {
+#pragma unroll
+                    for (int c = 0; c < NB; ++c) v[i][c] = s_rowp[c];
+                }
+                if (r == p) {
+#pragma unroll
+                    for (int c = 0; c < NB; ++c) v[i][c] = s_rowj[c];
+                }
+            }
+        }
+        const T pv = s_rowp[j];
+        if (pv == T(0)) {
+            if (tid == 0 && *info == 0) *info = k + j + 1;
+        } else {
+#pragma unroll
+            for (int i = 0; i < RPT; ++i) {
+                const int r = tid + i * (int)blockDim.x;
+                if (r > j && r < rows) {
+                    const T l = v[i][j] / pv;
+                    v[i][j] = l;
+#pragma unroll
+                    for (int c = j + 1; c < NB; ++c)
+                        if (c < nb) v[i][c] -= l * s_rowp[c];
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+        const int r = tid + i * (int)blockDim.x;
+        if (r < rows) {
+#pragma unroll
+            for (int c = 0; c < NB; ++c) P[r * LDP + c] = v[i][c];
+        }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < rows * NB; idx += blockDim.x) {
+        const int r = idx / NB, c = idx % NB;
+        if (c < nb) a[(int64_t)(k + r) * n + k + c] = P[r * LDP + c];
+    }
+}
+
+// One panel at column k: the register form where its rows fit (at most 2048), else the
+// shared-memory form; both stage the panel in the same dynamic shared memory.
+template <typename T, int NB>
+static void launch_panel(T* a, int n, int k, int32_t* piv, int* info, const int* run_flag, cudaStream_t s) {
+    const int rows = n - k;
+    const size_t smem = (size_t)rows * (NB + 1) * sizeof(T);
+    if (rows <= 1024)
+        lu_panel_reg_kernel<T, NB, 1><<<1, 1024, smem, s>>>(a, n, k, piv, info, run_flag);
+    else if (rows <= 2048)
+        lu_panel_reg_kernel<T, NB, 2><<<1, 1024, smem, s>>>(a, n, k, piv, info, run_flag);
+    else
+        lu_panel_kernel<T, NB><<<1, 1024, smem, s>>>(a, n, k, piv, info, run_flag);
+    note_launch();
+}
+
 // Row swaps of the panel at column k for every other column; U12 = L11^-1 A12 for the
 // columns [k + nb, c_end).  The panel's swaps (applied in order, as getrf) compose to one
 // permutation of the at most 2 NB rows they touch; thread 0 works it out in shared memory,
@@ -246,11 +402,12 @@ static int lu_factor_impl(T* a, int n, int32_t* piv, int* d_info, cudaStream_t s
     const size_t smem = (size_t)n * (NB + 1) * sizeof(T);
     if (smem > 220 * 1024) return fail(FJ_ERR_UNSUPPORTED, "lu_factor: n=%d too large for the shared-memory panel", n);
     FJ_TRY(allow_dynamic_smem((const void*)lu_panel_kernel<T, NB>, (size_t)smem));
+    FJ_TRY(allow_dynamic_smem((const void*)lu_panel_reg_kernel<T, NB, 1>, (size_t)smem));
+    FJ_TRY(allow_dynamic_smem((const void*)lu_panel_reg_kernel<T, NB, 2>, (size_t)smem));
     FJ_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int), s));
     for (int k = 0; k < n; k += NB) {
         const int nb = min(NB, n - k);
-        lu_panel_kernel<T, NB><<<1, 1024, (size_t)(n - k) * (NB + 1) * sizeof(T), s>>>(a, n, k, piv, d_info,
-                                                                                         run_flag); note_launch();
+        launch_panel<T, NB>(a, n, k, piv, d_info, run_flag, s);
         if (n > nb) {
             lu_swap_trsm_kernel<T, NB><<<(n + 255) / 256, 256, 0, s>>>(a, n, k, piv, n, run_flag); note_launch();
         }
@@ -503,14 +660,14 @@ static int lu_factor32_tc_impl(float* a, int n, int32_t* piv, int* d_info, int* 
     const size_t smem = (size_t)n * (NB + 1) * sizeof(float);
     if (smem > 220 * 1024) return fail(FJ_ERR_UNSUPPORTED, "lu_factor: n=%d too large for the shared-memory panel", n);
     FJ_TRY(allow_dynamic_smem((const void*)lu_panel_kernel<float, NB>, smem));
+    FJ_TRY(allow_dynamic_smem((const void*)lu_panel_reg_kernel<float, NB, 1>, smem));
+    FJ_TRY(allow_dynamic_smem((const void*)lu_panel_reg_kernel<float, NB, 2>, smem));
     FJ_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int), s));
     for (int k = 0; k < n; k += kTcBlk) {
         const int kb = min(kTcBlk, n - k), ke = k + kb;
         for (int j = k; j < ke; j += NB) {
             const int nb = min(NB, n - j);
-            lu_panel_kernel<float, NB><<<1, 1024, (size_t)(n - j) * (NB + 1) * sizeof(float), s>>>(a, n, j, piv, d_info,
-                                                                                              nullptr);
-            note_launch();
+            launch_panel<float, NB>(a, n, j, piv, d_info, nullptr, s);
             if (n > nb) {
                 lu_swap_trsm_kernel<float, NB><<<(n + 255) / 256, 256, 0, s>>>(a, n, j, piv, ke, nullptr);
                 note_launch();
