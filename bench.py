@@ -440,7 +440,7 @@ def main():
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "ms_per_step": t_ms / K,
                               "steps": K, "warmup": W, "roofline": roof, "gpu_launches": int(launches),
-                              "note": "kernels only: no other legs"}))
+                              "autotune": autotune, "note": "kernels only: no other legs"}))
         return 0
 
     # -- plain FP64 path and the mixed path's force-coefficient error -------------------

@@ -1314,7 +1314,7 @@ static void assign_splits(std::vector<VindJob>& jobs, int precision) {
 }
 
 static int launch_sum(const std::vector<VindJob>& jobs, const std::vector<int64_t>& cta0, char* d_jobs, char* d_cta0,
-                      int precision, int kernel, double r_cut, cudaStream_t s, bool persistent) {
+                      int precision, int kernel, double r_cut, cudaStream_t s, bool persistent, int tile) {
     if (jobs.empty()) return FJ_OK;
     double pairs = 0.0;
     int64_t max_t = 0;
@@ -1323,7 +1323,7 @@ static int launch_sum(const std::vector<VindJob>& jobs, const std::vector<int64_
         max_t = std::max(max_t, j.n_targets);
     }
     FJ_TRY(vind_launch_jobs((const VindJob*)d_jobs, (const int64_t*)d_cta0, (int)jobs.size(), cta0.back(), pairs,
-                            precision, kernel, r_cut, s, persistent));
+                            precision, kernel, r_cut, s, persistent, tile));
     return reduce_jobs((const VindJob*)d_jobs, (int)jobs.size(), max_t, s);
 }
 
@@ -1573,15 +1573,31 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
             if (cap < 1) return fail(FJ_ERR_NOMEM, "partial buffer too small for %lld targets", (long long)j.n_targets);
             j.n_split = (int)std::min<int64_t>(j.n_split, cap);
         }
-    auto fill_cta = [&](const std::vector<VindJob>& jobs, size_t off, int prec) {
+    // one tile (targets per thread) per FP32 launch: the autotuned choice of its largest job
+    auto phase_tile = [&](const std::vector<VindJob>& jobs) {
+        double most = -1.0;
+        int tile = 0;
+        for (const VindJob& j : jobs) {
+            const double w = (double)j.n_targets * (double)j.n_links;
+            if (w > most) {
+                most = w;
+                tile = choose_tile(j.n_targets, j.n_elem, precision);
+            }
+        }
+        return tile;
+    };
+    const int tf = phase_tile(jf), tr = phase_tile(jr), tfo = phase_tile(jfo);
+    auto fill_cta = [&](const std::vector<VindJob>& jobs, size_t off, int prec, int tile) {
         int64_t* c0 = (int64_t*)(h.data() + off);
         c0[0] = 0;
-        for (size_t q = 0; q < jobs.size(); ++q) c0[q + 1] = c0[q] + vind_ctas(jobs[q].n_targets, jobs[q].n_split, prec);
+        for (size_t q = 0; q < jobs.size(); ++q)
+            c0[q + 1] = c0[q] + vind_ctas(jobs[q].n_targets, jobs[q].n_split, prec, tile);
         return std::vector<int64_t>(c0, c0 + jobs.size() + 1);
     };
-    const std::vector<int64_t> cf = fill_cta(jf, tl.cta_free, precision), cr = fill_cta(jr, tl.cta_rhs, precision),
-                               cfo = fill_cta(jfo, tl.cta_force, precision),
-                               crn = fill_cta(jrn, tl.cta_near, FJ_PREC_FP64);
+    const std::vector<int64_t> cf = fill_cta(jf, tl.cta_free, precision, tf),
+                               cr = fill_cta(jr, tl.cta_rhs, precision, tr),
+                               cfo = fill_cta(jfo, tl.cta_force, precision, tfo),
+                               crn = fill_cta(jrn, tl.cta_near, FJ_PREC_FP64, 0);
     memcpy(h.data() + tl.pack_free, pf.data(), K * sizeof(PackJob));
     memcpy(h.data() + tl.pack_wake, pw.data(), K * sizeof(PackJob));
     memcpy(h.data() + tl.pack_bound, pb.data(), K * sizeof(PackJob));
@@ -1610,7 +1626,7 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
         };
         g = {precision, kernel, rc_bits, K, max_v, max_p, max_w, max_wt, max_f, max_n, max_fil, any_mirror, any_free,
              any_changed, any_var, any_polar, max_xw, max_cols, max_e_free, max_e_wake, max_e_bound, max_e_near,
-             (int64_t)ref.size()};
+             (int64_t)ref.size(), tf, tr, tfo};
         sum_sig(jf);
         sum_sig(jr);
         sum_sig(jrn);
@@ -1647,7 +1663,8 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
     if (any_free) {
         FJ_TRY(pack_jobs((const PackJob*)(d_tab + tl.pack_free), K, max_e_free, precision, s));
         k_gather_wake_targets<<<dim3(nblk(max_wt), K), b, 0, s>>>(dC); note_launch();
-        FJ_TRY(launch_sum(jf, cf, d_tab + tl.job_free, d_tab + tl.cta_free, precision, kernel, r_cut, s, persistent_sums));
+        FJ_TRY(launch_sum(jf, cf, d_tab + tl.job_free, d_tab + tl.cta_free, precision, kernel, r_cut, s, persistent_sums,
+                          tf));
     }
     k_wake_shed<<<dim3(nblk(max_w), K), b, 0, s>>>(dC); note_launch();
     if (any_var) {  // delta_w surfaces: convect all rows, then re-discretise (aero/utils.py:452-491)
@@ -1667,8 +1684,9 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
     for (int k = 0; k < K; ++k)  // cases without (far) wake filaments: zero, then the near rows add
         if (rhs_far[k] == 0 && items[k].p.nb > 0)
             FJ_CUDA(cudaMemsetAsync(items[k].p.v, 0, items[k].p.nb * 3 * sizeof(double), s));
-    FJ_TRY(launch_sum(jr, cr, d_tab + tl.job_rhs, d_tab + tl.cta_rhs, precision, kernel, r_cut, s, persistent_sums));
-    FJ_TRY(launch_sum(jrn, crn, d_tab + tl.job_near, d_tab + tl.cta_near, FJ_PREC_FP64, kernel, r_cut, s, persistent_sums));
+    FJ_TRY(launch_sum(jr, cr, d_tab + tl.job_rhs, d_tab + tl.cta_rhs, precision, kernel, r_cut, s, persistent_sums, tr));
+    FJ_TRY(launch_sum(jrn, crn, d_tab + tl.job_near, d_tab + tl.cta_near, FJ_PREC_FP64, kernel, r_cut, s, persistent_sums,
+                      0));
     k_rhs<<<dim3(nblk(max_n), K), b, 0, s>>>(dC); note_launch();
     FJ_LAUNCH_CHECK("step: geometry, wake, RHS");
     // 5. solve
@@ -1694,7 +1712,8 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
     // 6. forces with bound(n) + wake(n)
     FJ_TRY(pack_jobs((const PackJob*)(d_tab + tl.pack_bound), K, max_e_bound, precision, s));
     k_force_targets<<<dim3(nblk(max_f), K), b, 0, s>>>(dC); note_launch();
-    FJ_TRY(launch_sum(jfo, cfo, d_tab + tl.job_force, d_tab + tl.cta_force, precision, kernel, r_cut, s, persistent_sums));
+    FJ_TRY(launch_sum(jfo, cfo, d_tab + tl.job_force, d_tab + tl.cta_force, precision, kernel, r_cut, s, persistent_sums,
+                      tfo));
     k_force_filament<<<dim3(nblk(max_f), K), b, 0, s>>>(dC); note_launch();
     // 7. gamma_dot, vertex forces, strip alpha, totals
     if (!any_polar) {

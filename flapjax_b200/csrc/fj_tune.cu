@@ -9,7 +9,10 @@
 // has the real element layout, chain breaks included) and seeded targets above it, times
 // the sum + reduction at candidate split counts with CUDA events, and publishes the
 // fastest into a new immutable table (keyed by precision, log2 targets, log2 stream
-// length) that choose_split consults from then on.
+// length) that choose_split consults from then on.  The FP32 sums are also timed with four
+// targets per thread instead of two (the tile shape: twice the targets share each staged
+// filament element, at twice the registers and half the resident CTAs); the table records
+// which tile won beside the split.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -152,15 +155,22 @@ int fj_autotune_vind(int precision, int kernel, double r_cut, const int64_t* n_t
         for (int& c : cand) c = std::max(1, std::min(c, bound));
         std::sort(cand.begin(), cand.end());
         cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
-        int best = h;
+        int best = h, best_tile = 2;
         float best_ms = 0.0f, h_ms = 0.0f;
+        // FP32: each split count with two and with four targets per thread
+        std::vector<std::pair<int, int>> trials;
         for (int sp : cand) {
+            trials.push_back({sp, 2});
+            if (precision == FJ_PREC_MIXED) trials.push_back({sp, 4});
+        }
+        for (const auto& trial : trials) {
+            const int sp = trial.first, tile = trial.second;
             VindJob job{targets, nt, strm, ne, sp, part, ne, out};
             float t = 1e30f;
             for (int rep = 0; rep < 4 && st == FJ_OK; ++rep) {
                 float ms = 0.0f;
                 st = cuda_status(cudaEventRecord(e0, s), "autotune event");
-                if (st == FJ_OK) st = vind_launch(job, precision, kernel, r_cut, s);
+                if (st == FJ_OK) st = vind_launch(job, precision, kernel, r_cut, s, tile);
                 if (st == FJ_OK) st = reduce_partials(part, sp, nt, out, 0, 1.0, s);
                 if (st == FJ_OK) st = cuda_status(cudaEventRecord(e1, s), "autotune event");
                 if (st == FJ_OK) st = cuda_status(cudaEventSynchronize(e1), "autotune sync");
@@ -168,16 +178,18 @@ int fj_autotune_vind(int precision, int kernel, double r_cut, const int64_t* n_t
                 if (rep > 0) t = std::min(t, ms);  // the first run warms up
             }
             if (st != FJ_OK) break;
-            if (sp == h) h_ms = t;
-            if (best_ms == 0.0f || t < best_ms * 0.98f || (t <= best_ms * 1.02f && sp == h)) {
+            if (sp == h && tile == 2) h_ms = t;
+            // a challenger must be 2 % faster; the rule's split with the default tile wins ties
+            if (best_ms == 0.0f || t < best_ms * 0.98f || (t <= best_ms * 1.02f && sp == h && tile == 2)) {
                 best = sp;
+                best_tile = tile;
                 best_ms = t;
             }
         }
         if (st != FJ_OK) break;
         table->split[precision == FJ_PREC_FP64 ? 0 : 1][tune_bucket_targets(nt)][tune_bucket_elem(ne)] =
-            (int16_t)best;
-        if (chosen) chosen[i] = best;
+            (int16_t)encode_tuned(best, best_tile);
+        if (chosen) chosen[i] = encode_tuned(best, best_tile);
         if (heuristic) heuristic[i] = h;
         if (chosen_ms) chosen_ms[i] = best_ms;
         if (heuristic_ms) heuristic_ms[i] = h_ms;
@@ -214,8 +226,14 @@ int fj_autotune_set(const int16_t* entries, int n_entries) {
     }
     if (!entries || n_entries != (int)(sizeof(TuneTable) / sizeof(int16_t)))
         return fail(FJ_ERR_SHAPE, "autotune: table has %d entries", (int)(sizeof(TuneTable) / sizeof(int16_t)));
-    for (int i = 0; i < n_entries; ++i)
-        if (entries[i] < 0 || entries[i] > 1024) return fail(FJ_ERR_SHAPE, "autotune: entry %d = %d", i, entries[i]);
+    // entries: 0 (not tuned) or a split count in 1..1024, the FP32 block's with bit 12 for
+    // the four-target tile
+    const int half = n_entries / 2;
+    for (int i = 0; i < n_entries; ++i) {
+        const int v = entries[i], split = v & 0xFFF, extra = v & ~0xFFF;
+        const bool ok = v >= 0 && split <= 1024 && (extra == 0 || (extra == 0x1000 && i >= half && split >= 1));
+        if (!ok) return fail(FJ_ERR_SHAPE, "autotune: entry %d = %d", i, v);
+    }
     TuneTable* t = new TuneTable();
     std::copy(entries, entries + n_entries, &t->split[0][0][0]);
     tune_publish(t);

@@ -433,6 +433,13 @@ constexpr int kDup = 7;  // float4 per staged element
 // Six resident CTAs per SM (registers capped at 80): the sum is FMA-pipe bound and the
 // extra warps hide the MUFU and FMA latencies better than the registers they cost.
 constexpr int kMinCtas32 = 6;
+// Four targets per thread (two packed pairs) share each staged element between twice the
+// targets at about twice the registers: three resident CTAs per SM.
+constexpr int kMinCtas32Wide = 3;
+template <int T>
+struct MinCtas32 {
+    static constexpr int value = T == 2 ? kMinCtas32 : kMinCtas32Wide;
+};
 constexpr int kFold = 16;  // elements per FP32 partial sum (even: the ping-pong takes pairs)
 
 __device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
@@ -622,7 +629,7 @@ __device__ __forceinline__ void vind32_body(const double* __restrict__ tgt, int6
 }
 
 template <int KER, int T>
-__global__ void __launch_bounds__(kBlock, kMinCtas32) vind32_kernel(VindJob job) {
+__global__ void __launch_bounds__(kBlock, MinCtas32<T>::value) vind32_kernel(VindJob job) {
     vind32_body<KER, T>(job.targets, job.n_targets, (const Elem32*)job.stream, job.n_elem, job.n_split, job.part,
                         blockIdx.x, blockIdx.y);
 }
@@ -646,7 +653,7 @@ __device__ __forceinline__ int find_job(const int64_t* __restrict__ cta0, int n_
 // of the SMs (9 % slower on the 16 x 128 free-wake step than hardware scheduling, whose
 // last partial wave spreads over every SM).
 template <int KER, int T>
-__global__ void __launch_bounds__(kBlock, kMinCtas32) vind32_jobs_kernel(const VindJob* __restrict__ jobs,
+__global__ void __launch_bounds__(kBlock, MinCtas32<T>::value) vind32_jobs_kernel(const VindJob* __restrict__ jobs,
                                                              const int64_t* __restrict__ cta0, int n_jobs) {
     const int64_t total = cta0[n_jobs];
     for (int64_t b = blockIdx.x; b < total; b += gridDim.x) {
@@ -713,10 +720,12 @@ int reduce_partials(const double* part, int n_split, int64_t n_targets, double* 
 }
 
 constexpr int kT64 = 2;
-constexpr int kT32 = 2;
+constexpr int kT32 = 2;      // FP32 targets per thread unless the tuned table says otherwise
+constexpr int kT32Wide = 4;  // the wide tile the autotuner may choose instead
+constexpr int kTileWideFlag = 0x1000;  // tuned entry: split | flag when the wide tile won
 
 // CTAs resident per SM for the sum kernels and the SM count, queried once.
-static int g_sms = 0, g_res64 = 0, g_res32 = 0;
+static int g_sms = 0, g_res64 = 0, g_res32 = 0, g_res32w = 0;
 
 static std::once_flag g_occ_once;
 
@@ -724,12 +733,14 @@ static void query_occupancy() {
     std::call_once(g_occ_once, [] {
         int dev = 0;
         cudaGetDevice(&dev);
-        int sms = 0, r64 = 0, r32 = 0;
+        int sms = 0, r64 = 0, r32 = 0, r32w = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r64, vind64_kernel<FJ_KERNEL_EPSILON, kT64>, kBlock, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r32, vind32_kernel<FJ_KERNEL_CUTOFF, kT32>, kBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r32w, vind32_kernel<FJ_KERNEL_CUTOFF, kT32Wide>, kBlock, 0);
         g_res64 = r64 > 0 ? r64 : 1;
         g_res32 = r32 > 0 ? r32 : 1;
+        g_res32w = r32w > 0 ? r32w : 1;
         g_sms = sms > 0 ? sms : 148;
     });
 }
@@ -769,10 +780,21 @@ int tune_bucket_elem(int64_t n_elem) {
 int choose_split(int64_t n_targets, int64_t n_elem, int precision) {
     if (const TuneTable* t = tune_table()) {
         const int v = t->split[precision == FJ_PREC_FP64 ? 0 : 1][tune_bucket_targets(n_targets)][tune_bucket_elem(n_elem)];
-        if (v > 0) return std::min(v, split_bound(n_targets, n_elem, precision));
+        if (v > 0) return std::min(v & (kTileWideFlag - 1), split_bound(n_targets, n_elem, precision));
     }
     return heuristic_split(n_targets, n_elem, precision);
 }
+
+int choose_tile(int64_t n_targets, int64_t n_elem, int precision) {
+    if (precision == FJ_PREC_FP64) return kT64;
+    if (const TuneTable* t = tune_table()) {
+        const int v = t->split[1][tune_bucket_targets(n_targets)][tune_bucket_elem(n_elem)];
+        if (v > 0 && (v & kTileWideFlag)) return kT32Wide;
+    }
+    return kT32;
+}
+
+int encode_tuned(int split, int tile) { return split | (tile == kT32Wide ? kTileWideFlag : 0); }
 
 int heuristic_split(int64_t n_targets, int64_t n_elem, int precision) {
     query_occupancy();
@@ -800,10 +822,11 @@ int heuristic_split(int64_t n_targets, int64_t n_elem, int precision) {
     return (int)best;
 }
 
-int vind_launch(const VindJob& job, int precision, int kernel, double r_cut, cudaStream_t s) {
+int vind_launch(const VindJob& job, int precision, int kernel, double r_cut, cudaStream_t s, int tile) {
     if (job.n_targets == 0) return FJ_OK;
     query_occupancy();
-    const int T = precision == FJ_PREC_FP64 ? kT64 : kT32;
+    const int T = precision == FJ_PREC_FP64 ? kT64 : (tile ? tile : choose_tile(job.n_targets, job.n_elem, precision));
+    if (T != kT32 && T != kT32Wide) return fail(FJ_ERR_SHAPE, "vind: tile %d (2 or 4 targets per thread)", T);
     const int64_t gx = (job.n_targets + (int64_t)kBlock * T - 1) / ((int64_t)kBlock * T);
     if (gx > 0x7fffffff || job.n_split > 65535) return fail(FJ_ERR_SHAPE, "vind: grid too large");
     dim3 grid((unsigned)gx, (unsigned)job.n_split);
@@ -826,10 +849,14 @@ int vind_launch(const VindJob& job, int precision, int kernel, double r_cut, cud
     } else {
         switch (kernel) {
             case FJ_KERNEL_EPSILON:
-                vind32_kernel<FJ_KERNEL_EPSILON, kT32><<<grid, kBlock, 0, s>>>(job); note_launch();
+                if (T == kT32) vind32_kernel<FJ_KERNEL_EPSILON, kT32><<<grid, kBlock, 0, s>>>(job);
+                else vind32_kernel<FJ_KERNEL_EPSILON, kT32Wide><<<grid, kBlock, 0, s>>>(job);
+                note_launch();
                 break;
             case FJ_KERNEL_CUTOFF:
-                vind32_kernel<FJ_KERNEL_CUTOFF, kT32><<<grid, kBlock, 0, s>>>(job); note_launch();
+                if (T == kT32) vind32_kernel<FJ_KERNEL_CUTOFF, kT32><<<grid, kBlock, 0, s>>>(job);
+                else vind32_kernel<FJ_KERNEL_CUTOFF, kT32Wide><<<grid, kBlock, 0, s>>>(job);
+                note_launch();
                 break;
             default:
                 return fail(FJ_ERR_UNSUPPORTED, "vind: kernel %d has no FP32 variant (use FJ_PREC_FP64)", kernel);
@@ -840,19 +867,22 @@ int vind_launch(const VindJob& job, int precision, int kernel, double r_cut, cud
     return FJ_OK;
 }
 
-int64_t vind_ctas(int64_t n_targets, int n_split, int precision) {
-    const int T = precision == FJ_PREC_FP64 ? kT64 : kT32;
+int64_t vind_ctas(int64_t n_targets, int n_split, int precision, int tile) {
+    const int T = precision == FJ_PREC_FP64 ? kT64 : (tile ? tile : kT32);
     return (n_targets + (int64_t)kBlock * T - 1) / ((int64_t)kBlock * T) * n_split;
 }
 
 int vind_launch_jobs(const VindJob* d_jobs, const int64_t* d_cta0, int n_jobs, int64_t total_ctas, double pairs,
-                     int precision, int kernel, double r_cut, cudaStream_t s, bool persistent) {
+                     int precision, int kernel, double r_cut, cudaStream_t s, bool persistent, int tile) {
     if (n_jobs == 0 || total_ctas == 0) return FJ_OK;
     if (total_ctas > 0x7fffffff) return fail(FJ_ERR_SHAPE, "vind jobs: grid too large");
     query_occupancy();
     // one CTA per virtual CTA (the hardware schedules them, and a last partial wave spreads
     // over every SM), or, persistent, the CTAs the GPU holds at once whatever the jobs need
-    const int64_t resident = (int64_t)g_sms * (precision == FJ_PREC_FP64 ? g_res64 : g_res32);
+    const bool wide = precision != FJ_PREC_FP64 && tile == kT32Wide;
+    if (precision != FJ_PREC_FP64 && tile != 0 && tile != kT32 && tile != kT32Wide)
+        return fail(FJ_ERR_SHAPE, "vind jobs: tile %d (2 or 4 targets per thread)", tile);
+    const int64_t resident = (int64_t)g_sms * (precision == FJ_PREC_FP64 ? g_res64 : (wide ? g_res32w : g_res32));
     const unsigned g = (unsigned)std::max<int64_t>(1, persistent ? resident : total_ctas);
     const int prof = prof_start(s);
     if (precision == FJ_PREC_FP64) {
@@ -873,10 +903,14 @@ int vind_launch_jobs(const VindJob* d_jobs, const int64_t* d_cta0, int n_jobs, i
     } else {
         switch (kernel) {
             case FJ_KERNEL_EPSILON:
-                vind32_jobs_kernel<FJ_KERNEL_EPSILON, kT32><<<g, kBlock, 0, s>>>(d_jobs, d_cta0, n_jobs); note_launch();
+                if (!wide) vind32_jobs_kernel<FJ_KERNEL_EPSILON, kT32><<<g, kBlock, 0, s>>>(d_jobs, d_cta0, n_jobs);
+                else vind32_jobs_kernel<FJ_KERNEL_EPSILON, kT32Wide><<<g, kBlock, 0, s>>>(d_jobs, d_cta0, n_jobs);
+                note_launch();
                 break;
             case FJ_KERNEL_CUTOFF:
-                vind32_jobs_kernel<FJ_KERNEL_CUTOFF, kT32><<<g, kBlock, 0, s>>>(d_jobs, d_cta0, n_jobs); note_launch();
+                if (!wide) vind32_jobs_kernel<FJ_KERNEL_CUTOFF, kT32><<<g, kBlock, 0, s>>>(d_jobs, d_cta0, n_jobs);
+                else vind32_jobs_kernel<FJ_KERNEL_CUTOFF, kT32Wide><<<g, kBlock, 0, s>>>(d_jobs, d_cta0, n_jobs);
+                note_launch();
                 break;
             default:
                 return fail(FJ_ERR_UNSUPPORTED, "vind: kernel %d has no FP32 variant (use FJ_PREC_FP64)", kernel);

@@ -92,26 +92,35 @@ struct PackJob {
 //  vind: CTAs of job j are cta0[j] .. cta0[j+1]-1 (ctas_x(j) * n_split(j) of them);
 //  all jobs of one launch share precision and kernel.
 int vind_launch_jobs(const VindJob* d_jobs, const int64_t* d_cta0, int n_jobs, int64_t total_ctas, double pairs,
-                     int precision, int kernel, double r_cut, cudaStream_t s, bool persistent = false);
+                     int precision, int kernel, double r_cut, cudaStream_t s, bool persistent = false,
+                     int tile = 0);
 int pack_jobs(const PackJob* d_jobs, int n_jobs, int64_t max_elem, int precision, cudaStream_t s);
 int reduce_jobs(const VindJob* d_jobs, int n_jobs, int64_t max_targets, cudaStream_t s);
-// CTAs of one sum (target tiles x splits), for building cta0.
-int64_t vind_ctas(int64_t n_targets, int n_split, int precision);
+// CTAs of one sum (target tiles x splits), for building cta0; tile = targets per thread of
+// the FP32 sum (2 or 4; 0 = 2), ignored for FP64.
+int64_t vind_ctas(int64_t n_targets, int n_split, int precision, int tile = 0);
 
 // filaments of an (rows, cols) lattice: rows(cols+1) chordwise + (rows+1)cols spanwise
 inline int64_t lattice_links(int rows, int cols) {
     return (int64_t)rows * (cols + 1) + (int64_t)(rows + 1) * cols;
 }
 
-int vind_launch(const VindJob& job, int precision, int kernel, double r_cut, cudaStream_t s);
+// tile: FP32 targets per thread (2 or 4); 0 takes the tuned table's choice for the shape.
+int vind_launch(const VindJob& job, int precision, int kernel, double r_cut, cudaStream_t s, int tile = 0);
 int reduce_partials(const double* part, int n_split, int64_t n_targets, double* out,
                     int accumulate, double scale, cudaStream_t s);
 int choose_split(int64_t n_targets, int64_t n_elem, int precision);
+// FP32 targets per thread for a shape: 4 where the autotuner found the wide tile faster,
+// else 2 (FP64: 2).
+int choose_tile(int64_t n_targets, int64_t n_elem, int precision);
+// A tuned table entry: the split count, with bit 12 set when the wide tile won.
+int encode_tuned(int split, int tile);
 // The wave-filling rule choose_split falls back to where no tuned entry exists.
 int heuristic_split(int64_t n_targets, int64_t n_elem, int precision);
 
-// Tuned split counts, by precision (0 FP64, 1 FP32), log2 of the target count and log2 of
-// the stream length; 0 = not tuned.  A published table is immutable.
+// Tuned split counts (and, FP32, the tile: bit 12 set for four targets per thread), by
+// precision (0 FP64, 1 FP32), log2 of the target count and log2 of the stream length;
+// 0 = not tuned.  A published table is immutable.
 constexpr int kTuneTargetBuckets = 24, kTuneElemBuckets = 28;
 struct TuneTable {
     int16_t split[2][kTuneTargetBuckets][kTuneElemBuckets];

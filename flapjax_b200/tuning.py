@@ -1,8 +1,9 @@
 """Autotuning of the Biot-Savart sum launches (fj_autotune_vind).
 
 A sum of n_targets points over a stream of filament elements runs as target tiles x
-splits CTAs.  ``autotune`` times candidate split counts for given shapes on the device
-and publishes the fastest in the library's immutable table, which every later launch of
+splits CTAs.  ``autotune`` times candidate split counts, and for the FP32 sums both tile
+shapes (two or four targets per thread), for given shapes on the device and publishes the
+fastest in the library's immutable table, which every later launch of
 that (precision, log2 targets, log2 stream length) bucket uses; ``step_shapes`` lists the
 three sums of one UVLM time step of a case (wake RHS, forces, free-wake convection,
 aero/uvlm.py:912-941, 961-983, 1023-1033).  ``save``/``load`` carry a table to another
@@ -49,8 +50,9 @@ def autotune(shapes, precision="mixed", kernel=None, r_cut=0.0, device=None):
     cms, hms = (C.c_double * k)(), (C.c_double * k)()
     _lib.call("fj_autotune_vind", prec, kern, float(r_cut), nt, ne, k, chosen, heur, cms, hms, ws.data_ptr(),
               ws.numel(), torch.cuda.current_stream(dev).cuda_stream)
-    return [{"n_targets": int(nt[i]), "n_elem": int(ne[i]), "split": chosen[i], "rule_split": heur[i],
-             "ms": cms[i], "rule_ms": hms[i]} for i in range(k)]
+    return [{"n_targets": int(nt[i]), "n_elem": int(ne[i]), "split": chosen[i] & 0xFFF,
+             "targets_per_thread": 4 if chosen[i] & 0x1000 else 2, "rule_split": heur[i], "ms": cms[i],
+             "rule_ms": hms[i]} for i in range(k)]
 
 
 def table() -> np.ndarray:

@@ -447,14 +447,18 @@ FJ_API int fj_tc_wait_selftest(int* d_err, float* d_scratch, fj_stream_t stream)
  * immutable table, by precision, log2 n_targets and log2 stream length, that every later
  * launch consults.  Per shape it reports the split chosen, the rule's split and both
  * times (ms); any of those arrays may be NULL.  precision: FJ_PREC_FP64 or
- * FJ_PREC_MIXED (the FP32 sums). */
+ * FJ_PREC_MIXED (the FP32 sums).  The FP32 sums are also tried with four targets per
+ * thread instead of two (the tile shape): chosen[i] is then the split plus 4096 when the
+ * four-target tile won. */
 FJ_API int fj_autotune_vind_workspace_size(int precision, const int64_t* n_targets, const int64_t* n_elem,
                                            int n_shapes, size_t* bytes);
 FJ_API int fj_autotune_vind(int precision, int kernel, double r_cut, const int64_t* n_targets,
                             const int64_t* n_elem, int n_shapes, int* chosen, int* heuristic, double* chosen_ms,
                             double* heuristic_ms, void* d_ws, size_t ws_bytes, fj_stream_t stream);
 /* The published table as int16 entries (fj_autotune_table_size of them; 0 = not tuned),
- * to save it and load it into another process; fj_autotune_set(NULL, 0) drops it. */
+ * to save it and load it into another process; fj_autotune_set(NULL, 0) drops it.  The
+ * first half is the FP64 sums' split counts (1..1024), the second the FP32 sums', each
+ * plus 4096 where four targets per thread won; fj_autotune_set refuses anything else. */
 FJ_API int fj_autotune_table_size(int* n_entries);
 FJ_API int fj_autotune_get(int16_t* entries, int n_entries);
 FJ_API int fj_autotune_set(const int16_t* entries, int n_entries);

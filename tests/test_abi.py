@@ -167,3 +167,24 @@ def test_jax_binding_is_import_guarded():
         assert f"FJ_API int {name}(" in header or f"FJ_API const char* {name}(" in header, name
     for sym in fj_jax._TARGETS.values():
         assert f"XLA_FFI_DEFINE_HANDLER_SYMBOL({sym}," in src
+
+
+def test_autotune_table_accepts_tiles_only_for_fp32():
+    """A tuned table entry is a split count (1..1024), plus 4096 for the four-target tile
+    in the FP32 half only; fj_autotune_set checks that on the host, with no GPU."""
+    import numpy as np
+
+    from flapjax_b200 import tuning
+
+    n = C.c_int()
+    _lib.call("fj_autotune_table_size", C.byref(n))
+    t = np.zeros(n.value, dtype=np.int16)
+    t[n.value // 2] = 8 | 0x1000
+    tuning.set_table(t)
+    assert tuning.table()[n.value // 2] == 8 | 0x1000
+    for bad_at, bad in ((0, 8 | 0x1000), (1, 1025), (n.value - 1, 0x1000)):
+        b = np.zeros_like(t)
+        b[bad_at] = bad
+        with pytest.raises(_lib.FjError):
+            tuning.set_table(b)
+    tuning.set_table(None)

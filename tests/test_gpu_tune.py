@@ -41,3 +41,36 @@ def test_tuned_splits_give_the_same_answer(cuda, precision, tol, tmp_path):
     tuning.load(p)
     assert np.array_equal(tuning.table(), t)
     tuning.set_table(None)
+
+
+def test_wide_tile_gives_the_same_answer(cuda):
+    """Four targets per thread (the tile the autotuner may pick for an FP32 sum) against
+    the default two: a table that asks for the wide tile and 8 splits on every FP32 shape
+    reproduces the default run within the mixed tolerance (1e-6), single-case and batched."""
+    from flapjax_b200 import tuning
+    from flapjax_b200.serving import BatchStepper
+
+    c = cases.wing_free(m=6, n=24, m_star=30, n_steps=4, seed=3)
+    tuning.set_table(None)
+    want = _solve(c, "mixed")
+    t = np.zeros_like(tuning.table())
+    half = t.size // 2  # the FP64 block first, then the FP32 block
+    t[half:] = 8 | 0x1000
+    tuning.set_table(t)
+    try:
+        got = _solve(c, "mixed")
+        uv, _ = device_uvlm(c, "mixed")
+        dc = uv.make_device_case(c.n_tstep)
+        uv.load_initial(dc, uv.solve_static())
+        dc.set_hg(c.hg_t, c.hg_dot_t)
+        dc.solve_dynamic(1, 2)
+        st = BatchStepper(2, cuda)
+        for i in range(2, c.n_tstep):
+            st.step([dc], [i], [True])
+        batched = uv._to_case(dc)
+        st.close()
+    finally:
+        tuning.set_table(None)
+    for case in (got, batched):
+        for a, b in zip(case.gamma_b, want.gamma_b):
+            assert rel_err(a, b) < 1e-6
