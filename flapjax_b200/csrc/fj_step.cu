@@ -1812,39 +1812,82 @@ static BatchItem step_item(const Plan& p, const fj_case_buffers* B, int k, bool 
 // *step_ctr, runs the step's kernels on the fixed table area and advances the counter.
 // The capture runs on a private stream (the legacy default stream cannot be captured);
 // the replays go to the caller's stream.
+//
+// The executable graph is kept for later calls on the same workspace: its kernels take
+// only workspace pointers and the host values of the step's launch signature, so a call
+// whose first step has the same signature replays it without a new capture.  A small
+// cache (least recently used out) bounds the graphs held.
+struct RangeGraph {
+    const void* tab = nullptr;
+    std::vector<int64_t> sig;
+    cudaGraphExec_t exec = nullptr;
+    int64_t kernels = 0;
+    uint64_t used = 0;
+};
+constexpr int kRangeGraphs = 16;
+static std::mutex g_rg_mu;
+static std::vector<RangeGraph> g_rg;
+static uint64_t g_rg_clock = 0;
+
 static int run_range_graph(const Plan& p, const fj_case_buffers* B, int g0, int g1, cudaStream_t s) {
     std::vector<char> h((size_t)(g1 - g0) * p.tab_bytes);
+    std::vector<int64_t> sig;
     for (int k = g0; k < g1; ++k) {
         std::vector<BatchItem> one(1, step_item(p, B, k, false));
-        FJ_TRY(run_steps(one, p.tab, p.tab_bytes, s, kStepBuild, h.data() + (size_t)(k - g0) * p.tab_bytes));
+        FJ_TRY(run_steps(one, p.tab, p.tab_bytes, s, kStepBuild, h.data() + (size_t)(k - g0) * p.tab_bytes,
+                         k == g0 ? &sig : nullptr));
     }
     FJ_TRY(upload(p.tab_all + (size_t)g0 * p.tab_bytes, h.data(), h.size(), s));
     FJ_TRY(upload(p.step_ctr, &g0, sizeof(int), s));
 
-    cudaStream_t cs = nullptr;
-    FJ_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-    cudaGraph_t graph = nullptr;
-    const int64_t launches0 = launch_count();
-    int st = cuda_status(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "step graph capture");
-    if (st == FJ_OK) {
-        k_select_table<<<32, 256, 0, cs>>>(p.tab_all, p.tab_bytes, p.step_ctr, p.tab); note_launch();
-        std::vector<BatchItem> one(1, step_item(p, B, g0, false));
-        st = run_steps(one, p.tab, p.tab_bytes, cs, kStepLaunch);
-        k_advance<<<1, 32, 0, cs>>>(p.step_ctr); note_launch();
-        const int st_end = cuda_status(cudaStreamEndCapture(cs, &graph), "step graph capture");
-        if (st == FJ_OK) st = st_end;
+    std::lock_guard<std::mutex> lk(g_rg_mu);
+    RangeGraph* rg = nullptr;
+    for (RangeGraph& r : g_rg)
+        if (r.tab == p.tab) rg = &r;
+    if (rg == nullptr || rg->sig != sig || rg->exec == nullptr) {
+        cudaStream_t cs = nullptr;
+        FJ_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaGraph_t graph = nullptr;
+        const int64_t launches0 = launch_count();
+        int st = cuda_status(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "step graph capture");
+        if (st == FJ_OK) {
+            k_select_table<<<32, 256, 0, cs>>>(p.tab_all, p.tab_bytes, p.step_ctr, p.tab); note_launch();
+            std::vector<BatchItem> one(1, step_item(p, B, g0, false));
+            st = run_steps(one, p.tab, p.tab_bytes, cs, kStepLaunch);
+            k_advance<<<1, 32, 0, cs>>>(p.step_ctr); note_launch();
+            const int st_end = cuda_status(cudaStreamEndCapture(cs, &graph), "step graph capture");
+            if (st == FJ_OK) st = st_end;
+        }
+        cudaStreamDestroy(cs);
+        cudaGraphExec_t exec = nullptr;
+        if (st == FJ_OK) st = cuda_status(cudaGraphInstantiate(&exec, graph, 0), "step graph instantiate");
+        if (graph) cudaGraphDestroy(graph);
+        if (st != FJ_OK) return st;
+        if (rg == nullptr) {
+            if ((int)g_rg.size() < kRangeGraphs) {
+                g_rg.emplace_back();
+                rg = &g_rg.back();
+            } else {  // least recently used out
+                rg = &g_rg[0];
+                for (RangeGraph& r : g_rg)
+                    if (r.used < rg->used) rg = &r;
+            }
+        }
+        if (rg->exec) cudaGraphExecDestroy(rg->exec);
+        rg->tab = p.tab;
+        rg->sig.swap(sig);
+        rg->exec = exec;
+        // the capture counted the step's kernels once; the first replay runs them
+        rg->kernels = launch_count() - launches0;
+        note_launch((int)(-rg->kernels));
     }
-    const int64_t per_step = launch_count() - launches0;
-    cudaGraphExec_t exec = nullptr;
-    if (st == FJ_OK) st = cuda_status(cudaGraphInstantiate(&exec, graph, 0), "step graph instantiate");
-    for (int k = g0; k < g1 && st == FJ_OK; ++k) st = cuda_status(cudaGraphLaunch(exec, s), "step graph launch");
-    if (st == FJ_OK) {
-        note_launch((int)(per_step * (g1 - g0 - 1)));  // kernels executed by the replays beyond the capture
-        st = cuda_status(cudaStreamSynchronize(s), "step graph replay");
+    rg->used = ++g_rg_clock;
+    int st = FJ_OK;
+    for (int k = g0; k < g1 && st == FJ_OK; ++k) {
+        st = cuda_status(cudaGraphLaunch(rg->exec, s), "step graph launch");
+        note_launch((int)rg->kernels);
     }
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    cudaStreamDestroy(cs);
+    if (st == FJ_OK) st = cuda_status(cudaStreamSynchronize(s), "step graph replay");
     return st;
 }
 

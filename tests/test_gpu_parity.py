@@ -392,3 +392,32 @@ def test_graph_replayed_steps_match_direct_launches(cuda, precision):
     assert np.array_equal(a["t"], b["t"]) and np.array_equal(a["force_total"], b["force_total"])
     # the launch counter counts the kernels the replays executed (plus the graph's two)
     assert nb >= na
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_cached_step_graph_across_calls(cuda, precision):
+    """Consecutive calls on one workspace replay the step graph captured by the first
+    (the chunked calls of a streaming caller); the slots equal one direct-launch run bit
+    for bit, and a second case on another workspace gets its own graph."""
+    import torch
+
+    c = cases.wing_free(m=4, n=10, m_star=12, n_steps=13)
+    got = []
+    for chunks in ([(1, c.n_tstep)], [(1, 2), (2, 5), (5, 9), (9, c.n_tstep)]):
+        for graph in ((False,) if len(chunks) == 1 else (True,)):
+            uv, _ = device_uvlm(c, precision)
+            dc = uv.make_device_case(c.n_tstep)
+            uv.load_initial(dc, uv.solve_static())
+            dc.set_hg(c.hg_t, c.hg_dot_t)
+            other = uv.make_device_case(c.n_tstep)  # interleaved calls on another workspace
+            uv.load_initial(other, uv.solve_static())
+            other.set_hg(c.hg_t, c.hg_dot_t)
+            for i0, i1 in chunks:
+                dc.solve_dynamic(i0, i1, reuse_factors=i0 > 1, graph=graph)
+                other.solve_dynamic(i0, i1, reuse_factors=i0 > 1, graph=graph)
+            torch.cuda.synchronize()
+            got.append((dc.host_arrays(), other.host_arrays()))
+    (a, _), (b, b2) = got
+    for f in ("gamma_b", "gamma_w", "zeta_w", "f_steady", "f_unsteady", "gamma_b_dot", "alpha"):
+        assert np.array_equal(a[f], b[f]), f
+        assert np.array_equal(b[f], b2[f]), f
