@@ -499,6 +499,7 @@ def main():
                "steps_per_call": 8}
         del dce
 
+    torch.cuda.empty_cache()  # the serving budget is half of the free memory: return the cached blocks first
     serving = serving_bench(args, torch) if args.serving_cases > 0 else None
     # below capacity (about a sixth of what one GPU serves), so that latency is the step's
     # and not the queue's
