@@ -197,6 +197,9 @@ _SIGS = {
     "fj_solve_mixed": (C.c_int, [_P, C.c_int, _P, _P, C.c_int, _P, _P, C.c_size_t, _P]),
     "fj_gemm_tf32": (C.c_int, [_P, C.c_int, _P, C.c_int, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
                                C.c_float, C.c_int, _P, _P]),
+    "fj_gemm_tf32_scratch_floats": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_size_t)]),
+    "fj_gemm_tf32_tma": (C.c_int, [_P, C.c_int, _P, C.c_int, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                   C.c_float, C.c_int, _P, C.c_size_t, _P, _P]),
     "fj_autotune_vind_workspace_size": (C.c_int, [C.c_int, _P, _P, C.c_int, C.POINTER(C.c_size_t)]),
     "fj_autotune_vind": (C.c_int, [C.c_int, C.c_int, C.c_double, _P, _P, C.c_int, _P, _P, _P, _P, _P, C.c_size_t,
                                    _P]),

@@ -13,6 +13,9 @@
 #include <climits>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
+
+#include <cooperative_groups.h>
 
 #include "fj_lu.cuh"
 #include "fj_tc.cuh"
@@ -648,8 +651,417 @@ int lu_inverse32(const float* lu, int n, const int32_t* piv, float* x, cudaStrea
 // Every product is a tensor-core GEMM; 2 n^3 flop in all.
 constexpr int kTcBlk = 128;
 
-size_t tc_tri_floats(int n) {
+// tri: the 2 x nblk inverted diagonal blocks (L's, then U's), then the TMA products'
+// operand-split scratch, enough for the largest product (m, n <= nblk x 128, K = 128),
+// then the row-swap list of one outer panel (kSwapInts ints).
+constexpr int kSwapInts = 1 + 2 * 2 * kTcBlk;  // count, then (destination, source) row pairs
+
+static size_t tc_inv_floats(int n) {
     return (size_t)2 * ((n + kTcBlk - 1) / kTcBlk) * kTcBlk * kTcBlk;
+}
+
+static size_t tc_scratch_floats(int n) {
+    const int np = (n + kTcBlk - 1) / kTcBlk * kTcBlk;
+    return tc_gemm_scratch_floats(np, np, kTcBlk, 3);
+}
+
+size_t tc_tri_floats(int n) {
+    return tc_inv_floats(n) + tc_scratch_floats(n) + (size_t)kSwapInts;
+}
+
+// ---------------------------------------------------------------------------------
+// One 128-column outer panel, (n - k) rows, factored by a single thread-block cluster
+// of 16-warp CTAs (up to 16 CTAs of 8-row warps where the device allows that cluster
+// size, else up to 8 CTAs of 16-row warps): getrf's partial pivoting and rank-1 updates
+// column by column, with the panel in registers.  Lanes are columns: lane L of a warp
+// holds columns L, L + 32, L + 64, L + 96 of the warp's RPW rows; CTA q holds panel rows
+// 16 RPW q .. in order over its warps.  The column loop runs in four groups of 32
+// (unrolled), so that a column's register is a compile-time index.  Per column j:
+//   a. every warp gathers column j of its rows (lane i takes row i from lane j % 32),
+//      finds the first maximum of |a(r, j)| over rows r >= j (keys are the magnitude's
+//      bits + 1, so one redux.sync orders them; NaN is never a candidate; the lowest
+//      lane, i.e. row, wins a tie) and copies the winning row into its candidate slot;
+//      the warp holding row j copies row j;
+//   b. one CTA barrier; four warps take the CTA's first maximum over its warps and push
+//      that row, its key, index and origin into every CTA's slot q (distributed shared
+//      memory stores); in CTA 0 four more warps push row j the same way;
+//   c. one cluster barrier;
+//   d. every warp reads the nc slot keys from its own shared memory and takes the first
+//      maximum (lowest CTA: the lowest row, getrf's tie rule; no candidate keeps the
+//      diagonal); rows j and p trade places (the pivot row and row j from the local
+//      slots); the rows below j are scaled as getrf scales them (by the reciprocal of the
+//      pivot when its magnitude is at least the smallest normal, else by division) and
+//      updated.
+// All slots alternate between two buffers with the column's parity: a buffer is written
+// again only after the next column's cluster barrier, which every CTA reaches after its
+// reads of it.  Lane i < RPW of a warp carries the original index of the warp's row i;
+// at the end the moved rows are listed as (destination, source) global row pairs, at
+// most 2 x 128, for lu_swap_rows_kernel.  Every thread passes every barrier (the loop
+// bounds are uniform over the cluster), so no wait depends on data.
+namespace cg = cooperative_groups;
+
+constexpr int kPcThreads = 512;
+constexpr int kPcWarps = kPcThreads / 32;
+constexpr int kPcMaxCtas = 16;
+
+// Candidate key: the magnitude's bits + 1, ordered as the magnitudes; 0 = no candidate
+// (inactive, or NaN, which never wins a getrf pivot search).
+__device__ __forceinline__ uint32_t pivot_key(float x) {
+    const float ax = fabsf(x);
+    return ax == ax ? __float_as_uint(ax) + 1u : 0u;
+}
+
+// Row `i` (a runtime index) of a thread's rows, as the 4 columns this lane holds.
+template <int RPW>
+__device__ __forceinline__ void pick_row(const float (&v)[RPW][4], int i, float (&out)[4]) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) out[c] = v[0][c];
+#pragma unroll
+    for (int r = 1; r < RPW; ++r)
+        if (r == i) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) out[c] = v[r][c];
+        }
+}
+
+template <int RPW>
+__device__ __forceinline__ void put_row(float (&v)[RPW][4], int i, const float (&in)[4]) {
+#pragma unroll
+    for (int r = 0; r < RPW; ++r)
+        if (r == i) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) v[r][c] = in[c];
+        }
+}
+
+// Rank-1 update of the rows below j with multipliers column(j) * s (mul) or / s (div).
+template <int RPW, int G, bool kDiv>
+__device__ __forceinline__ void panel_update(float (&v)[RPW][4], int rbase, int rows, int j, int jj, int lane,
+                                             float s, const float (&pc)[4]) {
+#pragma unroll
+    for (int i = 0; i < RPW; ++i) {
+        const int r = rbase + i;
+        if (r > j && r < rows) {  // uniform over the warp
+            float l = kDiv ? v[i][G] / s : v[i][G] * s;
+            l = __shfl_sync(0xffffffffu, l, jj);  // lane jj's is the multiplier
+            if (lane == jj) v[i][G] = l;
+#pragma unroll
+            for (int c = G + 1; c < 4; ++c) v[i][c] -= l * pc[c];
+            if (lane > jj) v[i][G] -= l * pc[G];
+        }
+    }
+}
+
+// The panel's shared state (static shared memory of lu_panel_cluster_kernel).
+struct PanelShared {
+    float cand[2][kPcWarps][kTcBlk];  // this CTA's warp candidates
+    uint32_t wkey[2][kPcWarps];
+    int wrow[2][kPcWarps], wsrc[2][kPcWarps];
+    float rowj_loc[2][kTcBlk];                // row j, in CTA 0
+    float slot[2][kPcMaxCtas][kTcBlk];        // every CTA's candidate, pushed by that CTA
+    uint32_t slot_key[2][kPcMaxCtas];
+    int slot_row[2][kPcMaxCtas], slot_src[2][kPcMaxCtas];
+    float rowj[2][kTcBlk];                    // row j, pushed by CTA 0
+    int rowj_src[2];
+    int rowj_src_loc[2];
+    int piv[kTcBlk];  // written out at the end: no global store inside the column loop
+    int info;
+    int wcnt[kPcWarps], cnt, off;
+};
+
+template <int RPW, int G>
+__device__ __forceinline__ void panel_columns(float (&v)[RPW][4], int& orig, int k, int kb, int rows, int q, int nc,
+                                              int tid, cg::cluster_group& cl, PanelShared& S) {
+    const int lane = tid & 31, warp = tid >> 5;
+    const int rbase = (q * kPcWarps + warp) * RPW;
+    const unsigned full = 0xffffffffu;
+    const int jend = min(kb, 32 * G + 32);
+#pragma unroll 1
+    for (int j = 32 * G; j < jend; ++j) {
+        const int jj = j & 31, par = j & 1;
+        // a. the warp's candidate: lane i < RPW takes column j of row i
+        float xj = 0.f;
+#pragma unroll
+        for (int i = 0; i < RPW; ++i) {
+            const float t = __shfl_sync(full, v[i][G], jj);
+            if (lane == i) xj = t;
+        }
+        const int r = rbase + lane;
+        const uint32_t key = (lane < RPW && r >= j && r < rows) ? pivot_key(xj) : 0u;
+        const uint32_t wmax = __reduce_max_sync(full, key);
+        const unsigned hit = __ballot_sync(full, wmax != 0u && key == wmax);
+        const int bi = hit ? __ffs(hit) - 1 : 0;
+        const int bsrc = __shfl_sync(full, orig, bi);
+        if (hit != 0u) {
+            float row[4];
+            pick_row<RPW>(v, bi, row);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) S.cand[par][warp][lane + 32 * c] = row[c];
+        }
+        if (lane == 0) {
+            S.wkey[par][warp] = wmax;
+            S.wrow[par][warp] = rbase + bi;
+            S.wsrc[par][warp] = bsrc;
+        }
+        const bool holds_j = j >= rbase && j < rbase + RPW;  // CTA 0 (its rows cover the 128 columns)
+        const int ij = j - rbase;
+        const int jsrc = __shfl_sync(full, orig, holds_j ? ij : 0);
+        if (holds_j) {
+            float row[4];
+            pick_row<RPW>(v, ij, row);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) S.rowj_loc[par][lane + 32 * c] = row[c];
+            if (lane == 0) S.rowj_src_loc[par] = jsrc;
+        }
+        __syncthreads();
+        // b. push: warps 0-3 the CTA's candidate, warps 4-7 of CTA 0 row j; thread t
+        //    stores float4 t % 32 into CTAs t / 32 % 4, + 4, + 8, + 12
+        if (warp < 8) {
+            const int t = tid & 127, f = t & 31, c0 = t >> 5;
+            if (warp < 4) {
+                const uint32_t kw = lane < kPcWarps ? S.wkey[par][lane] : 0u;
+                const uint32_t m = __reduce_max_sync(full, kw);
+                const unsigned h = __ballot_sync(full, m != 0u && kw == m);
+                const int w = h ? __ffs(h) - 1 : 0;
+                const float4 val = reinterpret_cast<const float4*>(S.cand[par][w])[f];
+                const int prow_r = S.wrow[par][w], prow_s = S.wsrc[par][w];
+#pragma unroll
+                for (int u = 0; u < kPcMaxCtas / 4; ++u) {
+                    const int c = c0 + 4 * u;
+                    if (c < nc) {
+                        PanelShared* R = cl.map_shared_rank(&S, c);
+                        reinterpret_cast<float4*>(R->slot[par][q])[f] = val;
+                        if (f == 0) {
+                            R->slot_key[par][q] = m;
+                            R->slot_row[par][q] = prow_r;
+                            R->slot_src[par][q] = prow_s;
+                        }
+                    }
+                }
+            } else if (q == 0) {
+                const float4 val = reinterpret_cast<const float4*>(S.rowj_loc[par])[f];
+                const int js = S.rowj_src_loc[par];
+#pragma unroll
+                for (int u = 0; u < kPcMaxCtas / 4; ++u) {
+                    const int c = c0 + 4 * u;
+                    if (c < nc) {
+                        PanelShared* R = cl.map_shared_rank(&S, c);
+                        reinterpret_cast<float4*>(R->rowj[par])[f] = val;
+                        if (f == 0) R->rowj_src[par] = js;
+                    }
+                }
+            }
+        }
+        cl.sync();
+        // d. the cluster's pivot, from this CTA's own slots (every warp)
+        const uint32_t ks = lane < nc ? S.slot_key[par][lane] : 0u;
+        const uint32_t m = __reduce_max_sync(full, ks);
+        const unsigned h = __ballot_sync(full, m != 0u && ks == m);
+        const int o = h ? __ffs(h) - 1 : 0;  // the lowest CTA with the maximum
+        const float* prow = m != 0u ? S.slot[par][o] : S.rowj[par];
+        const int p = m != 0u ? S.slot_row[par][o] : j;  // no candidate: row j stays the pivot row
+        if (p != j) {
+            if (holds_j) {  // row j takes the pivot row
+                float row[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) row[c] = prow[lane + 32 * c];
+                put_row<RPW>(v, ij, row);
+                if (lane == ij) orig = S.slot_src[par][o];
+            }
+            if (p >= rbase && p < rbase + RPW) {  // row p takes row j
+                float row[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) row[c] = S.rowj[par][lane + 32 * c];
+                put_row<RPW>(v, p - rbase, row);
+                if (lane == p - rbase) orig = S.rowj_src[par];
+            }
+        }
+        const float pv = prow[j];
+        if (tid == 0) {
+            S.piv[j] = k + p;
+            if (pv == 0.f && S.info == 0) S.info = k + j + 1;
+        }
+        if (pv != 0.f) {
+            float pc[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) pc[c] = prow[lane + 32 * c];
+            if (fabsf(pv) >= 1.17549435e-38f)  // FLT_MIN: getrf's sfmin test
+                panel_update<RPW, G, false>(v, rbase, rows, j, jj, lane, 1.0f / pv, pc);
+            else
+                panel_update<RPW, G, true>(v, rbase, rows, j, jj, lane, pv, pc);
+        }
+    }
+}
+
+template <int RPW>
+__global__ void __launch_bounds__(kPcThreads, 1)
+    lu_panel_cluster_kernel(float* __restrict__ a, int n, int k, int kb, int32_t* __restrict__ piv,
+                            int* __restrict__ info, int* __restrict__ swaps) {
+    cg::cluster_group cl = cg::this_cluster();
+    __shared__ __align__(16) PanelShared S;
+    const int q = (int)cl.block_rank(), nc = (int)cl.num_blocks();
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int rows = n - k;
+    const int rbase = (q * kPcWarps + warp) * RPW;  // the warp's first panel row
+    const unsigned full = 0xffffffffu;
+    if (tid == 0) S.info = 0;
+
+    float v[RPW][4];
+#pragma unroll
+    for (int i = 0; i < RPW; ++i) {
+        const bool has = rbase + i < rows;
+        const float* src = a + (int64_t)(k + (has ? rbase + i : 0)) * n + k + lane;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) v[i][c] = (has && lane + 32 * c < kb) ? src[32 * c] : 0.f;
+    }
+    int orig = rbase + lane;  // lanes < RPW: original panel row of the warp's row `lane`
+    cl.sync();                // every CTA of the cluster runs before any shared memory is written remotely
+
+    panel_columns<RPW, 0>(v, orig, k, kb, rows, q, nc, tid, cl, S);
+    panel_columns<RPW, 1>(v, orig, k, kb, rows, q, nc, tid, cl, S);
+    panel_columns<RPW, 2>(v, orig, k, kb, rows, q, nc, tid, cl, S);
+    panel_columns<RPW, 3>(v, orig, k, kb, rows, q, nc, tid, cl, S);
+#pragma unroll
+    for (int i = 0; i < RPW; ++i) {
+        if (rbase + i < rows) {
+            float* dst = a + (int64_t)(k + rbase + i) * n + k + lane;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (lane + 32 * c < kb) dst[32 * c] = v[i][c];
+        }
+    }
+    // the moved rows, in row order: (destination, source) global rows
+    const bool moved = lane < RPW && rbase + lane < rows && orig != rbase + lane;
+    const unsigned mb = __ballot_sync(full, moved);
+    if (lane == 0) S.wcnt[warp] = __popc(mb);
+    __syncthreads();  // also orders the last column's piv and info before their reads
+    if (q == 0) {
+        for (int j = tid; j < kb; j += kPcThreads) piv[k + j] = S.piv[j];
+        if (tid == 0 && S.info != 0 && *info == 0) *info = S.info;
+    }
+    if (warp == 0) {
+        const int cw = lane < kPcWarps ? S.wcnt[lane] : 0;
+        int inc = cw;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(full, inc, off);
+            if (lane >= off) inc += y;
+        }
+        if (lane < kPcWarps) S.wcnt[lane] = inc - cw;  // exclusive prefix over the warps
+        if (lane == 31) S.cnt = inc;
+    }
+    cl.sync();  // every CTA's count is published
+    if (tid == 0) {
+        int off = 0;
+        for (int c = 0; c < q; ++c) off += cl.map_shared_rank(&S, c)->cnt;
+        S.off = off;
+        if (q == nc - 1) swaps[0] = off + S.cnt;
+    }
+    __syncthreads();
+    if (moved) {
+        const int e = S.off + S.wcnt[warp] + __popc(mb & ((1u << lane) - 1u));
+        swaps[1 + 2 * e] = k + rbase + lane;
+        swaps[2 + 2 * e] = k + orig;
+    }
+    cl.sync();  // no CTA exits while another may still read its shared memory
+}
+
+// The outer panel's row permutation (lu_panel_cluster_kernel's list) for every column
+// outside the panel: a CTA takes 32 columns, loads every listed source row's values into
+// shared memory, then stores them to their destinations (all loads before any store, so
+// the permutation's cycles need no order).
+__global__ void __launch_bounds__(256) lu_swap_rows_kernel(float* __restrict__ a, int n, int k, int kb,
+                                                           const int* __restrict__ swaps) {
+    __shared__ int s_dst[2 * kTcBlk], s_src[2 * kTcBlk];
+    __shared__ float tile[2 * kTcBlk][33];
+    const int cnt = min(swaps[0], 2 * kTcBlk);
+    for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+        s_dst[e] = swaps[1 + 2 * e];
+        s_src[e] = swaps[2 + 2 * e];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int c = blockIdx.x * 32 + lane;
+    const bool col = c < n && (c < k || c >= k + kb);
+    for (int e = warp; e < cnt; e += 8)
+        if (col) tile[e][lane] = a[(int64_t)s_src[e] * n + c];
+    __syncthreads();
+    for (int e = warp; e < cnt; e += 8)
+        if (col) a[(int64_t)s_dst[e] * n + c] = tile[e][lane];
+}
+
+// The largest cluster of lu_panel_cluster_kernel CTAs the device runs (16 where the
+// non-portable size is allowed, else 8; 0 if none), checked once.
+static int cluster_panel_max() {
+    static std::once_flag once;
+    static int best = 0;
+    std::call_once(once, [] {
+        for (int size : {16, 8}) {
+            const void* fn = size == 16 ? (const void*)lu_panel_cluster_kernel<8> : (const void*)lu_panel_cluster_kernel<16>;
+            if (size == 16 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)size);
+            cfg.blockDim = dim3(kPcThreads);
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = (unsigned)size;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            int clusters = 0;
+            const cudaError_t e = size == 16 ? cudaOccupancyMaxActiveClusters(&clusters, lu_panel_cluster_kernel<8>, &cfg)
+                                             : cudaOccupancyMaxActiveClusters(&clusters, lu_panel_cluster_kernel<16>, &cfg);
+            cudaGetLastError();
+            if (e == cudaSuccess && clusters > 0) {
+                best = size;
+                break;
+            }
+        }
+    });
+    return best;
+}
+
+// Rows of the outer panel one cluster takes: 16 CTAs of 8-row warps, or 8 CTAs of
+// 16-row warps.
+static int cluster_panel_rows() {
+    const int m = cluster_panel_max();
+    return m == 16 ? 16 * 8 * kPcWarps : m == 8 ? 8 * 16 * kPcWarps : 0;
+}
+
+static int launch_panel_cluster(float* a, int n, int k, int kb, int32_t* piv, int* info, int* swaps,
+                                cudaStream_t s) {
+    const bool small = cluster_panel_max() == 16;  // 8-row warps
+    const int per_cta = (small ? 8 : 16) * kPcWarps;
+    const int nc = (n - k + per_cta - 1) / per_cta;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)nc);
+    cfg.blockDim = dim3(kPcThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)nc;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    if (small) FJ_CUDA(cudaLaunchKernelEx(&cfg, lu_panel_cluster_kernel<8>, a, n, k, kb, piv, info, swaps));
+    else FJ_CUDA(cudaLaunchKernelEx(&cfg, lu_panel_cluster_kernel<16>, a, n, k, kb, piv, info, swaps));
+    note_launch();
+    lu_swap_rows_kernel<<<(unsigned)((n + 31) / 32), 256, 0, s>>>(a, n, k, kb, swaps);
+    note_launch();
+    return FJ_OK;
+}
+
+// The factorisation's and the inverse's products: the TMA-fed tensor-core GEMM, its
+// operand split in the scratch that follows the diagonal-block inverses.
+static int tc_mul(const float* a, int lda, const float* b, int ldb, float* c, int ldc, int m, int n, int k,
+                  float alpha, float beta, int passes, float* tri, int nn, int* d_err, cudaStream_t s) {
+    return tc_gemm_tf32_tma(a, lda, b, ldb, c, ldc, m, n, k, alpha, beta, passes, tri + tc_inv_floats(nn),
+                            tc_scratch_floats(nn), d_err, s);
 }
 
 template <int NB>
@@ -663,9 +1075,14 @@ static int lu_factor32_tc_impl(float* a, int n, int32_t* piv, int* d_info, int* 
     FJ_TRY(allow_dynamic_smem((const void*)lu_panel_reg_kernel<float, NB, 1>, smem));
     FJ_TRY(allow_dynamic_smem((const void*)lu_panel_reg_kernel<float, NB, 2>, smem));
     FJ_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int), s));
+    int* swaps = reinterpret_cast<int*>(tri_l + tc_inv_floats(n) + tc_scratch_floats(n));
+    const int cluster_rows = cluster_panel_rows();
     for (int k = 0; k < n; k += kTcBlk) {
         const int kb = min(kTcBlk, n - k), ke = k + kb;
-        for (int j = k; j < ke; j += NB) {
+        if (n - k <= cluster_rows) {
+            FJ_TRY(launch_panel_cluster(a, n, k, kb, piv, d_info, swaps, s));
+        } else {
+          for (int j = k; j < ke; j += NB) {
             const int nb = min(NB, n - j);
             launch_panel<float, NB>(a, n, j, piv, d_info, nullptr, s);
             if (n > nb) {
@@ -677,6 +1094,7 @@ static int lu_factor32_tc_impl(float* a, int n, int32_t* piv, int* d_info, int* 
                 lu_update_kernel<float, NB><<<dim3((cols + 63) / 64, (rows + 63) / 64), 256, 0, s>>>(a, n, j, ke, nullptr);
                 note_launch();
             }
+          }
         }
         const int b = k / kTcBlk;
         float* linv = tri_l + (size_t)b * kTcBlk * kTcBlk;
@@ -684,9 +1102,9 @@ static int lu_factor32_tc_impl(float* a, int n, int32_t* piv, int* d_info, int* 
         const int rest = n - ke;
         if (rest > 0) {
             float* a12 = a + (int64_t)k * n + ke;
-            FJ_TRY(tc_gemm_tf32(linv, kTcBlk, a12, n, a12, n, kb, rest, kb, 1.0f, 0.0f, passes, d_err, s));
-            FJ_TRY(tc_gemm_tf32(a + (int64_t)ke * n + k, n, a12, n, a + (int64_t)ke * n + ke, n, rest, rest, kb,
-                                -1.0f, 1.0f, passes, d_err, s));
+            FJ_TRY(tc_mul(linv, kTcBlk, a12, n, a12, n, kb, rest, kb, 1.0f, 0.0f, passes, tri_l, n, d_err, s));
+            FJ_TRY(tc_mul(a + (int64_t)ke * n + k, n, a12, n, a + (int64_t)ke * n + ke, n, rest, rest, kb, -1.0f, 1.0f,
+                          passes, tri_l, n, d_err, s));
         }
     }
     FJ_LAUNCH_CHECK("lu_factor32_tc");
@@ -737,19 +1155,18 @@ int lu_inverse32_tc(const float* lu, int n, const int32_t* piv, float* x, float*
     for (int b = 0; b < nblk; ++b) {  // forward: unit lower
         const int i0 = b * kTcBlk, ib = min(kTcBlk, n - i0), below = n - i0 - ib;
         float* yi = x + (int64_t)i0 * n;
-        FJ_TRY(tc_gemm_tf32(tri_l + (size_t)b * kTcBlk * kTcBlk, kTcBlk, yi, n, yi, n, ib, n, ib, 1.0f, 0.0f, passes,
-                            d_err, s));
+        FJ_TRY(tc_mul(tri_l + (size_t)b * kTcBlk * kTcBlk, kTcBlk, yi, n, yi, n, ib, n, ib, 1.0f, 0.0f, passes, tri,
+                      n, d_err, s));
         if (below > 0)
-            FJ_TRY(tc_gemm_tf32(lu + (int64_t)(i0 + ib) * n + i0, n, yi, n, yi + (int64_t)ib * n, n, below, n, ib,
-                                -1.0f, 1.0f, passes, d_err, s));
+            FJ_TRY(tc_mul(lu + (int64_t)(i0 + ib) * n + i0, n, yi, n, yi + (int64_t)ib * n, n, below, n, ib, -1.0f,
+                          1.0f, passes, tri, n, d_err, s));
     }
     for (int b = nblk - 1; b >= 0; --b) {  // backward: upper
         const int i0 = b * kTcBlk, ib = min(kTcBlk, n - i0);
         float* yi = x + (int64_t)i0 * n;
-        FJ_TRY(tc_gemm_tf32(tri_u + (size_t)b * kTcBlk * kTcBlk, kTcBlk, yi, n, yi, n, ib, n, ib, 1.0f, 0.0f, passes,
-                            d_err, s));
-        if (i0 > 0)
-            FJ_TRY(tc_gemm_tf32(lu + i0, n, yi, n, x, n, i0, n, ib, -1.0f, 1.0f, passes, d_err, s));
+        FJ_TRY(tc_mul(tri_u + (size_t)b * kTcBlk * kTcBlk, kTcBlk, yi, n, yi, n, ib, n, ib, 1.0f, 0.0f, passes, tri,
+                      n, d_err, s));
+        if (i0 > 0) FJ_TRY(tc_mul(lu + i0, n, yi, n, x, n, i0, n, ib, -1.0f, 1.0f, passes, tri, n, d_err, s));
     }
     return FJ_OK;
 }

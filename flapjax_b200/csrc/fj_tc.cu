@@ -17,6 +17,11 @@
 // epilogue.  Every wait is bounded (about one second); on expiry the CTA records the
 // failure in *err, drains its MMAs with a second bounded wait, frees its tensor memory
 // and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
 #include "fj_tc.cuh"
 
 namespace fj {
@@ -353,6 +358,253 @@ __global__ void __launch_bounds__(512) tri_inv_kernel(const float* __restrict__ 
     }
 }
 
+// ---------------------------------------------------------------------------------
+// TMA-fed form, for the products of the factorisation.  The operands are first split
+// into TF32 hi (and lo) copies, A as (m x kp) and B transposed as (n x kp), K contiguous
+// and padded to whole 32-float slabs (tc_split_*_kernel), so that every slab is a
+// 128-row x 128-byte box a TMA load brings in already in the 128-byte-swizzled K-major
+// layout the MMA descriptors name.  Roles, 4 warps: lane 0 of warp 0 loads (cp.async.bulk
+// .tensor, no multicast) into a ring of kTmaStages slab stages, each completing a "full"
+// mbarrier by its transaction bytes; lane 0 of warp 1 waits on "full", issues the slab's
+// MMAs and commits them to the stage's "empty" mbarrier, which frees the stage for the
+// producer; after the last slab it commits to "done".  All eight warps read their share
+// of C into registers before the main loop (beta != 0), wait on "done", and write the
+// tile (TMEM -> registers -> a warp's shared-memory square -> C, coalesced).
+// Every wait is bounded (about one second); on expiry the CTA records the failure in
+// *err, waits (bounded) for the loads it issued, frees its tensor memory and returns
+// without writing C.
+constexpr int kTmaThreads = 256;
+constexpr int kTmaStages = 3;
+constexpr size_t kTmaSmem = (size_t)kTmaStages * kStageBytes + 1024;
+
+__device__ __forceinline__ void bar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void bar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// One box of a 2D tensor map (x = element column, y = row) into shared memory; the load
+// completes its bytes on *bar.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__global__ void __launch_bounds__(kTmaThreads, 1)
+    tc_gemm_tma_kernel(const __grid_constant__ CUtensorMap ta_hi, const __grid_constant__ CUtensorMap ta_lo,
+                       const __grid_constant__ CUtensorMap tb_hi, const __grid_constant__ CUtensorMap tb_lo,
+                       float* c, int ldc, int m, int n, int kp, float alpha, float beta, int passes,
+                       int* __restrict__ err) {
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[kTmaStages], empty[kTmaStages], done;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_fail, s_loaded, s_used;
+    unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+    const bool split = passes == 3;
+    const uint32_t stage_tx = (split ? 4u : 2u) * (uint32_t)kSlabBytes;
+    const int n_slab = kp / kBK;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < kTmaStages; ++st) {
+            bar_init(&full[st], 1);
+            bar_init(&empty[st], 1);
+        }
+        bar_init(&done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_fail = 0;
+        s_loaded = 0;
+        s_used = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    // this thread's C values for the epilogue: rows m0 + 32 (w%4) + r, columns
+    // n0 + 64 (w/4) + 32 cc + lane; the loads fly while the tile is computed
+    const int q = warp & 3, hc = warp >> 2;
+    float cpre[2][32];
+    if (beta != 0.0f) {
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+            const int col = n0 + 64 * hc + 32 * cc + lane;
+#pragma unroll
+            for (int r = 0; r < 32; ++r) {
+                const int row = m0 + 32 * q + r;
+                cpre[cc][r] = (row < m && col < n) ? c[(int64_t)row * ldc + col] : 0.0f;
+            }
+        }
+    }
+
+    if (warp == 0 && lane == 0) {  // producer
+        int loaded = 0;
+        for (int ks = 0; ks < n_slab; ++ks) {
+            const int st = ks % kTmaStages;
+            if (ks >= kTmaStages && !bar_wait(&empty[st], (uint32_t)(((ks - kTmaStages) / kTmaStages) & 1))) {
+                s_fail = 1;
+                break;
+            }
+            unsigned char* base = smem + st * kStageBytes;
+            bar_expect_tx(&full[st], stage_tx);
+            tma_load_2d(base, &ta_hi, ks * kBK, m0, &full[st]);
+            tma_load_2d(base + 2 * kSlabBytes, &tb_hi, ks * kBK, n0, &full[st]);
+            if (split) {
+                tma_load_2d(base + kSlabBytes, &ta_lo, ks * kBK, m0, &full[st]);
+                tma_load_2d(base + 3 * kSlabBytes, &tb_lo, ks * kBK, n0, &full[st]);
+            }
+            loaded = ks + 1;
+        }
+        s_loaded = loaded;
+    } else if (warp == 1 && lane == 0) {  // MMA issuer
+        int used = 0;
+        for (int ks = 0; ks < n_slab; ++ks) {
+            const int st = ks % kTmaStages;
+            if (!bar_wait(&full[st], (uint32_t)((ks / kTmaStages) & 1))) {
+                s_fail = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            unsigned char* base = smem + st * kStageBytes;
+            const uint32_t sa = smem_u32(base), sb = smem_u32(base + 2 * kSlabBytes);
+#pragma unroll
+            for (int kk = 0; kk < kBK / 8; ++kk) {
+                const uint32_t step = (uint32_t)kk * 32u;
+                const uint64_t ah = sw128_desc(sa + step), bh = sw128_desc(sb + step);
+                mma_tf32(tmem, ah, bh, (ks > 0 || kk > 0) ? 1u : 0u);
+                if (split) {
+                    mma_tf32(tmem, ah, sw128_desc(sb + kSlabBytes + step), 1u);
+                    mma_tf32(tmem, sw128_desc(sa + kSlabBytes + step), bh, 1u);
+                }
+            }
+            mma_commit(&empty[st]);
+            used = ks + 1;
+        }
+        mma_commit(&done);  // arrives once every MMA issued above has completed
+        s_used = used;
+    }
+    const bool w = bar_wait(&done, 0u);
+    const bool all = __syncthreads_and(w) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const bool ok = all && s_fail == 0 && s_used == n_slab;
+    if (ok) {
+        // warp w reads TMEM lanes 32 (w%4).. (tile rows) and columns 64 (w/4)..+63
+        float* sq = reinterpret_cast<float*>(smem) + warp * (32 * 33);
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+            const int col0 = 64 * hc + 32 * cc;
+            uint32_t v[32];
+            const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)col0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                  "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                  "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+                  "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                  "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int j = 0; j < 32; ++j) sq[lane * 33 + j] = __uint_as_float(v[j]);  // row lane, column j
+            __syncwarp();
+            const int col = n0 + col0 + lane;
+#pragma unroll
+            for (int r = 0; r < 32; ++r) {
+                const int row = m0 + 32 * q + r;
+                if (row < m && col < n) {
+                    const float acc = alpha * sq[r * 33 + lane];
+                    c[(int64_t)row * ldc + col] = beta != 0.0f ? acc + beta * cpre[cc][r] : acc;
+                }
+            }
+            __syncwarp();
+        }
+    } else if (threadIdx.x == 0) {
+        *err = 1;
+        // the loads issued and not consumed still land in shared memory: wait for them
+        for (int ks = s_used; ks < s_loaded; ++ks)
+            (void)bar_wait(&full[ks % kTmaStages], (uint32_t)((ks / kTmaStages) & 1));
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+    }
+}
+
+// hi (and lo) TF32 copies of A (m x k, lda) as (m x kp), columns k..kp zero.
+__global__ void tc_split_rows_kernel(const float* __restrict__ a, int lda, int m, int k, int kp, float* __restrict__ hi,
+                                     float* __restrict__ lo) {
+    const int64_t total = (int64_t)m * kp;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(i / kp), cc = (int)(i % kp);
+        const float v = cc < k ? a[(int64_t)r * lda + cc] : 0.0f;
+        const float h = tf32_hi(v);
+        hi[i] = h;
+        if (lo) lo[i] = v - h;
+    }
+}
+
+// hi (and lo) TF32 copies of B (k x n, ldb) transposed, (n x kp), through 32 x 32 tiles.
+__global__ void tc_split_cols_kernel(const float* __restrict__ b, int ldb, int k, int n, int kp, float* __restrict__ hi,
+                                     float* __restrict__ lo) {
+    __shared__ float t[32][33];
+    const int j0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {  // rows of B: k0 + r, columns j0 + tx
+        const int kk = k0 + r, j = j0 + threadIdx.x;
+        t[r][threadIdx.x] = (kk < k && j < n) ? b[(int64_t)kk * ldb + j] : 0.0f;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {  // rows of the copy: j0 + r, columns k0 + tx
+        const int j = j0 + r, kk = k0 + threadIdx.x;
+        if (j < n) {
+            const float v = t[threadIdx.x][r];
+            const float h = tf32_hi(v);
+            hi[(int64_t)j * kp + kk] = h;
+            if (lo) lo[(int64_t)j * kp + kk] = v - h;
+        }
+    }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        cudaGetLastError();
+    });
+    return fn;
+}
+
+// A row-major (rows x kp) FP32 matrix as 128-row x 32-float boxes, 128-byte swizzle.
+static bool encode_slabs(CUtensorMap* map, const float* base, int rows, int kp) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)kp * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)kBM};
+    const cuuint32_t elem[2] = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, elem,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 }  // namespace
 
 int tc_gemm_tf32(const float* a, int lda, const float* b, int ldb, float* c, int ldc, int m, int n, int k,
@@ -366,6 +618,48 @@ int tc_gemm_tf32(const float* a, int lda, const float* b, int ldb, float* c, int
     tc_gemm_tf32_kernel<<<grid, kThreads, kGemmSmem, s>>>(a, lda, b, ldb, c, ldc, m, n, k, alpha, beta, passes, d_err);
     note_launch();
     FJ_LAUNCH_CHECK("tc_gemm_tf32_kernel");
+    return FJ_OK;
+}
+
+size_t tc_gemm_scratch_floats(int m, int n, int k, int passes) {
+    const size_t kp = (size_t)((k + kBK - 1) / kBK) * kBK;
+    return (size_t)(m + n) * kp * (passes == 3 ? 2 : 1);
+}
+
+int tc_gemm_tf32_tma(const float* a, int lda, const float* b, int ldb, float* c, int ldc, int m, int n, int k,
+                     float alpha, float beta, int passes, float* scratch, size_t scratch_floats, int* d_err,
+                     cudaStream_t s) {
+    if (m < 0 || n < 0 || k <= 0 || lda < k || ldb < n || ldc < n)
+        return fail(FJ_ERR_SHAPE, "tc_gemm: m=%d n=%d k=%d lda=%d ldb=%d ldc=%d", m, n, k, lda, ldb, ldc);
+    if (passes != 1 && passes != 3) return fail(FJ_ERR_SHAPE, "tc_gemm: passes=%d (1 or 3)", passes);
+    if (m == 0 || n == 0) return FJ_OK;
+    const int kp = (k + kBK - 1) / kBK * kBK;
+    const bool split = passes == 3;
+    if (scratch == nullptr || scratch_floats < tc_gemm_scratch_floats(m, n, k, passes) ||
+        ((uintptr_t)scratch & 15) != 0 || tensor_map_encoder() == nullptr)
+        return tc_gemm_tf32(a, lda, b, ldb, c, ldc, m, n, k, alpha, beta, passes, d_err, s);
+    float* a_hi = scratch;
+    float* a_lo = split ? a_hi + (size_t)m * kp : nullptr;
+    float* b_hi = a_hi + (size_t)m * kp * (split ? 2 : 1);
+    float* b_lo = split ? b_hi + (size_t)n * kp : nullptr;
+    const int64_t ta = (int64_t)m * kp;
+    tc_split_rows_kernel<<<(unsigned)std::min<int64_t>((ta + 255) / 256, 148 * 8), 256, 0, s>>>(a, lda, m, k, kp,
+                                                                                                a_hi, a_lo);
+    note_launch();
+    tc_split_cols_kernel<<<dim3((unsigned)((n + 31) / 32), (unsigned)(kp / 32)), dim3(32, 8), 0, s>>>(b, ldb, k, n,
+                                                                                                      kp, b_hi, b_lo);
+    note_launch();
+    CUtensorMap mah, mal, mbh, mbl;
+    // rows are 16-byte multiples (kp x 4 bytes) and every box starts at a multiple of 32 floats
+    if (!encode_slabs(&mah, a_hi, m, kp) || !encode_slabs(&mbh, b_hi, n, kp) ||
+        !encode_slabs(&mal, split ? a_lo : a_hi, m, kp) || !encode_slabs(&mbl, split ? b_lo : b_hi, n, kp))
+        return fail(FJ_ERR_CUDA, "tc_gemm: cuTensorMapEncodeTiled failed");
+    FJ_TRY(allow_dynamic_smem((const void*)tc_gemm_tma_kernel, kTmaSmem));
+    dim3 grid((unsigned)((n + kBN - 1) / kBN), (unsigned)((m + kBM - 1) / kBM));
+    tc_gemm_tma_kernel<<<grid, kTmaThreads, kTmaSmem, s>>>(mah, mal, mbh, mbl, c, ldc, m, n, kp, alpha, beta, passes,
+                                                           d_err);
+    note_launch();
+    FJ_LAUNCH_CHECK("tc_gemm_tma_kernel");
     return FJ_OK;
 }
 
@@ -402,4 +696,22 @@ extern "C" int fj_gemm_tf32(const float* d_a, int lda, const float* d_b, int ldb
                             int k, float alpha, float beta, int passes, int* d_err, fj_stream_t stream) {
     if (!d_a || !d_b || !d_c || !d_err) return fj::fail(FJ_ERR_SHAPE, "gemm_tf32: null pointer");
     return fj::tc_gemm_tf32(d_a, lda, d_b, ldb, d_c, ldc, m, n, k, alpha, beta, passes, d_err, (cudaStream_t)stream);
+}
+
+extern "C" int fj_gemm_tf32_scratch_floats(int m, int n, int k, int passes, size_t* floats) {
+    if (!floats || m < 0 || n < 0 || k <= 0 || (passes != 1 && passes != 3))
+        return fj::fail(FJ_ERR_SHAPE, "gemm_tf32_scratch_floats: m=%d n=%d k=%d passes=%d", m, n, k, passes);
+    *floats = fj::tc_gemm_scratch_floats(m, n, k, passes);
+    return FJ_OK;
+}
+
+extern "C" int fj_gemm_tf32_tma(const float* d_a, int lda, const float* d_b, int ldb, float* d_c, int ldc, int m,
+                                int n, int k, float alpha, float beta, int passes, float* d_scratch,
+                                size_t scratch_floats, int* d_err, fj_stream_t stream) {
+    if (!d_a || !d_b || !d_c || !d_err || !d_scratch) return fj::fail(FJ_ERR_SHAPE, "gemm_tf32_tma: null pointer");
+    if (scratch_floats < fj::tc_gemm_scratch_floats(m, n, k, passes) || ((uintptr_t)d_scratch & 15) != 0)
+        return fj::fail(FJ_ERR_SHAPE, "gemm_tf32_tma: scratch of %zu floats at %p (%zu floats, 16-byte aligned)",
+                        scratch_floats, (void*)d_scratch, fj::tc_gemm_scratch_floats(m, n, k, passes));
+    return fj::tc_gemm_tf32_tma(d_a, lda, d_b, ldb, d_c, ldc, m, n, k, alpha, beta, passes, d_scratch, scratch_floats,
+                                d_err, (cudaStream_t)stream);
 }

@@ -432,6 +432,16 @@ FJ_API int fj_solve_mixed(const double* d_a, int n, const double* d_b, double* d
 FJ_API int fj_gemm_tf32(const float* d_a, int lda, const float* d_b, int ldb, float* d_c, int ldc, int m, int n,
                         int k, float alpha, float beta, int passes, int* d_err, fj_stream_t stream);
 
+/* The same product through the factorisation's TMA pipeline: the operands are first
+ * split into TF32 hi/lo copies in d_scratch (K-major, fj_gemm_tf32_scratch_floats
+ * floats, 16-byte aligned), which cp.async.bulk.tensor loads feed to the MMAs through a
+ * three-stage mbarrier ring (a producer thread apart from the MMA issuer).  C may alias
+ * A or B. */
+FJ_API int fj_gemm_tf32_scratch_floats(int m, int n, int k, int passes, size_t* floats);
+FJ_API int fj_gemm_tf32_tma(const float* d_a, int lda, const float* d_b, int ldb, float* d_c, int ldc, int m,
+                            int n, int k, float alpha, float beta, int passes, float* d_scratch,
+                            size_t scratch_floats, int* d_err, fj_stream_t stream);
+
 /* Failure-detection self-test of the tensor-core kernel's bounded waits: launches
  * fj_gemm_tf32's kernel with its MMAs and commits withheld, so that the mbarrier it waits
  * on never completes.  After about two seconds (the wait and a bounded drain) the kernel

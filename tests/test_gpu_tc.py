@@ -23,18 +23,35 @@ def _f32(a, dev):
     return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32)).to(dev)
 
 
-def _gemm(cuda, a, b, c, m, n, k, alpha, beta, passes):
-    """C <- alpha A B + beta C on the device; a, b, c are 2-D float32 host arrays whose
-    leading (m x k), (k x n), (m x n) blocks are the operands (row strides = their widths)."""
+def _call_gemm(cuda, kernel, pa, lda, pb, ldb, pc, ldc, m, n, k, alpha, beta, passes, err):
+    """One product through fj_gemm_tf32 (kernel "staged") or fj_gemm_tf32_tma ("tma",
+    with its operand-split scratch)."""
     import torch
 
     from flapjax_b200 import _lib
 
+    s = torch.cuda.current_stream(cuda).cuda_stream
+    if kernel == "staged":
+        _lib.call("fj_gemm_tf32", pa, lda, pb, ldb, pc, ldc, m, n, k, C.c_float(alpha), C.c_float(beta), passes,
+                  err.data_ptr(), s)
+        return
+    nf = C.c_size_t()
+    _lib.call("fj_gemm_tf32_scratch_floats", m, n, k, passes, C.byref(nf))
+    scratch = torch.full((nf.value + 4,), float("nan"), dtype=torch.float32, device=cuda)
+    _lib.call("fj_gemm_tf32_tma", pa, lda, pb, ldb, pc, ldc, m, n, k, C.c_float(alpha), C.c_float(beta), passes,
+              scratch.data_ptr(), nf.value, err.data_ptr(), s)
+    torch.cuda.synchronize(cuda)
+
+
+def _gemm(cuda, a, b, c, m, n, k, alpha, beta, passes, kernel="staged"):
+    """C <- alpha A B + beta C on the device; a, b, c are 2-D float32 host arrays whose
+    leading (m x k), (k x n), (m x n) blocks are the operands (row strides = their widths)."""
+    import torch
+
     ta, tb, tc = _f32(a, cuda), _f32(b, cuda), _f32(c, cuda)
     err = torch.zeros(1, dtype=torch.int32, device=cuda)
-    s = torch.cuda.current_stream(cuda).cuda_stream
-    _lib.call("fj_gemm_tf32", ta.data_ptr(), a.shape[1], tb.data_ptr(), b.shape[1], tc.data_ptr(), c.shape[1], m, n,
-              k, C.c_float(alpha), C.c_float(beta), passes, err.data_ptr(), s)
+    _call_gemm(cuda, kernel, ta.data_ptr(), a.shape[1], tb.data_ptr(), b.shape[1], tc.data_ptr(), c.shape[1], m, n,
+               k, alpha, beta, passes, err)
     out = tc.cpu().numpy()
     assert int(err.cpu()) == 0
     return out
@@ -43,13 +60,14 @@ def _gemm(cuda, a, b, c, m, n, k, alpha, beta, passes):
 @pytest.mark.parametrize("m,n,k,lda,ldb,ldc", [(128, 128, 32, 32, 128, 128), (200, 300, 100, 103, 301, 305),
                                                (5, 7, 3, 3, 7, 7), (384, 256, 128, 131, 257, 256)])
 @pytest.mark.parametrize("passes", [1, 3])
-def test_gemm_matches_fp64_product(cuda, m, n, k, lda, ldb, ldc, passes):
+@pytest.mark.parametrize("kernel", ["staged", "tma"])
+def test_gemm_matches_fp64_product(cuda, m, n, k, lda, ldb, ldc, passes, kernel):
     rng = np.random.default_rng(m + n + k + passes)
     a = rng.normal(size=(m, lda)).astype(np.float32)
     b = rng.normal(size=(k, ldb)).astype(np.float32)
     c = rng.normal(size=(m, ldc)).astype(np.float32)
     alpha, beta = -1.0, 1.0
-    got = _gemm(cuda, a, b, c, m, n, k, alpha, beta, passes)
+    got = _gemm(cuda, a, b, c, m, n, k, alpha, beta, passes, kernel)
     A, B = a[:, :k].astype(np.float64), b[:, :n].astype(np.float64)
     want = alpha * A @ B + beta * c[:, :n].astype(np.float64)
     scale = np.abs(A) @ np.abs(B) + np.abs(c[:, :n])
@@ -59,23 +77,23 @@ def test_gemm_matches_fp64_product(cuda, m, n, k, lda, ldb, ldc, passes):
     assert np.array_equal(got[:, n:], c[:, n:])
 
 
-def test_gemm_split_beats_single_pass_and_beta_zero_ignores_c(cuda):
+@pytest.mark.parametrize("kernel", ["staged", "tma"])
+def test_gemm_split_beats_single_pass_and_beta_zero_ignores_c(cuda, kernel):
     rng = np.random.default_rng(9)
     m, n, k = 256, 256, 128
     a = rng.normal(size=(m, k)).astype(np.float32)
     b = rng.normal(size=(k, n)).astype(np.float32)
     c = np.full((m, n), np.nan, np.float32)  # beta = 0 must not read C
     want = a.astype(np.float64) @ b.astype(np.float64)
-    e1 = rel_err(_gemm(cuda, a, b, c, m, n, k, 1.0, 0.0, 1), want)
-    e3 = rel_err(_gemm(cuda, a, b, c, m, n, k, 1.0, 0.0, 3), want)
+    e1 = rel_err(_gemm(cuda, a, b, c, m, n, k, 1.0, 0.0, 1, kernel), want)
+    e3 = rel_err(_gemm(cuda, a, b, c, m, n, k, 1.0, 0.0, 3, kernel), want)
     assert e3 < 5e-6 and 100 * e3 < e1 < 1e-2
 
 
-def test_gemm_in_place_on_b(cuda):
+@pytest.mark.parametrize("kernel", ["staged", "tma"])
+def test_gemm_in_place_on_b(cuda, kernel):
     """U12 = L11^-1 A12 runs in place (C is B's memory, m <= 128)."""
     import torch
-
-    from flapjax_b200 import _lib
 
     rng = np.random.default_rng(3)
     m = k = 128
@@ -84,11 +102,34 @@ def test_gemm_in_place_on_b(cuda):
     b = rng.normal(size=(k, n)).astype(np.float32)
     ta, tb = _f32(a, cuda), _f32(b, cuda)
     err = torch.zeros(1, dtype=torch.int32, device=cuda)
-    s = torch.cuda.current_stream(cuda).cuda_stream
-    _lib.call("fj_gemm_tf32", ta.data_ptr(), k, tb.data_ptr(), n, tb.data_ptr(), n, m, n, k, C.c_float(1.0),
-              C.c_float(0.0), 3, err.data_ptr(), s)
+    _call_gemm(cuda, kernel, ta.data_ptr(), k, tb.data_ptr(), n, tb.data_ptr(), n, m, n, k, 1.0, 0.0, 3, err)
     want = a.astype(np.float64) @ b.astype(np.float64)
     assert rel_err(tb.cpu().numpy(), want) < 5e-6
+    assert int(err.cpu()) == 0
+
+
+def test_gemm_tma_overlapping_update(cuda):
+    """A22 -= A21 A12 inside one matrix (the trailing update's aliasing: A and B are
+    blocks of C's own matrix), several K slabs, ragged edges."""
+    import torch
+
+    rng = np.random.default_rng(11)
+    n, k0 = 700, 160
+    a = rng.normal(size=(n, n)).astype(np.float32)
+    ta = _f32(a, cuda)
+    err = torch.zeros(1, dtype=torch.int32, device=cuda)
+    base, es = ta.data_ptr(), 4
+    rest = n - k0
+    _call_gemm(cuda, "tma", base + k0 * n * es, n, base + k0 * es, n, base + (k0 * n + k0) * es, n, rest, rest, k0,
+               -1.0, 1.0, 3, err)
+    A = a.astype(np.float64)
+    want = A.copy()
+    want[k0:, k0:] -= A[k0:, :k0] @ A[:k0, k0:]
+    got = ta.cpu().numpy()
+    scale = np.abs(A[k0:, :k0]) @ np.abs(A[:k0, k0:]) + np.abs(A[k0:, k0:])
+    assert np.all(np.abs(got[k0:, k0:] - want[k0:, k0:]) <= 1e-5 * scale)
+    assert np.array_equal(got[:k0], a[:k0]) and np.array_equal(got[:, :k0], a[:, :k0])
+    assert int(err.cpu()) == 0
 
 
 def _solve_mixed(cuda, a, b):
@@ -128,7 +169,7 @@ def test_mixed_solve_through_tensor_core_factors(cuda, n, monkeypatch):
     assert r1 < 1e-2
 
 
-@pytest.mark.parametrize("n", [300, 520])
+@pytest.mark.parametrize("n", [300, 520, 1100, 2200])
 def test_mixed_solve_heavy_pivoting(cuda, n, monkeypatch):
     """No diagonal dominance: pivot rows come from far below the outer panel, so the row
     swaps must reach the columns to its right before their updates.  Such a matrix
@@ -143,6 +184,25 @@ def test_mixed_solve_heavy_pivoting(cuda, n, monkeypatch):
     monkeypatch.setenv("FJ_MIXED_FACTOR", "tf32x3")
     x, r = _solve_mixed(cuda, a, b)
     assert r < max(1e-12, 10 * rc) and rel_err(x, want) < 1e-8 and rel_err(xc, want) < 1e-8
+
+
+@pytest.mark.parametrize("n", [640, 1029])
+def test_mixed_solve_pivot_ties(cuda, n, monkeypatch):
+    """Entries of +-1 (and a few exact zeros): the first columns' pivot searches meet
+    equal magnitudes everywhere, and the first maximum (the lowest row) must win in the
+    cluster-wide search as in getrf.  n = 1029 also leaves a ragged last outer panel and
+    rows that start off 16-byte boundaries."""
+    rng = np.random.default_rng(7 + n)
+    a = rng.choice([-1.0, 1.0], size=(n, n))
+    a[rng.random(size=(n, n)) < 0.01] = 0.0
+    b = rng.normal(size=n)
+    want = np.linalg.solve(a, b)
+    monkeypatch.setenv("FJ_MIXED_FACTOR", "cuda")
+    xc, rc = _solve_mixed(cuda, a, b)
+    monkeypatch.setenv("FJ_MIXED_FACTOR", "tf32x3")
+    x, r = _solve_mixed(cuda, a, b)
+    assert np.isfinite(r) and r < max(1e-12, 10 * rc)
+    assert rel_err(x, want) < max(1e-8, 10 * rel_err(xc, want))
 
 
 def test_mixed_solve_of_an_aic(cuda):
