@@ -591,23 +591,17 @@ def factor_bench(dc, case, torch):
             os.environ["FJ_MIXED_FACTOR"] = old
     out["tensor_core_speedup_over_cuda_cores"] = (out["cuda"]["factor_inverse_solve_ms"] /
                                                    out["tf32x3"]["factor_inverse_solve_ms"])
-    # the GEMM alone
+    # the GEMM alone at the first trailing update's shape, through the factorisation's own
+    # path (fj_gemm_tf32_tma: the hi/lo operand split, then the TMA-fed kernel; both inside
+    # the events) and through the staged kernel (fj_gemm_tf32)
     g = max(nb - 128, 128)
     A = torch.randn((g, 128), dtype=torch.float32, device=dev)
     B = torch.randn((128, g), dtype=torch.float32, device=dev)
     Cm = torch.randn((g, g), dtype=torch.float32, device=dev)
     err = torch.zeros(1, dtype=torch.int32, device=dev)
-    times = []
-    for it in range(8):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        _lib.call("fj_gemm_tf32", A.data_ptr(), 128, B.data_ptr(), g, Cm.data_ptr(), g, g, g, 128, C.c_float(-1.0),
-                  C.c_float(1.0), 3, err.data_ptr(), s)
-        e1.record()
-        torch.cuda.synchronize()
-        if it >= 3:
-            times.append(e0.elapsed_time(e1))
-    t = float(np.median(times))
+    nf = C.c_size_t()
+    _lib.call("fj_gemm_tf32_scratch_floats", g, g, 128, 3, C.byref(nf))
+    scratch = torch.empty(nf.value, dtype=torch.float32, device=dev)
     peaks = measured_peaks()
     if "bf16_tflops" in peaks:
         tf32_peak = peaks["bf16_tflops"] / 2
@@ -615,9 +609,30 @@ def factor_bench(dc, case, torch):
     else:
         tf32_peak = 1590.0 / 2
         src = "half of the fallback 1590 TFLOP/s bf16 (MEASURED_PEAKS.json absent; dense TF32 is half bf16)"
-    achieved = 3 * 2.0 * g * g * 128 / (t * 1e-3) / 1e12
-    out["gemm"] = {"shape": [g, g, 128], "passes": 3, "ms": t, "tflops_tf32_issued": achieved,
-                   "tf32_peak_tflops": tf32_peak, "frac": achieved / tf32_peak, "peak_source": src}
+
+    def gemm_ms(path):
+        times = []
+        for it in range(8):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            if path == "tma":
+                _lib.call("fj_gemm_tf32_tma", A.data_ptr(), 128, B.data_ptr(), g, Cm.data_ptr(), g, g, g, 128,
+                          C.c_float(-1.0), C.c_float(1.0), 3, scratch.data_ptr(), scratch.numel(), err.data_ptr(), s)
+            else:
+                _lib.call("fj_gemm_tf32", A.data_ptr(), 128, B.data_ptr(), g, Cm.data_ptr(), g, g, g, 128,
+                          C.c_float(-1.0), C.c_float(1.0), 3, err.data_ptr(), s)
+            e1.record()
+            torch.cuda.synchronize()
+            if it >= 3:
+                times.append(e0.elapsed_time(e1))
+        return float(np.median(times))
+
+    out["gemm"] = {"shape": [g, g, 128], "passes": 3, "tf32_peak_tflops": tf32_peak, "peak_source": src}
+    for path in ("tma", "staged"):
+        t = gemm_ms(path)
+        achieved = 3 * 2.0 * g * g * 128 / (t * 1e-3) / 1e12
+        out["gemm"][path] = {"ms": t, "tflops_tf32_issued": achieved, "frac": achieved / tf32_peak}
+    out["gemm"]["tma"]["includes"] = "the operand split (two launches) and the TMA-fed product"
     return out
 
 

@@ -431,11 +431,6 @@ static bool panel_fits(int n, int nb) {
     return (size_t)n * (nb + 1) * sizeof(T) <= (size_t)220 * 1024;
 }
 
-int lu_factor64(double* a, int n, int32_t* piv, int* d_info, cudaStream_t s, const int* run_flag) {
-    if (panel_fits<double>(n, 8)) return lu_factor_impl<double, 8>(a, n, piv, d_info, s, run_flag);
-    if (panel_fits<double>(n, 4)) return lu_factor_impl<double, 4>(a, n, piv, d_info, s, run_flag);
-    return lu_factor_impl<double, 2>(a, n, piv, d_info, s, run_flag);
-}
 int lu_factor32(float* a, int n, int32_t* piv, int* d_info, cudaStream_t s) {
     if (panel_fits<float>(n, 16)) return lu_factor_impl<float, 16>(a, n, piv, d_info, s, nullptr);
     return lu_factor_impl<float, 8>(a, n, piv, d_info, s, nullptr);
@@ -472,35 +467,64 @@ __global__ void __launch_bounds__(1024) permute_kernel(const int32_t* __restrict
 }
 
 // Solve the diagonal block [i0, i0+bw) of L (unit lower, upper = false) or U (upper = true)
-// in place on x, with the block held in shared memory.
+// in place on x.  The block comes into shared memory with every element's cp.async in
+// flight at once; then one warp substitutes, lane l holding x of rows l + 32 q (q < 4) in
+// registers and x_j reaching every lane by a shuffle, so no step waits on a CTA barrier.
+// Per row the operations are getrs's, in its order.
+__device__ __forceinline__ double pick4(const double (&v)[4], int q) {
+    return q == 0 ? v[0] : q == 1 ? v[1] : q == 2 ? v[2] : v[3];
+}
+
 __global__ void __launch_bounds__(kTrsvBlk) trsv_diag_kernel(const double* __restrict__ lu, int n, int i0, int bw,
                                                              bool upper, double* __restrict__ x) {
+    static_assert(kTrsvBlk == 128, "four rows per lane");
     extern __shared__ double blk[];  // bw x (bw + 1)
-    __shared__ double xs[kTrsvBlk];
     const int ld = bw + 1;
     for (int idx = threadIdx.x; idx < bw * bw; idx += blockDim.x) {
         const int r = idx / bw, c = idx % bw;
-        blk[r * ld + c] = lu[(int64_t)(i0 + r) * n + i0 + c];
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(blk + r * ld + c)),
+                     "l"(lu + (int64_t)(i0 + r) * n + i0 + c)
+                     : "memory");
     }
-    const int r = threadIdx.x;
-    if (r < bw) xs[r] = x[i0 + r];
+    asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    const unsigned full = 0xffffffffu;
+    double v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = lane + 32 * q < bw ? x[i0 + lane + 32 * q] : 0.0;
     if (!upper) {
+#pragma unroll 1
         for (int j = 0; j < bw; ++j) {
-            const double xj = xs[j];
-            if (r > j && r < bw) xs[r] -= blk[r * ld + j] * xj;
-            __syncthreads();
+            const double xj = __shfl_sync(full, pick4(v, j >> 5), j & 31);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = lane + 32 * q;
+                if (r > j && r < bw) v[q] -= blk[r * ld + j] * xj;
+            }
         }
     } else {
+#pragma unroll 1
         for (int j = bw - 1; j >= 0; --j) {
-            if (r == j) xs[j] = xs[j] / blk[j * ld + j];
-            __syncthreads();
-            const double xj = xs[j];
-            if (r < j) xs[r] -= blk[r * ld + j] * xj;
-            __syncthreads();
+            const int qj = j >> 5;
+            if (lane == (j & 31)) {
+                const double d = blk[j * ld + j];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (q == qj) v[q] = v[q] / d;
+            }
+            const double xj = __shfl_sync(full, pick4(v, qj), j & 31);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = lane + 32 * q;
+                if (r < j) v[q] -= blk[r * ld + j] * xj;
+            }
         }
     }
-    if (r < bw) x[i0 + r] = xs[r];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        if (lane + 32 * q < bw) x[i0 + lane + 32 * q] = v[q];
 }
 
 // x[i] -= sum_{j in [j0, j0+bw)} lu[i][j] x[j] for i in [r0, r1): one warp per row.
@@ -704,74 +728,108 @@ constexpr int kPcThreads = 512;
 constexpr int kPcWarps = kPcThreads / 32;
 constexpr int kPcMaxCtas = 16;
 
-// Candidate key: the magnitude's bits + 1, ordered as the magnitudes; 0 = no candidate
-// (inactive, or NaN, which never wins a getrf pivot search).
-__device__ __forceinline__ uint32_t pivot_key(float x) {
-    const float ax = fabsf(x);
-    return ax == ax ? __float_as_uint(ax) + 1u : 0u;
+// Panel element types.  A panel row is 512 bytes either way: 128 FP32 columns (the mixed
+// path's outer panel) or 64 FP64 columns (the FP64 path's); lane L holds columns L + 32 c,
+// c < NG.  The candidate key is the magnitude's bits + 1, ordered as the magnitudes; 0 = no
+// candidate (inactive, or NaN, which never wins a getrf pivot search).
+template <typename T>
+struct PanelType;
+template <>
+struct PanelType<float> {
+    static constexpr int NG = 4;
+    using Key = uint32_t;
+    __device__ static __forceinline__ Key key(float x) {
+        const float ax = fabsf(x);
+        return ax == ax ? __float_as_uint(ax) + 1u : 0u;
+    }
+    __device__ static __forceinline__ bool normal(float x) { return fabsf(x) >= 1.17549435e-38f; }  // FLT_MIN
+};
+template <>
+struct PanelType<double> {
+    static constexpr int NG = 2;
+    using Key = unsigned long long;
+    __device__ static __forceinline__ Key key(double x) {
+        const double ax = fabs(x);
+        return ax == ax ? (Key)__double_as_longlong(ax) + 1ull : 0ull;
+    }
+    __device__ static __forceinline__ bool normal(double x) { return fabs(x) >= 2.2250738585072014e-308; }  // DBL_MIN
+};
+
+// The warp's largest key (every lane gets it).
+__device__ __forceinline__ uint32_t warp_key_max(uint32_t k) { return __reduce_max_sync(0xffffffffu, k); }
+__device__ __forceinline__ unsigned long long warp_key_max(unsigned long long k) {
+    const uint32_t hi = (uint32_t)(k >> 32);
+    const uint32_t mhi = __reduce_max_sync(0xffffffffu, hi);
+    const uint32_t mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? (uint32_t)k : 0u);
+    return ((unsigned long long)mhi << 32) | mlo;
 }
 
-// Row `i` (a runtime index) of a thread's rows, as the 4 columns this lane holds.
-template <int RPW>
-__device__ __forceinline__ void pick_row(const float (&v)[RPW][4], int i, float (&out)[4]) {
+// Row `i` (a runtime index) of a thread's rows, as the NG columns this lane holds.
+template <typename T, int NG, int RPW>
+__device__ __forceinline__ void pick_row(const T (&v)[RPW][NG], int i, T (&out)[NG]) {
 #pragma unroll
-    for (int c = 0; c < 4; ++c) out[c] = v[0][c];
+    for (int c = 0; c < NG; ++c) out[c] = v[0][c];
 #pragma unroll
     for (int r = 1; r < RPW; ++r)
         if (r == i) {
 #pragma unroll
-            for (int c = 0; c < 4; ++c) out[c] = v[r][c];
+            for (int c = 0; c < NG; ++c) out[c] = v[r][c];
         }
 }
 
-template <int RPW>
-__device__ __forceinline__ void put_row(float (&v)[RPW][4], int i, const float (&in)[4]) {
+template <typename T, int NG, int RPW>
+__device__ __forceinline__ void put_row(T (&v)[RPW][NG], int i, const T (&in)[NG]) {
 #pragma unroll
     for (int r = 0; r < RPW; ++r)
         if (r == i) {
 #pragma unroll
-            for (int c = 0; c < 4; ++c) v[r][c] = in[c];
+            for (int c = 0; c < NG; ++c) v[r][c] = in[c];
         }
 }
 
 // Rank-1 update of the rows below j with multipliers column(j) * s (mul) or / s (div).
-template <int RPW, int G, bool kDiv>
-__device__ __forceinline__ void panel_update(float (&v)[RPW][4], int rbase, int rows, int j, int jj, int lane,
-                                             float s, const float (&pc)[4]) {
+template <typename T, int NG, int RPW, int G, bool kDiv>
+__device__ __forceinline__ void panel_update(T (&v)[RPW][NG], int rbase, int rows, int j, int jj, int lane, T s,
+                                             const T (&pc)[NG]) {
 #pragma unroll
     for (int i = 0; i < RPW; ++i) {
         const int r = rbase + i;
         if (r > j && r < rows) {  // uniform over the warp
-            float l = kDiv ? v[i][G] / s : v[i][G] * s;
+            T l = kDiv ? v[i][G] / s : v[i][G] * s;
             l = __shfl_sync(0xffffffffu, l, jj);  // lane jj's is the multiplier
             if (lane == jj) v[i][G] = l;
 #pragma unroll
-            for (int c = G + 1; c < 4; ++c) v[i][c] -= l * pc[c];
+            for (int c = G + 1; c < NG; ++c) v[i][c] -= l * pc[c];
             if (lane > jj) v[i][G] -= l * pc[G];
         }
     }
 }
 
 // The panel's shared state (static shared memory of lu_panel_cluster_kernel).
+template <typename T>
 struct PanelShared {
-    float cand[2][kPcWarps][kTcBlk];  // this CTA's warp candidates
-    uint32_t wkey[2][kPcWarps];
+    static constexpr int KB = 32 * PanelType<T>::NG;
+    using Key = typename PanelType<T>::Key;
+    T cand[2][kPcWarps][KB];  // this CTA's warp candidates
+    Key wkey[2][kPcWarps];
     int wrow[2][kPcWarps], wsrc[2][kPcWarps];
-    float rowj_loc[2][kTcBlk];                // row j, in CTA 0
-    float slot[2][kPcMaxCtas][kTcBlk];        // every CTA's candidate, pushed by that CTA
-    uint32_t slot_key[2][kPcMaxCtas];
+    T rowj_loc[2][KB];                // row j, in CTA 0
+    T slot[2][kPcMaxCtas][KB];        // every CTA's candidate, pushed by that CTA
+    Key slot_key[2][kPcMaxCtas];
     int slot_row[2][kPcMaxCtas], slot_src[2][kPcMaxCtas];
-    float rowj[2][kTcBlk];                    // row j, pushed by CTA 0
+    T rowj[2][KB];                    // row j, pushed by CTA 0
     int rowj_src[2];
     int rowj_src_loc[2];
-    int piv[kTcBlk];  // written out at the end: no global store inside the column loop
+    int piv[KB];  // written out at the end: no global store inside the column loop
     int info;
     int wcnt[kPcWarps], cnt, off;
 };
 
-template <int RPW, int G>
-__device__ __forceinline__ void panel_columns(float (&v)[RPW][4], int& orig, int k, int kb, int rows, int q, int nc,
-                                              int tid, cg::cluster_group& cl, PanelShared& S) {
+template <typename T, int RPW, int G>
+__device__ __forceinline__ void panel_columns(T (&v)[RPW][PanelType<T>::NG], int& orig, int k, int kb, int rows,
+                                              int q, int nc, int tid, cg::cluster_group& cl, PanelShared<T>& S) {
+    constexpr int NG = PanelType<T>::NG;
+    using Key = typename PanelType<T>::Key;
     const int lane = tid & 31, warp = tid >> 5;
     const int rbase = (q * kPcWarps + warp) * RPW;
     const unsigned full = 0xffffffffu;
@@ -780,48 +838,48 @@ __device__ __forceinline__ void panel_columns(float (&v)[RPW][4], int& orig, int
     for (int j = 32 * G; j < jend; ++j) {
         const int jj = j & 31, par = j & 1;
         // a. the warp's candidate: lane i < RPW takes column j of row i
-        float xj = 0.f;
+        T xj = T(0);
 #pragma unroll
         for (int i = 0; i < RPW; ++i) {
-            const float t = __shfl_sync(full, v[i][G], jj);
+            const T t = __shfl_sync(full, v[i][G], jj);
             if (lane == i) xj = t;
         }
         const int r = rbase + lane;
-        const uint32_t key = (lane < RPW && r >= j && r < rows) ? pivot_key(xj) : 0u;
-        const uint32_t wmax = __reduce_max_sync(full, key);
-        const unsigned hit = __ballot_sync(full, wmax != 0u && key == wmax);
+        const Key key = (lane < RPW && r >= j && r < rows) ? PanelType<T>::key(xj) : Key(0);
+        const Key wmax = warp_key_max(key);
+        const unsigned hit = __ballot_sync(full, wmax != Key(0) && key == wmax);
         const int bi = hit ? __ffs(hit) - 1 : 0;
         const int bsrc = __shfl_sync(full, orig, bi);
         if (hit != 0u) {
-            float row[4];
-            pick_row<RPW>(v, bi, row);
+            T row[NG];
+            pick_row<T, NG, RPW>(v, bi, row);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) S.cand[par][warp][lane + 32 * c] = row[c];
+            for (int c = 0; c < NG; ++c) S.cand[par][warp][lane + 32 * c] = row[c];
         }
         if (lane == 0) {
             S.wkey[par][warp] = wmax;
             S.wrow[par][warp] = rbase + bi;
             S.wsrc[par][warp] = bsrc;
         }
-        const bool holds_j = j >= rbase && j < rbase + RPW;  // CTA 0 (its rows cover the 128 columns)
+        const bool holds_j = j >= rbase && j < rbase + RPW;  // CTA 0 (its rows cover the panel's columns)
         const int ij = j - rbase;
         const int jsrc = __shfl_sync(full, orig, holds_j ? ij : 0);
         if (holds_j) {
-            float row[4];
-            pick_row<RPW>(v, ij, row);
+            T row[NG];
+            pick_row<T, NG, RPW>(v, ij, row);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) S.rowj_loc[par][lane + 32 * c] = row[c];
+            for (int c = 0; c < NG; ++c) S.rowj_loc[par][lane + 32 * c] = row[c];
             if (lane == 0) S.rowj_src_loc[par] = jsrc;
         }
         __syncthreads();
-        // b. push: warps 0-3 the CTA's candidate, warps 4-7 of CTA 0 row j; thread t
-        //    stores float4 t % 32 into CTAs t / 32 % 4, + 4, + 8, + 12
+        // b. push: warps 0-3 the CTA's candidate, warps 4-7 of CTA 0 row j; a row is 512
+        //    bytes, and thread t stores its float4 t % 32 into CTAs t / 32 % 4, + 4, + 8, + 12
         if (warp < 8) {
             const int t = tid & 127, f = t & 31, c0 = t >> 5;
             if (warp < 4) {
-                const uint32_t kw = lane < kPcWarps ? S.wkey[par][lane] : 0u;
-                const uint32_t m = __reduce_max_sync(full, kw);
-                const unsigned h = __ballot_sync(full, m != 0u && kw == m);
+                const Key kw = lane < kPcWarps ? S.wkey[par][lane] : Key(0);
+                const Key m = warp_key_max(kw);
+                const unsigned h = __ballot_sync(full, m != Key(0) && kw == m);
                 const int w = h ? __ffs(h) - 1 : 0;
                 const float4 val = reinterpret_cast<const float4*>(S.cand[par][w])[f];
                 const int prow_r = S.wrow[par][w], prow_s = S.wsrc[par][w];
@@ -829,7 +887,7 @@ __device__ __forceinline__ void panel_columns(float (&v)[RPW][4], int& orig, int
                 for (int u = 0; u < kPcMaxCtas / 4; ++u) {
                     const int c = c0 + 4 * u;
                     if (c < nc) {
-                        PanelShared* R = cl.map_shared_rank(&S, c);
+                        PanelShared<T>* R = cl.map_shared_rank(&S, c);
                         reinterpret_cast<float4*>(R->slot[par][q])[f] = val;
                         if (f == 0) {
                             R->slot_key[par][q] = m;
@@ -845,7 +903,7 @@ __device__ __forceinline__ void panel_columns(float (&v)[RPW][4], int& orig, int
                 for (int u = 0; u < kPcMaxCtas / 4; ++u) {
                     const int c = c0 + 4 * u;
                     if (c < nc) {
-                        PanelShared* R = cl.map_shared_rank(&S, c);
+                        PanelShared<T>* R = cl.map_shared_rank(&S, c);
                         reinterpret_cast<float4*>(R->rowj[par])[f] = val;
                         if (f == 0) R->rowj_src[par] = js;
                     }
@@ -854,51 +912,55 @@ __device__ __forceinline__ void panel_columns(float (&v)[RPW][4], int& orig, int
         }
         cl.sync();
         // d. the cluster's pivot, from this CTA's own slots (every warp)
-        const uint32_t ks = lane < nc ? S.slot_key[par][lane] : 0u;
-        const uint32_t m = __reduce_max_sync(full, ks);
-        const unsigned h = __ballot_sync(full, m != 0u && ks == m);
+        const Key ks = lane < nc ? S.slot_key[par][lane] : Key(0);
+        const Key m = warp_key_max(ks);
+        const unsigned h = __ballot_sync(full, m != Key(0) && ks == m);
         const int o = h ? __ffs(h) - 1 : 0;  // the lowest CTA with the maximum
-        const float* prow = m != 0u ? S.slot[par][o] : S.rowj[par];
-        const int p = m != 0u ? S.slot_row[par][o] : j;  // no candidate: row j stays the pivot row
+        const T* prow = m != Key(0) ? S.slot[par][o] : S.rowj[par];
+        const int p = m != Key(0) ? S.slot_row[par][o] : j;  // no candidate: row j stays the pivot row
         if (p != j) {
             if (holds_j) {  // row j takes the pivot row
-                float row[4];
+                T row[NG];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) row[c] = prow[lane + 32 * c];
-                put_row<RPW>(v, ij, row);
+                for (int c = 0; c < NG; ++c) row[c] = prow[lane + 32 * c];
+                put_row<T, NG, RPW>(v, ij, row);
                 if (lane == ij) orig = S.slot_src[par][o];
             }
             if (p >= rbase && p < rbase + RPW) {  // row p takes row j
-                float row[4];
+                T row[NG];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) row[c] = S.rowj[par][lane + 32 * c];
-                put_row<RPW>(v, p - rbase, row);
+                for (int c = 0; c < NG; ++c) row[c] = S.rowj[par][lane + 32 * c];
+                put_row<T, NG, RPW>(v, p - rbase, row);
                 if (lane == p - rbase) orig = S.rowj_src[par];
             }
         }
-        const float pv = prow[j];
+        const T pv = prow[j];
         if (tid == 0) {
             S.piv[j] = k + p;
-            if (pv == 0.f && S.info == 0) S.info = k + j + 1;
+            if (pv == T(0) && S.info == 0) S.info = k + j + 1;
         }
-        if (pv != 0.f) {
-            float pc[4];
+        if (pv != T(0)) {
+            T pc[NG];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) pc[c] = prow[lane + 32 * c];
-            if (fabsf(pv) >= 1.17549435e-38f)  // FLT_MIN: getrf's sfmin test
-                panel_update<RPW, G, false>(v, rbase, rows, j, jj, lane, 1.0f / pv, pc);
+            for (int c = 0; c < NG; ++c) pc[c] = prow[lane + 32 * c];
+            if (PanelType<T>::normal(pv))  // getrf's sfmin test
+                panel_update<T, NG, RPW, G, false>(v, rbase, rows, j, jj, lane, T(1) / pv, pc);
             else
-                panel_update<RPW, G, true>(v, rbase, rows, j, jj, lane, pv, pc);
+                panel_update<T, NG, RPW, G, true>(v, rbase, rows, j, jj, lane, pv, pc);
         }
     }
 }
 
-template <int RPW>
+// swaps (may be null: the FP64 path derives the moves from the pivots instead) receives
+// the moved rows; run_flag (may be null): every CTA returns at once when *run_flag == 0.
+template <typename T, int RPW>
 __global__ void __launch_bounds__(kPcThreads, 1)
-    lu_panel_cluster_kernel(float* __restrict__ a, int n, int k, int kb, int32_t* __restrict__ piv,
-                            int* __restrict__ info, int* __restrict__ swaps) {
+    lu_panel_cluster_kernel(T* __restrict__ a, int n, int k, int kb, int32_t* __restrict__ piv,
+                            int* __restrict__ info, int* __restrict__ swaps, const int* __restrict__ run_flag) {
+    if (run_flag != nullptr && *run_flag == 0) return;  // the same for every CTA of the cluster
+    constexpr int NG = PanelType<T>::NG;
     cg::cluster_group cl = cg::this_cluster();
-    __shared__ __align__(16) PanelShared S;
+    __shared__ __align__(16) PanelShared<T> S;
     const int q = (int)cl.block_rank(), nc = (int)cl.num_blocks();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int rows = n - k;
@@ -906,27 +968,29 @@ __global__ void __launch_bounds__(kPcThreads, 1)
     const unsigned full = 0xffffffffu;
     if (tid == 0) S.info = 0;
 
-    float v[RPW][4];
+    T v[RPW][NG];
 #pragma unroll
     for (int i = 0; i < RPW; ++i) {
         const bool has = rbase + i < rows;
-        const float* src = a + (int64_t)(k + (has ? rbase + i : 0)) * n + k + lane;
+        const T* src = a + (int64_t)(k + (has ? rbase + i : 0)) * n + k + lane;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) v[i][c] = (has && lane + 32 * c < kb) ? src[32 * c] : 0.f;
+        for (int c = 0; c < NG; ++c) v[i][c] = (has && lane + 32 * c < kb) ? src[32 * c] : T(0);
     }
     int orig = rbase + lane;  // lanes < RPW: original panel row of the warp's row `lane`
     cl.sync();                // every CTA of the cluster runs before any shared memory is written remotely
 
-    panel_columns<RPW, 0>(v, orig, k, kb, rows, q, nc, tid, cl, S);
-    panel_columns<RPW, 1>(v, orig, k, kb, rows, q, nc, tid, cl, S);
-    panel_columns<RPW, 2>(v, orig, k, kb, rows, q, nc, tid, cl, S);
-    panel_columns<RPW, 3>(v, orig, k, kb, rows, q, nc, tid, cl, S);
+    panel_columns<T, RPW, 0>(v, orig, k, kb, rows, q, nc, tid, cl, S);
+    panel_columns<T, RPW, 1>(v, orig, k, kb, rows, q, nc, tid, cl, S);
+    if constexpr (NG > 2) {
+        panel_columns<T, RPW, 2>(v, orig, k, kb, rows, q, nc, tid, cl, S);
+        panel_columns<T, RPW, 3>(v, orig, k, kb, rows, q, nc, tid, cl, S);
+    }
 #pragma unroll
     for (int i = 0; i < RPW; ++i) {
         if (rbase + i < rows) {
-            float* dst = a + (int64_t)(k + rbase + i) * n + k + lane;
+            T* dst = a + (int64_t)(k + rbase + i) * n + k + lane;
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
+            for (int c = 0; c < NG; ++c)
                 if (lane + 32 * c < kb) dst[32 * c] = v[i][c];
         }
     }
@@ -955,10 +1019,10 @@ __global__ void __launch_bounds__(kPcThreads, 1)
         int off = 0;
         for (int c = 0; c < q; ++c) off += cl.map_shared_rank(&S, c)->cnt;
         S.off = off;
-        if (q == nc - 1) swaps[0] = off + S.cnt;
+        if (q == nc - 1 && swaps != nullptr) swaps[0] = off + S.cnt;
     }
     __syncthreads();
-    if (moved) {
+    if (moved && swaps != nullptr) {
         const int e = S.off + S.wcnt[warp] + __popc(mb & ((1u << lane) - 1u));
         swaps[1 + 2 * e] = k + rbase + lane;
         swaps[2 + 2 * e] = k + orig;
@@ -990,14 +1054,15 @@ __global__ void __launch_bounds__(256) lu_swap_rows_kernel(float* __restrict__ a
         if (col) a[(int64_t)s_dst[e] * n + c] = tile[e][lane];
 }
 
-// The largest cluster of lu_panel_cluster_kernel CTAs the device runs (16 where the
-// non-portable size is allowed, else 8; 0 if none), checked once.
+// The largest cluster of lu_panel_cluster_kernel<T> CTAs the device runs (16 where the
+// non-portable size is allowed, else 8; 0 if none), checked once per element type.
+template <typename T>
 static int cluster_panel_max() {
     static std::once_flag once;
     static int best = 0;
     std::call_once(once, [] {
         for (int size : {16, 8}) {
-            const void* fn = size == 16 ? (const void*)lu_panel_cluster_kernel<8> : (const void*)lu_panel_cluster_kernel<16>;
+            const void* fn = size == 16 ? (const void*)lu_panel_cluster_kernel<T, 8> : (const void*)lu_panel_cluster_kernel<T, 16>;
             if (size == 16 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
                 cudaGetLastError();
                 continue;
@@ -1013,8 +1078,8 @@ static int cluster_panel_max() {
             cfg.attrs = at;
             cfg.numAttrs = 1;
             int clusters = 0;
-            const cudaError_t e = size == 16 ? cudaOccupancyMaxActiveClusters(&clusters, lu_panel_cluster_kernel<8>, &cfg)
-                                             : cudaOccupancyMaxActiveClusters(&clusters, lu_panel_cluster_kernel<16>, &cfg);
+            const cudaError_t e = size == 16 ? cudaOccupancyMaxActiveClusters(&clusters, lu_panel_cluster_kernel<T, 8>, &cfg)
+                                             : cudaOccupancyMaxActiveClusters(&clusters, lu_panel_cluster_kernel<T, 16>, &cfg);
             cudaGetLastError();
             if (e == cudaSuccess && clusters > 0) {
                 best = size;
@@ -1027,14 +1092,17 @@ static int cluster_panel_max() {
 
 // Rows of the outer panel one cluster takes: 16 CTAs of 8-row warps, or 8 CTAs of
 // 16-row warps.
+template <typename T>
 static int cluster_panel_rows() {
-    const int m = cluster_panel_max();
+    const int m = cluster_panel_max<T>();
     return m == 16 ? 16 * 8 * kPcWarps : m == 8 ? 8 * 16 * kPcWarps : 0;
 }
 
-static int launch_panel_cluster(float* a, int n, int k, int kb, int32_t* piv, int* info, int* swaps,
-                                cudaStream_t s) {
-    const bool small = cluster_panel_max() == 16;  // 8-row warps
+// The cluster panel at column k (kb columns, n - k <= cluster_panel_rows<T>() rows).
+template <typename T>
+static int launch_cluster_panel(T* a, int n, int k, int kb, int32_t* piv, int* info, int* swaps,
+                                const int* run_flag, cudaStream_t s) {
+    const bool small = cluster_panel_max<T>() == 16;  // 8-row warps
     const int per_cta = (small ? 8 : 16) * kPcWarps;
     const int nc = (n - k + per_cta - 1) / per_cta;
     cudaLaunchConfig_t cfg = {};
@@ -1048,9 +1116,15 @@ static int launch_panel_cluster(float* a, int n, int k, int kb, int32_t* piv, in
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    if (small) FJ_CUDA(cudaLaunchKernelEx(&cfg, lu_panel_cluster_kernel<8>, a, n, k, kb, piv, info, swaps));
-    else FJ_CUDA(cudaLaunchKernelEx(&cfg, lu_panel_cluster_kernel<16>, a, n, k, kb, piv, info, swaps));
+    if (small) FJ_CUDA(cudaLaunchKernelEx(&cfg, lu_panel_cluster_kernel<T, 8>, a, n, k, kb, piv, info, swaps, run_flag));
+    else FJ_CUDA(cudaLaunchKernelEx(&cfg, lu_panel_cluster_kernel<T, 16>, a, n, k, kb, piv, info, swaps, run_flag));
     note_launch();
+    return FJ_OK;
+}
+
+static int launch_panel_cluster(float* a, int n, int k, int kb, int32_t* piv, int* info, int* swaps,
+                                cudaStream_t s) {
+    FJ_TRY(launch_cluster_panel<float>(a, n, k, kb, piv, info, swaps, nullptr, s));
     lu_swap_rows_kernel<<<(unsigned)((n + 31) / 32), 256, 0, s>>>(a, n, k, kb, swaps);
     note_launch();
     return FJ_OK;
@@ -1076,7 +1150,7 @@ static int lu_factor32_tc_impl(float* a, int n, int32_t* piv, int* d_info, int* 
     FJ_TRY(allow_dynamic_smem((const void*)lu_panel_reg_kernel<float, NB, 2>, smem));
     FJ_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int), s));
     int* swaps = reinterpret_cast<int*>(tri_l + tc_inv_floats(n) + tc_scratch_floats(n));
-    const int cluster_rows = cluster_panel_rows();
+    const int cluster_rows = cluster_panel_rows<float>();
     for (int k = 0; k < n; k += kTcBlk) {
         const int kb = min(kTcBlk, n - k), ke = k + kb;
         if (n - k <= cluster_rows) {
@@ -1171,6 +1245,242 @@ int lu_inverse32_tc(const float* lu, int n, const int32_t* piv, float* x, float*
     return FJ_OK;
 }
 
+// ---------------------------------------------------------------------------------
+// FP64 factorisation (the plain path's getrf), blocked twice.  Outer panels of kDB = 64
+// columns; where a panel's rows fit one cluster (n - k <= cluster_panel_rows<double>())
+// one lu_panel_cluster_kernel<double> launch factors it, else 2- to 8-column panels do,
+// with their U rows and updates confined to the outer panel.  Then
+//   lu_swap_trsm64_kernel: the outer panel's row swaps for every column outside it, and
+//                          U12 = L11^-1 A12 for the columns to its right;
+//   lu_gemm64_kernel:      A22 -= L21 U12 (K = 64, FP64 FMA).
+// Pivots are getrf's (first maximum of the column below the diagonal); the trailing
+// matrix is updated once per 64 columns instead of once per column, so the factors
+// differ from a column-by-column getrf only by rounding.
+constexpr int kDB = 64;
+
+// The composed row moves of the outer panel at column k, from its kb pivots applied in
+// order (getrf's laswp): map[i] = the panel row whose values end at panel row i.  A move
+// lands on a row < k + kb, or on a pivot row at or below k + kb.  For the columns outside
+// the panel each CTA (32 columns, one per lane) loads every moved value before it stores
+// any.  Then, for the CTA's columns right of the panel, the kb x kb unit-lower L11 solves
+// its rows k .. k + kb: warp w takes columns 4w .. 4w + 3, lane l rows l and l + 32.
+__global__ void __launch_bounds__(256)
+    lu_swap_trsm64_kernel(double* __restrict__ a, int n, int k, int kb, const int32_t* __restrict__ piv,
+                          int do_swaps, const int* __restrict__ run_flag) {
+    if (run_flag != nullptr && *run_flag == 0) return;
+    extern __shared__ __align__(16) unsigned char sm64[];
+    double* tile = reinterpret_cast<double*>(sm64);            // [2 kDB][32] moved values; then x [kDB][33]
+    double* ls = tile + 2 * kDB * 33;                          // [kDB][kDB + 1] L11
+    int* map = reinterpret_cast<int*>(ls + kDB * (kDB + 1));  // [n - k]
+    __shared__ int s_dst[2 * kDB], s_src[2 * kDB];
+    __shared__ int s_cnt;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int rows = n - k, c0 = blockIdx.x * 32, c = c0 + lane;
+    if (do_swaps) {
+        for (int i = threadIdx.x; i < rows; i += blockDim.x) map[i] = i;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int j = 0; j < kb; ++j) {
+                const int p = piv[k + j] - k;
+                if (p != j && p > j && p < rows) {
+                    const int t = map[j];
+                    map[j] = map[p];
+                    map[p] = t;
+                }
+            }
+        }
+        __syncthreads();
+        if (warp == 0) {  // the moves, listed: rows [0, kb), then the pivot rows at or below kb
+            int base = 0;
+            for (int e0 = 0; e0 < 2 * kb; e0 += 32) {
+                const int e = e0 + lane;
+                int pos = -1;
+                if (e < kb) {
+                    pos = e;
+                } else if (e < 2 * kb) {
+                    const int p = piv[k + e - kb] - k;
+                    if (p >= kb && p < rows) pos = p;
+                }
+                const bool mv = pos >= 0 && map[pos] != pos;
+                const unsigned m = __ballot_sync(full, mv);
+                if (mv) {
+                    const int o = base + __popc(m & ((1u << lane) - 1u));
+                    s_dst[o] = k + pos;
+                    s_src[o] = k + map[pos];
+                }
+                base += __popc(m);
+            }
+            if (lane == 0) s_cnt = base;
+        }
+        __syncthreads();
+        const int cnt = s_cnt;
+        const bool col = c < n && (c < k || c >= k + kb);
+        for (int e = warp; e < cnt; e += 8)
+            if (col) tile[e * 32 + lane] = a[(int64_t)s_src[e] * n + c];
+        __syncthreads();
+        for (int e = warp; e < cnt; e += 8)
+            if (col) a[(int64_t)s_dst[e] * n + c] = tile[e * 32 + lane];
+        __syncthreads();  // the CTA's stores are seen by its loads below
+    }
+    if (c0 + 31 < k + kb || kb < 2) return;  // no column right of the panel (uniform over the CTA)
+    for (int idx = threadIdx.x; idx < kDB * kDB; idx += blockDim.x) {
+        const int r = idx / kDB, j = idx % kDB;
+        ls[r * (kDB + 1) + j] = (r < kb && j < r) ? a[(int64_t)(k + r) * n + k + j] : 0.0;
+    }
+    double* xs = tile;
+    for (int idx = threadIdx.x; idx < kDB * 32; idx += blockDim.x) {
+        const int r = idx >> 5, cc = idx & 31, cg_ = c0 + cc;
+        xs[r * 33 + cc] = (r < kb && cg_ >= k + kb && cg_ < n) ? a[(int64_t)(k + r) * n + cg_] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int t = 0; t < 4; ++t) {
+        const int cc = warp * 4 + t;
+        double x0 = xs[lane * 33 + cc], x1 = xs[(lane + 32) * 33 + cc];
+#pragma unroll 4
+        for (int j = 0; j < kb - 1; ++j) {
+            const double xj = __shfl_sync(full, j < 32 ? x0 : x1, j & 31);
+            if (lane > j) x0 -= ls[lane * (kDB + 1) + j] * xj;
+            x1 -= ls[(lane + 32) * (kDB + 1) + j] * xj;  // rows >= kb: zero multipliers
+        }
+        xs[lane * 33 + cc] = x0;
+        xs[(lane + 32) * 33 + cc] = x1;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kDB * 32; idx += blockDim.x) {
+        const int r = idx >> 5, cc = idx & 31, cg_ = c0 + cc;
+        if (r >= 1 && r < kb && cg_ >= k + kb && cg_ < n) a[(int64_t)(k + r) * n + cg_] = xs[r * 33 + cc];
+    }
+}
+
+constexpr size_t kSwapTrsm64Fixed = (size_t)(2 * kDB * 33 + kDB * (kDB + 1)) * sizeof(double);
+
+// A22 -= L21 U12 with K = kDB, on one 64 x 64 tile of the trailing matrix per CTA: the
+// CTA's 64 rows of L21 and 64 columns of U12 come into shared memory (cp.async, zero past
+// the matrix), then thread (tx, ty) updates rows ty + 16 p and columns tx + 16 q (p, q < 4)
+// with the 64 products in order, as the column-by-column update would.
+__global__ void __launch_bounds__(256)
+    lu_gemm64_kernel(double* __restrict__ a, int n, int k, const int* __restrict__ run_flag) {
+    if (run_flag != nullptr && *run_flag == 0) return;
+    extern __shared__ __align__(16) unsigned char smg64[];
+    double* as = reinterpret_cast<double*>(smg64);  // [64][kDB]: L21 rows
+    double* bs = as + 64 * kDB;                      // [kDB][64]: U12 columns
+    const int k2 = k + kDB;
+    const int r0 = k2 + blockIdx.y * 64, c0 = k2 + blockIdx.x * 64;
+    for (int idx = threadIdx.x; idx < 64 * kDB; idx += blockDim.x) {
+        const int r = idx / kDB, j = idx % kDB;
+        const bool oka = r0 + r < n;
+        const double* srca = a + (int64_t)(oka ? r0 + r : 0) * n + k + j;
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"((unsigned)__cvta_generic_to_shared(as + idx)),
+                     "l"(srca), "r"(oka ? 8 : 0)
+                     : "memory");
+        const int jb = idx / 64, cb = idx % 64;
+        const bool okb = c0 + cb < n;
+        const double* srcb = a + (int64_t)(k + jb) * n + (okb ? c0 + cb : 0);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"((unsigned)__cvta_generic_to_shared(bs + idx)),
+                     "l"(srcb), "r"(okb ? 8 : 0)
+                     : "memory");
+    }
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    double acc[4][4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = r0 + ty + 16 * p, cc = c0 + tx + 16 * q;
+            acc[p][q] = (r < n && cc < n) ? a[(int64_t)r * n + cc] : 0.0;
+        }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+#pragma unroll 8
+    for (int j = 0; j < kDB; ++j) {
+        double ar[4], br[4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) ar[p] = as[(ty + 16 * p) * kDB + j];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) br[q] = bs[j * 64 + tx + 16 * q];
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[p][q] -= ar[p] * br[q];
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = r0 + ty + 16 * p, cc = c0 + tx + 16 * q;
+            if (r < n && cc < n) a[(int64_t)r * n + cc] = acc[p][q];
+        }
+}
+
+constexpr size_t kGemm64Smem = (size_t)2 * 64 * kDB * sizeof(double);
+
+// The outer panel at column k in NB-column panels (rows beyond one cluster): swaps over
+// every column, U rows and updates inside the outer panel [k, ke).
+template <int NB>
+static int lu_outer_panel_narrow64(double* a, int n, int k, int ke, int32_t* piv, int* d_info, const int* run_flag,
+                                   cudaStream_t s) {
+    const size_t smem = (size_t)n * (NB + 1) * sizeof(double);
+    FJ_TRY(allow_dynamic_smem((const void*)lu_panel_kernel<double, NB>, smem));
+    FJ_TRY(allow_dynamic_smem((const void*)lu_panel_reg_kernel<double, NB, 1>, smem));
+    FJ_TRY(allow_dynamic_smem((const void*)lu_panel_reg_kernel<double, NB, 2>, smem));
+    for (int j = k; j < ke; j += NB) {
+        const int nb = min(NB, n - j);
+        launch_panel<double, NB>(a, n, j, piv, d_info, run_flag, s);
+        if (n > nb) {
+            lu_swap_trsm_kernel<double, NB><<<(n + 255) / 256, 256, 0, s>>>(a, n, j, piv, ke, run_flag);
+            note_launch();
+        }
+        const int rows = n - j - nb, cols = ke - j - nb;
+        if (nb == NB && rows > 0 && cols > 0) {
+            lu_update_kernel<double, NB><<<dim3((cols + 63) / 64, (rows + 63) / 64), 256, 0, s>>>(a, n, j, ke, run_flag);
+            note_launch();
+        }
+    }
+    return FJ_OK;
+}
+
+int lu_factor64(double* a, int n, int32_t* piv, int* d_info, cudaStream_t s, const int* run_flag) {
+    if (n <= 0) return fail(FJ_ERR_SHAPE, "lu_factor: n=%d", n);
+    int nb_narrow = 0;
+    for (int nb : {8, 4, 2})
+        if (nb_narrow == 0 && panel_fits<double>(n, nb)) nb_narrow = nb;
+    const int cluster_rows = cluster_panel_rows<double>();
+    if (nb_narrow == 0 && n > cluster_rows)
+        return fail(FJ_ERR_UNSUPPORTED, "lu_factor: n=%d too large for the shared-memory panel", n);
+    const size_t st_smem = kSwapTrsm64Fixed + (size_t)n * sizeof(int);
+    FJ_TRY(allow_dynamic_smem((const void*)lu_swap_trsm64_kernel, st_smem));
+    FJ_TRY(allow_dynamic_smem((const void*)lu_gemm64_kernel, kGemm64Smem));
+    FJ_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int), s));
+    for (int k = 0; k < n; k += kDB) {
+        const int kb = min(kDB, n - k), ke = k + kb;
+        const bool cluster = n - k <= cluster_rows;
+        if (cluster) {
+            FJ_TRY(launch_cluster_panel<double>(a, n, k, kb, piv, d_info, nullptr, run_flag, s));
+        } else if (nb_narrow == 8) {
+            FJ_TRY(lu_outer_panel_narrow64<8>(a, n, k, ke, piv, d_info, run_flag, s));
+        } else if (nb_narrow == 4) {
+            FJ_TRY(lu_outer_panel_narrow64<4>(a, n, k, ke, piv, d_info, run_flag, s));
+        } else {
+            FJ_TRY(lu_outer_panel_narrow64<2>(a, n, k, ke, piv, d_info, run_flag, s));
+        }
+        if (n > kb) {
+            lu_swap_trsm64_kernel<<<(unsigned)((n + 31) / 32), 256, st_smem, s>>>(a, n, k, kb, piv, cluster ? 1 : 0,
+                                                                                    run_flag);
+            note_launch();
+        }
+        const int rest = n - ke;
+        if (rest > 0) {  // kb == kDB here
+            lu_gemm64_kernel<<<dim3((unsigned)((rest + 63) / 64), (unsigned)((rest + 63) / 64)), 256, kGemm64Smem, s>>>(
+                a, n, k, run_flag);
+            note_launch();
+        }
+    }
+    FJ_LAUNCH_CHECK("lu_factor64");
+    return FJ_OK;
+}
+
 // Factor path of the mixed solve.  FJ_MIXED_FACTOR selects it: "cuda" (FP32 CUDA cores),
 // "tf32" (tensor cores, one TF32 pass) or the default "tf32x3" (three-pass split); the
 // tensor-core paths apply from n >= kTcMinN.
@@ -1210,16 +1520,73 @@ int convert64to32(const double* a, float* b, int64_t count, cudaStream_t s) {
 // Refinement GEMVs: one warp per row, FP64 accumulation.
 //   mode 0: y = X v        mode 1: y += X v        (X FP32)
 //   residual: r = b - A x  (A FP64)
+// Row dot products of the refinement (HBM-bound: one pass over the matrix row).  A warp
+// takes a row; where the row and the vector are 16-byte aligned and n a multiple of 4 (2
+// for FP64 rows) each lane loads whole 16-byte vectors, four in flight, into four
+// independent FP64 partial sums; else element by element.  The warp's sum comes back in
+// every lane.
+__device__ __forceinline__ double warp_sum(double a) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+    return a;
+}
+
+__device__ __forceinline__ double row_dot32(const float* __restrict__ xr, const double* __restrict__ v, int n,
+                                            int lane) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    if ((n & 3) == 0 && (((uintptr_t)xr | (uintptr_t)v) & 15) == 0) {
+        const float4* x4 = reinterpret_cast<const float4*>(xr);
+        const double2* v2 = reinterpret_cast<const double2*>(v);
+        const int n4 = n >> 2;
+#pragma unroll 4
+        for (int j = lane; j < n4; j += 32) {
+            const float4 x = __ldg(x4 + j);
+            const double2 p = v2[2 * j], q = v2[2 * j + 1];
+            a0 = fma((double)x.x, p.x, a0);
+            a1 = fma((double)x.y, p.y, a1);
+            a2 = fma((double)x.z, q.x, a2);
+            a3 = fma((double)x.w, q.y, a3);
+        }
+    } else {
+        for (int j = lane; j < n; j += 32) a0 = fma((double)xr[j], v[j], a0);
+    }
+    return warp_sum((a0 + a1) + (a2 + a3));
+}
+
+__device__ __forceinline__ double row_dot64(const double* __restrict__ ar, const double* __restrict__ x, int n,
+                                            int lane) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    if ((n & 1) == 0 && (((uintptr_t)ar | (uintptr_t)x) & 15) == 0) {
+        const double2* r2 = reinterpret_cast<const double2*>(ar);
+        const double2* x2 = reinterpret_cast<const double2*>(x);
+        const int n2 = n >> 1;
+        int j = lane;
+#pragma unroll 2
+        for (; j + 32 < n2; j += 64) {
+            const double2 p = __ldg(r2 + j), q = __ldg(r2 + j + 32);
+            const double2 u = x2[j], w = x2[j + 32];
+            a0 = fma(p.x, u.x, a0);
+            a1 = fma(p.y, u.y, a1);
+            a2 = fma(q.x, w.x, a2);
+            a3 = fma(q.y, w.y, a3);
+        }
+        if (j < n2) {
+            const double2 p = __ldg(r2 + j), u = x2[j];
+            a0 = fma(p.x, u.x, a0);
+            a1 = fma(p.y, u.y, a1);
+        }
+    } else {
+        for (int j = lane; j < n; j += 32) a0 = fma(ar[j], x[j], a0);
+    }
+    return warp_sum((a0 + a1) + (a2 + a3));
+}
+
 __global__ void gemv32_kernel(const float* __restrict__ X, const double* __restrict__ v, int n,
                               double* __restrict__ y, int accumulate) {
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (row >= n) return;
-    const float* xr = X + (int64_t)row * n;
-    double acc = 0.0;
-    for (int j = lane; j < n; j += 32) acc += (double)xr[j] * v[j];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    const double acc = row_dot32(X + (int64_t)row * n, v, n, lane);
     if (lane == 0) y[row] = accumulate ? y[row] + acc : acc;
 }
 
@@ -1228,11 +1595,7 @@ __global__ void residual64_kernel(const double* __restrict__ A, const double* __
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (row >= n) return;
-    const double* ar = A + (int64_t)row * n;
-    double acc = 0.0;
-    for (int j = lane; j < n; j += 32) acc += ar[j] * x[j];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    const double acc = row_dot64(A + (int64_t)row * n, x, n, lane);
     if (lane == 0) r[row] = b[row] - acc;
 }
 
@@ -1286,12 +1649,7 @@ __global__ void gemv32_jobs_kernel(const RefineJob* __restrict__ jobs, int from_
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (row >= J.n) return;
-    const float* xr = J.xinv + (int64_t)row * J.n;
-    const double* v = from_residual ? J.r : J.b;
-    double acc = 0.0;
-    for (int j = lane; j < J.n; j += 32) acc += (double)xr[j] * v[j];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    const double acc = row_dot32(J.xinv + (int64_t)row * J.n, from_residual ? J.r : J.b, J.n, lane);
     if (lane == 0) J.x[row] = accumulate ? J.x[row] + acc : acc;
 }
 
@@ -1300,11 +1658,7 @@ __global__ void residual64_jobs_kernel(const RefineJob* __restrict__ jobs) {
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (row >= J.n) return;
-    const double* ar = J.a + (int64_t)row * J.n;
-    double acc = 0.0;
-    for (int j = lane; j < J.n; j += 32) acc += ar[j] * J.x[j];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    const double acc = row_dot64(J.a + (int64_t)row * J.n, J.x, J.n, lane);
     if (lane == 0) J.r[row] = J.b[row] - acc;
 }
 

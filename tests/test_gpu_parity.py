@@ -232,7 +232,9 @@ def test_lu_factor_solve_and_mixed(cuda):
     from flapjax_b200 import _lib
 
     rng = np.random.default_rng(4)
-    for n in (1, 7, 64, 333, 1000):
+    # orders below, at and across the 64-column outer panel, and one whose first panels have
+    # more rows than one thread-block cluster holds (2048)
+    for n in (1, 7, 64, 65, 333, 1000, 2100):
         a = rng.normal(size=(n, n)) + n * 0.05 * np.eye(n)
         b = rng.normal(size=n)
         want = np.linalg.solve(a, b)
@@ -249,8 +251,11 @@ def test_lu_factor_solve_and_mixed(cuda):
         # pivots follow LAPACK getrf
         import scipy.linalg
 
-        _, piv_ref = scipy.linalg.lu_factor(a)
+        lu_ref, piv_ref = scipy.linalg.lu_factor(a)
         assert np.array_equal(piv.cpu().numpy(), piv_ref)
+        # the factors themselves, to rounding (blocked updates sum in another order)
+        _lib.call("fj_lu_factor", ta.copy_(_t(a, cuda)).data_ptr(), n, piv.data_ptr(), ws.data_ptr(), ws.numel(), s)
+        assert rel_err(ta.cpu().numpy(), lu_ref) < 1e-11
         # mixed: FP32 factors + FP64 refinement
         nbytes = C.c_size_t()
         _lib.call("fj_solve_mixed_workspace_size", n, C.byref(nbytes))
