@@ -660,13 +660,13 @@ int lu_inverse32(const float* lu, int n, const int32_t* piv, float* x, cudaStrea
 // ---------------------------------------------------------------------------------
 // Tensor-core factorisation and inverse (mixed path, n >= kTcMinN).
 //
-// lu_factor32_tc: the same partial-pivoting LU, blocked twice.  Inside an outer panel of
-// 128 columns the 16-column panels run as above (row swaps over all columns), with their
-// U rows and updates confined to the outer panel.  The columns to its right receive only
-// the row swaps until the outer panel is done; then, with L11^-1 (tri_inverse32_blocks),
-//   U12 = L11^-1 A12        (tensor cores; in place, one 128-row tile)
+// lu_factor32_tc: the same partial-pivoting LU, blocked twice.  One thread-block cluster
+// factors each outer panel of 128 columns (lu_panel_cluster_kernel; the 16-column panels
+// above where the rows exceed one cluster, their U rows and updates confined to the outer
+// panel).  The columns to its right receive only the row swaps until the outer panel is
+// done; then
+//   U12 = L11^-1 A12        (lu_trsm32_kernel: forward substitution, CUDA cores, in place)
 //   A22 -= L21 U12          (tensor cores, K = 128)
-// L11^-1 of every outer panel is kept for the inverse.
 //
 // lu_inverse32_tc: X = U^-1 L^-1 P by blocked substitution on the n x n right-hand side
 // P (the getrf row swaps applied to the identity), 128 rows at a time:
@@ -1130,6 +1130,60 @@ static int launch_panel_cluster(float* a, int n, int k, int kb, int32_t* piv, in
     return FJ_OK;
 }
 
+// U12 = L11^-1 A12 for the mixed factorisation's outer panel at column k (kb <= 128
+// rows, L11 unit lower from the factored panel), in place on the columns [c0, n).  A CTA
+// takes 16 columns: L11 and the columns' panel rows come into shared memory (coalesced),
+// then warp w substitutes columns 2w and 2w + 1, lane l holding rows l + 32 q (q < 4) in
+// registers, each x_j reaching every lane by a shuffle.  Forward substitution in FP32,
+// as the CUDA-core path's lu_swap_trsm_kernel computes its U rows.
+constexpr int kTrsmCols = 16;
+constexpr size_t kTrsm32Smem = (size_t)(kTcBlk * (kTcBlk + 1) + kTcBlk * (kTrsmCols + 1)) * sizeof(float);
+
+__device__ __forceinline__ float pick4f(const float (&v)[4], int q) {
+    return q == 0 ? v[0] : q == 1 ? v[1] : q == 2 ? v[2] : v[3];
+}
+
+__global__ void __launch_bounds__(256) lu_trsm32_kernel(float* __restrict__ a, int n, int k, int kb, int c0) {
+    extern __shared__ __align__(16) float smt[];
+    float* ls = smt;                               // [128][129]
+    float* xs = smt + kTcBlk * (kTcBlk + 1);       // [128][17]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int cb = c0 + blockIdx.x * kTrsmCols;
+    for (int idx = threadIdx.x; idx < kTcBlk * kTcBlk; idx += blockDim.x) {
+        const int r = idx >> 7, j = idx & 127;
+        ls[r * (kTcBlk + 1) + j] = (r < kb && j < r) ? a[(int64_t)(k + r) * n + k + j] : 0.0f;
+    }
+    for (int idx = threadIdx.x; idx < kTcBlk * kTrsmCols; idx += blockDim.x) {
+        const int r = idx / kTrsmCols, cc = idx % kTrsmCols, col = cb + cc;
+        xs[r * (kTrsmCols + 1) + cc] = (r < kb && col < n) ? a[(int64_t)(k + r) * n + col] : 0.0f;
+    }
+    __syncthreads();
+    const unsigned full = 0xffffffffu;
+#pragma unroll 1
+    for (int t = 0; t < 2; ++t) {
+        const int cc = 2 * warp + t;
+        float x[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) x[q] = xs[(lane + 32 * q) * (kTrsmCols + 1) + cc];
+#pragma unroll 4
+        for (int j = 0; j < kb - 1; ++j) {
+            const float xj = __shfl_sync(full, pick4f(x, j >> 5), j & 31);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = lane + 32 * q;
+                if (r > j) x[q] -= ls[r * (kTcBlk + 1) + j] * xj;  // rows >= kb: zero multipliers
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) xs[(lane + 32 * q) * (kTrsmCols + 1) + cc] = x[q];
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kTcBlk * kTrsmCols; idx += blockDim.x) {
+        const int r = idx / kTrsmCols, cc = idx % kTrsmCols, col = cb + cc;
+        if (r >= 1 && r < kb && col < n) a[(int64_t)(k + r) * n + col] = xs[r * (kTrsmCols + 1) + cc];
+    }
+}
+
 // The factorisation's and the inverse's products: the TMA-fed tensor-core GEMM, its
 // operand split in the scratch that follows the diagonal-block inverses.
 static int tc_mul(const float* a, int lda, const float* b, int ldb, float* c, int ldc, int m, int n, int k,
@@ -1148,6 +1202,7 @@ static int lu_factor32_tc_impl(float* a, int n, int32_t* piv, int* d_info, int* 
     FJ_TRY(allow_dynamic_smem((const void*)lu_panel_kernel<float, NB>, smem));
     FJ_TRY(allow_dynamic_smem((const void*)lu_panel_reg_kernel<float, NB, 1>, smem));
     FJ_TRY(allow_dynamic_smem((const void*)lu_panel_reg_kernel<float, NB, 2>, smem));
+    FJ_TRY(allow_dynamic_smem((const void*)lu_trsm32_kernel, kTrsm32Smem));
     FJ_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int), s));
     int* swaps = reinterpret_cast<int*>(tri_l + tc_inv_floats(n) + tc_scratch_floats(n));
     const int cluster_rows = cluster_panel_rows<float>();
@@ -1170,13 +1225,11 @@ static int lu_factor32_tc_impl(float* a, int n, int32_t* piv, int* d_info, int* 
             }
           }
         }
-        const int b = k / kTcBlk;
-        float* linv = tri_l + (size_t)b * kTcBlk * kTcBlk;
-        FJ_TRY(tri_inverse32_blocks(a, n, b, 1, false, tri_l, s));
         const int rest = n - ke;
-        if (rest > 0) {
+        if (rest > 0) {  // U12 = L11^-1 A12 (CUDA cores), then A22 -= L21 U12 (tensor cores)
             float* a12 = a + (int64_t)k * n + ke;
-            FJ_TRY(tc_mul(linv, kTcBlk, a12, n, a12, n, kb, rest, kb, 1.0f, 0.0f, passes, tri_l, n, d_err, s));
+            lu_trsm32_kernel<<<(unsigned)((rest + kTrsmCols - 1) / kTrsmCols), 256, kTrsm32Smem, s>>>(a, n, k, kb, ke);
+            note_launch();
             FJ_TRY(tc_mul(a + (int64_t)ke * n + k, n, a12, n, a + (int64_t)ke * n + ke, n, rest, rest, kb, -1.0f, 1.0f,
                           passes, tri_l, n, d_err, s));
         }
@@ -1218,8 +1271,11 @@ __global__ void __launch_bounds__(1024) perm_identity_kernel(const int32_t* __re
 int lu_inverse32_tc(const float* lu, int n, const int32_t* piv, float* x, float* tri, int passes, int* d_err,
                     cudaStream_t s) {
     const int nblk = (n + kTcBlk - 1) / kTcBlk;
-    const float* tri_l = tri;  // from the factorisation
+    float* tri_l = tri;
     float* tri_u = tri + (size_t)nblk * kTcBlk * kTcBlk;
+    // the diagonal blocks' inverses, L's and U's, each set in one launch (a CTA per block);
+    // L's blocks are final once their panel is factored (later swaps touch lower rows only)
+    FJ_TRY(tri_inverse32_blocks(lu, n, 0, nblk, false, tri_l, s));
     FJ_TRY(tri_inverse32_blocks(lu, n, 0, nblk, true, tri_u, s));
     FJ_CUDA(cudaMemsetAsync(x, 0, (size_t)n * n * sizeof(float), s));
     FJ_TRY(allow_dynamic_smem((const void*)perm_identity_kernel, (size_t)2 * n * sizeof(int)));
