@@ -17,20 +17,23 @@
 
 namespace fj {
 
+// Per vertex one reciprocal square root and per link one division (1 / (4 pi D)); the
+// other quotients are products with these reciprocals (the FP64 divide and square root
+// are multi-instruction sequences on the FP64 pipe).
 struct VtxA {
     double d[3];  // x - y
     double u[3];  // d / n
-    double n;     // sqrt(|d|^2 + eps^2)
+    double rn;    // 1 / n, n = sqrt(|d|^2 + eps^2)
 };
 
 __device__ __forceinline__ void vtxa(const double x[3], double yx, double yy, double yz, VtxA& o) {
     o.d[0] = x[0] - yx;
     o.d[1] = x[1] - yy;
     o.d[2] = x[2] - yz;
-    o.n = sqrt(o.d[0] * o.d[0] + o.d[1] * o.d[1] + o.d[2] * o.d[2] + kEps * kEps);
-    o.u[0] = o.d[0] / o.n;
-    o.u[1] = o.d[1] / o.n;
-    o.u[2] = o.d[2] / o.n;
+    o.rn = rsqrt(o.d[0] * o.d[0] + o.d[1] * o.d[1] + o.d[2] * o.d[2] + kEps * kEps);
+    o.u[0] = o.d[0] * o.rn;
+    o.u[1] = o.d[1] * o.rn;
+    o.u[2] = o.d[2] * o.rn;
 }
 
 __device__ __forceinline__ void cross3(const double a[3], const double b[3], double o[3]) {
@@ -81,10 +84,10 @@ __device__ __forceinline__ void link_vjp(const VtxA& A, const VtxA& B, const dou
         dD1[k] = 2.0 * r2c[k] + e4 * r0[k];
         dD2[k] = 2.0 * cr1[k] - e4 * r0[k];
     }
-    const double q = dot / D;
+    const double q = kFourPi * s;  // dot / D
     for (int k = 0; k < 3; ++k) {
-        const double dd1 = du[k] + (r0[k] - r0u1 * A.u[k]) / A.n;
-        const double dd2 = -du[k] - (r0[k] - r0u2 * B.u[k]) / B.n;
+        const double dd1 = du[k] + (r0[k] - r0u1 * A.u[k]) * A.rn;
+        const double dd2 = -du[k] - (r0[k] - r0u2 * B.u[k]) * B.rn;
         g1[k] = g * (s * t1[k] + a * (dd1 - q * dD1[k]) * inv);
         g2[k] = g * (s * t2[k] + a * (dd2 - q * dD2[k]) * inv);
     }

@@ -861,7 +861,7 @@ __device__ __forceinline__ void panel_columns(T (&v)[RPW][PanelType<T>::NG], int
             S.wrow[par][warp] = rbase + bi;
             S.wsrc[par][warp] = bsrc;
         }
-        const bool holds_j = j >= rbase && j < rbase + RPW;  // CTA 0 (its rows cover the panel's columns)
+        const bool holds_j = j >= rbase && j < rbase + RPW;
         const int ij = j - rbase;
         const int jsrc = __shfl_sync(full, orig, holds_j ? ij : 0);
         if (holds_j) {
@@ -872,8 +872,9 @@ __device__ __forceinline__ void panel_columns(T (&v)[RPW][PanelType<T>::NG], int
             if (lane == 0) S.rowj_src_loc[par] = jsrc;
         }
         __syncthreads();
-        // b. push: warps 0-3 the CTA's candidate, warps 4-7 of CTA 0 row j; a row is 512
-        //    bytes, and thread t stores its float4 t % 32 into CTAs t / 32 % 4, + 4, + 8, + 12
+        // b. push: warps 0-3 the CTA's candidate, warps 4-7 of the CTA holding row j that
+        //    row; a row is 512 bytes, and thread t stores its float4 t % 32 into CTAs
+        //    t / 32 % 4, + 4, + 8, + 12
         if (warp < 8) {
             const int t = tid & 127, f = t & 31, c0 = t >> 5;
             if (warp < 4) {
@@ -896,7 +897,7 @@ __device__ __forceinline__ void panel_columns(T (&v)[RPW][PanelType<T>::NG], int
                         }
                     }
                 }
-            } else if (q == 0) {
+            } else if (q == j / (kPcWarps * RPW)) {
                 const float4 val = reinterpret_cast<const float4*>(S.rowj_loc[par])[f];
                 const int js = S.rowj_src_loc[par];
 #pragma unroll
@@ -1098,13 +1099,19 @@ static int cluster_panel_rows() {
     return m == 16 ? 16 * 8 * kPcWarps : m == 8 ? 8 * 16 * kPcWarps : 0;
 }
 
-// The cluster panel at column k (kb columns, n - k <= cluster_panel_rows<T>() rows).
-template <typename T>
-static int launch_cluster_panel(T* a, int n, int k, int kb, int32_t* piv, int* info, int* swaps,
-                                const int* run_flag, cudaStream_t s) {
-    const bool small = cluster_panel_max<T>() == 16;  // 8-row warps
-    const int per_cta = (small ? 8 : 16) * kPcWarps;
-    const int nc = (n - k + per_cta - 1) / per_cta;
+// One cluster panel launch with RPW rows per warp: nc CTAs of kPcWarps warps.
+template <typename T, int RPW>
+static int launch_cluster_rpw(T* a, int n, int k, int kb, int32_t* piv, int* info, int* swaps, const int* run_flag,
+                              int nc, cudaStream_t s) {
+    if (nc > 8) {  // non-portable cluster size: allowed once per instantiation
+        static std::once_flag once;
+        static cudaError_t e = cudaSuccess;
+        std::call_once(once, [] {
+            e = cudaFuncSetAttribute((const void*)lu_panel_cluster_kernel<T, RPW>,
+                                     cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        });
+        FJ_CUDA(e);
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)nc);
     cfg.blockDim = dim3(kPcThreads);
@@ -1116,10 +1123,30 @@ static int launch_cluster_panel(T* a, int n, int k, int kb, int32_t* piv, int* i
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    if (small) FJ_CUDA(cudaLaunchKernelEx(&cfg, lu_panel_cluster_kernel<T, 8>, a, n, k, kb, piv, info, swaps, run_flag));
-    else FJ_CUDA(cudaLaunchKernelEx(&cfg, lu_panel_cluster_kernel<T, 16>, a, n, k, kb, piv, info, swaps, run_flag));
+    FJ_CUDA(cudaLaunchKernelEx(&cfg, lu_panel_cluster_kernel<T, RPW>, a, n, k, kb, piv, info, swaps, run_flag));
     note_launch();
     return FJ_OK;
+}
+
+// The cluster panel at column k (kb columns, n - k <= cluster_panel_rows<T>() rows), with
+// the fewest rows per warp (2, 4, 8 or 16) whose cluster the device runs: a column's
+// serial work in a warp grows with its rows (8-CTA clusters of 16-row warps factor the
+// 2048-row AIC 18 % slower than 16-CTA clusters of 8-row warps).
+template <typename T>
+static int launch_cluster_panel(T* a, int n, int k, int kb, int32_t* piv, int* info, int* swaps,
+                                const int* run_flag, cudaStream_t s) {
+    const int max_nc = cluster_panel_max<T>();
+    const int rows = n - k;
+    int rpw = 2;
+    while (rpw < 16 && (rows + kPcWarps * rpw - 1) / (kPcWarps * rpw) > max_nc) rpw *= 2;
+    const int nc = (rows + kPcWarps * rpw - 1) / (kPcWarps * rpw);
+    if (nc > max_nc || nc < 1) return fail(FJ_ERR_UNSUPPORTED, "cluster panel: %d rows", rows);
+    switch (rpw) {
+        case 2: return launch_cluster_rpw<T, 2>(a, n, k, kb, piv, info, swaps, run_flag, nc, s);
+        case 4: return launch_cluster_rpw<T, 4>(a, n, k, kb, piv, info, swaps, run_flag, nc, s);
+        case 8: return launch_cluster_rpw<T, 8>(a, n, k, kb, piv, info, swaps, run_flag, nc, s);
+        default: return launch_cluster_rpw<T, 16>(a, n, k, kb, piv, info, swaps, run_flag, nc, s);
+    }
 }
 
 static int launch_panel_cluster(float* a, int n, int k, int kb, int32_t* piv, int* info, int* swaps,

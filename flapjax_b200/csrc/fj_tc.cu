@@ -543,36 +543,44 @@ __global__ void __launch_bounds__(kTmaThreads, 1)
     }
 }
 
-// hi (and lo) TF32 copies of A (m x k, lda) as (m x kp), columns k..kp zero.
-__global__ void tc_split_rows_kernel(const float* __restrict__ a, int lda, int m, int k, int kp, float* __restrict__ hi,
-                                     float* __restrict__ lo) {
-    const int64_t total = (int64_t)m * kp;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int r = (int)(i / kp), cc = (int)(i % kp);
-        const float v = cc < k ? a[(int64_t)r * lda + cc] : 0.0f;
-        const float h = tf32_hi(v);
-        hi[i] = h;
-        if (lo) lo[i] = v - h;
+// hi (and lo) TF32 copies of both operands in one launch.  CTAs [0, n_row_ctas): A (m x k,
+// lda) as (m x kp), columns k..kp zero, grid-stride.  The rest: B (k x n, ldb) transposed
+// to (n x kp), one 32 x 32 tile per CTA through shared memory (tile t: columns
+// 32 (t % tiles_n), rows 32 (t / tiles_n) of B).
+__global__ void __launch_bounds__(256) tc_split_kernel(const float* __restrict__ a, int lda, int m,
+                                                       const float* __restrict__ b, int ldb, int n, int k, int kp,
+                                                       float* __restrict__ a_hi, float* __restrict__ a_lo,
+                                                       float* __restrict__ b_hi, float* __restrict__ b_lo,
+                                                       int n_row_ctas) {
+    if ((int)blockIdx.x < n_row_ctas) {
+        const int64_t total = (int64_t)m * kp;
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+             i += (int64_t)n_row_ctas * blockDim.x) {
+            const int r = (int)(i / kp), cc = (int)(i % kp);
+            const float v = cc < k ? a[(int64_t)r * lda + cc] : 0.0f;
+            const float h = tf32_hi(v);
+            a_hi[i] = h;
+            if (a_lo) a_lo[i] = v - h;
+        }
+        return;
     }
-}
-
-// hi (and lo) TF32 copies of B (k x n, ldb) transposed, (n x kp), through 32 x 32 tiles.
-__global__ void tc_split_cols_kernel(const float* __restrict__ b, int ldb, int k, int n, int kp, float* __restrict__ hi,
-                                     float* __restrict__ lo) {
     __shared__ float t[32][33];
-    const int j0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
-    for (int r = threadIdx.y; r < 32; r += blockDim.y) {  // rows of B: k0 + r, columns j0 + tx
-        const int kk = k0 + r, j = j0 + threadIdx.x;
-        t[r][threadIdx.x] = (kk < k && j < n) ? b[(int64_t)kk * ldb + j] : 0.0f;
+    const int tiles_n = (n + 31) / 32;
+    const int tile = (int)blockIdx.x - n_row_ctas;
+    const int j0 = (tile % tiles_n) * 32, k0 = (tile / tiles_n) * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int r = ty; r < 32; r += 8) {  // rows of B: k0 + r, columns j0 + tx
+        const int kk = k0 + r, j = j0 + tx;
+        t[r][tx] = (kk < k && j < n) ? b[(int64_t)kk * ldb + j] : 0.0f;
     }
     __syncthreads();
-    for (int r = threadIdx.y; r < 32; r += blockDim.y) {  // rows of the copy: j0 + r, columns k0 + tx
-        const int j = j0 + r, kk = k0 + threadIdx.x;
+    for (int r = ty; r < 32; r += 8) {  // rows of the copy: j0 + r, columns k0 + tx
+        const int j = j0 + r, kk = k0 + tx;
         if (j < n) {
-            const float v = t[threadIdx.x][r];
+            const float v = t[tx][r];
             const float h = tf32_hi(v);
-            hi[(int64_t)j * kp + kk] = h;
-            if (lo) lo[(int64_t)j * kp + kk] = v - h;
+            b_hi[(int64_t)j * kp + kk] = h;
+            if (b_lo) b_lo[(int64_t)j * kp + kk] = v - h;
         }
     }
 }
@@ -643,11 +651,10 @@ int tc_gemm_tf32_tma(const float* a, int lda, const float* b, int ldb, float* c,
     float* b_hi = a_hi + (size_t)m * kp * (split ? 2 : 1);
     float* b_lo = split ? b_hi + (size_t)n * kp : nullptr;
     const int64_t ta = (int64_t)m * kp;
-    tc_split_rows_kernel<<<(unsigned)std::min<int64_t>((ta + 255) / 256, 148 * 8), 256, 0, s>>>(a, lda, m, k, kp,
-                                                                                                a_hi, a_lo);
-    note_launch();
-    tc_split_cols_kernel<<<dim3((unsigned)((n + 31) / 32), (unsigned)(kp / 32)), dim3(32, 8), 0, s>>>(b, ldb, k, n,
-                                                                                                      kp, b_hi, b_lo);
+    const int row_ctas = (int)std::min<int64_t>((ta + 255) / 256, 148 * 4);
+    const int col_ctas = ((n + 31) / 32) * (kp / 32);
+    tc_split_kernel<<<(unsigned)(row_ctas + col_ctas), 256, 0, s>>>(a, lda, m, b, ldb, n, k, kp, a_hi, a_lo, b_hi, b_lo,
+                                                                   row_ctas);
     note_launch();
     CUtensorMap mah, mal, mbh, mbl;
     // rows are 16-byte multiples (kp x 4 bytes) and every box starts at a multiple of 32 floats
