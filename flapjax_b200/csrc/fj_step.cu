@@ -1155,9 +1155,16 @@ __global__ void k_keep_lattice(const StepCase* __restrict__ C, double* __restric
 
 // Graph-replayed steps: copy the table of slot *ctr into the fixed table area, and
 // advance *ctr after the step.
+// The slot counter is checked against the slot count the graph was captured with: out of
+// range, nothing is copied and *bad (a status word) is set.
 __global__ void k_select_table(const char* __restrict__ all, size_t stride, const int* __restrict__ ctr,
-                               char* __restrict__ tab) {
-    const int4* src = reinterpret_cast<const int4*>(all + (size_t)(*ctr) * stride);
+                               int n_slots, char* __restrict__ tab, int* __restrict__ bad) {
+    const int c = *ctr;
+    if (c < 0 || c >= n_slots) {
+        if (threadIdx.x == 0 && blockIdx.x == 0) *bad = 1;
+        return;
+    }
+    const int4* src = reinterpret_cast<const int4*>(all + (size_t)c * stride);
     int4* dst = reinterpret_cast<int4*>(tab);
     for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < stride / 16; w += (size_t)gridDim.x * blockDim.x)
         dst[w] = src[w];
@@ -1776,18 +1783,20 @@ static int check_buffers(const Plan& p, const fj_case_buffers* B, bool dynamic) 
 
 // Status words of a case-level call: flags[0] the LU info of the last factorisation
 // (first zero pivot + 1), flags[2] the lowest slot with a non-finite total force,
-// flags[3] set when a bounded wait of the tensor-core factorisation expired.
+// flags[3] set when a bounded wait of the tensor-core factorisation expired, flags[4] set
+// when a replayed step graph found its slot counter out of range.
 static constexpr int kNoSlot = 0x7f7f7f7f;  // the byte pattern 0x7f repeated
 
 static int clear_status(const Plan& p, cudaStream_t s) {
-    FJ_CUDA(cudaMemsetAsync(p.flags + 3, 0, sizeof(int), s));
+    FJ_CUDA(cudaMemsetAsync(p.flags + 3, 0, 2 * sizeof(int), s));
     return cuda_status(cudaMemsetAsync(p.flags + 2, 0x7f, sizeof(int), s), "status reset");
 }
 
 static int read_status(const Plan& p, cudaStream_t s) {
-    int w[4] = {0, 0, 0, 0};
+    int w[5] = {0, 0, 0, 0, 0};
     FJ_CUDA(cudaMemcpyAsync(w, p.flags, sizeof(w), cudaMemcpyDeviceToHost, s));
     FJ_CUDA(cudaStreamSynchronize(s));
+    if (w[4] != 0) return fail(FJ_ERR_CUDA, "a replayed step graph found its slot counter out of range");
     if (w[3] != 0) return fail(FJ_ERR_TIMEOUT, "a tensor-core wait of the AIC factorisation expired");
     if (w[2] != kNoSlot) return fail(FJ_ERR_NONFINITE, "non-finite forces at time slot %d", w[2]);
     if (w[0] != 0) return fail(FJ_ERR_SINGULAR, "zero pivot in column %d of the AIC factorisation", w[0] - 1);
@@ -1837,6 +1846,14 @@ static int run_range_graph(const Plan& p, const fj_case_buffers* B, int g0, int 
         FJ_TRY(run_steps(one, p.tab, p.tab_bytes, s, kStepBuild, h.data() + (size_t)(k - g0) * p.tab_bytes,
                          k == g0 ? &sig : nullptr));
     }
+    // the graph's own select and advance kernels take the slot tables, the counter and a
+    // status word: the counter's place in the workspace follows the slot count, so a
+    // workspace at the same address for a case of another length must not replay this graph
+    sig.push_back((int64_t)(uintptr_t)p.tab_all);
+    sig.push_back((int64_t)(uintptr_t)p.step_ctr);
+    sig.push_back((int64_t)(uintptr_t)p.flags);
+    sig.push_back((int64_t)p.tab_bytes);
+    sig.push_back((int64_t)p.cfg.n_tstep);
     FJ_TRY(upload(p.tab_all + (size_t)g0 * p.tab_bytes, h.data(), h.size(), s));
     FJ_TRY(upload(p.step_ctr, &g0, sizeof(int), s));
 
@@ -1851,7 +1868,8 @@ static int run_range_graph(const Plan& p, const fj_case_buffers* B, int g0, int 
         const int64_t launches0 = launch_count();
         int st = cuda_status(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "step graph capture");
         if (st == FJ_OK) {
-            k_select_table<<<32, 256, 0, cs>>>(p.tab_all, p.tab_bytes, p.step_ctr, p.tab); note_launch();
+            k_select_table<<<32, 256, 0, cs>>>(p.tab_all, p.tab_bytes, p.step_ctr, p.cfg.n_tstep, p.tab, p.flags + 4);
+            note_launch();
             std::vector<BatchItem> one(1, step_item(p, B, g0, false));
             st = run_steps(one, p.tab, p.tab_bytes, cs, kStepLaunch);
             k_advance<<<1, 32, 0, cs>>>(p.step_ctr); note_launch();

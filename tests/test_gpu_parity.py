@@ -426,3 +426,35 @@ def test_cached_step_graph_across_calls(cuda, precision):
     for f in ("gamma_b", "gamma_w", "zeta_w", "f_steady", "f_unsteady", "gamma_b_dot", "alpha"):
         assert np.array_equal(a[f], b[f]), f
         assert np.array_equal(b[f], b2[f]), f
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_cached_step_graph_not_replayed_for_another_length(cuda, precision):
+    """A shorter case on the workspace of a longer one (the same address, as a caching
+    allocator hands out after a free) has the same step table address but its slot counter
+    elsewhere: it captures its own step graph.  Its slots equal a direct-launch run on a
+    workspace of its own, bit for bit.  The longer case stays alive, so its graph's
+    pointers stay valid memory whatever is replayed."""
+    import torch
+
+    long_c = cases.wing_free(m=4, n=10, m_star=12, n_steps=20)
+    short_c = cases.wing_free(m=4, n=10, m_star=12, n_steps=10)
+    uv, _ = device_uvlm(long_c, precision)
+    dl = uv.make_device_case(long_c.n_tstep)
+    uv.load_initial(dl, uv.solve_static())
+    dl.set_hg(long_c.hg_t, long_c.hg_dot_t)
+    dl.solve_dynamic(1, long_c.n_tstep, graph=True)
+    got = []
+    for shared in (True, False):
+        uv_s, _ = device_uvlm(short_c, precision)
+        ds = uv_s.make_device_case(short_c.n_tstep)
+        if shared:
+            assert ds.ws.numel() <= dl.ws.numel()
+            ds.ws = dl.ws[: ds.ws.numel()]
+        uv_s.load_initial(ds, uv_s.solve_static())
+        ds.set_hg(short_c.hg_t, short_c.hg_dot_t)
+        ds.solve_dynamic(1, short_c.n_tstep, graph=shared)
+        torch.cuda.synchronize()
+        got.append(ds.host_arrays())
+    for f in ("gamma_b", "gamma_w", "zeta_w", "f_steady", "f_unsteady", "gamma_b_dot", "alpha"):
+        assert np.array_equal(got[0][f], got[1][f]), f
