@@ -1,7 +1,10 @@
 // fj_bs.cuh -- the reference's Biot-Savart segment kernels in FP64, split into a
 // per-(target, vertex) part and a per-(target, filament) part so that chains of
-// filaments can share vertex work.  The arithmetic of each filament is that of
-// aero/utils.py:580-648.
+// filaments can share vertex work.  The formulas of each filament are those of
+// aero/utils.py:580-648; the quotients are formed as products with one reciprocal square
+// root per vertex and one division per filament (the FP64 divide and square root are
+// multi-instruction sequences on the FP64 pipe), and the cutoff kernel's radial distance
+// from the filament line is computed as the reference computes it.
 #pragma once
 
 #include "fj_common.cuh"
@@ -21,22 +24,12 @@ __device__ __forceinline__ void vtx64(const double x[3], double yx, double yy, d
     o.d[1] = x[1] - yy;
     o.d[2] = x[2] - yz;
     const double n2 = o.d[0] * o.d[0] + o.d[1] * o.d[1] + o.d[2] * o.d[2];
-    if (KER == FJ_KERNEL_PLAIN) {
-        const double nr = sqrt(n2);  // r / jnp.linalg.norm(r), aero/utils.py:591
-        o.u[0] = o.d[0] / nr;
-        o.u[1] = o.d[1] / nr;
-        o.u[2] = o.d[2] / nr;
-    } else if (KER == FJ_KERNEL_CUTOFF) {
-        const double nr = sqrt(n2 + kEps * kEps);  // make_unit_epsilon, aero/utils.py:603
-        o.u[0] = o.d[0] / nr;
-        o.u[1] = o.d[1] / nr;
-        o.u[2] = o.d[2] / nr;
-    } else {
-        const double inv = rsqrt(n2 + kEps * kEps);  // aero/utils.py:617-618
-        o.u[0] = o.d[0] * inv;
-        o.u[1] = o.d[1] * inv;
-        o.u[2] = o.d[2] * inv;
-    }
+    // r / jnp.linalg.norm(r) (plain, aero/utils.py:591); r / ||r||_eps (make_unit_epsilon,
+    // :603, and the epsilon kernel's rsqrt, :617-618)
+    const double inv = rsqrt(KER == FJ_KERNEL_PLAIN ? n2 : n2 + kEps * kEps);
+    o.u[0] = o.d[0] * inv;
+    o.u[1] = o.d[1] * inv;
+    o.u[2] = o.d[2] * inv;
 }
 
 template <int KER>
@@ -61,16 +54,17 @@ __device__ __forceinline__ void link64(const Vtx64<KER>& a, const Vtx64<KER>& b,
         const double mx = a.d[0] - sm * r0x, my = a.d[1] - sm * r0y, mz = a.d[2] - sm * r0z;
         const double r2 = mx * mx + my * my + mz * mz;
         if (r2 > rc2) {
-            acc[0] += (cx / c2 / kFourPi * dot) * g;
-            acc[1] += (cy / c2 / kFourPi * dot) * g;
-            acc[2] += (cz / c2 / kFourPi * dot) * g;
+            const double val = dot / (kFourPi * c2);
+            acc[0] += (cx * val) * g;
+            acc[1] += (cy * val) * g;
+            acc[2] += (cz * val) * g;
         }
     } else {
         // aero/utils.py:587-592
-        const double den = c2 * 4.0 * kPi;
-        acc[0] += (cx / den * dot) * g;
-        acc[1] += (cy / den * dot) * g;
-        acc[2] += (cz / den * dot) * g;
+        const double val = dot / (c2 * 4.0 * kPi);
+        acc[0] += (cx * val) * g;
+        acc[1] += (cy * val) * g;
+        acc[2] += (cz * val) * g;
     }
 }
 
