@@ -208,35 +208,52 @@ __global__ void unpack_gamma_kernel(UnpackArgs u, const double* __restrict__ el,
 // ------------------------------------------------------------------------------------
 constexpr int kTBlk = 64;
 
+// The diagonal block [i0, i0 + bw) of the factors comes into shared memory as it lies in
+// memory (row-major, every element's cp.async in flight at once); one warp substitutes,
+// lane l holding x of rows l and l + 32 in registers and x_j reaching every lane by a
+// shuffle, reading the block transposed.  Per row the operations are those of the
+// column-by-column transposed substitution, in its order.
 __global__ void __launch_bounds__(kTBlk) trsv_t_diag_kernel(const double* __restrict__ lu, int n, int i0, int bw,
                                                             bool upper_of_lt, double* __restrict__ x) {
     // upper_of_lt == false: solve with U^T (lower, diagonal U[j][j]) forward
     // upper_of_lt == true:  solve with L^T (upper, unit diagonal) backward
-    __shared__ double blk[kTBlk][kTBlk + 1];
-    __shared__ double xs[kTBlk];
+    static_assert(kTBlk == 64, "two rows per lane");
+    __shared__ __align__(16) double blk[kTBlk][kTBlk + 1];  // blk[j][r] = lu[i0 + j][i0 + r]
     for (int idx = threadIdx.x; idx < bw * bw; idx += blockDim.x) {
-        const int r = idx / bw, c = idx % bw;
-        blk[r][c] = lu[(int64_t)(i0 + c) * n + i0 + r];  // transposed
+        const int j = idx / bw, r = idx % bw;
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(&blk[j][r])),
+                     "l"(lu + (int64_t)(i0 + j) * n + i0 + r)
+                     : "memory");
     }
-    const int r = threadIdx.x;
-    if (r < bw) xs[r] = x[i0 + r];
+    asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    const unsigned full = 0xffffffffu;
+    double v0 = lane < bw ? x[i0 + lane] : 0.0;
+    double v1 = lane + 32 < bw ? x[i0 + lane + 32] : 0.0;
     if (!upper_of_lt) {
+#pragma unroll 1
         for (int j = 0; j < bw; ++j) {
-            if (r == j) xs[j] = xs[j] / blk[j][j];
-            __syncthreads();
-            const double xj = xs[j];
-            if (r > j && r < bw) xs[r] -= blk[r][j] * xj;
-            __syncthreads();
+            const bool hi = j >= 32;
+            if (lane == (j & 31)) {
+                if (hi) v1 = v1 / blk[j][j];
+                else v0 = v0 / blk[j][j];
+            }
+            const double xj = __shfl_sync(full, hi ? v1 : v0, j & 31);
+            if (lane > j && lane < bw) v0 -= blk[j][lane] * xj;
+            if (lane + 32 > j && lane + 32 < bw) v1 -= blk[j][lane + 32] * xj;
         }
     } else {
+#pragma unroll 1
         for (int j = bw - 1; j >= 0; --j) {
-            const double xj = xs[j];
-            if (r < j) xs[r] -= blk[r][j] * xj;
-            __syncthreads();
+            const double xj = __shfl_sync(full, j >= 32 ? v1 : v0, j & 31);
+            if (lane < j) v0 -= blk[j][lane] * xj;
+            if (lane + 32 < j) v1 -= blk[j][lane + 32] * xj;
         }
     }
-    if (r < bw) x[i0 + r] = xs[r];
+    if (lane < bw) x[i0 + lane] = v0;
+    if (lane + 32 < bw) x[i0 + lane + 32] = v1;
 }
 
 // x[i] -= sum_{j in [j0, j0+bw)} lu[j][i] x[j] for i in [r0, r1)
