@@ -1159,8 +1159,8 @@ static int launch_panel_cluster(float* a, int n, int k, int kb, int32_t* piv, in
 
 // U12 = L11^-1 A12 for the mixed factorisation's outer panel at column k (kb <= 128
 // rows, L11 unit lower from the factored panel), in place on the columns [c0, n).  A CTA
-// takes 16 columns: L11 and the columns' panel rows come into shared memory (coalesced),
-// then warp w substitutes columns 2w and 2w + 1, lane l holding rows l + 32 q (q < 4) in
+// of 16 warps takes 16 columns: L11 and the columns' panel rows come into shared memory
+// (coalesced), then warp w substitutes column w, lane l holding rows l + 32 q (q < 4) in
 // registers, each x_j reaching every lane by a shuffle.  Forward substitution in FP32,
 // as the CUDA-core path's lu_swap_trsm_kernel computes its U rows.
 constexpr int kTrsmCols = 16;
@@ -1170,7 +1170,9 @@ __device__ __forceinline__ float pick4f(const float (&v)[4], int q) {
     return q == 0 ? v[0] : q == 1 ? v[1] : q == 2 ? v[2] : v[3];
 }
 
-__global__ void __launch_bounds__(256) lu_trsm32_kernel(float* __restrict__ a, int n, int k, int kb, int c0) {
+constexpr int kTrsmThreads = 32 * kTrsmCols;
+
+__global__ void __launch_bounds__(kTrsmThreads) lu_trsm32_kernel(float* __restrict__ a, int n, int k, int kb, int c0) {
     extern __shared__ __align__(16) float smt[];
     float* ls = smt;                               // [128][129]
     float* xs = smt + kTcBlk * (kTcBlk + 1);       // [128][17]
@@ -1186,9 +1188,8 @@ __global__ void __launch_bounds__(256) lu_trsm32_kernel(float* __restrict__ a, i
     }
     __syncthreads();
     const unsigned full = 0xffffffffu;
-#pragma unroll 1
-    for (int t = 0; t < 2; ++t) {
-        const int cc = 2 * warp + t;
+    {
+        const int cc = warp;
         float x[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) x[q] = xs[(lane + 32 * q) * (kTrsmCols + 1) + cc];
@@ -1255,7 +1256,8 @@ static int lu_factor32_tc_impl(float* a, int n, int32_t* piv, int* d_info, int* 
         const int rest = n - ke;
         if (rest > 0) {  // U12 = L11^-1 A12 (CUDA cores), then A22 -= L21 U12 (tensor cores)
             float* a12 = a + (int64_t)k * n + ke;
-            lu_trsm32_kernel<<<(unsigned)((rest + kTrsmCols - 1) / kTrsmCols), 256, kTrsm32Smem, s>>>(a, n, k, kb, ke);
+            lu_trsm32_kernel<<<(unsigned)((rest + kTrsmCols - 1) / kTrsmCols), kTrsmThreads, kTrsm32Smem, s>>>(a, n, k,
+                                                                                                          kb, ke);
             note_launch();
             FJ_TRY(tc_mul(a + (int64_t)ke * n + k, n, a12, n, a + (int64_t)ke * n + ke, n, rest, rest, kb, -1.0f, 1.0f,
                           passes, tri_l, n, d_err, s));
@@ -1346,8 +1348,10 @@ constexpr int kDB = 64;
 // lands on a row < k + kb, or on a pivot row at or below k + kb.  For the columns outside
 // the panel each CTA (32 columns, one per lane) loads every moved value before it stores
 // any.  Then, for the CTA's columns right of the panel, the kb x kb unit-lower L11 solves
-// its rows k .. k + kb: warp w takes columns 4w .. 4w + 3, lane l rows l and l + 32.
-__global__ void __launch_bounds__(256)
+// its rows k .. k + kb: warp w (of 16) takes columns 2w and 2w + 1, lane l rows l and l + 32.
+constexpr int kSwapTrsm64Warps = 16;
+
+__global__ void __launch_bounds__(32 * kSwapTrsm64Warps)
     lu_swap_trsm64_kernel(double* __restrict__ a, int n, int k, int kb, const int32_t* __restrict__ piv,
                           int do_swaps, const int* __restrict__ run_flag) {
     if (run_flag != nullptr && *run_flag == 0) return;
@@ -1399,10 +1403,10 @@ __global__ void __launch_bounds__(256)
         __syncthreads();
         const int cnt = s_cnt;
         const bool col = c < n && (c < k || c >= k + kb);
-        for (int e = warp; e < cnt; e += 8)
+        for (int e = warp; e < cnt; e += kSwapTrsm64Warps)
             if (col) tile[e * 32 + lane] = a[(int64_t)s_src[e] * n + c];
         __syncthreads();
-        for (int e = warp; e < cnt; e += 8)
+        for (int e = warp; e < cnt; e += kSwapTrsm64Warps)
             if (col) a[(int64_t)s_dst[e] * n + c] = tile[e * 32 + lane];
         __syncthreads();  // the CTA's stores are seen by its loads below
     }
@@ -1418,8 +1422,8 @@ __global__ void __launch_bounds__(256)
     }
     __syncthreads();
 #pragma unroll 1
-    for (int t = 0; t < 4; ++t) {
-        const int cc = warp * 4 + t;
+    for (int t = 0; t < 2; ++t) {
+        const int cc = warp * 2 + t;
         double x0 = xs[lane * 33 + cc], x1 = xs[(lane + 32) * 33 + cc];
 #pragma unroll 4
         for (int j = 0; j < kb - 1; ++j) {
@@ -1549,8 +1553,8 @@ int lu_factor64(double* a, int n, int32_t* piv, int* d_info, cudaStream_t s, con
             FJ_TRY(lu_outer_panel_narrow64<2>(a, n, k, ke, piv, d_info, run_flag, s));
         }
         if (n > kb) {
-            lu_swap_trsm64_kernel<<<(unsigned)((n + 31) / 32), 256, st_smem, s>>>(a, n, k, kb, piv, cluster ? 1 : 0,
-                                                                                    run_flag);
+            lu_swap_trsm64_kernel<<<(unsigned)((n + 31) / 32), 32 * kSwapTrsm64Warps, st_smem, s>>>(
+                a, n, k, kb, piv, cluster ? 1 : 0, run_flag);
             note_launch();
         }
         const int rest = n - ke;
