@@ -158,9 +158,12 @@ struct StepCase {
     double polar_scale;     // polar_circulation_scale
 };
 
+// Also clears the lattice-changed flag that k_changed sets later in the step (nothing in
+// between reads it).
 __global__ void k_time(const StepCase* __restrict__ T) {
     const StepCase& C = T[blockIdx.y];
     if (threadIdx.x == 0 && C.advance_time && C.i > 0) C.t[C.i] = C.t[C.i - 1] + C.dt;  // uvlm.py:1158-1161
+    if (threadIdx.x == 0 && C.changed != nullptr) *C.changed = 0;
 }
 
 // hg_to_zeta_b / hg_dot_to_zeta_b_dot (aero/uvlm.py:537-621), one thread per vertex.
@@ -465,11 +468,6 @@ __global__ void static_gamma_w_kernel(Layout L, const double* __restrict__ gamma
 }
 
 // Mixed path: flag a lattice that differs (bitwise) from the one of the cached AIC.
-__global__ void k_clear_changed(const StepCase* __restrict__ T) {
-    const StepCase& C = T[blockIdx.y];
-    if (threadIdx.x == 0 && C.changed != nullptr) *C.changed = 0;
-}
-
 __global__ void k_changed(const StepCase* __restrict__ T) {
     const StepCase& C = T[blockIdx.y];
     if (C.changed == nullptr) return;
@@ -1681,7 +1679,6 @@ static int run_steps(std::vector<BatchItem>& items, char* d_tab, size_t tab_byte
     }
     // 3. AIC (mixed: only where the lattice changed since the factorisation)
     if (any_changed) {
-        k_clear_changed<<<dim3(1, K), 32, 0, s>>>(dC); note_launch();
         k_changed<<<dim3(nblk(max_v * 3), K), b, 0, s>>>(dC); note_launch();
     }
     FJ_TRY(aic_launch_jobs((const AicArgs*)(d_tab + tl.aic), K, max_n, max_fil, any_mirror, kernel, s));
